@@ -1,0 +1,155 @@
+/*
+ * wrfgpu.h -- C ABI of the B200-native split-explicit ARW RK3 dycore step.
+ *
+ * This replaces wrf_gpu's ``_rk_scan_step(carry, namelist, *, debug,
+ * lead_seconds, physics_tendencies, capture_pre_halo)``
+ * (src/gpuwrf/runtime/operational_mode.py:3319-3534): one full RK3 step --
+ * flux-form advection, large-step PGF/Coriolis, small_step_prep, the acoustic
+ * substep loop (advance_uv, advance_mu_t, advance_w with its tridiagonal
+ * solve, calc_p_rho) and small_step_finish -- on device arrays.
+ *
+ * Conventions (the reference's data contract, contracts/state.py:82-206 and
+ * contracts/grid.py:66-126):
+ *   - every array is float64, C order (k, j, i), i fastest, contiguous;
+ *   - u: (nz, ny, nx+1); v: (nz, ny+1, nx); w, ph, ww: (nz+1, ny, nx);
+ *     mass fields: (nz, ny, nx); 2-D fields: (ny, nx);
+ *   - map factors msfux/msfuy: (ny, nx+1); msfvx/msfvy: (ny+1, nx);
+ *     msftx/msfty, f, e, sina, cosa: (ny, nx);
+ *   - specified boundary strips u_bdy/v_bdy: (ntime, 4, width, nz, side_len)
+ *     with sides W, E, S, N (contracts/state.py:96-106).
+ *
+ * Ownership: inputs are const device pointers, outputs caller-allocated
+ * device pointers that must not alias any input; scratch is one
+ * caller-provided workspace of wrfgpu_step_workspace_size() bytes.  Every
+ * entry point takes a cudaStream_t and never synchronises, allocates or reads
+ * device memory from the host, so a step can be captured in a CUDA graph.
+ *
+ * Errors: the reference raises at trace time for unsupported static
+ * configurations (e.g. core/calc_p_rho.py:119-122); here every call returns
+ * an int status, 0 on success, and wrfgpu_last_error_string() describes the
+ * last failure of the calling thread.
+ */
+#ifndef WRFGPU_H
+#define WRFGPU_H
+
+#include <stddef.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WRFGPU_OK 0
+#define WRFGPU_ERR_UNSUPPORTED_CONFIG 1
+#define WRFGPU_ERR_BAD_SHAPE 2
+#define WRFGPU_ERR_CUDA 3
+#define WRFGPU_ERR_NULL_POINTER 4
+#define WRFGPU_ERR_WORKSPACE 5
+
+#define WRFGPU_PRECISION_FP64 0
+#define WRFGPU_PRECISION_MIXED 1
+
+#define WRFGPU_NMOIST 6 /* qv, qc, qr, qi, qs, qg (operational_mode.py:3095) */
+
+/* Static step controls: the OperationalNamelist fields the step reads
+ * (runtime/operational_mode.py:410-700).  Fill with wrfgpu_step_params_init()
+ * first; its defaults equal the reference dataclass defaults. */
+typedef struct wrfgpu_step_params {
+  int nx, ny, nz;
+  double dx, dy;               /* grid.projection.dx_m / dy_m */
+  double dt;                   /* namelist.dt_s */
+  int acoustic_substeps;       /* namelist.acoustic_substeps */
+  double epssm;                /* namelist.epssm (0.1) */
+  int top_lid;                 /* namelist.top_lid */
+  int w_damping;               /* 0 | 1 */
+  int damp_opt;                /* 0 | 3 */
+  double dampcoef, zdamp;
+  int hypsometric_opt;         /* 1 (linear) | 2 (log) */
+  int h_sca_adv_order;         /* rhs_ph horizontal order; <= 2 supported */
+  int scalar_adv_opt;          /* theta limiter: 0 | 1 (PD) | 2 (mono) */
+  int moist_adv_opt;           /* moisture advection: 0 (off) | 1 | 2 */
+  int run_boundary;            /* namelist.run_boundary */
+  int bc_ideal;                /* grid.bc.source == "ideal" */
+  int spec_zone, relax_zone;   /* boundary_config (1, 4) */
+  double update_cadence_s;     /* boundary_config.update_cadence_s */
+  double normal_bdy_relax_strength; /* <0 selects the reference default 20 */
+  int moist_cqw;               /* GPUWRF_MOIST_CQW (default on) */
+  int w_coriolis;              /* GPUWRF_W_CORIOLIS (default on) */
+  int precision;               /* WRFGPU_PRECISION_FP64 | _MIXED */
+  /* scalar metrics (DycoreMetrics.cf1/cf2/cf3/p_top) */
+  double cf1, cf2, cf3, p_top;
+  /* top-face extrapolation weights of the large-step PGF
+   * (core/rk_addtend_dry.py:282-288): cfn = (0.5*dnw[nz-1] + dn[nz-1])/dn[nz-1],
+   * cfn1 = -0.5*dnw[nz-1]/dn[nz-1] */
+  double cfn, cfn1;
+} wrfgpu_step_params;
+
+/* DycoreMetrics device arrays (contracts/grid.py:66-126). */
+typedef struct wrfgpu_metrics {
+  const double *c1h, *c2h, *c3h, *c4h;      /* (nz)   */
+  const double *c1f, *c2f, *c3f, *c4f;      /* (nz+1) */
+  const double *dn, *dnw, *rdn, *rdnw, *fnm, *fnp; /* (nz) */
+  const double *msftx, *msfty;              /* (ny, nx)   */
+  const double *msfux, *msfuy;              /* (ny, nx+1) */
+  const double *msfvx, *msfvy;              /* (ny+1, nx) */
+  const double *f, *e, *sina, *cosa;        /* (ny, nx)   */
+} wrfgpu_metrics;
+
+/* Step inputs: the OperationalCarry leaves the step reads
+ * (runtime/operational_state.py:30-127). */
+typedef struct wrfgpu_step_inputs {
+  const double *u, *v, *w, *theta;
+  const double *p_total, *p_perturbation, *ph_total, *ph_perturbation;
+  const double *mu_total, *mu_perturbation;
+  const double *q[WRFGPU_NMOIST];   /* may be NULL (dry: treated as zero) */
+  const double *mudf;               /* carry.mudf (ny, nx) */
+  /* namelist.tendencies base leaves, NULL = zero (the reference default) */
+  const double *base_u, *base_v, *base_w, *base_theta, *base_mu;
+  /* specified lateral boundary strips; NULL unless run_boundary */
+  const double *u_bdy, *v_bdy;
+  int bdy_ntime, bdy_width, bdy_side_len;
+} wrfgpu_step_inputs;
+
+/* Step outputs: the returned OperationalCarry (operational_mode.py:2234-2265). */
+typedef struct wrfgpu_step_outputs {
+  double *u, *v, *w, *theta;
+  double *p_total, *p_perturbation, *ph_total, *ph_perturbation;
+  double *mu_total, *mu_perturbation;
+  double *q[WRFGPU_NMOIST];         /* written when the input q is non-NULL */
+  double *t_2ave, *ww, *mudf, *muave, *muts, *ph_tend;
+  double *u_save, *v_save, *w_save, *t_save, *ph_save, *mu_save, *ww_save;
+} wrfgpu_step_outputs;
+
+/* Fill params with the reference defaults (no grid).  Replaces
+ * OperationalNamelist defaults (runtime/operational_mode.py:410-700). */
+int wrfgpu_step_params_init(wrfgpu_step_params *params);
+
+/* Check params against what this build supports; 0 when supported.
+ * Mirrors the reference's trace-time ValueError/NotImplementedError. */
+int wrfgpu_step_params_validate(const wrfgpu_step_params *params);
+
+/* Workspace bytes one wrfgpu_rk3_step call needs for these params. */
+int wrfgpu_step_workspace_size(const wrfgpu_step_params *params, size_t *bytes);
+
+/* One RK3 dycore step.  Replaces _rk_scan_step
+ * (runtime/operational_mode.py:3319-3534).  lead_seconds is the forecast
+ * clock at step start (NaN = None); it only selects the boundary strip time. */
+int wrfgpu_rk3_step(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                    const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
+                    double lead_seconds, void *workspace, size_t workspace_bytes,
+                    cudaStream_t stream);
+
+/* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
+int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
+
+/* Last error of the calling host thread ("" when none). */
+const char *wrfgpu_last_error_string(void);
+
+/* Library version string. */
+const char *wrfgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WRFGPU_H */

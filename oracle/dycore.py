@@ -1,0 +1,1252 @@
+"""NumPy float64 restatement of wrf_gpu's RK3 split-explicit dycore step.
+
+TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).  Arrays are ``(k, j, i)``
+C-order; u lives on ``(nz, ny, nx+1)`` x-faces, v on ``(nz, ny+1, nx)``
+y-faces, w/ph on ``(nz+1, ny, nx)`` full levels, 2-D fields are ``(ny, nx)``.
+Reference paths below are relative to ``src/gpuwrf``.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field, replace
+from types import SimpleNamespace
+
+import numpy as np
+
+# --- constants: dynamics/acoustic_wrf.py:27-75, core/advance_w.py:28,87-88,
+#     runtime/operational_mode.py:202, core/acoustic.py:846-847, calc_p_rho.py:24
+R_D = 287.0
+CP_D = 7.0 * R_D / 2.0
+P0 = 100000.0
+CPOVCV = CP_D / (CP_D - R_D)
+CVPM = -(CP_D - R_D) / CP_D
+G = 9.81
+T0 = 300.0
+MIN_ACOUSTIC_ALT = 0.1
+W_RERADIUS = 1.0 / 6370.0e3
+W_ALPHA = 0.3
+W_BETA = 1.0
+PD_EPS = 1.0e-20
+EMDIV = 0.01
+SMDIV = 0.1
+MIN_MUTS_FRACTION = 0.5
+MIN_MUTS_PA = 1.0
+NORMAL_BDY_RELAX_STRENGTH = 20.0
+MOIST_SPECIES = ("qv", "qc", "qr", "qi", "qs", "qg")
+SIDES = ("W", "E", "S", "N")
+
+
+# ----------------------------------------------------------------------------
+# containers
+# ----------------------------------------------------------------------------
+
+@dataclass
+class Namelist:
+    """The ``OperationalNamelist`` fields the step reads (operational_mode.py:410-700)."""
+
+    metrics: SimpleNamespace
+    dx: float
+    dy: float
+    dt_s: float = 10.0
+    acoustic_substeps: int = 10
+    epssm: float = 0.1
+    top_lid: bool = False
+    w_damping: int = 0
+    damp_opt: int = 0
+    dampcoef: float = 0.0
+    zdamp: float = 5000.0
+    hypsometric_opt: int = 1
+    h_sca_adv_order: int = 2
+    scalar_adv_opt: int = 0
+    moist_adv_opt: int = 0
+    run_boundary: bool = False
+    bc_ideal: bool = True
+    spec_zone: int = 1
+    relax_zone: int = 4
+    update_cadence_s: float = 3600.0
+    normal_bdy_relax_strength: float | None = None
+    moist_cqw: bool = True          # GPUWRF_MOIST_CQW default (operational_mode.py:219)
+    w_coriolis: bool = True         # GPUWRF_W_CORIOLIS default (operational_mode.py:1793)
+    base_tend: dict | None = None   # namelist.tendencies u/v/w/theta/mu (zero when None)
+
+
+def lateral_flags(nl: Namelist):
+    """``_acoustic_lateral_bc_flags`` (operational_mode.py:1247-1254); force_geopotential=True."""
+    if not (nl.run_boundary and not nl.bc_ideal):
+        return True, False, False
+    return False, True, False
+
+
+def copy_state(s: SimpleNamespace) -> SimpleNamespace:
+    return SimpleNamespace(**{k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in vars(s).items()})
+
+
+# ----------------------------------------------------------------------------
+# small helpers
+# ----------------------------------------------------------------------------
+
+def _col(a):
+    return np.asarray(a)[:, None, None]
+
+
+def xpair(f):
+    """Edge-padded x-face pair (core/acoustic.py:544-547)."""
+    left = np.concatenate([f[..., :1], f], axis=-1)
+    right = np.concatenate([f, f[..., -1:]], axis=-1)
+    return left, right
+
+
+def ypair(f):
+    """Edge-padded y-face pair (core/acoustic.py:550-553)."""
+    south = np.concatenate([f[..., :1, :], f], axis=-2)
+    north = np.concatenate([f, f[..., -1:, :]], axis=-2)
+    return south, north
+
+
+def u_face_average_2d(f):
+    """core/small_step_prep.py:75-79."""
+    return np.concatenate((f[:, :1], 0.5 * (f[:, :-1] + f[:, 1:]), f[:, -1:]), axis=1)
+
+
+def v_face_average_2d(f):
+    """core/small_step_prep.py:82-86."""
+    return np.concatenate((f[:1, :], 0.5 * (f[:-1, :] + f[1:, :]), f[-1:, :]), axis=0)
+
+
+def inv_density(theta, p):
+    """dynamics/acoustic_wrf.py:187-206 (qvf = 1)."""
+    return (R_D / P0) * theta * 1.0 * ((np.maximum(p, 1.0) / P0) ** CVPM)
+
+
+def pressure_from_theta_alt(theta, alt):
+    """dynamics/acoustic_wrf.py:209-221 (qvf = 1)."""
+    argument = (R_D * theta * 1.0) / (P0 * np.maximum(alt, 1.0e-8))
+    return P0 * (np.maximum(argument, 1.0e-12) ** CPOVCV)
+
+
+def qtot_of(s):
+    return s.qv + s.qc + s.qr + s.qi + s.qs + s.qg
+
+
+def moisture_coupling_factors(s):
+    """dynamics/acoustic_wrf.py:305-320."""
+    qtot = qtot_of(s)
+    ql, qr = xpair(qtot)
+    qs_, qn = ypair(qtot)
+    return 1.0 / (1.0 + 0.5 * (ql + qr)), 1.0 / (1.0 + 0.5 * (qs_ + qn))
+
+
+# ----------------------------------------------------------------------------
+# flux-form advection: dynamics/flux_advection.py
+# ----------------------------------------------------------------------------
+
+def flux5_face(f, vel, axis):
+    """flux_advection.py:53-88: left-face 5th-order upwind value."""
+    q_im3 = np.roll(f, 3, axis=axis)
+    q_im2 = np.roll(f, 2, axis=axis)
+    q_im1 = np.roll(f, 1, axis=axis)
+    q_ip1 = np.roll(f, -1, axis=axis)
+    q_ip2 = np.roll(f, -2, axis=axis)
+    f6 = (37.0 * (f + q_im1) - 8.0 * (q_ip1 + q_im2) + (q_ip2 + q_im3)) / 60.0
+    corr = ((q_ip2 - q_im3) - 5.0 * (q_ip1 - q_im2) + 10.0 * (f - q_im1)) / 60.0
+    return f6 - np.sign(vel) * corr
+
+
+def couple_velocities_periodic(u, v, mu_total, m, rdx, rdy):
+    """flux_advection.py:394-470 (calc_ww_cp on periodic collapsed faces)."""
+    nz = u.shape[0]
+    ny, nx = mu_total.shape
+    u_f = u[..., :nx]
+    v_f = v[:, :ny, :]
+    msfuy = m.msfuy[:, :nx]
+    msfvx = m.msfvx[:ny, :]
+    muu = 0.5 * (mu_total + np.roll(mu_total, 1, axis=-1))
+    muv = 0.5 * (mu_total + np.roll(mu_total, 1, axis=-2))
+    mass_u = _col(m.c1h) * muu[None] + _col(m.c2h)
+    mass_v = _col(m.c1h) * muv[None] + _col(m.c2h)
+    ru = mass_u * u_f / msfuy[None]
+    rv = mass_v * v_f / msfvx[None]
+    divv = _col(m.dnw) * m.msftx[None] * (rdx * (np.roll(ru, -1, -1) - ru) + rdy * (np.roll(rv, -1, -2) - rv))
+    dmdt = np.sum(divv, axis=0, keepdims=True)
+    inc = -(_col(m.dnw) * _col(m.c1h) * dmdt) - divv
+    cum = np.cumsum(inc, axis=0)
+    rom = np.zeros((nz + 1, ny, nx))
+    rom[1:nz] = cum[: nz - 1]
+    return SimpleNamespace(ru=ru, rv=rv, rom=rom, msftx=m.msftx, msfux=m.msfux[:, :nx],
+                           msfvy=m.msfvy[:ny, :], msfvx=msfvx)
+
+
+def stage_omega_specified(u, v, mu_total, m, rdx, rdy):
+    """flux_advection.py:180-232 (edge-faithful calc_ww_cp)."""
+    nz = u.shape[0]
+    ny, nx = mu_total.shape
+    mpx = np.pad(mu_total, ((0, 0), (1, 0)), mode="edge")
+    muu = 0.5 * (mpx[:, 1:] + mpx[:, :-1])
+    muu = np.concatenate([muu, mu_total[:, -1:]], axis=1)
+    mpy = np.pad(mu_total, ((1, 0), (0, 0)), mode="edge")
+    muv = 0.5 * (mpy[1:, :] + mpy[:-1, :])
+    muv = np.concatenate([muv, mu_total[-1:, :]], axis=0)
+    c1 = _col(m.c1h)
+    c2 = _col(m.c2h)
+    ru = (c1 * muu[None] + c2) * u / m.msfuy[None]
+    rv = (c1 * muv[None] + c2) * v / m.msfvx[None]
+    divv = m.msftx[None] * _col(m.dnw) * (rdx * (ru[:, :, 1:] - ru[:, :, :-1]) + rdy * (rv[:, 1:, :] - rv[:, :-1, :]))
+    dmdt = np.sum(divv, axis=0, keepdims=True)
+    inc = -(_col(m.dnw) * _col(m.c1h) * dmdt) - divv
+    cum = np.cumsum(inc, axis=0)
+    rom = np.zeros((nz + 1, ny, nx))
+    rom[1:nz] = cum[: nz - 1]
+    return rom
+
+
+def _vflux_scalar(f, rom, fzm, fzp):
+    """flux_advection.py:534-562 / 678-711 (order-3 vertical flux, rigid ends)."""
+    nz = f.shape[0]
+    vflux = np.zeros((nz + 1,) + f.shape[1:])
+    q_km2, q_km1, q_k, q_kp1 = f[: nz - 3], f[1 : nz - 2], f[2 : nz - 1], f[3:nz]
+    velz = -rom[2 : nz - 1]
+    flux4 = (7.0 * (q_k + q_km1) - (q_kp1 + q_km2)) / 12.0
+    corr = ((q_kp1 - q_km2) - 3.0 * (q_k - q_km1)) / 12.0
+    vflux[2 : nz - 1] = rom[2 : nz - 1] * (flux4 + np.sign(velz) * corr)
+    vflux[1] = rom[1] * (fzm[1] * f[1] + fzp[1] * f[0])
+    vflux[nz - 1] = rom[nz - 1] * (fzm[nz - 1] * f[nz - 1] + fzp[nz - 1] * f[nz - 2])
+    return vflux
+
+
+def advect_scalar_flux(f, vel, rdx, rdy, rdzw, fzm, fzp):
+    """flux_advection.py:482-568 (h5/v3 periodic)."""
+    msftx = vel.msftx[None]
+    fqx = vel.ru * flux5_face(f, vel.ru, 2)
+    tend = -msftx * rdx * (np.roll(fqx, -1, 2) - fqx)
+    fqy = vel.rv * flux5_face(f, vel.rv, 1)
+    tend = tend - msftx * rdy * (np.roll(fqy, -1, 1) - fqy)
+    nz = f.shape[0]
+    vflux = _vflux_scalar(f, vel.rom, fzm, fzp)
+    return tend - _col(rdzw) * (vflux[1:] - vflux[:nz])
+
+
+def _flux_upwind_face(fo, vel, mu_face, dxy, dt, axis):
+    """flux_advection.py:614-641."""
+    q_im1 = np.roll(fo, 1, axis=axis)
+    cr = vel * dt / dxy / mu_face
+    a = np.abs(cr)
+    return mu_face * (dxy / dt) * (0.5 * np.minimum(1.0, cr + a) * q_im1 + 0.5 * np.maximum(-1.0, cr - a) * fo)
+
+
+def _flux_upwind_face_z(fo, rom, mu_h, rdzw, dt):
+    """flux_advection.py:644-675."""
+    nz = fo.shape[0]
+    out = np.zeros((nz + 1,) + fo.shape[1:])
+    q_km1, q_k = fo[: nz - 1], fo[1:nz]
+    dz = 2.0 / (_col(rdzw[1:nz]) + _col(rdzw[: nz - 1]))
+    mu_face = 0.5 * (mu_h[1:nz] + mu_h[: nz - 1])
+    cr = rom[1:nz] * dt / dz / mu_face
+    a = np.abs(cr)
+    out[1:nz] = mu_face * (dz / dt) * (0.5 * np.minimum(1.0, cr + a) * q_km1 + 0.5 * np.maximum(-1.0, cr - a) * q_k)
+    return out
+
+
+def advect_scalar_flux_limited(f, fo, vel, opt, mut, mu_old, m, rdx, rdy, dt):
+    """flux_advection.py:736-1000 (PD opt 1 / monotonic opt 2, periodic path)."""
+    nz = f.shape[0]
+    msftx = vel.msftx[None]
+    rdzw = m.rdnw
+    c1, c2 = _col(m.c1h), _col(m.c2h)
+    mu_h = c1 * mut[None] + c2
+    muu = 0.5 * (mut + np.roll(mut, 1, -1))
+    muv = 0.5 * (mut + np.roll(mut, 1, -2))
+    mu_u = c1 * muu[None] + c2
+    mu_v = c1 * muv[None] + c2
+    dx, dy = 1.0 / rdx, 1.0 / rdy
+    fqxl = _flux_upwind_face(fo, vel.ru, mu_u, dx, dt, 2)
+    fqyl = _flux_upwind_face(fo, vel.rv, mu_v, dy, dt, 1)
+    fqzl = _flux_upwind_face_z(fo, vel.rom, mu_h, rdzw, dt)
+    fqx = vel.ru * flux5_face(f, vel.ru, 2) - fqxl
+    fqy = vel.rv * flux5_face(f, vel.rv, 1) - fqyl
+    fqz = _vflux_scalar(f, vel.rom, m.fnm, m.fnp) - fqzl
+    mass_old = c1 * mu_old[None] + c2
+    div_low = (msftx * msftx * (rdx * (np.roll(fqxl, -1, 2) - fqxl) + rdy * (np.roll(fqyl, -1, 1) - fqyl))
+               + msftx * _col(rdzw) * (fqzl[1:] - fqzl[:nz]))
+    ph_low = mass_old * fo - dt * div_low
+    fqx_ip1 = np.roll(fqx, -1, 2)
+    fqy_jp1 = np.roll(fqy, -1, 1)
+    fqz_kp1, fqz_k = fqz[1:], fqz[:nz]
+    pos = lambda a: np.maximum(0.0, a)
+    neg = lambda a: np.minimum(0.0, a)
+    flux_out = dt * (msftx * msftx * (rdx * (pos(fqx_ip1) - neg(fqx)) + rdy * (pos(fqy_jp1) - neg(fqy)))
+                     + msftx * _col(rdzw) * (neg(fqz_kp1) - pos(fqz_k)))
+    if opt == 1:
+        scale = np.where(flux_out > ph_low, np.maximum(0.0, ph_low / (flux_out + PD_EPS)), 1.0)
+        sx = np.roll(scale, 1, 2)
+        sy = np.roll(scale, 1, 1)
+        fqx_lim = np.where(fqx > 0.0, sx * fqx, np.where(fqx < 0.0, scale * fqx, fqx))
+        fqy_lim = np.where(fqy > 0.0, sy * fqy, np.where(fqy < 0.0, scale * fqy, fqy))
+        sp = np.concatenate((scale[:1], scale, scale[-1:]), axis=0)
+        fqz_lim = np.where(fqz < 0.0, sp[0 : nz + 1] * fqz, np.where(fqz > 0.0, sp[1 : nz + 2] * fqz, fqz))
+    elif opt == 2:
+        qmax, qmin = fo, fo
+        for ax in (2, 1):
+            a1, a2 = np.roll(fo, 1, axis=ax), np.roll(fo, -1, axis=ax)
+            qmax = np.maximum(qmax, np.maximum(a1, a2))
+            qmin = np.minimum(qmin, np.minimum(a1, a2))
+        up = np.concatenate((fo[:1], fo[:-1]), axis=0)
+        dn = np.concatenate((fo[1:], fo[-1:]), axis=0)
+        qmax = np.maximum(qmax, np.maximum(up, dn))
+        qmin = np.minimum(qmin, np.minimum(up, dn))
+        flux_in = -dt * (msftx * msftx * (rdx * (neg(fqx_ip1) - pos(fqx)) + rdy * (neg(fqy_jp1) - pos(fqy)))
+                         + msftx * _col(rdzw) * (pos(fqz_kp1) - neg(fqz_k)))
+        ph_hi = qmax * mass_old - ph_low
+        ph_lo = ph_low - qmin * mass_old
+        s_in = np.where(flux_in > ph_hi, np.maximum(0.0, ph_hi / (flux_in + PD_EPS)), 1.0)
+        s_out = np.where(flux_out > ph_lo, np.maximum(0.0, ph_lo / (flux_out + PD_EPS)), 1.0)
+        fqx_lim = np.where(fqx > 0.0, np.minimum(s_in, np.roll(s_out, 1, 2)) * fqx,
+                           np.minimum(s_out, np.roll(s_in, 1, 2)) * fqx)
+        fqy_lim = np.where(fqy > 0.0, np.minimum(s_in, np.roll(s_out, 1, 1)) * fqy,
+                           np.minimum(s_out, np.roll(s_in, 1, 1)) * fqy)
+        sip = np.concatenate((s_in[:1], s_in, s_in[-1:]), axis=0)
+        sop = np.concatenate((s_out[:1], s_out, s_out[-1:]), axis=0)
+        fqz_lim = np.where(fqz < 0.0, np.minimum(sip[1 : nz + 2], sop[0 : nz + 1]) * fqz,
+                           np.minimum(sop[1 : nz + 2], sip[0 : nz + 1]) * fqz)
+    else:
+        raise ValueError(f"limiter option {opt} unsupported")
+    fx = fqx_lim + fqxl
+    fy = fqy_lim + fqyl
+    fz = fqz_lim + fqzl
+    tend = -msftx * rdx * (np.roll(fx, -1, 2) - fx)
+    tend = tend - msftx * rdy * (np.roll(fy, -1, 1) - fy)
+    return tend - _col(rdzw) * (fz[1:] - fz[:nz])
+
+
+def _vdiv3(f, romq, rdzw, fzm, fzp):
+    """flux_advection.py:1362-1407 (u/v vertical flux divergence, -sign(vel) correction)."""
+    nz = f.shape[0]
+    vflux = np.zeros((nz + 1,) + f.shape[1:])
+    q_km2, q_km1, q_k, q_kp1 = f[: nz - 3], f[1 : nz - 2], f[2 : nz - 1], f[3:nz]
+    rk = romq[2 : nz - 1]
+    flux4 = (7.0 * (q_k + q_km1) - (q_kp1 + q_km2)) / 12.0
+    corr = ((q_kp1 - q_km2) - 3.0 * (q_k - q_km1)) / 12.0
+    vflux[2 : nz - 1] = rk * (flux4 + np.sign(-rk) * corr)
+    vflux[1] = romq[1] * (fzm[1] * f[1] + fzp[1] * f[0])
+    vflux[nz - 1] = romq[nz - 1] * (fzm[nz - 1] * f[nz - 1] + fzp[nz - 1] * f[nz - 2])
+    return -_col(rdzw) * (vflux[1:] - vflux[:nz])
+
+
+def _vdiv_w(w, rom, rdn, top_lid):
+    """flux_advection.py:1410-1482 (vertical flux divergence of w)."""
+    nz = w.shape[0] - 1
+    vel = 0.5 * (rom + np.roll(rom, 1, axis=0))
+    vflux = np.zeros_like(w)
+
+    def f3(k):
+        q_km2, q_km1, q_k, q_kp1 = w[k - 2], w[k - 1], w[k], w[k + 1]
+        flux4 = (7.0 * (q_k + q_km1) - (q_kp1 + q_km2)) / 12.0
+        corr = ((q_kp1 - q_km2) - 3.0 * (q_k - q_km1)) / 12.0
+        return vel[k] * (flux4 + np.sign(-vel[k]) * corr)
+
+    for k in range(3, nz):
+        vflux[k] = f3(k)
+    vflux[1] = vel[1] * 0.5 * (w[1] + w[0])
+    vflux[2] = f3(2)
+    vflux[nz - 1] = f3(nz - 1)
+    if not top_lid:
+        vflux[nz] = vel[nz] * 0.5 * (w[nz] + w[nz - 1])
+    tend = np.zeros_like(w)
+    tend[1:nz] = -_col(rdn[1:nz]) * (vflux[2 : nz + 1] - vflux[1:nz])
+    if not top_lid:
+        tend[nz] = tend[nz] + 2.0 * rdn[nz - 1] * vflux[nz]
+    return tend
+
+
+def advect_u_flux(u, vel, rdx, rdy, m):
+    """flux_advection.py:1131-1202 (periodic path)."""
+    nx = vel.ru.shape[-1]
+    ny = u.shape[1]
+    u_f = u[..., :nx]
+    msfux = vel.msfux[None]
+    velx = 0.5 * (vel.ru + np.roll(vel.ru, 1, -1))
+    fqx = velx * flux5_face(u_f, velx, 2)
+    tend = -msfux * rdx * (np.roll(fqx, -1, 2) - fqx)
+    if ny > 1:
+        vely = 0.5 * (vel.rv + np.roll(vel.rv, 1, -1))
+        fqy = vely * flux5_face(u_f, vely, 1)
+        tend = tend - msfux * rdy * (np.roll(fqy, -1, 1) - fqy)
+    tend = tend + _vdiv3(u_f, 0.5 * (vel.rom + np.roll(vel.rom, 1, -1)), m.rdnw, m.fnm, m.fnp)
+    return np.concatenate((tend, tend[:, :, :1]), axis=2)
+
+
+def advect_v_flux(v, vel, rdx, rdy, m):
+    """flux_advection.py:1205-1274 (periodic path)."""
+    ny = vel.rv.shape[-2]
+    v_f = v[:, :ny, :]
+    msfvy = vel.msfvy[None]
+    msfvx = vel.msfvx[None]
+    ru_c = vel.ru[:, :ny, :]
+    velx = 0.5 * (ru_c + np.roll(ru_c, 1, -2))
+    fqx = velx * flux5_face(v_f, velx, 2)
+    tend = -msfvy * rdx * (np.roll(fqx, -1, 2) - fqx)
+    vely = 0.5 * (vel.rv + np.roll(vel.rv, 1, -2))
+    fqy = vely * flux5_face(v_f, vely, 1)
+    tend = tend - msfvy * rdy * (np.roll(fqy, -1, 1) - fqy)
+    tend = tend + (msfvy / msfvx) * _vdiv3(v_f, 0.5 * (vel.rom + np.roll(vel.rom, 1, -2)), m.rdnw, m.fnm, m.fnp)
+    return np.concatenate((tend, tend[:, :1, :]), axis=1)
+
+
+def _mass_to_full(f, fzm, fzp):
+    """flux_advection.py:1332-1352."""
+    nz = f.shape[0]
+    out = np.zeros((nz + 1,) + f.shape[1:])
+    out[1:nz] = _col(fzm[1:nz]) * f[1:nz] + _col(fzp[1:nz]) * f[: nz - 1]
+    out[0] = f[0]
+    out[nz] = f[nz - 1]
+    return out
+
+
+def advect_w_flux(w, vel, rdx, rdy, m, top_lid):
+    """flux_advection.py:1277-1329 (periodic path)."""
+    msftx = vel.msftx[None]
+    ru_w = _mass_to_full(vel.ru, m.fnm, m.fnp)
+    rv_w = _mass_to_full(vel.rv, m.fnm, m.fnp)
+    fqx = ru_w * flux5_face(w, ru_w, 2)
+    tend = -msftx * rdx * (np.roll(fqx, -1, 2) - fqx)
+    if w.shape[1] > 1:
+        fqy = rv_w * flux5_face(w, rv_w, 1)
+        tend = tend - msftx * rdy * (np.roll(fqy, -1, 1) - fqy)
+    return tend + _vdiv_w(w, vel.rom, m.rdn, top_lid)
+
+
+# ----------------------------------------------------------------------------
+# large-step PGF / Coriolis: dynamics/core/rk_addtend_dry.py
+# ----------------------------------------------------------------------------
+
+def _log_alpha(dph, mass_col, m):
+    p_top = float(m.p_top)
+    pfu = _col(m.c3f[1:]) * mass_col + _col(m.c4f[1:]) + p_top
+    pfd = _col(m.c3f[:-1]) * mass_col + _col(m.c4f[:-1]) + p_top
+    phm = _col(m.c3h) * mass_col + _col(m.c4h) + p_top
+    return dph / phm / np.log(pfd / pfu)
+
+
+def absolute_diagnostics(s, m, hyps):
+    """rk_addtend_dry.py:127-230 (base_state None)."""
+    mub = s.mu_total - s.mu_perturbation
+    alt = inv_density(s.theta, s.p_total)
+    p_pert = s.p_perturbation
+    phb = s.ph_total - s.ph_perturbation
+    mass_base = _col(m.c1h) * mub[None] + _col(m.c2h)
+    safe_base = np.where(np.abs(mass_base) > 1.0e-12, mass_base, 1.0e-12)
+    alb = -_col(m.rdnw) * (phb[1:] - phb[:-1]) / safe_base
+    if hyps == 2:
+        dph_tot = (phb[1:] + s.ph_perturbation[1:]) - (phb[:-1] + s.ph_perturbation[:-1])
+        al = _log_alpha(dph_tot, s.mu_total[None], m) - _log_alpha(phb[1:] - phb[:-1], mub[None], m)
+    else:
+        muts = s.mu_total + s.mu_perturbation
+        mass_t = _col(m.c1h) * muts[None] + _col(m.c2h)
+        safe_t = np.where(np.abs(mass_t) > 1.0e-12, mass_t, 1.0e-12)
+        mu_term = _col(m.c1h) * s.mu_perturbation[None]
+        al = -(alb * mu_term + _col(m.rdnw) * (s.ph_perturbation[1:] - s.ph_perturbation[:-1])) / safe_t
+    pht = phb + s.ph_perturbation
+    php = 0.5 * (pht[:-1] + pht[1:])
+    return s.ph_perturbation, p_pert, al, alt, php
+
+
+def _cfn(m):
+    dn_top = m.dn[-1]
+    dn_safe = dn_top if abs(dn_top) > 1.0e-30 else 1.0
+    return (0.5 * m.dnw[-1] + m.dn[-1]) / dn_safe, -0.5 * m.dnw[-1] / dn_safe
+
+
+def large_step_horizontal_pgf(s, m, rdx, rdy, top_lid, hyps):
+    """rk_addtend_dry.py:233-362."""
+    ph, p_abs, al, alt, php = absolute_diagnostics(s, m, hyps)
+    pb = s.p_total - s.p_perturbation
+    mub = s.mu_total - s.mu_perturbation
+    mu_pert = s.mu_perturbation
+    cqu, cqv = moisture_coupling_factors(s)
+    c1h, c2h, rdnw = _col(m.c1h), _col(m.c2h), _col(m.rdnw)
+    msf_u = (m.msfux / m.msfuy)[None]
+    msf_v = (m.msfvy / m.msfvx)[None]
+    mu_total = mub + mu_pert
+    cfn, cfn1 = _cfn(m)
+
+    def dpn_faces(ps):
+        nz = ps.shape[0]
+        dpn = np.zeros((nz + 1,) + ps.shape[1:])
+        dpn[0] = 0.5 * (m.cf1 * ps[0] + m.cf2 * ps[1] + m.cf3 * ps[2])
+        dpn[1:nz] = 0.5 * (_col(m.fnm[1:]) * ps[1:] + _col(m.fnp[1:]) * ps[:-1])
+        if top_lid:
+            dpn[nz] = 0.5 * (cfn * ps[-1] + cfn1 * ps[-2])
+        return dpn
+
+    ph_l, ph_r = xpair(ph)
+    p_l, p_r = xpair(p_abs)
+    pb_l, pb_r = xpair(pb)
+    al_l, al_r = xpair(al)
+    alt_l, alt_r = xpair(alt)
+    a, b = xpair(mu_total)
+    muu = 0.5 * (a + b)
+    mass_u = c1h * muu[None] + c2h
+    dpx = msf_u * 0.5 * rdx * mass_u * (((ph_r[1:] - ph_l[1:]) + (ph_r[:-1] - ph_l[:-1]))
+                                        + (alt_l + alt_r) * (p_r - p_l) + (al_l + al_r) * (pb_r - pb_l))
+    php_l, php_r = xpair(php)
+    dpn = dpn_faces(p_l + p_r)
+    mu_l, mu_r = xpair(mu_pert)
+    bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_l + mu_r)[None])
+    dpx = dpx + msf_u * rdx * (php_r - php_l) * bracket
+
+    ph_s, ph_n = ypair(ph)
+    p_s, p_n = ypair(p_abs)
+    pb_s, pb_n = ypair(pb)
+    al_s, al_n = ypair(al)
+    alt_s, alt_n = ypair(alt)
+    a, b = ypair(mu_total)
+    muv = 0.5 * (a + b)
+    mass_v = c1h * muv[None] + c2h
+    dpy = msf_v * 0.5 * rdy * mass_v * (((ph_n[1:] - ph_s[1:]) + (ph_n[:-1] - ph_s[:-1]))
+                                        + (alt_s + alt_n) * (p_n - p_s) + (al_s + al_n) * (pb_n - pb_s))
+    php_s, php_n = ypair(php)
+    dpn = dpn_faces(p_s + p_n)
+    mu_s, mu_n = ypair(mu_pert)
+    bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_s + mu_n)[None])
+    dpy = dpy + msf_v * rdy * (php_n - php_s) * bracket
+    return -cqu * dpx, -cqv * dpy
+
+
+def large_step_coriolis(s, m, specified):
+    """rk_addtend_dry.py:364-484."""
+    c1h, c2h, c1f, c2f = _col(m.c1h), _col(m.c2h), _col(m.c1f), _col(m.c2f)
+    a, b = xpair(s.mu_total)
+    muu = 0.5 * (a + b)
+    a, b = ypair(s.mu_total)
+    muv = 0.5 * (a + b)
+    ru = s.u * (c1h * muu[None] + c2h) / m.msfuy[None]
+    rv = s.v * (c1h * muv[None] + c2h) / m.msfvx[None]
+    rw = s.w * (c1f * s.mu_total[None] + c2f) / m.msfty[None]
+
+    def xavg(f):
+        a, b = xpair(f)
+        return 0.5 * (a + b)
+
+    def yavg(f):
+        a, b = ypair(f)
+        return 0.5 * (a + b)
+
+    f_u, e_u, cosa_u = xavg(m.f), xavg(m.e), xavg(m.cosa)
+    f_v, e_v, sina_v = yavg(m.f), yavg(m.e), yavg(m.sina)
+    msf_u = (m.msfux / m.msfuy)[None]
+    msf_v = (m.msfvy / m.msfvx)[None]
+    rv_im1, rv_i = xpair(rv)
+    rv_quad = 0.25 * (rv_im1[:, :-1, :] + rv_i[:, :-1, :] + rv_im1[:, 1:, :] + rv_i[:, 1:, :])
+    ru_cor = msf_u * f_u[None] * rv_quad
+    rw_im1, rw_i = xpair(rw)
+    rw_u = 0.25 * (rw_im1[:-1] + rw_im1[1:] + rw_i[:-1] + rw_i[1:])
+    ru_cor = ru_cor - e_u[None] * cosa_u[None] * rw_u
+    if specified:
+        ru_cor[:, :, 0] *= 0.0
+        ru_cor[:, :, -1] *= 0.0
+    ru_jm1, ru_j = ypair(ru)
+    ru_quad = 0.25 * (ru_jm1[:, :, :-1] + ru_jm1[:, :, 1:] + ru_j[:, :, :-1] + ru_j[:, :, 1:])
+    rv_cor = -msf_v * f_v[None] * ru_quad
+    rw_jm1, rw_j = ypair(rw)
+    rw_v = 0.25 * (rw_jm1[:-1] + rw_jm1[1:] + rw_j[:-1] + rw_j[1:])
+    rv_cor = rv_cor + msf_v * e_v[None] * sina_v[None] * rw_v
+    if specified:
+        rv_cor[:, 0, :] *= 0.0
+        rv_cor[:, -1, :] *= 0.0
+    return ru_cor, rv_cor
+
+
+# ----------------------------------------------------------------------------
+# large-step tendency assembly: runtime/operational_mode.py:2722-3093, 3162-3316
+# ----------------------------------------------------------------------------
+
+def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step):
+    """operational_mode.py:2722-3093 (flux advection on, diffusion off, physics off)."""
+    m = nl.metrics
+    rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
+    c1h, c2h, c1f, c2f = _col(m.c1h), _col(m.c2h), _col(m.c1f), _col(m.c2f)
+    bt = nl.base_tend or {}
+    muu = u_face_average_2d(s.mu_total)
+    muv = v_face_average_2d(s.mu_total)
+    mass_u = c1h * muu[None] + c2h
+    mass_v = c1h * muv[None] + c2h
+    mass_h = c1h * s.mu_total[None] + c2h
+    mass_f = c1f * s.mu_total[None] + c2f
+    nz, ny, nx = s.theta.shape
+    bu = bt.get("u", np.zeros((nz, ny, nx + 1)))
+    bv = bt.get("v", np.zeros((nz, ny + 1, nx)))
+    bw = bt.get("w", np.zeros((nz + 1, ny, nx)))
+    bth = bt.get("theta", np.zeros((nz, ny, nx)))
+    bmu = bt.get("mu", np.zeros((ny, nx)))
+    u_t = bu * mass_u + advect_u_flux(s.u, vel, rdx, rdy, m)
+    v_t = bv * mass_v + advect_v_flux(s.v, vel, rdx, rdy, m)
+    w_t = bw * mass_f + advect_w_flux(s.w, vel, rdx, rdy, m, nl.top_lid)
+    use_lim = nl.scalar_adv_opt in (1, 2) and rk_step == 3
+    if use_lim:
+        adv = advect_scalar_flux_limited(s.theta - T0, origin.theta - T0, vel, nl.scalar_adv_opt,
+                                         s.mu_total, origin.mu_total, m, rdx, rdy, nl.dt_s)
+    else:
+        adv = advect_scalar_flux(s.theta - T0, vel, rdx, rdy, m.rdnw, m.fnm, m.fnp)
+    th_t = bth * mass_h + adv
+    ru_pgf, rv_pgf = large_step_horizontal_pgf(s, m, rdx, rdy, nl.top_lid, nl.hypsometric_opt)
+    u_t = u_t + ru_pgf
+    v_t = v_t + rv_pgf
+    ru_cor, rv_cor = large_step_coriolis(s, m, bool(nl.run_boundary))
+    u_t = u_t + ru_cor
+    v_t = v_t + rv_cor
+    return SimpleNamespace(u=u_t, v=v_t, w=w_t, theta=th_t, mu=bmu.copy())
+
+
+def moisture_coupled_tendencies(s, origin, vel, nl: Namelist, rk_step):
+    """operational_mode.py:3162-3237 -> flux_advection.py:1002-1100."""
+    m = nl.metrics
+    rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
+    use_lim = nl.moist_adv_opt in (1, 2) and rk_step == 3
+    out = []
+    for name in MOIST_SPECIES:
+        q = getattr(s, name)
+        if use_lim:
+            out.append(advect_scalar_flux_limited(q, getattr(origin, name), vel, nl.moist_adv_opt,
+                                                  s.mu_total, origin.mu_total, m, rdx, rdy, nl.dt_s))
+        else:
+            out.append(advect_scalar_flux(q, vel, rdx, rdy, m.rdnw, m.fnm, m.fnp))
+    return out
+
+
+# ----------------------------------------------------------------------------
+# small step prep / calc_p_rho / coefficients
+# ----------------------------------------------------------------------------
+
+def small_step_prep(s, ref, rk_step, m, ww):
+    """core/small_step_prep.py:216-394 (base_state None)."""
+    c1h, c2h, c1f, c2f = _col(m.c1h), _col(m.c2h), _col(m.c1f), _col(m.c2f)
+    theta_ref = ref.theta - T0
+    theta_cur = s.theta - T0
+    mub = s.mu_total - s.mu_perturbation
+    mu_cur = s.mu_perturbation
+    mu_ref = ref.mu_perturbation
+    mu_work = np.zeros_like(mu_cur) if rk_step == 1 else mu_ref - mu_cur
+    mut = mub + mu_cur
+    muts = mut + mu_work
+    muu, muv = u_face_average_2d(mut), v_face_average_2d(mut)
+    muus, muvs = u_face_average_2d(muts), v_face_average_2d(muts)
+    mass_u_ref, mass_u_cur = c1h * muus[None] + c2h, c1h * muu[None] + c2h
+    mass_v_ref, mass_v_cur = c1h * muvs[None] + c2h, c1h * muv[None] + c2h
+    mass_h_ref, mass_h_cur = c1h * muts[None] + c2h, c1h * mut[None] + c2h
+    mass_f_ref, mass_f_cur = c1f * muts[None] + c2f, c1f * mut[None] + c2f
+    p = SimpleNamespace()
+    p.rk_step = rk_step
+    p.u_work = (mass_u_ref * ref.u - mass_u_cur * s.u) / m.msfuy[None]
+    p.v_work = (mass_v_ref * ref.v - mass_v_cur * s.v) / m.msfvx[None]
+    p.theta_work = mass_h_ref * theta_ref - mass_h_cur * theta_cur
+    p.w_work = (mass_f_ref * ref.w - mass_f_cur * s.w) / m.msfty[None]
+    p.ph_work = ref.ph_perturbation - s.ph_perturbation
+    alt = inv_density(s.theta, s.p_total)
+    p.p_pert = s.p_perturbation
+    p.pb = s.p_total - s.p_perturbation
+    p.alt = np.maximum(alt, MIN_ACOUSTIC_ALT)
+    p.c2a = CPOVCV * (p.pb + p.p_pert) / p.alt
+    p.cqu, p.cqv = moisture_coupling_factors(s)
+    p.phb = s.ph_total - s.ph_perturbation
+    ph = s.ph_perturbation
+    p.php = 0.5 * (p.phb[:-1] + p.phb[1:] + ph[:-1] + ph[1:])
+    p.ww_save = ww.copy()
+    p.theta_1 = theta_ref
+    p.ph_1 = ref.ph_perturbation
+    p.u_save, p.v_save, p.w_save = s.u, s.v, s.w
+    p.t_save = theta_cur
+    p.ph_save = s.ph_perturbation
+    p.mu_save = mu_cur
+    p.mub, p.mut, p.muts, p.mu_work = mub, mut, muts, mu_work
+    p.muu, p.muv, p.muus, p.muvs = muu, muv, muus, muvs
+    return p
+
+
+def calc_al_p(mu_work, muts, ph_work, theta_work, theta_1, c2a, alt, m):
+    """core/calc_p_rho.py:52-101."""
+    mass_h = _col(m.c1h) * muts[None] + _col(m.c2h)
+    safe = np.where(np.abs(mass_h) > 1.0e-12, mass_h, 1.0e-12)
+    mu_term = _col(m.c1h) * mu_work[None]
+    al = -(alt * mu_term + _col(m.rdnw) * (ph_work[1:] - ph_work[:-1])) / safe
+    ttr = T0 + theta_1
+    sttr = np.where(np.abs(ttr) > 1.0e-6, ttr, 1.0e-6)
+    pp = c2a * (alt * (theta_work - mu_term * theta_1) / (safe * sttr) - al)
+    return al, pp
+
+
+def calc_coef_w(mut, m, dts, epssm, top_lid, cqw, c2a):
+    """dynamics/acoustic_wrf.py:783-852."""
+    nz = m.c1h.shape[0]
+    ny, nx = mut.shape
+    mass_h = _col(m.c1h) * mut[None] + _col(m.c2h)
+    mass_f = _col(m.c1f) * mut[None] + _col(m.c2f)
+    rdn, rdnw = m.rdn, m.rdnw
+    cof = (0.5 * dts * G * (1.0 + epssm)) ** 2
+    lid = 0.0 if top_lid else 1.0
+    a = np.zeros((nz + 1, ny, nx))
+    alpha = np.ones((nz + 1, ny, nx))
+    gamma = np.zeros((nz + 1, ny, nx))
+    a[nz] = -2.0 * cof * rdnw[nz - 1] ** 2 * c2a[nz - 1] * lid / (mass_h[nz - 1] * mass_f[nz - 1])
+    for kk in range(2, nz):
+        k = kk - 1
+        a[kk] = -cqw[kk] * cof * rdn[kk] * rdnw[kk - 1] * c2a[kk - 1] / (mass_h[k] * mass_f[k])
+    for k in range(1, nz):
+        b = 1.0 + cqw[k] * cof * rdn[k] * (rdnw[k] * c2a[k] / (mass_h[k] * mass_f[k])
+                                           + rdnw[k - 1] * c2a[k - 1] / (mass_h[k - 1] * mass_f[k]))
+        c = -cqw[k] * cof * rdn[k] * rdnw[k] * c2a[k] / (mass_h[k] * mass_f[k + 1])
+        alpha[k] = 1.0 / (b - a[k] * gamma[k - 1])
+        gamma[k] = c * alpha[k]
+    b_top = 1.0 + 2.0 * cof * rdnw[nz - 1] ** 2 * c2a[nz - 1] / (mass_h[nz - 1] * mass_f[nz])
+    alpha[nz] = 1.0 / (b_top - a[nz] * gamma[nz - 1])
+    gamma[nz] = 0.0
+    return a, alpha, gamma
+
+
+def pg_buoy_w_moist(p, mu_prime, mub, qtot, m):
+    """core/advance_w.py:195-290 (moist form; identical to dry when qtot == 0)."""
+    nz = p.shape[0]
+    cqw_calc = np.zeros((nz + 1,) + p.shape[1:])
+    cqw_calc[1:nz] = 0.5 * (qtot[1:nz] + qtot[: nz - 1])
+    minv = (1.0 / m.msfty)[None]
+    rw = np.zeros_like(cqw_calc)
+    cqw = np.zeros_like(cqw_calc)
+    ci = cqw_calc[1:nz]
+    cq1 = 1.0 / (1.0 + ci)
+    cq2 = ci * cq1
+    rw[1:nz] = minv * G * (cq1 * _col(m.rdn[1:nz]) * (p[1:nz] - p[: nz - 1]) - _col(m.c1f[1:nz]) * mu_prime[None]
+                           - cq2 * (_col(m.c1f[1:nz]) * mub[None] + _col(m.c2f[1:nz])))
+    cqw[1:nz] = cq1
+    ct = cqw_calc[nz - 1]
+    c1t = 1.0 / (1.0 + ct)
+    c2t = ct * c1t
+    rw[nz] = minv[0] * G * (c1t * 2.0 * m.rdnw[nz - 1] * (-p[nz - 1]) - m.c1f[nz] * mu_prime - c2t * (m.c1f[nz] * mub + m.c2f[nz]))
+    return rw, cqw
+
+
+def pg_buoy_w_dry(p, mu_prime, m):
+    """core/advance_w.py:146-192."""
+    nz = p.shape[0]
+    minv = (1.0 / m.msfty)[None]
+    rw = np.zeros((nz + 1,) + p.shape[1:])
+    rw[1:nz] = minv * G * (_col(m.rdn[1:nz]) * (p[1:nz] - p[: nz - 1]) - _col(m.c1f[1:nz]) * mu_prime[None])
+    rw[nz] = minv[0] * G * (2.0 * m.rdnw[nz - 1] * (-p[nz - 1]) - m.c1f[nz] * mu_prime)
+    cqw = np.zeros_like(rw)
+    cqw[1:nz] = 1.0
+    return rw, cqw
+
+
+def rhs_ph_order2(u, v, ww, ph, phb, w, mut, muu, muv, m, rdx, rdy, top_lid):
+    """core/rhs_ph.py:175-401 (advective_order <= 2 periodic path)."""
+    nz = ph.shape[0] - 1
+    pht = ph + phb
+    minv = (1.0 / m.msfty)[None]
+    out = np.zeros_like(ph)
+    dphi = pht[1:] - pht[:-1]
+    wdwn = 0.5 * (ww[1:] + ww[:-1]) * _col(m.rdnw) * dphi
+    term3 = _col(m.fnm[1:nz]) * wdwn[1:nz] + _col(m.fnp[1:nz]) * wdwn[: nz - 1]
+    out[1:nz] = out[1:nz] + (-term3)
+    mass_f = _col(m.c1f) * mut[None] + _col(m.c2f)
+    gw = mass_f * G * w * minv
+    out[1:nz] = out[1:nz] + gw[1:nz]
+    out[nz] = 0.0 if top_lid else gw[nz]
+    c1f_int = _col(m.c1f[1:nz])
+    c2f_int = _col(m.c2f[1:nz])
+    v_pair = v[1:nz] + v[: nz - 1]
+    muvf = c1f_int * muv[None] + c2f_int
+    pti = pht[1:nz]
+    dn_ = np.roll(pti, -1, -2) - pti
+    ds_ = pti - np.roll(pti, 1, -2)
+    flux_y = muvf[:, 1:, :] * v_pair[:, 1:, :] * dn_ + muvf[:, :-1, :] * v_pair[:, :-1, :] * ds_
+    out[1:nz] = out[1:nz] + (-(0.25 * rdy * minv) * flux_y)
+    u_pair = u[1:nz] + u[: nz - 1]
+    muuf = c1f_int * muu[None] + c2f_int
+    de_ = np.roll(pti, -1, -1) - pti
+    dw_ = pti - np.roll(pti, 1, -1)
+    flux_x = muuf[:, :, 1:] * u_pair[:, :, 1:] * de_ + muuf[:, :, :-1] * u_pair[:, :, :-1] * dw_
+    out[1:nz] = out[1:nz] + (-(0.25 * rdx * minv) * flux_x)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# lateral boundary in-step pieces: coupling/boundary_apply.py
+# ----------------------------------------------------------------------------
+
+def interpolate_boundary_leaf(leaf, lead_seconds, cadence):
+    """boundary_apply.py:329-345."""
+    mx = leaf.shape[0] - 1
+    li = float(lead_seconds) / float(cadence)
+    lo = int(np.clip(np.floor(li), 0, mx))
+    hi = int(np.clip(lo + 1, 0, mx))
+    a = float(np.clip(li - lo, 0.0, 1.0))
+    return leaf[lo] * (1.0 - a) + leaf[hi] * a
+
+
+def _strip(forcing, side, b, z_len, side_len):
+    """boundary_apply.py:528-549."""
+    sv = forcing[SIDES.index(side)]
+    b = min(max(int(b), 0), sv.shape[0] - 1)
+    return sv[b, :z_len, :side_len]
+
+
+def normal_bdy_work_target_u(strip, u_save, mass_cur, mass_stage, msfuy, nzone):
+    """boundary_apply.py:729-758."""
+    z, y, x = u_save.shape
+    t = np.zeros_like(u_save)
+    for b in range(nzone):
+        ws, es = _strip(strip, "W", b, z, y), _strip(strip, "E", b, z, y)
+        cw, ce = b, x - 1 - b
+        t[:, :, cw] = (ws * mass_stage[:, :, cw] - u_save[:, :, cw] * mass_cur[:, :, cw]) / msfuy[:, cw][None]
+        t[:, :, ce] = (es * mass_stage[:, :, ce] - u_save[:, :, ce] * mass_cur[:, :, ce]) / msfuy[:, ce][None]
+    return t
+
+
+def normal_bdy_work_target_v(strip, v_save, mass_cur, mass_stage, msfvx, nzone):
+    """boundary_apply.py:761-781."""
+    z, y, x = v_save.shape
+    t = np.zeros_like(v_save)
+    for b in range(nzone):
+        ss, ns = _strip(strip, "S", b, z, x), _strip(strip, "N", b, z, x)
+        rs, rn = b, y - 1 - b
+        t[:, rs, :] = (ss * mass_stage[:, rs, :] - v_save[:, rs, :] * mass_cur[:, rs, :]) / msfvx[rs, :][None]
+        t[:, rn, :] = (ns * mass_stage[:, rn, :] - v_save[:, rn, :] * mass_cur[:, rn, :]) / msfvx[rn, :][None]
+    return t
+
+
+def normal_relax_weights(y_len, x_len, sub_ratio, axis, spec_zone=1, relax_zone=4):
+    """boundary_apply.py:803-855 (DEFAULT_BOUNDARY_CONFIG spec/relax widths)."""
+    w = np.zeros((y_len, x_len))
+    for b in range(spec_zone):
+        if axis == "u":
+            w[:, b] = 1.0
+            w[:, x_len - 1 - b] = 1.0
+        else:
+            w[b, :] = 1.0
+            w[y_len - 1 - b, :] = 1.0
+    for b in range(spec_zone, relax_zone):
+        linear = max(0.0, (spec_zone + relax_zone - (b + 1)) / float(relax_zone - 1)) if relax_zone > 1 else 0.0
+        weight = min(1.0, max(0.0, sub_ratio * 0.1 * linear))
+        if axis == "u":
+            w[b + 1 : y_len - b - 1, b] = weight
+            w[b + 1 : y_len - b - 1, x_len - 1 - b] = weight
+        else:
+            w[b, b : x_len - b] = weight
+            w[y_len - 1 - b, b : x_len - b] = weight
+    return w[None]
+
+
+# ----------------------------------------------------------------------------
+# acoustic substep: core/acoustic.py, dynamics/mu_t_advance.py, core/advance_w.py
+# ----------------------------------------------------------------------------
+
+def _dpn_acoustic(ps, m, top_lid):
+    """core/acoustic.py:563-580."""
+    nz = ps.shape[0]
+    dpn = np.zeros((nz + 1,) + ps.shape[1:])
+    dpn[0] = 0.5 * (m.cf1 * ps[0] + m.cf2 * ps[1] + m.cf3 * ps[2])
+    dpn[1:nz] = 0.5 * (_col(m.fnm[1:]) * ps[1:] + _col(m.fnp[1:]) * ps[:-1])
+    if top_lid:
+        dpn[nz] = 0.5 * (m.cf1 * ps[-1] + m.cf2 * ps[-2] + m.cf3 * ps[-3])
+    return dpn
+
+
+def advance_uv(a, m, dts, rdx, rdy, dx, dy, top_lid, bdy=None):
+    """core/acoustic.py:626-786 (emdiv = 0.01)."""
+    u = a.u + dts * a.u_tend
+    v = a.v + dts * a.v_tend
+    c1h, c2h, rdnw = _col(m.c1h), _col(m.c2h), _col(m.rdnw)
+    ph_l, ph_r = xpair(a.ph)
+    p_l, p_r = xpair(a.p)
+    pb_l, pb_r = xpair(a.pb)
+    al_l, al_r = xpair(a.al)
+    alt_l, alt_r = xpair(a.alt)
+    mass_x = c1h * a.muu[None] + c2h
+    dpx = (m.msfux / m.msfuy)[None] * 0.5 * rdx * mass_x * (((ph_r[1:] - ph_l[1:]) + (ph_r[:-1] - ph_l[:-1]))
+                                                             + (alt_l + alt_r) * (p_r - p_l) + (al_l + al_r) * (pb_r - pb_l))
+    php_l, php_r = xpair(a.php)
+    dpn = _dpn_acoustic(p_l + p_r, m, top_lid)
+    mu_work = a.muts - a.mut
+    mu_l, mu_r = xpair(mu_work)
+    bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_l + mu_r)[None])
+    dpx = dpx + (m.msfux / m.msfuy)[None] * rdx * (php_r - php_l) * bracket
+    u = u - dts * a.cqu * dpx
+    md_l, md_r = xpair(a.mudf)
+    u = u + c1h * (-EMDIV * dx * (md_r - md_l) / m.msfuy)[None]
+
+    ph_s, ph_n = ypair(a.ph)
+    p_s, p_n = ypair(a.p)
+    pb_s, pb_n = ypair(a.pb)
+    al_s, al_n = ypair(a.al)
+    alt_s, alt_n = ypair(a.alt)
+    mass_y = c1h * a.muv[None] + c2h
+    dpy = (m.msfvy / m.msfvx)[None] * 0.5 * rdy * mass_y * (((ph_n[1:] - ph_s[1:]) + (ph_n[:-1] - ph_s[:-1]))
+                                                             + (alt_s + alt_n) * (p_n - p_s) + (al_s + al_n) * (pb_n - pb_s))
+    php_s, php_n = ypair(a.php)
+    dpn = _dpn_acoustic(p_s + p_n, m, top_lid)
+    mu_s, mu_n = ypair(mu_work)
+    bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_s + mu_n)[None])
+    dpy = dpy + (m.msfvy / m.msfvx)[None] * rdy * (php_n - php_s) * bracket
+    v = v - dts * a.cqv * dpy
+    md_s, md_n = ypair(a.mudf)
+    v = v + c1h * (-EMDIV * dy * (md_n - md_s) * (1.0 / m.msfvx))[None]
+    if bdy is not None:
+        u = u + bdy.wu * (bdy.u_target - u)
+        v = v + bdy.wv * (bdy.v_target - v)
+    a.u, a.v = u, v
+
+
+def advance_mu_t(a, m, dts, rdx, rdy, epssm, specified):
+    """dynamics/mu_t_advance.py:131-292 (periodic) and :295-451 (specified)."""
+    nz = a.theta_work.shape[0]
+    ny, nx = a.mu.shape
+    msfvx_inv = 1.0 / m.msfvx
+    if specified:
+        y0, y1, x0, x1 = 1, ny - 1, 1, nx - 1
+    else:
+        y0, y1, x0, x1 = 0, ny, 0, nx
+    ys, xs = slice(y0, y1), slice(x0, x1)
+    ysn, xse = slice(y0 + 1, y1 + 1), slice(x0 + 1, x1 + 1)
+    msftx, msfty = m.msftx[ys, xs], m.msfty[ys, xs]
+    dvdxi = np.zeros((nz, y1 - y0, x1 - x0))
+    for k in range(nz):
+        c1, c2 = m.c1h[k], m.c2h[k]
+        vn = a.v[k, ysn, xs] + (c1 * a.muv[ysn, xs] + c2) * a.v_1[k, ysn, xs] * msfvx_inv[ysn, xs]
+        vs = a.v[k, ys, xs] + (c1 * a.muv[ys, xs] + c2) * a.v_1[k, ys, xs] * msfvx_inv[ys, xs]
+        ue = a.u[k, ys, xse] + (c1 * a.muu[ys, xse] + c2) * a.u_1[k, ys, xse] / m.msfuy[ys, xse]
+        uw = a.u[k, ys, xs] + (c1 * a.muu[ys, xs] + c2) * a.u_1[k, ys, xs] / m.msfuy[ys, xs]
+        dvdxi[k] = msftx * msfty * (rdy * (vn - vs) + rdx * (ue - uw))
+    dmdt = np.sum(_col(m.dnw) * dvdxi, axis=0)
+    mu_work_old = a.muts[ys, xs] - a.mut[ys, xs]
+    mu_save = a.mu[ys, xs] - mu_work_old
+    mu_tend = a.mu_tend[ys, xs]
+    mu_tendency = dmdt + mu_tend
+    if specified:
+        mutc = a.mut[ys, xs]
+        floor = np.maximum(MIN_MUTS_PA, MIN_MUTS_FRACTION * mutc)
+        muts_old = mutc + mu_work_old
+        raw = dts * mu_tendency
+        allowed = np.maximum(muts_old - floor, 0.0)
+        loss = -raw
+        finite = np.isfinite(raw) & np.isfinite(muts_old)
+        scale = np.where(finite & (loss > allowed), allowed / np.maximum(loss, 1.0), np.where(finite, 1.0, 0.0))
+        scale = np.clip(scale, 0.0, 1.0)
+        mu_tendency = mu_tendency * scale
+        dmdt = dmdt * scale
+        dvdxi = dvdxi * scale[None]
+        mu_tend = mu_tend * scale
+    mu_work_new = mu_work_old + dts * mu_tendency
+    a.mu[ys, xs] = mu_save + mu_work_new
+    a.mudf[ys, xs] = mu_tendency
+    a.muts[ys, xs] = a.mut[ys, xs] + mu_work_new
+    a.muave[ys, xs] = 0.5 * ((1.0 + epssm) * mu_work_new + (1.0 - epssm) * mu_work_old)
+    rows = [a.ww[0, ys, xs]]
+    for kk in range(1, nz):
+        k = kk - 1
+        inc = m.dnw[kk - 1] * (m.c1h[k] * dmdt + dvdxi[kk - 1] + m.c1h[k] * mu_tend) / msfty
+        rows.append(rows[-1] - inc)
+    rows.append(a.ww[nz, ys, xs])
+    wwa = np.stack(rows, axis=0)
+    wwa[:nz] = wwa[:nz] - a.ww_1[:nz, ys, xs]
+    a.ww[:, ys, xs] = wwa
+    th1 = a.theta_1
+    theta_i = a.theta_work[:, ys, xs] + msfty[None] * dts * a.theta_tend[:, ys, xs]
+    wdtn = np.zeros((nz + 1, y1 - y0, x1 - x0))
+    for k in range(1, nz):
+        wdtn[k] = wwa[k] * (m.fnm[k] * th1[k, ys, xs] + m.fnp[k] * th1[k - 1, ys, xs])
+    for k in range(nz):
+        th = th1[k]
+        if specified:
+            th_e, th_w = th[ys, x0 + 1 : x1 + 1], th[ys, x0 - 1 : x1 - 1]
+        else:
+            th_e, th_w = np.roll(th, -1, -1)[ys, xs], np.roll(th, 1, -1)[ys, xs]
+        if specified:
+            th_n, th_s = th[y0 + 1 : y1 + 1, xs], th[y0 - 1 : y1 - 1, xs]
+        else:
+            th_n, th_s = np.roll(th, -1, -2)[ys, xs], np.roll(th, 1, -2)[ys, xs]
+        thc = th[ys, xs]
+        v_flux = a.v[k, ysn, xs] * (th_n + thc) - a.v[k, ys, xs] * (thc + th_s)
+        u_flux = a.u[k, ys, xse] * (th_e + thc) - a.u[k, ys, xs] * (thc + th_w)
+        tend = msftx * (0.5 * rdy * v_flux + 0.5 * rdx * u_flux) + m.rdnw[k] * (wdtn[k + 1] - wdtn[k])
+        a.theta_work[k, ys, xs] = theta_i[k] - dts * msfty * tend
+
+
+def advance_w(a, m, nl: Namelist, dts, rdx, rdy):
+    """core/advance_w.py:293-627."""
+    nz = a.w.shape[0] - 1
+    eps_p, eps_m = 1.0 + nl.epssm, 1.0 - nl.epssm
+    minv = (1.0 / m.msfty)[None]
+    c1h, c2h, c1f, c2f = _col(m.c1h), _col(m.c2h), _col(m.c1f), _col(m.c2f)
+    rw_tend = a.rw_tend.copy()
+    w, ww, mut, muts, muave = a.w, a.ww, a.mut, a.muts, a.muave
+    if nl.w_damping == 1:
+        mass_f = _col(m.c1f[1:nz]) * mut[None] + _col(m.c2f[1:nz])
+        safe = np.where(np.abs(mass_f) > 1.0e-12, mass_f, 1.0e-12)
+        vert_cfl = np.abs(ww[1:nz] / safe * _col(m.rdnw[1:nz]) * dts)
+        damp = -np.sign(w[1:nz]) * W_ALPHA * (vert_cfl - W_BETA) * mass_f
+        damp = np.where(vert_cfl > W_BETA, damp, 0.0)
+        rw_tend[1:nz] = rw_tend[1:nz] + damp
+    mass_h = c1h * muts[None] + c2h
+    t2a = (0.5 * (eps_p * a.theta_work + eps_m * a.t_2ave) + (c1h * muave[None]) * T0) / (mass_h * (T0 + a.theta_1))
+    rhs = np.zeros_like(w)
+    rhs[1:] = dts * (a.ph_tend[1:] + 0.5 * G * eps_m * w[1:])
+    pt1 = a.ph_1 + a.phb
+    wdwn = np.zeros_like(w)
+    wdwn[1:] = 0.5 * (ww[1:] + ww[:-1]) * _col(m.rdnw) * (pt1[1:] - pt1[:-1])
+    rhs[1:nz] = rhs[1:nz] + (-(dts * (_col(m.fnm[1:nz]) * wdwn[2:] + _col(m.fnp[1:nz]) * wdwn[1:nz])))
+    mass_f_mut = c1f * mut[None] + c2f
+    rhs[1:] = a.ph[1:] + m.msfty[None] * rhs[1:] / mass_f_mut[1:]
+    if nl.top_lid:
+        rhs[nz] = 0.0
+    ht = a.phb[0] / G
+    htp = np.pad(ht, ((0, 1), (0, 0)), mode="edge")
+    htm = np.pad(ht, ((1, 0), (0, 0)), mode="edge")
+    dy_n = htp[1:, :] - ht
+    dy_s = ht - htm[:-1, :]
+    htp = np.pad(ht, ((0, 0), (0, 1)), mode="edge")
+    htm = np.pad(ht, ((0, 0), (1, 0)), mode="edge")
+    dx_e = htp[:, 1:] - ht
+    dx_w = ht - htm[:, :-1]
+    cf = lambda f3: m.cf1 * f3[0] + m.cf2 * f3[1] + m.cf3 * f3[2]
+    v1, u1 = a.v_1, a.u_1
+    w_surface = (m.msfty * 0.5 * rdy * (dy_n * cf(v1[:3, 1:, :]) + dy_s * cf(v1[:3, :-1, :]))
+                 + m.msftx * 0.5 * rdx * (dx_e * cf(u1[:3, :, 1:]) + dx_w * cf(u1[:3, :, :-1])))
+    mass_h_mut = c1h * mut[None] + c2h
+    smhm = np.where(np.abs(mass_h_mut) > 1.0e-12, mass_h_mut, 1.0e-12)
+    coef = a.c2a * _col(m.rdnw) / smhm
+    w_next = w + dts * rw_tend
+    ph = a.ph
+    tA_u = coef[1:nz] * (eps_p * (rhs[2 : nz + 1] - rhs[1:nz]) + eps_m * (ph[2 : nz + 1] - ph[1:nz]))
+    tA_l = coef[0 : nz - 1] * (eps_p * (rhs[1:nz] - rhs[0 : nz - 1]) + eps_m * (ph[1:nz] - ph[0 : nz - 1]))
+    tA = minv * a.cqw[1:nz] * (0.5 * dts * G * _col(m.rdn[1:nz])) * (tA_u - tA_l)
+    buoy = a.c2a * a.alt * t2a
+    tB = dts * G * minv * (_col(m.rdn[1:nz]) * (buoy[1:nz] - buoy[0 : nz - 1]) - (_col(m.c1f[1:nz]) * muave[None]))
+    w_next[1:nz] = w_next[1:nz] + (tA + tB)
+    km1 = nz - 1
+    tA_top = (-0.5 * dts * G / smhm[km1] * m.rdnw[km1] ** 2 * 2.0 * a.c2a[km1]
+              * (eps_p * (rhs[nz] - rhs[nz - 1]) + eps_m * (ph[nz] - ph[nz - 1])))
+    tB_top = -dts * G * (2.0 * m.rdnw[km1] * a.c2a[km1] * a.alt[km1] * t2a[km1] + (m.c1f[nz] * muave))
+    w_top = w[nz] + dts * rw_tend[nz] + minv[0] * (tA_top + tB_top)
+    w_next[nz] = 0.0 if nl.top_lid else w_top
+    w_next[0] = w_surface
+    wf = w_next.copy()
+    for k in range(1, nz + 1):
+        wf[k] = (w_next[k] - a.a[k] * wf[k - 1]) * a.alpha[k]
+    ws = wf.copy()
+    for k in range(nz - 1, 0, -1):
+        ws[k] = wf[k] - a.gamma[k] * ws[k + 1]
+    if nl.damp_opt == 3 and nl.dampcoef > 0.0:
+        dampmag = dts * nl.dampcoef
+        hdepth = nl.zdamp
+        ptd = a.ph_1 + a.phb
+        htop = ptd[nz] / G
+        hk = ptd / G
+        hbot = (htop - hdepth)[None]
+        ramp = np.sin(0.5 * np.pi * (hk - hbot) / hdepth) ** 2
+        dampwt = np.where(hk >= hbot, dampmag * ramp, 0.0)
+        wd = (ws - dampwt * mass_f_mut * a.w_save) / (1.0 + dampwt)
+        ws[1:] = wd[1:]
+    mass_f_muts = c1f * muts[None] + c2f
+    ph_next = ph.copy()
+    ph_next[1:] = rhs[1:] + m.msfty[None] * 0.5 * dts * G * eps_p * ws[1:] / mass_f_muts[1:]
+    a.w, a.ph, a.t_2ave = ws, ph_next, t2a
+
+
+def acoustic_substep(a, m, nl: Namelist, dts, bdy=None):
+    """core/acoustic.py:837-1150."""
+    rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
+    _, specified, _ = lateral_flags(nl)
+    advance_uv(a, m, dts, rdx, rdy, nl.dx, nl.dy, nl.top_lid, bdy)
+    advance_mu_t(a, m, dts, rdx, rdy, nl.epssm, specified)
+    advance_w(a, m, nl, dts, rdx, rdy)
+    mu_work = a.muts - a.mut
+    al, pp = calc_al_p(mu_work, a.muts, a.ph, a.theta_work, a.theta_1, a.c2a, a.alt, m)
+    a.p = pp + SMDIV * (pp - a.pm1)
+    a.pm1 = pp
+    a.al = al
+
+
+# ----------------------------------------------------------------------------
+# stage / step: runtime/operational_mode.py:1682-2265, 3319-3534
+# ----------------------------------------------------------------------------
+
+def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Namelist, dts, lead_seconds):
+    """operational_mode.py:1682-2166 (no specified cadence, no nested forcing)."""
+    m = nl.metrics
+    rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
+    nz, ny, nx = s.theta.shape
+    mu_prime = prep.mut - prep.mub
+    if nl.moist_cqw:
+        rw, cqw = pg_buoy_w_moist(s.p_perturbation, mu_prime, prep.mub, qtot_of(s), m)
+    else:
+        rw, cqw = pg_buoy_w_dry(s.p_perturbation, mu_prime, m)
+    rw = rw + tend.w
+    if nl.w_coriolis:
+        c1h, c2h = _col(m.c1h), _col(m.c2h)
+        ru_s = (c1h * prep.muu[None] + c2h) * s.u / m.msfuy[None]
+        rv_s = (c1h * prep.muv[None] + c2h) * s.v / m.msfvx[None]
+        ru_m = 0.5 * (ru_s[:, :, :-1] + ru_s[:, :, 1:])
+        u_m = 0.5 * (s.u[:, :, :-1] + s.u[:, :, 1:])
+        rv_m = 0.5 * (rv_s[:, :-1, :] + rv_s[:, 1:, :])
+        v_m = 0.5 * (s.v[:, :-1, :] + s.v[:, 1:, :])
+        fnm_f, fnp_f = _col(m.fnm[1:nz]), _col(m.fnp[1:nz])
+        face = lambda f: fnm_f * f[1:nz] + fnp_f * f[: nz - 1]
+        ru_f, u_f, rv_f, v_f = face(ru_m), face(u_m), face(rv_m), face(v_m)
+        mxy = (m.msftx / m.msfty)[None]
+        cor = m.e[None] * (m.cosa[None] * ru_f - mxy * m.sina[None] * rv_f)
+        curv = W_RERADIUS * (ru_f * u_f + mxy * rv_f * v_f)
+        rw[1:nz] = rw[1:nz] + (cor + curv)
+    ph_tend = rhs_ph_order2(s.u, s.v, prep.ww_save, s.ph_perturbation, prep.phb, s.w, prep.mut,
+                            prep.muu, prep.muv, m, rdx, rdy, nl.top_lid)
+    a = SimpleNamespace()
+    a.ww = prep.ww_save.copy()
+    a.ww_1 = prep.ww_save
+    a.u, a.v, a.w = prep.u_work.copy(), prep.v_work.copy(), prep.w_work.copy()
+    a.u_1, a.v_1 = prep.u_save, prep.v_save
+    a.mu = prep.mu_save + prep.mu_work
+    a.mut = prep.mut
+    a.muave = np.zeros_like(prep.mu_work)
+    a.muts = prep.muts.copy()
+    a.muu, a.muv = prep.muu, prep.muv
+    a.mudf = carry_mudf.copy()
+    a.theta_1 = prep.t_save
+    a.theta_tend = tend.theta
+    a.mu_tend = tend.mu
+    a.ph_tend = ph_tend
+    a.ph = prep.ph_work.copy()
+    a.p = p0
+    a.pm1 = pm1
+    a.al = al0
+    a.t_2ave = np.zeros_like(prep.theta_work)
+    a.theta_work = prep.theta_work.copy()
+    a.u_tend, a.v_tend = tend.u, tend.v
+    a.pb, a.alt, a.c2a, a.cqw = prep.pb, prep.alt, prep.c2a, cqw
+    a.cqu, a.cqv = prep.cqu, prep.cqv
+    a.phb, a.ph_1 = prep.phb, prep.ph_1
+    a.w_save = prep.w_save
+    a.rw_tend = rw
+    a.php = prep.php
+    bdy = None
+    if nl.run_boundary and lead_seconds is not None:
+        c1h, c2h = _col(m.c1h), _col(m.c2h)
+        nzone = nl.spec_zone + nl.relax_zone
+        us = interpolate_boundary_leaf(s.u_bdy, lead_seconds, nl.update_cadence_s)
+        vs = interpolate_boundary_leaf(s.v_bdy, lead_seconds, nl.update_cadence_s)
+        bdy = SimpleNamespace()
+        bdy.u_target = normal_bdy_work_target_u(us, prep.u_save, c1h * prep.muu[None] + c2h,
+                                                c1h * prep.muus[None] + c2h, m.msfuy, nzone)
+        bdy.v_target = normal_bdy_work_target_v(vs, prep.v_save, c1h * prep.muv[None] + c2h,
+                                                c1h * prep.muvs[None] + c2h, m.msfvx, nzone)
+        strength = NORMAL_BDY_RELAX_STRENGTH if nl.normal_bdy_relax_strength is None else nl.normal_bdy_relax_strength
+        sub = strength * (dts / nl.dt_s if nl.dt_s != 0.0 else 0.0)
+        bdy.wu = normal_relax_weights(ny, nx + 1, sub, "u")
+        bdy.wv = normal_relax_weights(ny + 1, nx, sub, "v")
+    return a, bdy
+
+
+def small_step_finish_and_refresh(s, prep, a, nl: Namelist):
+    """core/small_step_finish.py:419-498 + operational_mode.py:2169-2231."""
+    m = nl.metrics
+    c1h, c2h, c1f, c2f = _col(m.c1h), _col(m.c2h), _col(m.c1f), _col(m.c2f)
+    ms_u = c1h * prep.muus[None] + c2h
+    mc_u = c1h * prep.muu[None] + c2h
+    ms_v = c1h * prep.muvs[None] + c2h
+    mc_v = c1h * prep.muv[None] + c2h
+    ms_w = c1f * a.muts[None] + c2f
+    mc_w = c1f * prep.mut[None] + c2f
+    ms_t = c1h * a.muts[None] + c2h
+    mc_t = c1h * prep.mut[None] + c2h
+
+    def sd(x):
+        return np.where(np.abs(x) > 1.0e-12, x, np.where(x >= 0.0, 1.0e-12, -1.0e-12))
+
+    n = copy_state(s)
+    n.u = (m.msfuy[None] * a.u + prep.u_save * mc_u) / sd(ms_u)
+    n.v = (m.msfvx[None] * a.v + prep.v_save * mc_v) / sd(ms_v)
+    n.w = (m.msfty[None] * a.w + prep.w_save * mc_w) / sd(ms_w)
+    n.theta = (a.theta_work + prep.t_save * mc_t) / sd(ms_t) + T0
+    ph_pert = a.ph + prep.ph_save
+    p_base = s.p_total - s.p_perturbation
+    ph_base = s.ph_total - s.ph_perturbation
+    mu_base = s.mu_total - s.mu_perturbation
+    n.p_total = p_base + a.p
+    n.p_perturbation = a.p
+    n.ph_total = ph_base + ph_pert
+    n.ph_perturbation = ph_pert
+    n.mu_total = mu_base + a.mu
+    n.mu_perturbation = a.mu.copy()
+    # refresh grid%p (operational_mode.py:2169-2231 -> acoustic_wrf.py:322-438)
+    pb = prep.pb
+    phb = n.ph_total - n.ph_perturbation
+    mub = prep.mub
+    mhb = _col(m.c1h) * mub[None] + _col(m.c2h)
+    dphb = phb[1:] - phb[:-1]
+    den = _col(m.dnw) * mhb
+    alb = -dphb / np.where(np.abs(den) > 1.0e-12, den, 1.0e-12)
+    muts = mub + n.mu_perturbation
+    mw = _col(m.c1h) * muts[None] + _col(m.c2h)
+    smw = np.where(np.abs(mw) > 1.0e-12, mw, 1.0e-12)
+    php_ = n.ph_perturbation
+    if nl.hypsometric_opt == 2:
+        dph_tot = (phb[1:] + php_[1:]) - (phb[:-1] + php_[:-1])
+        alb_used = _log_alpha(phb[1:] - phb[:-1], mub[None], m)
+        al = _log_alpha(dph_tot, muts[None], m) - alb_used
+    else:
+        al = -(alb * _col(m.c1h) * n.mu_perturbation[None] + _col(m.rdnw) * (php_[1:] - php_[:-1])) / smw
+        alb_used = alb
+    alt = al + alb_used
+    p_pert = pressure_from_theta_alt(n.theta, alt) - pb
+    p_base2 = n.p_total - n.p_perturbation
+    n.p_total = p_base2 + p_pert
+    n.p_perturbation = p_pert
+    return n
+
+
+def rk_scan_step(carry, nl: Namelist, lead_seconds=None):
+    """``_rk_scan_step`` (operational_mode.py:3319-3534).
+
+    ``carry`` is a SimpleNamespace with ``state`` and ``mudf``; the returned
+    carry adds t_2ave, ww, mudf, muave, muts, ph_tend and the *_save family.
+    """
+    m = nl.metrics
+    rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
+    origin = copy_state(carry.state)
+    dt = float(nl.dt_s)
+    ns = int(nl.acoustic_substeps)
+    stages = ((1, dt / 3.0, dt / 3.0, 1), (2, 0.5 * dt, dt / float(ns), max(1, ns // 2)), (3, dt, dt / float(ns), ns))
+    _, specified, nested = lateral_flags(nl)
+    moist = nl.moist_adv_opt != 0
+    state = origin
+    mudf = carry.mudf.copy()
+    out = SimpleNamespace()
+    for rk_step, dt_rk, dts, nsub in stages:
+        s = state
+        vel = couple_velocities_periodic(s.u, s.v, s.mu_total, m, rdx, rdy)
+        tend = augment_large_step_tendencies(s, origin, vel, nl, rk_step)
+        q_tend = moisture_coupled_tendencies(s, origin, vel, nl, rk_step) if moist else None
+        ww_stage = stage_omega_specified(s.u, s.v, s.mu_total, m, rdx, rdy) if (specified or nested) else vel.rom
+        prep = small_step_prep(s, origin, rk_step, m, ww_stage)
+        al0, p0 = calc_al_p(prep.mu_work, prep.muts, prep.ph_work, prep.theta_work, prep.theta_1, prep.c2a, prep.alt, m)
+        a, bdy = acoustic_state_from_prep(s, prep, al0, p0, p0.copy(), tend, mudf, nl, dts, lead_seconds)
+        a.a, a.alpha, a.gamma = calc_coef_w(prep.mut, m, dts, nl.epssm, nl.top_lid, a.cqw, prep.c2a)
+        for _ in range(nsub):
+            acoustic_substep(a, m, nl, dts, bdy)
+        n = small_step_finish_and_refresh(s, prep, a, nl)
+        if moist:
+            mo = _col(m.c1h) * origin.mu_total[None] + _col(m.c2h)
+            mn = _col(m.c1h) * n.mu_total[None] + _col(m.c2h)
+            inv = 1.0 / mn
+            for name, qt in zip(MOIST_SPECIES, q_tend):
+                setattr(n, name, (mo * getattr(origin, name) + dt_rk * qt) * inv)
+        state = n
+        mudf = a.mudf
+        out.t_2ave = a.t_2ave + T0
+        out.ww = a.ww + prep.ww_save
+        out.muave = a.muave
+        out.muts = a.muts
+        out.ph_tend = a.ph_tend
+        out.u_save, out.v_save, out.w_save = prep.u_save, prep.v_save, prep.w_save
+        out.t_save = prep.t_save + T0
+        out.ph_save = prep.ph_save
+        out.mu_save = prep.mu_save
+        out.ww_save = prep.ww_save
+    out.state = state
+    out.mudf = mudf
+    return out

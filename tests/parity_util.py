@@ -1,0 +1,55 @@
+"""Shared helpers for the parity tests: run the oracle and the CUDA step on the
+same seeded case and compare every prognostic and carry field."""
+
+from __future__ import annotations
+
+from types import SimpleNamespace
+
+import numpy as np
+
+from oracle import dycore as D
+
+STATE_KEYS = ("u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total", "ph_perturbation",
+              "mu_total", "mu_perturbation", "qv", "qc", "qr", "qi", "qs", "qg")
+CARRY_KEYS = ("t_2ave", "ww", "mudf", "muave", "muts", "ph_tend", "u_save", "v_save", "w_save", "t_save",
+              "ph_save", "mu_save", "ww_save")
+
+
+def oracle_namelist(case):
+    return D.Namelist(metrics=case.metrics, **case.controls)
+
+
+def oracle_steps(case, nsteps, lead0=0.0):
+    nl = oracle_namelist(case)
+    carry = SimpleNamespace(state=D.copy_state(case.state), mudf=case.mudf.copy())
+    for i in range(nsteps):
+        carry = D.rk_scan_step(carry, nl, lead_seconds=lead0 + i * nl.dt_s)
+    return carry
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = float(np.max(np.abs(b))) if b.size else 0.0
+    diff = float(np.max(np.abs(a - b))) if b.size else 0.0
+    if scale == 0.0:
+        return diff
+    return diff / scale
+
+
+def compare(gpu_carry, ora_carry, keys_state=STATE_KEYS, keys_carry=CARRY_KEYS):
+    out = {}
+    gs = gpu_carry.state
+    for k in keys_state:
+        g = getattr(gs, k, None)
+        o = getattr(ora_carry.state, k, None)
+        if g is None or o is None:
+            continue
+        out[k] = rel_err(g.cpu().numpy(), o)
+    for k in keys_carry:
+        g = getattr(gpu_carry, k, None)
+        o = getattr(ora_carry, k, None)
+        if g is None or o is None:
+            continue
+        out[k] = rel_err(g.cpu().numpy(), o)
+    return out

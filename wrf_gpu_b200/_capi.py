@@ -1,0 +1,121 @@
+"""ctypes binding of the C ABI declared in ``include/wrfgpu.h``.
+
+The shared library ``libwrfgpu.so`` is built in-tree by ``wrf_gpu_b200.build``.
+Loading fails loudly (``RuntimeError``) when it is missing: there is no CPU
+fallback for the step.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libwrfgpu.so"
+
+WRFGPU_OK = 0
+WRFGPU_ERR_UNSUPPORTED_CONFIG = 1
+WRFGPU_ERR_BAD_SHAPE = 2
+WRFGPU_ERR_CUDA = 3
+WRFGPU_ERR_NULL_POINTER = 4
+WRFGPU_ERR_WORKSPACE = 5
+WRFGPU_PRECISION_FP64 = 0
+WRFGPU_PRECISION_MIXED = 1
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+
+
+class StepParams(ctypes.Structure):
+    _fields_ = [
+        ("nx", _I), ("ny", _I), ("nz", _I),
+        ("dx", _D), ("dy", _D), ("dt", _D),
+        ("acoustic_substeps", _I), ("epssm", _D), ("top_lid", _I), ("w_damping", _I), ("damp_opt", _I),
+        ("dampcoef", _D), ("zdamp", _D),
+        ("hypsometric_opt", _I), ("h_sca_adv_order", _I), ("scalar_adv_opt", _I), ("moist_adv_opt", _I),
+        ("run_boundary", _I), ("bc_ideal", _I), ("spec_zone", _I), ("relax_zone", _I),
+        ("update_cadence_s", _D), ("normal_bdy_relax_strength", _D),
+        ("moist_cqw", _I), ("w_coriolis", _I), ("precision", _I),
+        ("cf1", _D), ("cf2", _D), ("cf3", _D), ("p_top", _D),
+        ("cfn", _D), ("cfn1", _D),
+    ]
+
+
+METRIC_FIELDS = ("c1h", "c2h", "c3h", "c4h", "c1f", "c2f", "c3f", "c4f", "dn", "dnw", "rdn", "rdnw", "fnm", "fnp",
+                 "msftx", "msfty", "msfux", "msfuy", "msfvx", "msfvy", "f", "e", "sina", "cosa")
+
+
+class Metrics(ctypes.Structure):
+    _fields_ = [(n, _P) for n in METRIC_FIELDS]
+
+
+STATE_FIELDS = ("u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total", "ph_perturbation",
+                "mu_total", "mu_perturbation")
+
+
+class StepInputs(ctypes.Structure):
+    _fields_ = [(n, _P) for n in STATE_FIELDS] + [
+        ("q", _P * 6), ("mudf", _P),
+        ("base_u", _P), ("base_v", _P), ("base_w", _P), ("base_theta", _P), ("base_mu", _P),
+        ("u_bdy", _P), ("v_bdy", _P), ("bdy_ntime", _I), ("bdy_width", _I), ("bdy_side_len", _I),
+    ]
+
+
+CARRY_OUT_FIELDS = ("t_2ave", "ww", "mudf", "muave", "muts", "ph_tend", "u_save", "v_save", "w_save", "t_save",
+                    "ph_save", "mu_save", "ww_save")
+
+
+class StepOutputs(ctypes.Structure):
+    _fields_ = [(n, _P) for n in STATE_FIELDS] + [("q", _P * 6)] + [(n, _P) for n in CARRY_OUT_FIELDS]
+
+
+EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
+            "wrfgpu_rk3_step", "wrfgpu_step_launch_count", "wrfgpu_last_error_string", "wrfgpu_version")
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None):
+    """Load ``libwrfgpu.so`` (raises ``RuntimeError`` if it is absent)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"wrf_gpu_b200: CUDA library {p} is missing; build it with "
+            "`python -c 'import wrf_gpu_b200.build as b; b.build()'` (there is no CPU fallback)")
+    lib = ctypes.CDLL(str(p))
+    lib.wrfgpu_step_params_init.argtypes = [ctypes.POINTER(StepParams)]
+    lib.wrfgpu_step_params_init.restype = _I
+    lib.wrfgpu_step_params_validate.argtypes = [ctypes.POINTER(StepParams)]
+    lib.wrfgpu_step_params_validate.restype = _I
+    lib.wrfgpu_step_workspace_size.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_size_t)]
+    lib.wrfgpu_step_workspace_size.restype = _I
+    lib.wrfgpu_step_launch_count.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(_I)]
+    lib.wrfgpu_step_launch_count.restype = _I
+    lib.wrfgpu_rk3_step.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), ctypes.POINTER(StepInputs),
+                                    ctypes.POINTER(StepOutputs), _D, _P, ctypes.c_size_t, _P]
+    lib.wrfgpu_rk3_step.restype = _I
+    lib.wrfgpu_last_error_string.argtypes = []
+    lib.wrfgpu_last_error_string.restype = ctypes.c_char_p
+    lib.wrfgpu_version.argtypes = []
+    lib.wrfgpu_version.restype = ctypes.c_char_p
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class WrfGpuError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"wrfgpu error {code}: {message}")
+        self.code = code
+
+
+def check(code: int) -> None:
+    if code != WRFGPU_OK:
+        raise WrfGpuError(code, load().wrfgpu_last_error_string().decode())

@@ -1,0 +1,534 @@
+// Host orchestration and C ABI of the fp64 RK3 dycore step.
+//
+// One wrfgpu_rk3_step call replaces _rk_scan_step
+// (src/gpuwrf/runtime/operational_mode.py:3319-3534): three RK stages of
+// 1, ns/2 and ns acoustic substeps (operational_mode.py:3524-3530), each
+// stage = stage kernels -> substep kernels -> finish kernels, all enqueued on
+// the caller's stream with no host synchronisation or allocation.
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+
+#include "../../include/wrfgpu.h"
+#include "dycore_common.cuh"
+#include "stage_kernels.cuh"
+#include "acoustic_kernels.cuh"
+#include "finish_kernels.cuh"
+
+using namespace wg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+struct Dims {
+  size_t m, u, v, w, s2, su, sv;  // element counts
+};
+
+Dims dims_of(const wrfgpu_step_params &p) {
+  Dims d;
+  const size_t nx = p.nx, ny = p.ny, nz = p.nz;
+  d.m = nz * ny * nx;
+  d.u = nz * ny * (nx + 1);
+  d.v = nz * (ny + 1) * nx;
+  d.w = (nz + 1) * ny * nx;
+  d.s2 = ny * nx;
+  d.su = ny * (nx + 1);
+  d.sv = (ny + 1) * nx;
+  return d;
+}
+
+// Bump allocator over the caller's workspace (256-byte aligned slices).
+struct Carver {
+  char *base;
+  size_t off, cap;
+  bool dry;
+  double *take(size_t n) {
+    off = (off + 255) & ~(size_t)255;
+    double *p = dry ? nullptr : reinterpret_cast<double *>(base + off);
+    off += n * sizeof(double);
+    return p;
+  }
+};
+
+struct Work {
+  // 2-D
+  double *mub, *mut, *muts0, *mu_work0, *muu, *muus, *muv, *muvs, *mu, *muts, *muave, *mudf, *phb0;
+  // mass
+  double *alt_raw, *alt, *pb, *c2a, *qtot, *al_ls, *php_ls, *php, *t_tend, *theta_w, *t2ave, *p, *pm1, *al;
+  double *s1, *s2, *ru, *rv;
+  double *qtend[6];
+  // u / v faces
+  double *u_tend, *u_w, *cqu, *u_target, *v_tend, *v_w, *cqv, *v_target;
+  // w faces
+  double *rom, *ww_spec, *rw_tend, *ph_tend, *cqw, *w_w, *ph_w, *pt1, *ww, *a, *alpha, *gamma;
+  // intermediate states after stages 1 and 2
+  StateW st[2];
+};
+
+bool is_moist(const wrfgpu_step_params &p) { return p.moist_adv_opt != 0; }
+
+void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
+  const Dims d = dims_of(p);
+  w.mub = c.take(d.s2); w.mut = c.take(d.s2); w.muts0 = c.take(d.s2); w.mu_work0 = c.take(d.s2);
+  w.muu = c.take(d.su); w.muus = c.take(d.su); w.muv = c.take(d.sv); w.muvs = c.take(d.sv);
+  w.mu = c.take(d.s2); w.muts = c.take(d.s2); w.muave = c.take(d.s2); w.mudf = c.take(d.s2);
+  w.phb0 = c.take(d.s2);
+  w.alt_raw = c.take(d.m); w.alt = c.take(d.m); w.pb = c.take(d.m); w.c2a = c.take(d.m);
+  w.qtot = c.take(d.m); w.al_ls = c.take(d.m); w.php_ls = c.take(d.m); w.php = c.take(d.m);
+  w.t_tend = c.take(d.m); w.theta_w = c.take(d.m); w.t2ave = c.take(d.m); w.p = c.take(d.m);
+  w.pm1 = c.take(d.m); w.al = c.take(d.m); w.ru = c.take(d.m); w.rv = c.take(d.m);
+  const bool lim = (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2 || p.moist_adv_opt == 1 || p.moist_adv_opt == 2);
+  w.s1 = lim ? c.take(d.m) : nullptr;
+  w.s2 = lim ? c.take(d.m) : nullptr;
+  for (int s = 0; s < 6; ++s) w.qtend[s] = is_moist(p) ? c.take(d.m) : nullptr;
+  w.u_tend = c.take(d.u); w.u_w = c.take(d.u); w.cqu = c.take(d.u);
+  w.v_tend = c.take(d.v); w.v_w = c.take(d.v); w.cqv = c.take(d.v);
+  const bool bdy = p.run_boundary != 0;
+  w.u_target = bdy ? c.take(d.u) : nullptr;
+  w.v_target = bdy ? c.take(d.v) : nullptr;
+  w.rom = c.take(d.w);
+  const bool spec = p.run_boundary && !p.bc_ideal;
+  w.ww_spec = spec ? c.take(d.w) : nullptr;
+  w.rw_tend = c.take(d.w); w.ph_tend = c.take(d.w); w.cqw = c.take(d.w); w.w_w = c.take(d.w);
+  w.ph_w = c.take(d.w); w.pt1 = c.take(d.w); w.ww = c.take(d.w);
+  w.a = c.take(d.w); w.alpha = c.take(d.w); w.gamma = c.take(d.w);
+  for (int s = 0; s < 2; ++s) {
+    StateW &S = w.st[s];
+    S.u = c.take(d.u); S.v = c.take(d.v); S.w = c.take(d.w); S.theta = c.take(d.m);
+    S.p_total = c.take(d.m); S.p_pert = c.take(d.m); S.ph_total = c.take(d.w); S.ph_pert = c.take(d.w);
+    S.mu_total = c.take(d.s2); S.mu_pert = c.take(d.s2);
+    for (int q = 0; q < 6; ++q) S.q[q] = is_moist(p) ? c.take(d.m) : nullptr;
+  }
+}
+
+StateR as_read(const StateW &s) {
+  StateR r;
+  r.u = s.u; r.v = s.v; r.w = s.w; r.theta = s.theta; r.p_total = s.p_total; r.p_pert = s.p_pert;
+  r.ph_total = s.ph_total; r.ph_pert = s.ph_pert; r.mu_total = s.mu_total; r.mu_pert = s.mu_pert;
+  for (int q = 0; q < 6; ++q) r.q[q] = s.q[q];
+  return r;
+}
+
+Grid make_grid(const wrfgpu_step_params &p, const wrfgpu_metrics &m, const double *dn_host_top) {
+  (void)dn_host_top;
+  Grid g;
+  g.nx = p.nx; g.ny = p.ny; g.nz = p.nz;
+  g.dx = p.dx; g.dy = p.dy; g.rdx = 1.0 / p.dx; g.rdy = 1.0 / p.dy;
+  g.c1h = m.c1h; g.c2h = m.c2h; g.c3h = m.c3h; g.c4h = m.c4h;
+  g.c1f = m.c1f; g.c2f = m.c2f; g.c3f = m.c3f; g.c4f = m.c4f;
+  g.dn = m.dn; g.dnw = m.dnw; g.rdn = m.rdn; g.rdnw = m.rdnw; g.fnm = m.fnm; g.fnp = m.fnp;
+  g.msftx = m.msftx; g.msfty = m.msfty; g.msfux = m.msfux; g.msfuy = m.msfuy; g.msfvx = m.msfvx; g.msfvy = m.msfvy;
+  g.f = m.f; g.e = m.e; g.sina = m.sina; g.cosa = m.cosa;
+  g.cf1 = p.cf1; g.cf2 = p.cf2; g.cf3 = p.cf3; g.p_top = p.p_top;
+  g.cfn = p.cfn; g.cfn1 = p.cfn1;
+  return g;
+}
+
+// Specified boundary work targets (coupling/boundary_apply.py:729-781) for
+// the normal momentum, from the time-interpolated strips.
+struct BdyLeaf {
+  const double *leaf;
+  int ntime, width, side_len, lo, hi;
+  double alpha;
+};
+
+__device__ __forceinline__ double strip_at(const BdyLeaf &b, int nz, int side, int bb, int k, int t) {
+  bb = bb < 0 ? 0 : (bb > b.width - 1 ? b.width - 1 : bb);
+  auto at = [&](int tt) {
+    return ld(b.leaf, ((((size_t)tt * 4 + side) * b.width + bb) * nz + k) * b.side_len + t);
+  };
+  return at(b.lo) * (1.0 - b.alpha) + at(b.hi) * b.alpha;
+}
+
+__global__ void k_bdy_target_u(Grid g, BdyLeaf b, const double *u_save, const double *muu, const double *muus,
+                               int nzone, double *target) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i > nx || j >= ny) return;
+  const int x_len = nx + 1;
+  const size_t cu = ix3(k, j, i, ny, x_len);
+  // last writer in the reference loop order: for b: W col b, then E col x_len-1-b
+  int best = -1, side = 0;
+  for (int bb = 0; bb < nzone; ++bb) {
+    if (i == bb) { best = bb; side = 0; }
+    if (i == x_len - 1 - bb) { best = bb; side = 1; }
+  }
+  double t = 0.0;
+  if (best >= 0) {
+    const size_t f2 = ix2(j, i, x_len);
+    const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+    const double ms = c1 * ld(muus, f2) + c2, mc = c1 * ld(muu, f2) + c2;
+    t = (strip_at(b, nz, side, best, k, j) * ms - ld(u_save, cu) * mc) / ld(g.msfuy, f2);
+  }
+  target[cu] = t;
+}
+
+__global__ void k_bdy_target_v(Grid g, BdyLeaf b, const double *v_save, const double *muv, const double *muvs,
+                               int nzone, double *target) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j > ny) return;
+  const int y_len = ny + 1;
+  const size_t cv = ix3(k, j, i, y_len, nx);
+  int best = -1, side = 2;
+  for (int bb = 0; bb < nzone; ++bb) {
+    if (j == bb) { best = bb; side = 2; }
+    if (j == y_len - 1 - bb) { best = bb; side = 3; }
+  }
+  double t = 0.0;
+  if (best >= 0) {
+    const size_t f2 = ix2(j, i, nx);
+    const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+    const double ms = c1 * ld(muvs, f2) + c2, mc = c1 * ld(muv, f2) + c2;
+    t = (strip_at(b, nz, side, best, k, i) * ms - ld(v_save, cv) * mc) / ld(g.msfvx, f2);
+  }
+  target[cv] = t;
+}
+
+inline dim3 blk2() { return dim3(32, 4, 1); }
+inline dim3 grd(int nxx, int nyy, int nzz) { return dim3((nxx + 31) / 32, (nyy + 3) / 4, nzz); }
+
+int check_launch(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(WRFGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return WRFGPU_OK;
+}
+
+#define LAUNCH_CHECK(name)                      \
+  do {                                          \
+    int _rc = check_launch(name);               \
+    if (_rc != WRFGPU_OK) return _rc;           \
+  } while (0)
+
+}  // namespace
+
+extern "C" {
+
+const char *wrfgpu_last_error_string(void) { return g_last_error.c_str(); }
+
+const char *wrfgpu_version(void) { return "wrfgpu-b200 0.1.0 (fp64 reference-order kernels, sm_100a)"; }
+
+int wrfgpu_step_params_init(wrfgpu_step_params *p) {
+  if (p == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params is NULL");
+  std::memset(p, 0, sizeof(*p));
+  p->dt = 10.0;
+  p->acoustic_substeps = 10;
+  p->epssm = 0.1;
+  p->top_lid = 0;
+  p->w_damping = 0;
+  p->damp_opt = 0;
+  p->dampcoef = 0.0;
+  p->zdamp = 5000.0;
+  p->hypsometric_opt = 1;
+  p->h_sca_adv_order = 2;
+  p->scalar_adv_opt = 0;
+  p->moist_adv_opt = 0;
+  p->run_boundary = 0;
+  p->bc_ideal = 1;
+  p->spec_zone = 1;
+  p->relax_zone = 4;
+  p->update_cadence_s = 3600.0;
+  p->normal_bdy_relax_strength = -1.0;
+  p->moist_cqw = 1;
+  p->w_coriolis = 1;
+  p->precision = WRFGPU_PRECISION_FP64;
+  return WRFGPU_OK;
+}
+
+int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
+  if (p == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params is NULL");
+  if (p->nz < 4) return fail(WRFGPU_ERR_BAD_SHAPE, "nz must be >= 4");
+  if (p->nx < 1 || p->ny < 1) return fail(WRFGPU_ERR_BAD_SHAPE, "nx and ny must be >= 1");
+  if (!(p->dx > 0.0) || !(p->dy > 0.0) || !(p->dt > 0.0)) return fail(WRFGPU_ERR_BAD_SHAPE, "dx, dy, dt must be > 0");
+  if (p->acoustic_substeps < 1) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "acoustic_substeps must be >= 1");
+  if (p->hypsometric_opt != 1 && p->hypsometric_opt != 2)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "hypsometric_opt must be 1 or 2");
+  if (p->scalar_adv_opt < 0 || p->scalar_adv_opt > 2)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "scalar_adv_opt must be 0, 1 or 2 (WENO options are not built)");
+  if (p->moist_adv_opt < 0 || p->moist_adv_opt > 2)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "moist_adv_opt must be 0, 1 or 2");
+  const bool spec = p->run_boundary && !p->bc_ideal;
+  if (spec && p->h_sca_adv_order >= 4)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "rhs_ph order-6 specified-boundary branch (h_sca_adv_order >= 4) is not built");
+  if (spec && (p->nx < 3 || p->ny < 3)) return fail(WRFGPU_ERR_BAD_SHAPE, "specified boundaries need nx, ny >= 3");
+  if (p->run_boundary && (p->spec_zone != 1 || p->relax_zone != 4))
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "boundary zones other than spec_zone=1, relax_zone=4 are not built");
+  if (p->precision != WRFGPU_PRECISION_FP64 && p->precision != WRFGPU_PRECISION_MIXED)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "unknown precision mode");
+  if (p->precision == WRFGPU_PRECISION_MIXED)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "mixed precision is not built in this library version");
+  return WRFGPU_OK;
+}
+
+int wrfgpu_step_workspace_size(const wrfgpu_step_params *p, size_t *bytes) {
+  if (p == nullptr || bytes == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/bytes is NULL");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  Carver c{nullptr, 0, 0, true};
+  Work w;
+  carve(*p, c, w);
+  *bytes = c.off + 256;
+  return WRFGPU_OK;
+}
+
+int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
+  if (p == nullptr || launches == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/launches is NULL");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  const int ns = p->acoustic_substeps;
+  const int nsub[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
+  const bool bdy = p->run_boundary != 0;
+  int n = 0;
+  for (int s = 0; s < 3; ++s) {
+    n += 8;  // mass2d, transport, diag, uface, vface, mass, wface, coef
+    if (s == 2 && (p->scalar_adv_opt == 1 || p->scalar_adv_opt == 2)) n += 2;
+    if (s == 2 && (p->moist_adv_opt == 1 || p->moist_adv_opt == 2)) n += 12;
+    if (bdy) n += 2;
+    n += 3 * nsub[s];
+    n += 3;  // finish u, v, col
+  }
+  *launches = n;
+  return WRFGPU_OK;
+}
+
+int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const wrfgpu_step_inputs *in,
+                    const wrfgpu_step_outputs *out, double lead_seconds, void *workspace, size_t workspace_bytes,
+                    cudaStream_t stream) {
+  if (pp == nullptr || mm == nullptr || in == nullptr || out == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "params/metrics/inputs/outputs is NULL");
+  int rc = wrfgpu_step_params_validate(pp);
+  if (rc) return rc;
+  const wrfgpu_step_params &p = *pp;
+  size_t need = 0;
+  wrfgpu_step_workspace_size(pp, &need);
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(WRFGPU_ERR_WORKSPACE, "workspace is NULL or smaller than wrfgpu_step_workspace_size()");
+  const double *req_in[] = {in->u, in->v, in->w, in->theta, in->p_total, in->p_perturbation, in->ph_total,
+                            in->ph_perturbation, in->mu_total, in->mu_perturbation};
+  for (const double *q : req_in)
+    if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "a required state input pointer is NULL");
+  double *req_out[] = {out->u, out->v, out->w, out->theta, out->p_total, out->p_perturbation, out->ph_total,
+                       out->ph_perturbation, out->mu_total, out->mu_perturbation};
+  for (double *q : req_out)
+    if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "a required state output pointer is NULL");
+  const bool moist = is_moist(p);
+  const bool have_q = in->q[0] != nullptr;
+  if (have_q)
+    for (int s = 0; s < 6; ++s)
+      if (in->q[s] == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "moisture inputs must be all NULL or all set");
+  if (moist && !have_q) return fail(WRFGPU_ERR_NULL_POINTER, "moist_adv_opt != 0 needs the six moisture inputs");
+  if (have_q)
+    for (int s = 0; s < 6; ++s)
+      if (out->q[s] == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "moisture outputs must be set when inputs are");
+  const bool bdy_active = p.run_boundary && !std::isnan(lead_seconds);
+  if (bdy_active && (in->u_bdy == nullptr || in->v_bdy == nullptr || in->bdy_ntime < 1 || in->bdy_width < 1 ||
+                     in->bdy_side_len < (p.nx > p.ny ? p.nx + 1 : p.ny + 1)))
+    return fail(WRFGPU_ERR_BAD_SHAPE, "run_boundary needs u_bdy/v_bdy strips (ntime, 4, width, nz, side_len)");
+
+  const Dims d = dims_of(p);
+  Carver cv{reinterpret_cast<char *>(workspace), 0, workspace_bytes, false};
+  Work w;
+  carve(p, cv, w);
+  Grid g = make_grid(p, *mm, nullptr);
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const bool specified = p.run_boundary && !p.bc_ideal;
+  const double dt = p.dt;
+  const int ns = p.acoustic_substeps;
+  const double dt_rk[3] = {dt / 3.0, 0.5 * dt, dt};
+  const double dts_rk[3] = {dt / 3.0, dt / (double)ns, dt / (double)ns};
+  const int nsub[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
+
+  StateR origin;
+  origin.u = in->u; origin.v = in->v; origin.w = in->w; origin.theta = in->theta;
+  origin.p_total = in->p_total; origin.p_pert = in->p_perturbation;
+  origin.ph_total = in->ph_total; origin.ph_pert = in->ph_perturbation;
+  origin.mu_total = in->mu_total; origin.mu_pert = in->mu_perturbation;
+  for (int s = 0; s < 6; ++s) origin.q[s] = in->q[s];
+  StateW final_out;
+  final_out.u = out->u; final_out.v = out->v; final_out.w = out->w; final_out.theta = out->theta;
+  final_out.p_total = out->p_total; final_out.p_pert = out->p_perturbation;
+  final_out.ph_total = out->ph_total; final_out.ph_pert = out->ph_perturbation;
+  final_out.mu_total = out->mu_total; final_out.mu_pert = out->mu_perturbation;
+  for (int s = 0; s < 6; ++s) final_out.q[s] = have_q ? out->q[s] : nullptr;
+
+  // mudf carried across stages (operational_mode.py:2046)
+  if (in->mudf != nullptr) {
+    if (cudaMemcpyAsync(w.mudf, in->mudf, d.s2 * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "mudf copy failed");
+  } else if (cudaMemsetAsync(w.mudf, 0, d.s2 * sizeof(double), stream) != cudaSuccess) {
+    return fail(WRFGPU_ERR_CUDA, "mudf clear failed");
+  }
+
+  const double eps1 = 1.0 + p.epssm;
+  BdyLeaf bl_u{}, bl_v{};
+  if (bdy_active) {
+    const int mx = in->bdy_ntime - 1;
+    const double li = lead_seconds / p.update_cadence_s;
+    int lo = (int)std::floor(li);
+    lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
+    int hi = lo + 1;
+    hi = hi < 0 ? 0 : (hi > mx ? mx : hi);
+    double a = li - (double)lo;
+    a = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
+    bl_u = BdyLeaf{in->u_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
+    bl_v = BdyLeaf{in->v_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
+  }
+
+  StateR s = origin;
+  for (int stage = 0; stage < 3; ++stage) {
+    const int rk = stage + 1;
+    const double dts = dts_rk[stage];
+    StateW o = (stage == 2) ? final_out : w.st[stage];
+    if (!moist && stage < 2) {
+      for (int q = 0; q < 6; ++q) o.q[q] = nullptr;  // moisture passes through untouched
+    }
+    Mass2D m2{w.mub, w.mut, w.muts0, w.mu_work0, w.muu, w.muus, w.muv, w.muvs, w.mu, w.muts, w.muave};
+    k_mass2d<<<grd(nx + 1, ny + 1, 1), blk2(), 0, stream>>>(g, s, origin.mu_pert, rk, m2);
+    LAUNCH_CHECK("k_mass2d");
+    k_transport<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, s.u, s.v, s.mu_total, w.ru, w.rv, w.rom,
+                                                       specified ? w.ww_spec : nullptr);
+    LAUNCH_CHECK("k_transport");
+    Diag dg{w.alt_raw, w.alt, w.pb, w.c2a, w.qtot, w.al_ls, w.php_ls, w.php};
+    k_diag<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, s, p.hypsometric_opt, dg);
+    LAUNCH_CHECK("k_diag");
+    UFaceOut uo{w.u_tend, w.u_w, w.cqu};
+    k_uface<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
+                                                       in->base_u, p.top_lid, p.run_boundary, uo);
+    LAUNCH_CHECK("k_uface");
+    VFaceOut vo{w.v_tend, w.v_w, w.cqv};
+    k_vface<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
+                                                       in->base_v, p.top_lid, p.run_boundary, vo);
+    LAUNCH_CHECK("k_vface");
+    const bool lim_theta = (rk == 3) && (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2);
+    const bool lim_moist = moist && (rk == 3) && (p.moist_adv_opt == 1 || p.moist_adv_opt == 2);
+    MassOut mo;
+    mo.t_tend = w.t_tend;
+    mo.theta_w = w.theta_w;
+    for (int q = 0; q < 6; ++q) mo.q_tend[q] = w.qtend[q];
+    k_mass<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta,
+                                                   lim_theta ? 0 : 1, (moist && !lim_moist) ? 1 : 0, mo);
+    LAUNCH_CHECK("k_mass");
+    if (lim_theta || lim_moist) {
+      LimArgs la;
+      la.ru = w.ru; la.rv = w.rv; la.rom = w.rom; la.mut = s.mu_total; la.mu_old = origin.mu_total; la.dt = dt;
+      if (lim_theta) {
+        la.opt = p.scalar_adv_opt;
+        la.offset = T0;
+        k_lim_scale<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2);
+        LAUNCH_CHECK("k_lim_scale");
+        k_lim_tend<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2, in->base_theta,
+                                                           s.mu_total, w.t_tend);
+        LAUNCH_CHECK("k_lim_tend");
+      }
+      if (lim_moist) {
+        la.opt = p.moist_adv_opt;
+        la.offset = 0.0;
+        for (int q = 0; q < 6; ++q) {
+          k_lim_scale<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2);
+          LAUNCH_CHECK("k_lim_scale");
+          k_lim_tend<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr,
+                                                             s.mu_total, w.qtend[q]);
+          LAUNCH_CHECK("k_lim_tend");
+        }
+      }
+    }
+    const double *ww_stage = specified ? w.ww_spec : w.rom;
+    WFaceOut wo{w.rw_tend, w.ph_tend, w.cqw, w.w_w, w.ph_w, w.pt1, w.ww, w.phb0};
+    k_wface<<<grd(nx, ny, nz + 1), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot, w.mub,
+                                                       w.mut, w.muts0, w.muu, w.muv, in->base_w, p.top_lid,
+                                                       p.moist_cqw, p.w_coriolis, wo);
+    LAUNCH_CHECK("k_wface");
+    const double x = 0.5 * dts * G * eps1;
+    const double cof = x * x;
+    CoefOut co{w.a, w.alpha, w.gamma, w.p, w.pm1, w.al, w.t2ave};
+    k_coef<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, w.mut, w.muts0, w.mu_work0, w.c2a, w.cqw, w.alt, w.theta_w,
+                                                  w.ph_w, origin.theta, cof, p.top_lid, co);
+    LAUNCH_CHECK("k_coef");
+
+    BdyArgs ba{};
+    ba.active = bdy_active ? 1 : 0;
+    if (bdy_active) {
+      const int nzone = p.spec_zone + p.relax_zone;
+      k_bdy_target_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, bl_u, s.u, w.muu, w.muus, nzone, w.u_target);
+      LAUNCH_CHECK("k_bdy_target_u");
+      k_bdy_target_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, bl_v, s.v, w.muv, w.muvs, nzone, w.v_target);
+      LAUNCH_CHECK("k_bdy_target_v");
+      const double strength = (p.normal_bdy_relax_strength < 0.0) ? 20.0 : p.normal_bdy_relax_strength;
+      ba.u_target = w.u_target;
+      ba.v_target = w.v_target;
+      ba.sub_ratio = strength * (dt != 0.0 ? dts / dt : 0.0);
+      ba.spec_zone = 1;  // apply_normal_bdy_work uses DEFAULT_BOUNDARY_CONFIG widths
+      ba.relax_zone = 4;
+    }
+
+    Acoustic A;
+    A.u = w.u_w; A.v = w.v_w; A.w = w.w_w; A.ph = w.ph_w; A.theta_w = w.theta_w; A.t2ave = w.t2ave;
+    A.p = w.p; A.pm1 = w.pm1; A.al = w.al; A.ww = w.ww;
+    A.mu = w.mu; A.muts = w.muts; A.muave = w.muave; A.mudf = w.mudf;
+    A.u_tend = w.u_tend; A.v_tend = w.v_tend; A.t_tend = w.t_tend; A.rw_tend = w.rw_tend; A.ph_tend = w.ph_tend;
+    A.alt = w.alt; A.pb = w.pb; A.c2a = w.c2a; A.cqu = w.cqu; A.cqv = w.cqv; A.cqw = w.cqw; A.php = w.php;
+    A.pt1 = w.pt1; A.a = w.a; A.alpha = w.alpha; A.gamma = w.gamma; A.ww_1 = ww_stage;
+    A.mut = w.mut; A.muu = w.muu; A.muv = w.muv; A.muus = w.muus; A.muvs = w.muvs;
+    A.mu_tend = in->base_mu;
+    A.u_1 = s.u; A.v_1 = s.v; A.w_save = s.w; A.theta_s = s.theta; A.phb0 = w.phb0;
+    ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp};
+    for (int it = 0; it < nsub[stage]; ++it) {
+      k_advance_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
+      LAUNCH_CHECK("k_advance_u");
+      k_advance_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
+      LAUNCH_CHECK("k_advance_v");
+      k_column<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, A, ca);
+      LAUNCH_CHECK("k_column");
+    }
+
+    k_finish_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, w.u_w, s.u, w.muu, w.muus, o.u);
+    LAUNCH_CHECK("k_finish_u");
+    k_finish_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, w.v_w, s.v, w.muv, w.muvs, o.v);
+    LAUNCH_CHECK("k_finish_v");
+    FinishArgs fa;
+    fa.w_w = w.w_w; fa.ph_w = w.ph_w; fa.theta_w = w.theta_w; fa.p_ac = w.p; fa.mu_ac = w.mu; fa.muts_ac = w.muts;
+    fa.t2ave = w.t2ave; fa.ww_ac = w.ww; fa.mut = w.mut; fa.ww_stage = ww_stage;
+    for (int q = 0; q < 6; ++q) fa.q_tend[q] = w.qtend[q];
+    fa.dt_rk = dt_rk[stage];
+    fa.hyps = p.hypsometric_opt;
+    fa.moist = moist ? 1 : 0;
+    fa.t_2ave_out = (stage == 2) ? out->t_2ave : nullptr;
+    fa.ww_out = (stage == 2) ? out->ww : nullptr;
+    fa.t_save_out = (stage == 2) ? out->t_save : nullptr;
+    k_finish_col<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, s, origin, fa, o);
+    LAUNCH_CHECK("k_finish_col");
+
+    if (stage == 2) {
+      struct Cp { double *dst; const double *src; size_t n; } cps[] = {
+          {out->mudf, w.mudf, d.s2},       {out->muave, w.muave, d.s2},   {out->muts, w.muts, d.s2},
+          {out->ph_tend, w.ph_tend, d.w},  {out->u_save, s.u, d.u},       {out->v_save, s.v, d.v},
+          {out->w_save, s.w, d.w},         {out->ph_save, s.ph_pert, d.w}, {out->mu_save, s.mu_pert, d.s2},
+          {out->ww_save, ww_stage, d.w}};
+      for (const Cp &c : cps) {
+        if (c.dst == nullptr) continue;
+        if (cudaMemcpyAsync(c.dst, c.src, c.n * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+          return fail(WRFGPU_ERR_CUDA, "carry output copy failed");
+      }
+    }
+    StateR next = as_read(o);
+    if (!moist) {
+      for (int q = 0; q < 6; ++q) next.q[q] = (stage == 2) ? next.q[q] : origin.q[q];
+    }
+    s = next;
+  }
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+}  // extern "C"

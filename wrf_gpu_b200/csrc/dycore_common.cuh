@@ -1,0 +1,102 @@
+// Shared device helpers for the fp64 dycore kernels.
+//
+// Layout: float64 SoA, C order (k, j, i), i fastest.  Mass fields (nz, ny, nx),
+// u (nz, ny, nx+1), v (nz, ny+1, nx), w/ph/ww (nz+1, ny, nx), 2-D (ny, nx),
+// u-face 2-D (ny, nx+1), v-face 2-D (ny+1, nx).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cmath>
+
+namespace wg {
+
+// Physical constants (src/gpuwrf/dynamics/acoustic_wrf.py:27-75,
+// dynamics/core/advance_w.py:28,87-88, runtime/operational_mode.py:202).
+constexpr double R_D = 287.0;
+constexpr double CP_D = 7.0 * R_D / 2.0;
+constexpr double P0 = 100000.0;
+constexpr double CPOVCV = CP_D / (CP_D - R_D);
+constexpr double CVPM = -(CP_D - R_D) / CP_D;
+constexpr double G = 9.81;
+constexpr double T0 = 300.0;
+constexpr double MIN_ACOUSTIC_ALT = 0.1;
+constexpr double W_RERADIUS = 1.0 / 6370.0e3;
+constexpr double W_ALPHA = 0.3;
+constexpr double W_BETA = 1.0;
+constexpr double PD_EPS = 1.0e-20;
+constexpr double EMDIV = 0.01;
+constexpr double SMDIV = 0.1;
+constexpr double MIN_MUTS_FRACTION = 0.5;
+constexpr double MIN_MUTS_PA = 1.0;
+
+// Grid geometry and metrics passed by value to every kernel.
+struct Grid {
+  int nx, ny, nz;
+  double rdx, rdy, dx, dy;
+  const double *c1h, *c2h, *c3h, *c4h, *c1f, *c2f, *c3f, *c4f;
+  const double *dn, *dnw, *rdn, *rdnw, *fnm, *fnp;
+  const double *msftx, *msfty, *msfux, *msfuy, *msfvx, *msfvy;
+  const double *f, *e, *sina, *cosa;
+  double cf1, cf2, cf3, p_top;
+  double cfn, cfn1;  // top-face extrapolation weights (rk_addtend_dry.py:282-288)
+};
+
+// A read-only view of a model state (the reference State leaves the step uses).
+struct StateR {
+  const double *u, *v, *w, *theta, *p_total, *p_pert, *ph_total, *ph_pert, *mu_total, *mu_pert;
+  const double *q[6];
+};
+
+struct StateW {
+  double *u, *v, *w, *theta, *p_total, *p_pert, *ph_total, *ph_pert, *mu_total, *mu_pert;
+  double *q[6];
+};
+
+__device__ __forceinline__ size_t ix3(int k, int j, int i, int ny, int nx) {
+  return ((size_t)k * (size_t)ny + (size_t)j) * (size_t)nx + (size_t)i;
+}
+__device__ __forceinline__ size_t ix2(int j, int i, int nx) { return (size_t)j * (size_t)nx + (size_t)i; }
+
+__device__ __forceinline__ int wrp(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ double sgn(double x) { return (double)((x > 0.0) - (x < 0.0)); }
+
+__device__ __forceinline__ double ld(const double *p, size_t i) { return __ldg(p + i); }
+
+// jnp.maximum / jnp.minimum semantics are not needed for NaN here; plain compares.
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+
+// WRF flux5 left-face value (src/gpuwrf/dynamics/flux_advection.py:53-88).
+__device__ __forceinline__ double flux5(double qm3, double qm2, double qm1, double q0, double qp1, double qp2,
+                                        double vel) {
+  double f6 = (37.0 * (q0 + qm1) - 8.0 * (qp1 + qm2) + (qp2 + qm3)) / 60.0;
+  double c = ((qp2 - qm3) - 5.0 * (qp1 - qm2) + 10.0 * (q0 - qm1)) / 60.0;
+  return f6 - sgn(vel) * c;
+}
+
+// flux3 with the -sign(vel) upwind correction (flux_advection.py:534-562, 1362-1407).
+__device__ __forceinline__ double flux3v(double qkm2, double qkm1, double qk, double qkp1, double vel) {
+  double flux4 = (7.0 * (qk + qkm1) - (qkp1 + qkm2)) / 12.0;
+  double corr = ((qkp1 - qkm2) - 3.0 * (qk - qkm1)) / 12.0;
+  return vel * (flux4 + sgn(-vel) * corr);
+}
+
+// Dry inverse density from the EOS (acoustic_wrf.py:187-206, qvf = 1).
+__device__ __forceinline__ double inv_density(double theta, double p) {
+  return (R_D / P0) * theta * 1.0 * pow(dmax(p, 1.0) / P0, CVPM);
+}
+
+// EOS pressure inversion (acoustic_wrf.py:209-221, qvf = 1).
+__device__ __forceinline__ double pressure_from_theta_alt(double theta, double alt) {
+  double argument = (R_D * theta * 1.0) / (P0 * dmax(alt, 1.0e-8));
+  return P0 * pow(dmax(argument, 1.0e-12), CPOVCV);
+}
+
+__device__ __forceinline__ double safe12(double x) { return fabs(x) > 1.0e-12 ? x : 1.0e-12; }
+
+}  // namespace wg

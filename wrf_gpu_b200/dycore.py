@@ -1,0 +1,420 @@
+"""Host-side mirror of wrf_gpu's RK3 dycore step interface, on the CUDA C ABI.
+
+``rk_scan_step(carry, namelist, *, debug, lead_seconds, physics_tendencies,
+capture_pre_halo)`` keeps the signature of the reference's ``_rk_scan_step``
+(``src/gpuwrf/runtime/operational_mode.py:3319-3327``) and returns a new
+``OperationalCarry`` (functional, like the reference).  The data types mirror
+``State`` (``contracts/state.py:82-206``), ``DycoreMetrics``
+(``contracts/grid.py:66-126``), ``OperationalCarry``
+(``runtime/operational_state.py:30-127``) and the ``OperationalNamelist``
+fields the step reads (``runtime/operational_mode.py:410-700``), with torch
+float64 CUDA tensors as leaves.  PyTorch only provides device memory and the
+current stream; all arithmetic runs in ``libwrfgpu.so``.
+
+Unsupported static configurations raise ``NotImplementedError`` before any
+launch, as the reference raises at trace time.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field, fields, replace
+from typing import Any
+
+import numpy as np
+import torch
+
+from . import _capi
+
+MOIST = ("qv", "qc", "qr", "qi", "qs", "qg")
+STATE_FIELDS = _capi.STATE_FIELDS
+CARRY_FIELDS = _capi.CARRY_OUT_FIELDS
+METRIC_ARRAYS = _capi.METRIC_FIELDS
+
+
+def _dev(x, device) -> torch.Tensor:
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=torch.float64).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(np.asarray(x, dtype=np.float64)), device=device)
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    if t.dtype != torch.float64 or not t.is_contiguous() or not t.is_cuda:
+        raise ValueError("wrf_gpu_b200 arrays must be contiguous float64 CUDA tensors")
+    return t.data_ptr()
+
+
+@dataclass
+class DycoreMetrics:
+    """``DycoreMetrics`` leaves on the device (contracts/grid.py:66-126)."""
+
+    c1h: torch.Tensor
+    c2h: torch.Tensor
+    c3h: torch.Tensor
+    c4h: torch.Tensor
+    c1f: torch.Tensor
+    c2f: torch.Tensor
+    c3f: torch.Tensor
+    c4f: torch.Tensor
+    dn: torch.Tensor
+    dnw: torch.Tensor
+    rdn: torch.Tensor
+    rdnw: torch.Tensor
+    fnm: torch.Tensor
+    fnp: torch.Tensor
+    msftx: torch.Tensor
+    msfty: torch.Tensor
+    msfux: torch.Tensor
+    msfuy: torch.Tensor
+    msfvx: torch.Tensor
+    msfvy: torch.Tensor
+    f: torch.Tensor
+    e: torch.Tensor
+    sina: torch.Tensor
+    cosa: torch.Tensor
+    cf1: float
+    cf2: float
+    cf3: float
+    p_top: float
+
+    @classmethod
+    def from_host(cls, m, device="cuda") -> "DycoreMetrics":
+        kw = {n: _dev(getattr(m, n), device) for n in METRIC_ARRAYS}
+        return cls(**kw, cf1=float(m.cf1), cf2=float(m.cf2), cf3=float(m.cf3), p_top=float(m.p_top))
+
+    def cfn(self) -> tuple[float, float]:
+        """Top-face weights of the large-step PGF (core/rk_addtend_dry.py:282-288)."""
+        dn_top = float(self.dn[-1].item())
+        dnw_top = float(self.dnw[-1].item())
+        dn_safe = dn_top if abs(dn_top) > 1.0e-30 else 1.0
+        return (0.5 * dnw_top + dn_top) / dn_safe, -0.5 * dnw_top / dn_safe
+
+
+@dataclass
+class State:
+    """The ``State`` leaves the step reads and writes (contracts/state.py:82-206)."""
+
+    u: torch.Tensor
+    v: torch.Tensor
+    w: torch.Tensor
+    theta: torch.Tensor
+    p_total: torch.Tensor
+    p_perturbation: torch.Tensor
+    ph_total: torch.Tensor
+    ph_perturbation: torch.Tensor
+    mu_total: torch.Tensor
+    mu_perturbation: torch.Tensor
+    qv: torch.Tensor | None = None
+    qc: torch.Tensor | None = None
+    qr: torch.Tensor | None = None
+    qi: torch.Tensor | None = None
+    qs: torch.Tensor | None = None
+    qg: torch.Tensor | None = None
+    u_bdy: torch.Tensor | None = None
+    v_bdy: torch.Tensor | None = None
+
+    @property
+    def p(self):
+        return self.p_total
+
+    @property
+    def ph(self):
+        return self.ph_total
+
+    @property
+    def mu(self):
+        return self.mu_total
+
+    def replace(self, **kw) -> "State":
+        return replace(self, **kw)
+
+    @classmethod
+    def from_host(cls, s, device="cuda") -> "State":
+        kw = {}
+        for f_ in fields(cls):
+            v = getattr(s, f_.name, None)
+            kw[f_.name] = None if v is None else _dev(v, device)
+        return cls(**kw)
+
+    def to_host(self) -> dict:
+        return {f_.name: getattr(self, f_.name).cpu().numpy() for f_ in fields(self)
+                if getattr(self, f_.name) is not None}
+
+
+@dataclass
+class OperationalCarry:
+    """``OperationalCarry`` (runtime/operational_state.py:30-127), dycore leaves only."""
+
+    state: State
+    t_2ave: torch.Tensor | None = None
+    ww: torch.Tensor | None = None
+    mudf: torch.Tensor | None = None
+    muave: torch.Tensor | None = None
+    muts: torch.Tensor | None = None
+    ph_tend: torch.Tensor | None = None
+    u_save: torch.Tensor | None = None
+    v_save: torch.Tensor | None = None
+    w_save: torch.Tensor | None = None
+    t_save: torch.Tensor | None = None
+    ph_save: torch.Tensor | None = None
+    mu_save: torch.Tensor | None = None
+    ww_save: torch.Tensor | None = None
+    base_state: Any = None
+
+    def replace(self, **kw) -> "OperationalCarry":
+        return replace(self, **kw)
+
+
+def initial_operational_carry(state: State) -> OperationalCarry:
+    """``initial_operational_carry`` (runtime/operational_state.py:141-211), dycore leaves."""
+    ny, nx = state.mu_total.shape
+    z = lambda t: torch.zeros_like(t)
+    return OperationalCarry(
+        state=state, t_2ave=z(state.theta), ww=z(state.w), mudf=z(state.mu_total), muave=z(state.mu_total),
+        muts=state.mu_total.clone(), ph_tend=z(state.ph_perturbation), u_save=state.u.clone(),
+        v_save=state.v.clone(), w_save=state.w.clone(), t_save=state.theta.clone(),
+        ph_save=state.ph_perturbation.clone(), mu_save=state.mu_perturbation.clone(), ww_save=z(state.w))
+
+
+@dataclass
+class Tendencies:
+    """``namelist.tendencies`` base leaves (contracts/state.py Tendencies); None = zero."""
+
+    u: torch.Tensor | None = None
+    v: torch.Tensor | None = None
+    w: torch.Tensor | None = None
+    theta: torch.Tensor | None = None
+    mu: torch.Tensor | None = None
+
+
+@dataclass
+class BoundaryConfig:
+    """``BoundaryConfig`` (coupling/boundary_apply.py:71-151) fields the step reads."""
+
+    spec_bdy_width: int = 5
+    spec_zone: int = 1
+    relax_zone: int = 4
+    update_cadence_s: float = 3600.0
+    force_geopotential: bool = True
+    normal_bdy_relax_strength: float | None = None
+
+
+@dataclass
+class OperationalNamelist:
+    """The ``OperationalNamelist`` controls the RK3 step reads
+    (runtime/operational_mode.py:410-700).  Defaults are the reference's."""
+
+    metrics: DycoreMetrics
+    nx: int
+    ny: int
+    nz: int
+    dx_m: float
+    dy_m: float
+    tendencies: Tendencies = field(default_factory=Tendencies)
+    dt_s: float = 10.0
+    acoustic_substeps: int = 10
+    rk_order: int = 3
+    epssm: float = 0.1
+    hypsometric_opt: int = 1
+    h_sca_adv_order: int = 2
+    specified_bdy_cadence: bool = False
+    specified_adv_degrade: bool = False
+    top_lid: bool = False
+    run_physics: bool = True
+    run_boundary: bool = True
+    bc_source: str = "ideal"
+    boundary_config: BoundaryConfig = field(default_factory=BoundaryConfig)
+    use_vertical_solver: bool = True
+    w_damping: int = 0
+    damp_opt: int = 0
+    dampcoef: float = 0.0
+    zdamp: float = 5000.0
+    diff_opt: int = 0
+    km_opt: int = 0
+    diff_6th_opt: int = 0
+    const_nu_m2_s: float = 0.0
+    use_flux_advection: bool = False
+    scalar_adv_opt: int = 0
+    moist_adv_opt: int = 0
+    mp_physics: int = 8
+    acoustic_precision_mode: str = "fp64_default"
+    moist_cqw: bool = True
+    w_coriolis: bool = True
+    precision: str = "fp64"
+
+    @classmethod
+    def from_case(cls, case, metrics: DycoreMetrics | None = None, device="cuda", **overrides) -> "OperationalNamelist":
+        c = case.controls
+        m = metrics if metrics is not None else DycoreMetrics.from_host(case.metrics, device)
+        bc = BoundaryConfig(spec_zone=c["spec_zone"], relax_zone=c["relax_zone"],
+                            update_cadence_s=c["update_cadence_s"],
+                            normal_bdy_relax_strength=c["normal_bdy_relax_strength"])
+        kw = dict(metrics=m, nx=case.nx, ny=case.ny, nz=case.nz, dx_m=c["dx"], dy_m=c["dy"], dt_s=c["dt_s"],
+                  acoustic_substeps=c["acoustic_substeps"], epssm=c["epssm"], hypsometric_opt=c["hypsometric_opt"],
+                  h_sca_adv_order=c["h_sca_adv_order"], top_lid=c["top_lid"], run_physics=False,
+                  run_boundary=c["run_boundary"], bc_source="ideal" if c["bc_ideal"] else "wrfbdy",
+                  boundary_config=bc, w_damping=c["w_damping"], damp_opt=c["damp_opt"], dampcoef=c["dampcoef"],
+                  zdamp=c["zdamp"], use_flux_advection=True, scalar_adv_opt=c["scalar_adv_opt"],
+                  moist_adv_opt=c["moist_adv_opt"], moist_cqw=c["moist_cqw"], w_coriolis=c["w_coriolis"])
+        kw.update(overrides)
+        return cls(**kw)
+
+
+def _unsupported(nl: OperationalNamelist, physics_tendencies) -> str | None:
+    if not nl.use_flux_advection:
+        return "use_flux_advection=False (primitive M4 advection path) is not built"
+    if not nl.use_vertical_solver:
+        return "use_vertical_solver=False is not built"
+    if nl.rk_order != 3:
+        return "rk_order must be 3"
+    if nl.diff_opt or nl.km_opt or nl.diff_6th_opt or nl.const_nu_m2_s > 0.0:
+        return "explicit diffusion options are not built"
+    if nl.specified_bdy_cadence:
+        return "specified_bdy_cadence is not built"
+    if nl.specified_adv_degrade:
+        return "specified_adv_degrade is not built"
+    if not nl.boundary_config.force_geopotential and nl.run_boundary and nl.bc_source != "ideal":
+        return "nested (force_geopotential=False) boundaries are not built"
+    if nl.moist_adv_opt and nl.mp_physics in (7, 17, 18, 19, 21, 22, 24, 26, 27, 28, 38):
+        return "extra advected species of this mp_physics family are not built"
+    if nl.acoustic_precision_mode != "fp64_default":
+        return "acoustic_precision_mode other than fp64_default is not built"
+    if physics_tendencies is not None:
+        return "physics_tendencies (rk_addtend_dry merge) is not built"
+    return None
+
+
+def step_params(nl: OperationalNamelist) -> _capi.StepParams:
+    lib = _capi.load()
+    p = _capi.StepParams()
+    _capi.check(lib.wrfgpu_step_params_init(ctypes.byref(p)))
+    p.nx, p.ny, p.nz = nl.nx, nl.ny, nl.nz
+    p.dx, p.dy, p.dt = nl.dx_m, nl.dy_m, nl.dt_s
+    p.acoustic_substeps = nl.acoustic_substeps
+    p.epssm = nl.epssm
+    p.top_lid = int(bool(nl.top_lid))
+    p.w_damping, p.damp_opt = int(nl.w_damping), int(nl.damp_opt)
+    p.dampcoef, p.zdamp = float(nl.dampcoef), float(nl.zdamp)
+    p.hypsometric_opt, p.h_sca_adv_order = int(nl.hypsometric_opt), int(nl.h_sca_adv_order)
+    p.scalar_adv_opt, p.moist_adv_opt = int(nl.scalar_adv_opt), int(nl.moist_adv_opt)
+    p.run_boundary = int(bool(nl.run_boundary))
+    p.bc_ideal = int(nl.bc_source == "ideal")
+    p.spec_zone, p.relax_zone = nl.boundary_config.spec_zone, nl.boundary_config.relax_zone
+    p.update_cadence_s = float(nl.boundary_config.update_cadence_s)
+    s = nl.boundary_config.normal_bdy_relax_strength
+    p.normal_bdy_relax_strength = -1.0 if s is None else float(s)
+    p.moist_cqw, p.w_coriolis = int(bool(nl.moist_cqw)), int(bool(nl.w_coriolis))
+    p.precision = _capi.WRFGPU_PRECISION_MIXED if nl.precision == "mixed" else _capi.WRFGPU_PRECISION_FP64
+    m = nl.metrics
+    p.cf1, p.cf2, p.cf3, p.p_top = m.cf1, m.cf2, m.cf3, m.p_top
+    p.cfn, p.cfn1 = m.cfn()
+    return p
+
+
+class Stepper:
+    """Prepared step for one namelist: params, metrics struct, workspace."""
+
+    def __init__(self, nl: OperationalNamelist, device="cuda"):
+        reason = _unsupported(nl, None)
+        if reason:
+            raise NotImplementedError(reason)
+        self.lib = _capi.load()
+        self.nl = nl
+        self.params = step_params(nl)
+        _capi.check(self.lib.wrfgpu_step_params_validate(ctypes.byref(self.params)))
+        nbytes = ctypes.c_size_t(0)
+        _capi.check(self.lib.wrfgpu_step_workspace_size(ctypes.byref(self.params), ctypes.byref(nbytes)))
+        self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8, device=device)
+        self.metrics = _capi.Metrics(*[_ptr(getattr(nl.metrics, n)) for n in METRIC_ARRAYS])
+        n = ctypes.c_int(0)
+        _capi.check(self.lib.wrfgpu_step_launch_count(ctypes.byref(self.params), ctypes.byref(n)))
+        self.launches_per_step = int(n.value)
+
+    def alloc_carry(self, like: OperationalCarry) -> OperationalCarry:
+        s = like.state
+        st = State(**{f_.name: (None if getattr(s, f_.name) is None else torch.empty_like(getattr(s, f_.name)))
+                      for f_ in fields(State) if f_.name not in ("u_bdy", "v_bdy")},
+                   u_bdy=s.u_bdy, v_bdy=s.v_bdy)
+        e = lambda t: torch.empty_like(t)
+        return OperationalCarry(state=st, t_2ave=e(s.theta), ww=e(s.w), mudf=e(s.mu_total), muave=e(s.mu_total),
+                                muts=e(s.mu_total), ph_tend=e(s.w), u_save=e(s.u), v_save=e(s.v), w_save=e(s.w),
+                                t_save=e(s.theta), ph_save=e(s.w), mu_save=e(s.mu_total), ww_save=e(s.w))
+
+    def step_into(self, carry: OperationalCarry, out: OperationalCarry, lead_seconds=None, stream=None) -> None:
+        """Enqueue one step from ``carry`` into the preallocated ``out`` (no sync)."""
+        s, o, nl = carry.state, out.state, self.nl
+        ins = _capi.StepInputs()
+        for n in STATE_FIELDS:
+            setattr(ins, n, _ptr(getattr(s, n)))
+        have_q = s.qv is not None
+        for k_, n in enumerate(MOIST):
+            ins.q[k_] = _ptr(getattr(s, n)) if have_q else None
+        ins.mudf = _ptr(carry.mudf)
+        t = nl.tendencies
+        ins.base_u, ins.base_v, ins.base_w = _ptr(t.u), _ptr(t.v), _ptr(t.w)
+        ins.base_theta, ins.base_mu = _ptr(t.theta), _ptr(t.mu)
+        if nl.run_boundary and s.u_bdy is not None:
+            ins.u_bdy, ins.v_bdy = _ptr(s.u_bdy), _ptr(s.v_bdy)
+            ins.bdy_ntime, _, ins.bdy_width, _, ins.bdy_side_len = s.u_bdy.shape
+        outs = _capi.StepOutputs()
+        for n in STATE_FIELDS:
+            setattr(outs, n, _ptr(getattr(o, n)))
+        for k_, n in enumerate(MOIST):
+            outs.q[k_] = _ptr(getattr(o, n)) if have_q else None
+        for n in CARRY_FIELDS:
+            setattr(outs, n, _ptr(getattr(out, n)))
+        lead = float("nan") if lead_seconds is None else float(lead_seconds)
+        st = torch.cuda.current_stream() if stream is None else stream
+        rc = self.lib.wrfgpu_rk3_step(ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(ins),
+                                      ctypes.byref(outs), lead, ctypes.c_void_p(self.workspace.data_ptr()),
+                                      ctypes.c_size_t(self.workspace.numel()), ctypes.c_void_p(st.cuda_stream))
+        _capi.check(rc)
+
+
+_STEPPERS: dict[int, Stepper] = {}
+
+
+@dataclass
+class PreHaloCaptureResult:
+    """``_PreHaloCaptureResult`` (operational_mode.py): carry + pre-halo state.
+    On one GPU the halo exchange is a no-op, so both are the same state."""
+
+    carry: OperationalCarry
+    pre_halo_state: State
+
+
+def rk_scan_step(carry: OperationalCarry, namelist: OperationalNamelist, *, debug: bool = False, lead_seconds=None,
+                 physics_tendencies=None, capture_pre_halo: bool = False):
+    """Drop-in for ``_rk_scan_step`` (runtime/operational_mode.py:3319-3534).
+
+    Returns a new ``OperationalCarry``; ``carry`` is not modified.  The step is
+    enqueued on the current CUDA stream and is not synchronised.
+    """
+    reason = _unsupported(namelist, physics_tendencies)
+    if reason:
+        raise NotImplementedError(reason)
+    key = id(namelist)
+    stp = _STEPPERS.get(key)
+    if stp is None or stp.nl is not namelist:
+        stp = Stepper(namelist, device=carry.state.u.device)
+        _STEPPERS[key] = stp
+    if carry.mudf is None:
+        carry = carry.replace(mudf=torch.zeros_like(carry.state.mu_total))
+    out = stp.alloc_carry(carry)
+    stp.step_into(carry, out, lead_seconds=lead_seconds)
+    out.base_state = carry.base_state
+    if debug:
+        print("wrfgpu rk3 step: 3 stages, substeps", 1, max(1, namelist.acoustic_substeps // 2),
+              namelist.acoustic_substeps)
+    if capture_pre_halo:
+        return PreHaloCaptureResult(out, out.state)
+    return out
+
+
+def carry_from_case(case, device="cuda") -> OperationalCarry:
+    st = State.from_host(case.state, device)
+    c = initial_operational_carry(st)
+    return c.replace(mudf=_dev(case.mudf, device))
