@@ -1,0 +1,347 @@
+"""Benchmark of the B200-native RK3 dycore step (cell-substeps/s).
+
+Default workload (N=1): the real-like moist synthetic case at 433 x 433 x 50
+(dx 1 km, top 20 km, seeded k^-2 terrain 0-3 km, theta 295 K + N=0.011,
+5->20 m/s shear + noise, qv/qc/qr, specified lateral boundaries,
+moist_adv_opt 1, dt 6 s, 6 acoustic substeps = 10 substeps per RK3 step).
+Each timed step is one full RK3 step of that workload from the same resident
+input carry (every input array is ~75 MB, far larger than the 126 MB L2 in
+aggregate, so no L2 flush is needed).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  ``--impl reference`` times the reference
+algorithm's CPU implementation available here -- the NumPy restatement in
+``oracle/`` (JAX, the reference's own runtime, is not installed) -- on the
+host cores, on bounded 64 x 64 x 50 samples of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "cell-substeps/s"
+NX, NY, NZ = 433, 433, 50
+SAMPLE = (64, 64, 50)
+
+
+def _workload_name(nx, ny, nz, precision):
+    return f"real_like_moist_{nx}x{ny}x{nz}_specified_lbc_moist_adv_opt1_dt6_ns6_{precision}"
+
+
+# ---------------------------------------------------------------------------
+# CPU reference arm: the oracle restatement on bounded samples
+# ---------------------------------------------------------------------------
+
+def _cpu_worker(args):
+    """Run W warm-up + K oracle steps on a bounded sample; return step seconds."""
+    nx, ny, nz, steps, warmup, seed = args
+    sys.path.insert(0, HERE)
+    from types import SimpleNamespace
+    from oracle import dycore as D
+    from wrf_gpu_b200 import cases
+    case = cases.real_like_moist(nx, ny, nz, seed=seed)
+    nl = D.Namelist(metrics=case.metrics, **case.controls)
+    carry0 = SimpleNamespace(state=case.state, mudf=case.mudf)
+    with np.errstate(all="ignore"):
+        for _ in range(warmup):
+            D.rk_scan_step(carry0, nl, lead_seconds=0.0)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            D.rk_scan_step(carry0, nl, lead_seconds=0.0)
+        t1 = time.perf_counter()
+    return t1 - t0
+
+
+def cpu_reference(steps, warmup, procs):
+    import multiprocessing as mp
+    nx, ny, nz = SAMPLE
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        times = pool.map(_cpu_worker, [(nx, ny, nz, steps, warmup, i) for i in range(procs)])
+    tmax = max(times)
+    units = procs * steps * nx * ny * nz * 10
+    return units / tmax, tmax
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def _peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    from wrf_gpu_b200 import build, cases, dycore, perfmodel, _capi
+    build.build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nx, ny, nz = args.nx, args.ny, args.nz
+    case = cases.real_like_moist(nx, ny, nz, seed=rank)
+    nl = dycore.OperationalNamelist.from_case(case, device=dev, precision=args.precision)
+    carry = dycore.carry_from_case(case, device=dev)
+    stp = dycore.Stepper(nl, device=dev)
+    out = stp.alloc_carry(carry)
+    stream = torch.cuda.current_stream(dev)
+    ns = nl.acoustic_substeps
+    nsub = perfmodel.substeps_per_step(ns)
+    cells = nx * ny * nz
+
+    def step():
+        stp.step_into(carry, out, lead_seconds=0.0)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    # capture one step in a CUDA graph (launch-bound overhead removed)
+    graph = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(stream)
+    with torch.cuda.stream(s):
+        step()
+    stream.wait_stream(s)
+    torch.cuda.synchronize(dev)
+    with torch.cuda.graph(graph):
+        step()
+    graph.replay()
+    torch.cuda.synchronize(dev)
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = world * cells * nsub * args.steps / (ms / 1000.0)
+
+    # per-kernel timing over a second, instrumented region of the same steps
+    _capi.profile_enable(True, max_records=stp.launches_per_step * args.steps + 16)
+    for _ in range(args.steps):
+        step()
+    prof = _capi.profile_read()
+    _capi.profile_enable(False)
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_n) = dom
+    hbm, peak_src = _peaks()
+    bpl = perfmodel.kernel_bytes_per_launch(dom_name, nx, ny, nz, damp_opt=nl.damp_opt)
+    roof = None
+    if bpl is not None and dom_n:
+        achieved = bpl / (dom_ms / dom_n / 1000.0) / 1e9
+        roof = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": hbm,
+                "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "bytes_per_launch": bpl, "avg_launch_ms": round(dom_ms / dom_n, 4),
+                "traffic": None, "kernel_share": round(dom_ms / sum(v[0] for v in prof.values()), 4)}
+    step_bytes = perfmodel.step_bytes(nx, ny, nz, ns, moist=True)
+    whole = {"bytes_per_step": step_bytes, "achieved_gbs": round(step_bytes / (ms_per_step / 1000.0) / 1e9, 1),
+             "frac": round(step_bytes / (ms_per_step / 1000.0) / 1e9 / hbm, 4)}
+    kernels = {k: {"ms_per_step": round(v[0] / args.steps, 4), "launches_per_step": v[1] // args.steps}
+               for k, v in prof.items() if v[1]}
+
+    # end to end through the C ABI with host buffers (pinned), copies timed
+    host_in = {}
+    for f in ("u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total", "ph_perturbation", "mu_total",
+              "mu_perturbation", "qv", "qc", "qr", "qi", "qs", "qg", "u_bdy", "v_bdy"):
+        host_in[f] = getattr(carry.state, f).cpu().pin_memory()
+    host_in["mudf"] = carry.mudf.cpu().pin_memory()
+    out_tensors = [getattr(out.state, f) for f in ("u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total",
+                                                   "ph_perturbation", "mu_total", "mu_perturbation", "qv", "qc",
+                                                   "qr", "qi", "qs", "qg")]
+    out_tensors += [getattr(out, f) for f in _capi.CARRY_OUT_FIELDS]
+    host_out = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in out_tensors]
+    h2d = sum(t.numel() * 8 for t in host_in.values())
+    d2h = sum(t.numel() * 8 for t in host_out)
+
+    def e2e_step():
+        for f, h in host_in.items():
+            dst = carry.mudf if f == "mudf" else getattr(carry.state, f)
+            dst.copy_(h, non_blocking=True)
+        step()
+        for h, t in zip(host_out, out_tensors):
+            h.copy_(t, non_blocking=True)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    k_e2e = max(1, min(args.steps, 5))
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(k_e2e):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = f0.elapsed_time(f1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * cells * nsub * k_e2e / (e2e_ms / 1000.0)
+    out_ok = bool(torch.isfinite(out.state.w).all().item() and torch.isfinite(out.state.theta).all().item())
+    del graph
+    return dict(value=value, ms_per_step=ms_per_step, clocks=clk, roofline=roof, whole_step_roofline=whole,
+                kernels=kernels, e2e={"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                                      "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e},
+                launches=stp.launches_per_step * args.steps, finite=out_ok)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--nz", type=int, default=NZ)
+    ap.add_argument("--cpu-procs", type=int, default=0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    workload = _workload_name(args.nx, args.ny, args.nz, args.precision)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        procs = args.cpu_procs or max(1, min(os.cpu_count() or 1, 32))
+        value, tmax = cpu_reference(args.steps, args.warmup, procs)
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tmax * 1000.0 / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": workload, "sample": f"{SAMPLE[0]}x{SAMPLE[1]}x{SAMPLE[2]} crops x {procs} procs"},
+                "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "port",
+                                 "sample": f"{procs} processes x {args.steps} RK3 steps of a "
+                                           f"{SAMPLE[0]}x{SAMPLE[1]}x{SAMPLE[2]} real-like moist sample (NumPy oracle; "
+                                           "JAX is not installed, so the reference's own JAX-CPU step cannot run)"},
+                "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    r = run_gpu(args, rank, world, local_rank)
+    cpu = None
+    if rank == 0:
+        # bounded CPU baseline sample: 1 process, 2 steps of the 64x64x50 sample
+        v, tmax = cpu_reference(2, 0, 1)
+        cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": "port",
+               "sample": f"2 RK3 steps of a {SAMPLE[0]}x{SAMPLE[1]}x{SAMPLE[2]} crop of the same workload "
+                         f"on 1 core (NumPy oracle), {tmax:.1f} s"}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64",
+                "data": "synthetic",
+                "config": {"workload": workload, "nx": args.nx, "ny": args.ny, "nz": args.nz,
+                           "substeps_per_step": 10, "l2": "inputs larger than L2 (no flush)",
+                           "parallelism": f"replicas x{world}", "cuda_graph": True},
+                "e2e": r["e2e"], "roofline": r["roofline"], "whole_step_roofline": r["whole_step_roofline"],
+                "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": r["launches"],
+                "kernels": r["kernels"], "finite": r["finite"]}
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -142,6 +142,17 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *params, const wrfgpu_metrics *metr
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 
+/* Per-kernel device timing (no counterpart in the reference: its XLA program
+ * is profiled with nsys).  When enabled, every launch of wrfgpu_rk3_step is
+ * bracketed by CUDA events from a pool of max_records pairs;
+ * wrfgpu_profile_read synchronises on the last event, returns the summed
+ * milliseconds and launch counts per kernel class and resets the pool.
+ * Not for use inside CUDA graph capture. */
+int wrfgpu_profile_enable(int enable, int max_records);
+int wrfgpu_profile_read(double *total_ms, int *counts, int nclasses, int *dropped);
+int wrfgpu_profile_class_count(void);
+const char *wrfgpu_profile_class_name(int cls);
+
 /* Last error of the calling host thread ("" when none). */
 const char *wrfgpu_last_error_string(void);
 

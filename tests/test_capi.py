@@ -1,0 +1,130 @@
+"""C ABI and host-logic tests that need no GPU: the library loads, exports
+every entry point declared in include/wrfgpu.h, and rejects unsupported
+configurations before touching the device (the reference raises at trace
+time for these, e.g. core/calc_p_rho.py:119-122)."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from wrf_gpu_b200 import _capi, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return _capi.load()
+
+
+def _declared_functions():
+    text = open(os.path.join(ROOT, "include", "wrfgpu.h")).read()
+    return sorted(set(re.findall(r"\b(wrfgpu_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = _declared_functions()
+    assert "wrfgpu_rk3_step" in names
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_capi.EXPORTED)
+
+
+def test_params_init_defaults_match_reference_namelist(lib):
+    p = _capi.StepParams()
+    assert lib.wrfgpu_step_params_init(ctypes.byref(p)) == 0
+    # OperationalNamelist defaults (runtime/operational_mode.py:410-700)
+    assert p.dt == 10.0 and p.acoustic_substeps == 10 and p.epssm == 0.1
+    assert p.top_lid == 0 and p.w_damping == 0 and p.damp_opt == 0 and p.zdamp == 5000.0
+    assert p.hypsometric_opt == 1 and p.h_sca_adv_order == 2
+    assert p.scalar_adv_opt == 0 and p.moist_adv_opt == 0
+    assert p.spec_zone == 1 and p.relax_zone == 4 and p.update_cadence_s == 3600.0
+    assert p.moist_cqw == 1 and p.w_coriolis == 1
+
+
+def _params(lib, **kw):
+    p = _capi.StepParams()
+    lib.wrfgpu_step_params_init(ctypes.byref(p))
+    p.nx, p.ny, p.nz, p.dx, p.dy = 16, 12, 10, 1000.0, 1000.0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+@pytest.mark.parametrize("kw,code", [
+    (dict(nz=3), _capi.WRFGPU_ERR_BAD_SHAPE),
+    (dict(nx=0), _capi.WRFGPU_ERR_BAD_SHAPE),
+    (dict(dx=0.0), _capi.WRFGPU_ERR_BAD_SHAPE),
+    (dict(hypsometric_opt=3), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(scalar_adv_opt=3), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(moist_adv_opt=4), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(run_boundary=1, bc_ideal=0, h_sca_adv_order=5), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(run_boundary=1, relax_zone=6), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(precision=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+])
+def test_validate_rejects(lib, kw, code):
+    p = _params(lib, **kw)
+    assert lib.wrfgpu_step_params_validate(ctypes.byref(p)) == code
+    assert lib.wrfgpu_last_error_string().decode() != ""
+
+
+def test_validate_accepts_reference_defaults(lib):
+    p = _params(lib)
+    assert lib.wrfgpu_step_params_validate(ctypes.byref(p)) == 0
+
+
+def test_workspace_size_grows_with_grid_and_options(lib):
+    sizes = []
+    for kw in (dict(), dict(nx=32), dict(moist_adv_opt=1), dict(run_boundary=1, bc_ideal=0)):
+        p = _params(lib, **kw)
+        n = ctypes.c_size_t(0)
+        assert lib.wrfgpu_step_workspace_size(ctypes.byref(p), ctypes.byref(n)) == 0
+        sizes.append(n.value)
+    assert sizes[0] > 0 and sizes[1] > sizes[0] and sizes[2] > sizes[0] and sizes[3] > sizes[0]
+
+
+def test_launch_count(lib):
+    p = _params(lib, acoustic_substeps=6)
+    n = ctypes.c_int(0)
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(n)) == 0
+    # 3 stages x (8 stage + 3 finish) + 3 launches per substep x (1 + 3 + 6)
+    assert n.value == 3 * 11 + 3 * 10
+
+
+def test_null_pointers_rejected_before_any_launch(lib):
+    p = _params(lib)
+    m = _capi.Metrics()
+    ins = _capi.StepInputs()
+    outs = _capi.StepOutputs()
+    rc = lib.wrfgpu_rk3_step(ctypes.byref(p), ctypes.byref(m), ctypes.byref(ins), ctypes.byref(outs),
+                             float("nan"), None, 0, None)
+    assert rc in (_capi.WRFGPU_ERR_WORKSPACE, _capi.WRFGPU_ERR_NULL_POINTER)
+    assert lib.wrfgpu_rk3_step(None, None, None, None, 0.0, None, 0, None) == _capi.WRFGPU_ERR_NULL_POINTER
+
+
+def test_host_shim_rejects_unsupported_namelist():
+    import numpy as np
+    import torch
+
+    from wrf_gpu_b200 import cases, dycore
+
+    case = cases.warm_bubble_3d(8, 6, 6)
+    m = dycore.DycoreMetrics(**{n: torch.as_tensor(np.asarray(getattr(case.metrics, n)))
+                                for n in _capi.METRIC_FIELDS},
+                             cf1=case.metrics.cf1, cf2=case.metrics.cf2, cf3=case.metrics.cf3,
+                             p_top=case.metrics.p_top)
+    st = dycore.State.from_host(case.state, device="cpu")
+    carry = dycore.initial_operational_carry(st)
+    for kw in (dict(use_flux_advection=False), dict(diff_opt=2), dict(specified_bdy_cadence=True),
+               dict(const_nu_m2_s=75.0), dict(acoustic_precision_mode="mixed_perturb_fp32")):
+        nl = dycore.OperationalNamelist.from_case(case, metrics=m, **kw)
+        with pytest.raises(NotImplementedError):
+            dycore.rk_scan_step(carry, nl)
+    nl = dycore.OperationalNamelist.from_case(case, metrics=m)
+    with pytest.raises(NotImplementedError):
+        dycore.rk_scan_step(carry, nl, physics_tendencies=object())

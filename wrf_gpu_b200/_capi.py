@@ -72,7 +72,9 @@ class StepOutputs(ctypes.Structure):
 
 
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
-            "wrfgpu_rk3_step", "wrfgpu_step_launch_count", "wrfgpu_last_error_string", "wrfgpu_version")
+            "wrfgpu_rk3_step", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
+            "wrfgpu_version")
 
 _lib = None
 
@@ -99,6 +101,14 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_rk3_step.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), ctypes.POINTER(StepInputs),
                                     ctypes.POINTER(StepOutputs), _D, _P, ctypes.c_size_t, _P]
     lib.wrfgpu_rk3_step.restype = _I
+    lib.wrfgpu_profile_enable.argtypes = [_I, _I]
+    lib.wrfgpu_profile_enable.restype = _I
+    lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]
+    lib.wrfgpu_profile_read.restype = _I
+    lib.wrfgpu_profile_class_count.argtypes = []
+    lib.wrfgpu_profile_class_count.restype = _I
+    lib.wrfgpu_profile_class_name.argtypes = [_I]
+    lib.wrfgpu_profile_class_name.restype = ctypes.c_char_p
     lib.wrfgpu_last_error_string.argtypes = []
     lib.wrfgpu_last_error_string.restype = ctypes.c_char_p
     lib.wrfgpu_version.argtypes = []
@@ -119,3 +129,18 @@ class WrfGpuError(RuntimeError):
 def check(code: int) -> None:
     if code != WRFGPU_OK:
         raise WrfGpuError(code, load().wrfgpu_last_error_string().decode())
+
+
+def profile_enable(enable: bool, max_records: int = 8192) -> None:
+    check(load().wrfgpu_profile_enable(int(bool(enable)), int(max_records)))
+
+
+def profile_read() -> dict:
+    """Summed device milliseconds and launch counts per kernel class (synchronises)."""
+    lib = load()
+    n = lib.wrfgpu_profile_class_count()
+    ms = (_D * n)()
+    cnt = (_I * n)()
+    dropped = _I(0)
+    check(lib.wrfgpu_profile_read(ms, cnt, n, ctypes.byref(dropped)))
+    return {lib.wrfgpu_profile_class_name(c).decode(): (float(ms[c]), int(cnt[c])) for c in range(n)}

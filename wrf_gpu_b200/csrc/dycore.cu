@@ -9,6 +9,7 @@
 #include <cstring>
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "../../include/wrfgpu.h"
 #include "dycore_common.cuh"
@@ -205,17 +206,114 @@ int check_launch(const char *what) {
   return WRFGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Optional per-kernel timing: when enabled, every launch is bracketed by a
+// pair of CUDA events (from a pool created at enable time) so a caller can
+// read the device time of each kernel class over a region of steps.
+// ---------------------------------------------------------------------------
+struct ProfState {
+  bool on = false;
+  int cap = 0;
+  int used = 0;
+  std::vector<cudaEvent_t> ev;   // 2 per record
+  std::vector<int> cls;
+  cudaStream_t stream = nullptr;
+};
+ProfState g_prof;
+
+const char *kClassNames[] = {"k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
+                             "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_u",
+                             "k_advance_v", "k_column", "k_finish_u", "k_finish_v", "k_finish_col"};
+constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
+
+int class_of(const char *name) {
+  for (int c = 0; c < kNumClasses; ++c)
+    if (std::strcmp(kClassNames[c], name) == 0) return c;
+  return -1;
+}
+
+int g_pending_class = -1;
+
+void prof_begin(const char *name, cudaStream_t s) {
+  if (!g_prof.on) return;
+  g_pending_class = -1;
+  if (g_prof.used >= g_prof.cap) return;
+  const int c = class_of(name);
+  if (c < 0) return;
+  cudaEventRecord(g_prof.ev[2 * g_prof.used], s);
+  g_pending_class = c;
+  g_prof.stream = s;
+}
+
+void prof_end(cudaStream_t s) {
+  if (!g_prof.on || g_pending_class < 0) return;
+  cudaEventRecord(g_prof.ev[2 * g_prof.used + 1], s);
+  g_prof.cls[g_prof.used] = g_pending_class;
+  g_prof.used += 1;
+  g_pending_class = -1;
+}
+
 #define LAUNCH_CHECK(name)                      \
   do {                                          \
+    prof_end(stream);                           \
     int _rc = check_launch(name);               \
     if (_rc != WRFGPU_OK) return _rc;           \
   } while (0)
+
+#define PROF(name) prof_begin(name, stream)
 
 }  // namespace
 
 extern "C" {
 
 const char *wrfgpu_last_error_string(void) { return g_last_error.c_str(); }
+
+int wrfgpu_profile_enable(int enable, int max_records) {
+  if (g_prof.on) {
+    for (cudaEvent_t e : g_prof.ev) cudaEventDestroy(e);
+    g_prof.ev.clear();
+    g_prof.cls.clear();
+    g_prof.on = false;
+  }
+  if (!enable) return WRFGPU_OK;
+  if (max_records < 1) return fail(WRFGPU_ERR_BAD_SHAPE, "max_records must be >= 1");
+  g_prof.ev.resize(2 * (size_t)max_records);
+  g_prof.cls.assign(max_records, -1);
+  for (auto &e : g_prof.ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "cudaEventCreate failed");
+  g_prof.cap = max_records;
+  g_prof.used = 0;
+  g_prof.on = true;
+  return WRFGPU_OK;
+}
+
+int wrfgpu_profile_read(double *total_ms, int *counts, int nclasses, int *dropped) {
+  if (total_ms == nullptr || counts == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "output arrays are NULL");
+  for (int c = 0; c < nclasses; ++c) {
+    total_ms[c] = 0.0;
+    counts[c] = 0;
+  }
+  if (!g_prof.on) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "profiling is not enabled");
+  if (g_prof.used > 0 && cudaEventSynchronize(g_prof.ev[2 * (g_prof.used - 1) + 1]) != cudaSuccess)
+    return fail(WRFGPU_ERR_CUDA, "cudaEventSynchronize failed");
+  for (int r = 0; r < g_prof.used; ++r) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, g_prof.ev[2 * r], g_prof.ev[2 * r + 1]) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "cudaEventElapsedTime failed");
+    const int c = g_prof.cls[r];
+    if (c >= 0 && c < nclasses) {
+      total_ms[c] += ms;
+      counts[c] += 1;
+    }
+  }
+  if (dropped) *dropped = 0;
+  g_prof.used = 0;
+  return WRFGPU_OK;
+}
+
+int wrfgpu_profile_class_count(void) { return kNumClasses; }
+
+const char *wrfgpu_profile_class_name(int c) { return (c >= 0 && c < kNumClasses) ? kClassNames[c] : ""; }
 
 const char *wrfgpu_version(void) { return "wrfgpu-b200 0.1.0 (fp64 reference-order kernels, sm_100a)"; }
 
@@ -394,19 +492,24 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       for (int q = 0; q < 6; ++q) o.q[q] = nullptr;  // moisture passes through untouched
     }
     Mass2D m2{w.mub, w.mut, w.muts0, w.mu_work0, w.muu, w.muus, w.muv, w.muvs, w.mu, w.muts, w.muave};
+    PROF("k_mass2d");
     k_mass2d<<<grd(nx + 1, ny + 1, 1), blk2(), 0, stream>>>(g, s, origin.mu_pert, rk, m2);
     LAUNCH_CHECK("k_mass2d");
+    PROF("k_transport");
     k_transport<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, s.u, s.v, s.mu_total, w.ru, w.rv, w.rom,
                                                        specified ? w.ww_spec : nullptr);
     LAUNCH_CHECK("k_transport");
     Diag dg{w.alt_raw, w.alt, w.pb, w.c2a, w.qtot, w.al_ls, w.php_ls, w.php};
+    PROF("k_diag");
     k_diag<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, s, p.hypsometric_opt, dg);
     LAUNCH_CHECK("k_diag");
     UFaceOut uo{w.u_tend, w.u_w, w.cqu};
+    PROF("k_uface");
     k_uface<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
                                                        in->base_u, p.top_lid, p.run_boundary, uo);
     LAUNCH_CHECK("k_uface");
     VFaceOut vo{w.v_tend, w.v_w, w.cqv};
+    PROF("k_vface");
     k_vface<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
                                                        in->base_v, p.top_lid, p.run_boundary, vo);
     LAUNCH_CHECK("k_vface");
@@ -416,6 +519,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     mo.t_tend = w.t_tend;
     mo.theta_w = w.theta_w;
     for (int q = 0; q < 6; ++q) mo.q_tend[q] = w.qtend[q];
+    PROF("k_mass");
     k_mass<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta,
                                                    lim_theta ? 0 : 1, (moist && !lim_moist) ? 1 : 0, mo);
     LAUNCH_CHECK("k_mass");
@@ -425,8 +529,10 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       if (lim_theta) {
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
+        PROF("k_lim_scale");
         k_lim_scale<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2);
         LAUNCH_CHECK("k_lim_scale");
+        PROF("k_lim_tend");
         k_lim_tend<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2, in->base_theta,
                                                            s.mu_total, w.t_tend);
         LAUNCH_CHECK("k_lim_tend");
@@ -435,8 +541,10 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.opt = p.moist_adv_opt;
         la.offset = 0.0;
         for (int q = 0; q < 6; ++q) {
+          PROF("k_lim_scale");
           k_lim_scale<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2);
           LAUNCH_CHECK("k_lim_scale");
+          PROF("k_lim_tend");
           k_lim_tend<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr,
                                                              s.mu_total, w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
@@ -445,6 +553,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     }
     const double *ww_stage = specified ? w.ww_spec : w.rom;
     WFaceOut wo{w.rw_tend, w.ph_tend, w.cqw, w.w_w, w.ph_w, w.pt1, w.ww, w.phb0};
+    PROF("k_wface");
     k_wface<<<grd(nx, ny, nz + 1), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot, w.mub,
                                                        w.mut, w.muts0, w.muu, w.muv, in->base_w, p.top_lid,
                                                        p.moist_cqw, p.w_coriolis, wo);
@@ -452,6 +561,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     const double x = 0.5 * dts * G * eps1;
     const double cof = x * x;
     CoefOut co{w.a, w.alpha, w.gamma, w.p, w.pm1, w.al, w.t2ave};
+    PROF("k_coef");
     k_coef<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, w.mut, w.muts0, w.mu_work0, w.c2a, w.cqw, w.alt, w.theta_w,
                                                   w.ph_w, origin.theta, cof, p.top_lid, co);
     LAUNCH_CHECK("k_coef");
@@ -460,8 +570,10 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     ba.active = bdy_active ? 1 : 0;
     if (bdy_active) {
       const int nzone = p.spec_zone + p.relax_zone;
+      PROF("k_bdy_target_u");
       k_bdy_target_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, bl_u, s.u, w.muu, w.muus, nzone, w.u_target);
       LAUNCH_CHECK("k_bdy_target_u");
+      PROF("k_bdy_target_v");
       k_bdy_target_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, bl_v, s.v, w.muv, w.muvs, nzone, w.v_target);
       LAUNCH_CHECK("k_bdy_target_v");
       const double strength = (p.normal_bdy_relax_strength < 0.0) ? 20.0 : p.normal_bdy_relax_strength;
@@ -484,16 +596,21 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     A.u_1 = s.u; A.v_1 = s.v; A.w_save = s.w; A.theta_s = s.theta; A.phb0 = w.phb0;
     ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp};
     for (int it = 0; it < nsub[stage]; ++it) {
+      PROF("k_advance_u");
       k_advance_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
       LAUNCH_CHECK("k_advance_u");
+      PROF("k_advance_v");
       k_advance_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
       LAUNCH_CHECK("k_advance_v");
+      PROF("k_column");
       k_column<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, A, ca);
       LAUNCH_CHECK("k_column");
     }
 
+    PROF("k_finish_u");
     k_finish_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, w.u_w, s.u, w.muu, w.muus, o.u);
     LAUNCH_CHECK("k_finish_u");
+    PROF("k_finish_v");
     k_finish_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, w.v_w, s.v, w.muv, w.muvs, o.v);
     LAUNCH_CHECK("k_finish_v");
     FinishArgs fa;
@@ -506,6 +623,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     fa.t_2ave_out = (stage == 2) ? out->t_2ave : nullptr;
     fa.ww_out = (stage == 2) ? out->ww : nullptr;
     fa.t_save_out = (stage == 2) ? out->t_save : nullptr;
+    PROF("k_finish_col");
     k_finish_col<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, s, origin, fa, o);
     LAUNCH_CHECK("k_finish_col");
 
