@@ -1,0 +1,313 @@
+// Column kernel of one acoustic substep, level-parallel version.
+//
+// A block owns TX = 32 adjacent columns of one row j and all levels.  Its 8
+// warps split the levels (warp w handles k = w, w+8, ...) for every part of
+// advance_mu_t / advance_w / calc_p_rho that is independent across levels;
+// only the four genuine column recurrences run serially, one thread per
+// column, out of shared memory:
+//   * dmdt = sum_k dnw*dvdxi            (dynamics/mu_t_advance.py:205)
+//   * the ww prefix subtraction         (dynamics/mu_t_advance.py:229-237)
+//   * the Thomas forward and back sweeps (core/advance_w.py:558-592)
+// Every expression keeps the operation order of the thread-per-column form
+// (and of the reference), so results are identical to it bit for bit.
+#pragma once
+#include "dycore_common.cuh"
+#include "acoustic_kernels.cuh"
+
+namespace wg {
+
+constexpr int COL_TX = 32;
+constexpr int COL_TY = 8;
+constexpr int COL_NARR = 7;
+
+inline size_t column_tiled_smem_bytes(int nz) { return (size_t)COL_NARR * (nz + 1) * COL_TX * sizeof(double); }
+
+__global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoustic A, ColArgs c) {
+  extern __shared__ double sm[];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * COL_TX + tx;
+  const int j = blockIdx.y;
+  const bool valid = i < nx;
+  const int L = nz + 1;
+  auto S = [&](int a, int k) -> double & { return sm[((size_t)a * L + k) * COL_TX + tx]; };
+  // array roles (see the phase list below)
+  constexpr int A0 = 0, A1 = 1, A2 = 2, A3 = 3, A4 = 4, A5 = 5, A6 = 6;
+  const size_t c2d = valid ? ix2(j, i, nx) : 0;
+  auto M = [&](int k) { return ix3(k, j, i, ny, nx); };
+  const double dts = c.dts;
+  const double eps_p = 1.0 + c.epssm, eps_m = 1.0 - c.epssm;
+  const double msftx = valid ? ld(g.msftx, c2d) : 1.0;
+  const double msfty = valid ? ld(g.msfty, c2d) : 1.0;
+  const double mut = valid ? ld(A.mut, c2d) : 1.0;
+  const bool active = valid && (!c.specified || (j >= 1 && j <= ny - 2 && i >= 1 && i <= nx - 2));
+  auto T1 = [&](int k, int jj, int ii2) { return ld(A.theta_s, ix3(k, jj, ii2, ny, nx)) - T0; };
+  const int nxu = nx + 1, nyv = ny + 1;
+
+  __shared__ double s_dmdt[COL_TX], s_mutend[COL_TX], s_scale[COL_TX];
+
+  // ---------------- P1: dvdxi per level -> A0 ----------------
+  if (active) {
+    const double muv_n = ld(A.muv, ix2(j + 1, i, nx)), muv_s = ld(A.muv, ix2(j, i, nx));
+    const double muu_e = ld(A.muu, ix2(j, i + 1, nxu)), muu_w = ld(A.muu, ix2(j, i, nxu));
+    const double fvi_n = 1.0 / ld(g.msfvx, ix2(j + 1, i, nx)), fvi_s = 1.0 / ld(g.msfvx, ix2(j, i, nx));
+    const double fuy_e = ld(g.msfuy, ix2(j, i + 1, nxu)), fuy_w = ld(g.msfuy, ix2(j, i, nxu));
+    for (int k = ty; k < nz; k += COL_TY) {
+      const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+      const double vn = A.v[ix3(k, j + 1, i, nyv, nx)] + (c1 * muv_n + c2) * ld(A.v_1, ix3(k, j + 1, i, nyv, nx)) * fvi_n;
+      const double vs = A.v[ix3(k, j, i, nyv, nx)] + (c1 * muv_s + c2) * ld(A.v_1, ix3(k, j, i, nyv, nx)) * fvi_s;
+      const double ue = A.u[ix3(k, j, i + 1, ny, nxu)] + (c1 * muu_e + c2) * ld(A.u_1, ix3(k, j, i + 1, ny, nxu)) / fuy_e;
+      const double uw = A.u[ix3(k, j, i, ny, nxu)] + (c1 * muu_w + c2) * ld(A.u_1, ix3(k, j, i, ny, nxu)) / fuy_w;
+      S(A0, k) = msftx * msfty * (g.rdy * (vn - vs) + g.rdx * (ue - uw));
+    }
+  }
+  __syncthreads();
+  // ---------------- P2: column sum and 2-D mass updates (serial, ty == 0) ----------------
+  if (ty == 0 && active) {
+    double dmdt = 0.0;
+    for (int k = 0; k < nz; ++k) {
+      const double t = ld(g.dnw, k) * S(A0, k);
+      dmdt = (k == 0) ? t : dmdt + t;
+    }
+    const double mu_work_old = A.muts[c2d] - mut;
+    const double mu_save = A.mu[c2d] - mu_work_old;
+    double mu_tend = (A.mu_tend != nullptr) ? ld(A.mu_tend, c2d) : 0.0;
+    double mu_tendency = dmdt + mu_tend;
+    double scale = 1.0;
+    if (c.specified) {
+      const double floor_ = dmax(MIN_MUTS_PA, MIN_MUTS_FRACTION * mut);
+      const double muts_old = mut + mu_work_old;
+      const double raw = dts * mu_tendency;
+      const double allowed = dmax(muts_old - floor_, 0.0);
+      const double loss = -raw;
+      const bool finite = isfinite(raw) && isfinite(muts_old);
+      scale = (finite && (loss > allowed)) ? allowed / dmax(loss, 1.0) : (finite ? 1.0 : 0.0);
+      scale = dmin(dmax(scale, 0.0), 1.0);
+      mu_tendency = mu_tendency * scale;
+      dmdt = dmdt * scale;
+      mu_tend = mu_tend * scale;
+    }
+    const double mu_work_new = mu_work_old + dts * mu_tendency;
+    A.mu[c2d] = mu_save + mu_work_new;
+    A.mudf[c2d] = mu_tendency;
+    A.muts[c2d] = mut + mu_work_new;
+    A.muave[c2d] = 0.5 * ((1.0 + c.epssm) * mu_work_new + (1.0 - c.epssm) * mu_work_old);
+    s_dmdt[tx] = dmdt;
+    s_mutend[tx] = mu_tend;
+    s_scale[tx] = scale;
+  }
+  __syncthreads();
+  // ---------------- P3: ww increments -> A1, ww_1 -> A2, old ww (inactive) -> A3 ----------------
+  if (valid) {
+    if (active) {
+      const double dmdt = s_dmdt[tx], mu_tend = s_mutend[tx], scale = s_scale[tx];
+      for (int kk = 1 + ty; kk < nz; kk += COL_TY) {
+        const int k = kk - 1;
+        double dv = S(A0, k);
+        if (c.specified) dv = dv * scale;
+        S(A1, kk) = ld(g.dnw, k) * (ld(g.c1h, k) * dmdt + dv + ld(g.c1h, k) * mu_tend) / msfty;
+      }
+      for (int k = ty; k <= nz; k += COL_TY) S(A2, k) = ld(A.ww_1, M(k));
+    } else {
+      for (int k = ty; k <= nz; k += COL_TY) S(A3, k) = A.ww[M(k)];
+    }
+  }
+  __syncthreads();
+  // ---------------- P4: ww prefix (serial) -> A3 ----------------
+  if (ty == 0 && active) {
+    double prev = A.ww[M(0)];
+    S(A3, 0) = prev - S(A2, 0);
+    for (int kk = 1; kk < nz; ++kk) {
+      const double cur = prev - S(A1, kk);
+      S(A3, kk) = cur - S(A2, kk);
+      prev = cur;
+    }
+    S(A3, nz) = A.ww[M(nz)];
+  }
+  __syncthreads();
+  // ---------------- P5: theta update, t_2ave, wd -> A0, buoy -> A1 ----------------
+  const double muts = valid ? A.muts[c2d] : 1.0;
+  const double muave = valid ? A.muave[c2d] : 0.0;
+  if (valid) {
+    for (int k = ty; k <= nz; k += COL_TY) A.ww[M(k)] = S(A3, k);
+    int ie = 0, iw = 0, jn = 0, js = 0;
+    if (c.specified) {
+      ie = i + 1; iw = i - 1; jn = j + 1; js = j - 1;
+    } else {
+      ie = wrp(i + 1, nx); iw = wrp(i - 1, nx); jn = wrp(j + 1, ny); js = wrp(j - 1, ny);
+    }
+    for (int k = ty; k < nz; k += COL_TY) {
+      double thw = A.theta_w[M(k)];
+      if (active) {
+        const double wdtn_hi = (k + 1 <= nz - 1)
+                                   ? S(A3, k + 1) * (ld(g.fnm, k + 1) * T1(k + 1, j, i) + ld(g.fnp, k + 1) * T1(k, j, i))
+                                   : 0.0;
+        const double wdtn_lo = (k >= 1) ? S(A3, k) * (ld(g.fnm, k) * T1(k, j, i) + ld(g.fnp, k) * T1(k - 1, j, i)) : 0.0;
+        const double th = T1(k, j, i);
+        const double v_flux = A.v[ix3(k, j + 1, i, nyv, nx)] * (T1(k, jn, i) + th) - A.v[ix3(k, j, i, nyv, nx)] * (th + T1(k, js, i));
+        const double u_flux = A.u[ix3(k, j, i + 1, ny, nxu)] * (T1(k, j, ie) + th) - A.u[ix3(k, j, i, ny, nxu)] * (th + T1(k, j, iw));
+        const double tend = msftx * (0.5 * g.rdy * v_flux + 0.5 * g.rdx * u_flux) + ld(g.rdnw, k) * (wdtn_hi - wdtn_lo);
+        const double theta_i = thw + msfty * dts * ld(A.t_tend, M(k));
+        thw = theta_i - dts * msfty * tend;
+        A.theta_w[M(k)] = thw;
+      }
+      const double mass_h = ld(g.c1h, k) * muts + ld(g.c2h, k);
+      const double half = 0.5 * (eps_p * thw + eps_m * A.t2ave[M(k)]);
+      const double t2a = (half + (ld(g.c1h, k) * muave) * T0) / (mass_h * (T0 + T1(k, j, i)));
+      A.t2ave[M(k)] = t2a;
+      S(A1, k) = ld(A.c2a, M(k)) * ld(A.alt, M(k)) * t2a;
+      const double wwm = 0.5 * (S(A3, k + 1) + S(A3, k));
+      S(A0, k) = wwm * ld(g.rdnw, k) * (ld(A.pt1, M(k + 1)) - ld(A.pt1, M(k)));
+    }
+  }
+  __syncthreads();
+  // ---------------- P6: rhs -> A2 (faces 1..nz), old ph -> A4 (faces 0..nz) ----------------
+  const double c05gem = 0.5 * G * eps_m;
+  if (valid) {
+    for (int f = ty; f <= nz; f += COL_TY) {
+      const double phf = A.ph[M(f)];
+      S(A4, f) = phf;
+      if (f == 0) {
+        S(A2, 0) = 0.0;
+        continue;
+      }
+      double r = dts * (ld(A.ph_tend, M(f)) + c05gem * A.w[M(f)]);
+      if (f < nz) r = r + (-(dts * (ld(g.fnm, f) * S(A0, f) + ld(g.fnp, f) * S(A0, f - 1))));
+      const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
+      r = phf + msfty * r / mf;
+      if (f == nz && c.top_lid) r = 0.0;
+      S(A2, f) = r;
+    }
+  }
+  __syncthreads();
+  // ---------------- P7: explicit w -> A5, a -> A0, alpha -> A3, gamma -> A6 ----------------
+  const double minv = 1.0 / msfty;
+  if (valid) {
+    const double c05dg = 0.5 * dts * G;
+    const double dtsg = dts * G;
+    for (int f = ty; f <= nz; f += COL_TY) {
+      double wn;
+      if (f == 0) {
+        auto HT = [&](int jj, int ii2) {
+          jj = jj < 0 ? 0 : (jj > ny - 1 ? ny - 1 : jj);
+          ii2 = ii2 < 0 ? 0 : (ii2 > nx - 1 ? nx - 1 : ii2);
+          return ld(A.phb0, ix2(jj, ii2, nx)) / G;
+        };
+        const double htc = HT(j, i);
+        const double dy_n = HT(j + 1, i) - htc, dy_s = htc - HT(j - 1, i);
+        const double dx_e = HT(j, i + 1) - htc, dx_w = htc - HT(j, i - 1);
+        auto vcf = [&](int jv) {
+          return g.cf1 * ld(A.v_1, ix3(0, jv, i, nyv, nx)) + g.cf2 * ld(A.v_1, ix3(1, jv, i, nyv, nx)) +
+                 g.cf3 * ld(A.v_1, ix3(2, jv, i, nyv, nx));
+        };
+        auto ucf = [&](int iu) {
+          return g.cf1 * ld(A.u_1, ix3(0, j, iu, ny, nxu)) + g.cf2 * ld(A.u_1, ix3(1, j, iu, ny, nxu)) +
+                 g.cf3 * ld(A.u_1, ix3(2, j, iu, ny, nxu));
+        };
+        wn = msfty * 0.5 * g.rdy * (dy_n * vcf(j + 1) + dy_s * vcf(j)) +
+             msftx * 0.5 * g.rdx * (dx_e * ucf(i + 1) + dx_w * ucf(i));
+      } else if (f < nz) {
+        const double w_old = A.w[M(f)];
+        double rw = ld(A.rw_tend, M(f));
+        if (c.w_damping == 1) {
+          const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
+          const double vert_cfl = fabs(S(A3, f) / safe12(mf) * ld(g.rdnw, f) * dts);
+          double damp = -sgn(w_old) * W_ALPHA * (vert_cfl - W_BETA) * mf;
+          damp = (vert_cfl > W_BETA) ? damp : 0.0;
+          rw = rw + damp;
+        }
+        wn = w_old + dts * rw;
+        const double coef_f = ld(A.c2a, M(f)) * ld(g.rdnw, f) / safe12(ld(g.c1h, f) * mut + ld(g.c2h, f));
+        const double coef_m1 = ld(A.c2a, M(f - 1)) * ld(g.rdnw, f - 1) / safe12(ld(g.c1h, f - 1) * mut + ld(g.c2h, f - 1));
+        const double tA_u = coef_f * (eps_p * (S(A2, f + 1) - S(A2, f)) + eps_m * (S(A4, f + 1) - S(A4, f)));
+        const double tA_l = coef_m1 * (eps_p * (S(A2, f) - S(A2, f - 1)) + eps_m * (S(A4, f) - S(A4, f - 1)));
+        const double tA = minv * ld(A.cqw, M(f)) * (c05dg * ld(g.rdn, f)) * (tA_u - tA_l);
+        const double tB = dtsg * minv * (ld(g.rdn, f) * (S(A1, f) - S(A1, f - 1)) - (ld(g.c1f, f) * muave));
+        wn = wn + (tA + tB);
+      } else {
+        const int km1 = nz - 1;
+        const double mhm = safe12(ld(g.c1h, km1) * mut + ld(g.c2h, km1));
+        const double rdnw_t = ld(g.rdnw, km1);
+        const double t2a_t = A.t2ave[M(km1)];
+        const double tA_top = -0.5 * dts * G / mhm * (rdnw_t * rdnw_t) * 2.0 * ld(A.c2a, M(km1)) *
+                              (eps_p * (S(A2, nz) - S(A2, nz - 1)) + eps_m * (S(A4, nz) - S(A4, nz - 1)));
+        const double tB_top = -dts * G * (2.0 * rdnw_t * ld(A.c2a, M(km1)) * ld(A.alt, M(km1)) * t2a_t + (ld(g.c1f, nz) * muave));
+        const double w_top = A.w[M(nz)] + dts * ld(A.rw_tend, M(nz)) + minv * (tA_top + tB_top);
+        wn = c.top_lid ? 0.0 : w_top;
+      }
+      S(A5, f) = wn;
+      S(A0, f) = ld(A.a, M(f));
+      S(A6, f) = ld(A.gamma, M(f));
+    }
+  }
+  __syncthreads();
+  if (valid) {
+    for (int f = ty; f <= nz; f += COL_TY) S(A3, f) = ld(A.alpha, M(f));
+  }
+  __syncthreads();
+  // ---------------- P8: Thomas forward + back substitution (serial) ----------------
+  if (ty == 0 && valid) {
+    double wf_prev = S(A5, 0);
+    for (int f = 1; f <= nz; ++f) {
+      const double wf = (S(A5, f) - S(A0, f) * wf_prev) * S(A3, f);
+      S(A5, f) = wf;
+      wf_prev = wf;
+    }
+    double ws_next = S(A5, nz);
+    for (int f = nz - 1; f >= 1; --f) {
+      const double ws = S(A5, f) - S(A6, f) * ws_next;
+      S(A5, f) = ws;
+      ws_next = ws;
+    }
+  }
+  __syncthreads();
+  // ---------------- P9: Rayleigh damping, w out, phi finish -> A4 ----------------
+  if (valid) {
+    const bool do_damp = (c.damp_opt == 3 && c.dampcoef > 0.0);
+    double dampmag = 0.0, hbot = 0.0;
+    if (do_damp) {
+      dampmag = dts * c.dampcoef;
+      hbot = ld(A.pt1, M(nz)) / G - c.zdamp;
+    }
+    for (int f = ty; f <= nz; f += COL_TY) {
+      double ws = S(A5, f);
+      if (f >= 1) {
+        if (do_damp) {
+          const double hk = ld(A.pt1, M(f)) / G;
+          const double sv = sin(0.5 * 3.141592653589793 * (hk - hbot) / c.zdamp);
+          const double ramp = sv * sv;
+          const double dampwt = (hk >= hbot) ? dampmag * ramp : 0.0;
+          const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
+          ws = (ws - dampwt * mf * ld(A.w_save, M(f))) / (1.0 + dampwt);
+        }
+        const double mfs = ld(g.c1f, f) * muts + ld(g.c2f, f);
+        const double phn = S(A2, f) + msfty * 0.5 * dts * G * eps_p * ws / mfs;
+        S(A4, f) = phn;
+        A.ph[M(f)] = phn;
+      }
+      A.w[M(f)] = ws;
+    }
+  }
+  __syncthreads();
+  // ---------------- P10: calc_p_rho with smdiv memory ----------------
+  if (valid) {
+    const double mu_work = muts - mut;
+    for (int k = ty; k < nz; k += COL_TY) {
+      const double mass = ld(g.c1h, k) * muts + ld(g.c2h, k);
+      const double safe = safe12(mass);
+      const double mu_term = ld(g.c1h, k) * mu_work;
+      const double altc = ld(A.alt, M(k));
+      const double al = -(altc * mu_term + ld(g.rdnw, k) * (S(A4, k + 1) - S(A4, k))) / safe;
+      const double t1 = T1(k, j, i);
+      const double ttr = T0 + t1;
+      const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
+      const double pp = ld(A.c2a, M(k)) * (altc * (A.theta_w[M(k)] - mu_term * t1) / (safe * sttr) - al);
+      const double pm1 = A.pm1[M(k)];
+      A.p[M(k)] = pp + SMDIV * (pp - pm1);
+      A.pm1[M(k)] = pp;
+      A.al[M(k)] = al;
+    }
+  }
+}
+
+}  // namespace wg

@@ -16,6 +16,9 @@
 #include "stage_kernels.cuh"
 #include "acoustic_kernels.cuh"
 #include "finish_kernels.cuh"
+#include "column_tiled.cuh"
+#include "tiled_stencils.cuh"
+#include "tiled_faces.cuh"
 
 using namespace wg;
 
@@ -198,6 +201,8 @@ __global__ void k_bdy_target_v(Grid g, BdyLeaf b, const double *v_save, const do
 }
 
 inline dim3 blk2() { return dim3(32, 4, 1); }
+inline dim3 tblk() { return dim3(TSX, TSY, 1); }
+inline dim3 tgrd(int nxx, int nyy, int nzz) { return dim3((nxx + TSX - 1) / TSX, (nyy + TSY - 1) / TSY, nzz); }
 inline dim3 grd(int nxx, int nyy, int nzz) { return dim3((nxx + 31) / 32, (nyy + 3) / 4, nzz); }
 
 int check_launch(const char *what) {
@@ -496,8 +501,8 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     k_mass2d<<<grd(nx + 1, ny + 1, 1), blk2(), 0, stream>>>(g, s, origin.mu_pert, rk, m2);
     LAUNCH_CHECK("k_mass2d");
     PROF("k_transport");
-    k_transport<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, s.u, s.v, s.mu_total, w.ru, w.rv, w.rom,
-                                                       specified ? w.ww_spec : nullptr);
+    k_transport_tiled<<<dim3((nx + 31) / 32, ny, 1), dim3(32, 8, 1), transport_smem_bytes(nz), stream>>>(
+        g, s.u, s.v, s.mu_total, w.ru, w.rv, w.rom, specified ? w.ww_spec : nullptr);
     LAUNCH_CHECK("k_transport");
     Diag dg{w.alt_raw, w.alt, w.pb, w.c2a, w.qtot, w.al_ls, w.php_ls, w.php};
     PROF("k_diag");
@@ -505,13 +510,13 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     LAUNCH_CHECK("k_diag");
     UFaceOut uo{w.u_tend, w.u_w, w.cqu};
     PROF("k_uface");
-    k_uface<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
-                                                       in->base_u, p.top_lid, p.run_boundary, uo);
+    k_uface_tiled<<<tgrd(nx + 1, ny, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
+                                                               in->base_u, p.top_lid, p.run_boundary, uo);
     LAUNCH_CHECK("k_uface");
     VFaceOut vo{w.v_tend, w.v_w, w.cqv};
     PROF("k_vface");
-    k_vface<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
-                                                       in->base_v, p.top_lid, p.run_boundary, vo);
+    k_vface_tiled<<<tgrd(nx, ny + 1, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
+                                                               in->base_v, p.top_lid, p.run_boundary, vo);
     LAUNCH_CHECK("k_vface");
     const bool lim_theta = (rk == 3) && (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2);
     const bool lim_moist = moist && (rk == 3) && (p.moist_adv_opt == 1 || p.moist_adv_opt == 2);
@@ -520,8 +525,9 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     mo.theta_w = w.theta_w;
     for (int q = 0; q < 6; ++q) mo.q_tend[q] = w.qtend[q];
     PROF("k_mass");
-    k_mass<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta,
-                                                   lim_theta ? 0 : 1, (moist && !lim_moist) ? 1 : 0, mo);
+    k_scalar_adv_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0,
+                                                                in->base_theta, lim_theta ? 0 : 1,
+                                                                (moist && !lim_moist) ? 1 : 0, mo);
     LAUNCH_CHECK("k_mass");
     if (lim_theta || lim_moist) {
       LimArgs la;
@@ -530,11 +536,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
         PROF("k_lim_scale");
-        k_lim_scale<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2);
+        k_lim_scale_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
-        k_lim_tend<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2, in->base_theta,
-                                                           s.mu_total, w.t_tend);
+        k_lim_tend_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2,
+                                                                   in->base_theta, s.mu_total, w.t_tend);
         LAUNCH_CHECK("k_lim_tend");
       }
       if (lim_moist) {
@@ -542,11 +548,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.offset = 0.0;
         for (int q = 0; q < 6; ++q) {
           PROF("k_lim_scale");
-          k_lim_scale<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2);
+          k_lim_scale_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2);
           LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
-          k_lim_tend<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr,
-                                                             s.mu_total, w.qtend[q]);
+          k_lim_tend_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr,
+                                                                     s.mu_total, w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
         }
       }
@@ -554,9 +560,9 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     const double *ww_stage = specified ? w.ww_spec : w.rom;
     WFaceOut wo{w.rw_tend, w.ph_tend, w.cqw, w.w_w, w.ph_w, w.pt1, w.ww, w.phb0};
     PROF("k_wface");
-    k_wface<<<grd(nx, ny, nz + 1), blk2(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot, w.mub,
-                                                       w.mut, w.muts0, w.muu, w.muv, in->base_w, p.top_lid,
-                                                       p.moist_cqw, p.w_coriolis, wo);
+    k_wface_tiled<<<tgrd(nx, ny, nz + 1), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot,
+                                                               w.mub, w.mut, w.muts0, w.muu, w.muv, in->base_w,
+                                                               p.top_lid, p.moist_cqw, p.w_coriolis, wo);
     LAUNCH_CHECK("k_wface");
     const double x = 0.5 * dts * G * eps1;
     const double cof = x * x;
@@ -595,6 +601,10 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     A.mu_tend = in->base_mu;
     A.u_1 = s.u; A.v_1 = s.v; A.w_save = s.w; A.theta_s = s.theta; A.phb0 = w.phb0;
     ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp};
+    const size_t col_smem = column_tiled_smem_bytes(nz);
+    if (stage == 0 &&
+        cudaFuncSetAttribute(k_column_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_column_tiled (nz too large)");
     for (int it = 0; it < nsub[stage]; ++it) {
       PROF("k_advance_u");
       k_advance_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
@@ -603,7 +613,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       k_advance_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
       LAUNCH_CHECK("k_advance_v");
       PROF("k_column");
-      k_column<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, A, ca);
+      k_column_tiled<<<dim3((nx + COL_TX - 1) / COL_TX, ny, 1), dim3(COL_TX, COL_TY, 1), col_smem, stream>>>(g, A, ca);
       LAUNCH_CHECK("k_column");
     }
 
@@ -624,7 +634,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     fa.ww_out = (stage == 2) ? out->ww : nullptr;
     fa.t_save_out = (stage == 2) ? out->t_save : nullptr;
     PROF("k_finish_col");
-    k_finish_col<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, s, origin, fa, o);
+    k_finish_cells<<<grd(nx, ny, nz + 1), blk2(), 0, stream>>>(g, s, origin, fa, o);
     LAUNCH_CHECK("k_finish_col");
 
     if (stage == 2) {

@@ -58,7 +58,9 @@ __device__ __forceinline__ size_t ix3(int k, int j, int i, int ny, int nx) {
 }
 __device__ __forceinline__ size_t ix2(int j, int i, int nx) { return (size_t)j * (size_t)nx + (size_t)i; }
 
+// Periodic index wrap; the in-range test keeps the common case branch-only.
 __device__ __forceinline__ int wrp(int i, int n) {
+  if (i >= 0 && i < n) return i;
   int r = i % n;
   return r < 0 ? r + n : r;
 }

@@ -53,87 +53,96 @@ struct FinishArgs {
   double *t_2ave_out, *ww_out, *t_save_out;
 };
 
-// One thread per column: w, theta, ph, p (with refresh), mu, moisture.
-__global__ void k_finish_col(Grid g, StateR s, StateR origin, FinishArgs a, StateW o) {
+// One thread per (k, j, i) with k in 0..nz: face work (w, ph, ww) for every
+// k, mass work (theta, p refresh, moisture, t_2ave, t_save) for k < nz and
+// the 2-D mass fields at k == 0.  The refresh recomputes the finished ph' at
+// k and k+1 from its inputs, with the same arithmetic as the face work.
+__global__ void k_finish_cells(Grid g, StateR s, StateR origin, FinishArgs a, StateW o) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   if (i >= nx || j >= ny) return;
   const size_t c2d = ix2(j, i, nx);
-  auto M = [&](int k) { return ix3(k, j, i, ny, nx); };
+  auto M = [&](int kk) { return ix3(kk, j, i, ny, nx); };
   const double muts = ld(a.muts_ac, c2d);
   const double mut = ld(a.mut, c2d);
-  const double msfty = ld(g.msfty, c2d);
   const double mu_ac = ld(a.mu_ac, c2d);
   const double mu_base = ld(s.mu_total, c2d) - ld(s.mu_pert, c2d);
   const double mu_total_out = mu_base + mu_ac;
-  o.mu_total[c2d] = mu_total_out;
-  o.mu_pert[c2d] = mu_ac;
-  // w and ph on faces
-  for (int f = 0; f <= nz; ++f) {
+  auto ph_out = [&](int f, double &php, double &pht) {
+    php = ld(a.ph_w, M(f)) + ld(s.ph_pert, M(f));
+    const double phb = ld(s.ph_total, M(f)) - ld(s.ph_pert, M(f));
+    pht = phb + php;
+  };
+  {
+    const int f = k;
+    const double msfty = ld(g.msfty, c2d);
     const double ms = ld(g.c1f, f) * muts + ld(g.c2f, f);
     const double mc = ld(g.c1f, f) * mut + ld(g.c2f, f);
     o.w[M(f)] = (msfty * ld(a.w_w, M(f)) + ld(s.w, M(f)) * mc) / safe_den(ms);
-    const double php = ld(a.ph_w, M(f)) + ld(s.ph_pert, M(f));
-    const double phb = ld(s.ph_total, M(f)) - ld(s.ph_pert, M(f));
+    double php, pht;
+    ph_out(f, php, pht);
     o.ph_pert[M(f)] = php;
-    o.ph_total[M(f)] = phb + php;
+    o.ph_total[M(f)] = pht;
     if (a.ww_out != nullptr) a.ww_out[M(f)] = ld(a.ww_ac, M(f)) + ld(a.ww_stage, M(f));
   }
-  // theta, p refresh, moisture on mass levels
-  const double mub = mu_base;
-  const double mass_old_c1 = ld(origin.mu_total, c2d);
-  for (int k = 0; k < nz; ++k) {
-    const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-    const double ms = c1 * muts + c2;
-    const double mc = c1 * mut + c2;
-    const double t_save = ld(s.theta, M(k)) - T0;
-    const double theta_out = (ld(a.theta_w, M(k)) + t_save * mc) / safe_den(ms) + T0;
-    o.theta[M(k)] = theta_out;
-    const double p_base = ld(s.p_total, M(k)) - ld(s.p_pert, M(k));
-    const double pac = ld(a.p_ac, M(k));
-    const double p_total1 = p_base + pac;
-    // refresh grid%p from the finished ph' and theta
-    const double php0 = o.ph_pert[M(k)], php1 = o.ph_pert[M(k + 1)];
-    const double phb0 = o.ph_total[M(k)] - php0, phb1 = o.ph_total[M(k + 1)] - php1;
-    double al, alb_used;
-    if (a.hyps == 2) {
-      const double muts_r = mub + mu_ac;
-      const double c3f0 = ld(g.c3f, k), c3f1 = ld(g.c3f, k + 1), c4f0 = ld(g.c4f, k), c4f1 = ld(g.c4f, k + 1);
-      const double c3h = ld(g.c3h, k), c4h = ld(g.c4h, k);
-      double pfu = c3f1 * mub + c4f1 + g.p_top, pfd = c3f0 * mub + c4f0 + g.p_top, phm = c3h * mub + c4h + g.p_top;
-      alb_used = (phb1 - phb0) / phm / log(pfd / pfu);
-      const double dph_tot = (phb1 + php1) - (phb0 + php0);
-      pfu = c3f1 * muts_r + c4f1 + g.p_top;
-      pfd = c3f0 * muts_r + c4f0 + g.p_top;
-      phm = c3h * muts_r + c4h + g.p_top;
-      al = dph_tot / phm / log(pfd / pfu) - alb_used;
-    } else {
-      const double mhb = c1 * mub + c2;
-      const double den = ld(g.dnw, k) * mhb;
-      const double alb = -(phb1 - phb0) / (fabs(den) > 1.0e-12 ? den : 1.0e-12);
-      const double muts_r = mub + mu_ac;
-      const double mw = c1 * muts_r + c2;
-      al = -(alb * c1 * mu_ac + ld(g.rdnw, k) * (php1 - php0)) / safe12(mw);
-      alb_used = alb;
-    }
-    const double alt = al + alb_used;
-    const double p_pert2 = pressure_from_theta_alt(theta_out, alt) - p_base;
-    o.p_total[M(k)] = (p_total1 - pac) + p_pert2;
-    o.p_pert[M(k)] = p_pert2;
-    if (a.moist) {
-      const double mass_old = c1 * mass_old_c1 + c2;
-      const double mass_new = c1 * mu_total_out + c2;
-      const double inv = 1.0 / mass_new;
-      for (int sp = 0; sp < 6; ++sp) {
-        o.q[sp][M(k)] = (mass_old * ld(origin.q[sp], M(k)) + a.dt_rk * ld(a.q_tend[sp], M(k))) * inv;
-      }
-    } else if (o.q[0] != nullptr && s.q[0] != nullptr) {
-      for (int sp = 0; sp < 6; ++sp) o.q[sp][M(k)] = ld(s.q[sp], M(k));
-    }
-    if (a.t_2ave_out != nullptr) a.t_2ave_out[M(k)] = ld(a.t2ave, M(k)) + T0;
-    if (a.t_save_out != nullptr) a.t_save_out[M(k)] = t_save + T0;
+  if (k == 0) {
+    o.mu_total[c2d] = mu_total_out;
+    o.mu_pert[c2d] = mu_ac;
   }
+  if (k >= nz) return;
+  const double mub = mu_base;
+  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+  const double ms = c1 * muts + c2;
+  const double mc = c1 * mut + c2;
+  const double t_save = ld(s.theta, M(k)) - T0;
+  const double theta_out = (ld(a.theta_w, M(k)) + t_save * mc) / safe_den(ms) + T0;
+  o.theta[M(k)] = theta_out;
+  const double p_base = ld(s.p_total, M(k)) - ld(s.p_pert, M(k));
+  const double pac = ld(a.p_ac, M(k));
+  const double p_total1 = p_base + pac;
+  double php0, pht0, php1, pht1;
+  ph_out(k, php0, pht0);
+  ph_out(k + 1, php1, pht1);
+  const double phb0 = pht0 - php0, phb1 = pht1 - php1;
+  double al, alb_used;
+  if (a.hyps == 2) {
+    const double muts_r = mub + mu_ac;
+    const double c3f0 = ld(g.c3f, k), c3f1 = ld(g.c3f, k + 1), c4f0 = ld(g.c4f, k), c4f1 = ld(g.c4f, k + 1);
+    const double c3h = ld(g.c3h, k), c4h = ld(g.c4h, k);
+    double pfu = c3f1 * mub + c4f1 + g.p_top, pfd = c3f0 * mub + c4f0 + g.p_top, phm = c3h * mub + c4h + g.p_top;
+    alb_used = (phb1 - phb0) / phm / log(pfd / pfu);
+    const double dph_tot = (phb1 + php1) - (phb0 + php0);
+    pfu = c3f1 * muts_r + c4f1 + g.p_top;
+    pfd = c3f0 * muts_r + c4f0 + g.p_top;
+    phm = c3h * muts_r + c4h + g.p_top;
+    al = dph_tot / phm / log(pfd / pfu) - alb_used;
+  } else {
+    const double mhb = c1 * mub + c2;
+    const double den = ld(g.dnw, k) * mhb;
+    const double alb = -(phb1 - phb0) / (fabs(den) > 1.0e-12 ? den : 1.0e-12);
+    const double muts_r = mub + mu_ac;
+    const double mw = c1 * muts_r + c2;
+    al = -(alb * c1 * mu_ac + ld(g.rdnw, k) * (php1 - php0)) / safe12(mw);
+    alb_used = alb;
+  }
+  const double alt = al + alb_used;
+  const double p_pert2 = pressure_from_theta_alt(theta_out, alt) - p_base;
+  o.p_total[M(k)] = (p_total1 - pac) + p_pert2;
+  o.p_pert[M(k)] = p_pert2;
+  if (a.moist) {
+    const double mass_old = c1 * ld(origin.mu_total, c2d) + c2;
+    const double mass_new = c1 * mu_total_out + c2;
+    const double inv = 1.0 / mass_new;
+    for (int sp = 0; sp < 6; ++sp) {
+      o.q[sp][M(k)] = (mass_old * ld(origin.q[sp], M(k)) + a.dt_rk * ld(a.q_tend[sp], M(k))) * inv;
+    }
+  } else if (o.q[0] != nullptr && s.q[0] != nullptr) {
+    for (int sp = 0; sp < 6; ++sp) o.q[sp][M(k)] = ld(s.q[sp], M(k));
+  }
+  if (a.t_2ave_out != nullptr) a.t_2ave_out[M(k)] = ld(a.t2ave, M(k)) + T0;
+  if (a.t_save_out != nullptr) a.t_save_out[M(k)] = t_save + T0;
 }
 
 }  // namespace wg

@@ -1,0 +1,598 @@
+// Tiled u/v/w-face stage kernels and the level-parallel transport kernel.
+//
+// The flux-form momentum advection (flux_advection.py:1131-1329) reads its
+// horizontal stencils from shared-memory plane tiles (periodic wrap applied
+// once per staged element); the large-step PGF, Coriolis, pg_buoy_w and
+// rhs_ph terms keep the global-load form of stage_kernels.cuh.  The wrap face
+// (i = nx for u, j = ny for v) takes the global-load advection path, which is
+// the reference's periodic copy of face 0.  Arithmetic order is unchanged.
+#pragma once
+#include "dycore_common.cuh"
+#include "stage_kernels.cuh"
+#include "tiled_stencils.cuh"
+
+namespace wg {
+
+// Advection of u at collapsed face ii (global loads), as in k_uface.
+__device__ __forceinline__ double u_adv_global(const Grid &g, const StateR &s, const double *ru, const double *rv,
+                                               const double *rom, int k, int j, int ii) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1;
+  auto uf = [&](int kk, int jj, int mm) { return ld(s.u, ix3(kk, wrp(jj, ny), wrp(mm, nx), ny, nxu)); };
+  auto fqx = [&](int m) {
+    int rm = wrp(m, nx);
+    double vel = 0.5 * (ld(ru, ix3(k, j, rm, ny, nx)) + ld(ru, ix3(k, j, wrp(rm - 1, nx), ny, nx)));
+    return vel * flux5(uf(k, j, rm - 3), uf(k, j, rm - 2), uf(k, j, rm - 1), uf(k, j, rm), uf(k, j, rm + 1),
+                       uf(k, j, rm + 2), vel);
+  };
+  const double msfux_c = ld(g.msfux, ix2(j, ii, nxu));
+  double tend = -msfux_c * g.rdx * (fqx(ii + 1) - fqx(ii));
+  if (ny > 1) {
+    auto fqy = [&](int n) {
+      int rn = wrp(n, ny);
+      double vel = 0.5 * (ld(rv, ix3(k, rn, ii, ny, nx)) + ld(rv, ix3(k, rn, wrp(ii - 1, nx), ny, nx)));
+      return vel * flux5(uf(k, rn - 3, ii), uf(k, rn - 2, ii), uf(k, rn - 1, ii), uf(k, rn, ii), uf(k, rn + 1, ii),
+                         uf(k, rn + 2, ii), vel);
+    };
+    tend = tend - msfux_c * g.rdy * (fqy(j + 1) - fqy(j));
+  }
+  auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, ii, ny, nx)) + ld(rom, ix3(m, j, wrp(ii - 1, nx), ny, nx))); };
+  auto q = [&](int kk) { return ld(s.u, ix3(kk, j, ii, ny, nxu)); };
+  const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
+  const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+  return tend + (-ld(g.rdnw, k)) * (v1 - v0);
+}
+
+// Advection of v at collapsed face jj (global loads), as in k_vface.
+__device__ __forceinline__ double v_adv_global(const Grid &g, const StateR &s, const double *ru, const double *rv,
+                                               const double *rom, int k, int jj, int i) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nyv = ny + 1;
+  auto vf = [&](int kk, int jv, int ic) { return ld(s.v, ix3(kk, wrp(jv, ny), wrp(ic, nx), nyv, nx)); };
+  const double msfvy_c = ld(g.msfvy, ix2(jj, i, nx));
+  const double msfvx_c = ld(g.msfvx, ix2(jj, i, nx));
+  auto fqx = [&](int m) {
+    int rm = wrp(m, nx);
+    double vel = 0.5 * (ld(ru, ix3(k, jj, rm, ny, nx)) + ld(ru, ix3(k, wrp(jj - 1, ny), rm, ny, nx)));
+    return vel * flux5(vf(k, jj, rm - 3), vf(k, jj, rm - 2), vf(k, jj, rm - 1), vf(k, jj, rm), vf(k, jj, rm + 1),
+                       vf(k, jj, rm + 2), vel);
+  };
+  double tend = -msfvy_c * g.rdx * (fqx(i + 1) - fqx(i));
+  auto fqy = [&](int n) {
+    int rn = wrp(n, ny);
+    double vel = 0.5 * (ld(rv, ix3(k, rn, i, ny, nx)) + ld(rv, ix3(k, wrp(rn - 1, ny), i, ny, nx)));
+    return vel * flux5(vf(k, rn - 3, i), vf(k, rn - 2, i), vf(k, rn - 1, i), vf(k, rn, i), vf(k, rn + 1, i),
+                       vf(k, rn + 2, i), vel);
+  };
+  tend = tend - msfvy_c * g.rdy * (fqy(jj + 1) - fqy(jj));
+  auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, jj, i, ny, nx)) + ld(rom, ix3(m, wrp(jj - 1, ny), i, ny, nx))); };
+  auto q = [&](int kk) { return ld(s.v, ix3(kk, jj, i, nyv, nx)); };
+  const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
+  const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+  return tend + (msfvy_c / msfvx_c) * ((-ld(g.rdnw, k)) * (v1 - v0));
+}
+
+// ---------------------------------------------------------------------------
+// u faces, tiled advection.  Grid over faces 0..nx.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TSX *TSY) k_uface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+                                                           const double *rv, const double *rom, Diag d,
+                                                           const double *muu, const double *muus,
+                                                           const double *base_u, int top_lid, int run_boundary,
+                                                           UFaceOut o) {
+  using TQ = Tile<3, 3>;
+  using TR = Tile<1, 0>;
+  using TV = Tile<1, 1>;
+  __shared__ double su[TQ::N];
+  __shared__ double sru[TR::N];
+  __shared__ double srv[TV::N];
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  load_tile<3, 3>(su, s.u + (size_t)k * ny * nxu, nxu, i0, j0, nx, ny, 0.0);
+  load_tile<1, 0>(sru, ru + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
+  load_tile<1, 1>(srv, rv + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
+  __syncthreads();
+  if (i > nx || j >= ny) return;
+  const size_t cu = ix3(k, j, i, ny, nxu);
+  double tend;
+  if (i < nx) {
+    auto Q = [&](int r, int cc) { return su[(r + 3) * TQ::W + (cc + 3)]; };
+    auto RU = [&](int cc) { return sru[ty * TR::W + (cc + 1)]; };
+    auto RV = [&](int r, int cc) { return srv[(r + 1) * TV::W + (cc + 1)]; };
+    auto fqx = [&](int m) {
+      const double vel = 0.5 * (RU(m) + RU(m - 1));
+      return vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
+    };
+    const double msfux_c = ld(g.msfux, ix2(j, i, nxu));
+    tend = -msfux_c * g.rdx * (fqx(tx + 1) - fqx(tx));
+    if (ny > 1) {
+      auto fqy = [&](int r) {
+        const double vel = 0.5 * (RV(r, tx) + RV(r, tx - 1));
+        return vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
+      };
+      tend = tend - msfux_c * g.rdy * (fqy(ty + 1) - fqy(ty));
+    }
+    const int im = wrp(i - 1, nx);
+    auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, i, ny, nx)) + ld(rom, ix3(m, j, im, ny, nx))); };
+    auto q = [&](int kk) { return ld(s.u, ix3(kk, j, i, ny, nxu)); };
+    const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
+    const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+    tend = tend + (-ld(g.rdnw, k)) * (v1 - v0);
+  } else {
+    tend = u_adv_global(g, s, ru, rv, rom, k, j, 0);
+  }
+  const int l = (i == 0) ? 0 : i - 1;
+  const int r = (i == nx) ? nx - 1 : i;
+  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+  double u_t;
+  if (base_u != nullptr) {
+    const double mu_l = ld(s.mu_total, ix2(j, l, nx)), mu_r = ld(s.mu_total, ix2(j, r, nx));
+    const double muu_a = (i == 0) ? mu_l : (i == nx ? mu_r : 0.5 * (mu_l + mu_r));
+    u_t = ld(base_u, cu) * (c1 * muu_a + c2) + tend;
+  } else {
+    u_t = tend;
+  }
+  {
+    auto P = [&](const double *a, int kk, int ic) { return ld(a, ix3(kk, j, ic, ny, nx)); };
+    const double ph_term = (P(s.ph_pert, k + 1, r) - P(s.ph_pert, k + 1, l)) + (P(s.ph_pert, k, r) - P(s.ph_pert, k, l));
+    const double p_term = (P(d.alt_raw, k, l) + P(d.alt_raw, k, r)) * (P(s.p_pert, k, r) - P(s.p_pert, k, l));
+    const double pb_term = (P(d.al_ls, k, l) + P(d.al_ls, k, r)) * (P(d.pb, k, r) - P(d.pb, k, l));
+    const double mp_l = ld(s.mu_pert, ix2(j, l, nx)), mp_r = ld(s.mu_pert, ix2(j, r, nx));
+    const double mt_l = (ld(s.mu_total, ix2(j, l, nx)) - mp_l) + mp_l;
+    const double mt_r = (ld(s.mu_total, ix2(j, r, nx)) - mp_r) + mp_r;
+    const double mass_u = c1 * (0.5 * (mt_l + mt_r)) + c2;
+    const double msf_u = ld(g.msfux, ix2(j, i, nxu)) / ld(g.msfuy, ix2(j, i, nxu));
+    double dpx = msf_u * 0.5 * g.rdx * mass_u * (ph_term + p_term + pb_term);
+    auto ps = [&](int m) { return P(s.p_pert, m, l) + P(s.p_pert, m, r); };
+    const double bracket = ld(g.rdnw, k) * (dpn_large(g, k + 1, top_lid, ps) - dpn_large(g, k, top_lid, ps)) -
+                           0.5 * (c1 * (mp_l + mp_r));
+    dpx = dpx + msf_u * g.rdx * (P(d.php_ls, k, r) - P(d.php_ls, k, l)) * bracket;
+    const double cqu = 1.0 / (1.0 + 0.5 * (P(d.qtot, k, l) + P(d.qtot, k, r)));
+    u_t = u_t + (-cqu) * dpx;
+    o.cqu[cu] = cqu;
+  }
+  {
+    auto mu2 = [&](int jj, int ic) { return ld(s.mu_total, ix2(jj, ic, nx)); };
+    auto rvq = [&](int jv, int ic) {
+      const int js = (jv == 0) ? 0 : jv - 1, jn = (jv == ny) ? ny - 1 : jv;
+      const double muv_c = 0.5 * (mu2(js, ic) + mu2(jn, ic));
+      return ld(s.v, ix3(k, jv, ic, ny + 1, nx)) * (c1 * muv_c + c2) / ld(g.msfvx, ix2(jv, ic, nx));
+    };
+    auto rwq = [&](int kf, int ic) {
+      return ld(s.w, ix3(kf, j, ic, ny, nx)) * (ld(g.c1f, kf) * mu2(j, ic) + ld(g.c2f, kf)) /
+             ld(g.msfty, ix2(j, ic, nx));
+    };
+    const double f_u = 0.5 * (ld(g.f, ix2(j, l, nx)) + ld(g.f, ix2(j, r, nx)));
+    const double e_u = 0.5 * (ld(g.e, ix2(j, l, nx)) + ld(g.e, ix2(j, r, nx)));
+    const double cosa_u = 0.5 * (ld(g.cosa, ix2(j, l, nx)) + ld(g.cosa, ix2(j, r, nx)));
+    const double msf_u = ld(g.msfux, ix2(j, i, nxu)) / ld(g.msfuy, ix2(j, i, nxu));
+    double ru_cor = 0.0;
+    if (f_u != 0.0 || e_u != 0.0) {
+      const double rv_quad = 0.25 * (rvq(j, l) + rvq(j, r) + rvq(j + 1, l) + rvq(j + 1, r));
+      ru_cor = msf_u * f_u * rv_quad;
+      const double rw_quad = 0.25 * (rwq(k, l) + rwq(k + 1, l) + rwq(k, r) + rwq(k + 1, r));
+      ru_cor = ru_cor - e_u * cosa_u * rw_quad;
+    } else {
+      // f = e = 0 (e.g. idealized frames): the products are exact zeros; keep
+      // the reference's (+/-)0 arithmetic by multiplying the zero factors.
+      ru_cor = msf_u * f_u * 0.0;
+      ru_cor = ru_cor - e_u * cosa_u * 0.0;
+    }
+    if (run_boundary && (i == 0 || i == nx)) ru_cor = ru_cor * 0.0;
+    u_t = u_t + ru_cor;
+  }
+  o.u_tend[cu] = u_t;
+  const size_t f2 = ix2(j, i, nxu);
+  const double mass_ref = c1 * ld(muus, f2) + c2;
+  const double mass_cur = c1 * ld(muu, f2) + c2;
+  o.u_w[cu] = (mass_ref * ld(ref.u, cu) - mass_cur * ld(s.u, cu)) / ld(g.msfuy, f2);
+}
+
+// ---------------------------------------------------------------------------
+// v faces, tiled advection.  Grid over faces 0..ny.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TSX *TSY) k_vface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+                                                           const double *rv, const double *rom, Diag d,
+                                                           const double *muv, const double *muvs,
+                                                           const double *base_v, int top_lid, int run_boundary,
+                                                           VFaceOut o) {
+  using TQ = Tile<3, 3>;
+  using TR = Tile<1, 1>;
+  using TV = Tile<0, 1>;
+  __shared__ double sv[TQ::N];
+  __shared__ double sru[TR::N];
+  __shared__ double srv[TV::N];
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nyv = ny + 1;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  load_tile<3, 3>(sv, s.v + (size_t)k * nyv * nx, nx, i0, j0, nx, ny, 0.0);
+  load_tile<1, 1>(sru, ru + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
+  load_tile<0, 1>(srv, rv + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
+  __syncthreads();
+  if (i >= nx || j > ny) return;
+  const size_t cv = ix3(k, j, i, nyv, nx);
+  double tend;
+  if (j < ny) {
+    auto Q = [&](int r, int cc) { return sv[(r + 3) * TQ::W + (cc + 3)]; };
+    auto RU = [&](int r, int cc) { return sru[(r + 1) * TR::W + (cc + 1)]; };
+    auto RV = [&](int r) { return srv[(r + 1) * TV::W + tx]; };
+    const double msfvy_c = ld(g.msfvy, ix2(j, i, nx));
+    const double msfvx_c = ld(g.msfvx, ix2(j, i, nx));
+    auto fqx = [&](int m) {
+      const double vel = 0.5 * (RU(ty, m) + RU(ty - 1, m));
+      return vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
+    };
+    tend = -msfvy_c * g.rdx * (fqx(tx + 1) - fqx(tx));
+    auto fqy = [&](int r) {
+      const double vel = 0.5 * (RV(r) + RV(r - 1));
+      return vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
+    };
+    tend = tend - msfvy_c * g.rdy * (fqy(ty + 1) - fqy(ty));
+    const int jm = wrp(j - 1, ny);
+    auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, i, ny, nx)) + ld(rom, ix3(m, jm, i, ny, nx))); };
+    auto q = [&](int kk) { return ld(s.v, ix3(kk, j, i, nyv, nx)); };
+    const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
+    const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+    tend = tend + (msfvy_c / msfvx_c) * ((-ld(g.rdnw, k)) * (v1 - v0));
+  } else {
+    tend = v_adv_global(g, s, ru, rv, rom, k, 0, i);
+  }
+  const int sj = (j == 0) ? 0 : j - 1;
+  const int nj = (j == ny) ? ny - 1 : j;
+  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+  double v_t;
+  if (base_v != nullptr) {
+    const double mu_s = ld(s.mu_total, ix2(sj, i, nx)), mu_n = ld(s.mu_total, ix2(nj, i, nx));
+    const double muv_a = (j == 0) ? mu_s : (j == ny ? mu_n : 0.5 * (mu_s + mu_n));
+    v_t = ld(base_v, cv) * (c1 * muv_a + c2) + tend;
+  } else {
+    v_t = tend;
+  }
+  {
+    auto P = [&](const double *a, int kk, int jc) { return ld(a, ix3(kk, jc, i, ny, nx)); };
+    const double ph_term = (P(s.ph_pert, k + 1, nj) - P(s.ph_pert, k + 1, sj)) + (P(s.ph_pert, k, nj) - P(s.ph_pert, k, sj));
+    const double p_term = (P(d.alt_raw, k, sj) + P(d.alt_raw, k, nj)) * (P(s.p_pert, k, nj) - P(s.p_pert, k, sj));
+    const double pb_term = (P(d.al_ls, k, sj) + P(d.al_ls, k, nj)) * (P(d.pb, k, nj) - P(d.pb, k, sj));
+    const double mp_s = ld(s.mu_pert, ix2(sj, i, nx)), mp_n = ld(s.mu_pert, ix2(nj, i, nx));
+    const double mt_s = (ld(s.mu_total, ix2(sj, i, nx)) - mp_s) + mp_s;
+    const double mt_n = (ld(s.mu_total, ix2(nj, i, nx)) - mp_n) + mp_n;
+    const double mass_v = c1 * (0.5 * (mt_s + mt_n)) + c2;
+    const double msf_v = ld(g.msfvy, ix2(j, i, nx)) / ld(g.msfvx, ix2(j, i, nx));
+    double dpy = msf_v * 0.5 * g.rdy * mass_v * (ph_term + p_term + pb_term);
+    auto ps = [&](int m) { return P(s.p_pert, m, sj) + P(s.p_pert, m, nj); };
+    const double bracket = ld(g.rdnw, k) * (dpn_large(g, k + 1, top_lid, ps) - dpn_large(g, k, top_lid, ps)) -
+                           0.5 * (c1 * (mp_s + mp_n));
+    dpy = dpy + msf_v * g.rdy * (P(d.php_ls, k, nj) - P(d.php_ls, k, sj)) * bracket;
+    const double cqv = 1.0 / (1.0 + 0.5 * (P(d.qtot, k, sj) + P(d.qtot, k, nj)));
+    v_t = v_t + (-cqv) * dpy;
+    o.cqv[cv] = cqv;
+  }
+  {
+    auto mu2 = [&](int jc, int ic) { return ld(s.mu_total, ix2(jc, ic, nx)); };
+    auto ruq = [&](int jc, int iu) {
+      const int il = (iu == 0) ? 0 : iu - 1, ir = (iu == nx) ? nx - 1 : iu;
+      const double muu_c = 0.5 * (mu2(jc, il) + mu2(jc, ir));
+      return ld(s.u, ix3(k, jc, iu, ny, nx + 1)) * (c1 * muu_c + c2) / ld(g.msfuy, ix2(jc, iu, nx + 1));
+    };
+    auto rwq = [&](int kf, int jc) {
+      return ld(s.w, ix3(kf, jc, i, ny, nx)) * (ld(g.c1f, kf) * mu2(jc, i) + ld(g.c2f, kf)) /
+             ld(g.msfty, ix2(jc, i, nx));
+    };
+    const double f_v = 0.5 * (ld(g.f, ix2(sj, i, nx)) + ld(g.f, ix2(nj, i, nx)));
+    const double e_v = 0.5 * (ld(g.e, ix2(sj, i, nx)) + ld(g.e, ix2(nj, i, nx)));
+    const double sina_v = 0.5 * (ld(g.sina, ix2(sj, i, nx)) + ld(g.sina, ix2(nj, i, nx)));
+    const double msf_v = ld(g.msfvy, ix2(j, i, nx)) / ld(g.msfvx, ix2(j, i, nx));
+    double rv_cor;
+    if (f_v != 0.0 || e_v != 0.0) {
+      const double ru_quad = 0.25 * (ruq(sj, i) + ruq(sj, i + 1) + ruq(nj, i) + ruq(nj, i + 1));
+      rv_cor = -msf_v * f_v * ru_quad;
+      const double rw_quad = 0.25 * (rwq(k, sj) + rwq(k + 1, sj) + rwq(k, nj) + rwq(k + 1, nj));
+      rv_cor = rv_cor + msf_v * e_v * sina_v * rw_quad;
+    } else {
+      rv_cor = -msf_v * f_v * 0.0;
+      rv_cor = rv_cor + msf_v * e_v * sina_v * 0.0;
+    }
+    if (run_boundary && (j == 0 || j == ny)) rv_cor = rv_cor * 0.0;
+    v_t = v_t + rv_cor;
+  }
+  o.v_tend[cv] = v_t;
+  const size_t f2 = ix2(j, i, nx);
+  const double mass_ref = c1 * ld(muvs, f2) + c2;
+  const double mass_cur = c1 * ld(muv, f2) + c2;
+  o.v_w[cv] = (mass_ref * ld(ref.v, cv) - mass_cur * ld(s.v, cv)) / ld(g.msfvx, f2);
+}
+
+// ---------------------------------------------------------------------------
+// w faces, tiled: w advection and rhs_ph horizontal stencils from tiles.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TSX *TSY) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+                                                           const double *rv, const double *rom,
+                                                           const double *ww_stage, const double *qtot,
+                                                           const double *mub, const double *mut, const double *muts0,
+                                                           const double *muu, const double *muv,
+                                                           const double *base_w, int top_lid, int moist_cqw,
+                                                           int w_coriolis, WFaceOut o) {
+  using TQ = Tile<3, 3>;
+  using TR = Tile<1, 0>;
+  using TV = Tile<0, 1>;
+  using TP = Tile<1, 1>;
+  __shared__ double sw[TQ::N];
+  __shared__ double sru[TR::N];
+  __shared__ double srv[TV::N];
+  __shared__ double spt[TP::N];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  const size_t pm = (size_t)ny * nx;
+  load_tile<3, 3>(sw, s.w + (size_t)k * pm, nx, i0, j0, nx, ny, 0.0);
+  // ru / rv interpolated to the full level k (flux_advection.py:1332-1352)
+  {
+    const int kh = (k == nz) ? nz - 1 : k;
+    for (int e = ty * TSX + tx; e < TR::N; e += TSX * TSY) {
+      const int r = e / TR::W, cc = e - r * TR::W;
+      const int jj = wrp(j0 + r, ny), ii = wrp(i0 - 1 + cc, nx);
+      double val;
+      if (k == 0 || k == nz) {
+        val = ld(ru, ix3(kh, jj, ii, ny, nx));
+      } else {
+        val = ld(g.fnm, k) * ld(ru, ix3(k, jj, ii, ny, nx)) + ld(g.fnp, k) * ld(ru, ix3(k - 1, jj, ii, ny, nx));
+      }
+      sru[e] = val;
+    }
+    for (int e = ty * TSX + tx; e < TV::N; e += TSX * TSY) {
+      const int r = e / TV::W, cc = e - r * TV::W;
+      const int jj = wrp(j0 - 1 + r, ny), ii = wrp(i0 + cc, nx);
+      double val;
+      if (k == 0 || k == nz) {
+        val = ld(rv, ix3(kh, jj, ii, ny, nx));
+      } else {
+        val = ld(g.fnm, k) * ld(rv, ix3(k, jj, ii, ny, nx)) + ld(g.fnp, k) * ld(rv, ix3(k - 1, jj, ii, ny, nx));
+      }
+      srv[e] = val;
+    }
+    for (int e = ty * TSX + tx; e < TP::N; e += TSX * TSY) {
+      const int r = e / TP::W, cc = e - r * TP::W;
+      const size_t q = (size_t)k * pm + (size_t)wrp(j0 - 1 + r, ny) * nx + wrp(i0 - 1 + cc, nx);
+      const double p = ld(s.ph_pert, q);
+      spt[e] = p + (ld(s.ph_total, q) - p);
+    }
+  }
+  __syncthreads();
+  if (i >= nx || j >= ny) return;
+  const size_t cw = ix3(k, j, i, ny, nx);
+  const size_t c2d = ix2(j, i, nx);
+  auto W_ = [&](int r, int cc) { return sw[(r + 3) * TQ::W + (cc + 3)]; };
+  const double msftx = ld(g.msftx, c2d);
+  auto fqx = [&](int m) {
+    const double vel = sru[ty * TR::W + (m + 1)];
+    return vel * flux5(W_(ty, m - 3), W_(ty, m - 2), W_(ty, m - 1), W_(ty, m), W_(ty, m + 1), W_(ty, m + 2), vel);
+  };
+  double adv = -msftx * g.rdx * (fqx(tx + 1) - fqx(tx));
+  if (ny > 1) {
+    auto fqy = [&](int r) {
+      const double vel = srv[(r + 1) * TV::W + tx];
+      return vel * flux5(W_(r - 3, tx), W_(r - 2, tx), W_(r - 1, tx), W_(r, tx), W_(r + 1, tx), W_(r + 2, tx), vel);
+    };
+    adv = adv - msftx * g.rdy * (fqy(ty + 1) - fqy(ty));
+  }
+  {
+    auto wc = [&](int kk) { return ld(s.w, ix3(kk, j, i, ny, nx)); };
+    auto velf = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, i, ny, nx)) + ld(rom, ix3(m - 1, j, i, ny, nx))); };
+    auto vfw = [&](int m) {
+      if (m <= 0) return 0.0;
+      if (m == 1) return velf(1) * 0.5 * (wc(1) + wc(0));
+      if (m < nz) return flux3v(wc(m - 2), wc(m - 1), wc(m), wc(m + 1), velf(m));
+      if (m == nz && !top_lid) return velf(nz) * 0.5 * (wc(nz) + wc(nz - 1));
+      return 0.0;
+    };
+    double vt = 0.0;
+    if (k >= 1 && k <= nz - 1) vt = -ld(g.rdn, k) * (vfw(k + 1) - vfw(k));
+    if (k == nz && !top_lid) vt = 0.0 + 2.0 * ld(g.rdn, nz - 1) * vfw(nz);
+    adv = adv + vt;
+  }
+  double w_t;
+  if (base_w != nullptr) {
+    const double mass_f = ld(g.c1f, k) * ld(s.mu_total, c2d) + ld(g.c2f, k);
+    w_t = ld(base_w, cw) * mass_f + adv;
+  } else {
+    w_t = adv;
+  }
+  const double mub_c = ld(mub, c2d), mut_c = ld(mut, c2d);
+  const double mu_prime = mut_c - mub_c;
+  const double minv = 1.0 / ld(g.msfty, c2d);
+  auto Pp = [&](int kk) { return ld(s.p_pert, ix3(kk, j, i, ny, nx)); };
+  auto Qt = [&](int kk) { return ld(qtot, ix3(kk, j, i, ny, nx)); };
+  double rw = 0.0, cqw = 0.0;
+  if (k >= 1 && k <= nz - 1) {
+    if (moist_cqw) {
+      const double ci = 0.5 * (Qt(k) + Qt(k - 1));
+      const double cq1 = 1.0 / (1.0 + ci);
+      const double cq2 = ci * cq1;
+      rw = minv * G * (cq1 * ld(g.rdn, k) * (Pp(k) - Pp(k - 1)) - ld(g.c1f, k) * mu_prime -
+                       cq2 * (ld(g.c1f, k) * mub_c + ld(g.c2f, k)));
+      cqw = cq1;
+    } else {
+      rw = minv * G * (ld(g.rdn, k) * (Pp(k) - Pp(k - 1)) - ld(g.c1f, k) * mu_prime);
+      cqw = 1.0;
+    }
+  } else if (k == nz) {
+    if (moist_cqw) {
+      const double ct = 0.5 * (Qt(nz - 1) + Qt(nz - 2));
+      const double c1t = 1.0 / (1.0 + ct);
+      const double c2t = ct * c1t;
+      rw = minv * G * (c1t * 2.0 * ld(g.rdnw, nz - 1) * (-Pp(nz - 1)) - ld(g.c1f, nz) * mu_prime -
+                       c2t * (ld(g.c1f, nz) * mub_c + ld(g.c2f, nz)));
+    } else {
+      rw = minv * G * (2.0 * ld(g.rdnw, nz - 1) * (-Pp(nz - 1)) - ld(g.c1f, nz) * mu_prime);
+    }
+  }
+  rw = rw + w_t;
+  if (w_coriolis && k >= 1 && k <= nz - 1) {
+    const double muu_i = ld(muu, ix2(j, i, nx + 1)), muu_ip = ld(muu, ix2(j, i + 1, nx + 1));
+    const double muv_j = ld(muv, ix2(j, i, nx)), muv_jp = ld(muv, ix2(j + 1, i, nx));
+    const double fuy_i = ld(g.msfuy, ix2(j, i, nx + 1)), fuy_ip = ld(g.msfuy, ix2(j, i + 1, nx + 1));
+    const double fvx_j = ld(g.msfvx, ix2(j, i, nx)), fvx_jp = ld(g.msfvx, ix2(j + 1, i, nx));
+    auto lev = [&](int kk, double &ru_m, double &u_m, double &rv_m, double &v_m) {
+      const double c1 = ld(g.c1h, kk), c2 = ld(g.c2h, kk);
+      const double u0 = ld(s.u, ix3(kk, j, i, ny, nx + 1)), u1 = ld(s.u, ix3(kk, j, i + 1, ny, nx + 1));
+      const double v0 = ld(s.v, ix3(kk, j, i, ny + 1, nx)), v1 = ld(s.v, ix3(kk, j + 1, i, ny + 1, nx));
+      const double rs0 = (c1 * muu_i + c2) * u0 / fuy_i, rs1 = (c1 * muu_ip + c2) * u1 / fuy_ip;
+      const double vs0 = (c1 * muv_j + c2) * v0 / fvx_j, vs1 = (c1 * muv_jp + c2) * v1 / fvx_jp;
+      ru_m = 0.5 * (rs0 + rs1);
+      u_m = 0.5 * (u0 + u1);
+      rv_m = 0.5 * (vs0 + vs1);
+      v_m = 0.5 * (v0 + v1);
+    };
+    double ru_a, u_a, rv_a, v_a, ru_b, u_b, rv_b, v_b;
+    lev(k, ru_a, u_a, rv_a, v_a);
+    lev(k - 1, ru_b, u_b, rv_b, v_b);
+    const double fm = ld(g.fnm, k), fp = ld(g.fnp, k);
+    const double ru_f = fm * ru_a + fp * ru_b, u_f = fm * u_a + fp * u_b;
+    const double rv_f = fm * rv_a + fp * rv_b, v_f = fm * v_a + fp * v_b;
+    const double mxy = ld(g.msftx, c2d) / ld(g.msfty, c2d);
+    const double cor = ld(g.e, c2d) * (ld(g.cosa, c2d) * ru_f - mxy * ld(g.sina, c2d) * rv_f);
+    const double curv = W_RERADIUS * (ru_f * u_f + mxy * rv_f * v_f);
+    rw = rw + (cor + curv);
+  }
+  o.rw_tend[cw] = rw;
+  o.cqw[cw] = cqw;
+  {
+    auto PT = [&](int r, int cc) { return spt[(r + 1) * TP::W + (cc + 1)]; };
+    auto pht = [&](int kk) {  // column value at level kk
+      const size_t q = ix3(kk, j, i, ny, nx);
+      const double p = ld(s.ph_pert, q);
+      return p + (ld(s.ph_total, q) - p);
+    };
+    double out = 0.0;
+    if (k >= 1 && k <= nz - 1) {
+      auto wdwn = [&](int m) {
+        const double wwm = 0.5 * (ld(ww_stage, ix3(m + 1, j, i, ny, nx)) + ld(ww_stage, ix3(m, j, i, ny, nx)));
+        return wwm * ld(g.rdnw, m) * (pht(m + 1) - pht(m));
+      };
+      const double term3 = ld(g.fnm, k) * wdwn(k) + ld(g.fnp, k) * wdwn(k - 1);
+      out = 0.0 + (-term3);
+      const double mass_f = ld(g.c1f, k) * mut_c + ld(g.c2f, k);
+      out = out + mass_f * G * ld(s.w, cw) * minv;
+      const double c1f = ld(g.c1f, k), c2f = ld(g.c2f, k);
+      auto vpair = [&](int jv) { return ld(s.v, ix3(k, jv, i, ny + 1, nx)) + ld(s.v, ix3(k - 1, jv, i, ny + 1, nx)); };
+      auto muvf = [&](int jv) { return c1f * ld(muv, ix2(jv, i, nx)) + c2f; };
+      const double pti = PT(ty, tx);
+      const double dn_ = PT(ty + 1, tx) - pti;
+      const double ds_ = pti - PT(ty - 1, tx);
+      const double flux_y = muvf(j + 1) * vpair(j + 1) * dn_ + muvf(j) * vpair(j) * ds_;
+      out = out + (-(0.25 * g.rdy * minv)) * flux_y;
+      auto upair = [&](int iu) { return ld(s.u, ix3(k, j, iu, ny, nx + 1)) + ld(s.u, ix3(k - 1, j, iu, ny, nx + 1)); };
+      auto muuf = [&](int iu) { return c1f * ld(muu, ix2(j, iu, nx + 1)) + c2f; };
+      const double de_ = PT(ty, tx + 1) - pti;
+      const double dw_ = pti - PT(ty, tx - 1);
+      const double flux_x = muuf(i + 1) * upair(i + 1) * de_ + muuf(i) * upair(i) * dw_;
+      out = out + (-(0.25 * g.rdx * minv)) * flux_x;
+    } else if (k == nz && !top_lid) {
+      const double mass_f = ld(g.c1f, nz) * mut_c + ld(g.c2f, nz);
+      out = mass_f * G * ld(s.w, cw) * minv;
+    }
+    o.ph_tend[cw] = out;
+  }
+  const double mass_f_ref = ld(g.c1f, k) * ld(muts0, c2d) + ld(g.c2f, k);
+  const double mass_f_cur = ld(g.c1f, k) * mut_c + ld(g.c2f, k);
+  o.w_w[cw] = (mass_f_ref * ld(ref.w, cw) - mass_f_cur * ld(s.w, cw)) / ld(g.msfty, c2d);
+  const double php = ld(s.ph_pert, cw);
+  o.ph_w[cw] = ld(ref.ph_pert, cw) - php;
+  o.pt1[cw] = ld(ref.ph_pert, cw) + (ld(s.ph_total, cw) - php);
+  o.ww[cw] = ld(ww_stage, cw);
+  if (k == 0) o.phb0[c2d] = ld(s.ph_total, cw) - php;
+}
+
+// ---------------------------------------------------------------------------
+// Transport velocities (flux_advection.py:394-470) and the specified stage
+// omega (flux_advection.py:180-232), level-parallel: a block owns 32 columns,
+// its warps split the levels, and the column sum / cumulative sum run serially
+// per column out of shared memory (same order as the reference).
+// ---------------------------------------------------------------------------
+inline size_t transport_smem_bytes(int nz) { return (size_t)2 * nz * 32 * sizeof(double); }
+
+__global__ void __launch_bounds__(256) k_transport_tiled(Grid g, const double *u, const double *v,
+                                                          const double *mu_total, double *ru, double *rv, double *rom,
+                                                          double *ww_spec) {
+  extern __shared__ double sm[];
+  const int tx = threadIdx.x, ty = threadIdx.y;  // blockDim (32, 8)
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * 32 + tx, j = blockIdx.y;
+  const bool valid = i < nx;
+  auto D0 = [&](int k) -> double & { return sm[(size_t)k * 32 + tx]; };
+  auto D1 = [&](int k) -> double & { return sm[(size_t)(nz + k) * 32 + tx]; };
+  int ip = 0, im = 0, jp = 0, jm = 0;
+  double mu_c = 0, muu_i = 0, muu_ip = 0, muv_j = 0, muv_jp = 0, msfuy_i = 1, msfuy_ip = 1, msfvx_j = 1, msfvx_jp = 1,
+         msftx = 1;
+  double muu_s_i = 0, muu_s_ip = 0, muv_s_j = 0, muv_s_jp = 0, fuy_ip = 1, fvx_jp = 1;
+  if (valid) {
+    ip = wrp(i + 1, nx); im = wrp(i - 1, nx); jp = wrp(j + 1, ny); jm = wrp(j - 1, ny);
+    mu_c = ld(mu_total, ix2(j, i, nx));
+    muu_i = 0.5 * (mu_c + ld(mu_total, ix2(j, im, nx)));
+    muu_ip = 0.5 * (ld(mu_total, ix2(j, ip, nx)) + mu_c);
+    muv_j = 0.5 * (mu_c + ld(mu_total, ix2(jm, i, nx)));
+    muv_jp = 0.5 * (ld(mu_total, ix2(jp, i, nx)) + mu_c);
+    msfuy_i = ld(g.msfuy, ix2(j, i, nx + 1)); msfuy_ip = ld(g.msfuy, ix2(j, ip, nx + 1));
+    msfvx_j = ld(g.msfvx, ix2(j, i, nx)); msfvx_jp = ld(g.msfvx, ix2(jp, i, nx));
+    msftx = ld(g.msftx, ix2(j, i, nx));
+    if (ww_spec != nullptr) {
+      const double mu_w = (i == 0) ? mu_c : ld(mu_total, ix2(j, i - 1, nx));
+      muu_s_i = 0.5 * (mu_c + mu_w);
+      muu_s_ip = (i + 1 == nx) ? mu_c : 0.5 * (ld(mu_total, ix2(j, i + 1, nx)) + mu_c);
+      const double mu_s = (j == 0) ? mu_c : ld(mu_total, ix2(j - 1, i, nx));
+      muv_s_j = 0.5 * (mu_c + mu_s);
+      muv_s_jp = (j + 1 == ny) ? mu_c : 0.5 * (ld(mu_total, ix2(j + 1, i, nx)) + mu_c);
+      fuy_ip = ld(g.msfuy, ix2(j, i + 1, nx + 1));
+      fvx_jp = ld(g.msfvx, ix2(j + 1, i, nx));
+    }
+  }
+  if (valid) {
+    for (int k = ty; k < nz; k += 8) {
+      const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+      const double u_i = ld(u, ix3(k, j, i, ny, nx + 1)), v_j = ld(v, ix3(k, j, i, ny + 1, nx));
+      const double ru_i = (c1 * muu_i + c2) * u_i / msfuy_i;
+      const double ru_ip = (c1 * muu_ip + c2) * ld(u, ix3(k, j, ip, ny, nx + 1)) / msfuy_ip;
+      const double rv_j = (c1 * muv_j + c2) * v_j / msfvx_j;
+      const double rv_jp = (c1 * muv_jp + c2) * ld(v, ix3(k, jp, i, ny + 1, nx)) / msfvx_jp;
+      D0(k) = ld(g.dnw, k) * msftx * (g.rdx * (ru_ip - ru_i) + g.rdy * (rv_jp - rv_j));
+      ru[ix3(k, j, i, ny, nx)] = ru_i;
+      rv[ix3(k, j, i, ny, nx)] = rv_j;
+      if (ww_spec != nullptr) {
+        const double a0 = (c1 * muu_s_i + c2) * u_i / msfuy_i;
+        const double a1 = (c1 * muu_s_ip + c2) * ld(u, ix3(k, j, i + 1, ny, nx + 1)) / fuy_ip;
+        const double b0 = (c1 * muv_s_j + c2) * v_j / msfvx_j;
+        const double b1 = (c1 * muv_s_jp + c2) * ld(v, ix3(k, j + 1, i, ny + 1, nx)) / fvx_jp;
+        D1(k) = msftx * ld(g.dnw, k) * (g.rdx * (a1 - a0) + g.rdy * (b1 - b0));
+      }
+    }
+  }
+  __syncthreads();
+  if (ty == 0 && valid) {
+    double dmdt = D0(0);
+    for (int k = 1; k < nz; ++k) dmdt = dmdt + D0(k);
+    double cum = 0.0;
+    rom[ix3(0, j, i, ny, nx)] = 0.0;
+    for (int k = 0; k < nz - 1; ++k) {
+      const double inc = -(ld(g.dnw, k) * ld(g.c1h, k) * dmdt) - D0(k);
+      cum = (k == 0) ? inc : cum + inc;
+      rom[ix3(k + 1, j, i, ny, nx)] = cum;
+    }
+    rom[ix3(nz, j, i, ny, nx)] = 0.0;
+  }
+  if (ty == 1 && valid && ww_spec != nullptr) {
+    double dm = D1(0);
+    for (int k = 1; k < nz; ++k) dm = dm + D1(k);
+    double cm = 0.0;
+    ww_spec[ix3(0, j, i, ny, nx)] = 0.0;
+    for (int k = 0; k < nz - 1; ++k) {
+      const double inc = -(ld(g.dnw, k) * ld(g.c1h, k) * dm) - D1(k);
+      cm = (k == 0) ? inc : cm + inc;
+      ww_spec[ix3(k + 1, j, i, ny, nx)] = cm;
+    }
+    ww_spec[ix3(nz, j, i, ny, nx)] = 0.0;
+  }
+}
+
+}  // namespace wg

@@ -1,0 +1,335 @@
+// Shared-memory tiled versions of the horizontal-stencil stage kernels.
+//
+// A block computes a 32 x 8 tile of one level.  Every field a stencil needs is
+// staged once per block as a (8 + 2*HY) x (32 + 2*HX) plane tile, with the
+// periodic wrap of the reference's jnp.roll applied once per staged element;
+// the flux stencils then read shared memory with fixed offsets.  Vertical
+// stencils read global memory at the thread's own column.  The arithmetic is
+// the same expression sequence as the untiled kernels (operation order of the
+// reference), so results are bit-identical to them.
+#pragma once
+#include "dycore_common.cuh"
+#include "stage_kernels.cuh"
+
+namespace wg {
+
+constexpr int TSX = 32;
+constexpr int TSY = 8;
+
+template <int HX, int HY>
+struct Tile {
+  static constexpr int W = TSX + 2 * HX;
+  static constexpr int H = TSY + 2 * HY;
+  static constexpr int N = W * H;
+};
+
+// Stage one plane tile: element (r, c) holds src[wrap(j0-HY+r), wrap(i0-HX+c)] - sub.
+template <int HX, int HY>
+__device__ __forceinline__ void load_tile(double *t, const double *plane, int pitch, int i0, int j0, int px, int py,
+                                          double sub) {
+  using T = Tile<HX, HY>;
+  for (int e = threadIdx.y * TSX + threadIdx.x; e < T::N; e += TSX * TSY) {
+    const int r = e / T::W, c = e - r * T::W;
+    const int jj = wrp(j0 - HY + r, py), ii = wrp(i0 - HX + c, px);
+    t[e] = __ldg(plane + (size_t)jj * pitch + ii) - sub;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain h5/v3 scalar advection (flux_advection.py:482-568) for theta and the
+// moisture species, plus theta_work (small_step_prep.py:321).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_tiled(Grid g, StateR s, StateR ref, const double *ru,
+                                                                const double *rv, const double *rom, const double *mut,
+                                                                const double *muts0, const double *base_theta,
+                                                                int theta_plain, int moist_plain, MassOut o) {
+  using TQ = Tile<3, 3>;
+  using TR = Tile<1, 0>;
+  using TV = Tile<0, 1>;
+  __shared__ double sq[TQ::N];
+  __shared__ double sru[TR::N];
+  __shared__ double srv[TV::N];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool valid = i < nx && j < ny;
+  const size_t plane = (size_t)k * ny * nx;
+  load_tile<1, 0>(sru, ru + plane, nx, i0, j0, nx, ny, 0.0);
+  load_tile<0, 1>(srv, rv + plane, nx, i0, j0, nx, ny, 0.0);
+  const size_t c = valid ? ix3(k, j, i, ny, nx) : 0;
+  const size_t c2d = valid ? ix2(j, i, nx) : 0;
+  const double msftx = valid ? ld(g.msftx, c2d) : 1.0;
+  const double rom0 = valid ? ld(rom, ix3(k, j, i, ny, nx)) : 0.0;
+  const double rom1 = valid ? ld(rom, ix3(k + 1, j, i, ny, nx)) : 0.0;
+  auto tend_of = [&](const double *fld, double sub) {
+    __syncthreads();
+    load_tile<3, 3>(sq, fld + plane, nx, i0, j0, nx, ny, sub);
+    __syncthreads();
+    if (!valid) return 0.0;
+    auto Q = [&](int r, int cc) { return sq[(r + 3) * TQ::W + (cc + 3)]; };  // local (row, col)
+    auto fqx = [&](int m) {  // face at local column m
+      const double vel = sru[ty * TR::W + (m + 1)];
+      return vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
+    };
+    auto fqy = [&](int r) {
+      const double vel = srv[(r + 1) * TV::W + tx];
+      return vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
+    };
+    double tend = -msftx * g.rdx * (fqx(tx + 1) - fqx(tx));
+    tend = tend - msftx * g.rdy * (fqy(ty + 1) - fqy(ty));
+    auto qc = [&](int kk) { return ld(fld, ix3(kk, j, i, ny, nx)) - sub; };
+    const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, rom1, qc) : 0.0;
+    const double v0 = (k >= 1) ? vflux3_at(g, k, rom0, qc) : 0.0;
+    return tend - ld(g.rdnw, k) * (v1 - v0);
+  };
+  if (theta_plain) {
+    const double adv = tend_of(s.theta, T0);
+    if (valid) {
+      if (base_theta != nullptr) {
+        const double mass_h = ld(g.c1h, k) * ld(s.mu_total, c2d) + ld(g.c2h, k);
+        o.t_tend[c] = ld(base_theta, c) * mass_h + adv;
+      } else {
+        o.t_tend[c] = adv;
+      }
+    }
+  }
+  if (moist_plain) {
+#pragma unroll
+    for (int sp = 0; sp < 6; ++sp) {
+      const double adv = tend_of(s.q[sp], 0.0);
+      if (valid) o.q_tend[sp][c] = adv;
+    }
+  }
+  if (valid) {
+    const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+    const double mass_ref = c1 * ld(muts0, c2d) + c2;
+    const double mass_cur = c1 * ld(mut, c2d) + c2;
+    o.theta_w[c] = mass_ref * (ld(ref.theta, c) - T0) - mass_cur * (ld(s.theta, c) - T0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PD / monotonic limited scalar advection (flux_advection.py:736-1000),
+// tiled.  Pass 1 writes the per-cell scale(s); pass 2 the tendency.
+// ---------------------------------------------------------------------------
+struct LimTiles {
+  double *q;    // Tile<3,3>: field - offset
+  double *qo;   // Tile<1,1>: field_old - offset
+  double *ru;   // Tile<1,0>
+  double *rv;   // Tile<0,1>
+  double *mt;   // Tile<1,1>: current total dry mass (2-D)
+};
+
+__device__ __forceinline__ void lim_stage_tiles(const Grid &g, const LimArgs &a, const double *field,
+                                                const double *field_old, int i0, int j0, int k, LimTiles &t) {
+  const int nx = g.nx, ny = g.ny;
+  const size_t plane = (size_t)k * ny * nx;
+  load_tile<3, 3>(t.q, field + plane, nx, i0, j0, nx, ny, a.offset);
+  load_tile<1, 1>(t.qo, field_old + plane, nx, i0, j0, nx, ny, a.offset);
+  load_tile<1, 0>(t.ru, a.ru + plane, nx, i0, j0, nx, ny, 0.0);
+  load_tile<0, 1>(t.rv, a.rv + plane, nx, i0, j0, nx, ny, 0.0);
+  load_tile<1, 1>(t.mt, a.mut, nx, i0, j0, nx, ny, 0.0);
+}
+
+// The 12 face fluxes of cell (k, j, i) from the staged tiles (same algebra as
+// cell_fluxes in stage_kernels.cuh).
+__device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int j,
+                                                  int i, const double *field, const double *field_old,
+                                                  CellFluxes &cf) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  using TQ = Tile<3, 3>;
+  using TO = Tile<1, 1>;
+  using TR = Tile<1, 0>;
+  using TV = Tile<0, 1>;
+  const double dx = 1.0 / g.rdx, dy = 1.0 / g.rdy;
+  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+  auto Q = [&](int r, int cc) { return t.q[(r + 3) * TQ::W + (cc + 3)]; };
+  auto QO = [&](int r, int cc) { return t.qo[(r + 1) * TO::W + (cc + 1)]; };
+  auto MT = [&](int r, int cc) { return t.mt[(r + 1) * TO::W + (cc + 1)]; };
+  auto upw = [&](double fo_m1, double fo_0, double vel, double mu_face, double dxy) {
+    double cr = vel * a.dt / dxy / mu_face;
+    double ab = fabs(cr);
+    return mu_face * (dxy / a.dt) * (0.5 * dmin(1.0, cr + ab) * fo_m1 + 0.5 * dmax(-1.0, cr - ab) * fo_0);
+  };
+  auto xf = [&](int m, double &lo, double &an) {
+    const double vel = t.ru[ty * TR::W + (m + 1)];
+    const double muu = 0.5 * (MT(ty, m) + MT(ty, m - 1));
+    const double mu_u = c1 * muu + c2;
+    lo = upw(QO(ty, m - 1), QO(ty, m), vel, mu_u, dx);
+    const double hi = vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
+    an = hi - lo;
+  };
+  auto yf = [&](int r, double &lo, double &an) {
+    const double vel = t.rv[(r + 1) * TV::W + tx];
+    const double muv = 0.5 * (MT(r, tx) + MT(r - 1, tx));
+    const double mu_v = c1 * muv + c2;
+    lo = upw(QO(r - 1, tx), QO(r, tx), vel, mu_v, dy);
+    const double hi = vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
+    an = hi - lo;
+  };
+  auto qf = [&](int kk) { return ld(field, ix3(kk, j, i, ny, nx)) - a.offset; };
+  auto qo = [&](int kk) { return ld(field_old, ix3(kk, j, i, ny, nx)) - a.offset; };
+  auto zf = [&](int m, double &lo, double &an) {
+    if (m <= 0 || m >= nz) {
+      lo = 0.0;
+      an = 0.0;
+      return;
+    }
+    const double romv = ld(a.rom, ix3(m, j, i, ny, nx));
+    const double mtc = MT(ty, tx);
+    const double muh_m = ld(g.c1h, m) * mtc + ld(g.c2h, m);
+    const double muh_mm1 = ld(g.c1h, m - 1) * mtc + ld(g.c2h, m - 1);
+    const double dz = 2.0 / (ld(g.rdnw, m) + ld(g.rdnw, m - 1));
+    const double mu_face = 0.5 * (muh_m + muh_mm1);
+    const double cr = romv * a.dt / dz / mu_face;
+    const double ab = fabs(cr);
+    lo = mu_face * (dz / a.dt) * (0.5 * dmin(1.0, cr + ab) * qo(m - 1) + 0.5 * dmax(-1.0, cr - ab) * qo(m));
+    const double hi = vflux3_at(g, m, romv, qf);
+    an = hi - lo;
+  };
+  xf(tx, cf.lx0, cf.ax0);
+  xf(tx + 1, cf.lx1, cf.ax1);
+  yf(ty, cf.ly0, cf.ay0);
+  yf(ty + 1, cf.ly1, cf.ay1);
+  zf(k, cf.lz0, cf.az0);
+  zf(k + 1, cf.lz1, cf.az1);
+}
+
+struct LimSmem {
+  double q[Tile<3, 3>::N];
+  double qo[Tile<1, 1>::N];
+  double ru[Tile<1, 0>::N];
+  double rv[Tile<0, 1>::N];
+  double mt[Tile<1, 1>::N];
+  double s1[Tile<1, 1>::N];
+  double s2[Tile<1, 1>::N];
+};
+
+__global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a, const double *field,
+                                                               const double *field_old, double *s1, double *s2) {
+  __shared__ LimSmem sm;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt};
+  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
+  __syncthreads();
+  if (i >= nx || j >= ny) return;
+  CellFluxes cf;
+  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
+  using TO = Tile<1, 1>;
+  auto QO = [&](int r, int cc) { return sm.qo[(r + 1) * TO::W + (cc + 1)]; };
+  const double msftx = ld(g.msftx, ix2(j, i, nx));
+  const double rdzw = ld(g.rdnw, k);
+  const double mass_old = ld(g.c1h, k) * ld(a.mu_old, ix2(j, i, nx)) + ld(g.c2h, k);
+  const double fo = QO(ty, tx);
+  const double div_low = msftx * msftx * (g.rdx * (cf.lx1 - cf.lx0) + g.rdy * (cf.ly1 - cf.ly0)) +
+                         msftx * rdzw * (cf.lz1 - cf.lz0);
+  const double ph_low = mass_old * fo - a.dt * div_low;
+  auto pos = [](double x) { return dmax(0.0, x); };
+  auto neg = [](double x) { return dmin(0.0, x); };
+  const double flux_out = a.dt * (msftx * msftx * (g.rdx * (pos(cf.ax1) - neg(cf.ax0)) + g.rdy * (pos(cf.ay1) - neg(cf.ay0))) +
+                                  msftx * rdzw * (neg(cf.az1) - pos(cf.az0)));
+  double r1, r2;
+  if (a.opt == 1) {
+    r1 = (flux_out > ph_low) ? dmax(0.0, ph_low / (flux_out + PD_EPS)) : 1.0;
+    r2 = r1;
+  } else {
+    auto qov = [&](int kk) { return ld(field_old, ix3(kk, j, i, ny, nx)) - a.offset; };
+    double qmax = fo, qmin = fo;
+    const double n0 = QO(ty, tx - 1), n1 = QO(ty, tx + 1), n2 = QO(ty - 1, tx), n3 = QO(ty + 1, tx);
+    const double n4 = (k == 0) ? fo : qov(k - 1), n5 = (k == nz - 1) ? fo : qov(k + 1);
+    qmax = dmax(qmax, dmax(n0, n1));
+    qmin = dmin(qmin, dmin(n0, n1));
+    qmax = dmax(qmax, dmax(n2, n3));
+    qmin = dmin(qmin, dmin(n2, n3));
+    qmax = dmax(qmax, dmax(n4, n5));
+    qmin = dmin(qmin, dmin(n4, n5));
+    const double flux_in = -a.dt * (msftx * msftx * (g.rdx * (neg(cf.ax1) - pos(cf.ax0)) + g.rdy * (neg(cf.ay1) - pos(cf.ay0))) +
+                                    msftx * rdzw * (pos(cf.az1) - neg(cf.az0)));
+    const double ph_hi = qmax * mass_old - ph_low;
+    const double ph_lo = ph_low - qmin * mass_old;
+    r1 = (flux_in > ph_hi) ? dmax(0.0, ph_hi / (flux_in + PD_EPS)) : 1.0;
+    r2 = (flux_out > ph_lo) ? dmax(0.0, ph_lo / (flux_out + PD_EPS)) : 1.0;
+  }
+  const size_t c = ix3(k, j, i, ny, nx);
+  s1[c] = r1;
+  s2[c] = r2;
+}
+
+__global__ void __launch_bounds__(TSX *TSY) k_lim_tend_tiled(Grid g, LimArgs a, const double *field,
+                                                              const double *field_old, const double *s1,
+                                                              const double *s2, const double *base,
+                                                              const double *mu_total_stage, double *tend_out) {
+  __shared__ LimSmem sm;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt};
+  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
+  const size_t plane = (size_t)k * ny * nx;
+  load_tile<1, 1>(sm.s1, s1 + plane, nx, i0, j0, nx, ny, 0.0);
+  load_tile<1, 1>(sm.s2, s2 + plane, nx, i0, j0, nx, ny, 0.0);
+  __syncthreads();
+  if (i >= nx || j >= ny) return;
+  CellFluxes cf;
+  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
+  using TO = Tile<1, 1>;
+  auto S1 = [&](int r, int cc) { return sm.s1[(r + 1) * TO::W + (cc + 1)]; };
+  auto S2 = [&](int r, int cc) { return sm.s2[(r + 1) * TO::W + (cc + 1)]; };
+  auto S1k = [&](int kk) { return ld(s1, ix3(kk, j, i, ny, nx)); };
+  auto S2k = [&](int kk) { return ld(s2, ix3(kk, j, i, ny, nx)); };
+  double fx0, fx1, fy0, fy1, fz0, fz1;
+  if (a.opt == 1) {
+    auto limh = [&](double A, double s_m1, double s_c) { return A > 0.0 ? s_m1 * A : (A < 0.0 ? s_c * A : A); };
+    fx0 = limh(cf.ax0, S1(ty, tx - 1), S1(ty, tx));
+    fx1 = limh(cf.ax1, S1(ty, tx), S1(ty, tx + 1));
+    fy0 = limh(cf.ay0, S1(ty - 1, tx), S1(ty, tx));
+    fy1 = limh(cf.ay1, S1(ty, tx), S1(ty + 1, tx));
+    auto limz = [&](double A, double below, double above) { return A < 0.0 ? below * A : (A > 0.0 ? above * A : A); };
+    const double sc = S1(ty, tx);
+    fz0 = limz(cf.az0, k == 0 ? sc : S1k(k - 1), sc);
+    fz1 = limz(cf.az1, sc, k + 1 >= nz ? sc : S1k(k + 1));
+  } else {
+    auto limh = [&](double A, double in_c, double out_c, double in_m1, double out_m1) {
+      return A > 0.0 ? dmin(in_c, out_m1) * A : dmin(out_c, in_m1) * A;
+    };
+    fx0 = limh(cf.ax0, S1(ty, tx), S2(ty, tx), S1(ty, tx - 1), S2(ty, tx - 1));
+    fx1 = limh(cf.ax1, S1(ty, tx + 1), S2(ty, tx + 1), S1(ty, tx), S2(ty, tx));
+    fy0 = limh(cf.ay0, S1(ty, tx), S2(ty, tx), S1(ty - 1, tx), S2(ty - 1, tx));
+    fy1 = limh(cf.ay1, S1(ty + 1, tx), S2(ty + 1, tx), S1(ty, tx), S2(ty, tx));
+    auto limz = [&](double A, double in_above, double out_above, double in_below, double out_below) {
+      return A < 0.0 ? dmin(in_above, out_below) * A : dmin(out_above, in_below) * A;
+    };
+    const int kb = (k == 0) ? 0 : k - 1;
+    const int ka = (k + 1 >= nz) ? nz - 1 : k + 1;
+    const double s1c = S1(ty, tx), s2c = S2(ty, tx);
+    const double s1b = (kb == k) ? s1c : S1k(kb), s2b = (kb == k) ? s2c : S2k(kb);
+    const double s1a = (ka == k) ? s1c : S1k(ka), s2a = (ka == k) ? s2c : S2k(ka);
+    fz0 = limz(cf.az0, s1c, s2c, s1b, s2b);
+    fz1 = limz(cf.az1, s1a, s2a, s1c, s2c);
+  }
+  fx0 = fx0 + cf.lx0;
+  fx1 = fx1 + cf.lx1;
+  fy0 = fy0 + cf.ly0;
+  fy1 = fy1 + cf.ly1;
+  fz0 = fz0 + cf.lz0;
+  fz1 = fz1 + cf.lz1;
+  const double msftx = ld(g.msftx, ix2(j, i, nx));
+  double tend = -msftx * g.rdx * (fx1 - fx0);
+  tend = tend - msftx * g.rdy * (fy1 - fy0);
+  tend = tend - ld(g.rdnw, k) * (fz1 - fz0);
+  const size_t c = ix3(k, j, i, ny, nx);
+  if (base != nullptr) {
+    const double mass_h = ld(g.c1h, k) * ld(mu_total_stage, ix2(j, i, nx)) + ld(g.c2h, k);
+    tend_out[c] = ld(base, c) * mass_h + tend;
+  } else {
+    tend_out[c] = tend;
+  }
+}
+
+}  // namespace wg
