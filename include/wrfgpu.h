@@ -139,6 +139,33 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *params, const wrfgpu_metrics *metr
                     double lead_seconds, void *workspace, size_t workspace_bytes,
                     cudaStream_t stream);
 
+/* Size of the workspace that the library itself holds for
+ * wrfgpu_rk3_step_static_workspace: 32 MiB per GPU, reserved in every
+ * process that loads the library, on every GPU it runs on, until exit. */
+#define WRFGPU_STATIC_WORKSPACE_BYTES ((size_t)32 << 20)
+
+/* One RK3 step, like wrfgpu_rk3_step, but with its scratch taken from a
+ * fixed array the library holds on each GPU (WRFGPU_STATIC_WORKSPACE_BYTES)
+ * instead of a caller workspace.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory at all -- a host framework whose
+ * own pool owns the GPU's memory (so a cudaMalloc of ours could fail or
+ * fragment it), or a host model that calls one routine per step with a fixed
+ * argument list and has nowhere to keep a workspace between calls.  It calls
+ * no cudaMalloc/cudaFree and no allocating library routine.
+ *   - Grids whose wrfgpu_step_workspace_size() exceeds
+ *     WRFGPU_STATIC_WORKSPACE_BYTES are rejected with WRFGPU_ERR_WORKSPACE.
+ *   - The first call on a GPU looks up the array's device address (with that
+ *     GPU current); make that first call before any stream capture.
+ *   - Nothing in the array needs to start at zero: the step writes every
+ *     scratch value before reading it, and clears or copies mudf itself.
+ *   - Every call on one GPU shares the one array, which keeps the previous
+ *     call's contents: calls that overlap on that GPU (other streams, other
+ *     host threads) race and corrupt each other's results.  Order them on one
+ *     stream, or use wrfgpu_rk3_step with separate workspaces. */
+int wrfgpu_rk3_step_static_workspace(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                                     const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
+                                     double lead_seconds, cudaStream_t stream);
+
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 

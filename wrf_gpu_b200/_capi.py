@@ -22,6 +22,7 @@ WRFGPU_ERR_NULL_POINTER = 4
 WRFGPU_ERR_WORKSPACE = 5
 WRFGPU_PRECISION_FP64 = 0
 WRFGPU_PRECISION_MIXED = 1
+WRFGPU_STATIC_WORKSPACE_BYTES = 32 << 20  # include/wrfgpu.h
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -72,7 +73,7 @@ class StepOutputs(ctypes.Structure):
 
 
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
-            "wrfgpu_rk3_step", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version")
 
@@ -101,6 +102,9 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_rk3_step.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), ctypes.POINTER(StepInputs),
                                     ctypes.POINTER(StepOutputs), _D, _P, ctypes.c_size_t, _P]
     lib.wrfgpu_rk3_step.restype = _I
+    lib.wrfgpu_rk3_step_static_workspace.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
+                                                     ctypes.POINTER(StepInputs), ctypes.POINTER(StepOutputs), _D, _P]
+    lib.wrfgpu_rk3_step_static_workspace.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

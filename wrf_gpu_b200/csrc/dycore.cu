@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -660,3 +661,51 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Step with a library-held workspace, for callers that cannot allocate device
+// memory.  The array lives in this module on every GPU that loads it; its
+// device address is looked up once per GPU (with that GPU current) and then
+// reused.  No cudaMalloc/cudaFree or allocating library routine is called.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_static_workspace[WRFGPU_STATIC_WORKSPACE_BYTES];
+
+namespace {
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_ws_mutex;
+void *g_static_ws_addr[kMaxStaticDevices] = {};
+}  // namespace
+
+extern "C" int wrfgpu_rk3_step_static_workspace(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm,
+                                                const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
+                                                double lead_seconds, cudaStream_t stream) {
+  if (pp == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params is NULL");
+  int rc = wrfgpu_step_params_validate(pp);
+  if (rc) return rc;
+  size_t need = 0;
+  rc = wrfgpu_step_workspace_size(pp, &need);
+  if (rc) return rc;
+  if (need > WRFGPU_STATIC_WORKSPACE_BYTES)
+    return fail(WRFGPU_ERR_WORKSPACE,
+                "grid needs " + std::to_string(need) + " workspace bytes but the library-held workspace has " +
+                    std::to_string((size_t)WRFGPU_STATIC_WORKSPACE_BYTES) +
+                    "; use wrfgpu_rk3_step with a caller workspace for this grid");
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "cudaGetDevice failed");
+  if (dev < 0 || dev >= kMaxStaticDevices)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "device ordinal out of range for the library-held workspace");
+  void *ws = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_static_ws_mutex);
+    if (g_static_ws_addr[dev] == nullptr) {
+      void *addr = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_workspace);
+      if (e != cudaSuccess || addr == nullptr)
+        return fail(WRFGPU_ERR_CUDA, std::string("cudaGetSymbolAddress of the library-held workspace failed: ") +
+                                         cudaGetErrorString(e));
+      g_static_ws_addr[dev] = addr;
+    }
+    ws = g_static_ws_addr[dev];
+  }
+  return wrfgpu_rk3_step(pp, mm, in, out, lead_seconds, ws, WRFGPU_STATIC_WORKSPACE_BYTES, stream);
+}
