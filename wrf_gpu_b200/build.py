@@ -14,6 +14,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libwrfgpu.so"
+SELFTEST_LIB = HERE / "libwrfgpu_selftest.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -28,24 +29,31 @@ def sources() -> list[Path]:
     return [CSRC / "dycore.cu"]
 
 
-def _stale() -> bool:
-    if not LIB.exists():
+# (output library, its sources).  The self-test library holds device checks
+# of numerical helpers that only the tests load.
+TARGETS = ((LIB, [CSRC / "dycore.cu"]), (SELFTEST_LIB, [CSRC / "selftest.cu"]))
+
+
+def _stale(lib: Path = LIB) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
+    t = lib.stat().st_mtime
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "wrfgpu.h"]
     return any(p.stat().st_mtime > t for p in deps)
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile ``libwrfgpu.so`` for sm_100a if any source is newer than it."""
-    if not force and not _stale():
-        return LIB
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-shared",
-           "-I", str(HERE.parent / "include"), "-o", str(LIB) + ".tmp", *map(str, sources())]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    os.replace(str(LIB) + ".tmp", LIB)
+    """Compile ``libwrfgpu.so`` (and the self-test library) for sm_100a if any
+    source is newer than it."""
+    for lib, srcs in TARGETS:
+        if not force and not _stale(lib):
+            continue
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-shared",
+               "-I", str(HERE.parent / "include"), "-o", str(lib) + ".tmp", *map(str, srcs)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        os.replace(str(lib) + ".tmp", lib)
     return LIB
 
 

@@ -533,6 +533,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     if (lim_theta || lim_moist) {
       LimArgs la;
       la.ru = w.ru; la.rv = w.rv; la.rom = w.rom; la.mut = s.mu_total; la.mu_old = origin.mu_total; la.dt = dt;
+      set_lim_constants(la, g.rdx, g.rdy);
       if (lim_theta) {
         la.opt = p.scalar_adv_opt;
         la.offset = T0;

@@ -73,18 +73,36 @@ __device__ __forceinline__ double ld(const double *p, size_t i) { return __ldg(p
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 
+// a / b, correctly rounded, for a divisor b whose reciprocal rb = RN(1/b) is
+// known in advance (a literal or a per-launch constant).  This is Markstein's
+// correction step (P. Markstein, IBM J. Res. Dev. 34(1):111-119, 1990; J.-M.
+// Muller et al., Handbook of Floating-Point Arithmetic, ch. "Division"):
+// q0 = RN(a*rb) is within one ulp of a/b, the residual r = a - b*q0 is exact
+// in one fma, and RN(q0 + r*rb) is the correctly rounded quotient.  For normal
+// operands and quotients the result equals the IEEE quotient a / b bit for bit
+// (a zero a may come back as +0 where a / b gives -0); it costs one multiply
+// and two fmas instead of a full division sequence.
+__device__ __forceinline__ double div_rcp(double a, double b, double rb) {
+  const double q0 = __dmul_rn(a, rb);
+  const double r = __fma_rn(-b, q0, a);
+  return __fma_rn(r, rb, q0);
+}
+constexpr double R60 = 1.0 / 60.0;
+constexpr double R12 = 1.0 / 12.0;
+constexpr double RG = 1.0 / G;
+
 // WRF flux5 left-face value (src/gpuwrf/dynamics/flux_advection.py:53-88).
 __device__ __forceinline__ double flux5(double qm3, double qm2, double qm1, double q0, double qp1, double qp2,
                                         double vel) {
-  double f6 = (37.0 * (q0 + qm1) - 8.0 * (qp1 + qm2) + (qp2 + qm3)) / 60.0;
-  double c = ((qp2 - qm3) - 5.0 * (qp1 - qm2) + 10.0 * (q0 - qm1)) / 60.0;
+  double f6 = div_rcp(37.0 * (q0 + qm1) - 8.0 * (qp1 + qm2) + (qp2 + qm3), 60.0, R60);
+  double c = div_rcp((qp2 - qm3) - 5.0 * (qp1 - qm2) + 10.0 * (q0 - qm1), 60.0, R60);
   return f6 - sgn(vel) * c;
 }
 
 // flux3 with the -sign(vel) upwind correction (flux_advection.py:534-562, 1362-1407).
 __device__ __forceinline__ double flux3v(double qkm2, double qkm1, double qk, double qkp1, double vel) {
-  double flux4 = (7.0 * (qk + qkm1) - (qkp1 + qkm2)) / 12.0;
-  double corr = ((qkp1 - qkm2) - 3.0 * (qk - qkm1)) / 12.0;
+  double flux4 = div_rcp(7.0 * (qk + qkm1) - (qkp1 + qkm2), 12.0, R12);
+  double corr = div_rcp((qkp1 - qkm2) - 3.0 * (qk - qkm1), 12.0, R12);
   return vel * (flux4 + sgn(-vel) * corr);
 }
 

@@ -571,7 +571,21 @@ struct LimArgs {
   double dt;
   int opt;               // 1 PD, 2 mono
   double offset;         // subtracted from both fields (300 for theta, 0 for q)
+  // Per-launch constants of the upwind fluxes (set by set_lim_constants):
+  // dx = 1/rdx and dy = 1/rdy as the reference forms them, their correctly
+  // rounded reciprocals (divisors for div_rcp), 1/dt, dx/dt and dy/dt.
+  double dxl, dyl, rdxl, rdyl, rdt, dxl_dt, dyl_dt;
 };
+
+inline void set_lim_constants(LimArgs &a, double rdx, double rdy) {
+  a.dxl = 1.0 / rdx;
+  a.dyl = 1.0 / rdy;
+  a.rdxl = 1.0 / a.dxl;
+  a.rdyl = 1.0 / a.dyl;
+  a.rdt = 1.0 / a.dt;
+  a.dxl_dt = a.dxl / a.dt;
+  a.dyl_dt = a.dyl / a.dt;
+}
 
 struct CellFluxes {
   double lx0, lx1, ly0, ly1, lz0, lz1;  // low-order fluxes at the 6 faces

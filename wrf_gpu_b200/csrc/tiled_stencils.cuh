@@ -46,9 +46,13 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_tiled(Grid g, StateR s,
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
+  constexpr int NXF = TSY * (TSX + 1);  // x faces of the tile, each computed once
+  constexpr int NYF = (TSY + 1) * TSX;  // y faces
   __shared__ double sq[TQ::N];
   __shared__ double sru[TR::N];
   __shared__ double srv[TV::N];
+  __shared__ double sfx[NXF];
+  __shared__ double sfy[NYF];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
@@ -66,18 +70,32 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_tiled(Grid g, StateR s,
     __syncthreads();
     load_tile<3, 3>(sq, fld + plane, nx, i0, j0, nx, ny, sub);
     __syncthreads();
-    if (!valid) return 0.0;
     auto Q = [&](int r, int cc) { return sq[(r + 3) * TQ::W + (cc + 3)]; };  // local (row, col)
-    auto fqx = [&](int m) {  // face at local column m
-      const double vel = sru[ty * TR::W + (m + 1)];
-      return vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
+    auto fqx = [&](int r, int m) {  // x face at local column m of row r
+      const double vel = sru[r * TR::W + (m + 1)];
+      return vel * flux5(Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2), vel);
     };
-    auto fqy = [&](int r) {
-      const double vel = srv[(r + 1) * TV::W + tx];
-      return vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
+    auto fqy = [&](int r, int cc) {  // y face at local row r of column cc
+      const double vel = srv[(r + 1) * TV::W + cc];
+      return vel * flux5(Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc), vel);
     };
-    double tend = -msftx * g.rdx * (fqx(tx + 1) - fqx(tx));
-    tend = tend - msftx * g.rdy * (fqy(ty + 1) - fqy(ty));
+    // Every face flux of the tile once (the tile's stencil reads are in
+    // shared memory and wrap periodically, so edge tiles compute harmless
+    // extra faces).
+    for (int e = ty * TSX + tx; e < NXF + NYF; e += TSX * TSY) {
+      if (e < NXF) {
+        const int r = e / (TSX + 1), m = e - r * (TSX + 1);
+        sfx[e] = fqx(r, m);
+      } else {
+        const int e2 = e - NXF;
+        const int r = e2 / TSX, cc = e2 - r * TSX;
+        sfy[e2] = fqy(r, cc);
+      }
+    }
+    __syncthreads();
+    if (!valid) return 0.0;
+    double tend = -msftx * g.rdx * (sfx[ty * (TSX + 1) + tx + 1] - sfx[ty * (TSX + 1) + tx]);
+    tend = tend - msftx * g.rdy * (sfy[(ty + 1) * TSX + tx] - sfy[ty * TSX + tx]);
     auto qc = [&](int kk) { return ld(fld, ix3(kk, j, i, ny, nx)) - sub; };
     const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, rom1, qc) : 0.0;
     const double v0 = (k >= 1) ? vflux3_at(g, k, rom0, qc) : 0.0;
@@ -113,12 +131,20 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_tiled(Grid g, StateR s,
 // PD / monotonic limited scalar advection (flux_advection.py:736-1000),
 // tiled.  Pass 1 writes the per-cell scale(s); pass 2 the tendency.
 // ---------------------------------------------------------------------------
+// Vertical spacing of the two faces of the block's level (k and k+1):
+// dz = 2/(rdnw[m] + rdnw[m-1]) (flux_advection.py upwind z flux), its
+// correctly rounded reciprocal and dz/dt.  Computed once per block.
+struct ZConst {
+  double dz, rdz, dz_dt;
+};
+
 struct LimTiles {
   double *q;    // Tile<3,3>: field - offset
   double *qo;   // Tile<1,1>: field_old - offset
   double *ru;   // Tile<1,0>
   double *rv;   // Tile<0,1>
   double *mt;   // Tile<1,1>: current total dry mass (2-D)
+  const struct ZConst *zc;  // the level's two faces: dz, 1/dz, dz/dt
 };
 
 __device__ __forceinline__ void lim_stage_tiles(const Grid &g, const LimArgs &a, const double *field,
@@ -132,6 +158,20 @@ __device__ __forceinline__ void lim_stage_tiles(const Grid &g, const LimArgs &a,
   load_tile<1, 1>(t.mt, a.mut, nx, i0, j0, nx, ny, 0.0);
 }
 
+__device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int k, ZConst *zc) {
+  const int f = threadIdx.y * TSX + threadIdx.x;
+  if (f < 2) {
+    const int m = k + f;
+    ZConst z{1.0, 1.0, 1.0};
+    if (m >= 1 && m < g.nz) {
+      z.dz = 2.0 / (ld(g.rdnw, m) + ld(g.rdnw, m - 1));
+      z.rdz = 1.0 / z.dz;
+      z.dz_dt = z.dz / a.dt;
+    }
+    zc[f] = z;
+  }
+}
+
 // The 12 face fluxes of cell (k, j, i) from the staged tiles (same algebra as
 // cell_fluxes in stage_kernels.cuh).
 __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int j,
@@ -143,21 +183,22 @@ __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &
   using TO = Tile<1, 1>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
-  const double dx = 1.0 / g.rdx, dy = 1.0 / g.rdy;
   const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
   auto Q = [&](int r, int cc) { return t.q[(r + 3) * TQ::W + (cc + 3)]; };
   auto QO = [&](int r, int cc) { return t.qo[(r + 1) * TO::W + (cc + 1)]; };
   auto MT = [&](int r, int cc) { return t.mt[(r + 1) * TO::W + (cc + 1)]; };
-  auto upw = [&](double fo_m1, double fo_0, double vel, double mu_face, double dxy) {
-    double cr = vel * a.dt / dxy / mu_face;
+  // cr = vel*dt/dxy/mu_face and mu_face*(dxy/dt)*(...) with the constant
+  // divisions done by div_rcp / per-launch constants (same bits).
+  auto upw = [&](double fo_m1, double fo_0, double vel, double mu_face, double dxy, double rdxy, double dxy_dt) {
+    double cr = div_rcp(vel * a.dt, dxy, rdxy) / mu_face;
     double ab = fabs(cr);
-    return mu_face * (dxy / a.dt) * (0.5 * dmin(1.0, cr + ab) * fo_m1 + 0.5 * dmax(-1.0, cr - ab) * fo_0);
+    return mu_face * dxy_dt * (0.5 * dmin(1.0, cr + ab) * fo_m1 + 0.5 * dmax(-1.0, cr - ab) * fo_0);
   };
   auto xf = [&](int m, double &lo, double &an) {
     const double vel = t.ru[ty * TR::W + (m + 1)];
     const double muu = 0.5 * (MT(ty, m) + MT(ty, m - 1));
     const double mu_u = c1 * muu + c2;
-    lo = upw(QO(ty, m - 1), QO(ty, m), vel, mu_u, dx);
+    lo = upw(QO(ty, m - 1), QO(ty, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
     const double hi = vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
     an = hi - lo;
   };
@@ -165,7 +206,7 @@ __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &
     const double vel = t.rv[(r + 1) * TV::W + tx];
     const double muv = 0.5 * (MT(r, tx) + MT(r - 1, tx));
     const double mu_v = c1 * muv + c2;
-    lo = upw(QO(r - 1, tx), QO(r, tx), vel, mu_v, dy);
+    lo = upw(QO(r - 1, tx), QO(r, tx), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
     const double hi = vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
     an = hi - lo;
   };
@@ -181,11 +222,11 @@ __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &
     const double mtc = MT(ty, tx);
     const double muh_m = ld(g.c1h, m) * mtc + ld(g.c2h, m);
     const double muh_mm1 = ld(g.c1h, m - 1) * mtc + ld(g.c2h, m - 1);
-    const double dz = 2.0 / (ld(g.rdnw, m) + ld(g.rdnw, m - 1));
+    const int zi = m - k;  // 0: bottom face of this level, 1: top face
     const double mu_face = 0.5 * (muh_m + muh_mm1);
-    const double cr = romv * a.dt / dz / mu_face;
+    const double cr = div_rcp(romv * a.dt, t.zc[zi].dz, t.zc[zi].rdz) / mu_face;
     const double ab = fabs(cr);
-    lo = mu_face * (dz / a.dt) * (0.5 * dmin(1.0, cr + ab) * qo(m - 1) + 0.5 * dmax(-1.0, cr - ab) * qo(m));
+    lo = mu_face * t.zc[zi].dz_dt * (0.5 * dmin(1.0, cr + ab) * qo(m - 1) + 0.5 * dmax(-1.0, cr - ab) * qo(m));
     const double hi = vflux3_at(g, m, romv, qf);
     an = hi - lo;
   };
@@ -205,6 +246,7 @@ struct LimSmem {
   double mt[Tile<1, 1>::N];
   double s1[Tile<1, 1>::N];
   double s2[Tile<1, 1>::N];
+  ZConst zc[2];
 };
 
 __global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a, const double *field,
@@ -214,8 +256,9 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a,
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
   const int i = i0 + tx, j = j0 + ty;
-  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt};
+  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc};
   lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
+  lim_zconst(g, a, k, sm.zc);
   __syncthreads();
   if (i >= nx || j >= ny) return;
   CellFluxes cf;
@@ -269,8 +312,9 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_tend_tiled(Grid g, LimArgs a, 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
   const int i = i0 + tx, j = j0 + ty;
-  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt};
+  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc};
   lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
+  lim_zconst(g, a, k, sm.zc);
   const size_t plane = (size_t)k * ny * nx;
   load_tile<1, 1>(sm.s1, s1 + plane, nx, i0, j0, nx, ny, 0.0);
   load_tile<1, 1>(sm.s2, s2 + plane, nx, i0, j0, nx, ny, 0.0);
