@@ -92,8 +92,9 @@ def test_launch_count(lib):
     p = _params(lib, acoustic_substeps=6)
     n = ctypes.c_int(0)
     assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(n)) == 0
-    # 3 stages x (8 stage + 3 finish) + 3 launches per substep x (1 + 3 + 6)
-    assert n.value == 3 * 11 + 3 * 10
+    # map-factor reciprocals + 3 stages x (8 stage + 3 finish)
+    # + 3 launches per substep x (1 + 3 + 6)
+    assert n.value == 1 + 3 * 11 + 3 * 10
 
 
 def test_null_pointers_rejected_before_any_launch(lib):

@@ -16,13 +16,24 @@
 
 namespace wg {
 
-constexpr int COL_TX = 32;
-constexpr int COL_TY = 8;
+// Block shape: COL_TX columns x COL_TY level lanes; COL_MINB resident blocks
+// per SM requested from the register allocator.
+#ifndef WG_COL_TX
+#define WG_COL_TX 32
+#endif
+#ifndef WG_COL_TY
+#define WG_COL_TY 16
+#endif
+#ifndef WG_COL_MINB
+#define WG_COL_MINB 2
+#endif
+constexpr int COL_TX = WG_COL_TX;
+constexpr int COL_TY = WG_COL_TY;
 constexpr int COL_NARR = 7;
 
 inline size_t column_tiled_smem_bytes(int nz) { return (size_t)COL_NARR * (nz + 1) * COL_TX * sizeof(double); }
 
-__global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoustic A, ColArgs c) {
+__global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(Grid g, Acoustic A, ColArgs c) {
   extern __shared__ double sm[];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -40,6 +51,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
   const double msftx = valid ? ld(g.msftx, c2d) : 1.0;
   const double msfty = valid ? ld(g.msfty, c2d) : 1.0;
   const double mut = valid ? ld(A.mut, c2d) : 1.0;
+  const double minv = valid ? ld(g.rmsfty, c2d) : 1.0;  // == 1.0 / msfty
   const bool active = valid && (!c.specified || (j >= 1 && j <= ny - 2 && i >= 1 && i <= nx - 2));
   auto T1 = [&](int k, int jj, int ii2) { return ld(A.theta_s, ix3(k, jj, ii2, ny, nx)) - T0; };
   const int nxu = nx + 1, nyv = ny + 1;
@@ -50,14 +62,15 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
   if (active) {
     const double muv_n = ld(A.muv, ix2(j + 1, i, nx)), muv_s = ld(A.muv, ix2(j, i, nx));
     const double muu_e = ld(A.muu, ix2(j, i + 1, nxu)), muu_w = ld(A.muu, ix2(j, i, nxu));
-    const double fvi_n = 1.0 / ld(g.msfvx, ix2(j + 1, i, nx)), fvi_s = 1.0 / ld(g.msfvx, ix2(j, i, nx));
+    const double fvi_n = ld(g.rmsfvx, ix2(j + 1, i, nx)), fvi_s = ld(g.rmsfvx, ix2(j, i, nx));  // 1/msfvx
     const double fuy_e = ld(g.msfuy, ix2(j, i + 1, nxu)), fuy_w = ld(g.msfuy, ix2(j, i, nxu));
+    const double rfuy_e = ld(g.rmsfuy, ix2(j, i + 1, nxu)), rfuy_w = ld(g.rmsfuy, ix2(j, i, nxu));
     for (int k = ty; k < nz; k += COL_TY) {
       const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-      const double vn = A.v[ix3(k, j + 1, i, nyv, nx)] + (c1 * muv_n + c2) * ld(A.v_1, ix3(k, j + 1, i, nyv, nx)) * fvi_n;
-      const double vs = A.v[ix3(k, j, i, nyv, nx)] + (c1 * muv_s + c2) * ld(A.v_1, ix3(k, j, i, nyv, nx)) * fvi_s;
-      const double ue = A.u[ix3(k, j, i + 1, ny, nxu)] + (c1 * muu_e + c2) * ld(A.u_1, ix3(k, j, i + 1, ny, nxu)) / fuy_e;
-      const double uw = A.u[ix3(k, j, i, ny, nxu)] + (c1 * muu_w + c2) * ld(A.u_1, ix3(k, j, i, ny, nxu)) / fuy_w;
+      const double vn = ld(A.v, ix3(k, j + 1, i, nyv, nx)) + (c1 * muv_n + c2) * ld(A.v_1, ix3(k, j + 1, i, nyv, nx)) * fvi_n;
+      const double vs = ld(A.v, ix3(k, j, i, nyv, nx)) + (c1 * muv_s + c2) * ld(A.v_1, ix3(k, j, i, nyv, nx)) * fvi_s;
+      const double ue = ld(A.u, ix3(k, j, i + 1, ny, nxu)) + div_rcp((c1 * muu_e + c2) * ld(A.u_1, ix3(k, j, i + 1, ny, nxu)), fuy_e, rfuy_e);
+      const double uw = ld(A.u, ix3(k, j, i, ny, nxu)) + div_rcp((c1 * muu_w + c2) * ld(A.u_1, ix3(k, j, i, ny, nxu)), fuy_w, rfuy_w);
       S(A0, k) = msftx * msfty * (g.rdy * (vn - vs) + g.rdx * (ue - uw));
     }
   }
@@ -105,7 +118,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
         const int k = kk - 1;
         double dv = S(A0, k);
         if (c.specified) dv = dv * scale;
-        S(A1, kk) = ld(g.dnw, k) * (ld(g.c1h, k) * dmdt + dv + ld(g.c1h, k) * mu_tend) / msfty;
+        S(A1, kk) = div_rcp(ld(g.dnw, k) * (ld(g.c1h, k) * dmdt + dv + ld(g.c1h, k) * mu_tend), msfty, minv);
       }
       for (int k = ty; k <= nz; k += COL_TY) S(A2, k) = ld(A.ww_1, M(k));
     } else {
@@ -125,7 +138,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
     S(A3, nz) = A.ww[M(nz)];
   }
   __syncthreads();
-  // ---------------- P5: theta update, t_2ave, wd -> A0, buoy -> A1 ----------------
+  // ---------------- P5: theta update, t_2ave, wd -> A0, buoy -> A1, coef -> A5 ----------------
   const double muts = valid ? A.muts[c2d] : 1.0;
   const double muave = valid ? A.muave[c2d] : 0.0;
   if (valid) {
@@ -144,8 +157,8 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
                                    : 0.0;
         const double wdtn_lo = (k >= 1) ? S(A3, k) * (ld(g.fnm, k) * T1(k, j, i) + ld(g.fnp, k) * T1(k - 1, j, i)) : 0.0;
         const double th = T1(k, j, i);
-        const double v_flux = A.v[ix3(k, j + 1, i, nyv, nx)] * (T1(k, jn, i) + th) - A.v[ix3(k, j, i, nyv, nx)] * (th + T1(k, js, i));
-        const double u_flux = A.u[ix3(k, j, i + 1, ny, nxu)] * (T1(k, j, ie) + th) - A.u[ix3(k, j, i, ny, nxu)] * (th + T1(k, j, iw));
+        const double v_flux = ld(A.v, ix3(k, j + 1, i, nyv, nx)) * (T1(k, jn, i) + th) - ld(A.v, ix3(k, j, i, nyv, nx)) * (th + T1(k, js, i));
+        const double u_flux = ld(A.u, ix3(k, j, i + 1, ny, nxu)) * (T1(k, j, ie) + th) - ld(A.u, ix3(k, j, i, ny, nxu)) * (th + T1(k, j, iw));
         const double tend = msftx * (0.5 * g.rdy * v_flux + 0.5 * g.rdx * u_flux) + ld(g.rdnw, k) * (wdtn_hi - wdtn_lo);
         const double theta_i = thw + msfty * dts * ld(A.t_tend, M(k));
         thw = theta_i - dts * msfty * tend;
@@ -155,7 +168,9 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
       const double half = 0.5 * (eps_p * thw + eps_m * A.t2ave[M(k)]);
       const double t2a = (half + (ld(g.c1h, k) * muave) * T0) / (mass_h * (T0 + T1(k, j, i)));
       A.t2ave[M(k)] = t2a;
-      S(A1, k) = ld(A.c2a, M(k)) * ld(A.alt, M(k)) * t2a;
+      const double c2a_k = ld(A.c2a, M(k));
+      S(A1, k) = c2a_k * ld(A.alt, M(k)) * t2a;
+      S(A5, k) = c2a_k * ld(g.rdnw, k) / safe12(ld(g.c1h, k) * mut + ld(g.c2h, k));  // coef(k) for P7
       const double wwm = 0.5 * (S(A3, k + 1) + S(A3, k));
       S(A0, k) = wwm * ld(g.rdnw, k) * (ld(A.pt1, M(k + 1)) - ld(A.pt1, M(k)));
     }
@@ -180,8 +195,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
     }
   }
   __syncthreads();
-  // ---------------- P7: explicit w -> A5, a -> A0, alpha -> A3, gamma -> A6 ----------------
-  const double minv = 1.0 / msfty;
+  // ---------------- P7: explicit w -> A6 (coef from A5); then a -> A0, alpha -> A3, gamma -> A5 ----------------
   if (valid) {
     const double c05dg = 0.5 * dts * G;
     const double dtsg = dts * G;
@@ -217,8 +231,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
           rw = rw + damp;
         }
         wn = w_old + dts * rw;
-        const double coef_f = ld(A.c2a, M(f)) * ld(g.rdnw, f) / safe12(ld(g.c1h, f) * mut + ld(g.c2h, f));
-        const double coef_m1 = ld(A.c2a, M(f - 1)) * ld(g.rdnw, f - 1) / safe12(ld(g.c1h, f - 1) * mut + ld(g.c2h, f - 1));
+        const double coef_f = S(A5, f), coef_m1 = S(A5, f - 1);
         const double tA_u = coef_f * (eps_p * (S(A2, f + 1) - S(A2, f)) + eps_m * (S(A4, f + 1) - S(A4, f)));
         const double tA_l = coef_m1 * (eps_p * (S(A2, f) - S(A2, f - 1)) + eps_m * (S(A4, f) - S(A4, f - 1)));
         const double tA = minv * ld(A.cqw, M(f)) * (c05dg * ld(g.rdn, f)) * (tA_u - tA_l);
@@ -235,28 +248,30 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
         const double w_top = A.w[M(nz)] + dts * ld(A.rw_tend, M(nz)) + minv * (tA_top + tB_top);
         wn = c.top_lid ? 0.0 : w_top;
       }
-      S(A5, f) = wn;
-      S(A0, f) = ld(A.a, M(f));
-      S(A6, f) = ld(A.gamma, M(f));
+      S(A6, f) = wn;
     }
   }
   __syncthreads();
   if (valid) {
-    for (int f = ty; f <= nz; f += COL_TY) S(A3, f) = ld(A.alpha, M(f));
+    for (int f = ty; f <= nz; f += COL_TY) {
+      S(A0, f) = ld(A.a, M(f));
+      S(A3, f) = ld(A.alpha, M(f));
+      S(A5, f) = ld(A.gamma, M(f));
+    }
   }
   __syncthreads();
   // ---------------- P8: Thomas forward + back substitution (serial) ----------------
   if (ty == 0 && valid) {
-    double wf_prev = S(A5, 0);
+    double wf_prev = S(A6, 0);
     for (int f = 1; f <= nz; ++f) {
-      const double wf = (S(A5, f) - S(A0, f) * wf_prev) * S(A3, f);
-      S(A5, f) = wf;
+      const double wf = (S(A6, f) - S(A0, f) * wf_prev) * S(A3, f);
+      S(A6, f) = wf;
       wf_prev = wf;
     }
-    double ws_next = S(A5, nz);
+    double ws_next = S(A6, nz);
     for (int f = nz - 1; f >= 1; --f) {
-      const double ws = S(A5, f) - S(A6, f) * ws_next;
-      S(A5, f) = ws;
+      const double ws = S(A6, f) - S(A5, f) * ws_next;
+      S(A6, f) = ws;
       ws_next = ws;
     }
   }
@@ -267,14 +282,14 @@ __global__ void __launch_bounds__(COL_TX * COL_TY) k_column_tiled(Grid g, Acoust
     double dampmag = 0.0, hbot = 0.0;
     if (do_damp) {
       dampmag = dts * c.dampcoef;
-      hbot = ld(A.pt1, M(nz)) / G - c.zdamp;
+      hbot = div_rcp(ld(A.pt1, M(nz)), G, RG) - c.zdamp;
     }
     for (int f = ty; f <= nz; f += COL_TY) {
-      double ws = S(A5, f);
+      double ws = S(A6, f);
       if (f >= 1) {
         if (do_damp) {
-          const double hk = ld(A.pt1, M(f)) / G;
-          const double sv = sin(0.5 * 3.141592653589793 * (hk - hbot) / c.zdamp);
+          const double hk = div_rcp(ld(A.pt1, M(f)), G, RG);
+          const double sv = sin(over_zdamp(0.5 * 3.141592653589793 * (hk - hbot), c));
           const double ramp = sv * sv;
           const double dampwt = (hk >= hbot) ? dampmag * ramp : 0.0;
           const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);

@@ -65,6 +65,7 @@ struct Carver {
 struct Work {
   // 2-D
   double *mub, *mut, *muts0, *mu_work0, *muu, *muus, *muv, *muvs, *mu, *muts, *muave, *mudf, *phb0;
+  double *rmsftx, *rmsfty, *rmsfux, *rmsfuy, *rmsfvx, *rmsfvy;  // map-factor reciprocals
   // mass
   double *alt_raw, *alt, *pb, *c2a, *qtot, *al_ls, *php_ls, *php, *t_tend, *theta_w, *t2ave, *p, *pm1, *al;
   double *s1, *s2, *ru, *rv;
@@ -85,6 +86,8 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   w.muu = c.take(d.su); w.muus = c.take(d.su); w.muv = c.take(d.sv); w.muvs = c.take(d.sv);
   w.mu = c.take(d.s2); w.muts = c.take(d.s2); w.muave = c.take(d.s2); w.mudf = c.take(d.s2);
   w.phb0 = c.take(d.s2);
+  w.rmsftx = c.take(d.s2); w.rmsfty = c.take(d.s2); w.rmsfux = c.take(d.su); w.rmsfuy = c.take(d.su);
+  w.rmsfvx = c.take(d.sv); w.rmsfvy = c.take(d.sv);
   w.alt_raw = c.take(d.m); w.alt = c.take(d.m); w.pb = c.take(d.m); w.c2a = c.take(d.m);
   w.qtot = c.take(d.m); w.al_ls = c.take(d.m); w.php_ls = c.take(d.m); w.php = c.take(d.m);
   w.t_tend = c.take(d.m); w.theta_w = c.take(d.m); w.t2ave = c.take(d.m); w.p = c.take(d.m);
@@ -172,7 +175,7 @@ __global__ void k_bdy_target_u(Grid g, BdyLeaf b, const double *u_save, const do
     const size_t f2 = ix2(j, i, x_len);
     const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
     const double ms = c1 * ld(muus, f2) + c2, mc = c1 * ld(muu, f2) + c2;
-    t = (strip_at(b, nz, side, best, k, j) * ms - ld(u_save, cu) * mc) / ld(g.msfuy, f2);
+    t = div_msf(strip_at(b, nz, side, best, k, j) * ms - ld(u_save, cu) * mc, g.msfuy, g.rmsfuy, f2);
   }
   target[cu] = t;
 }
@@ -196,9 +199,32 @@ __global__ void k_bdy_target_v(Grid g, BdyLeaf b, const double *v_save, const do
     const size_t f2 = ix2(j, i, nx);
     const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
     const double ms = c1 * ld(muvs, f2) + c2, mc = c1 * ld(muv, f2) + c2;
-    t = (strip_at(b, nz, side, best, k, i) * ms - ld(v_save, cv) * mc) / ld(g.msfvx, f2);
+    t = div_msf(strip_at(b, nz, side, best, k, i) * ms - ld(v_save, cv) * mc, g.msfvx, g.rmsfvx, f2);
   }
   target[cv] = t;
+}
+
+// Correctly rounded map-factor reciprocals, once per step (index space
+// (ny+1) x (nx+1) covers the mass, u-face and v-face 2-D shapes).
+__global__ void k_recip_msf(Grid g, double *rtx, double *rty, double *rux, double *ruy, double *rvx, double *rvy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = g.nx, ny = g.ny;
+  if (i < nx && j < ny) {
+    const size_t c = ix2(j, i, nx);
+    rtx[c] = 1.0 / ld(g.msftx, c);
+    rty[c] = 1.0 / ld(g.msfty, c);
+  }
+  if (i <= nx && j < ny) {
+    const size_t c = ix2(j, i, nx + 1);
+    rux[c] = 1.0 / ld(g.msfux, c);
+    ruy[c] = 1.0 / ld(g.msfuy, c);
+  }
+  if (i < nx && j <= ny) {
+    const size_t c = ix2(j, i, nx);
+    rvx[c] = 1.0 / ld(g.msfvx, c);
+    rvy[c] = 1.0 / ld(g.msfvy, c);
+  }
 }
 
 inline dim3 blk2() { return dim3(32, 4, 1); }
@@ -227,7 +253,7 @@ struct ProfState {
 };
 ProfState g_prof;
 
-const char *kClassNames[] = {"k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
+const char *kClassNames[] = {"k_recip_msf", "k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
                              "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_u",
                              "k_advance_v", "k_column", "k_finish_u", "k_finish_v", "k_finish_col"};
 constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
@@ -393,7 +419,7 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
   const int ns = p->acoustic_substeps;
   const int nsub[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
   const bool bdy = p->run_boundary != 0;
-  int n = 0;
+  int n = 1;  // map-factor reciprocals
   for (int s = 0; s < 3; ++s) {
     n += 8;  // mass2d, transport, diag, uface, vface, mass, wface, coef
     if (s == 2 && (p->scalar_adv_opt == 1 || p->scalar_adv_opt == 2)) n += 2;
@@ -445,6 +471,8 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   Work w;
   carve(p, cv, w);
   Grid g = make_grid(p, *mm, nullptr);
+  g.rmsftx = w.rmsftx; g.rmsfty = w.rmsfty; g.rmsfux = w.rmsfux; g.rmsfuy = w.rmsfuy;
+  g.rmsfvx = w.rmsfvx; g.rmsfvy = w.rmsfvy;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const bool specified = p.run_boundary && !p.bc_ideal;
   const double dt = p.dt;
@@ -488,6 +516,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     bl_u = BdyLeaf{in->u_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
     bl_v = BdyLeaf{in->v_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
   }
+
+  PROF("k_recip_msf");
+  k_recip_msf<<<grd(nx + 1, ny + 1, 1), blk2(), 0, stream>>>(g, w.rmsftx, w.rmsfty, w.rmsfux, w.rmsfuy, w.rmsfvx,
+                                                             w.rmsfvy);
+  LAUNCH_CHECK("k_recip_msf");
 
   StateR s = origin;
   for (int stage = 0; stage < 3; ++stage) {
@@ -590,6 +623,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       ba.sub_ratio = strength * (dt != 0.0 ? dts / dt : 0.0);
       ba.spec_zone = 1;  // apply_normal_bdy_work uses DEFAULT_BOUNDARY_CONFIG widths
       ba.relax_zone = 4;
+      set_bdy_weights(ba);
     }
 
     Acoustic A;
@@ -602,7 +636,8 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     A.mut = w.mut; A.muu = w.muu; A.muv = w.muv; A.muus = w.muus; A.muvs = w.muvs;
     A.mu_tend = in->base_mu;
     A.u_1 = s.u; A.v_1 = s.v; A.w_save = s.w; A.theta_s = s.theta; A.phb0 = w.phb0;
-    ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp};
+    ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp,
+               (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0};
     const size_t col_smem = column_tiled_smem_bytes(nz);
     if (stage == 0 &&
         cudaFuncSetAttribute(k_column_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) != cudaSuccess)

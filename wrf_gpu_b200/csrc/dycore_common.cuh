@@ -38,6 +38,9 @@ struct Grid {
   const double *dn, *dnw, *rdn, *rdnw, *fnm, *fnp;
   const double *msftx, *msfty, *msfux, *msfuy, *msfvx, *msfvy;
   const double *f, *e, *sina, *cosa;
+  // Correctly rounded reciprocals of the map factors (filled once per step),
+  // so a division by a map factor is an exact div_rcp.
+  const double *rmsftx, *rmsfty, *rmsfux, *rmsfuy, *rmsfvx, *rmsfvy;
   double cf1, cf2, cf3, p_top;
   double cfn, cfn1;  // top-face extrapolation weights (rk_addtend_dry.py:282-288)
 };
@@ -86,6 +89,10 @@ __device__ __forceinline__ double div_rcp(double a, double b, double rb) {
   const double q0 = __dmul_rn(a, rb);
   const double r = __fma_rn(-b, q0, a);
   return __fma_rn(r, rb, q0);
+}
+// a / msf[idx] with the map factor's precomputed reciprocal.
+__device__ __forceinline__ double div_msf(double a, const double *msf, const double *rmsf, size_t idx) {
+  return div_rcp(a, __ldg(msf + idx), __ldg(rmsf + idx));
 }
 constexpr double R60 = 1.0 / 60.0;
 constexpr double R12 = 1.0 / 12.0;

@@ -3,7 +3,7 @@
 // The flux-form momentum advection (flux_advection.py:1131-1329) reads its
 // horizontal stencils from shared-memory plane tiles (periodic wrap applied
 // once per staged element); the large-step PGF, Coriolis, pg_buoy_w and
-// rhs_ph terms keep the global-load form of stage_kernels.cuh.  The wrap face
+// rhs_ph terms read global memory (L1-cached neighbours).  The wrap face
 // (i = nx for u, j = ny for v) takes the global-load advection path, which is
 // the reference's periodic copy of face 0.  Arithmetic order is unchanged.
 #pragma once
@@ -13,7 +13,12 @@
 
 namespace wg {
 
-// Advection of u at collapsed face ii (global loads), as in k_uface.
+// Resident blocks per SM requested for the face kernels (register budget).
+#ifndef WG_FACE_MINB
+#define WG_FACE_MINB 4
+#endif
+
+// Advection of u at collapsed face ii from global loads (the periodic wrap face).
 __device__ __forceinline__ double u_adv_global(const Grid &g, const StateR &s, const double *ru, const double *rv,
                                                const double *rom, int k, int j, int ii) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1;
@@ -42,7 +47,7 @@ __device__ __forceinline__ double u_adv_global(const Grid &g, const StateR &s, c
   return tend + (-ld(g.rdnw, k)) * (v1 - v0);
 }
 
-// Advection of v at collapsed face jj (global loads), as in k_vface.
+// Advection of v at collapsed face jj from global loads (the periodic wrap face).
 __device__ __forceinline__ double v_adv_global(const Grid &g, const StateR &s, const double *ru, const double *rv,
                                                const double *rom, int k, int jj, int i) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nyv = ny + 1;
@@ -67,13 +72,13 @@ __device__ __forceinline__ double v_adv_global(const Grid &g, const StateR &s, c
   auto q = [&](int kk) { return ld(s.v, ix3(kk, jj, i, nyv, nx)); };
   const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
   const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
-  return tend + (msfvy_c / msfvx_c) * ((-ld(g.rdnw, k)) * (v1 - v0));
+  return tend + div_rcp(msfvy_c, msfvx_c, ld(g.rmsfvx, ix2(jj, i, nx))) * ((-ld(g.rdnw, k)) * (v1 - v0));
 }
 
 // ---------------------------------------------------------------------------
 // u faces, tiled advection.  Grid over faces 0..nx.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TSX *TSY) k_uface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+__global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muu, const double *muus,
                                                            const double *base_u, int top_lid, int run_boundary,
@@ -141,7 +146,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_uface_tiled(Grid g, StateR s, Stat
     const double mt_l = (ld(s.mu_total, ix2(j, l, nx)) - mp_l) + mp_l;
     const double mt_r = (ld(s.mu_total, ix2(j, r, nx)) - mp_r) + mp_r;
     const double mass_u = c1 * (0.5 * (mt_l + mt_r)) + c2;
-    const double msf_u = ld(g.msfux, ix2(j, i, nxu)) / ld(g.msfuy, ix2(j, i, nxu));
+    const double msf_u = div_msf(ld(g.msfux, ix2(j, i, nxu)), g.msfuy, g.rmsfuy, ix2(j, i, nxu));
     double dpx = msf_u * 0.5 * g.rdx * mass_u * (ph_term + p_term + pb_term);
     auto ps = [&](int m) { return P(s.p_pert, m, l) + P(s.p_pert, m, r); };
     const double bracket = ld(g.rdnw, k) * (dpn_large(g, k + 1, top_lid, ps) - dpn_large(g, k, top_lid, ps)) -
@@ -156,7 +161,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_uface_tiled(Grid g, StateR s, Stat
     auto rvq = [&](int jv, int ic) {
       const int js = (jv == 0) ? 0 : jv - 1, jn = (jv == ny) ? ny - 1 : jv;
       const double muv_c = 0.5 * (mu2(js, ic) + mu2(jn, ic));
-      return ld(s.v, ix3(k, jv, ic, ny + 1, nx)) * (c1 * muv_c + c2) / ld(g.msfvx, ix2(jv, ic, nx));
+      return div_msf(ld(s.v, ix3(k, jv, ic, ny + 1, nx)) * (c1 * muv_c + c2), g.msfvx, g.rmsfvx, ix2(jv, ic, nx));
     };
     auto rwq = [&](int kf, int ic) {
       return ld(s.w, ix3(kf, j, ic, ny, nx)) * (ld(g.c1f, kf) * mu2(j, ic) + ld(g.c2f, kf)) /
@@ -165,7 +170,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_uface_tiled(Grid g, StateR s, Stat
     const double f_u = 0.5 * (ld(g.f, ix2(j, l, nx)) + ld(g.f, ix2(j, r, nx)));
     const double e_u = 0.5 * (ld(g.e, ix2(j, l, nx)) + ld(g.e, ix2(j, r, nx)));
     const double cosa_u = 0.5 * (ld(g.cosa, ix2(j, l, nx)) + ld(g.cosa, ix2(j, r, nx)));
-    const double msf_u = ld(g.msfux, ix2(j, i, nxu)) / ld(g.msfuy, ix2(j, i, nxu));
+    const double msf_u = div_msf(ld(g.msfux, ix2(j, i, nxu)), g.msfuy, g.rmsfuy, ix2(j, i, nxu));
     double ru_cor = 0.0;
     if (f_u != 0.0 || e_u != 0.0) {
       const double rv_quad = 0.25 * (rvq(j, l) + rvq(j, r) + rvq(j + 1, l) + rvq(j + 1, r));
@@ -185,13 +190,13 @@ __global__ void __launch_bounds__(TSX *TSY) k_uface_tiled(Grid g, StateR s, Stat
   const size_t f2 = ix2(j, i, nxu);
   const double mass_ref = c1 * ld(muus, f2) + c2;
   const double mass_cur = c1 * ld(muu, f2) + c2;
-  o.u_w[cu] = (mass_ref * ld(ref.u, cu) - mass_cur * ld(s.u, cu)) / ld(g.msfuy, f2);
+  o.u_w[cu] = div_msf(mass_ref * ld(ref.u, cu) - mass_cur * ld(s.u, cu), g.msfuy, g.rmsfuy, f2);
 }
 
 // ---------------------------------------------------------------------------
 // v faces, tiled advection.  Grid over faces 0..ny.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TSX *TSY) k_vface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+__global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muv, const double *muvs,
                                                            const double *base_v, int top_lid, int run_boundary,
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_vface_tiled(Grid g, StateR s, Stat
     auto q = [&](int kk) { return ld(s.v, ix3(kk, j, i, nyv, nx)); };
     const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
     const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
-    tend = tend + (msfvy_c / msfvx_c) * ((-ld(g.rdnw, k)) * (v1 - v0));
+    tend = tend + div_rcp(msfvy_c, msfvx_c, ld(g.rmsfvx, ix2(j, i, nx))) * ((-ld(g.rdnw, k)) * (v1 - v0));
   } else {
     tend = v_adv_global(g, s, ru, rv, rom, k, 0, i);
   }
@@ -258,7 +263,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_vface_tiled(Grid g, StateR s, Stat
     const double mt_s = (ld(s.mu_total, ix2(sj, i, nx)) - mp_s) + mp_s;
     const double mt_n = (ld(s.mu_total, ix2(nj, i, nx)) - mp_n) + mp_n;
     const double mass_v = c1 * (0.5 * (mt_s + mt_n)) + c2;
-    const double msf_v = ld(g.msfvy, ix2(j, i, nx)) / ld(g.msfvx, ix2(j, i, nx));
+    const double msf_v = div_msf(ld(g.msfvy, ix2(j, i, nx)), g.msfvx, g.rmsfvx, ix2(j, i, nx));
     double dpy = msf_v * 0.5 * g.rdy * mass_v * (ph_term + p_term + pb_term);
     auto ps = [&](int m) { return P(s.p_pert, m, sj) + P(s.p_pert, m, nj); };
     const double bracket = ld(g.rdnw, k) * (dpn_large(g, k + 1, top_lid, ps) - dpn_large(g, k, top_lid, ps)) -
@@ -273,7 +278,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_vface_tiled(Grid g, StateR s, Stat
     auto ruq = [&](int jc, int iu) {
       const int il = (iu == 0) ? 0 : iu - 1, ir = (iu == nx) ? nx - 1 : iu;
       const double muu_c = 0.5 * (mu2(jc, il) + mu2(jc, ir));
-      return ld(s.u, ix3(k, jc, iu, ny, nx + 1)) * (c1 * muu_c + c2) / ld(g.msfuy, ix2(jc, iu, nx + 1));
+      return div_msf(ld(s.u, ix3(k, jc, iu, ny, nx + 1)) * (c1 * muu_c + c2), g.msfuy, g.rmsfuy, ix2(jc, iu, nx + 1));
     };
     auto rwq = [&](int kf, int jc) {
       return ld(s.w, ix3(kf, jc, i, ny, nx)) * (ld(g.c1f, kf) * mu2(jc, i) + ld(g.c2f, kf)) /
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_vface_tiled(Grid g, StateR s, Stat
     const double f_v = 0.5 * (ld(g.f, ix2(sj, i, nx)) + ld(g.f, ix2(nj, i, nx)));
     const double e_v = 0.5 * (ld(g.e, ix2(sj, i, nx)) + ld(g.e, ix2(nj, i, nx)));
     const double sina_v = 0.5 * (ld(g.sina, ix2(sj, i, nx)) + ld(g.sina, ix2(nj, i, nx)));
-    const double msf_v = ld(g.msfvy, ix2(j, i, nx)) / ld(g.msfvx, ix2(j, i, nx));
+    const double msf_v = div_msf(ld(g.msfvy, ix2(j, i, nx)), g.msfvx, g.rmsfvx, ix2(j, i, nx));
     double rv_cor;
     if (f_v != 0.0 || e_v != 0.0) {
       const double ru_quad = 0.25 * (ruq(sj, i) + ruq(sj, i + 1) + ruq(nj, i) + ruq(nj, i + 1));
@@ -300,13 +305,13 @@ __global__ void __launch_bounds__(TSX *TSY) k_vface_tiled(Grid g, StateR s, Stat
   const size_t f2 = ix2(j, i, nx);
   const double mass_ref = c1 * ld(muvs, f2) + c2;
   const double mass_cur = c1 * ld(muv, f2) + c2;
-  o.v_w[cv] = (mass_ref * ld(ref.v, cv) - mass_cur * ld(s.v, cv)) / ld(g.msfvx, f2);
+  o.v_w[cv] = div_msf(mass_ref * ld(ref.v, cv) - mass_cur * ld(s.v, cv), g.msfvx, g.rmsfvx, f2);
 }
 
 // ---------------------------------------------------------------------------
 // w faces, tiled: w advection and rhs_ph horizontal stencils from tiles.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TSX *TSY) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+__global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom,
                                                            const double *ww_stage, const double *qtot,
                                                            const double *mub, const double *mut, const double *muts0,
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_wface_tiled(Grid g, StateR s, Stat
   }
   const double mub_c = ld(mub, c2d), mut_c = ld(mut, c2d);
   const double mu_prime = mut_c - mub_c;
-  const double minv = 1.0 / ld(g.msfty, c2d);
+  const double minv = ld(g.rmsfty, c2d);  // == 1.0 / msfty
   auto Pp = [&](int kk) { return ld(s.p_pert, ix3(kk, j, i, ny, nx)); };
   auto Qt = [&](int kk) { return ld(qtot, ix3(kk, j, i, ny, nx)); };
   double rw = 0.0, cqw = 0.0;
@@ -434,12 +439,16 @@ __global__ void __launch_bounds__(TSX *TSY) k_wface_tiled(Grid g, StateR s, Stat
     const double muv_j = ld(muv, ix2(j, i, nx)), muv_jp = ld(muv, ix2(j + 1, i, nx));
     const double fuy_i = ld(g.msfuy, ix2(j, i, nx + 1)), fuy_ip = ld(g.msfuy, ix2(j, i + 1, nx + 1));
     const double fvx_j = ld(g.msfvx, ix2(j, i, nx)), fvx_jp = ld(g.msfvx, ix2(j + 1, i, nx));
+    const double rfuy_i = ld(g.rmsfuy, ix2(j, i, nx + 1)), rfuy_ip = ld(g.rmsfuy, ix2(j, i + 1, nx + 1));
+    const double rfvx_j = ld(g.rmsfvx, ix2(j, i, nx)), rfvx_jp = ld(g.rmsfvx, ix2(j + 1, i, nx));
     auto lev = [&](int kk, double &ru_m, double &u_m, double &rv_m, double &v_m) {
       const double c1 = ld(g.c1h, kk), c2 = ld(g.c2h, kk);
       const double u0 = ld(s.u, ix3(kk, j, i, ny, nx + 1)), u1 = ld(s.u, ix3(kk, j, i + 1, ny, nx + 1));
       const double v0 = ld(s.v, ix3(kk, j, i, ny + 1, nx)), v1 = ld(s.v, ix3(kk, j + 1, i, ny + 1, nx));
-      const double rs0 = (c1 * muu_i + c2) * u0 / fuy_i, rs1 = (c1 * muu_ip + c2) * u1 / fuy_ip;
-      const double vs0 = (c1 * muv_j + c2) * v0 / fvx_j, vs1 = (c1 * muv_jp + c2) * v1 / fvx_jp;
+      const double rs0 = div_rcp((c1 * muu_i + c2) * u0, fuy_i, rfuy_i);
+      const double rs1 = div_rcp((c1 * muu_ip + c2) * u1, fuy_ip, rfuy_ip);
+      const double vs0 = div_rcp((c1 * muv_j + c2) * v0, fvx_j, rfvx_j);
+      const double vs1 = div_rcp((c1 * muv_jp + c2) * v1, fvx_jp, rfvx_jp);
       ru_m = 0.5 * (rs0 + rs1);
       u_m = 0.5 * (u0 + u1);
       rv_m = 0.5 * (vs0 + vs1);
@@ -451,7 +460,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_wface_tiled(Grid g, StateR s, Stat
     const double fm = ld(g.fnm, k), fp = ld(g.fnp, k);
     const double ru_f = fm * ru_a + fp * ru_b, u_f = fm * u_a + fp * u_b;
     const double rv_f = fm * rv_a + fp * rv_b, v_f = fm * v_a + fp * v_b;
-    const double mxy = ld(g.msftx, c2d) / ld(g.msfty, c2d);
+    const double mxy = div_msf(ld(g.msftx, c2d), g.msfty, g.rmsfty, c2d);
     const double cor = ld(g.e, c2d) * (ld(g.cosa, c2d) * ru_f - mxy * ld(g.sina, c2d) * rv_f);
     const double curv = W_RERADIUS * (ru_f * u_f + mxy * rv_f * v_f);
     rw = rw + (cor + curv);
@@ -497,7 +506,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_wface_tiled(Grid g, StateR s, Stat
   }
   const double mass_f_ref = ld(g.c1f, k) * ld(muts0, c2d) + ld(g.c2f, k);
   const double mass_f_cur = ld(g.c1f, k) * mut_c + ld(g.c2f, k);
-  o.w_w[cw] = (mass_f_ref * ld(ref.w, cw) - mass_f_cur * ld(s.w, cw)) / ld(g.msfty, c2d);
+  o.w_w[cw] = div_msf(mass_f_ref * ld(ref.w, cw) - mass_f_cur * ld(s.w, cw), g.msfty, g.rmsfty, c2d);
   const double php = ld(s.ph_pert, cw);
   o.ph_w[cw] = ld(ref.ph_pert, cw) - php;
   o.pt1[cw] = ld(ref.ph_pert, cw) + (ld(s.ph_total, cw) - php);
@@ -527,6 +536,7 @@ __global__ void __launch_bounds__(256) k_transport_tiled(Grid g, const double *u
   double mu_c = 0, muu_i = 0, muu_ip = 0, muv_j = 0, muv_jp = 0, msfuy_i = 1, msfuy_ip = 1, msfvx_j = 1, msfvx_jp = 1,
          msftx = 1;
   double muu_s_i = 0, muu_s_ip = 0, muv_s_j = 0, muv_s_jp = 0, fuy_ip = 1, fvx_jp = 1;
+  double rmsfuy_i = 1, rmsfuy_ip = 1, rmsfvx_j = 1, rmsfvx_jp = 1, rfuy_ip = 1, rfvx_jp = 1;
   if (valid) {
     ip = wrp(i + 1, nx); im = wrp(i - 1, nx); jp = wrp(j + 1, ny); jm = wrp(j - 1, ny);
     mu_c = ld(mu_total, ix2(j, i, nx));
@@ -536,6 +546,8 @@ __global__ void __launch_bounds__(256) k_transport_tiled(Grid g, const double *u
     muv_jp = 0.5 * (ld(mu_total, ix2(jp, i, nx)) + mu_c);
     msfuy_i = ld(g.msfuy, ix2(j, i, nx + 1)); msfuy_ip = ld(g.msfuy, ix2(j, ip, nx + 1));
     msfvx_j = ld(g.msfvx, ix2(j, i, nx)); msfvx_jp = ld(g.msfvx, ix2(jp, i, nx));
+    rmsfuy_i = ld(g.rmsfuy, ix2(j, i, nx + 1)); rmsfuy_ip = ld(g.rmsfuy, ix2(j, ip, nx + 1));
+    rmsfvx_j = ld(g.rmsfvx, ix2(j, i, nx)); rmsfvx_jp = ld(g.rmsfvx, ix2(jp, i, nx));
     msftx = ld(g.msftx, ix2(j, i, nx));
     if (ww_spec != nullptr) {
       const double mu_w = (i == 0) ? mu_c : ld(mu_total, ix2(j, i - 1, nx));
@@ -546,24 +558,26 @@ __global__ void __launch_bounds__(256) k_transport_tiled(Grid g, const double *u
       muv_s_jp = (j + 1 == ny) ? mu_c : 0.5 * (ld(mu_total, ix2(j + 1, i, nx)) + mu_c);
       fuy_ip = ld(g.msfuy, ix2(j, i + 1, nx + 1));
       fvx_jp = ld(g.msfvx, ix2(j + 1, i, nx));
+      rfuy_ip = ld(g.rmsfuy, ix2(j, i + 1, nx + 1));
+      rfvx_jp = ld(g.rmsfvx, ix2(j + 1, i, nx));
     }
   }
   if (valid) {
     for (int k = ty; k < nz; k += 8) {
       const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
       const double u_i = ld(u, ix3(k, j, i, ny, nx + 1)), v_j = ld(v, ix3(k, j, i, ny + 1, nx));
-      const double ru_i = (c1 * muu_i + c2) * u_i / msfuy_i;
-      const double ru_ip = (c1 * muu_ip + c2) * ld(u, ix3(k, j, ip, ny, nx + 1)) / msfuy_ip;
-      const double rv_j = (c1 * muv_j + c2) * v_j / msfvx_j;
-      const double rv_jp = (c1 * muv_jp + c2) * ld(v, ix3(k, jp, i, ny + 1, nx)) / msfvx_jp;
+      const double ru_i = div_rcp((c1 * muu_i + c2) * u_i, msfuy_i, rmsfuy_i);
+      const double ru_ip = div_rcp((c1 * muu_ip + c2) * ld(u, ix3(k, j, ip, ny, nx + 1)), msfuy_ip, rmsfuy_ip);
+      const double rv_j = div_rcp((c1 * muv_j + c2) * v_j, msfvx_j, rmsfvx_j);
+      const double rv_jp = div_rcp((c1 * muv_jp + c2) * ld(v, ix3(k, jp, i, ny + 1, nx)), msfvx_jp, rmsfvx_jp);
       D0(k) = ld(g.dnw, k) * msftx * (g.rdx * (ru_ip - ru_i) + g.rdy * (rv_jp - rv_j));
       ru[ix3(k, j, i, ny, nx)] = ru_i;
       rv[ix3(k, j, i, ny, nx)] = rv_j;
       if (ww_spec != nullptr) {
-        const double a0 = (c1 * muu_s_i + c2) * u_i / msfuy_i;
-        const double a1 = (c1 * muu_s_ip + c2) * ld(u, ix3(k, j, i + 1, ny, nx + 1)) / fuy_ip;
-        const double b0 = (c1 * muv_s_j + c2) * v_j / msfvx_j;
-        const double b1 = (c1 * muv_s_jp + c2) * ld(v, ix3(k, j + 1, i, ny + 1, nx)) / fvx_jp;
+        const double a0 = div_rcp((c1 * muu_s_i + c2) * u_i, msfuy_i, rmsfuy_i);
+        const double a1 = div_rcp((c1 * muu_s_ip + c2) * ld(u, ix3(k, j, i + 1, ny, nx + 1)), fuy_ip, rfuy_ip);
+        const double b0 = div_rcp((c1 * muv_s_j + c2) * v_j, msfvx_j, rmsfvx_j);
+        const double b1 = div_rcp((c1 * muv_s_jp + c2) * ld(v, ix3(k, j + 1, i, ny + 1, nx)), fvx_jp, rfvx_jp);
         D1(k) = msftx * ld(g.dnw, k) * (g.rdx * (a1 - a0) + g.rdy * (b1 - b0));
       }
     }

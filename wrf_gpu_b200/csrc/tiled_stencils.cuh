@@ -4,9 +4,8 @@
 // staged once per block as a (8 + 2*HY) x (32 + 2*HX) plane tile, with the
 // periodic wrap of the reference's jnp.roll applied once per staged element;
 // the flux stencils then read shared memory with fixed offsets.  Vertical
-// stencils read global memory at the thread's own column.  The arithmetic is
-// the same expression sequence as the untiled kernels (operation order of the
-// reference), so results are bit-identical to them.
+// stencils read global memory at the thread's own column.  The arithmetic
+// keeps the reference's expression order.
 #pragma once
 #include "dycore_common.cuh"
 #include "stage_kernels.cuh"
@@ -172,8 +171,9 @@ __device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int 
   }
 }
 
-// The 12 face fluxes of cell (k, j, i) from the staged tiles (same algebra as
-// cell_fluxes in stage_kernels.cuh).
+// The 12 face fluxes of cell (k, j, i) from the staged tiles: low-order
+// upwind (flux_advection.py:614-675) and antidiffusive = high order
+// (:678-711) minus low order, at the cell's two x, y and z faces.
 __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int j,
                                                   int i, const double *field, const double *field_old,
                                                   CellFluxes &cf) {
