@@ -27,9 +27,69 @@ namespace wg {
 #ifndef WG_COL_MINB
 #define WG_COL_MINB 2
 #endif
+// L2 prefetch of the block's input rows: 0 off, 1 all at block start, 2 in
+// two groups (advance_mu_t inputs at start, advance_w inputs after P4).
+#ifndef WG_COL_PREFETCH
+#define WG_COL_PREFETCH 2
+#endif
 constexpr int COL_TX = WG_COL_TX;
 constexpr int COL_TY = WG_COL_TY;
 constexpr int COL_NARR = 7;
+static_assert(COL_TY >= 2, "the Thomas phase needs a second warp row to stage gamma");
+
+// Bulk L2 prefetch of the rows (levels 0..nz) this column block will read.
+// group 0: advance_mu_t / theta / t_2ave inputs; group 1: advance_w and
+// calc_p_rho inputs.
+__device__ __forceinline__ void column_prefetch(const Grid &g, const Acoustic &A, const ColArgs &c, int group, int i0,
+                                                int j) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz, L = nz + 1;
+  const int wm = min(COL_TX, nx - i0), wu = min(COL_TX + 1, nx + 1 - i0);
+  const int jm = (j == 0) ? (c.specified ? 0 : ny - 1) : j - 1;
+  const int jp = (j == ny - 1) ? (c.specified ? ny - 1 : 0) : j + 1;
+  const int nrows = (group == 0) ? 17 : 10;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int e = tid; e < nrows * L; e += blockDim.x * blockDim.y) {
+    const int r = e / L, k = e - r * L;
+    const double *p = nullptr;
+    int w = wm;
+    const bool mass = k < nz;
+    if (group == 0) {
+      switch (r) {
+        case 0: if (mass) { p = A.u + ix3(k, j, i0, ny, nx + 1); w = wu; } break;
+        case 1: if (mass) { p = A.u_1 + ix3(k, j, i0, ny, nx + 1); w = wu; } break;
+        case 2: if (mass) p = A.v + ix3(k, j, i0, ny + 1, nx); break;
+        case 3: if (mass) p = A.v + ix3(k, j + 1, i0, ny + 1, nx); break;
+        case 4: if (mass) p = A.v_1 + ix3(k, j, i0, ny + 1, nx); break;
+        case 5: if (mass) p = A.v_1 + ix3(k, j + 1, i0, ny + 1, nx); break;
+        case 6: p = A.ww_1 + ix3(k, j, i0, ny, nx); break;
+        case 7: p = A.ww + ix3(k, j, i0, ny, nx); break;
+        case 8: if (mass) p = A.theta_w + ix3(k, j, i0, ny, nx); break;
+        case 9: if (mass) p = A.t2ave + ix3(k, j, i0, ny, nx); break;
+        case 10: if (mass) p = A.t_tend + ix3(k, j, i0, ny, nx); break;
+        case 11: if (mass) p = A.theta_s + ix3(k, j, i0, ny, nx); break;
+        case 12: if (mass) p = A.theta_s + ix3(k, jm, i0, ny, nx); break;
+        case 13: if (mass) p = A.theta_s + ix3(k, jp, i0, ny, nx); break;
+        case 14: if (mass) p = A.c2a + ix3(k, j, i0, ny, nx); break;
+        case 15: if (mass) p = A.alt + ix3(k, j, i0, ny, nx); break;
+        default: p = A.pt1 + ix3(k, j, i0, ny, nx); break;
+      }
+    } else {
+      switch (r) {
+        case 0: p = A.ph + ix3(k, j, i0, ny, nx); break;
+        case 1: p = A.ph_tend + ix3(k, j, i0, ny, nx); break;
+        case 2: p = A.w + ix3(k, j, i0, ny, nx); break;
+        case 3: p = A.rw_tend + ix3(k, j, i0, ny, nx); break;
+        case 4: p = A.cqw + ix3(k, j, i0, ny, nx); break;
+        case 5: p = A.a + ix3(k, j, i0, ny, nx); break;
+        case 6: p = A.alpha + ix3(k, j, i0, ny, nx); break;
+        case 7: p = A.gamma + ix3(k, j, i0, ny, nx); break;
+        case 8: if (c.damp_opt == 3) p = A.w_save + ix3(k, j, i0, ny, nx); break;
+        default: if (mass) p = A.pm1 + ix3(k, j, i0, ny, nx); break;
+      }
+    }
+    if (p != nullptr) l2_prefetch_row(p, w);
+  }
+}
 
 inline size_t column_tiled_smem_bytes(int nz) { return (size_t)COL_NARR * (nz + 1) * COL_TX * sizeof(double); }
 
@@ -57,6 +117,15 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   const int nxu = nx + 1, nyv = ny + 1;
 
   __shared__ double s_dmdt[COL_TX], s_mutend[COL_TX], s_scale[COL_TX];
+  // 2-D inputs of the serial phases, loaded early so their latency overlaps P1
+  double muts_in = 0.0, mu_in = 0.0, mu_tend_in = 0.0;
+  if (ty == 0 && active) {
+    muts_in = A.muts[c2d];
+    mu_in = A.mu[c2d];
+    mu_tend_in = (A.mu_tend != nullptr) ? ld(A.mu_tend, c2d) : 0.0;
+  }
+  if (WG_COL_PREFETCH >= 1) column_prefetch(g, A, c, 0, blockIdx.x * COL_TX, j);
+  if (WG_COL_PREFETCH == 1) column_prefetch(g, A, c, 1, blockIdx.x * COL_TX, j);
 
   // ---------------- P1: dvdxi per level -> A0 ----------------
   if (active) {
@@ -82,9 +151,9 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
       const double t = ld(g.dnw, k) * S(A0, k);
       dmdt = (k == 0) ? t : dmdt + t;
     }
-    const double mu_work_old = A.muts[c2d] - mut;
-    const double mu_save = A.mu[c2d] - mu_work_old;
-    double mu_tend = (A.mu_tend != nullptr) ? ld(A.mu_tend, c2d) : 0.0;
+    const double mu_work_old = muts_in - mut;
+    const double mu_save = mu_in - mu_work_old;
+    double mu_tend = mu_tend_in;
     double mu_tendency = dmdt + mu_tend;
     double scale = 1.0;
     if (c.specified) {
@@ -111,6 +180,11 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   }
   __syncthreads();
   // ---------------- P3: ww increments -> A1, ww_1 -> A2, old ww (inactive) -> A3 ----------------
+  double ww_bot = 0.0, ww_top = 0.0;  // old ww at faces 0 and nz, for P4
+  if (ty == 0 && active) {
+    ww_bot = A.ww[M(0)];
+    ww_top = A.ww[M(nz)];
+  }
   if (valid) {
     if (active) {
       const double dmdt = s_dmdt[tx], mu_tend = s_mutend[tx], scale = s_scale[tx];
@@ -128,16 +202,17 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   __syncthreads();
   // ---------------- P4: ww prefix (serial) -> A3 ----------------
   if (ty == 0 && active) {
-    double prev = A.ww[M(0)];
+    double prev = ww_bot;
     S(A3, 0) = prev - S(A2, 0);
     for (int kk = 1; kk < nz; ++kk) {
       const double cur = prev - S(A1, kk);
       S(A3, kk) = cur - S(A2, kk);
       prev = cur;
     }
-    S(A3, nz) = A.ww[M(nz)];
+    S(A3, nz) = ww_top;
   }
   __syncthreads();
+  if (WG_COL_PREFETCH == 2) column_prefetch(g, A, c, 1, blockIdx.x * COL_TX, j);
   // ---------------- P5: theta update, t_2ave, wd -> A0, buoy -> A1, coef -> A5 ----------------
   const double muts = valid ? A.muts[c2d] : 1.0;
   const double muave = valid ? A.muave[c2d] : 0.0;
@@ -151,6 +226,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
     }
     for (int k = ty; k < nz; k += COL_TY) {
       double thw = A.theta_w[M(k)];
+      const double t2ave_old = A.t2ave[M(k)];
       if (active) {
         const double wdtn_hi = (k + 1 <= nz - 1)
                                    ? S(A3, k + 1) * (ld(g.fnm, k + 1) * T1(k + 1, j, i) + ld(g.fnp, k + 1) * T1(k, j, i))
@@ -165,7 +241,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
         A.theta_w[M(k)] = thw;
       }
       const double mass_h = ld(g.c1h, k) * muts + ld(g.c2h, k);
-      const double half = 0.5 * (eps_p * thw + eps_m * A.t2ave[M(k)]);
+      const double half = 0.5 * (eps_p * thw + eps_m * t2ave_old);
       const double t2a = (half + (ld(g.c1h, k) * muave) * T0) / (mass_h * (T0 + T1(k, j, i)));
       A.t2ave[M(k)] = t2a;
       const double c2a_k = ld(A.c2a, M(k));
@@ -180,13 +256,13 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   const double c05gem = 0.5 * G * eps_m;
   if (valid) {
     for (int f = ty; f <= nz; f += COL_TY) {
-      const double phf = A.ph[M(f)];
+      const double phf = ld(A.ph, M(f));
       S(A4, f) = phf;
       if (f == 0) {
         S(A2, 0) = 0.0;
         continue;
       }
-      double r = dts * (ld(A.ph_tend, M(f)) + c05gem * A.w[M(f)]);
+      double r = dts * (ld(A.ph_tend, M(f)) + c05gem * ld(A.w, M(f)));
       if (f < nz) r = r + (-(dts * (ld(g.fnm, f) * S(A0, f) + ld(g.fnp, f) * S(A0, f - 1))));
       const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
       r = phf + msfty * r / mf;
@@ -200,6 +276,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
     const double c05dg = 0.5 * dts * G;
     const double dtsg = dts * G;
     for (int f = ty; f <= nz; f += COL_TY) {
+      const double a_f = ld(A.a, M(f)), alpha_f = ld(A.alpha, M(f));
       double wn;
       if (f == 0) {
         auto HT = [&](int jj, int ii2) {
@@ -221,7 +298,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
         wn = msfty * 0.5 * g.rdy * (dy_n * vcf(j + 1) + dy_s * vcf(j)) +
              msftx * 0.5 * g.rdx * (dx_e * ucf(i + 1) + dx_w * ucf(i));
       } else if (f < nz) {
-        const double w_old = A.w[M(f)];
+        const double w_old = ld(A.w, M(f));
         double rw = ld(A.rw_tend, M(f));
         if (c.w_damping == 1) {
           const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
@@ -245,29 +322,31 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
         const double tA_top = -0.5 * dts * G / mhm * (rdnw_t * rdnw_t) * 2.0 * ld(A.c2a, M(km1)) *
                               (eps_p * (S(A2, nz) - S(A2, nz - 1)) + eps_m * (S(A4, nz) - S(A4, nz - 1)));
         const double tB_top = -dts * G * (2.0 * rdnw_t * ld(A.c2a, M(km1)) * ld(A.alt, M(km1)) * t2a_t + (ld(g.c1f, nz) * muave));
-        const double w_top = A.w[M(nz)] + dts * ld(A.rw_tend, M(nz)) + minv * (tA_top + tB_top);
+        const double w_top = ld(A.w, M(nz)) + dts * ld(A.rw_tend, M(nz)) + minv * (tA_top + tB_top);
         wn = c.top_lid ? 0.0 : w_top;
       }
       S(A6, f) = wn;
+      S(A0, f) = a_f;      // wd(f) was last read in P6
+      S(A3, f) = alpha_f;  // ww(f) was last read above, by this thread
     }
   }
   __syncthreads();
-  if (valid) {
-    for (int f = ty; f <= nz; f += COL_TY) {
-      S(A0, f) = ld(A.a, M(f));
-      S(A3, f) = ld(A.alpha, M(f));
-      S(A5, f) = ld(A.gamma, M(f));
+  // ---------------- P8: Thomas forward (serial) while the other warps stage gamma -> A5 ----------------
+  if (ty == 0) {
+    if (valid) {
+      double wf_prev = S(A6, 0);
+      for (int f = 1; f <= nz; ++f) {
+        const double wf = (S(A6, f) - S(A0, f) * wf_prev) * S(A3, f);
+        S(A6, f) = wf;
+        wf_prev = wf;
+      }
     }
+  } else if (valid) {
+    for (int f = ty - 1; f <= nz; f += COL_TY - 1) S(A5, f) = ld(A.gamma, M(f));
   }
   __syncthreads();
-  // ---------------- P8: Thomas forward + back substitution (serial) ----------------
+  // ---------------- P8b: Thomas back substitution (serial) ----------------
   if (ty == 0 && valid) {
-    double wf_prev = S(A6, 0);
-    for (int f = 1; f <= nz; ++f) {
-      const double wf = (S(A6, f) - S(A0, f) * wf_prev) * S(A3, f);
-      S(A6, f) = wf;
-      wf_prev = wf;
-    }
     double ws_next = S(A6, nz);
     for (int f = nz - 1; f >= 1; --f) {
       const double ws = S(A6, f) - S(A5, f) * ws_next;
@@ -317,7 +396,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
       const double ttr = T0 + t1;
       const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
       const double pp = ld(A.c2a, M(k)) * (altc * (A.theta_w[M(k)] - mu_term * t1) / (safe * sttr) - al);
-      const double pm1 = A.pm1[M(k)];
+      const double pm1 = ld(A.pm1, M(k));
       A.p[M(k)] = pp + SMDIV * (pp - pm1);
       A.pm1[M(k)] = pp;
       A.al[M(k)] = al;

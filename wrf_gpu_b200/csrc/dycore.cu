@@ -20,6 +20,7 @@
 #include "column_tiled.cuh"
 #include "tiled_stencils.cuh"
 #include "tiled_faces.cuh"
+#include "tiled_march.cuh"
 
 using namespace wg;
 
@@ -559,9 +560,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     mo.theta_w = w.theta_w;
     for (int q = 0; q < 6; ++q) mo.q_tend[q] = w.qtend[q];
     PROF("k_mass");
-    k_scalar_adv_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0,
-                                                                in->base_theta, lim_theta ? 0 : 1,
-                                                                (moist && !lim_moist) ? 1 : 0, mo);
+    {
+      const int nfields = 1 + ((moist && !lim_moist) ? 6 : 0);
+      const int nchunk = march_nchunk(nz);
+      k_scalar_adv_march<<<tgrd(nx, ny, nfields * nchunk), tblk(), 0, stream>>>(
+          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, mo);
+    }
     LAUNCH_CHECK("k_mass");
     if (lim_theta || lim_moist) {
       LimArgs la;
@@ -571,11 +575,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
         PROF("k_lim_scale");
-        k_lim_scale_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2);
+        k_lim_march<false><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+            g, la, s.theta, origin.theta, w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
-        k_lim_tend_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1, w.s2,
-                                                                   in->base_theta, s.mu_total, w.t_tend);
+        k_lim_march<true><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+            g, la, s.theta, origin.theta, nullptr, nullptr, w.s1, w.s2, in->base_theta, s.mu_total, w.t_tend);
         LAUNCH_CHECK("k_lim_tend");
       }
       if (lim_moist) {
@@ -583,11 +588,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.offset = 0.0;
         for (int q = 0; q < 6; ++q) {
           PROF("k_lim_scale");
-          k_lim_scale_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2);
+          k_lim_march<false><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+              g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
           LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
-          k_lim_tend_tiled<<<tgrd(nx, ny, nz), tblk(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr,
-                                                                     s.mu_total, w.qtend[q]);
+          k_lim_march<true><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+              g, la, s.q[q], origin.q[q], nullptr, nullptr, w.s1, w.s2, nullptr, s.mu_total, w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
         }
       }

@@ -124,6 +124,16 @@ __device__ __forceinline__ double pressure_from_theta_alt(double theta, double a
   return P0 * pow(dmax(argument, 1.0e-12), CPOVCV);
 }
 
+// Hint: pull the row of n doubles starting at p into L2 with one bulk
+// prefetch (cp.async.bulk.prefetch.L2).  Only the 16-byte-aligned part that
+// lies strictly inside the row is named, so nothing outside it is touched.
+__device__ __forceinline__ void l2_prefetch_row(const double *p, int n) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uintptr_t lo = (a + 15) & ~uintptr_t(15);
+  const uintptr_t hi = (a + (uintptr_t)n * sizeof(double)) & ~uintptr_t(15);
+  if (hi > lo) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
+}
+
 __device__ __forceinline__ double safe12(double x) { return fabs(x) > 1.0e-12 ? x : 1.0e-12; }
 
 }  // namespace wg

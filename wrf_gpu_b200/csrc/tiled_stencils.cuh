@@ -144,14 +144,20 @@ struct LimTiles {
   double *rv;   // Tile<0,1>
   double *mt;   // Tile<1,1>: current total dry mass (2-D)
   const struct ZConst *zc;  // the level's two faces: dz, 1/dz, dz/dt
+  // low-order and antidiffusive fluxes of the tile's x faces (TSY rows of
+  // TSX+1 faces) and y faces (TSY+1 rows of TSX faces), each computed once
+  double *fxl, *fxa, *fyl, *fya;
 };
+
+constexpr int LIM_NXF = TSY * (TSX + 1);
+constexpr int LIM_NYF = (TSY + 1) * TSX;
 
 __device__ __forceinline__ void lim_stage_tiles(const Grid &g, const LimArgs &a, const double *field,
                                                 const double *field_old, int i0, int j0, int k, LimTiles &t) {
   const int nx = g.nx, ny = g.ny;
   const size_t plane = (size_t)k * ny * nx;
-  load_tile<3, 3>(t.q, field + plane, nx, i0, j0, nx, ny, a.offset);
-  load_tile<1, 1>(t.qo, field_old + plane, nx, i0, j0, nx, ny, a.offset);
+  load_tile<3, 3>(t.q, field + plane, nx, i0, j0, nx, ny, 0.0);  // raw; the offset is taken at use
+  load_tile<1, 1>(t.qo, field_old + plane, nx, i0, j0, nx, ny, 0.0);
   load_tile<1, 0>(t.ru, a.ru + plane, nx, i0, j0, nx, ny, 0.0);
   load_tile<0, 1>(t.rv, a.rv + plane, nx, i0, j0, nx, ny, 0.0);
   load_tile<1, 1>(t.mt, a.mut, nx, i0, j0, nx, ny, 0.0);
@@ -171,21 +177,18 @@ __device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int 
   }
 }
 
-// The 12 face fluxes of cell (k, j, i) from the staged tiles: low-order
-// upwind (flux_advection.py:614-675) and antidiffusive = high order
-// (:678-711) minus low order, at the cell's two x, y and z faces.
-__device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int j,
-                                                  int i, const double *field, const double *field_old,
-                                                  CellFluxes &cf) {
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int tx = threadIdx.x, ty = threadIdx.y;
+// Low-order upwind (flux_advection.py:614-675) and antidiffusive (high
+// order :678-711 minus low order) fluxes of every x and y face of the tile,
+// one face per thread item, into shared memory.  Edge tiles compute a few
+// harmless extra faces from the periodically wrapped staged values.
+__device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a, const LimTiles &t, int k) {
   using TQ = Tile<3, 3>;
   using TO = Tile<1, 1>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
   const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-  auto Q = [&](int r, int cc) { return t.q[(r + 3) * TQ::W + (cc + 3)]; };
-  auto QO = [&](int r, int cc) { return t.qo[(r + 1) * TO::W + (cc + 1)]; };
+  auto Q = [&](int r, int cc) { return t.q[(r + 3) * TQ::W + (cc + 3)] - a.offset; };
+  auto QO = [&](int r, int cc) { return t.qo[(r + 1) * TO::W + (cc + 1)] - a.offset; };
   auto MT = [&](int r, int cc) { return t.mt[(r + 1) * TO::W + (cc + 1)]; };
   // cr = vel*dt/dxy/mu_face and mu_face*(dxy/dt)*(...) with the constant
   // divisions done by div_rcp / per-launch constants (same bits).
@@ -194,22 +197,42 @@ __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &
     double ab = fabs(cr);
     return mu_face * dxy_dt * (0.5 * dmin(1.0, cr + ab) * fo_m1 + 0.5 * dmax(-1.0, cr - ab) * fo_0);
   };
-  auto xf = [&](int m, double &lo, double &an) {
-    const double vel = t.ru[ty * TR::W + (m + 1)];
-    const double muu = 0.5 * (MT(ty, m) + MT(ty, m - 1));
-    const double mu_u = c1 * muu + c2;
-    lo = upw(QO(ty, m - 1), QO(ty, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
-    const double hi = vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
-    an = hi - lo;
-  };
-  auto yf = [&](int r, double &lo, double &an) {
-    const double vel = t.rv[(r + 1) * TV::W + tx];
-    const double muv = 0.5 * (MT(r, tx) + MT(r - 1, tx));
-    const double mu_v = c1 * muv + c2;
-    lo = upw(QO(r - 1, tx), QO(r, tx), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
-    const double hi = vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
-    an = hi - lo;
-  };
+  for (int e = threadIdx.y * TSX + threadIdx.x; e < LIM_NXF + LIM_NYF; e += TSX * TSY) {
+    if (e < LIM_NXF) {
+      const int r = e / (TSX + 1), m = e - r * (TSX + 1);  // x face at local column m of row r
+      const double vel = t.ru[r * TR::W + (m + 1)];
+      const double muu = 0.5 * (MT(r, m) + MT(r, m - 1));
+      const double mu_u = c1 * muu + c2;
+      const double lo = upw(QO(r, m - 1), QO(r, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
+      const double hi = vel * flux5(Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2), vel);
+      t.fxl[e] = lo;
+      t.fxa[e] = hi - lo;
+    } else {
+      const int e2 = e - LIM_NXF;
+      const int r = e2 / TSX, cc = e2 - r * TSX;  // y face at local row r of column cc
+      const double vel = t.rv[(r + 1) * TV::W + cc];
+      const double muv = 0.5 * (MT(r, cc) + MT(r - 1, cc));
+      const double mu_v = c1 * muv + c2;
+      const double lo = upw(QO(r - 1, cc), QO(r, cc), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
+      const double hi = vel * flux5(Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc), vel);
+      t.fyl[e2] = lo;
+      t.fya[e2] = hi - lo;
+    }
+  }
+}
+
+// The 12 face fluxes of cell (k, j, i) from the staged tiles: low-order
+// upwind (flux_advection.py:614-675) and antidiffusive = high order
+// (:678-711) minus low order, at the cell's two x, y and z faces.
+// With have_z0 the bottom-face z fluxes are taken from cf.lz0/cf.az0 (carried
+// up from the level below) instead of being recomputed.
+__device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int j,
+                                                  int i, const double *field, const double *field_old,
+                                                  CellFluxes &cf, bool have_z0 = false) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  using TO = Tile<1, 1>;
+  auto MT = [&](int r, int cc) { return t.mt[(r + 1) * TO::W + (cc + 1)]; };
   auto qf = [&](int kk) { return ld(field, ix3(kk, j, i, ny, nx)) - a.offset; };
   auto qo = [&](int kk) { return ld(field_old, ix3(kk, j, i, ny, nx)) - a.offset; };
   auto zf = [&](int m, double &lo, double &an) {
@@ -230,41 +253,24 @@ __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &
     const double hi = vflux3_at(g, m, romv, qf);
     an = hi - lo;
   };
-  xf(tx, cf.lx0, cf.ax0);
-  xf(tx + 1, cf.lx1, cf.ax1);
-  yf(ty, cf.ly0, cf.ay0);
-  yf(ty + 1, cf.ly1, cf.ay1);
-  zf(k, cf.lz0, cf.az0);
+  const int x0 = ty * (TSX + 1) + tx, y0 = ty * TSX + tx;
+  cf.lx0 = t.fxl[x0]; cf.ax0 = t.fxa[x0];
+  cf.lx1 = t.fxl[x0 + 1]; cf.ax1 = t.fxa[x0 + 1];
+  cf.ly0 = t.fyl[y0]; cf.ay0 = t.fya[y0];
+  cf.ly1 = t.fyl[y0 + TSX]; cf.ay1 = t.fya[y0 + TSX];
+  if (!have_z0) zf(k, cf.lz0, cf.az0);
   zf(k + 1, cf.lz1, cf.az1);
 }
 
-struct LimSmem {
-  double q[Tile<3, 3>::N];
-  double qo[Tile<1, 1>::N];
-  double ru[Tile<1, 0>::N];
-  double rv[Tile<0, 1>::N];
-  double mt[Tile<1, 1>::N];
-  double s1[Tile<1, 1>::N];
-  double s2[Tile<1, 1>::N];
-  ZConst zc[2];
-};
-
-__global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a, const double *field,
-                                                               const double *field_old, double *s1, double *s2) {
-  __shared__ LimSmem sm;
+// Scale(s) of the PD (opt 1) / monotonic (opt 2) limiter at cell (k, j, i)
+// from its 12 face fluxes (flux_advection.py:736-935).
+__device__ __forceinline__ void lim_cell_scales(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int j,
+                                                int i, const double *field_old, const CellFluxes &cf, double &r1,
+                                                double &r2) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
-  const int i = i0 + tx, j = j0 + ty;
-  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc};
-  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
-  lim_zconst(g, a, k, sm.zc);
-  __syncthreads();
-  if (i >= nx || j >= ny) return;
-  CellFluxes cf;
-  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
   using TO = Tile<1, 1>;
-  auto QO = [&](int r, int cc) { return sm.qo[(r + 1) * TO::W + (cc + 1)]; };
+  auto QO = [&](int r, int cc) { return t.qo[(r + 1) * TO::W + (cc + 1)] - a.offset; };
   const double msftx = ld(g.msftx, ix2(j, i, nx));
   const double rdzw = ld(g.rdnw, k);
   const double mass_old = ld(g.c1h, k) * ld(a.mu_old, ix2(j, i, nx)) + ld(g.c2h, k);
@@ -276,7 +282,6 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a,
   auto neg = [](double x) { return dmin(0.0, x); };
   const double flux_out = a.dt * (msftx * msftx * (g.rdx * (pos(cf.ax1) - neg(cf.ax0)) + g.rdy * (pos(cf.ay1) - neg(cf.ay0))) +
                                   msftx * rdzw * (neg(cf.az1) - pos(cf.az0)));
-  double r1, r2;
   if (a.opt == 1) {
     r1 = (flux_out > ph_low) ? dmax(0.0, ph_low / (flux_out + PD_EPS)) : 1.0;
     r2 = r1;
@@ -298,33 +303,19 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a,
     r1 = (flux_in > ph_hi) ? dmax(0.0, ph_hi / (flux_in + PD_EPS)) : 1.0;
     r2 = (flux_out > ph_lo) ? dmax(0.0, ph_lo / (flux_out + PD_EPS)) : 1.0;
   }
-  const size_t c = ix3(k, j, i, ny, nx);
-  s1[c] = r1;
-  s2[c] = r2;
 }
 
-__global__ void __launch_bounds__(TSX *TSY) k_lim_tend_tiled(Grid g, LimArgs a, const double *field,
-                                                              const double *field_old, const double *s1,
-                                                              const double *s2, const double *base,
-                                                              const double *mu_total_stage, double *tend_out) {
-  __shared__ LimSmem sm;
+// Limited tendency at cell (k, j, i) (flux_advection.py:937-1000) from its
+// face fluxes and the scale tiles s1t/s2t of level k (s1k/s2k: the scale
+// arrays, for the levels above and below).
+__device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a, const double *s1t,
+                                                const double *s2t, int k, int j, int i, const double *s1,
+                                                const double *s2, const CellFluxes &cf) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
-  const int i = i0 + tx, j = j0 + ty;
-  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc};
-  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
-  lim_zconst(g, a, k, sm.zc);
-  const size_t plane = (size_t)k * ny * nx;
-  load_tile<1, 1>(sm.s1, s1 + plane, nx, i0, j0, nx, ny, 0.0);
-  load_tile<1, 1>(sm.s2, s2 + plane, nx, i0, j0, nx, ny, 0.0);
-  __syncthreads();
-  if (i >= nx || j >= ny) return;
-  CellFluxes cf;
-  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
   using TO = Tile<1, 1>;
-  auto S1 = [&](int r, int cc) { return sm.s1[(r + 1) * TO::W + (cc + 1)]; };
-  auto S2 = [&](int r, int cc) { return sm.s2[(r + 1) * TO::W + (cc + 1)]; };
+  auto S1 = [&](int r, int cc) { return s1t[(r + 1) * TO::W + (cc + 1)]; };
+  auto S2 = [&](int r, int cc) { return s2t[(r + 1) * TO::W + (cc + 1)]; };
   auto S1k = [&](int kk) { return ld(s1, ix3(kk, j, i, ny, nx)); };
   auto S2k = [&](int kk) { return ld(s2, ix3(kk, j, i, ny, nx)); };
   double fx0, fx1, fy0, fy1, fz0, fz1;
@@ -367,6 +358,66 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_tend_tiled(Grid g, LimArgs a, 
   double tend = -msftx * g.rdx * (fx1 - fx0);
   tend = tend - msftx * g.rdy * (fy1 - fy0);
   tend = tend - ld(g.rdnw, k) * (fz1 - fz0);
+  return tend;
+}
+
+struct LimSmem {
+  double q[Tile<3, 3>::N];
+  double qo[Tile<1, 1>::N];
+  double ru[Tile<1, 0>::N];
+  double rv[Tile<0, 1>::N];
+  double mt[Tile<1, 1>::N];
+  double s1[Tile<1, 1>::N];
+  double s2[Tile<1, 1>::N];
+  double fxl[LIM_NXF], fxa[LIM_NXF], fyl[LIM_NYF], fya[LIM_NYF];
+  ZConst zc[2];
+};
+
+__global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a, const double *field,
+                                                               const double *field_old, double *s1, double *s2) {
+  __shared__ LimSmem sm;
+  const int nx = g.nx, ny = g.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc, sm.fxl, sm.fxa, sm.fyl, sm.fya};
+  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
+  lim_zconst(g, a, k, sm.zc);
+  __syncthreads();
+  lim_face_fluxes(g, a, t, k);
+  __syncthreads();
+  if (i >= nx || j >= ny) return;
+  CellFluxes cf;
+  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
+  double r1, r2;
+  lim_cell_scales(g, a, t, k, j, i, field_old, cf, r1, r2);
+  const size_t c = ix3(k, j, i, ny, nx);
+  s1[c] = r1;
+  s2[c] = r2;
+}
+
+__global__ void __launch_bounds__(TSX *TSY) k_lim_tend_tiled(Grid g, LimArgs a, const double *field,
+                                                              const double *field_old, const double *s1,
+                                                              const double *s2, const double *base,
+                                                              const double *mu_total_stage, double *tend_out) {
+  __shared__ LimSmem sm;
+  const int nx = g.nx, ny = g.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc, sm.fxl, sm.fxa, sm.fyl, sm.fya};
+  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
+  lim_zconst(g, a, k, sm.zc);
+  const size_t plane = (size_t)k * ny * nx;
+  load_tile<1, 1>(sm.s1, s1 + plane, nx, i0, j0, nx, ny, 0.0);
+  load_tile<1, 1>(sm.s2, s2 + plane, nx, i0, j0, nx, ny, 0.0);
+  __syncthreads();
+  lim_face_fluxes(g, a, t, k);
+  __syncthreads();
+  if (i >= nx || j >= ny) return;
+  CellFluxes cf;
+  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
+  const double tend = lim_cell_tend(g, a, sm.s1, sm.s2, k, j, i, s1, s2, cf);
   const size_t c = ix3(k, j, i, ny, nx);
   if (base != nullptr) {
     const double mass_h = ld(g.c1h, k) * ld(mu_total_stage, ix2(j, i, nx)) + ld(g.c2h, k);
