@@ -10,7 +10,9 @@ aggregate, so no L2 flush is needed).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints ONE JSON line (rank 0).  ``--impl reference`` times the reference
+Prints ONE JSON line (rank 0).  Beside the float64 step it also times the
+mixed-precision variant (FP32 advective fluxes, float64 accumulation) on the
+same input and reports it under "mixed" (skip with --no-mixed).  ``--impl reference`` times the reference
 algorithm's CPU implementation available here -- the NumPy restatement in
 ``oracle/`` (JAX, the reference's own runtime, is not installed) -- on the
 host cores, on bounded 64 x 64 x 50 samples of the same workload.
@@ -270,10 +272,61 @@ def run_gpu(args, rank, world, local_rank):
     e2e_value = world * cells * nsub * k_e2e / (e2e_ms / 1000.0)
     out_ok = bool(torch.isfinite(out.state.w).all().item() and torch.isfinite(out.state.theta).all().item())
     del graph
+
+    # the mixed-precision variant (FP32 advective fluxes, float64 accumulation)
+    # on the same input, timed the same way, beside the float64 line
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        nl_m = dycore.OperationalNamelist.from_case(case, device=dev, precision="mixed")
+        stp_m = dycore.Stepper(nl_m, device=dev)
+        out_m = stp_m.alloc_carry(carry)
+
+        def step_m():
+            stp_m.step_into(carry, out_m, lead_seconds=0.0)
+
+        for _ in range(args.warmup):
+            step_m()
+        torch.cuda.synchronize(dev)
+        graph_m = torch.cuda.CUDAGraph()
+        s2 = torch.cuda.Stream(dev)
+        s2.wait_stream(stream)
+        with torch.cuda.stream(s2):
+            step_m()
+        stream.wait_stream(s2)
+        torch.cuda.synchronize(dev)
+        with torch.cuda.graph(graph_m):
+            step_m()
+        graph_m.replay()
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            graph_m.replay()
+        g1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_m = g0.elapsed_time(g1)
+        if dist is not None:
+            t = torch.tensor([ms_m], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_m = float(t.item())
+        # one-step difference from the float64 step on this workload
+        diff = {}
+        for f in ("u", "v", "w", "theta"):
+            a, b = getattr(out_m.state, f), getattr(out.state, f)
+            diff[f] = float((a - b).abs().max().item() / max(b.abs().max().item(), 1e-300))
+        mixed = {"value": world * cells * nsub * args.steps / (ms_m / 1000.0), "unit": METRIC,
+                 "ms_per_step": ms_m / args.steps, "dtype": "f32 fluxes / f64 accumulation",
+                 "rel_diff_vs_fp64_one_step": diff,
+                 "stated_error": "<= 1e-5 relative max-abs on u, v, w, theta after 60 steps vs the float64 oracle "
+                                 "(tests/test_gpu_mixed.py)"}
+        del graph_m
     return dict(value=value, ms_per_step=ms_per_step, clocks=clk, roofline=roof, whole_step_roofline=whole,
                 kernels=kernels, e2e={"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                                       "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e},
-                launches=stp.launches_per_step * args.steps, finite=out_ok)
+                launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed)
 
 
 def main():
@@ -287,6 +340,7 @@ def main():
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nz", type=int, default=NZ)
     ap.add_argument("--cpu-procs", type=int, default=0)
+    ap.add_argument("--no-mixed", action="store_true", help="skip timing the mixed-precision variant")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -338,7 +392,7 @@ def main():
                            "parallelism": f"replicas x{world}", "cuda_graph": True},
                 "e2e": r["e2e"], "roofline": r["roofline"], "whole_step_roofline": r["whole_step_roofline"],
                 "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": r["launches"],
-                "kernels": r["kernels"], "finite": r["finite"]}
+                "kernels": r["kernels"], "finite": r["finite"], "mixed": r["mixed"]}
         print(json.dumps(line))
     return 0
 

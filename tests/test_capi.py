@@ -78,6 +78,11 @@ def test_validate_accepts_reference_defaults(lib):
     assert lib.wrfgpu_step_params_validate(ctypes.byref(p)) == 0
 
 
+def test_validate_accepts_mixed_precision(lib):
+    p = _params(lib, precision=_capi.WRFGPU_PRECISION_MIXED)
+    assert lib.wrfgpu_step_params_validate(ctypes.byref(p)) == 0
+
+
 def test_workspace_size_grows_with_grid_and_options(lib):
     sizes = []
     for kw in (dict(), dict(nx=32), dict(moist_adv_opt=1), dict(run_boundary=1, bc_ideal=0)):

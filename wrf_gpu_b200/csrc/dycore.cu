@@ -397,8 +397,6 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "boundary zones other than spec_zone=1, relax_zone=4 are not built");
   if (p->precision != WRFGPU_PRECISION_FP64 && p->precision != WRFGPU_PRECISION_MIXED)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "unknown precision mode");
-  if (p->precision == WRFGPU_PRECISION_MIXED)
-    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "mixed precision is not built in this library version");
   return WRFGPU_OK;
 }
 
@@ -523,6 +521,16 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
                                                              w.rmsfvy);
   LAUNCH_CHECK("k_recip_msf");
 
+  // Advective-flux arithmetic: float64 (the reference's), or the mixed
+  // variant's FP32 fluxes with float64 accumulation.
+  const bool mixed = p.precision == WRFGPU_PRECISION_MIXED;
+  auto kUface = mixed ? k_uface_tiled<float> : k_uface_tiled<double>;
+  auto kVface = mixed ? k_vface_tiled<float> : k_vface_tiled<double>;
+  auto kWface = mixed ? k_wface_tiled<float> : k_wface_tiled<double>;
+  auto kScalar = mixed ? k_scalar_adv_march<float> : k_scalar_adv_march<double>;
+  auto kLimScale = mixed ? k_lim_march<false, float> : k_lim_march<false, double>;
+  auto kLimTend = mixed ? k_lim_march<true, float> : k_lim_march<true, double>;
+
   StateR s = origin;
   for (int stage = 0; stage < 3; ++stage) {
     const int rk = stage + 1;
@@ -545,12 +553,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     LAUNCH_CHECK("k_diag");
     UFaceOut uo{w.u_tend, w.u_w, w.cqu};
     PROF("k_uface");
-    k_uface_tiled<<<tgrd(nx + 1, ny, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
+    kUface<<<tgrd(nx + 1, ny, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
                                                                in->base_u, p.top_lid, p.run_boundary, uo);
     LAUNCH_CHECK("k_uface");
     VFaceOut vo{w.v_tend, w.v_w, w.cqv};
     PROF("k_vface");
-    k_vface_tiled<<<tgrd(nx, ny + 1, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
+    kVface<<<tgrd(nx, ny + 1, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
                                                                in->base_v, p.top_lid, p.run_boundary, vo);
     LAUNCH_CHECK("k_vface");
     const bool lim_theta = (rk == 3) && (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2);
@@ -563,7 +571,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     {
       const int nfields = 1 + ((moist && !lim_moist) ? 6 : 0);
       const int nchunk = march_nchunk(nz);
-      k_scalar_adv_march<<<tgrd(nx, ny, nfields * nchunk), tblk(), 0, stream>>>(
+      kScalar<<<tgrd(nx, ny, nfields * nchunk), tblk(), 0, stream>>>(
           g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, mo);
     }
     LAUNCH_CHECK("k_mass");
@@ -575,11 +583,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
         PROF("k_lim_scale");
-        k_lim_march<false><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+        kLimScale<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
             g, la, s.theta, origin.theta, w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
-        k_lim_march<true><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+        kLimTend<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
             g, la, s.theta, origin.theta, nullptr, nullptr, w.s1, w.s2, in->base_theta, s.mu_total, w.t_tend);
         LAUNCH_CHECK("k_lim_tend");
       }
@@ -588,11 +596,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.offset = 0.0;
         for (int q = 0; q < 6; ++q) {
           PROF("k_lim_scale");
-          k_lim_march<false><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+          kLimScale<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
               g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
           LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
-          k_lim_march<true><<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
+          kLimTend<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
               g, la, s.q[q], origin.q[q], nullptr, nullptr, w.s1, w.s2, nullptr, s.mu_total, w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
         }
@@ -601,7 +609,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     const double *ww_stage = specified ? w.ww_spec : w.rom;
     WFaceOut wo{w.rw_tend, w.ph_tend, w.cqw, w.w_w, w.ph_w, w.pt1, w.ww, w.phb0};
     PROF("k_wface");
-    k_wface_tiled<<<tgrd(nx, ny, nz + 1), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot,
+    kWface<<<tgrd(nx, ny, nz + 1), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot,
                                                                w.mub, w.mut, w.muts0, w.muu, w.muv, in->base_w,
                                                                p.top_lid, p.moist_cqw, p.w_coriolis, wo);
     LAUNCH_CHECK("k_wface");

@@ -113,6 +113,40 @@ __device__ __forceinline__ double flux3v(double qkm2, double qkm1, double qk, do
   return vel * (flux4 + sgn(-vel) * corr);
 }
 
+// Advective face fluxes in the arithmetic type F.  F = double: the
+// reference's float64 expressions, bit for bit (vel*flux5, flux3v).  F =
+// float: the mixed-precision variant -- the stencil is evaluated in FP32 from
+// float64 inputs (perturbations are formed in float64 first by the callers)
+// and the flux is widened back to float64, so every flux divergence and
+// tendency sum stays a float64 accumulation.
+template <typename F>
+__device__ __forceinline__ double hflux5(double vel, double qm3, double qm2, double qm1, double q0, double qp1,
+                                         double qp2) {
+  return vel * flux5(qm3, qm2, qm1, q0, qp1, qp2, vel);
+}
+template <>
+__device__ __forceinline__ double hflux5<float>(double vel, double qm3, double qm2, double qm1, double q0, double qp1,
+                                                double qp2) {
+  const float v = (float)vel, a3 = (float)qm3, a2 = (float)qm2, a1 = (float)qm1, b0 = (float)q0, b1 = (float)qp1,
+              b2 = (float)qp2;
+  const float f6 = (37.0f * (b0 + a1) - 8.0f * (b1 + a2) + (b2 + a3)) * (1.0f / 60.0f);
+  const float c = ((b2 - a3) - 5.0f * (b1 - a2) + 10.0f * (b0 - a1)) * (1.0f / 60.0f);
+  const float s = (float)((v > 0.0f) - (v < 0.0f));
+  return (double)(v * (f6 - s * c));
+}
+template <typename F>
+__device__ __forceinline__ double vflux3(double vel, double qkm2, double qkm1, double qk, double qkp1) {
+  return flux3v(qkm2, qkm1, qk, qkp1, vel);
+}
+template <>
+__device__ __forceinline__ double vflux3<float>(double vel, double qkm2, double qkm1, double qk, double qkp1) {
+  const float v = (float)vel, a2 = (float)qkm2, a1 = (float)qkm1, b0 = (float)qk, b1 = (float)qkp1;
+  const float flux4 = (7.0f * (b0 + a1) - (b1 + a2)) * (1.0f / 12.0f);
+  const float corr = ((b1 - a2) - 3.0f * (b0 - a1)) * (1.0f / 12.0f);
+  const float s = (float)((-v > 0.0f) - (-v < 0.0f));
+  return (double)(v * (flux4 + s * corr));
+}
+
 // Dry inverse density from the EOS (acoustic_wrf.py:187-206, qvf = 1).
 __device__ __forceinline__ double inv_density(double theta, double p) {
   return (R_D / P0) * theta * 1.0 * pow(dmax(p, 1.0) / P0, CVPM);

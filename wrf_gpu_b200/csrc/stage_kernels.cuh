@@ -180,13 +180,13 @@ __device__ __forceinline__ double dpn_acoustic(const Grid &g, int m, int top_lid
 
 // Order-3 vertical flux of a mass-level field at face m (flux_advection.py:1362-1407
 // for u/v, :534-562 for scalars; both use -sign(vel)).
-template <typename Q>
+template <typename F = double, typename Q>
 __device__ __forceinline__ double vflux3_at(const Grid &g, int m, double romq, Q q) {
   const int nz = g.nz;
   if (m <= 0 || m >= nz) return 0.0;
   if (m == 1) return romq * (ld(g.fnm, 1) * q(1) + ld(g.fnp, 1) * q(0));
   if (m == nz - 1) return romq * (ld(g.fnm, nz - 1) * q(nz - 1) + ld(g.fnp, nz - 1) * q(nz - 2));
-  return flux3v(q(m - 2), q(m - 1), q(m), q(m + 1), romq);
+  return vflux3<F>(romq, q(m - 2), q(m - 1), q(m), q(m + 1));
 }
 
 // ---------------------------------------------------------------------------

@@ -19,6 +19,7 @@ namespace wg {
 #endif
 
 // Advection of u at collapsed face ii from global loads (the periodic wrap face).
+template <typename F>
 __device__ __forceinline__ double u_adv_global(const Grid &g, const StateR &s, const double *ru, const double *rv,
                                                const double *rom, int k, int j, int ii) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1;
@@ -26,8 +27,8 @@ __device__ __forceinline__ double u_adv_global(const Grid &g, const StateR &s, c
   auto fqx = [&](int m) {
     int rm = wrp(m, nx);
     double vel = 0.5 * (ld(ru, ix3(k, j, rm, ny, nx)) + ld(ru, ix3(k, j, wrp(rm - 1, nx), ny, nx)));
-    return vel * flux5(uf(k, j, rm - 3), uf(k, j, rm - 2), uf(k, j, rm - 1), uf(k, j, rm), uf(k, j, rm + 1),
-                       uf(k, j, rm + 2), vel);
+    return hflux5<F>(vel, uf(k, j, rm - 3), uf(k, j, rm - 2), uf(k, j, rm - 1), uf(k, j, rm), uf(k, j, rm + 1),
+                       uf(k, j, rm + 2));
   };
   const double msfux_c = ld(g.msfux, ix2(j, ii, nxu));
   double tend = -msfux_c * g.rdx * (fqx(ii + 1) - fqx(ii));
@@ -35,19 +36,20 @@ __device__ __forceinline__ double u_adv_global(const Grid &g, const StateR &s, c
     auto fqy = [&](int n) {
       int rn = wrp(n, ny);
       double vel = 0.5 * (ld(rv, ix3(k, rn, ii, ny, nx)) + ld(rv, ix3(k, rn, wrp(ii - 1, nx), ny, nx)));
-      return vel * flux5(uf(k, rn - 3, ii), uf(k, rn - 2, ii), uf(k, rn - 1, ii), uf(k, rn, ii), uf(k, rn + 1, ii),
-                         uf(k, rn + 2, ii), vel);
+      return hflux5<F>(vel, uf(k, rn - 3, ii), uf(k, rn - 2, ii), uf(k, rn - 1, ii), uf(k, rn, ii), uf(k, rn + 1, ii),
+                         uf(k, rn + 2, ii));
     };
     tend = tend - msfux_c * g.rdy * (fqy(j + 1) - fqy(j));
   }
   auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, ii, ny, nx)) + ld(rom, ix3(m, j, wrp(ii - 1, nx), ny, nx))); };
   auto q = [&](int kk) { return ld(s.u, ix3(kk, j, ii, ny, nxu)); };
-  const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
-  const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+  const double v1 = (k + 1 <= nz - 1) ? vflux3_at<F>(g, k + 1, romq(k + 1), q) : 0.0;
+  const double v0 = (k >= 1) ? vflux3_at<F>(g, k, romq(k), q) : 0.0;
   return tend + (-ld(g.rdnw, k)) * (v1 - v0);
 }
 
 // Advection of v at collapsed face jj from global loads (the periodic wrap face).
+template <typename F>
 __device__ __forceinline__ double v_adv_global(const Grid &g, const StateR &s, const double *ru, const double *rv,
                                                const double *rom, int k, int jj, int i) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nyv = ny + 1;
@@ -57,27 +59,28 @@ __device__ __forceinline__ double v_adv_global(const Grid &g, const StateR &s, c
   auto fqx = [&](int m) {
     int rm = wrp(m, nx);
     double vel = 0.5 * (ld(ru, ix3(k, jj, rm, ny, nx)) + ld(ru, ix3(k, wrp(jj - 1, ny), rm, ny, nx)));
-    return vel * flux5(vf(k, jj, rm - 3), vf(k, jj, rm - 2), vf(k, jj, rm - 1), vf(k, jj, rm), vf(k, jj, rm + 1),
-                       vf(k, jj, rm + 2), vel);
+    return hflux5<F>(vel, vf(k, jj, rm - 3), vf(k, jj, rm - 2), vf(k, jj, rm - 1), vf(k, jj, rm), vf(k, jj, rm + 1),
+                       vf(k, jj, rm + 2));
   };
   double tend = -msfvy_c * g.rdx * (fqx(i + 1) - fqx(i));
   auto fqy = [&](int n) {
     int rn = wrp(n, ny);
     double vel = 0.5 * (ld(rv, ix3(k, rn, i, ny, nx)) + ld(rv, ix3(k, wrp(rn - 1, ny), i, ny, nx)));
-    return vel * flux5(vf(k, rn - 3, i), vf(k, rn - 2, i), vf(k, rn - 1, i), vf(k, rn, i), vf(k, rn + 1, i),
-                       vf(k, rn + 2, i), vel);
+    return hflux5<F>(vel, vf(k, rn - 3, i), vf(k, rn - 2, i), vf(k, rn - 1, i), vf(k, rn, i), vf(k, rn + 1, i),
+                       vf(k, rn + 2, i));
   };
   tend = tend - msfvy_c * g.rdy * (fqy(jj + 1) - fqy(jj));
   auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, jj, i, ny, nx)) + ld(rom, ix3(m, wrp(jj - 1, ny), i, ny, nx))); };
   auto q = [&](int kk) { return ld(s.v, ix3(kk, jj, i, nyv, nx)); };
-  const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
-  const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+  const double v1 = (k + 1 <= nz - 1) ? vflux3_at<F>(g, k + 1, romq(k + 1), q) : 0.0;
+  const double v0 = (k >= 1) ? vflux3_at<F>(g, k, romq(k), q) : 0.0;
   return tend + div_rcp(msfvy_c, msfvx_c, ld(g.rmsfvx, ix2(jj, i, nx))) * ((-ld(g.rdnw, k)) * (v1 - v0));
 }
 
 // ---------------------------------------------------------------------------
 // u faces, tiled advection.  Grid over faces 0..nx.
 // ---------------------------------------------------------------------------
+template <typename F>
 __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muu, const double *muus,
@@ -106,25 +109,25 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
     auto RV = [&](int r, int cc) { return srv[(r + 1) * TV::W + (cc + 1)]; };
     auto fqx = [&](int m) {
       const double vel = 0.5 * (RU(m) + RU(m - 1));
-      return vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
+      return hflux5<F>(vel, Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2));
     };
     const double msfux_c = ld(g.msfux, ix2(j, i, nxu));
     tend = -msfux_c * g.rdx * (fqx(tx + 1) - fqx(tx));
     if (ny > 1) {
       auto fqy = [&](int r) {
         const double vel = 0.5 * (RV(r, tx) + RV(r, tx - 1));
-        return vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
+        return hflux5<F>(vel, Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx));
       };
       tend = tend - msfux_c * g.rdy * (fqy(ty + 1) - fqy(ty));
     }
     const int im = wrp(i - 1, nx);
     auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, i, ny, nx)) + ld(rom, ix3(m, j, im, ny, nx))); };
     auto q = [&](int kk) { return ld(s.u, ix3(kk, j, i, ny, nxu)); };
-    const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
-    const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+    const double v1 = (k + 1 <= nz - 1) ? vflux3_at<F>(g, k + 1, romq(k + 1), q) : 0.0;
+    const double v0 = (k >= 1) ? vflux3_at<F>(g, k, romq(k), q) : 0.0;
     tend = tend + (-ld(g.rdnw, k)) * (v1 - v0);
   } else {
-    tend = u_adv_global(g, s, ru, rv, rom, k, j, 0);
+    tend = u_adv_global<F>(g, s, ru, rv, rom, k, j, 0);
   }
   const int l = (i == 0) ? 0 : i - 1;
   const int r = (i == nx) ? nx - 1 : i;
@@ -196,6 +199,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
 // ---------------------------------------------------------------------------
 // v faces, tiled advection.  Grid over faces 0..ny.
 // ---------------------------------------------------------------------------
+template <typename F>
 __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muv, const double *muvs,
@@ -226,22 +230,22 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, 
     const double msfvx_c = ld(g.msfvx, ix2(j, i, nx));
     auto fqx = [&](int m) {
       const double vel = 0.5 * (RU(ty, m) + RU(ty - 1, m));
-      return vel * flux5(Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2), vel);
+      return hflux5<F>(vel, Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2));
     };
     tend = -msfvy_c * g.rdx * (fqx(tx + 1) - fqx(tx));
     auto fqy = [&](int r) {
       const double vel = 0.5 * (RV(r) + RV(r - 1));
-      return vel * flux5(Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx), vel);
+      return hflux5<F>(vel, Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx));
     };
     tend = tend - msfvy_c * g.rdy * (fqy(ty + 1) - fqy(ty));
     const int jm = wrp(j - 1, ny);
     auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, i, ny, nx)) + ld(rom, ix3(m, jm, i, ny, nx))); };
     auto q = [&](int kk) { return ld(s.v, ix3(kk, j, i, nyv, nx)); };
-    const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, romq(k + 1), q) : 0.0;
-    const double v0 = (k >= 1) ? vflux3_at(g, k, romq(k), q) : 0.0;
+    const double v1 = (k + 1 <= nz - 1) ? vflux3_at<F>(g, k + 1, romq(k + 1), q) : 0.0;
+    const double v0 = (k >= 1) ? vflux3_at<F>(g, k, romq(k), q) : 0.0;
     tend = tend + div_rcp(msfvy_c, msfvx_c, ld(g.rmsfvx, ix2(j, i, nx))) * ((-ld(g.rdnw, k)) * (v1 - v0));
   } else {
-    tend = v_adv_global(g, s, ru, rv, rom, k, 0, i);
+    tend = v_adv_global<F>(g, s, ru, rv, rom, k, 0, i);
   }
   const int sj = (j == 0) ? 0 : j - 1;
   const int nj = (j == ny) ? ny - 1 : j;
@@ -311,6 +315,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, 
 // ---------------------------------------------------------------------------
 // w faces, tiled: w advection and rhs_ph horizontal stencils from tiles.
 // ---------------------------------------------------------------------------
+template <typename F>
 __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom,
                                                            const double *ww_stage, const double *qtot,
@@ -372,13 +377,13 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
   const double msftx = ld(g.msftx, c2d);
   auto fqx = [&](int m) {
     const double vel = sru[ty * TR::W + (m + 1)];
-    return vel * flux5(W_(ty, m - 3), W_(ty, m - 2), W_(ty, m - 1), W_(ty, m), W_(ty, m + 1), W_(ty, m + 2), vel);
+    return hflux5<F>(vel, W_(ty, m - 3), W_(ty, m - 2), W_(ty, m - 1), W_(ty, m), W_(ty, m + 1), W_(ty, m + 2));
   };
   double adv = -msftx * g.rdx * (fqx(tx + 1) - fqx(tx));
   if (ny > 1) {
     auto fqy = [&](int r) {
       const double vel = srv[(r + 1) * TV::W + tx];
-      return vel * flux5(W_(r - 3, tx), W_(r - 2, tx), W_(r - 1, tx), W_(r, tx), W_(r + 1, tx), W_(r + 2, tx), vel);
+      return hflux5<F>(vel, W_(r - 3, tx), W_(r - 2, tx), W_(r - 1, tx), W_(r, tx), W_(r + 1, tx), W_(r + 2, tx));
     };
     adv = adv - msftx * g.rdy * (fqy(ty + 1) - fqy(ty));
   }
@@ -388,7 +393,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
     auto vfw = [&](int m) {
       if (m <= 0) return 0.0;
       if (m == 1) return velf(1) * 0.5 * (wc(1) + wc(0));
-      if (m < nz) return flux3v(wc(m - 2), wc(m - 1), wc(m), wc(m + 1), velf(m));
+      if (m < nz) return vflux3<F>(velf(m), wc(m - 2), wc(m - 1), wc(m), wc(m + 1));
       if (m == nz && !top_lid) return velf(nz) * 0.5 * (wc(nz) + wc(nz - 1));
       return 0.0;
     };

@@ -79,6 +79,7 @@ constexpr int MARCH_KC = WG_MARCH_KC;
 // written, the tendency only when theta is not limited), fields 1..6 the
 // species.
 // ---------------------------------------------------------------------------
+template <typename F>
 __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s, StateR ref, const double *ru,
                                                                 const double *rv, const double *rom, const double *mut,
                                                                 const double *muts0, const double *base_theta,
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
     cp_async_commit();
   };
   auto qc = [&](int kk) { return ld(fld, (size_t)kk * plane + c2d) - sub; };
-  auto vflux = [&](int m) { return vflux3_at(g, m, ld(rom, (size_t)m * plane + c2d), qc); };
+  auto vflux = [&](int m) { return vflux3_at<F>(g, m, ld(rom, (size_t)m * plane + c2d), qc); };
 
   if (advect) issue(k0, 0);
   double v_lo = 0.0;  // vertical flux at the current level's bottom face
@@ -147,12 +148,12 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
         if (e < NXF) {
           const int r = e / (TSX + 1), m = e - r * (TSX + 1);
           const double vel = RU[r * TR::W + (m + 1)];
-          sfx[e] = vel * flux5(Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2), vel);
+          sfx[e] = hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
         } else {
           const int e2 = e - NXF;
           const int r = e2 / TSX, cc = e2 - r * TSX;
           const double vel = RV[(r + 1) * TV::W + cc];
-          sfy[e2] = vel * flux5(Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc), vel);
+          sfy[e2] = hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc));
         }
       }
       __syncthreads();
@@ -209,7 +210,7 @@ struct LimMarchSmem {
   ZConst zc[2];
 };
 
-template <bool TEND>
+template <bool TEND, typename F>
 __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const double *field,
                                                          const double *field_old, double *s1w, double *s2w,
                                                          const double *s1r, const double *s2r, const double *base,
@@ -256,13 +257,13 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const
     lim_zconst(g, a, k, sm.zc);
     __syncthreads();
     LimTiles t{sm.q[b], sm.qo[b], sm.ru[b], sm.rv[b], sm.mt, sm.zc, sm.fxl, sm.fxa, sm.fyl, sm.fya};
-    lim_face_fluxes(g, a, t, k);
+    lim_face_fluxes<F>(g, a, t, k);
     __syncthreads();
     if (valid) {
       CellFluxes cf;
       cf.lz0 = zlo;
       cf.az0 = zan;
-      cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf, k > k0);
+      cell_fluxes_tiled<F>(g, a, t, k, j, i, field, field_old, cf, k > k0);
       zlo = cf.lz1;
       zan = cf.az1;
       const size_t c = (size_t)k * plane + ix2(j, i, nx);

@@ -1,11 +1,11 @@
-// Shared-memory tiled versions of the horizontal-stencil stage kernels.
+// Shared-memory plane tiles for the horizontal-stencil stage kernels, and the
+// per-level pieces of the PD / monotonic limiter that the marching kernels
+// (tiled_march.cuh) assemble.
 //
-// A block computes a 32 x 8 tile of one level.  Every field a stencil needs is
-// staged once per block as a (8 + 2*HY) x (32 + 2*HX) plane tile, with the
-// periodic wrap of the reference's jnp.roll applied once per staged element;
-// the flux stencils then read shared memory with fixed offsets.  Vertical
-// stencils read global memory at the thread's own column.  The arithmetic
-// keeps the reference's expression order.
+// A tile covers 32 x 8 cells of one level plus a halo: element (r, c) of a
+// (8 + 2*HY) x (32 + 2*HX) tile holds the field at the periodically wrapped
+// cell (j0 - HY + r, i0 - HX + c), so the flux stencils read shared memory at
+// fixed offsets.  The arithmetic keeps the reference's expression order.
 #pragma once
 #include "dycore_common.cuh"
 #include "stage_kernels.cuh"
@@ -35,100 +35,8 @@ __device__ __forceinline__ void load_tile(double *t, const double *plane, int pi
 }
 
 // ---------------------------------------------------------------------------
-// Plain h5/v3 scalar advection (flux_advection.py:482-568) for theta and the
-// moisture species, plus theta_work (small_step_prep.py:321).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_tiled(Grid g, StateR s, StateR ref, const double *ru,
-                                                                const double *rv, const double *rom, const double *mut,
-                                                                const double *muts0, const double *base_theta,
-                                                                int theta_plain, int moist_plain, MassOut o) {
-  using TQ = Tile<3, 3>;
-  using TR = Tile<1, 0>;
-  using TV = Tile<0, 1>;
-  constexpr int NXF = TSY * (TSX + 1);  // x faces of the tile, each computed once
-  constexpr int NYF = (TSY + 1) * TSX;  // y faces
-  __shared__ double sq[TQ::N];
-  __shared__ double sru[TR::N];
-  __shared__ double srv[TV::N];
-  __shared__ double sfx[NXF];
-  __shared__ double sfy[NYF];
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool valid = i < nx && j < ny;
-  const size_t plane = (size_t)k * ny * nx;
-  load_tile<1, 0>(sru, ru + plane, nx, i0, j0, nx, ny, 0.0);
-  load_tile<0, 1>(srv, rv + plane, nx, i0, j0, nx, ny, 0.0);
-  const size_t c = valid ? ix3(k, j, i, ny, nx) : 0;
-  const size_t c2d = valid ? ix2(j, i, nx) : 0;
-  const double msftx = valid ? ld(g.msftx, c2d) : 1.0;
-  const double rom0 = valid ? ld(rom, ix3(k, j, i, ny, nx)) : 0.0;
-  const double rom1 = valid ? ld(rom, ix3(k + 1, j, i, ny, nx)) : 0.0;
-  auto tend_of = [&](const double *fld, double sub) {
-    __syncthreads();
-    load_tile<3, 3>(sq, fld + plane, nx, i0, j0, nx, ny, sub);
-    __syncthreads();
-    auto Q = [&](int r, int cc) { return sq[(r + 3) * TQ::W + (cc + 3)]; };  // local (row, col)
-    auto fqx = [&](int r, int m) {  // x face at local column m of row r
-      const double vel = sru[r * TR::W + (m + 1)];
-      return vel * flux5(Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2), vel);
-    };
-    auto fqy = [&](int r, int cc) {  // y face at local row r of column cc
-      const double vel = srv[(r + 1) * TV::W + cc];
-      return vel * flux5(Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc), vel);
-    };
-    // Every face flux of the tile once (the tile's stencil reads are in
-    // shared memory and wrap periodically, so edge tiles compute harmless
-    // extra faces).
-    for (int e = ty * TSX + tx; e < NXF + NYF; e += TSX * TSY) {
-      if (e < NXF) {
-        const int r = e / (TSX + 1), m = e - r * (TSX + 1);
-        sfx[e] = fqx(r, m);
-      } else {
-        const int e2 = e - NXF;
-        const int r = e2 / TSX, cc = e2 - r * TSX;
-        sfy[e2] = fqy(r, cc);
-      }
-    }
-    __syncthreads();
-    if (!valid) return 0.0;
-    double tend = -msftx * g.rdx * (sfx[ty * (TSX + 1) + tx + 1] - sfx[ty * (TSX + 1) + tx]);
-    tend = tend - msftx * g.rdy * (sfy[(ty + 1) * TSX + tx] - sfy[ty * TSX + tx]);
-    auto qc = [&](int kk) { return ld(fld, ix3(kk, j, i, ny, nx)) - sub; };
-    const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, rom1, qc) : 0.0;
-    const double v0 = (k >= 1) ? vflux3_at(g, k, rom0, qc) : 0.0;
-    return tend - ld(g.rdnw, k) * (v1 - v0);
-  };
-  if (theta_plain) {
-    const double adv = tend_of(s.theta, T0);
-    if (valid) {
-      if (base_theta != nullptr) {
-        const double mass_h = ld(g.c1h, k) * ld(s.mu_total, c2d) + ld(g.c2h, k);
-        o.t_tend[c] = ld(base_theta, c) * mass_h + adv;
-      } else {
-        o.t_tend[c] = adv;
-      }
-    }
-  }
-  if (moist_plain) {
-#pragma unroll
-    for (int sp = 0; sp < 6; ++sp) {
-      const double adv = tend_of(s.q[sp], 0.0);
-      if (valid) o.q_tend[sp][c] = adv;
-    }
-  }
-  if (valid) {
-    const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-    const double mass_ref = c1 * ld(muts0, c2d) + c2;
-    const double mass_cur = c1 * ld(mut, c2d) + c2;
-    o.theta_w[c] = mass_ref * (ld(ref.theta, c) - T0) - mass_cur * (ld(s.theta, c) - T0);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// PD / monotonic limited scalar advection (flux_advection.py:736-1000),
-// tiled.  Pass 1 writes the per-cell scale(s); pass 2 the tendency.
+// PD / monotonic limited scalar advection (flux_advection.py:736-1000):
+// per-level face fluxes, cell scales and limited tendency.
 // ---------------------------------------------------------------------------
 // Vertical spacing of the two faces of the block's level (k and k+1):
 // dz = 2/(rdnw[m] + rdnw[m-1]) (flux_advection.py upwind z flux), its
@@ -152,17 +60,6 @@ struct LimTiles {
 constexpr int LIM_NXF = TSY * (TSX + 1);
 constexpr int LIM_NYF = (TSY + 1) * TSX;
 
-__device__ __forceinline__ void lim_stage_tiles(const Grid &g, const LimArgs &a, const double *field,
-                                                const double *field_old, int i0, int j0, int k, LimTiles &t) {
-  const int nx = g.nx, ny = g.ny;
-  const size_t plane = (size_t)k * ny * nx;
-  load_tile<3, 3>(t.q, field + plane, nx, i0, j0, nx, ny, 0.0);  // raw; the offset is taken at use
-  load_tile<1, 1>(t.qo, field_old + plane, nx, i0, j0, nx, ny, 0.0);
-  load_tile<1, 0>(t.ru, a.ru + plane, nx, i0, j0, nx, ny, 0.0);
-  load_tile<0, 1>(t.rv, a.rv + plane, nx, i0, j0, nx, ny, 0.0);
-  load_tile<1, 1>(t.mt, a.mut, nx, i0, j0, nx, ny, 0.0);
-}
-
 __device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int k, ZConst *zc) {
   const int f = threadIdx.y * TSX + threadIdx.x;
   if (f < 2) {
@@ -181,6 +78,7 @@ __device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int 
 // order :678-711 minus low order) fluxes of every x and y face of the tile,
 // one face per thread item, into shared memory.  Edge tiles compute a few
 // harmless extra faces from the periodically wrapped staged values.
+template <typename F>
 __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a, const LimTiles &t, int k) {
   using TQ = Tile<3, 3>;
   using TO = Tile<1, 1>;
@@ -204,7 +102,7 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
       const double muu = 0.5 * (MT(r, m) + MT(r, m - 1));
       const double mu_u = c1 * muu + c2;
       const double lo = upw(QO(r, m - 1), QO(r, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
-      const double hi = vel * flux5(Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2), vel);
+      const double hi = hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
       t.fxl[e] = lo;
       t.fxa[e] = hi - lo;
     } else {
@@ -214,7 +112,7 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
       const double muv = 0.5 * (MT(r, cc) + MT(r - 1, cc));
       const double mu_v = c1 * muv + c2;
       const double lo = upw(QO(r - 1, cc), QO(r, cc), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
-      const double hi = vel * flux5(Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc), vel);
+      const double hi = hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc));
       t.fyl[e2] = lo;
       t.fya[e2] = hi - lo;
     }
@@ -226,6 +124,7 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
 // (:678-711) minus low order, at the cell's two x, y and z faces.
 // With have_z0 the bottom-face z fluxes are taken from cf.lz0/cf.az0 (carried
 // up from the level below) instead of being recomputed.
+template <typename F>
 __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int j,
                                                   int i, const double *field, const double *field_old,
                                                   CellFluxes &cf, bool have_z0 = false) {
@@ -250,7 +149,7 @@ __device__ __forceinline__ void cell_fluxes_tiled(const Grid &g, const LimArgs &
     const double cr = div_rcp(romv * a.dt, t.zc[zi].dz, t.zc[zi].rdz) / mu_face;
     const double ab = fabs(cr);
     lo = mu_face * t.zc[zi].dz_dt * (0.5 * dmin(1.0, cr + ab) * qo(m - 1) + 0.5 * dmax(-1.0, cr - ab) * qo(m));
-    const double hi = vflux3_at(g, m, romv, qf);
+    const double hi = vflux3_at<F>(g, m, romv, qf);
     an = hi - lo;
   };
   const int x0 = ty * (TSX + 1) + tx, y0 = ty * TSX + tx;
@@ -359,72 +258,6 @@ __device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a,
   tend = tend - msftx * g.rdy * (fy1 - fy0);
   tend = tend - ld(g.rdnw, k) * (fz1 - fz0);
   return tend;
-}
-
-struct LimSmem {
-  double q[Tile<3, 3>::N];
-  double qo[Tile<1, 1>::N];
-  double ru[Tile<1, 0>::N];
-  double rv[Tile<0, 1>::N];
-  double mt[Tile<1, 1>::N];
-  double s1[Tile<1, 1>::N];
-  double s2[Tile<1, 1>::N];
-  double fxl[LIM_NXF], fxa[LIM_NXF], fyl[LIM_NYF], fya[LIM_NYF];
-  ZConst zc[2];
-};
-
-__global__ void __launch_bounds__(TSX *TSY) k_lim_scale_tiled(Grid g, LimArgs a, const double *field,
-                                                               const double *field_old, double *s1, double *s2) {
-  __shared__ LimSmem sm;
-  const int nx = g.nx, ny = g.ny;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
-  const int i = i0 + tx, j = j0 + ty;
-  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc, sm.fxl, sm.fxa, sm.fyl, sm.fya};
-  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
-  lim_zconst(g, a, k, sm.zc);
-  __syncthreads();
-  lim_face_fluxes(g, a, t, k);
-  __syncthreads();
-  if (i >= nx || j >= ny) return;
-  CellFluxes cf;
-  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
-  double r1, r2;
-  lim_cell_scales(g, a, t, k, j, i, field_old, cf, r1, r2);
-  const size_t c = ix3(k, j, i, ny, nx);
-  s1[c] = r1;
-  s2[c] = r2;
-}
-
-__global__ void __launch_bounds__(TSX *TSY) k_lim_tend_tiled(Grid g, LimArgs a, const double *field,
-                                                              const double *field_old, const double *s1,
-                                                              const double *s2, const double *base,
-                                                              const double *mu_total_stage, double *tend_out) {
-  __shared__ LimSmem sm;
-  const int nx = g.nx, ny = g.ny;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
-  const int i = i0 + tx, j = j0 + ty;
-  LimTiles t{sm.q, sm.qo, sm.ru, sm.rv, sm.mt, sm.zc, sm.fxl, sm.fxa, sm.fyl, sm.fya};
-  lim_stage_tiles(g, a, field, field_old, i0, j0, k, t);
-  lim_zconst(g, a, k, sm.zc);
-  const size_t plane = (size_t)k * ny * nx;
-  load_tile<1, 1>(sm.s1, s1 + plane, nx, i0, j0, nx, ny, 0.0);
-  load_tile<1, 1>(sm.s2, s2 + plane, nx, i0, j0, nx, ny, 0.0);
-  __syncthreads();
-  lim_face_fluxes(g, a, t, k);
-  __syncthreads();
-  if (i >= nx || j >= ny) return;
-  CellFluxes cf;
-  cell_fluxes_tiled(g, a, t, k, j, i, field, field_old, cf);
-  const double tend = lim_cell_tend(g, a, sm.s1, sm.s2, k, j, i, s1, s2, cf);
-  const size_t c = ix3(k, j, i, ny, nx);
-  if (base != nullptr) {
-    const double mass_h = ld(g.c1h, k) * ld(mu_total_stage, ix2(j, i, nx)) + ld(g.c2h, k);
-    tend_out[c] = ld(base, c) * mass_h + tend;
-  } else {
-    tend_out[c] = tend;
-  }
 }
 
 }  // namespace wg
