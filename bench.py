@@ -139,6 +139,18 @@ class ClockSampler:
 # GPU arm
 # ---------------------------------------------------------------------------
 
+def _measured_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    import glob
+    import re
+    for path in glob.glob(os.path.join(HERE, "profiles", "dram_*.md")):
+        with open(path) as f:
+            m = re.search(r"traffic_bytes_per_launch %s(?:_tiled)?: (\d+)" % re.escape(kernel), f.read())
+        if m:
+            return float(m.group(1)), os.path.relpath(path, HERE)
+    return None, None
+
+
 def _peaks():
     try:
         with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
@@ -225,6 +237,10 @@ def run_gpu(args, rank, world, local_rank):
                 "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "bytes_per_launch": bpl, "avg_launch_ms": round(dom_ms / dom_n, 4),
                 "traffic": None, "kernel_share": round(dom_ms / sum(v[0] for v in prof.values()), 4)}
+        traffic, src = _measured_traffic(dom_name)
+        if traffic is not None:
+            roof["traffic"] = traffic
+            roof["traffic_source"] = f"ncu dram__bytes_read.sum + dram__bytes_write.sum, {src}"
     step_bytes = perfmodel.step_bytes(nx, ny, nz, ns, moist=True)
     whole = {"bytes_per_step": step_bytes, "achieved_gbs": round(step_bytes / (ms_per_step / 1000.0) / 1e9, 1),
              "frac": round(step_bytes / (ms_per_step / 1000.0) / 1e9 / hbm, 4)}
