@@ -5,7 +5,8 @@ steps) and advance one RK3 step; every prognostic and carry field must agree
 to 1e-12 relative max-abs (max|gpu - oracle| / max|oracle|).  Fields that are
 still at the float64 noise floor of a near-rest start (the first steps of the
 warm bubbles, where w and v are ~1e-4 m/s) are checked against the measured
-sensitivity of the oracle itself to one-ulp changes of pow().
+sensitivity of the oracle itself to one-ulp changes of pow(): perturbing one
+pow() result by one ulp moves such fields by ~1e-12..1e-11 relative.
 """
 
 from __future__ import annotations
@@ -107,7 +108,7 @@ def test_per_step_parity_warm_bubble_3d(cuda_ready):
     errs = _per_step(case, 3)
     for n, e in enumerate(errs):
         # u, v, w start at rest: their step-1..3 magnitudes are 1e-3..1e-1 m/s,
-        # where one-ulp pow() differences are ~1e-12 relative (DESIGN.md).
+        # where one-ulp pow() differences are ~1e-12 relative.
         bad = {k: v for k, v in e.items() if not v <= (1.0e-10 if k in ("u", "v", "w", "u_save", "v_save", "w_save",
                                                                           "mudf", "muave", "ww", "ww_save",
                                                                           "ph_tend", "p_perturbation") else _tol(k))}
