@@ -22,7 +22,7 @@ namespace wg {
 #define WG_COL_TX 32
 #endif
 #ifndef WG_COL_TY
-#define WG_COL_TY 16
+#define WG_COL_TY 13
 #endif
 #ifndef WG_COL_MINB
 #define WG_COL_MINB 2
@@ -34,7 +34,7 @@ namespace wg {
 #endif
 constexpr int COL_TX = WG_COL_TX;
 constexpr int COL_TY = WG_COL_TY;
-constexpr int COL_NARR = 7;
+constexpr int COL_NARR = 8;
 static_assert(COL_TY >= 2, "the Thomas phase needs a second warp row to stage gamma");
 
 // Bulk L2 prefetch of the rows (levels 0..nz) this column block will read.
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   const int L = nz + 1;
   auto S = [&](int a, int k) -> double & { return sm[((size_t)a * L + k) * COL_TX + tx]; };
   // array roles (see the phase list below)
-  constexpr int A0 = 0, A1 = 1, A2 = 2, A3 = 3, A4 = 4, A5 = 5, A6 = 6;
+  constexpr int A0 = 0, A1 = 1, A2 = 2, A3 = 3, A4 = 4, A5 = 5, A6 = 6, A7 = 7;
   const size_t c2d = valid ? ix2(j, i, nx) : 0;
   auto M = [&](int k) { return ix3(k, j, i, ny, nx); };
   const double dts = c.dts;
@@ -180,6 +180,17 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   }
   __syncthreads();
   // ---------------- P3: ww increments -> A1, ww_1 -> A2, old ww (inactive) -> A3 ----------------
+  // P5's per-level inputs are copied asynchronously now, each level by the
+  // thread that will use it: theta_w -> A7 (kept to P10), old t_2ave -> A6
+  // and t_tend -> A4 (both free until P6/P7).
+  if (valid) {
+    for (int k = ty; k < nz; k += COL_TY) {
+      cp_async8(&S(A7, k), A.theta_w + M(k));
+      cp_async8(&S(A6, k), A.t2ave + M(k));
+      cp_async8(&S(A4, k), A.t_tend + M(k));
+    }
+  }
+  cp_async_commit();
   double ww_bot = 0.0, ww_top = 0.0;  // old ww at faces 0 and nz, for P4
   if (ty == 0 && active) {
     ww_bot = A.ww[M(0)];
@@ -224,9 +235,10 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
     } else {
       ie = wrp(i + 1, nx); iw = wrp(i - 1, nx); jn = wrp(j + 1, ny); js = wrp(j - 1, ny);
     }
+    cp_async_wait<0>();  // this thread's staged levels
     for (int k = ty; k < nz; k += COL_TY) {
-      double thw = A.theta_w[M(k)];
-      const double t2ave_old = A.t2ave[M(k)];
+      double thw = S(A7, k);
+      const double t2ave_old = S(A6, k);
       if (active) {
         const double wdtn_hi = (k + 1 <= nz - 1)
                                    ? S(A3, k + 1) * (ld(g.fnm, k + 1) * T1(k + 1, j, i) + ld(g.fnp, k + 1) * T1(k, j, i))
@@ -236,9 +248,10 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
         const double v_flux = ld(A.v, ix3(k, j + 1, i, nyv, nx)) * (T1(k, jn, i) + th) - ld(A.v, ix3(k, j, i, nyv, nx)) * (th + T1(k, js, i));
         const double u_flux = ld(A.u, ix3(k, j, i + 1, ny, nxu)) * (T1(k, j, ie) + th) - ld(A.u, ix3(k, j, i, ny, nxu)) * (th + T1(k, j, iw));
         const double tend = msftx * (0.5 * g.rdy * v_flux + 0.5 * g.rdx * u_flux) + ld(g.rdnw, k) * (wdtn_hi - wdtn_lo);
-        const double theta_i = thw + msfty * dts * ld(A.t_tend, M(k));
+        const double theta_i = thw + msfty * dts * S(A4, k);
         thw = theta_i - dts * msfty * tend;
         A.theta_w[M(k)] = thw;
+        S(A7, k) = thw;
       }
       const double mass_h = ld(g.c1h, k) * muts + ld(g.c2h, k);
       const double half = 0.5 * (eps_p * thw + eps_m * t2ave_old);
@@ -395,7 +408,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
       const double t1 = T1(k, j, i);
       const double ttr = T0 + t1;
       const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
-      const double pp = ld(A.c2a, M(k)) * (altc * (A.theta_w[M(k)] - mu_term * t1) / (safe * sttr) - al);
+      const double pp = ld(A.c2a, M(k)) * (altc * (S(A7, k) - mu_term * t1) / (safe * sttr) - al);
       const double pm1 = ld(A.pm1, M(k));
       A.p[M(k)] = pp + SMDIV * (pp - pm1);
       A.pm1[M(k)] = pp;

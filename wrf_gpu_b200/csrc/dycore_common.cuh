@@ -158,6 +158,18 @@ __device__ __forceinline__ double pressure_from_theta_alt(double theta, double a
   return P0 * pow(dmax(argument, 1.0e-12), CPOVCV);
 }
 
+// 8-byte asynchronous global->shared copy (cp.async), its group commit and
+// the wait for all but the N most recent groups of this thread.
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Hint: pull the row of n doubles starting at p into L2 with one bulk
 // prefetch (cp.async.bulk.prefetch.L2).  Only the 16-byte-aligned part that
 // lies strictly inside the row is named, so nothing outside it is touched.

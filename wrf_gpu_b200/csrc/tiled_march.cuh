@@ -16,16 +16,6 @@
 
 namespace wg {
 
-__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Per-thread share of one (TSY + 2*HY) x (TSX + 2*HX) plane tile: the
 // elements e = tid, tid + 256, ... with their wrapped in-plane offsets.
 template <int HX, int HY>
