@@ -160,6 +160,48 @@ __global__ void k_advance_v(Grid g, Acoustic A, double dts, int top_lid, BdyArgs
 }
 
 // ---------------------------------------------------------------------------
+// Horizontal parts of advance_mu_t that couple neighbouring columns, one
+// thread per cell, after advance_uv: the coupled mass-flux divergence dvdxi
+// (dynamics/mu_t_advance.py:186-204) and the horizontal theta flux divergence
+// msftx*(0.5*rdy*v_flux + 0.5*rdx*u_flux) (:239-262).  Both are written for
+// the interior columns the column kernel updates and read there per level.
+// ---------------------------------------------------------------------------
+__global__ void k_div_h(Grid g, Acoustic A, int specified, double *dvdxi, double *hdiv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nxu = nx + 1, nyv = ny + 1;
+  if (i >= nx || j >= ny) return;
+  if (specified && !(j >= 1 && j <= ny - 2 && i >= 1 && i <= nx - 2)) return;
+  const size_t c2d = ix2(j, i, nx);
+  const double msftx = ld(g.msftx, c2d), msfty = ld(g.msfty, c2d);
+  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+  const double v_n = ld(A.v, ix3(k, j + 1, i, nyv, nx)), v_s = ld(A.v, ix3(k, j, i, nyv, nx));
+  const double u_e = ld(A.u, ix3(k, j, i + 1, ny, nxu)), u_w = ld(A.u, ix3(k, j, i, ny, nxu));
+  const double vn = v_n + (c1 * ld(A.muv, ix2(j + 1, i, nx)) + c2) * ld(A.v_1, ix3(k, j + 1, i, nyv, nx)) *
+                              ld(g.rmsfvx, ix2(j + 1, i, nx));
+  const double vs = v_s + (c1 * ld(A.muv, ix2(j, i, nx)) + c2) * ld(A.v_1, ix3(k, j, i, nyv, nx)) *
+                              ld(g.rmsfvx, ix2(j, i, nx));
+  const double ue = u_e + div_msf((c1 * ld(A.muu, ix2(j, i + 1, nxu)) + c2) * ld(A.u_1, ix3(k, j, i + 1, ny, nxu)),
+                                  g.msfuy, g.rmsfuy, ix2(j, i + 1, nxu));
+  const double uw = u_w + div_msf((c1 * ld(A.muu, ix2(j, i, nxu)) + c2) * ld(A.u_1, ix3(k, j, i, ny, nxu)),
+                                  g.msfuy, g.rmsfuy, ix2(j, i, nxu));
+  const size_t c = ix3(k, j, i, ny, nx);
+  dvdxi[c] = msftx * msfty * (g.rdy * (vn - vs) + g.rdx * (ue - uw));
+  int ie, iw, jn, js;
+  if (specified) {
+    ie = i + 1; iw = i - 1; jn = j + 1; js = j - 1;
+  } else {
+    ie = wrp(i + 1, nx); iw = wrp(i - 1, nx); jn = wrp(j + 1, ny); js = wrp(j - 1, ny);
+  }
+  auto T1 = [&](int jj, int ii2) { return ld(A.theta_s, ix3(k, jj, ii2, ny, nx)) - T0; };
+  const double th = T1(j, i);
+  const double v_flux = v_n * (T1(jn, i) + th) - v_s * (th + T1(js, i));
+  const double u_flux = u_e * (T1(j, ie) + th) - u_w * (th + T1(j, iw));
+  hdiv[c] = msftx * (0.5 * g.rdy * v_flux + 0.5 * g.rdx * u_flux);
+}
+
+// ---------------------------------------------------------------------------
 // Arguments of the column kernel (advance_mu_t + advance_w + calc_p_rho for
 // one substep, column_tiled.cuh).
 // ---------------------------------------------------------------------------

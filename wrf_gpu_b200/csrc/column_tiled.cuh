@@ -93,7 +93,9 @@ __device__ __forceinline__ void column_prefetch(const Grid &g, const Acoustic &A
 
 inline size_t column_tiled_smem_bytes(int nz) { return (size_t)COL_NARR * (nz + 1) * COL_TX * sizeof(double); }
 
-__global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(Grid g, Acoustic A, ColArgs c) {
+__global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(Grid g, Acoustic A, ColArgs c,
+                                                                               const double *dvdxi,
+                                                                               const double *hdiv) {
   extern __shared__ double sm[];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -127,21 +129,9 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   if (WG_COL_PREFETCH >= 1) column_prefetch(g, A, c, 0, blockIdx.x * COL_TX, j);
   if (WG_COL_PREFETCH == 1) column_prefetch(g, A, c, 1, blockIdx.x * COL_TX, j);
 
-  // ---------------- P1: dvdxi per level -> A0 ----------------
+  // ---------------- P1: dvdxi per level (from k_div_h) -> A0 ----------------
   if (active) {
-    const double muv_n = ld(A.muv, ix2(j + 1, i, nx)), muv_s = ld(A.muv, ix2(j, i, nx));
-    const double muu_e = ld(A.muu, ix2(j, i + 1, nxu)), muu_w = ld(A.muu, ix2(j, i, nxu));
-    const double fvi_n = ld(g.rmsfvx, ix2(j + 1, i, nx)), fvi_s = ld(g.rmsfvx, ix2(j, i, nx));  // 1/msfvx
-    const double fuy_e = ld(g.msfuy, ix2(j, i + 1, nxu)), fuy_w = ld(g.msfuy, ix2(j, i, nxu));
-    const double rfuy_e = ld(g.rmsfuy, ix2(j, i + 1, nxu)), rfuy_w = ld(g.rmsfuy, ix2(j, i, nxu));
-    for (int k = ty; k < nz; k += COL_TY) {
-      const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-      const double vn = ld(A.v, ix3(k, j + 1, i, nyv, nx)) + (c1 * muv_n + c2) * ld(A.v_1, ix3(k, j + 1, i, nyv, nx)) * fvi_n;
-      const double vs = ld(A.v, ix3(k, j, i, nyv, nx)) + (c1 * muv_s + c2) * ld(A.v_1, ix3(k, j, i, nyv, nx)) * fvi_s;
-      const double ue = ld(A.u, ix3(k, j, i + 1, ny, nxu)) + div_rcp((c1 * muu_e + c2) * ld(A.u_1, ix3(k, j, i + 1, ny, nxu)), fuy_e, rfuy_e);
-      const double uw = ld(A.u, ix3(k, j, i, ny, nxu)) + div_rcp((c1 * muu_w + c2) * ld(A.u_1, ix3(k, j, i, ny, nxu)), fuy_w, rfuy_w);
-      S(A0, k) = msftx * msfty * (g.rdy * (vn - vs) + g.rdx * (ue - uw));
-    }
+    for (int k = ty; k < nz; k += COL_TY) S(A0, k) = ld(dvdxi, M(k));
   }
   __syncthreads();
   // ---------------- P2: column sum and 2-D mass updates (serial, ty == 0) ----------------
@@ -229,12 +219,6 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   const double muave = valid ? A.muave[c2d] : 0.0;
   if (valid) {
     for (int k = ty; k <= nz; k += COL_TY) A.ww[M(k)] = S(A3, k);
-    int ie = 0, iw = 0, jn = 0, js = 0;
-    if (c.specified) {
-      ie = i + 1; iw = i - 1; jn = j + 1; js = j - 1;
-    } else {
-      ie = wrp(i + 1, nx); iw = wrp(i - 1, nx); jn = wrp(j + 1, ny); js = wrp(j - 1, ny);
-    }
     cp_async_wait<0>();  // this thread's staged levels
     for (int k = ty; k < nz; k += COL_TY) {
       double thw = S(A7, k);
@@ -244,10 +228,8 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
                                    ? S(A3, k + 1) * (ld(g.fnm, k + 1) * T1(k + 1, j, i) + ld(g.fnp, k + 1) * T1(k, j, i))
                                    : 0.0;
         const double wdtn_lo = (k >= 1) ? S(A3, k) * (ld(g.fnm, k) * T1(k, j, i) + ld(g.fnp, k) * T1(k - 1, j, i)) : 0.0;
-        const double th = T1(k, j, i);
-        const double v_flux = ld(A.v, ix3(k, j + 1, i, nyv, nx)) * (T1(k, jn, i) + th) - ld(A.v, ix3(k, j, i, nyv, nx)) * (th + T1(k, js, i));
-        const double u_flux = ld(A.u, ix3(k, j, i + 1, ny, nxu)) * (T1(k, j, ie) + th) - ld(A.u, ix3(k, j, i, ny, nxu)) * (th + T1(k, j, iw));
-        const double tend = msftx * (0.5 * g.rdy * v_flux + 0.5 * g.rdx * u_flux) + ld(g.rdnw, k) * (wdtn_hi - wdtn_lo);
+        // horizontal theta flux divergence from k_div_h (same expression)
+        const double tend = ld(hdiv, M(k)) + ld(g.rdnw, k) * (wdtn_hi - wdtn_lo);
         const double theta_i = thw + msfty * dts * S(A4, k);
         thw = theta_i - dts * msfty * tend;
         A.theta_w[M(k)] = thw;

@@ -69,7 +69,7 @@ struct Work {
   double *rmsftx, *rmsfty, *rmsfux, *rmsfuy, *rmsfvx, *rmsfvy;  // map-factor reciprocals
   // mass
   double *alt_raw, *alt, *pb, *c2a, *qtot, *al_ls, *php_ls, *php, *t_tend, *theta_w, *t2ave, *p, *pm1, *al;
-  double *s1, *s2, *ru, *rv;
+  double *s1, *s2, *ru, *rv, *dvdxi, *hdiv;
   double *qtend[6];
   // u / v faces
   double *u_tend, *u_w, *cqu, *u_target, *v_tend, *v_w, *cqv, *v_target;
@@ -93,6 +93,7 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   w.qtot = c.take(d.m); w.al_ls = c.take(d.m); w.php_ls = c.take(d.m); w.php = c.take(d.m);
   w.t_tend = c.take(d.m); w.theta_w = c.take(d.m); w.t2ave = c.take(d.m); w.p = c.take(d.m);
   w.pm1 = c.take(d.m); w.al = c.take(d.m); w.ru = c.take(d.m); w.rv = c.take(d.m);
+  w.dvdxi = c.take(d.m); w.hdiv = c.take(d.m);
   const bool lim = (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2 || p.moist_adv_opt == 1 || p.moist_adv_opt == 2);
   w.s1 = lim ? c.take(d.m) : nullptr;
   w.s2 = lim ? c.take(d.m) : nullptr;
@@ -256,7 +257,7 @@ ProfState g_prof;
 
 const char *kClassNames[] = {"k_recip_msf", "k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
                              "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_u",
-                             "k_advance_v", "k_column", "k_finish_u", "k_finish_v", "k_finish_col"};
+                             "k_advance_v", "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col"};
 constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
 
 int class_of(const char *name) {
@@ -424,7 +425,7 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
     if (s == 2 && (p->scalar_adv_opt == 1 || p->scalar_adv_opt == 2)) n += 2;
     if (s == 2 && (p->moist_adv_opt == 1 || p->moist_adv_opt == 2)) n += 12;
     if (bdy) n += 2;
-    n += 3 * nsub[s];
+    n += 4 * nsub[s];  // advance_u, advance_v, div_h, column
     n += 3;  // finish u, v, col
   }
   *launches = n;
@@ -663,8 +664,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       PROF("k_advance_v");
       k_advance_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
       LAUNCH_CHECK("k_advance_v");
+      PROF("k_div_h");
+      k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, specified ? 1 : 0, w.dvdxi, w.hdiv);
+      LAUNCH_CHECK("k_div_h");
       PROF("k_column");
-      k_column_tiled<<<dim3((nx + COL_TX - 1) / COL_TX, ny, 1), dim3(COL_TX, COL_TY, 1), col_smem, stream>>>(g, A, ca);
+      k_column_tiled<<<dim3((nx + COL_TX - 1) / COL_TX, ny, 1), dim3(COL_TX, COL_TY, 1), col_smem, stream>>>(g, A, ca, w.dvdxi,
+                                                                                                      w.hdiv);
       LAUNCH_CHECK("k_column");
     }
 
