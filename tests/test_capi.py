@@ -98,8 +98,8 @@ def test_launch_count(lib):
     n = ctypes.c_int(0)
     assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(n)) == 0
     # map-factor reciprocals + 3 stages x (8 stage + 3 finish)
-    # + 4 launches per substep x (1 + 3 + 6)
-    assert n.value == 1 + 3 * 11 + 4 * 10
+    # + 3 launches per substep x (1 + 3 + 6)
+    assert n.value == 1 + 3 * 11 + 3 * 10
 
 
 def test_null_pointers_rejected_before_any_launch(lib):

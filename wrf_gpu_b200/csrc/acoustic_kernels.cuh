@@ -1,8 +1,9 @@
 // Acoustic substep kernels (fp64) and the end-of-stage finish.
 //
 // One substep is three launches:
-//   k_advance_u / k_advance_v  -- advance_uv on every u / v face
+//   k_advance_uv               -- advance_uv on every u and v face
 //                                 (core/acoustic.py:626-786), face-parallel;
+//   k_div_h                    -- the horizontal divergences the columns need;
 //   k_column_tiled             -- advance_mu_t (dynamics/mu_t_advance.py),
 //                                 advance_w with its Thomas solve
 //                                 (core/advance_w.py:293-627) and calc_p_rho
@@ -78,14 +79,11 @@ __device__ __forceinline__ double relax_weight_v(int j, int i, int y_len, int x_
 }
 
 // ---------------------------------------------------------------------------
-// advance_uv, u faces (core/acoustic.py:626-735).
+// advance_uv, one u face (core/acoustic.py:626-735).
 // ---------------------------------------------------------------------------
-__global__ void k_advance_u(Grid g, Acoustic A, double dts, int top_lid, BdyArgs bdy) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z;
+__device__ __forceinline__ void advance_u_face(const Grid &g, const Acoustic &A, double dts, int top_lid,
+                                               const BdyArgs &bdy, int i, int j, int k) {
   const int nx = g.nx, ny = g.ny;
-  if (i > nx || j >= ny) return;
   const int nxu = nx + 1;
   const size_t cu = ix3(k, j, i, ny, nxu);
   const size_t f2 = ix2(j, i, nxu);
@@ -119,13 +117,10 @@ __global__ void k_advance_u(Grid g, Acoustic A, double dts, int top_lid, BdyArgs
   A.u[cu] = u;
 }
 
-// advance_uv, v faces (core/acoustic.py:737-750).
-__global__ void k_advance_v(Grid g, Acoustic A, double dts, int top_lid, BdyArgs bdy) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z;
+// advance_uv, one v face (core/acoustic.py:737-750).
+__device__ __forceinline__ void advance_v_face(const Grid &g, const Acoustic &A, double dts, int top_lid,
+                                               const BdyArgs &bdy, int i, int j, int k) {
   const int nx = g.nx, ny = g.ny;
-  if (i >= nx || j > ny) return;
   const int nyv = ny + 1;
   const size_t cv = ix3(k, j, i, nyv, nx);
   const size_t f2 = ix2(j, i, nx);
@@ -157,6 +152,18 @@ __global__ void k_advance_v(Grid g, Acoustic A, double dts, int top_lid, BdyArgs
     if (w != 0.0) v = v + w * (ld(bdy.v_target, cv) - v);
   }
   A.v[cv] = v;
+}
+
+// advance_uv on both face kinds of one (k, j, i): the u face at i (j < ny)
+// and the v face at j (i < nx).  The two faces read the same mass-point
+// neighbourhood (p, al, alt, pb, php, ph, muts, mut, mudf), so one thread
+// doing both halves those reads; index space (nx+1) x (ny+1) x nz.
+__global__ void k_advance_uv(Grid g, Acoustic A, double dts, int top_lid, BdyArgs bdy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i <= g.nx && j < g.ny) advance_u_face(g, A, dts, top_lid, bdy, i, j, k);
+  if (i < g.nx && j <= g.ny) advance_v_face(g, A, dts, top_lid, bdy, i, j, k);
 }
 
 // ---------------------------------------------------------------------------

@@ -256,8 +256,8 @@ struct ProfState {
 ProfState g_prof;
 
 const char *kClassNames[] = {"k_recip_msf", "k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
-                             "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_u",
-                             "k_advance_v", "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col"};
+                             "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_uv",
+                             "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col"};
 constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
 
 int class_of(const char *name) {
@@ -425,7 +425,7 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
     if (s == 2 && (p->scalar_adv_opt == 1 || p->scalar_adv_opt == 2)) n += 2;
     if (s == 2 && (p->moist_adv_opt == 1 || p->moist_adv_opt == 2)) n += 12;
     if (bdy) n += 2;
-    n += 4 * nsub[s];  // advance_u, advance_v, div_h, column
+    n += 3 * nsub[s];  // advance_uv, div_h, column
     n += 3;  // finish u, v, col
   }
   *launches = n;
@@ -658,12 +658,9 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         cudaFuncSetAttribute(k_column_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) != cudaSuccess)
       return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_column_tiled (nz too large)");
     for (int it = 0; it < nsub[stage]; ++it) {
-      PROF("k_advance_u");
-      k_advance_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
-      LAUNCH_CHECK("k_advance_u");
-      PROF("k_advance_v");
-      k_advance_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
-      LAUNCH_CHECK("k_advance_v");
+      PROF("k_advance_uv");
+      k_advance_uv<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
+      LAUNCH_CHECK("k_advance_uv");
       PROF("k_div_h");
       k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, specified ? 1 : 0, w.dvdxi, w.hdiv);
       LAUNCH_CHECK("k_div_h");

@@ -12,11 +12,15 @@ Per kernel (each logically touched array counted once per launch, halo
 re-reads excluded):
 
 * ``k_column`` -- advance_mu_t + advance_w + calc_p_rho on one column: reads
-  u, v, u_1, v_1, theta_1, t_2, t_tend, ww_1, w, ph, ph_1+phb, ph_tend, c2a,
-  alt, cqw, rw_tend, a, alpha, gamma, t_2ave, pm1 (21) [+ w_save with
-  damp_opt 3], writes t_2, ww, w, ph, t_2ave, p, pm1, al (8): 232 (240) B/cell.
-* ``k_advance_u`` / ``k_advance_v`` -- advance_uv on one face: reads u, u_tend,
-  cqu, ph, p, alt, al, pb, php (9), writes u (1): 80 B/face.
+  dvdxi, theta flux divergence, theta_1, t_2, t_tend, ww_1, w, ph, ph_1+phb,
+  ph_tend, c2a, alt, cqw, rw_tend, a, alpha, gamma, t_2ave, pm1 (19) [+ w_save
+  with damp_opt 3], writes t_2, ww, w, ph, t_2ave, p, pm1, al (8): 216 (224)
+  B/cell.
+* ``k_advance_uv`` -- advance_uv on the u and v faces: per face reads u (v),
+  u_tend (v_tend), cqu (cqv) and writes u (v): 32 B/face; per cell reads the
+  mass-point planes ph, p, alt, al, pb, php once: 48 B/cell.
+* ``k_div_h`` -- the column-coupling horizontal divergences: reads u, v, u_1,
+  v_1, theta_1 (5), writes dvdxi and the theta flux divergence (2): 56 B/cell.
 """
 
 from __future__ import annotations
@@ -40,9 +44,10 @@ def step_bytes(nx: int, ny: int, nz: int, ns: int, moist: bool) -> float:
 def kernel_bytes_per_launch(name: str, nx: int, ny: int, nz: int, damp_opt: int = 0) -> float | None:
     cells = nx * ny * nz
     if name == "k_column":
-        return float(cells) * (240 if damp_opt == 3 else 232)
-    if name == "k_advance_u":
-        return float(nz * ny * (nx + 1)) * 80
-    if name == "k_advance_v":
-        return float(nz * (ny + 1) * nx) * 80
+        return float(cells) * (224 if damp_opt == 3 else 216)
+    if name == "k_advance_uv":
+        faces = nz * ny * (nx + 1) + nz * (ny + 1) * nx
+        return float(faces) * 32 + float(cells) * 48
+    if name == "k_div_h":
+        return float(cells) * 56
     return None
