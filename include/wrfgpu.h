@@ -82,6 +82,12 @@ typedef struct wrfgpu_step_params {
    * (core/rk_addtend_dry.py:282-288): cfn = (0.5*dnw[nz-1] + dn[nz-1])/dn[nz-1],
    * cfn1 = -0.5*dnw[nz-1]/dn[nz-1] */
   double cfn, cfn1;
+  /* Kernel tile shapes (no counterpart in the reference; results do not
+   * depend on them): levels per block of the level-marching stencil kernels
+   * (1..nz) and level lanes of the column kernel (8, 13 or 16); 0 selects the
+   * built-in defaults (10 and 13).  wrfgpu_autotune picks them per grid. */
+  int march_levels;
+  int column_lanes;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */
@@ -165,6 +171,27 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *params, const wrfgpu_metrics *metr
 int wrfgpu_rk3_step_static_workspace(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
                                      const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
                                      double lead_seconds, cudaStream_t stream);
+
+/* Advance n independent domains (ensemble members or nest levels, of any
+ * sizes) by one RK3 step each: member m is wrfgpu_rk3_step(&params[m],
+ * &metrics[m], &in[m], &out[m], lead_seconds[m], workspace[m],
+ * workspace_bytes[m], .).  Members are forked onto a pool of library-owned
+ * streams behind `stream` and joined back into it, so they run concurrently
+ * and a capture of `stream` records them as parallel graph branches.  The
+ * pool is created by the first call on a device; make that call before any
+ * stream capture.  Replaces the reference's separate per-domain
+ * _rk_scan_step calls (nests and ensemble members each call it). */
+int wrfgpu_rk3_step_batched(int n, const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                            const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
+                            const double *lead_seconds, void *const *workspace, const size_t *workspace_bytes,
+                            cudaStream_t stream);
+
+/* Time the tile-shape candidates on this grid (each a few full steps from
+ * `in` into `out`, which are overwritten) and write the fastest to
+ * params->march_levels / params->column_lanes.  No counterpart in the
+ * reference.  Synchronises `stream`; call it outside stream capture. */
+int wrfgpu_autotune(wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const wrfgpu_step_inputs *in,
+                    const wrfgpu_step_outputs *out, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);

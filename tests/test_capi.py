@@ -66,6 +66,8 @@ def _params(lib, **kw):
     (dict(run_boundary=1, bc_ideal=0, h_sca_adv_order=5), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(run_boundary=1, relax_zone=6), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(precision=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(column_lanes=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(march_levels=-1), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
 ])
 def test_validate_rejects(lib, kw, code):
     p = _params(lib, **kw)
@@ -76,6 +78,22 @@ def test_validate_rejects(lib, kw, code):
 def test_validate_accepts_reference_defaults(lib):
     p = _params(lib)
     assert lib.wrfgpu_step_params_validate(ctypes.byref(p)) == 0
+
+
+def test_batched_rejects_bad_members_before_any_launch(lib):
+    p = _params(lib)
+    P = (_capi.StepParams * 2)(_params(lib, nz=2), p)
+    M = (_capi.Metrics * 2)()
+    I = (_capi.StepInputs * 2)()
+    O = (_capi.StepOutputs * 2)()
+    L = (ctypes.c_double * 2)(0.0, 0.0)
+    W = (ctypes.c_void_p * 2)(None, None)
+    B = (ctypes.c_size_t * 2)(0, 0)
+    assert lib.wrfgpu_rk3_step_batched(2, P, M, I, O, L, W, B, None) == _capi.WRFGPU_ERR_BAD_SHAPE
+    P2 = (_capi.StepParams * 2)(p, p)
+    assert lib.wrfgpu_rk3_step_batched(2, P2, M, I, O, L, W, B, None) == _capi.WRFGPU_ERR_WORKSPACE
+    assert lib.wrfgpu_rk3_step_batched(-1, P, M, I, O, L, W, B, None) == _capi.WRFGPU_ERR_BAD_SHAPE
+    assert lib.wrfgpu_rk3_step_batched(0, P, M, I, O, L, W, B, None) == 0
 
 
 def test_validate_accepts_mixed_precision(lib):

@@ -41,6 +41,7 @@ class StepParams(ctypes.Structure):
         ("moist_cqw", _I), ("w_coriolis", _I), ("precision", _I),
         ("cf1", _D), ("cf2", _D), ("cf3", _D), ("p_top", _D),
         ("cfn", _D), ("cfn1", _D),
+        ("march_levels", _I), ("column_lanes", _I),
     ]
 
 
@@ -73,7 +74,8 @@ class StepOutputs(ctypes.Structure):
 
 
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
-            "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace",
+            "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version")
 
@@ -105,6 +107,13 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_rk3_step_static_workspace.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
                                                      ctypes.POINTER(StepInputs), ctypes.POINTER(StepOutputs), _D, _P]
     lib.wrfgpu_rk3_step_static_workspace.restype = _I
+    lib.wrfgpu_rk3_step_batched.argtypes = [_I, ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
+                                            ctypes.POINTER(StepInputs), ctypes.POINTER(StepOutputs),
+                                            ctypes.POINTER(_D), ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t), _P]
+    lib.wrfgpu_rk3_step_batched.restype = _I
+    lib.wrfgpu_autotune.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), ctypes.POINTER(StepInputs),
+                                    ctypes.POINTER(StepOutputs), _P, ctypes.c_size_t, _P]
+    lib.wrfgpu_autotune.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

@@ -16,8 +16,9 @@
 
 namespace wg {
 
-// Block shape: COL_TX columns x COL_TY level lanes; COL_MINB resident blocks
-// per SM requested from the register allocator.
+// Block shape: COL_TX columns x TY level lanes (a template parameter, tuned
+// per grid; COL_TY is the default); COL_MINB resident blocks per SM requested
+// from the register allocator.
 #ifndef WG_COL_TX
 #define WG_COL_TX 32
 #endif
@@ -35,7 +36,8 @@ namespace wg {
 constexpr int COL_TX = WG_COL_TX;
 constexpr int COL_TY = WG_COL_TY;
 constexpr int COL_NARR = 8;
-static_assert(COL_TY >= 2, "the Thomas phase needs a second warp row to stage gamma");
+// Level-lane counts the column kernel is instantiated for (the tuner's choices).
+constexpr int COL_TY_CHOICES[] = {8, 13, 16};
 
 // Bulk L2 prefetch of the rows (levels 0..nz) this column block will read.
 // group 0: advance_mu_t / theta / t_2ave inputs; group 1: advance_w and
@@ -93,9 +95,11 @@ __device__ __forceinline__ void column_prefetch(const Grid &g, const Acoustic &A
 
 inline size_t column_tiled_smem_bytes(int nz) { return (size_t)COL_NARR * (nz + 1) * COL_TX * sizeof(double); }
 
-__global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(Grid g, Acoustic A, ColArgs c,
+template <int TY>
+__global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid g, Acoustic A, ColArgs c,
                                                                                const double *dvdxi,
                                                                                const double *hdiv) {
+  static_assert(TY >= 2, "the Thomas phase needs a second warp row to stage gamma");
   extern __shared__ double sm[];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -131,7 +135,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
 
   // ---------------- P1: dvdxi per level (from k_div_h) -> A0 ----------------
   if (active) {
-    for (int k = ty; k < nz; k += COL_TY) S(A0, k) = ld(dvdxi, M(k));
+    for (int k = ty; k < nz; k += TY) S(A0, k) = ld(dvdxi, M(k));
   }
   __syncthreads();
   // ---------------- P2: column sum and 2-D mass updates (serial, ty == 0) ----------------
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   // thread that will use it: theta_w -> A7 (kept to P10), old t_2ave -> A6
   // and t_tend -> A4 (both free until P6/P7).
   if (valid) {
-    for (int k = ty; k < nz; k += COL_TY) {
+    for (int k = ty; k < nz; k += TY) {
       cp_async8(&S(A7, k), A.theta_w + M(k));
       cp_async8(&S(A6, k), A.t2ave + M(k));
       cp_async8(&S(A4, k), A.t_tend + M(k));
@@ -189,15 +193,15 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   if (valid) {
     if (active) {
       const double dmdt = s_dmdt[tx], mu_tend = s_mutend[tx], scale = s_scale[tx];
-      for (int kk = 1 + ty; kk < nz; kk += COL_TY) {
+      for (int kk = 1 + ty; kk < nz; kk += TY) {
         const int k = kk - 1;
         double dv = S(A0, k);
         if (c.specified) dv = dv * scale;
         S(A1, kk) = div_rcp(ld(g.dnw, k) * (ld(g.c1h, k) * dmdt + dv + ld(g.c1h, k) * mu_tend), msfty, minv);
       }
-      for (int k = ty; k <= nz; k += COL_TY) S(A2, k) = ld(A.ww_1, M(k));
+      for (int k = ty; k <= nz; k += TY) S(A2, k) = ld(A.ww_1, M(k));
     } else {
-      for (int k = ty; k <= nz; k += COL_TY) S(A3, k) = A.ww[M(k)];
+      for (int k = ty; k <= nz; k += TY) S(A3, k) = A.ww[M(k)];
     }
   }
   __syncthreads();
@@ -218,9 +222,9 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   const double muts = valid ? A.muts[c2d] : 1.0;
   const double muave = valid ? A.muave[c2d] : 0.0;
   if (valid) {
-    for (int k = ty; k <= nz; k += COL_TY) A.ww[M(k)] = S(A3, k);
+    for (int k = ty; k <= nz; k += TY) A.ww[M(k)] = S(A3, k);
     cp_async_wait<0>();  // this thread's staged levels
-    for (int k = ty; k < nz; k += COL_TY) {
+    for (int k = ty; k < nz; k += TY) {
       double thw = S(A7, k);
       const double t2ave_old = S(A6, k);
       if (active) {
@@ -250,7 +254,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   // ---------------- P6: rhs -> A2 (faces 1..nz), old ph -> A4 (faces 0..nz) ----------------
   const double c05gem = 0.5 * G * eps_m;
   if (valid) {
-    for (int f = ty; f <= nz; f += COL_TY) {
+    for (int f = ty; f <= nz; f += TY) {
       const double phf = ld(A.ph, M(f));
       S(A4, f) = phf;
       if (f == 0) {
@@ -270,7 +274,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   if (valid) {
     const double c05dg = 0.5 * dts * G;
     const double dtsg = dts * G;
-    for (int f = ty; f <= nz; f += COL_TY) {
+    for (int f = ty; f <= nz; f += TY) {
       const double a_f = ld(A.a, M(f)), alpha_f = ld(A.alpha, M(f));
       double wn;
       if (f == 0) {
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
       }
     }
   } else if (valid) {
-    for (int f = ty - 1; f <= nz; f += COL_TY - 1) S(A5, f) = ld(A.gamma, M(f));
+    for (int f = ty - 1; f <= nz; f += TY - 1) S(A5, f) = ld(A.gamma, M(f));
   }
   __syncthreads();
   // ---------------- P8b: Thomas back substitution (serial) ----------------
@@ -358,7 +362,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
       dampmag = dts * c.dampcoef;
       hbot = div_rcp(ld(A.pt1, M(nz)), G, RG) - c.zdamp;
     }
-    for (int f = ty; f <= nz; f += COL_TY) {
+    for (int f = ty; f <= nz; f += TY) {
       double ws = S(A6, f);
       if (f >= 1) {
         if (do_damp) {
@@ -381,7 +385,7 @@ __global__ void __launch_bounds__(COL_TX * COL_TY, WG_COL_MINB) k_column_tiled(G
   // ---------------- P10: calc_p_rho with smdiv memory ----------------
   if (valid) {
     const double mu_work = muts - mut;
-    for (int k = ty; k < nz; k += COL_TY) {
+    for (int k = ty; k < nz; k += TY) {
       const double mass = ld(g.c1h, k) * muts + ld(g.c2h, k);
       const double safe = safe12(mass);
       const double mu_term = ld(g.c1h, k) * mu_work;

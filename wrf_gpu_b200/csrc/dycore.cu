@@ -398,6 +398,9 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "boundary zones other than spec_zone=1, relax_zone=4 are not built");
   if (p->precision != WRFGPU_PRECISION_FP64 && p->precision != WRFGPU_PRECISION_MIXED)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "unknown precision mode");
+  if (p->march_levels < 0) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "march_levels must be >= 0");
+  if (p->column_lanes != 0 && p->column_lanes != 8 && p->column_lanes != 13 && p->column_lanes != 16)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13 or 16");
   return WRFGPU_OK;
 }
 
@@ -477,6 +480,8 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   const bool specified = p.run_boundary && !p.bc_ideal;
   const double dt = p.dt;
   const int ns = p.acoustic_substeps;
+  const int kc = (p.march_levels > 0) ? (p.march_levels < nz ? p.march_levels : nz) : MARCH_KC;
+  const int lanes = (p.column_lanes > 0) ? p.column_lanes : COL_TY;
   const double dt_rk[3] = {dt / 3.0, 0.5 * dt, dt};
   const double dts_rk[3] = {dt / 3.0, dt / (double)ns, dt / (double)ns};
   const int nsub[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
@@ -571,9 +576,9 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     PROF("k_mass");
     {
       const int nfields = 1 + ((moist && !lim_moist) ? 6 : 0);
-      const int nchunk = march_nchunk(nz);
+      const int nchunk = march_nchunk(nz, kc);
       kScalar<<<tgrd(nx, ny, nfields * nchunk), tblk(), 0, stream>>>(
-          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, mo);
+          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, kc, mo);
     }
     LAUNCH_CHECK("k_mass");
     if (lim_theta || lim_moist) {
@@ -584,12 +589,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
         PROF("k_lim_scale");
-        kLimScale<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
-            g, la, s.theta, origin.theta, w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
+        kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
+            g, la, s.theta, origin.theta, w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr, kc);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
-        kLimTend<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
-            g, la, s.theta, origin.theta, nullptr, nullptr, w.s1, w.s2, in->base_theta, s.mu_total, w.t_tend);
+        kLimTend<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
+            g, la, s.theta, origin.theta, nullptr, nullptr, w.s1, w.s2, in->base_theta, s.mu_total, w.t_tend, kc);
         LAUNCH_CHECK("k_lim_tend");
       }
       if (lim_moist) {
@@ -597,12 +602,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.offset = 0.0;
         for (int q = 0; q < 6; ++q) {
           PROF("k_lim_scale");
-          kLimScale<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
-              g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
+          kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
+              g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr, kc);
           LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
-          kLimTend<<<tgrd(nx, ny, march_nchunk(nz)), tblk(), 0, stream>>>(
-              g, la, s.q[q], origin.q[q], nullptr, nullptr, w.s1, w.s2, nullptr, s.mu_total, w.qtend[q]);
+          kLimTend<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
+              g, la, s.q[q], origin.q[q], nullptr, nullptr, w.s1, w.s2, nullptr, s.mu_total, w.qtend[q], kc);
           LAUNCH_CHECK("k_lim_tend");
         }
       }
@@ -654,8 +659,9 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp,
                (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0};
     const size_t col_smem = column_tiled_smem_bytes(nz);
-    if (stage == 0 &&
-        cudaFuncSetAttribute(k_column_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) != cudaSuccess)
+    auto kColumn = (lanes == 8) ? k_column_tiled<8> : (lanes == 16) ? k_column_tiled<16> : k_column_tiled<13>;
+    if (stage == 0 && cudaFuncSetAttribute(kColumn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) !=
+                          cudaSuccess)
       return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_column_tiled (nz too large)");
     for (int it = 0; it < nsub[stage]; ++it) {
       PROF("k_advance_uv");
@@ -665,7 +671,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, specified ? 1 : 0, w.dvdxi, w.hdiv);
       LAUNCH_CHECK("k_div_h");
       PROF("k_column");
-      k_column_tiled<<<dim3((nx + COL_TX - 1) / COL_TX, ny, 1), dim3(COL_TX, COL_TY, 1), col_smem, stream>>>(g, A, ca, w.dvdxi,
+      kColumn<<<dim3((nx + COL_TX - 1) / COL_TX, ny, 1), dim3(COL_TX, lanes, 1), col_smem, stream>>>(g, A, ca, w.dvdxi,
                                                                                                       w.hdiv);
       LAUNCH_CHECK("k_column");
     }
@@ -760,4 +766,145 @@ extern "C" int wrfgpu_rk3_step_static_workspace(const wrfgpu_step_params *pp, co
     ws = g_static_ws_addr[dev];
   }
   return wrfgpu_rk3_step(pp, mm, in, out, lead_seconds, ws, WRFGPU_STATIC_WORKSPACE_BYTES, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Batched step: members forked onto a per-device pool of library streams.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kPoolStreams = 8;
+constexpr int kMaxPoolDevices = 64;
+struct StreamPool {
+  cudaStream_t s[kPoolStreams];
+  cudaEvent_t fork;
+  cudaEvent_t join[kPoolStreams];
+  bool ready = false;
+};
+std::mutex g_pool_mutex;
+StreamPool g_pools[kMaxPoolDevices];
+
+int pool_for_current_device(StreamPool **out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "cudaGetDevice failed");
+  if (dev < 0 || dev >= kMaxPoolDevices) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  StreamPool &p = g_pools[dev];
+  if (!p.ready) {
+    if (cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "cannot create the batch fork event");
+    for (int k = 0; k < kPoolStreams; ++k) {
+      if (cudaStreamCreateWithFlags(&p.s[k], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&p.join[k], cudaEventDisableTiming) != cudaSuccess)
+        return fail(WRFGPU_ERR_CUDA, "cannot create the batch stream pool");
+    }
+    p.ready = true;
+  }
+  *out = &p;
+  return WRFGPU_OK;
+}
+}  // namespace
+
+extern "C" int wrfgpu_rk3_step_batched(int n, const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                                       const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
+                                       const double *lead_seconds, void *const *workspace,
+                                       const size_t *workspace_bytes, cudaStream_t stream) {
+  if (n < 0) return fail(WRFGPU_ERR_BAD_SHAPE, "n must be >= 0");
+  if (n == 0) return WRFGPU_OK;
+  if (params == nullptr || metrics == nullptr || in == nullptr || out == nullptr || lead_seconds == nullptr ||
+      workspace == nullptr || workspace_bytes == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "a batch array is NULL");
+  // validate every member before enqueueing anything
+  for (int m = 0; m < n; ++m) {
+    int rc = wrfgpu_step_params_validate(&params[m]);
+    if (rc) return rc;
+    size_t need = 0;
+    wrfgpu_step_workspace_size(&params[m], &need);
+    if (workspace[m] == nullptr || workspace_bytes[m] < need)
+      return fail(WRFGPU_ERR_WORKSPACE, "member " + std::to_string(m) + ": workspace is NULL or too small");
+  }
+  if (n == 1) return wrfgpu_rk3_step(&params[0], &metrics[0], &in[0], &out[0], lead_seconds[0], workspace[0],
+                                     workspace_bytes[0], stream);
+  StreamPool *pool = nullptr;
+  int rc = pool_for_current_device(&pool);
+  if (rc) return rc;
+  const int used = n < kPoolStreams ? n : kPoolStreams;
+  if (cudaEventRecord(pool->fork, stream) != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "fork record failed");
+  for (int k = 0; k < used; ++k)
+    if (cudaStreamWaitEvent(pool->s[k], pool->fork, 0) != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "fork wait failed");
+  int first_err = WRFGPU_OK;
+  std::string first_msg;
+  for (int m = 0; m < n; ++m) {
+    rc = wrfgpu_rk3_step(&params[m], &metrics[m], &in[m], &out[m], lead_seconds[m], workspace[m], workspace_bytes[m],
+                         pool->s[m % kPoolStreams]);
+    if (rc && first_err == WRFGPU_OK) {
+      first_err = rc;
+      first_msg = "member " + std::to_string(m) + ": " + g_last_error;
+    }
+  }
+  // always join, so `stream` never runs ahead of (or leaves dangling) member work
+  for (int k = 0; k < used; ++k) {
+    if (cudaEventRecord(pool->join[k], pool->s[k]) != cudaSuccess ||
+        cudaStreamWaitEvent(stream, pool->join[k], 0) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "join failed");
+  }
+  if (first_err) return fail(first_err, first_msg);
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tile-shape tuner: times whole steps for the candidate shapes on this grid.
+// ---------------------------------------------------------------------------
+extern "C" int wrfgpu_autotune(wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const wrfgpu_step_inputs *in,
+                               const wrfgpu_step_outputs *out, void *workspace, size_t workspace_bytes,
+                               cudaStream_t stream) {
+  if (pp == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params is NULL");
+  int rc = wrfgpu_step_params_validate(pp);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return fail(WRFGPU_ERR_CUDA, "cannot create timing events");
+  auto time_steps = [&](const wrfgpu_step_params &p, float *ms) -> int {
+    int r = wrfgpu_rk3_step(&p, mm, in, out, NAN, workspace, workspace_bytes, stream);  // warm-up
+    if (r) return r;
+    cudaEventRecord(e0, stream);
+    for (int t = 0; t < 3 && r == WRFGPU_OK; ++t)
+      r = wrfgpu_rk3_step(&p, mm, in, out, NAN, workspace, workspace_bytes, stream);
+    cudaEventRecord(e1, stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "timing synchronise failed");
+    cudaEventElapsedTime(ms, e0, e1);
+    return r;
+  };
+  wrfgpu_step_params best = *pp;
+  float best_ms = 1e30f;
+  // column lanes first (march levels at the default), then march levels
+  const int lanes_c[] = {8, 13, 16};
+  for (int l : lanes_c) {
+    wrfgpu_step_params p = *pp;
+    p.column_lanes = l;
+    p.march_levels = 0;
+    float ms = 0.f;
+    rc = time_steps(p, &ms);
+    if (rc) break;
+    if (ms < best_ms) { best_ms = ms; best = p; }
+  }
+  const int nz = pp->nz;
+  const int march_c[] = {5, 10, 17, 25, nz};
+  for (int kcand : march_c) {
+    if (rc) break;
+    if (kcand < 1 || kcand > nz) continue;
+    wrfgpu_step_params p = best;
+    p.march_levels = kcand;
+    float ms = 0.f;
+    rc = time_steps(p, &ms);
+    if (rc) break;
+    if (ms < best_ms) { best_ms = ms; best = p; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  pp->column_lanes = best.column_lanes;
+  pp->march_levels = best.march_levels;
+  g_last_error.clear();
+  return WRFGPU_OK;
 }

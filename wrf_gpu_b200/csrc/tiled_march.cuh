@@ -55,11 +55,8 @@ __device__ __forceinline__ P pick6(const P (&p)[6], int n) {
   return r;
 }
 
-// Levels per marching block.
-#ifndef WG_MARCH_KC
-#define WG_MARCH_KC 10
-#endif
-constexpr int MARCH_KC = WG_MARCH_KC;
+// Default levels per marching block (the tuner may choose others).
+constexpr int MARCH_KC = 10;
 
 // ---------------------------------------------------------------------------
 // Plain h5/v3 scalar advection (flux_advection.py:482-568) of theta and the
@@ -73,7 +70,7 @@ template <typename F>
 __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s, StateR ref, const double *ru,
                                                                 const double *rv, const double *rom, const double *mut,
                                                                 const double *muts0, const double *base_theta,
-                                                                int theta_plain, int nfields, MassOut o) {
+                                                                int theta_plain, int nfields, int kc, MassOut o) {
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
@@ -88,7 +85,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY;
   const int chunk = blockIdx.z / nfields, field = blockIdx.z - chunk * nfields;
-  const int k0 = chunk * MARCH_KC, k1 = min(nz, k0 + MARCH_KC);
+  const int k0 = chunk * kc, k1 = min(nz, k0 + kc);
   const int i = i0 + tx, j = j0 + ty;
   const bool valid = i < nx && j < ny;
   const double *fld = (field == 0) ? s.theta : pick6(s.q, field - 1);
@@ -179,7 +176,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
   }
 }
 
-inline int march_nchunk(int nz) { return (nz + MARCH_KC - 1) / MARCH_KC; }
+inline int march_nchunk(int nz, int kc) { return (nz + kc - 1) / kc; }
 
 // ---------------------------------------------------------------------------
 // PD / monotonic limited scalar advection (flux_advection.py:736-1000),
@@ -204,12 +201,12 @@ template <bool TEND, typename F>
 __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const double *field,
                                                          const double *field_old, double *s1w, double *s2w,
                                                          const double *s1r, const double *s2r, const double *base,
-                                                         const double *mu_total_stage, double *tend_out) {
+                                                         const double *mu_total_stage, double *tend_out, int kc) {
   __shared__ LimMarchSmem<TEND> sm;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY;
-  const int k0 = blockIdx.z * MARCH_KC, k1 = min(nz, k0 + MARCH_KC);
+  const int k0 = blockIdx.z * kc, k1 = min(nz, k0 + kc);
   const int i = i0 + tx, j = j0 + ty;
   const bool valid = i < nx && j < ny;
   const size_t plane = (size_t)ny * nx;

@@ -343,8 +343,8 @@ class Stepper:
                                 muts=e(s.mu_total), ph_tend=e(s.w), u_save=e(s.u), v_save=e(s.v), w_save=e(s.w),
                                 t_save=e(s.theta), ph_save=e(s.w), mu_save=e(s.mu_total), ww_save=e(s.w))
 
-    def step_into(self, carry: OperationalCarry, out: OperationalCarry, lead_seconds=None, stream=None) -> None:
-        """Enqueue one step from ``carry`` into the preallocated ``out`` (no sync)."""
+    def _structs(self, carry: OperationalCarry, out: OperationalCarry):
+        """C input/output structs for one step from ``carry`` into ``out``."""
         s, o, nl = carry.state, out.state, self.nl
         ins = _capi.StepInputs()
         for n in STATE_FIELDS:
@@ -366,12 +366,57 @@ class Stepper:
             outs.q[k_] = _ptr(getattr(o, n)) if have_q else None
         for n in CARRY_FIELDS:
             setattr(outs, n, _ptr(getattr(out, n)))
+        return ins, outs
+
+    def step_into(self, carry: OperationalCarry, out: OperationalCarry, lead_seconds=None, stream=None) -> None:
+        """Enqueue one step from ``carry`` into the preallocated ``out`` (no sync)."""
+        ins, outs = self._structs(carry, out)
         lead = float("nan") if lead_seconds is None else float(lead_seconds)
         st = torch.cuda.current_stream() if stream is None else stream
         rc = self.lib.wrfgpu_rk3_step(ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(ins),
                                       ctypes.byref(outs), lead, ctypes.c_void_p(self.workspace.data_ptr()),
                                       ctypes.c_size_t(self.workspace.numel()), ctypes.c_void_p(st.cuda_stream))
         _capi.check(rc)
+
+    def autotune(self, carry: OperationalCarry, out: OperationalCarry, stream=None) -> tuple[int, int]:
+        """Pick the kernel tile shapes for this grid by timing candidates
+        (overwrites ``out``; synchronises).  Returns (march_levels, column_lanes)."""
+        ins, outs = self._structs(carry, out)
+        st = torch.cuda.current_stream() if stream is None else stream
+        _capi.check(self.lib.wrfgpu_autotune(ctypes.byref(self.params), ctypes.byref(self.metrics),
+                                             ctypes.byref(ins), ctypes.byref(outs),
+                                             ctypes.c_void_p(self.workspace.data_ptr()),
+                                             ctypes.c_size_t(self.workspace.numel()), ctypes.c_void_p(st.cuda_stream)))
+        return int(self.params.march_levels), int(self.params.column_lanes)
+
+
+class BatchStepper:
+    """Several independent domains (ensemble members, nest levels; any sizes)
+    advanced together by ``wrfgpu_rk3_step_batched``: one call per step,
+    members running concurrently on the library's stream pool."""
+
+    def __init__(self, namelists, device="cuda"):
+        self.steppers = [Stepper(nl, device=device) for nl in namelists]
+        self.lib = _capi.load()
+
+    def alloc_carries(self, likes):
+        return [s.alloc_carry(c) for s, c in zip(self.steppers, likes)]
+
+    def step_into(self, carries, outs, lead_seconds=None, stream=None) -> None:
+        n = len(self.steppers)
+        if len(carries) != n or len(outs) != n:
+            raise ValueError("one carry and one output per member")
+        P = (_capi.StepParams * n)(*[s.params for s in self.steppers])
+        M = (_capi.Metrics * n)(*[s.metrics for s in self.steppers])
+        pairs = [s._structs(c, o) for s, c, o in zip(self.steppers, carries, outs)]
+        I = (_capi.StepInputs * n)(*[p[0] for p in pairs])
+        O = (_capi.StepOutputs * n)(*[p[1] for p in pairs])
+        leads = lead_seconds if isinstance(lead_seconds, (list, tuple)) else [lead_seconds] * n
+        L = (ctypes.c_double * n)(*[float("nan") if x is None else float(x) for x in leads])
+        W = (ctypes.c_void_p * n)(*[s.workspace.data_ptr() for s in self.steppers])
+        B = (ctypes.c_size_t * n)(*[s.workspace.numel() for s in self.steppers])
+        st = torch.cuda.current_stream() if stream is None else stream
+        _capi.check(self.lib.wrfgpu_rk3_step_batched(n, P, M, I, O, L, W, B, ctypes.c_void_p(st.cuda_stream)))
 
 
 _STEPPERS: dict[int, Stepper] = {}
