@@ -173,6 +173,7 @@ def run_gpu(args, rank, world, local_rank):
     stp = dycore.Stepper(nl, device=dev)
     out = stp.alloc_carry(carry)
     stream = torch.cuda.current_stream(dev)
+    tuned = stp.autotune(carry, out) if not args.no_tune else (0, 0)
     ns = nl.acoustic_substeps
     nsub = perfmodel.substeps_per_step(ns)
     cells = nx * ny * nz
@@ -296,6 +297,7 @@ def run_gpu(args, rank, world, local_rank):
         nl_m = dycore.OperationalNamelist.from_case(case, device=dev, precision="mixed")
         stp_m = dycore.Stepper(nl_m, device=dev)
         out_m = stp_m.alloc_carry(carry)
+        stp_m.params.march_levels, stp_m.params.column_lanes = stp.params.march_levels, stp.params.column_lanes
 
         def step_m():
             stp_m.step_into(carry, out_m, lead_seconds=0.0)
@@ -342,7 +344,8 @@ def run_gpu(args, rank, world, local_rank):
     return dict(value=value, ms_per_step=ms_per_step, clocks=clk, roofline=roof, whole_step_roofline=whole,
                 kernels=kernels, e2e={"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                                       "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e},
-                launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed)
+                launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed,
+                tuned={"march_levels": tuned[0], "column_lanes": tuned[1]})
 
 
 def main():
@@ -357,6 +360,7 @@ def main():
     ap.add_argument("--nz", type=int, default=NZ)
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--no-mixed", action="store_true", help="skip timing the mixed-precision variant")
+    ap.add_argument("--no-tune", action="store_true", help="skip the tile-shape tuner (built-in defaults)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -405,7 +409,7 @@ def main():
                 "data": "synthetic",
                 "config": {"workload": workload, "nx": args.nx, "ny": args.ny, "nz": args.nz,
                            "substeps_per_step": 10, "l2": "inputs larger than L2 (no flush)",
-                           "parallelism": f"replicas x{world}", "cuda_graph": True},
+                           "parallelism": f"replicas x{world}", "cuda_graph": True, "tile_shapes": r["tuned"]},
                 "e2e": r["e2e"], "roofline": r["roofline"], "whole_step_roofline": r["whole_step_roofline"],
                 "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": r["launches"],
                 "kernels": r["kernels"], "finite": r["finite"], "mixed": r["mixed"]}

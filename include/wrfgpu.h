@@ -84,7 +84,7 @@ typedef struct wrfgpu_step_params {
   double cfn, cfn1;
   /* Kernel tile shapes (no counterpart in the reference; results do not
    * depend on them): levels per block of the level-marching stencil kernels
-   * (1..nz) and level lanes of the column kernel (8, 13 or 16); 0 selects the
+   * (5, 10 or 25) and level lanes of the column kernel (8, 13 or 16); 0 selects the
    * built-in defaults (10 and 13).  wrfgpu_autotune picks them per grid. */
   int march_levels;
   int column_lanes;

@@ -398,7 +398,8 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "boundary zones other than spec_zone=1, relax_zone=4 are not built");
   if (p->precision != WRFGPU_PRECISION_FP64 && p->precision != WRFGPU_PRECISION_MIXED)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "unknown precision mode");
-  if (p->march_levels < 0) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "march_levels must be >= 0");
+  if (p->march_levels != 0 && p->march_levels != 5 && p->march_levels != 10 && p->march_levels != 25)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "march_levels must be 0, 5, 10 or 25");
   if (p->column_lanes != 0 && p->column_lanes != 8 && p->column_lanes != 13 && p->column_lanes != 16)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13 or 16");
   return WRFGPU_OK;
@@ -480,7 +481,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   const bool specified = p.run_boundary && !p.bc_ideal;
   const double dt = p.dt;
   const int ns = p.acoustic_substeps;
-  const int kc = (p.march_levels > 0) ? (p.march_levels < nz ? p.march_levels : nz) : MARCH_KC;
+  const int kc = (p.march_levels == 5 || p.march_levels == 25) ? p.march_levels : MARCH_KC;
   const int lanes = (p.column_lanes > 0) ? p.column_lanes : COL_TY;
   const double dt_rk[3] = {dt / 3.0, 0.5 * dt, dt};
   const double dts_rk[3] = {dt / 3.0, dt / (double)ns, dt / (double)ns};
@@ -533,9 +534,13 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   auto kUface = mixed ? k_uface_tiled<float> : k_uface_tiled<double>;
   auto kVface = mixed ? k_vface_tiled<float> : k_vface_tiled<double>;
   auto kWface = mixed ? k_wface_tiled<float> : k_wface_tiled<double>;
-  auto kScalar = mixed ? k_scalar_adv_march<float> : k_scalar_adv_march<double>;
-  auto kLimScale = mixed ? k_lim_march<false, float> : k_lim_march<false, double>;
-  auto kLimTend = mixed ? k_lim_march<true, float> : k_lim_march<true, double>;
+  // marching kernels for the chosen chunk size (5, 10 or 25 levels)
+#define WG_PICK_KC(tmpl, ...) \
+  (kc == 5 ? tmpl<__VA_ARGS__, 5> : kc == 25 ? tmpl<__VA_ARGS__, 25> : tmpl<__VA_ARGS__, 10>)
+  auto kScalar = mixed ? WG_PICK_KC(k_scalar_adv_march, float) : WG_PICK_KC(k_scalar_adv_march, double);
+  auto kLimScale = mixed ? WG_PICK_KC(k_lim_march, false, float) : WG_PICK_KC(k_lim_march, false, double);
+  auto kLimTend = mixed ? WG_PICK_KC(k_lim_march, true, float) : WG_PICK_KC(k_lim_march, true, double);
+#undef WG_PICK_KC
 
   StateR s = origin;
   for (int stage = 0; stage < 3; ++stage) {
@@ -578,7 +583,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       const int nfields = 1 + ((moist && !lim_moist) ? 6 : 0);
       const int nchunk = march_nchunk(nz, kc);
       kScalar<<<tgrd(nx, ny, nfields * nchunk), tblk(), 0, stream>>>(
-          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, kc, mo);
+          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, mo);
     }
     LAUNCH_CHECK("k_mass");
     if (lim_theta || lim_moist) {
@@ -590,11 +595,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.offset = T0;
         PROF("k_lim_scale");
         kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-            g, la, s.theta, origin.theta, w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr, kc);
+            g, la, s.theta, origin.theta, w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
         kLimTend<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-            g, la, s.theta, origin.theta, nullptr, nullptr, w.s1, w.s2, in->base_theta, s.mu_total, w.t_tend, kc);
+            g, la, s.theta, origin.theta, nullptr, nullptr, w.s1, w.s2, in->base_theta, s.mu_total, w.t_tend);
         LAUNCH_CHECK("k_lim_tend");
       }
       if (lim_moist) {
@@ -603,11 +608,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         for (int q = 0; q < 6; ++q) {
           PROF("k_lim_scale");
           kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-              g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr, kc);
+              g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
           LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
           kLimTend<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-              g, la, s.q[q], origin.q[q], nullptr, nullptr, w.s1, w.s2, nullptr, s.mu_total, w.qtend[q], kc);
+              g, la, s.q[q], origin.q[q], nullptr, nullptr, w.s1, w.s2, nullptr, s.mu_total, w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
         }
       }
@@ -888,11 +893,8 @@ extern "C" int wrfgpu_autotune(wrfgpu_step_params *pp, const wrfgpu_metrics *mm,
     if (rc) break;
     if (ms < best_ms) { best_ms = ms; best = p; }
   }
-  const int nz = pp->nz;
-  const int march_c[] = {5, 10, 17, 25, nz};
-  for (int kcand : march_c) {
+  for (int kcand : MARCH_KC_CHOICES) {
     if (rc) break;
-    if (kcand < 1 || kcand > nz) continue;
     wrfgpu_step_params p = best;
     p.march_levels = kcand;
     float ms = 0.f;

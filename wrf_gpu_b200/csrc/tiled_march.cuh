@@ -55,8 +55,10 @@ __device__ __forceinline__ P pick6(const P (&p)[6], int n) {
   return r;
 }
 
-// Default levels per marching block (the tuner may choose others).
+// Levels per marching block: the kernels are instantiated for these chunk
+// sizes (compile-time loop bounds); the default and the tuner's choices.
 constexpr int MARCH_KC = 10;
+constexpr int MARCH_KC_CHOICES[] = {5, 10, 25};
 
 // ---------------------------------------------------------------------------
 // Plain h5/v3 scalar advection (flux_advection.py:482-568) of theta and the
@@ -66,11 +68,11 @@ constexpr int MARCH_KC = 10;
 // written, the tendency only when theta is not limited), fields 1..6 the
 // species.
 // ---------------------------------------------------------------------------
-template <typename F>
+template <typename F, int KC>
 __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s, StateR ref, const double *ru,
                                                                 const double *rv, const double *rom, const double *mut,
                                                                 const double *muts0, const double *base_theta,
-                                                                int theta_plain, int nfields, int kc, MassOut o) {
+                                                                int theta_plain, int nfields, MassOut o) {
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY;
   const int chunk = blockIdx.z / nfields, field = blockIdx.z - chunk * nfields;
-  const int k0 = chunk * kc, k1 = min(nz, k0 + kc);
+  const int k0 = chunk * KC, k1 = min(nz, k0 + KC);
   const int i = i0 + tx, j = j0 + ty;
   const bool valid = i < nx && j < ny;
   const double *fld = (field == 0) ? s.theta : pick6(s.q, field - 1);
@@ -197,16 +199,16 @@ struct LimMarchSmem {
   ZConst zc[2];
 };
 
-template <bool TEND, typename F>
+template <bool TEND, typename F, int KC>
 __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const double *field,
                                                          const double *field_old, double *s1w, double *s2w,
                                                          const double *s1r, const double *s2r, const double *base,
-                                                         const double *mu_total_stage, double *tend_out, int kc) {
+                                                         const double *mu_total_stage, double *tend_out) {
   __shared__ LimMarchSmem<TEND> sm;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY;
-  const int k0 = blockIdx.z * kc, k1 = min(nz, k0 + kc);
+  const int k0 = blockIdx.z * KC, k1 = min(nz, k0 + KC);
   const int i = i0 + tx, j = j0 + ty;
   const bool valid = i < nx && j < ny;
   const size_t plane = (size_t)ny * nx;
