@@ -158,12 +158,21 @@ __device__ __forceinline__ void advance_v_face(const Grid &g, const Acoustic &A,
 // and the v face at j (i < nx).  The two faces read the same mass-point
 // neighbourhood (p, al, alt, pb, php, ph, muts, mut, mudf), so one thread
 // doing both halves those reads; index space (nx+1) x (ny+1) x nz.
+#ifndef WG_UV_KPER
+#define WG_UV_KPER 1
+#endif
+constexpr int UV_KPER = WG_UV_KPER;  // levels per thread (shares the ph / p planes of adjacent levels)
+
 __global__ void k_advance_uv(Grid g, Acoustic A, double dts, int top_lid, BdyArgs bdy) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i <= g.nx && j < g.ny) advance_u_face(g, A, dts, top_lid, bdy, i, j, k);
-  if (i < g.nx && j <= g.ny) advance_v_face(g, A, dts, top_lid, bdy, i, j, k);
+#pragma unroll
+  for (int kk = 0; kk < UV_KPER; ++kk) {
+    const int k = blockIdx.z * UV_KPER + kk;
+    if (k >= g.nz) break;
+    if (i <= g.nx && j < g.ny) advance_u_face(g, A, dts, top_lid, bdy, i, j, k);
+    if (i < g.nx && j <= g.ny) advance_v_face(g, A, dts, top_lid, bdy, i, j, k);
+  }
 }
 
 // ---------------------------------------------------------------------------
