@@ -382,6 +382,8 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
   if (p == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params is NULL");
   if (p->nz < 4) return fail(WRFGPU_ERR_BAD_SHAPE, "nz must be >= 4");
   if (p->nx < 1 || p->ny < 1) return fail(WRFGPU_ERR_BAD_SHAPE, "nx and ny must be >= 1");
+  if ((double)(p->nz + 1) * (double)(p->ny + 1) * (double)(p->nx + 1) >= 2147483647.0)
+    return fail(WRFGPU_ERR_BAD_SHAPE, "arrays of 2^31 or more elements are not supported (32-bit element offsets)");
   if (!(p->dx > 0.0) || !(p->dy > 0.0) || !(p->dt > 0.0)) return fail(WRFGPU_ERR_BAD_SHAPE, "dx, dy, dt must be > 0");
   if (p->acoustic_substeps < 1) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "acoustic_substeps must be >= 1");
   if (p->hypsometric_opt != 1 && p->hypsometric_opt != 2)

@@ -56,10 +56,13 @@ struct StateW {
   double *q[6];
 };
 
+// Element offsets.  Every array of a step has fewer than 2^31 elements (checked
+// by wrfgpu_step_params_validate), so the index arithmetic is 32-bit and only
+// the final offset is widened.
 __device__ __forceinline__ size_t ix3(int k, int j, int i, int ny, int nx) {
-  return ((size_t)k * (size_t)ny + (size_t)j) * (size_t)nx + (size_t)i;
+  return (size_t)(unsigned)((k * ny + j) * nx + i);
 }
-__device__ __forceinline__ size_t ix2(int j, int i, int nx) { return (size_t)j * (size_t)nx + (size_t)i; }
+__device__ __forceinline__ size_t ix2(int j, int i, int nx) { return (size_t)(unsigned)(j * nx + i); }
 
 // Periodic index wrap; the in-range test keeps the common case branch-only.
 __device__ __forceinline__ int wrp(int i, int n) {
