@@ -193,6 +193,23 @@ int wrfgpu_rk3_step_batched(int n, const wrfgpu_step_params *params, const wrfgp
 int wrfgpu_autotune(wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const wrfgpu_step_inputs *in,
                     const wrfgpu_step_outputs *out, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* The plain h5/v3 flux-form scalar advection operator on its own: tend =
+ * L(ru, rv, rom) q for one field q (nz, ny, nx), doubly periodic, with the
+ * transport velocities ru, rv (nz, ny, nx; west / south faces of each cell)
+ * and rom (nz+1, ny, nx) held fixed.  Replaces advect_scalar_flux
+ * (dynamics/flux_advection.py:482-568).  Uses params nx, ny, nz, dx, dy and
+ * metrics msftx, rdnw, fnm, fnp. */
+int wrfgpu_scalar_advection(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const double *q,
+                            const double *ru, const double *rv, const double *rom, double *tend,
+                            cudaStream_t stream);
+
+/* Its adjoint with respect to q: q_bar = L^T tend_bar (the vector-Jacobian
+ * product of wrfgpu_scalar_advection for fixed velocities).  No counterpart in
+ * the reference, which has no differentiation. */
+int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                                    const double *tend_bar, const double *ru, const double *rv, const double *rom,
+                                    double *q_bar, cudaStream_t stream);
+
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 

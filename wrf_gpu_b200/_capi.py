@@ -75,7 +75,8 @@ class StepOutputs(ctypes.Structure):
 
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
             "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace",
-            "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_scalar_advection",
+            "wrfgpu_scalar_advection_adjoint", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version")
 
@@ -114,6 +115,10 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_autotune.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), ctypes.POINTER(StepInputs),
                                     ctypes.POINTER(StepOutputs), _P, ctypes.c_size_t, _P]
     lib.wrfgpu_autotune.restype = _I
+    for name in ("wrfgpu_scalar_advection", "wrfgpu_scalar_advection_adjoint"):
+        fn = getattr(lib, name)
+        fn.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), _P, _P, _P, _P, _P, _P]
+        fn.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

@@ -21,6 +21,7 @@
 #include "tiled_stencils.cuh"
 #include "tiled_faces.cuh"
 #include "tiled_march.cuh"
+#include "adjoint.cuh"
 
 using namespace wg;
 
@@ -910,6 +911,46 @@ extern "C" int wrfgpu_autotune(wrfgpu_step_params *pp, const wrfgpu_metrics *mm,
   if (rc) return rc;
   pp->column_lanes = best.column_lanes;
   pp->march_levels = best.march_levels;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The scalar advection operator and its adjoint, standalone.
+// ---------------------------------------------------------------------------
+namespace {
+int adv_op_check(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const void *a, const void *ru, const void *rv,
+                 const void *rom, const void *b) {
+  if (p == nullptr || m == nullptr || a == nullptr || ru == nullptr || rv == nullptr || rom == nullptr || b == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "an argument is NULL");
+  if (m->msftx == nullptr || m->rdnw == nullptr || m->fnm == nullptr || m->fnp == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "metrics msftx/rdnw/fnm/fnp are needed");
+  return wrfgpu_step_params_validate(p);
+}
+}  // namespace
+
+extern "C" int wrfgpu_scalar_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
+                                       const double *ru, const double *rv, const double *rom, double *tend,
+                                       cudaStream_t stream) {
+  int rc = adv_op_check(p, m, q, ru, rv, rom, tend);
+  if (rc) return rc;
+  Grid g = make_grid(*p, *m, nullptr);
+  AdvOpArgs a{ru, rv, rom};
+  k_scalar_adv_op<<<grd(p->nx, p->ny, p->nz), blk2(), 0, stream>>>(g, a, q, tend);
+  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_op launch failed");
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *p, const wrfgpu_metrics *m,
+                                               const double *tend_bar, const double *ru, const double *rv,
+                                               const double *rom, double *q_bar, cudaStream_t stream) {
+  int rc = adv_op_check(p, m, tend_bar, ru, rv, rom, q_bar);
+  if (rc) return rc;
+  Grid g = make_grid(*p, *m, nullptr);
+  AdvOpArgs a{ru, rv, rom};
+  k_scalar_adv_adj<<<grd(p->nx, p->ny, p->nz), blk2(), 0, stream>>>(g, a, tend_bar, q_bar);
+  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_adj launch failed");
   g_last_error.clear();
   return WRFGPU_OK;
 }
