@@ -71,6 +71,7 @@ struct Work {
   // mass
   double *alt_raw, *alt, *pb, *c2a, *qtot, *al_ls, *php_ls, *php, *t_tend, *theta_w, *t2ave, *p, *pm1, *al;
   double *s1, *s2, *ru, *rv, *dvdxi, *hdiv;
+  LimFaces limf;  // limiter face fluxes (scale pass -> tendency pass)
   double *qtend[6];
   // u / v faces
   double *u_tend, *u_w, *cqu, *u_target, *v_tend, *v_w, *cqv, *v_target;
@@ -98,6 +99,9 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   const bool lim = (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2 || p.moist_adv_opt == 1 || p.moist_adv_opt == 2);
   w.s1 = lim ? c.take(d.m) : nullptr;
   w.s2 = lim ? c.take(d.m) : nullptr;
+  w.limf.lx = lim ? c.take(d.m) : nullptr; w.limf.ax = lim ? c.take(d.m) : nullptr;
+  w.limf.ly = lim ? c.take(d.m) : nullptr; w.limf.ay = lim ? c.take(d.m) : nullptr;
+  w.limf.lz = lim ? c.take(d.m) : nullptr; w.limf.az = lim ? c.take(d.m) : nullptr;
   for (int s = 0; s < 6; ++s) w.qtend[s] = is_moist(p) ? c.take(d.m) : nullptr;
   w.u_tend = c.take(d.u); w.u_w = c.take(d.u); w.cqu = c.take(d.u);
   w.v_tend = c.take(d.v); w.v_w = c.take(d.v); w.cqv = c.take(d.v);
@@ -541,8 +545,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
 #define WG_PICK_KC(tmpl, ...) \
   (kc == 5 ? tmpl<__VA_ARGS__, 5> : kc == 25 ? tmpl<__VA_ARGS__, 25> : tmpl<__VA_ARGS__, 10>)
   auto kScalar = mixed ? WG_PICK_KC(k_scalar_adv_march, float) : WG_PICK_KC(k_scalar_adv_march, double);
-  auto kLimScale = mixed ? WG_PICK_KC(k_lim_march, false, float) : WG_PICK_KC(k_lim_march, false, double);
-  auto kLimTend = mixed ? WG_PICK_KC(k_lim_march, true, float) : WG_PICK_KC(k_lim_march, true, double);
+  auto kLimScale = mixed ? WG_PICK_KC(k_lim_march, float) : WG_PICK_KC(k_lim_march, double);
 #undef WG_PICK_KC
 
   StateR s = origin;
@@ -597,12 +600,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
         PROF("k_lim_scale");
-        kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-            g, la, s.theta, origin.theta, w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
+        kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1,
+                                                                                  w.s2, w.limf);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
-        kLimTend<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-            g, la, s.theta, origin.theta, nullptr, nullptr, w.s1, w.s2, in->base_theta, s.mu_total, w.t_tend);
+        k_lim_tend_faces<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, w.limf, w.s1, w.s2, in->base_theta,
+                                                                 s.mu_total, w.t_tend);
         LAUNCH_CHECK("k_lim_tend");
       }
       if (lim_moist) {
@@ -610,12 +613,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         la.offset = 0.0;
         for (int q = 0; q < 6; ++q) {
           PROF("k_lim_scale");
-          kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-              g, la, s.q[q], origin.q[q], w.s1, w.s2, nullptr, nullptr, nullptr, nullptr, nullptr);
+          kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1,
+                                                                                    w.s2, w.limf);
           LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
-          kLimTend<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(
-              g, la, s.q[q], origin.q[q], nullptr, nullptr, w.s1, w.s2, nullptr, s.mu_total, w.qtend[q]);
+          k_lim_tend_faces<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, w.limf, w.s1, w.s2, nullptr, s.mu_total,
+                                                                   w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
         }
       }

@@ -181,30 +181,27 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
 inline int march_nchunk(int nz, int kc) { return (nz + kc - 1) / kc; }
 
 // ---------------------------------------------------------------------------
-// PD / monotonic limited scalar advection (flux_advection.py:736-1000),
-// marching.  TEND = false: the scale pass (writes s1/s2); TEND = true: the
-// tendency pass (reads them).  The bottom-face z fluxes of a level are the
-// top-face fluxes carried from the level below.
+// PD / monotonic limited scalar advection (flux_advection.py:736-1000): the
+// marching scale pass.  Writes the per-cell scale(s) and the west / south /
+// bottom face fluxes of every cell for the tendency pass (k_lim_tend_faces).
+// The bottom-face z fluxes of a level are the top-face fluxes carried from
+// the level below.
 // ---------------------------------------------------------------------------
-template <bool TEND>
 struct LimMarchSmem {
   double q[2][Tile<3, 3>::N];
   double qo[2][Tile<1, 1>::N];
   double ru[2][Tile<1, 0>::N];
   double rv[2][Tile<0, 1>::N];
-  double s1[TEND ? 2 : 1][TEND ? Tile<1, 1>::N : 1];
-  double s2[TEND ? 2 : 1][TEND ? Tile<1, 1>::N : 1];
   double mt[Tile<1, 1>::N];
   double fxl[LIM_NXF], fxa[LIM_NXF], fyl[LIM_NYF], fya[LIM_NYF];
   ZConst zc[2];
 };
 
-template <bool TEND, typename F, int KC>
+template <typename F, int KC>
 __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const double *field,
                                                          const double *field_old, double *s1w, double *s2w,
-                                                         const double *s1r, const double *s2r, const double *base,
-                                                         const double *mu_total_stage, double *tend_out) {
-  __shared__ LimMarchSmem<TEND> sm;
+                                                         LimFaces fo) {
+  __shared__ LimMarchSmem sm;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY;
@@ -226,10 +223,6 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const
     slo.issue(sm.qo[b], field_old + o);
     slu.issue(sm.ru[b], a.ru + o);
     slv.issue(sm.rv[b], a.rv + o);
-    if (TEND) {
-      slo.issue(sm.s1[b], s1r + o);
-      slo.issue(sm.s2[b], s2r + o);
-    }
     cp_async_commit();
   };
   load_tile<1, 1>(sm.mt, a.mut, nx, i0, j0, nx, ny, 0.0);  // 2-D, the same for every level
@@ -256,23 +249,18 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const
       zlo = cf.lz1;
       zan = cf.az1;
       const size_t c = (size_t)k * plane + ix2(j, i, nx);
-      if (!TEND) {
-        double r1, r2;
-        lim_cell_scales(g, a, t, k, j, i, field_old, cf, r1, r2);
-        s1w[c] = r1;
-        s2w[c] = r2;
-      } else {
-        const double tend = lim_cell_tend(g, a, sm.s1[b], sm.s2[b], k, j, i, s1r, s2r, cf);
-        if (base != nullptr) {
-          const double mass_h = ld(g.c1h, k) * ld(mu_total_stage, ix2(j, i, nx)) + ld(g.c2h, k);
-          tend_out[c] = ld(base, c) * mass_h + tend;
-        } else {
-          tend_out[c] = tend;
-        }
-      }
+      double r1, r2;
+      lim_cell_scales(g, a, t, k, j, i, field_old, cf, r1, r2);
+      s1w[c] = r1;
+      s2w[c] = r2;
+      fo.lx[c] = cf.lx0;
+      fo.ax[c] = cf.ax0;
+      fo.ly[c] = cf.ly0;
+      fo.ay[c] = cf.ay0;
+      fo.lz[c] = cf.lz0;
+      fo.az[c] = cf.az0;
     }
     __syncthreads();  // staged tiles of buffer b, face fluxes and zc are reused next level
   }
 }
-
 }  // namespace wg

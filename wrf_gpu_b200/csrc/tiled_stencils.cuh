@@ -204,44 +204,50 @@ __device__ __forceinline__ void lim_cell_scales(const Grid &g, const LimArgs &a,
   }
 }
 
+// West / south / bottom face fluxes of every cell (low order l*, antidiffusive
+// a*), written by the limiter's scale pass so the tendency pass reads them
+// instead of recomputing them; the east / north / top faces of a cell are the
+// west / south / bottom faces of its neighbours (the top face of level nz-1
+// carries no flux).
+struct LimFaces {
+  double *lx, *ax, *ly, *ay, *lz, *az;
+};
+
 // Limited tendency at cell (k, j, i) (flux_advection.py:937-1000) from its
-// face fluxes and the scale tiles s1t/s2t of level k (s1k/s2k: the scale
-// arrays, for the levels above and below).
-__device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a, const double *s1t,
-                                                const double *s2t, int k, int j, int i, const double *s1,
-                                                const double *s2, const CellFluxes &cf) {
+// face fluxes; S1(dr, dc) / S2(dr, dc) return the scales at the horizontal
+// neighbour (j + dr, i + dc) of level k, s1 / s2 are the scale arrays (for the
+// levels above and below).
+template <typename SA1, typename SA2>
+__device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a, SA1 S1, SA2 S2, int k, int j, int i,
+                                                const double *s1, const double *s2, const CellFluxes &cf) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  using TO = Tile<1, 1>;
-  auto S1 = [&](int r, int cc) { return s1t[(r + 1) * TO::W + (cc + 1)]; };
-  auto S2 = [&](int r, int cc) { return s2t[(r + 1) * TO::W + (cc + 1)]; };
   auto S1k = [&](int kk) { return ld(s1, ix3(kk, j, i, ny, nx)); };
   auto S2k = [&](int kk) { return ld(s2, ix3(kk, j, i, ny, nx)); };
   double fx0, fx1, fy0, fy1, fz0, fz1;
   if (a.opt == 1) {
     auto limh = [&](double A, double s_m1, double s_c) { return A > 0.0 ? s_m1 * A : (A < 0.0 ? s_c * A : A); };
-    fx0 = limh(cf.ax0, S1(ty, tx - 1), S1(ty, tx));
-    fx1 = limh(cf.ax1, S1(ty, tx), S1(ty, tx + 1));
-    fy0 = limh(cf.ay0, S1(ty - 1, tx), S1(ty, tx));
-    fy1 = limh(cf.ay1, S1(ty, tx), S1(ty + 1, tx));
+    fx0 = limh(cf.ax0, S1(0, -1), S1(0, 0));
+    fx1 = limh(cf.ax1, S1(0, 0), S1(0, 1));
+    fy0 = limh(cf.ay0, S1(-1, 0), S1(0, 0));
+    fy1 = limh(cf.ay1, S1(0, 0), S1(1, 0));
     auto limz = [&](double A, double below, double above) { return A < 0.0 ? below * A : (A > 0.0 ? above * A : A); };
-    const double sc = S1(ty, tx);
+    const double sc = S1(0, 0);
     fz0 = limz(cf.az0, k == 0 ? sc : S1k(k - 1), sc);
     fz1 = limz(cf.az1, sc, k + 1 >= nz ? sc : S1k(k + 1));
   } else {
     auto limh = [&](double A, double in_c, double out_c, double in_m1, double out_m1) {
       return A > 0.0 ? dmin(in_c, out_m1) * A : dmin(out_c, in_m1) * A;
     };
-    fx0 = limh(cf.ax0, S1(ty, tx), S2(ty, tx), S1(ty, tx - 1), S2(ty, tx - 1));
-    fx1 = limh(cf.ax1, S1(ty, tx + 1), S2(ty, tx + 1), S1(ty, tx), S2(ty, tx));
-    fy0 = limh(cf.ay0, S1(ty, tx), S2(ty, tx), S1(ty - 1, tx), S2(ty - 1, tx));
-    fy1 = limh(cf.ay1, S1(ty + 1, tx), S2(ty + 1, tx), S1(ty, tx), S2(ty, tx));
+    fx0 = limh(cf.ax0, S1(0, 0), S2(0, 0), S1(0, -1), S2(0, -1));
+    fx1 = limh(cf.ax1, S1(0, 1), S2(0, 1), S1(0, 0), S2(0, 0));
+    fy0 = limh(cf.ay0, S1(0, 0), S2(0, 0), S1(-1, 0), S2(-1, 0));
+    fy1 = limh(cf.ay1, S1(1, 0), S2(1, 0), S1(0, 0), S2(0, 0));
     auto limz = [&](double A, double in_above, double out_above, double in_below, double out_below) {
       return A < 0.0 ? dmin(in_above, out_below) * A : dmin(out_above, in_below) * A;
     };
     const int kb = (k == 0) ? 0 : k - 1;
     const int ka = (k + 1 >= nz) ? nz - 1 : k + 1;
-    const double s1c = S1(ty, tx), s2c = S2(ty, tx);
+    const double s1c = S1(0, 0), s2c = S2(0, 0);
     const double s1b = (kb == k) ? s1c : S1k(kb), s2b = (kb == k) ? s2c : S2k(kb);
     const double s1a = (ka == k) ? s1c : S1k(ka), s2a = (ka == k) ? s2c : S2k(ka);
     fz0 = limz(cf.az0, s1c, s2c, s1b, s2b);
@@ -258,6 +264,40 @@ __device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a,
   tend = tend - msftx * g.rdy * (fy1 - fy0);
   tend = tend - ld(g.rdnw, k) * (fz1 - fz0);
   return tend;
+}
+
+// The limiter's tendency pass, one thread per cell, from the face fluxes and
+// scales the scale pass stored.
+__global__ void k_lim_tend_faces(Grid g, LimArgs a, LimFaces fc, const double *s1, const double *s2,
+                                 const double *base, const double *mu_total_stage, double *tend_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j >= ny) return;
+  const size_t c = ix3(k, j, i, ny, nx);
+  const size_t ce = ix3(k, j, wrp(i + 1, nx), ny, nx), cn = ix3(k, wrp(j + 1, ny), i, ny, nx);
+  CellFluxes cf;
+  cf.lx0 = ld(fc.lx, c); cf.ax0 = ld(fc.ax, c); cf.lx1 = ld(fc.lx, ce); cf.ax1 = ld(fc.ax, ce);
+  cf.ly0 = ld(fc.ly, c); cf.ay0 = ld(fc.ay, c); cf.ly1 = ld(fc.ly, cn); cf.ay1 = ld(fc.ay, cn);
+  cf.lz0 = ld(fc.lz, c); cf.az0 = ld(fc.az, c);
+  if (k + 1 < nz) {
+    const size_t cu = ix3(k + 1, j, i, ny, nx);
+    cf.lz1 = ld(fc.lz, cu);
+    cf.az1 = ld(fc.az, cu);
+  } else {
+    cf.lz1 = 0.0;
+    cf.az1 = 0.0;
+  }
+  auto S1 = [&](int dr, int dc) { return ld(s1, ix3(k, wrp(j + dr, ny), wrp(i + dc, nx), ny, nx)); };
+  auto S2 = [&](int dr, int dc) { return ld(s2, ix3(k, wrp(j + dr, ny), wrp(i + dc, nx), ny, nx)); };
+  const double tend = lim_cell_tend(g, a, S1, S2, k, j, i, s1, s2, cf);
+  if (base != nullptr) {
+    const double mass_h = ld(g.c1h, k) * ld(mu_total_stage, ix2(j, i, nx)) + ld(g.c2h, k);
+    tend_out[c] = ld(base, c) * mass_h + tend;
+  } else {
+    tend_out[c] = tend;
+  }
 }
 
 }  // namespace wg
