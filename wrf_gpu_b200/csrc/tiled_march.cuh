@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const
       double r1, r2;
       lim_cell_scales(g, a, t, k, j, i, field_old, cf, r1, r2);
       s1w[c] = r1;
-      s2w[c] = r2;
+      if (a.opt == 2) s2w[c] = r2;  // the PD tendency reads s1 only
       fo.lx[c] = cf.lx0;
       fo.ax[c] = cf.ax0;
       fo.ly[c] = cf.ly0;
