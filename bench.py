@@ -173,7 +173,7 @@ def run_gpu(args, rank, world, local_rank):
     stp = dycore.Stepper(nl, device=dev)
     out = stp.alloc_carry(carry)
     stream = torch.cuda.current_stream(dev)
-    tuned = stp.autotune(carry, out) if not args.no_tune else (0, 0)
+    tuned = stp.autotune(carry, out) if not args.no_tune else (0, 0, 0)
     ns = nl.acoustic_substeps
     nsub = perfmodel.substeps_per_step(ns)
     cells = nx * ny * nz
@@ -298,6 +298,7 @@ def run_gpu(args, rank, world, local_rank):
         stp_m = dycore.Stepper(nl_m, device=dev)
         out_m = stp_m.alloc_carry(carry)
         stp_m.params.march_levels, stp_m.params.column_lanes = stp.params.march_levels, stp.params.column_lanes
+        stp_m.params.column_width = stp.params.column_width
 
         def step_m():
             stp_m.step_into(carry, out_m, lead_seconds=0.0)
@@ -345,7 +346,7 @@ def run_gpu(args, rank, world, local_rank):
                 kernels=kernels, e2e={"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                                       "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e},
                 launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed,
-                tuned={"march_levels": tuned[0], "column_lanes": tuned[1]})
+                tuned={"march_levels": tuned[0], "column_lanes": tuned[1], "column_width": tuned[2]})
 
 
 def run_batched(args):

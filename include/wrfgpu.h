@@ -84,10 +84,12 @@ typedef struct wrfgpu_step_params {
   double cfn, cfn1;
   /* Kernel tile shapes (no counterpart in the reference; results do not
    * depend on them): levels per block of the level-marching stencil kernels
-   * (5, 10 or 25) and level lanes of the column kernel (8, 13 or 16); 0 selects the
-   * built-in defaults (10 and 13).  wrfgpu_autotune picks them per grid. */
+   * (5, 10 or 25), level lanes of the column kernel (8, 13 or 16) and its
+   * columns per block (16 or 32); 0 selects the built-in defaults (10, 13
+   * and 32).  wrfgpu_autotune picks them per grid. */
   int march_levels;
   int column_lanes;
+  int column_width;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */
@@ -188,7 +190,7 @@ int wrfgpu_rk3_step_batched(int n, const wrfgpu_step_params *params, const wrfgp
 
 /* Time the tile-shape candidates on this grid (each a few full steps from
  * `in` into `out`, which are overwritten) and write the fastest to
- * params->march_levels / params->column_lanes.  No counterpart in the
+ * params->march_levels / column_lanes / column_width.  No counterpart in the
  * reference.  Synchronises `stream`; call it outside stream capture. */
 int wrfgpu_autotune(wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const wrfgpu_step_inputs *in,
                     const wrfgpu_step_outputs *out, void *workspace, size_t workspace_bytes, cudaStream_t stream);

@@ -67,6 +67,7 @@ def _params(lib, **kw):
     (dict(run_boundary=1, relax_zone=6), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(precision=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(column_lanes=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(column_width=24), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(march_levels=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
 ])
 def test_validate_rejects(lib, kw, code):

@@ -82,11 +82,12 @@ def test_autotune_picks_valid_shapes_and_results_do_not_depend_on_them(cuda_read
     ref = st.alloc_carry(carry)
     st.step_into(carry, ref, lead_seconds=0.0)
     scratch = st.alloc_carry(carry)
-    kc, lanes = st.autotune(carry, scratch)
+    kc, lanes, width = st.autotune(carry, scratch)
     assert kc in (0, 5, 10, 25)
     assert lanes in (0, 8, 13, 16)
-    for kc_, lanes_ in ((kc, lanes), (5, 8), (25, 16), (10, 13)):
-        st.params.march_levels, st.params.column_lanes = kc_, lanes_
+    assert width in (0, 16, 32)
+    for kc_, lanes_, width_ in ((kc, lanes, width), (5, 8, 16), (25, 16, 32), (10, 13, 16), (10, 16, 16)):
+        st.params.march_levels, st.params.column_lanes, st.params.column_width = kc_, lanes_, width_
         o = st.alloc_carry(carry)
         st.step_into(carry, o, lead_seconds=0.0)
         torch.cuda.synchronize()

@@ -1,10 +1,10 @@
 // Column kernel of one acoustic substep, level-parallel version.
 //
-// A block owns TX = 32 adjacent columns of one row j and all levels.  Its 8
-// warps split the levels (warp w handles k = w, w+8, ...) for every part of
-// advance_mu_t / advance_w / calc_p_rho that is independent across levels;
-// only the four genuine column recurrences run serially, one thread per
-// column, out of shared memory:
+// A block owns TX (16 or 32) adjacent columns of one row j and all levels.
+// Its TY level lanes split the levels (lane l handles k = l, l+TY, ...) for
+// every part of advance_mu_t / advance_w / calc_p_rho that is independent
+// across levels; only the four genuine column recurrences run serially, one
+// thread per column, out of shared memory:
 //   * dmdt = sum_k dnw*dvdxi            (dynamics/mu_t_advance.py:205)
 //   * the ww prefix subtraction         (dynamics/mu_t_advance.py:229-237)
 //   * the Thomas forward and back sweeps (core/advance_w.py:558-592)
@@ -16,9 +16,9 @@
 
 namespace wg {
 
-// Block shape: COL_TX columns x TY level lanes (a template parameter, tuned
-// per grid; COL_TY is the default); COL_MINB resident blocks per SM requested
-// from the register allocator.
+// Block shape: TX columns x TY level lanes (template parameters, tuned per
+// grid; COL_TX x COL_TY is the default); col_minb(TX) resident blocks per SM
+// requested from the register allocator.
 #ifndef WG_COL_TX
 #define WG_COL_TX 32
 #endif
@@ -36,43 +36,43 @@ namespace wg {
 constexpr int COL_TX = WG_COL_TX;
 constexpr int COL_TY = WG_COL_TY;
 constexpr int COL_NARR = 8;
-// Level-lane counts the column kernel is instantiated for (the tuner's choices).
+// Column widths and level-lane counts the column kernel is instantiated for
+// (the tuner's choices).  A 16-column block holds half the shared memory of a
+// 32-column one, so twice as many blocks are resident per SM.
+constexpr int COL_TX_CHOICES[] = {32, 16};
 constexpr int COL_TY_CHOICES[] = {8, 13, 16};
+constexpr int col_minb(int tx) { return tx == 16 ? 2 * WG_COL_MINB : WG_COL_MINB; }
+// Levels per software-pipelined batch of the serial recurrences: the batch's
+// shared-memory operands are loaded before its first store, so the loads
+// overlap instead of each waiting behind the previous level's store.
+constexpr int COL_SU = 8;
 
 // Bulk L2 prefetch of the rows (levels 0..nz) this column block will read.
 // group 0: advance_mu_t / theta / t_2ave inputs; group 1: advance_w and
-// calc_p_rho inputs.
-__device__ __forceinline__ void column_prefetch(const Grid &g, const Acoustic &A, const ColArgs &c, int group, int i0,
-                                                int j) {
+// calc_p_rho inputs.  (u_1 and v_1 are read at levels 0..2 only, for the
+// surface w, and are not prefetched.)
+template <int TX>
+__device__ __forceinline__ void column_prefetch(const Grid &g, const Acoustic &A, const ColArgs &c,
+                                                const double *hdiv, int group, int i0, int j) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, L = nz + 1;
-  const int wm = min(COL_TX, nx - i0), wu = min(COL_TX + 1, nx + 1 - i0);
-  const int jm = (j == 0) ? (c.specified ? 0 : ny - 1) : j - 1;
-  const int jp = (j == ny - 1) ? (c.specified ? ny - 1 : 0) : j + 1;
-  const int nrows = (group == 0) ? 17 : 10;
+  const int w = min(TX, nx - i0);
+  constexpr int nrows = 10;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int e = tid; e < nrows * L; e += blockDim.x * blockDim.y) {
     const int r = e / L, k = e - r * L;
     const double *p = nullptr;
-    int w = wm;
     const bool mass = k < nz;
     if (group == 0) {
       switch (r) {
-        case 0: if (mass) { p = A.u + ix3(k, j, i0, ny, nx + 1); w = wu; } break;
-        case 1: if (mass) { p = A.u_1 + ix3(k, j, i0, ny, nx + 1); w = wu; } break;
-        case 2: if (mass) p = A.v + ix3(k, j, i0, ny + 1, nx); break;
-        case 3: if (mass) p = A.v + ix3(k, j + 1, i0, ny + 1, nx); break;
-        case 4: if (mass) p = A.v_1 + ix3(k, j, i0, ny + 1, nx); break;
-        case 5: if (mass) p = A.v_1 + ix3(k, j + 1, i0, ny + 1, nx); break;
-        case 6: p = A.ww_1 + ix3(k, j, i0, ny, nx); break;
-        case 7: p = A.ww + ix3(k, j, i0, ny, nx); break;
-        case 8: if (mass) p = A.theta_w + ix3(k, j, i0, ny, nx); break;
-        case 9: if (mass) p = A.t2ave + ix3(k, j, i0, ny, nx); break;
-        case 10: if (mass) p = A.t_tend + ix3(k, j, i0, ny, nx); break;
-        case 11: if (mass) p = A.theta_s + ix3(k, j, i0, ny, nx); break;
-        case 12: if (mass) p = A.theta_s + ix3(k, jm, i0, ny, nx); break;
-        case 13: if (mass) p = A.theta_s + ix3(k, jp, i0, ny, nx); break;
-        case 14: if (mass) p = A.c2a + ix3(k, j, i0, ny, nx); break;
-        case 15: if (mass) p = A.alt + ix3(k, j, i0, ny, nx); break;
+        case 0: p = A.ww_1 + ix3(k, j, i0, ny, nx); break;
+        case 1: p = A.ww + ix3(k, j, i0, ny, nx); break;
+        case 2: if (mass) p = A.theta_w + ix3(k, j, i0, ny, nx); break;
+        case 3: if (mass) p = A.t2ave + ix3(k, j, i0, ny, nx); break;
+        case 4: if (mass) p = A.t_tend + ix3(k, j, i0, ny, nx); break;
+        case 5: if (mass) p = A.theta_s + ix3(k, j, i0, ny, nx); break;
+        case 6: if (mass) p = A.c2a + ix3(k, j, i0, ny, nx); break;
+        case 7: if (mass) p = A.alt + ix3(k, j, i0, ny, nx); break;
+        case 8: if (mass) p = hdiv + ix3(k, j, i0, ny, nx); break;
         default: p = A.pt1 + ix3(k, j, i0, ny, nx); break;
       }
     } else {
@@ -93,21 +93,23 @@ __device__ __forceinline__ void column_prefetch(const Grid &g, const Acoustic &A
   }
 }
 
-inline size_t column_tiled_smem_bytes(int nz) { return (size_t)COL_NARR * (nz + 1) * COL_TX * sizeof(double); }
+inline size_t column_tiled_smem_bytes(int nz, int tx) { return (size_t)COL_NARR * (nz + 1) * tx * sizeof(double); }
 
-template <int TY>
-__global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid g, Acoustic A, ColArgs c,
-                                                                               const double *dvdxi,
-                                                                               const double *hdiv) {
-  static_assert(TY >= 2, "the Thomas phase needs a second warp row to stage gamma");
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, Acoustic A, ColArgs c,
+                                                                         const double *dvdxi, const double *hdiv) {
+  static_assert(TX == 16 || TX == 32, "a column block is 16 or 32 columns wide");
+  // rows ty < R0 share warp 0 with the serial thread row ty == 0
+  constexpr int R0 = 32 / TX;
+  static_assert(TY > R0, "the Thomas phase needs a warp besides warp 0 to stage gamma");
   extern __shared__ double sm[];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = blockIdx.x * COL_TX + tx;
+  const int i = blockIdx.x * TX + tx;
   const int j = blockIdx.y;
   const bool valid = i < nx;
   const int L = nz + 1;
-  auto S = [&](int a, int k) -> double & { return sm[((size_t)a * L + k) * COL_TX + tx]; };
+  auto S = [&](int a, int k) -> double & { return sm[((size_t)a * L + k) * TX + tx]; };
   // array roles (see the phase list below)
   constexpr int A0 = 0, A1 = 1, A2 = 2, A3 = 3, A4 = 4, A5 = 5, A6 = 6, A7 = 7;
   const size_t c2d = valid ? ix2(j, i, nx) : 0;
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid 
   auto T1 = [&](int k, int jj, int ii2) { return ld(A.theta_s, ix3(k, jj, ii2, ny, nx)) - T0; };
   const int nxu = nx + 1, nyv = ny + 1;
 
-  __shared__ double s_dmdt[COL_TX], s_mutend[COL_TX], s_scale[COL_TX];
+  __shared__ double s_dmdt[TX], s_mutend[TX], s_scale[TX];
   // 2-D inputs of the serial phases, loaded early so their latency overlaps P1
   double muts_in = 0.0, mu_in = 0.0, mu_tend_in = 0.0;
   if (ty == 0 && active) {
@@ -130,8 +132,8 @@ __global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid 
     mu_in = A.mu[c2d];
     mu_tend_in = (A.mu_tend != nullptr) ? ld(A.mu_tend, c2d) : 0.0;
   }
-  if (WG_COL_PREFETCH >= 1) column_prefetch(g, A, c, 0, blockIdx.x * COL_TX, j);
-  if (WG_COL_PREFETCH == 1) column_prefetch(g, A, c, 1, blockIdx.x * COL_TX, j);
+  if (WG_COL_PREFETCH >= 1) column_prefetch<TX>(g, A, c, hdiv, 0, blockIdx.x * TX, j);
+  if (WG_COL_PREFETCH == 1) column_prefetch<TX>(g, A, c, hdiv, 1, blockIdx.x * TX, j);
 
   // ---------------- P1: dvdxi per level (from k_div_h) -> A0 ----------------
   if (active) {
@@ -141,7 +143,15 @@ __global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid 
   // ---------------- P2: column sum and 2-D mass updates (serial, ty == 0) ----------------
   if (ty == 0 && active) {
     double dmdt = 0.0;
-    for (int k = 0; k < nz; ++k) {
+    int k = 0;
+    for (; k + COL_SU <= nz; k += COL_SU) {
+      double t[COL_SU];
+#pragma unroll
+      for (int u = 0; u < COL_SU; ++u) t[u] = ld(g.dnw, k + u) * S(A0, k + u);
+#pragma unroll
+      for (int u = 0; u < COL_SU; ++u) dmdt = (k + u == 0) ? t[u] : dmdt + t[u];
+    }
+    for (; k < nz; ++k) {
       const double t = ld(g.dnw, k) * S(A0, k);
       dmdt = (k == 0) ? t : dmdt + t;
     }
@@ -209,7 +219,22 @@ __global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid 
   if (ty == 0 && active) {
     double prev = ww_bot;
     S(A3, 0) = prev - S(A2, 0);
-    for (int kk = 1; kk < nz; ++kk) {
+    int kk = 1;
+    for (; kk + COL_SU <= nz; kk += COL_SU) {
+      double r1[COL_SU], r2[COL_SU];
+#pragma unroll
+      for (int u = 0; u < COL_SU; ++u) {
+        r1[u] = S(A1, kk + u);
+        r2[u] = S(A2, kk + u);
+      }
+#pragma unroll
+      for (int u = 0; u < COL_SU; ++u) {
+        const double cur = prev - r1[u];
+        S(A3, kk + u) = cur - r2[u];
+        prev = cur;
+      }
+    }
+    for (; kk < nz; ++kk) {
       const double cur = prev - S(A1, kk);
       S(A3, kk) = cur - S(A2, kk);
       prev = cur;
@@ -217,7 +242,7 @@ __global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid 
     S(A3, nz) = ww_top;
   }
   __syncthreads();
-  if (WG_COL_PREFETCH == 2) column_prefetch(g, A, c, 1, blockIdx.x * COL_TX, j);
+  if (WG_COL_PREFETCH == 2) column_prefetch<TX>(g, A, c, hdiv, 1, blockIdx.x * TX, j);
   // ---------------- P5: theta update, t_2ave, wd -> A0, buoy -> A1, coef -> A5 ----------------
   const double muts = valid ? A.muts[c2d] : 1.0;
   const double muave = valid ? A.muave[c2d] : 0.0;
@@ -334,20 +359,51 @@ __global__ void __launch_bounds__(COL_TX * TY, WG_COL_MINB) k_column_tiled(Grid 
   if (ty == 0) {
     if (valid) {
       double wf_prev = S(A6, 0);
-      for (int f = 1; f <= nz; ++f) {
+      int f = 1;
+      for (; f + COL_SU - 1 <= nz; f += COL_SU) {
+        double r6[COL_SU], r0[COL_SU], r3[COL_SU];
+#pragma unroll
+        for (int u = 0; u < COL_SU; ++u) {
+          r6[u] = S(A6, f + u);
+          r0[u] = S(A0, f + u);
+          r3[u] = S(A3, f + u);
+        }
+#pragma unroll
+        for (int u = 0; u < COL_SU; ++u) {
+          const double wf = (r6[u] - r0[u] * wf_prev) * r3[u];
+          S(A6, f + u) = wf;
+          wf_prev = wf;
+        }
+      }
+      for (; f <= nz; ++f) {
         const double wf = (S(A6, f) - S(A0, f) * wf_prev) * S(A3, f);
         S(A6, f) = wf;
         wf_prev = wf;
       }
     }
-  } else if (valid) {
-    for (int f = ty - 1; f <= nz; f += TY - 1) S(A5, f) = ld(A.gamma, M(f));
+  } else if (ty >= R0 && valid) {
+    for (int f = ty - R0; f <= nz; f += TY - R0) S(A5, f) = ld(A.gamma, M(f));
   }
   __syncthreads();
   // ---------------- P8b: Thomas back substitution (serial) ----------------
   if (ty == 0 && valid) {
     double ws_next = S(A6, nz);
-    for (int f = nz - 1; f >= 1; --f) {
+    int f = nz - 1;
+    for (; f - COL_SU + 1 >= 1; f -= COL_SU) {
+      double r6[COL_SU], r5[COL_SU];
+#pragma unroll
+      for (int u = 0; u < COL_SU; ++u) {
+        r6[u] = S(A6, f - u);
+        r5[u] = S(A5, f - u);
+      }
+#pragma unroll
+      for (int u = 0; u < COL_SU; ++u) {
+        const double ws = r6[u] - r5[u] * ws_next;
+        S(A6, f - u) = ws;
+        ws_next = ws;
+      }
+    }
+    for (; f >= 1; --f) {
       const double ws = S(A6, f) - S(A5, f) * ws_next;
       S(A6, f) = ws;
       ws_next = ws;

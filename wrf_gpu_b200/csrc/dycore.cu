@@ -409,6 +409,8 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "march_levels must be 0, 5, 10 or 25");
   if (p->column_lanes != 0 && p->column_lanes != 8 && p->column_lanes != 13 && p->column_lanes != 16)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13 or 16");
+  if (p->column_width != 0 && p->column_width != 16 && p->column_width != 32)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 16 or 32");
   return WRFGPU_OK;
 }
 
@@ -490,6 +492,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   const int ns = p.acoustic_substeps;
   const int kc = (p.march_levels == 5 || p.march_levels == 25) ? p.march_levels : MARCH_KC;
   const int lanes = (p.column_lanes > 0) ? p.column_lanes : COL_TY;
+  const int cwidth = (p.column_width > 0) ? p.column_width : COL_TX;
   const double dt_rk[3] = {dt / 3.0, 0.5 * dt, dt};
   const double dts_rk[3] = {dt / 3.0, dt / (double)ns, dt / (double)ns};
   const int nsub[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
@@ -669,8 +672,10 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     A.u_1 = s.u; A.v_1 = s.v; A.w_save = s.w; A.theta_s = s.theta; A.phb0 = w.phb0;
     ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp,
                (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0};
-    const size_t col_smem = column_tiled_smem_bytes(nz);
-    auto kColumn = (lanes == 8) ? k_column_tiled<8> : (lanes == 16) ? k_column_tiled<16> : k_column_tiled<13>;
+    const size_t col_smem = column_tiled_smem_bytes(nz, cwidth);
+    auto kColumn = (cwidth == 16)
+                       ? ((lanes == 8) ? k_column_tiled<16, 8> : (lanes == 16) ? k_column_tiled<16, 16> : k_column_tiled<16, 13>)
+                       : ((lanes == 8) ? k_column_tiled<32, 8> : (lanes == 16) ? k_column_tiled<32, 16> : k_column_tiled<32, 13>);
     if (stage == 0 && cudaFuncSetAttribute(kColumn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) !=
                           cudaSuccess)
       return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_column_tiled (nz too large)");
@@ -683,7 +688,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, specified ? 1 : 0, w.dvdxi, w.hdiv);
       LAUNCH_CHECK("k_div_h");
       PROF("k_column");
-      kColumn<<<dim3((nx + COL_TX - 1) / COL_TX, ny, 1), dim3(COL_TX, lanes, 1), col_smem, stream>>>(g, A, ca, w.dvdxi,
+      kColumn<<<dim3((nx + cwidth - 1) / cwidth, ny, 1), dim3(cwidth, lanes, 1), col_smem, stream>>>(g, A, ca, w.dvdxi,
                                                                                                       w.hdiv);
       LAUNCH_CHECK("k_column");
     }
@@ -889,16 +894,19 @@ extern "C" int wrfgpu_autotune(wrfgpu_step_params *pp, const wrfgpu_metrics *mm,
   };
   wrfgpu_step_params best = *pp;
   float best_ms = 1e30f;
-  // column lanes first (march levels at the default), then march levels
-  const int lanes_c[] = {8, 13, 16};
-  for (int l : lanes_c) {
-    wrfgpu_step_params p = *pp;
-    p.column_lanes = l;
-    p.march_levels = 0;
-    float ms = 0.f;
-    rc = time_steps(p, &ms);
-    if (rc) break;
-    if (ms < best_ms) { best_ms = ms; best = p; }
+  // column block shapes first (march levels at the default), then march levels
+  for (int cw : COL_TX_CHOICES) {
+    for (int l : COL_TY_CHOICES) {
+      if (rc) break;
+      wrfgpu_step_params p = *pp;
+      p.column_width = cw;
+      p.column_lanes = l;
+      p.march_levels = 0;
+      float ms = 0.f;
+      rc = time_steps(p, &ms);
+      if (rc) break;
+      if (ms < best_ms) { best_ms = ms; best = p; }
+    }
   }
   for (int kcand : MARCH_KC_CHOICES) {
     if (rc) break;
@@ -913,6 +921,7 @@ extern "C" int wrfgpu_autotune(wrfgpu_step_params *pp, const wrfgpu_metrics *mm,
   cudaEventDestroy(e1);
   if (rc) return rc;
   pp->column_lanes = best.column_lanes;
+  pp->column_width = best.column_width;
   pp->march_levels = best.march_levels;
   g_last_error.clear();
   return WRFGPU_OK;

@@ -378,16 +378,17 @@ class Stepper:
                                       ctypes.c_size_t(self.workspace.numel()), ctypes.c_void_p(st.cuda_stream))
         _capi.check(rc)
 
-    def autotune(self, carry: OperationalCarry, out: OperationalCarry, stream=None) -> tuple[int, int]:
+    def autotune(self, carry: OperationalCarry, out: OperationalCarry, stream=None) -> tuple[int, int, int]:
         """Pick the kernel tile shapes for this grid by timing candidates
-        (overwrites ``out``; synchronises).  Returns (march_levels, column_lanes)."""
+        (overwrites ``out``; synchronises).  Returns (march_levels,
+        column_lanes, column_width)."""
         ins, outs = self._structs(carry, out)
         st = torch.cuda.current_stream() if stream is None else stream
         _capi.check(self.lib.wrfgpu_autotune(ctypes.byref(self.params), ctypes.byref(self.metrics),
                                              ctypes.byref(ins), ctypes.byref(outs),
                                              ctypes.c_void_p(self.workspace.data_ptr()),
                                              ctypes.c_size_t(self.workspace.numel()), ctypes.c_void_p(st.cuda_stream)))
-        return int(self.params.march_levels), int(self.params.column_lanes)
+        return int(self.params.march_levels), int(self.params.column_lanes), int(self.params.column_width)
 
 
 class BatchStepper:
