@@ -2,7 +2,7 @@
 //
 // One substep is three launches:
 //   k_advance_uv               -- advance_uv on every u and v face
-//                                 (core/acoustic.py:626-786), face-parallel;
+//                                 (core/acoustic.py:626-786), level-marching;
 //   k_div_h                    -- the horizontal divergences the columns need;
 //   k_column_tiled             -- advance_mu_t (dynamics/mu_t_advance.py),
 //                                 advance_w with its Thomas solve
@@ -79,99 +79,158 @@ __device__ __forceinline__ double relax_weight_v(int j, int i, int y_len, int x_
 }
 
 // ---------------------------------------------------------------------------
-// advance_uv, one u face (core/acoustic.py:626-735).
+// advance_uv (core/acoustic.py:626-786) on both face kinds of one horizontal
+// position (i, j), marching up a chunk of UV_KC levels: the u face at i
+// (j < ny; acoustic.py:626-735) and the v face at j (i < nx; :737-750).
+// Both faces read the mass points C = (jc, ic), W = (jc, i-1) and
+// S = (j-1, ic), edge-clamped like the reference's face pairs (u uses W|C,
+// v uses S|C).  p and ph of the three points are carried up the chunk in
+// registers and the level-invariant 2-D terms are formed once, so a level
+// loads only its new plane values; every expression keeps the reference's
+// operation order.  Index space (nx+1) x (ny+1) x ceil(nz / UV_KC).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void advance_u_face(const Grid &g, const Acoustic &A, double dts, int top_lid,
-                                               const BdyArgs &bdy, int i, int j, int k) {
-  const int nx = g.nx, ny = g.ny;
-  const int nxu = nx + 1;
-  const size_t cu = ix3(k, j, i, ny, nxu);
-  const size_t f2 = ix2(j, i, nxu);
-  double u = A.u[cu] + dts * ld(A.u_tend, cu);
-  const int l = (i == 0) ? 0 : i - 1;
-  const int r = (i == nx) ? nx - 1 : i;
-  auto P = [&](const double *a, int kk, int ic) { return ld(a, ix3(kk, j, ic, ny, nx)); };
-  auto PH = [&](int kk, int ic) { return ld(A.ph, ix3(kk, j, ic, ny, nx)); };
-  auto PP = [&](int kk, int ic) { return ld(A.p, ix3(kk, j, ic, ny, nx)); };
-  auto AL = [&](int kk, int ic) { return ld(A.al, ix3(kk, j, ic, ny, nx)); };
-  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-  const double ph_term = (PH(k + 1, r) - PH(k + 1, l)) + (PH(k, r) - PH(k, l));
-  const double p_term = (P(A.alt, k, l) + P(A.alt, k, r)) * (PP(k, r) - PP(k, l));
-  const double pb_term = (AL(k, l) + AL(k, r)) * (P(A.pb, k, r) - P(A.pb, k, l));
-  const double mass_x = c1 * ld(A.muu, f2) + c2;
-  const double msfr = div_msf(ld(g.msfux, f2), g.msfuy, g.rmsfuy, f2);
-  double dpx = msfr * 0.5 * g.rdx * mass_x * (ph_term + p_term + pb_term);
-  auto ps = [&](int m) { return PP(m, l) + PP(m, r); };
-  const double mw_l = ld(A.muts, ix2(j, l, nx)) - ld(A.mut, ix2(j, l, nx));
-  const double mw_r = ld(A.muts, ix2(j, r, nx)) - ld(A.mut, ix2(j, r, nx));
-  const double bracket = ld(g.rdnw, k) * (dpn_acoustic(g, k + 1, top_lid, ps) - dpn_acoustic(g, k, top_lid, ps)) -
-                         0.5 * (c1 * (mw_l + mw_r));
-  dpx = dpx + msfr * g.rdx * (P(A.php, k, r) - P(A.php, k, l)) * bracket;
-  u = u - dts * ld(A.cqu, cu) * dpx;
-  const double md = div_msf(-EMDIV * g.dx * (ld(A.mudf, ix2(j, r, nx)) - ld(A.mudf, ix2(j, l, nx))), g.msfuy, g.rmsfuy, f2);
-  u = u + c1 * md;
-  if (bdy.active) {
-    const double w = relax_weight_u(j, i, ny, nxu, bdy);
-    if (w != 0.0) u = u + w * (ld(bdy.u_target, cu) - u);
-  }
-  A.u[cu] = u;
-}
-
-// advance_uv, one v face (core/acoustic.py:737-750).
-__device__ __forceinline__ void advance_v_face(const Grid &g, const Acoustic &A, double dts, int top_lid,
-                                               const BdyArgs &bdy, int i, int j, int k) {
-  const int nx = g.nx, ny = g.ny;
-  const int nyv = ny + 1;
-  const size_t cv = ix3(k, j, i, nyv, nx);
-  const size_t f2 = ix2(j, i, nx);
-  double v = A.v[cv] + dts * ld(A.v_tend, cv);
-  const int sj = (j == 0) ? 0 : j - 1;
-  const int nj = (j == ny) ? ny - 1 : j;
-  auto P = [&](const double *a, int kk, int jc) { return ld(a, ix3(kk, jc, i, ny, nx)); };
-  auto PH = [&](int kk, int jc) { return ld(A.ph, ix3(kk, jc, i, ny, nx)); };
-  auto PP = [&](int kk, int jc) { return ld(A.p, ix3(kk, jc, i, ny, nx)); };
-  auto AL = [&](int kk, int jc) { return ld(A.al, ix3(kk, jc, i, ny, nx)); };
-  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-  const double ph_term = (PH(k + 1, nj) - PH(k + 1, sj)) + (PH(k, nj) - PH(k, sj));
-  const double p_term = (P(A.alt, k, sj) + P(A.alt, k, nj)) * (PP(k, nj) - PP(k, sj));
-  const double pb_term = (AL(k, sj) + AL(k, nj)) * (P(A.pb, k, nj) - P(A.pb, k, sj));
-  const double mass_y = c1 * ld(A.muv, f2) + c2;
-  const double msfr = div_msf(ld(g.msfvy, f2), g.msfvx, g.rmsfvx, f2);
-  double dpy = msfr * 0.5 * g.rdy * mass_y * (ph_term + p_term + pb_term);
-  auto ps = [&](int m) { return PP(m, sj) + PP(m, nj); };
-  const double mw_s = ld(A.muts, ix2(sj, i, nx)) - ld(A.mut, ix2(sj, i, nx));
-  const double mw_n = ld(A.muts, ix2(nj, i, nx)) - ld(A.mut, ix2(nj, i, nx));
-  const double bracket = ld(g.rdnw, k) * (dpn_acoustic(g, k + 1, top_lid, ps) - dpn_acoustic(g, k, top_lid, ps)) -
-                         0.5 * (c1 * (mw_s + mw_n));
-  dpy = dpy + msfr * g.rdy * (P(A.php, k, nj) - P(A.php, k, sj)) * bracket;
-  v = v - dts * ld(A.cqv, cv) * dpy;
-  const double md = -EMDIV * g.dy * (ld(A.mudf, ix2(nj, i, nx)) - ld(A.mudf, ix2(sj, i, nx))) * ld(g.rmsfvx, f2);
-  v = v + c1 * md;
-  if (bdy.active) {
-    const double w = relax_weight_v(j, i, nyv, nx, bdy);
-    if (w != 0.0) v = v + w * (ld(bdy.v_target, cv) - v);
-  }
-  A.v[cv] = v;
-}
-
-// advance_uv on both face kinds of one (k, j, i): the u face at i (j < ny)
-// and the v face at j (i < nx).  The two faces read the same mass-point
-// neighbourhood (p, al, alt, pb, php, ph, muts, mut, mudf), so one thread
-// doing both halves those reads; index space (nx+1) x (ny+1) x nz.
-#ifndef WG_UV_KPER
-#define WG_UV_KPER 1
+#ifndef WG_UV_KC
+#define WG_UV_KC 25
 #endif
-constexpr int UV_KPER = WG_UV_KPER;  // levels per thread (shares the ph / p planes of adjacent levels)
+constexpr int UV_KC = WG_UV_KC;
+// resident 128-thread blocks per SM requested from the register allocator
+#ifndef WG_UV_MINB
+#define WG_UV_MINB 1
+#endif
 
-__global__ void k_advance_uv(Grid g, Acoustic A, double dts, int top_lid, BdyArgs bdy) {
+__global__ void __launch_bounds__(128, WG_UV_MINB) k_advance_uv(Grid g, Acoustic A, double dts, int top_lid, BdyArgs bdy) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-#pragma unroll
-  for (int kk = 0; kk < UV_KPER; ++kk) {
-    const int k = blockIdx.z * UV_KPER + kk;
-    if (k >= g.nz) break;
-    if (i <= g.nx && j < g.ny) advance_u_face(g, A, dts, top_lid, bdy, i, j, k);
-    if (i < g.nx && j <= g.ny) advance_v_face(g, A, dts, top_lid, bdy, i, j, k);
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1, nyv = ny + 1;
+  if (i > nx || j > ny) return;
+  const int k0 = blockIdx.z * UV_KC;
+  const int k1 = min(k0 + UV_KC, nz);
+  const bool du = j < ny, dv = i < nx;
+  const int ic = min(i, nx - 1), jc = min(j, ny - 1);
+  const int oC = jc * nx + ic, oW = jc * nx + max(i - 1, 0), oS = max(j - 1, 0) * nx + ic;
+  const int plane = ny * nx, uplane = ny * nxu, vplane = nyv * nx;
+  const int fu = j * nxu + i, fv = j * nx + i;
+
+  // level-invariant parts of the u and v face updates
+  double muu = 0.0, msfr_u = 0.0, mwu = 0.0, mdu = 0.0, wu = 0.0;
+  if (du) {
+    muu = ld(A.muu, fu);
+    msfr_u = div_msf(ld(g.msfux, fu), g.msfuy, g.rmsfuy, fu);
+    const double mw_l = ld(A.muts, oW) - ld(A.mut, oW);
+    const double mw_r = ld(A.muts, oC) - ld(A.mut, oC);
+    mwu = mw_l + mw_r;
+    mdu = div_msf(-EMDIV * g.dx * (ld(A.mudf, oC) - ld(A.mudf, oW)), g.msfuy, g.rmsfuy, fu);
+    if (bdy.active) wu = relax_weight_u(j, i, ny, nxu, bdy);
+  }
+  double muv = 0.0, msfr_v = 0.0, mwv = 0.0, mdv = 0.0, wv = 0.0;
+  if (dv) {
+    muv = ld(A.muv, fv);
+    msfr_v = div_msf(ld(g.msfvy, fv), g.msfvx, g.rmsfvx, fv);
+    const double mw_s = ld(A.muts, oS) - ld(A.mut, oS);
+    const double mw_n = ld(A.muts, oC) - ld(A.mut, oC);
+    mwv = mw_s + mw_n;
+    mdv = -EMDIV * g.dy * (ld(A.mudf, oC) - ld(A.mudf, oS)) * ld(g.rmsfvx, fv);
+    if (bdy.active) wv = relax_weight_v(j, i, nyv, nx, bdy);
+  }
+
+  // register window: p at k-1 (m) and k (0), ph at k
+  const double *pp = A.p, *ph = A.ph;
+  int o = k0 * plane;
+  double pCm = 0.0, pWm = 0.0, pSm = 0.0;
+  if (k0 >= 1) {
+    pCm = ld(pp, o - plane + oC); pWm = ld(pp, o - plane + oW); pSm = ld(pp, o - plane + oS);
+  }
+  double pC0 = ld(pp, o + oC), pW0 = ld(pp, o + oW), pS0 = ld(pp, o + oS);
+  double hC0 = ld(ph, o + oC), hW0 = ld(ph, o + oW), hS0 = ld(ph, o + oS);
+
+  // one level's plane values: p and ph one level up, the four mass-point
+  // arrays and the two faces' own values
+  struct Lvl {
+    double pC1, pW1, pS1, hC1, hW1, hS1, altC, altW, altS, alC, alW, alS, pbC, pbW, pbS, phpC, phpW, phpS;
+    double u, ut, cqu, v, vt, cqv;
+  };
+  auto load_lvl = [&](int k, int ok) {
+    Lvl L;
+    L.pC1 = L.pW1 = L.pS1 = 0.0;
+    if (k + 1 < nz) {
+      L.pC1 = ld(pp, ok + plane + oC); L.pW1 = ld(pp, ok + plane + oW); L.pS1 = ld(pp, ok + plane + oS);
+    }
+    L.hC1 = ld(ph, ok + plane + oC); L.hW1 = ld(ph, ok + plane + oW); L.hS1 = ld(ph, ok + plane + oS);
+    L.altC = ld(A.alt, ok + oC); L.altW = ld(A.alt, ok + oW); L.altS = ld(A.alt, ok + oS);
+    L.alC = ld(A.al, ok + oC); L.alW = ld(A.al, ok + oW); L.alS = ld(A.al, ok + oS);
+    L.pbC = ld(A.pb, ok + oC); L.pbW = ld(A.pb, ok + oW); L.pbS = ld(A.pb, ok + oS);
+    L.phpC = ld(A.php, ok + oC); L.phpW = ld(A.php, ok + oW); L.phpS = ld(A.php, ok + oS);
+    L.u = L.ut = L.cqu = L.v = L.vt = L.cqv = 0.0;
+    if (du) {
+      const int cu = k * uplane + fu;
+      L.u = A.u[cu]; L.ut = ld(A.u_tend, cu); L.cqu = ld(A.cqu, cu);
+    }
+    if (dv) {
+      const int cv = k * vplane + fv;
+      L.v = A.v[cv]; L.vt = ld(A.v_tend, cv); L.cqv = ld(A.cqv, cv);
+    }
+    return L;
+  };
+  for (int k = k0; k < k1; ++k, o += plane) {
+    const Lvl L = load_lvl(k, o);
+    const double pC1 = L.pC1, pW1 = L.pW1, pS1 = L.pS1, hC1 = L.hC1, hW1 = L.hW1, hS1 = L.hS1;
+    const double altC = L.altC, altW = L.altW, altS = L.altS, alC = L.alC, alW = L.alW, alS = L.alS;
+    const double pbC = L.pbC, pbW = L.pbW, pbS = L.pbS, phpC = L.phpC, phpW = L.phpW, phpS = L.phpS;
+    const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k), rdnw = ld(g.rdnw, k);
+    // extra p levels of the boundary extrapolations: level 2 for the bottom
+    // face (k == 0), level nz-3 for a rigid lid's top face (k == nz-1)
+    double pCx = 0.0, pWx = 0.0, pSx = 0.0;
+    const bool bot = (k == 0), top = (k + 1 == nz) && top_lid;
+    if (bot || top) {
+      const int ox = (bot ? 2 : nz - 3) * plane;
+      pCx = ld(pp, ox + oC); pWx = ld(pp, ox + oW); pSx = ld(pp, ox + oS);
+    }
+    // dpn_acoustic at faces k+1 (hi) and k (lo) for the pair sums
+    // ps(m) = p(m, a) + p(m, C), a = W for u and S for v
+    auto dpn_pair = [&](double am, double a0, double a1, double ax, double cm, double c0, double c1v, double cx,
+                        double &hi, double &lo) {
+      if (k + 1 < nz) hi = 0.5 * (ld(g.fnm, k + 1) * (a1 + c1v) + ld(g.fnp, k + 1) * (a0 + c0));
+      else hi = top_lid ? 0.5 * (g.cf1 * (a0 + c0) + g.cf2 * (am + cm) + g.cf3 * (ax + cx)) : 0.0;
+      if (bot) lo = 0.5 * (g.cf1 * (a0 + c0) + g.cf2 * (a1 + c1v) + g.cf3 * (ax + cx));
+      else lo = 0.5 * (ld(g.fnm, k) * (a0 + c0) + ld(g.fnp, k) * (am + cm));
+    };
+    if (du) {
+      const int cu = k * uplane + fu;
+      double u = L.u + dts * L.ut;
+      const double ph_term = (hC1 - hW1) + (hC0 - hW0);
+      const double p_term = (altW + altC) * (pC0 - pW0);
+      const double pb_term = (alW + alC) * (pbC - pbW);
+      const double mass_x = c1 * muu + c2;
+      double dpx = msfr_u * 0.5 * g.rdx * mass_x * (ph_term + p_term + pb_term);
+      double hi, lo;
+      dpn_pair(pWm, pW0, pW1, pWx, pCm, pC0, pC1, pCx, hi, lo);
+      const double bracket = rdnw * (hi - lo) - 0.5 * (c1 * mwu);
+      dpx = dpx + msfr_u * g.rdx * (phpC - phpW) * bracket;
+      u = u - dts * L.cqu * dpx;
+      u = u + c1 * mdu;
+      if (wu != 0.0) u = u + wu * (ld(bdy.u_target, cu) - u);
+      A.u[cu] = u;
+    }
+    if (dv) {
+      const int cv = k * vplane + fv;
+      double v = L.v + dts * L.vt;
+      const double ph_term = (hC1 - hS1) + (hC0 - hS0);
+      const double p_term = (altS + altC) * (pC0 - pS0);
+      const double pb_term = (alS + alC) * (pbC - pbS);
+      const double mass_y = c1 * muv + c2;
+      double dpy = msfr_v * 0.5 * g.rdy * mass_y * (ph_term + p_term + pb_term);
+      double hi, lo;
+      dpn_pair(pSm, pS0, pS1, pSx, pCm, pC0, pC1, pCx, hi, lo);
+      const double bracket = rdnw * (hi - lo) - 0.5 * (c1 * mwv);
+      dpy = dpy + msfr_v * g.rdy * (phpC - phpS) * bracket;
+      v = v - dts * L.cqv * dpy;
+      v = v + c1 * mdv;
+      if (wv != 0.0) v = v + wv * (ld(bdy.v_target, cv) - v);
+      A.v[cv] = v;
+    }
+    pCm = pC0; pWm = pW0; pSm = pS0;
+    pC0 = pC1; pW0 = pW1; pS0 = pS1;
+    hC0 = hC1; hW0 = hW1; hS0 = hS1;
   }
 }
 

@@ -23,7 +23,7 @@ namespace wg {
 #define WG_COL_TX 32
 #endif
 #ifndef WG_COL_TY
-#define WG_COL_TY 13
+#define WG_COL_TY 16
 #endif
 #ifndef WG_COL_MINB
 #define WG_COL_MINB 2

@@ -681,7 +681,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_column_tiled (nz too large)");
     for (int it = 0; it < nsub[stage]; ++it) {
       PROF("k_advance_uv");
-      k_advance_uv<<<grd(nx + 1, ny + 1, (nz + UV_KPER - 1) / UV_KPER), blk2(), 0, stream>>>(g, A, dts, p.top_lid,
+      k_advance_uv<<<grd(nx + 1, ny + 1, (nz + UV_KC - 1) / UV_KC), blk2(), 0, stream>>>(g, A, dts, p.top_lid,
                                                                                               ba);
       LAUNCH_CHECK("k_advance_uv");
       PROF("k_div_h");
