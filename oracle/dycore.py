@@ -734,6 +734,89 @@ def pg_buoy_w_dry(p, mu_prime, m):
     return rw, cqw
 
 
+def _ph_adv_order6(a, flow_y, flow_x):
+    """Order<=6 horizontal phi advection sums under specified lateral BCs
+    (core/rhs_ph.py:87-173): per mass row j the y sum is 6th order on rows
+    3..ny-4, 4th order on rows 2 and ny-3, 2nd order on rows 1 and ny-2, none
+    on rows 0 and ny-1; per column i the x sum is 6th order on 3..nx-4, 2nd
+    order on 1 and nx-2, none on 0, 2, nx-3 and nx-1.  ``a`` is phi_total on
+    the faces' level(s), ``flow_y``/``flow_x`` the mass-weighted v/u face
+    flows.  Each branch is added as a masked term (where-sum order)."""
+    ny, nx = a.shape[-2], a.shape[-1]
+    lead = ((0, 0),) * (a.ndim - 2)
+    py = np.pad(a, lead + ((3, 3), (0, 0)))
+    d1 = py[..., 4:-2, :] - py[..., 2:-4, :]
+    d2 = py[..., 5:-1, :] - py[..., 1:-5, :]
+    d3 = py[..., 6:, :] - py[..., :-6, :]
+    dn = py[..., 4:-2, :] - py[..., 3:-3, :]
+    ds = py[..., 3:-3, :] - py[..., 2:-4, :]
+    fn, fs = flow_y[..., 1:, :], flow_y[..., :-1, :]
+    jj = np.arange(ny)[:, None]
+    adv_y = np.where((jj >= 3) & (jj <= ny - 4), (fn + fs) * ((45.0 * d1 - 9.0 * d2 + d3) / 60.0), 0.0)
+    adv_y = adv_y + np.where((jj == 2) | (jj == ny - 3), (fn + fs) * ((8.0 * d1 - d2) / 12.0), 0.0)
+    adv_y = adv_y + np.where((jj == 1) | (jj == ny - 2), fn * dn + fs * ds, 0.0)
+    px = np.pad(a, lead + ((0, 0), (3, 3)))
+    e1 = px[..., 4:-2] - px[..., 2:-4]
+    e2 = px[..., 5:-1] - px[..., 1:-5]
+    e3 = px[..., 6:] - px[..., :-6]
+    de = px[..., 4:-2] - px[..., 3:-3]
+    dw = px[..., 3:-3] - px[..., 2:-4]
+    fe, fw = flow_x[..., 1:], flow_x[..., :-1]
+    ii = np.arange(nx)[None, :]
+    adv_x = np.where((ii >= 3) & (ii <= nx - 4), (fe + fw) * ((45.0 * e1 - 9.0 * e2 + e3) / 60.0), 0.0)
+    adv_x = adv_x + np.where((ii == 1) | (ii == nx - 2), fe * de + fw * dw, 0.0)
+    return adv_y, adv_x
+
+
+def rhs_ph(u, v, ww, ph, phb, w, mut, muu, muv, m, rdx, rdy, top_lid, order=2, specified=False):
+    """core/rhs_ph.py:175-401: the vertical terms, then the horizontal phi
+    advection -- order 2 periodic (:347-401), or the order<=6 specified
+    branch (:281-345, with the open-top face row) when order >= 4 under
+    specified lateral BCs."""
+    if order >= 4 and specified:
+        return _rhs_ph_order6_specified(u, v, ww, ph, phb, w, mut, muu, muv, m, rdx, rdy, top_lid)
+    return rhs_ph_order2(u, v, ww, ph, phb, w, mut, muu, muv, m, rdx, rdy, top_lid)
+
+
+def _rhs_ph_vertical(ww, ph, phb, w, mut, m, top_lid):
+    """term3 (-omega dphi/deta) and gw of core/rhs_ph.py:248-279."""
+    nz = ph.shape[0] - 1
+    pht = ph + phb
+    minv = (1.0 / m.msfty)[None]
+    out = np.zeros_like(ph)
+    dphi = pht[1:] - pht[:-1]
+    wdwn = 0.5 * (ww[1:] + ww[:-1]) * _col(m.rdnw) * dphi
+    term3 = _col(m.fnm[1:nz]) * wdwn[1:nz] + _col(m.fnp[1:nz]) * wdwn[: nz - 1]
+    out[1:nz] = out[1:nz] + (-term3)
+    mass_f = _col(m.c1f) * mut[None] + _col(m.c2f)
+    gw = mass_f * G * w * minv
+    out[1:nz] = out[1:nz] + gw[1:nz]
+    out[nz] = 0.0 if top_lid else gw[nz]
+    return out, pht
+
+
+def _rhs_ph_order6_specified(u, v, ww, ph, phb, w, mut, muu, muv, m, rdx, rdy, top_lid):
+    """core/rhs_ph.py:281-345 with :87-173."""
+    nz = ph.shape[0] - 1
+    out, pht = _rhs_ph_vertical(ww, ph, phb, w, mut, m, top_lid)
+    c1f_int = _col(m.c1f[1:nz])
+    c2f_int = _col(m.c2f[1:nz])
+    flow_y = (c1f_int * muv[None] + c2f_int) * (v[1:nz] + v[: nz - 1]) * m.msfvy[None]
+    flow_x = (c1f_int * muu[None] + c2f_int) * (u[1:nz] + u[: nz - 1]) * m.msfux[None]
+    adv_y, adv_x = _ph_adv_order6(pht[1:nz], flow_y, flow_x)
+    adv = 0.25 * rdy / m.msfty[None] * adv_y + 0.25 * rdx / m.msfty[None] * adv_x
+    out[1:nz] = out[1:nz] + (-adv)
+    if not top_lid and nz >= 3:
+        cfn, cfn1 = _cfn(m)
+        v_top = cfn * v[nz - 1] + cfn1 * v[nz - 2]
+        u_top = cfn * u[nz - 1] + cfn1 * u[nz - 2]
+        fy = (m.c1f[nz] * muv + m.c2f[nz]) * v_top * m.msfvy
+        fx = (m.c1f[nz] * muu + m.c2f[nz]) * u_top * m.msfux
+        ay, ax = _ph_adv_order6(pht[nz], fy, fx)
+        out[nz] = out[nz] + (-(0.5 * rdy / m.msfty) * ay - (0.5 * rdx / m.msfty) * ax)
+    return out
+
+
 def rhs_ph_order2(u, v, ww, ph, phb, w, mut, muu, muv, m, rdx, rdy, top_lid):
     """core/rhs_ph.py:175-401 (advective_order <= 2 periodic path)."""
     nz = ph.shape[0] - 1
@@ -1093,8 +1176,9 @@ def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Nameli
         cor = m.e[None] * (m.cosa[None] * ru_f - mxy * m.sina[None] * rv_f)
         curv = W_RERADIUS * (ru_f * u_f + mxy * rv_f * v_f)
         rw[1:nz] = rw[1:nz] + (cor + curv)
-    ph_tend = rhs_ph_order2(s.u, s.v, prep.ww_save, s.ph_perturbation, prep.phb, s.w, prep.mut,
-                            prep.muu, prep.muv, m, rdx, rdy, nl.top_lid)
+    ph_tend = rhs_ph(s.u, s.v, prep.ww_save, s.ph_perturbation, prep.phb, s.w, prep.mut,
+                     prep.muu, prep.muv, m, rdx, rdy, nl.top_lid, order=nl.h_sca_adv_order,
+                     specified=lateral_flags(nl)[1])
     a = SimpleNamespace()
     a.ww = prep.ww_save.copy()
     a.ww_1 = prep.ww_save

@@ -63,7 +63,6 @@ def _params(lib, **kw):
     (dict(hypsometric_opt=3), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(scalar_adv_opt=3), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(moist_adv_opt=4), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
-    (dict(run_boundary=1, bc_ideal=0, h_sca_adv_order=5), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(run_boundary=1, relax_zone=6), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(precision=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(column_lanes=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),

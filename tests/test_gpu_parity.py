@@ -103,6 +103,41 @@ def test_per_step_parity_options(cuda_ready):
             assert not bad, f"{kw} step {n}: {bad}"
 
 
+def _with_map_factors(case, seed=7, amp=0.02):
+    """Seeded non-unit map factors on every staggering (the periodic wrap
+    face / row repeats face / row 0)."""
+    rng = np.random.default_rng(seed)
+    m = case.metrics
+    for k in ("msftx", "msfty", "msfux", "msfuy", "msfvx", "msfvy"):
+        a = 1.0 + amp * rng.standard_normal(getattr(m, k).shape)
+        if k in ("msfux", "msfuy"):
+            a[:, -1] = a[:, 0]
+        if k in ("msfvx", "msfvy"):
+            a[-1, :] = a[0, :]
+        setattr(m, k, a)
+    return case
+
+
+@pytest.mark.parametrize("top_lid", [False, True])
+def test_per_step_parity_rhs_ph_order6_specified(cuda_ready, top_lid):
+    """h_sca_adv_order 5 under specified lateral BCs: rhs_ph's order<=6
+    horizontal phi advection with its 4th/2nd-order edge rows and the open-top
+    face row, on non-unit map factors."""
+    case = _with_map_factors(cases.real_like_moist(24, 20, 14, hmax=800.0, specified=True))
+    case.controls["h_sca_adv_order"] = 5
+    case.controls["top_lid"] = top_lid
+    for n, e in enumerate(_per_step(case, 2)):
+        bad = {k: v for k, v in e.items() if not v <= _tol(k)}
+        assert not bad, f"top_lid={top_lid} step {n}: {bad}"
+
+
+def test_per_step_parity_map_factors_periodic(cuda_ready):
+    case = _with_map_factors(cases.real_like_moist(24, 20, 14, hmax=800.0, specified=False), seed=11)
+    for n, e in enumerate(_per_step(case, 2)):
+        bad = {k: v for k, v in e.items() if not v <= _tol(k)}
+        assert not bad, f"step {n}: {bad}"
+
+
 def test_per_step_parity_warm_bubble_3d(cuda_ready):
     case = cases.warm_bubble_3d(20, 16, 12)
     errs = _per_step(case, 3)

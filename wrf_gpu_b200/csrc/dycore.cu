@@ -398,8 +398,6 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
   if (p->moist_adv_opt < 0 || p->moist_adv_opt > 2)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "moist_adv_opt must be 0, 1 or 2");
   const bool spec = p->run_boundary && !p->bc_ideal;
-  if (spec && p->h_sca_adv_order >= 4)
-    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "rhs_ph order-6 specified-boundary branch (h_sca_adv_order >= 4) is not built");
   if (spec && (p->nx < 3 || p->ny < 3)) return fail(WRFGPU_ERR_BAD_SHAPE, "specified boundaries need nx, ny >= 3");
   if (p->run_boundary && (p->spec_zone != 1 || p->relax_zone != 4))
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "boundary zones other than spec_zone=1, relax_zone=4 are not built");
@@ -543,7 +541,10 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   const bool mixed = p.precision == WRFGPU_PRECISION_MIXED;
   auto kUface = mixed ? k_uface_tiled<float> : k_uface_tiled<double>;
   auto kVface = mixed ? k_vface_tiled<float> : k_vface_tiled<double>;
-  auto kWface = mixed ? k_wface_tiled<float> : k_wface_tiled<double>;
+  // rhs_ph's order<=6 specified-boundary branch (core/rhs_ph.py:281-345)
+  const bool ph_order6 = specified && p.h_sca_adv_order >= 4;
+  auto kWface = mixed ? (ph_order6 ? k_wface_tiled<float, true> : k_wface_tiled<float, false>)
+                      : (ph_order6 ? k_wface_tiled<double, true> : k_wface_tiled<double, false>);
   // marching kernels for the chosen chunk size (5, 10 or 25 levels)
 #define WG_PICK_KC(tmpl, ...) \
   (kc == 5 ? tmpl<__VA_ARGS__, 5> : kc == 25 ? tmpl<__VA_ARGS__, 25> : tmpl<__VA_ARGS__, 10>)
@@ -636,9 +637,13 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     const double x = 0.5 * dts * G * eps1;
     const double cof = x * x;
     CoefOut co{w.a, w.alpha, w.gamma, w.p, w.pm1, w.al, w.t2ave};
+    const size_t coef_smem = coef_smem_bytes(nz);
+    if (stage == 0 && cudaFuncSetAttribute(k_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coef_smem) !=
+                          cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_coef (nz too large)");
     PROF("k_coef");
-    k_coef<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, w.mut, w.muts0, w.mu_work0, w.c2a, w.cqw, w.alt, w.theta_w,
-                                                  w.ph_w, origin.theta, cof, p.top_lid, co);
+    k_coef<<<dim3((nx + 31) / 32, ny, 1), dim3(32, COEF_TY, 1), coef_smem, stream>>>(
+        g, w.mut, w.muts0, w.mu_work0, w.c2a, w.cqw, w.alt, w.theta_w, w.ph_w, origin.theta, cof, p.top_lid, co);
     LAUNCH_CHECK("k_coef");
 
     BdyArgs ba{};

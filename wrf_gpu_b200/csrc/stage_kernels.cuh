@@ -263,71 +263,122 @@ struct WFaceOut {
 };
 
 // ---------------------------------------------------------------------------
-// Column kernel: calc_coef_w (acoustic_wrf.py:783-852) and the step-0
-// calc_p_rho (core/calc_p_rho.py:52-134); seeds p, pm1, al and t_2ave.
+// calc_coef_w (acoustic_wrf.py:783-852) and the step-0 calc_p_rho
+// (core/calc_p_rho.py:52-134), which seeds p, pm1, al and t_2ave.
+// A block owns 32 adjacent columns of one row j; its COEF_TY level lanes form
+// the tridiagonal rows (a, b, c of every level) and the step-0 calc_p_rho
+// level-parallel, and only the factorisation alpha(k) = 1 / (b - a*gamma(k-1)),
+// gamma(k) = c * alpha(k) runs serially, one thread per column, out of shared
+// memory.  Operation order is the reference's.
 // ---------------------------------------------------------------------------
 struct CoefOut {
   double *a, *alpha, *gamma, *p, *pm1, *al, *t2ave;
 };
 
-__global__ void k_coef(Grid g, const double *mut, const double *muts0, const double *mu_work0, const double *c2a,
-                       const double *cqw, const double *alt, const double *theta_w, const double *ph_w,
-                       const double *ref_theta, double cof, int top_lid, CoefOut o) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  if (i >= nx || j >= ny) return;
-  const size_t c2d = ix2(j, i, nx);
-  const double mt = ld(mut, c2d);
-  auto mh = [&](int k) { return ld(g.c1h, k) * mt + ld(g.c2h, k); };
-  auto mf = [&](int k) { return ld(g.c1f, k) * mt + ld(g.c2f, k); };
-  auto C2A = [&](int k) { return ld(c2a, ix3(k, j, i, ny, nx)); };
-  auto CQW = [&](int k) { return ld(cqw, ix3(k, j, i, ny, nx)); };
-  const double lid = top_lid ? 0.0 : 1.0;
-  const double rdnw_t = ld(g.rdnw, nz - 1);
-  const double a_top = -2.0 * cof * (rdnw_t * rdnw_t) * C2A(nz - 1) * lid / (mh(nz - 1) * mf(nz - 1));
-  o.a[ix3(0, j, i, ny, nx)] = 0.0;
-  o.alpha[ix3(0, j, i, ny, nx)] = 1.0;
-  o.gamma[ix3(0, j, i, ny, nx)] = 0.0;
-  double gam_prev = 0.0;
-  for (int k = 1; k < nz; ++k) {
-    double ak = 0.0;
-    if (k >= 2) {
-      ak = -CQW(k) * cof * ld(g.rdn, k) * ld(g.rdnw, k - 1) * C2A(k - 1) / (mh(k - 1) * mf(k - 1));
+constexpr int COEF_TY = 8;
+inline size_t coef_smem_bytes(int nz) { return (size_t)3 * (nz + 1) * 32 * sizeof(double); }
+
+__global__ void __launch_bounds__(32 * COEF_TY) k_coef(Grid g, const double *mut, const double *muts0,
+                                                       const double *mu_work0, const double *c2a, const double *cqw,
+                                                       const double *alt, const double *theta_w, const double *ph_w,
+                                                       const double *ref_theta, double cof, int top_lid, CoefOut o) {
+  extern __shared__ double sm[];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, L = nz + 1;
+  const int i = blockIdx.x * 32 + tx, j = blockIdx.y;
+  const bool valid = i < nx;
+  // rows: SA = sub-diagonal a, SB = diagonal b -> alpha, SC = super-diagonal c -> gamma
+  auto SA = [&](int k) -> double & { return sm[(size_t)k * 32 + tx]; };
+  auto SB = [&](int k) -> double & { return sm[(size_t)(L + k) * 32 + tx]; };
+  auto SC = [&](int k) -> double & { return sm[(size_t)(2 * L + k) * 32 + tx]; };
+  auto M = [&](int k) { return ix3(k, j, i, ny, nx); };
+  if (valid) {
+    const size_t c2d = ix2(j, i, nx);
+    const double mt = ld(mut, c2d);
+    auto mh = [&](int k) { return ld(g.c1h, k) * mt + ld(g.c2h, k); };
+    auto mf = [&](int k) { return ld(g.c1f, k) * mt + ld(g.c2f, k); };
+    auto C2A = [&](int k) { return ld(c2a, M(k)); };
+    for (int k = 1 + ty; k < nz; k += COEF_TY) {
+      const double cq = ld(cqw, M(k));
+      double ak = 0.0;
+      if (k >= 2) {
+        ak = -cq * cof * ld(g.rdn, k) * ld(g.rdnw, k - 1) * C2A(k - 1) / (mh(k - 1) * mf(k - 1));
+      }
+      const double b = 1.0 + cq * cof * ld(g.rdn, k) *
+                                 (ld(g.rdnw, k) * C2A(k) / (mh(k) * mf(k)) + ld(g.rdnw, k - 1) * C2A(k - 1) / (mh(k - 1) * mf(k)));
+      const double cc = -cq * cof * ld(g.rdn, k) * ld(g.rdnw, k) * C2A(k) / (mh(k) * mf(k + 1));
+      SA(k) = ak;
+      SB(k) = b;
+      SC(k) = cc;
     }
-    const double b = 1.0 + CQW(k) * cof * ld(g.rdn, k) *
-                               (ld(g.rdnw, k) * C2A(k) / (mh(k) * mf(k)) + ld(g.rdnw, k - 1) * C2A(k - 1) / (mh(k - 1) * mf(k)));
-    const double cc = -CQW(k) * cof * ld(g.rdn, k) * ld(g.rdnw, k) * C2A(k) / (mh(k) * mf(k + 1));
-    const double al_k = 1.0 / (b - ak * gam_prev);
-    const double ga_k = cc * al_k;
-    const size_t f = ix3(k, j, i, ny, nx);
-    o.a[f] = ak;
-    o.alpha[f] = al_k;
-    o.gamma[f] = ga_k;
-    gam_prev = ga_k;
+    if (ty == COEF_TY - 1) {  // top row: a and b of face nz
+      const double lid = top_lid ? 0.0 : 1.0;
+      const double rdnw_t = ld(g.rdnw, nz - 1);
+      SA(nz) = -2.0 * cof * (rdnw_t * rdnw_t) * C2A(nz - 1) * lid / (mh(nz - 1) * mf(nz - 1));
+      SB(nz) = 1.0 + 2.0 * cof * (rdnw_t * rdnw_t) * C2A(nz - 1) / (mh(nz - 1) * mf(nz));
+    }
+    // step-0 calc_p_rho with muts = prep.muts and theta_1 = reference theta'
+    const double muts = ld(muts0, c2d), mu_work = ld(mu_work0, c2d);
+    for (int k = ty; k < nz; k += COEF_TY) {
+      const size_t c = M(k);
+      const double mass_h = ld(g.c1h, k) * muts + ld(g.c2h, k);
+      const double safe = safe12(mass_h);
+      const double mu_term = ld(g.c1h, k) * mu_work;
+      const double altc = ld(alt, c);
+      const double al = -(altc * mu_term + ld(g.rdnw, k) * (ld(ph_w, M(k + 1)) - ld(ph_w, c))) / safe;
+      const double t1 = ld(ref_theta, c) - T0;
+      const double ttr = T0 + t1;
+      const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
+      const double p = C2A(k) * (altc * (ld(theta_w, c) - mu_term * t1) / (safe * sttr) - al);
+      o.p[c] = p;
+      o.pm1[c] = p;
+      o.al[c] = al;
+      o.t2ave[c] = 0.0;
+    }
   }
-  const double b_top = 1.0 + 2.0 * cof * (rdnw_t * rdnw_t) * C2A(nz - 1) / (mh(nz - 1) * mf(nz));
-  const size_t ft = ix3(nz, j, i, ny, nx);
-  o.a[ft] = a_top;
-  o.alpha[ft] = 1.0 / (b_top - a_top * gam_prev);
-  o.gamma[ft] = 0.0;
-  // step-0 calc_p_rho with muts = prep.muts and theta_1 = reference theta'
-  const double muts = ld(muts0, c2d), mu_work = ld(mu_work0, c2d);
-  for (int k = 0; k < nz; ++k) {
-    const size_t c = ix3(k, j, i, ny, nx);
-    const double mass_h = ld(g.c1h, k) * muts + ld(g.c2h, k);
-    const double safe = safe12(mass_h);
-    const double mu_term = ld(g.c1h, k) * mu_work;
-    const double altc = ld(alt, c);
-    const double al = -(altc * mu_term + ld(g.rdnw, k) * (ld(ph_w, ix3(k + 1, j, i, ny, nx)) - ld(ph_w, c))) / safe;
-    const double t1 = ld(ref_theta, c) - T0;
-    const double ttr = T0 + t1;
-    const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
-    const double p = C2A(k) * (altc * (ld(theta_w, c) - mu_term * t1) / (safe * sttr) - al);
-    o.p[c] = p;
-    o.pm1[c] = p;
-    o.al[c] = al;
-    o.t2ave[c] = 0.0;
+  __syncthreads();
+  if (ty == 0 && valid) {
+    constexpr int SU = 8;  // levels per batch of shared-memory loads ahead of the chain
+    double gam_prev = 0.0;
+    int k = 1;
+    for (; k + SU <= nz; k += SU) {
+      double ra[SU], rb[SU], rc[SU];
+#pragma unroll
+      for (int u = 0; u < SU; ++u) {
+        ra[u] = SA(k + u);
+        rb[u] = SB(k + u);
+        rc[u] = SC(k + u);
+      }
+#pragma unroll
+      for (int u = 0; u < SU; ++u) {
+        const double al_k = 1.0 / (rb[u] - ra[u] * gam_prev);
+        const double ga_k = rc[u] * al_k;
+        SB(k + u) = al_k;
+        SC(k + u) = ga_k;
+        gam_prev = ga_k;
+      }
+    }
+    for (; k < nz; ++k) {
+      const double al_k = 1.0 / (SB(k) - SA(k) * gam_prev);
+      const double ga_k = SC(k) * al_k;
+      SB(k) = al_k;
+      SC(k) = ga_k;
+      gam_prev = ga_k;
+    }
+    SB(nz) = 1.0 / (SB(nz) - SA(nz) * gam_prev);
+    SC(nz) = 0.0;
+    SA(0) = 0.0;
+    SB(0) = 1.0;
+    SC(0) = 0.0;
+  }
+  __syncthreads();
+  if (valid) {
+    for (int f = ty; f <= nz; f += COEF_TY) {
+      const size_t c = M(f);
+      o.a[c] = SA(f);
+      o.alpha[c] = SB(f);
+      o.gamma[c] = SC(f);
+    }
   }
 }
 

@@ -313,9 +313,50 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, 
 }
 
 // ---------------------------------------------------------------------------
-// w faces, tiled: w advection and rhs_ph horizontal stencils from tiles.
+// Order<=6 horizontal phi advection sums of rhs_ph under specified lateral BCs
+// (core/rhs_ph.py:87-173) at mass cell (j, i) of one face level.  PT(dr, dc)
+// is phi_total at (j+dr, i+dc) (|dr|, |dc| <= 3, read only where the row and
+// column masks select), FY(jv) / FX(iu) the mass-weighted v / u face flows.
+// y: 6th order on rows 3..ny-4, 4th order on rows 2 and ny-3, 2nd order on
+// rows 1 and ny-2, none on rows 0 and ny-1; x: 6th order on columns 3..nx-4,
+// 2nd order on columns 1 and nx-2, none elsewhere.  The masked branches are
+// summed like the reference's where-terms.
 // ---------------------------------------------------------------------------
-template <typename F>
+template <typename PTF, typename FYF, typename FXF>
+__device__ __forceinline__ void ph_adv_order6(int j, int i, int ny, int nx, PTF PT, FYF FY, FXF FX, double &adv_y,
+                                              double &adv_x) {
+  double y6 = 0.0, y4 = 0.0, y2 = 0.0;
+  if (j >= 3 && j <= ny - 4) {
+    const double d1 = PT(1, 0) - PT(-1, 0), d2 = PT(2, 0) - PT(-2, 0), d3 = PT(3, 0) - PT(-3, 0);
+    y6 = (FY(j + 1) + FY(j)) * div_rcp(45.0 * d1 - 9.0 * d2 + d3, 60.0, R60);
+  }
+  if (j == 2 || j == ny - 3) {
+    const double d1 = PT(1, 0) - PT(-1, 0), d2 = PT(2, 0) - PT(-2, 0);
+    y4 = (FY(j + 1) + FY(j)) * div_rcp(8.0 * d1 - d2, 12.0, R12);
+  }
+  if (j == 1 || j == ny - 2) {
+    const double a0 = PT(0, 0);
+    y2 = FY(j + 1) * (PT(1, 0) - a0) + FY(j) * (a0 - PT(-1, 0));
+  }
+  adv_y = (y6 + y4) + y2;
+  double x6 = 0.0, x2 = 0.0;
+  if (i >= 3 && i <= nx - 4) {
+    const double d1 = PT(0, 1) - PT(0, -1), d2 = PT(0, 2) - PT(0, -2), d3 = PT(0, 3) - PT(0, -3);
+    x6 = (FX(i + 1) + FX(i)) * div_rcp(45.0 * d1 - 9.0 * d2 + d3, 60.0, R60);
+  }
+  if (i == 1 || i == nx - 2) {
+    const double a0 = PT(0, 0);
+    x2 = FX(i + 1) * (PT(0, 1) - a0) + FX(i) * (a0 - PT(0, -1));
+  }
+  adv_x = x6 + x2;
+}
+
+// ---------------------------------------------------------------------------
+// w faces, tiled: w advection and rhs_ph horizontal stencils from tiles.
+// ORD6 selects rhs_ph's order<=6 specified-boundary horizontal advection
+// (h_sca_adv_order >= 4 with specified lateral BCs), otherwise order 2.
+// ---------------------------------------------------------------------------
+template <typename F, bool ORD6>
 __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom,
                                                            const double *ww_stage, const double *qtot,
@@ -326,7 +367,8 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
-  using TP = Tile<1, 1>;
+  constexpr int PHH = ORD6 ? 3 : 1;  // halo of the phi_total tile
+  using TP = Tile<PHH, PHH>;
   __shared__ double sw[TQ::N];
   __shared__ double sru[TR::N];
   __shared__ double srv[TV::N];
@@ -364,7 +406,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
     }
     for (int e = ty * TSX + tx; e < TP::N; e += TSX * TSY) {
       const int r = e / TP::W, cc = e - r * TP::W;
-      const size_t q = (size_t)k * pm + (size_t)wrp(j0 - 1 + r, ny) * nx + wrp(i0 - 1 + cc, nx);
+      const size_t q = (size_t)k * pm + (size_t)wrp(j0 - PHH + r, ny) * nx + wrp(i0 - PHH + cc, nx);
       const double p = ld(s.ph_pert, q);
       spt[e] = p + (ld(s.ph_total, q) - p);
     }
@@ -473,7 +515,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
   o.rw_tend[cw] = rw;
   o.cqw[cw] = cqw;
   {
-    auto PT = [&](int r, int cc) { return spt[(r + 1) * TP::W + (cc + 1)]; };
+    auto PT = [&](int r, int cc) { return spt[(r + PHH) * TP::W + (cc + PHH)]; };
     auto pht = [&](int kk) {  // column value at level kk
       const size_t q = ix3(kk, j, i, ny, nx);
       const double p = ld(s.ph_pert, q);
@@ -492,20 +534,49 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
       const double c1f = ld(g.c1f, k), c2f = ld(g.c2f, k);
       auto vpair = [&](int jv) { return ld(s.v, ix3(k, jv, i, ny + 1, nx)) + ld(s.v, ix3(k - 1, jv, i, ny + 1, nx)); };
       auto muvf = [&](int jv) { return c1f * ld(muv, ix2(jv, i, nx)) + c2f; };
-      const double pti = PT(ty, tx);
-      const double dn_ = PT(ty + 1, tx) - pti;
-      const double ds_ = pti - PT(ty - 1, tx);
-      const double flux_y = muvf(j + 1) * vpair(j + 1) * dn_ + muvf(j) * vpair(j) * ds_;
-      out = out + (-(0.25 * g.rdy * minv)) * flux_y;
       auto upair = [&](int iu) { return ld(s.u, ix3(k, j, iu, ny, nx + 1)) + ld(s.u, ix3(k - 1, j, iu, ny, nx + 1)); };
       auto muuf = [&](int iu) { return c1f * ld(muu, ix2(j, iu, nx + 1)) + c2f; };
-      const double de_ = PT(ty, tx + 1) - pti;
-      const double dw_ = pti - PT(ty, tx - 1);
-      const double flux_x = muuf(i + 1) * upair(i + 1) * de_ + muuf(i) * upair(i) * dw_;
-      out = out + (-(0.25 * g.rdx * minv)) * flux_x;
+      if constexpr (ORD6) {
+        auto FY = [&](int jv) { return muvf(jv) * vpair(jv) * ld(g.msfvy, ix2(jv, i, nx)); };
+        auto FX = [&](int iu) { return muuf(iu) * upair(iu) * ld(g.msfux, ix2(j, iu, nx + 1)); };
+        auto PTo = [&](int dr, int dc) { return PT(ty + dr, tx + dc); };
+        double adv_y, adv_x;
+        ph_adv_order6(j, i, ny, nx, PTo, FY, FX, adv_y, adv_x);
+        const double msfty_c = ld(g.msfty, c2d);
+        const double adv = div_rcp(0.25 * g.rdy, msfty_c, minv) * adv_y + div_rcp(0.25 * g.rdx, msfty_c, minv) * adv_x;
+        out = out + (-adv);
+      } else {
+        const double pti = PT(ty, tx);
+        const double dn_ = PT(ty + 1, tx) - pti;
+        const double ds_ = pti - PT(ty - 1, tx);
+        const double flux_y = muvf(j + 1) * vpair(j + 1) * dn_ + muvf(j) * vpair(j) * ds_;
+        out = out + (-(0.25 * g.rdy * minv)) * flux_y;
+        const double de_ = PT(ty, tx + 1) - pti;
+        const double dw_ = pti - PT(ty, tx - 1);
+        const double flux_x = muuf(i + 1) * upair(i + 1) * de_ + muuf(i) * upair(i) * dw_;
+        out = out + (-(0.25 * g.rdx * minv)) * flux_x;
+      }
     } else if (k == nz && !top_lid) {
       const double mass_f = ld(g.c1f, nz) * mut_c + ld(g.c2f, nz);
       out = mass_f * G * ld(s.w, cw) * minv;
+      if constexpr (ORD6) {
+        // open-top face row: winds extrapolated with cfn/cfn1, weight 0.5
+        // (core/rhs_ph.py:290-343)
+        const double c1t = ld(g.c1f, nz), c2t = ld(g.c2f, nz);
+        auto FY = [&](int jv) {
+          const double vt = g.cfn * ld(s.v, ix3(nz - 1, jv, i, ny + 1, nx)) + g.cfn1 * ld(s.v, ix3(nz - 2, jv, i, ny + 1, nx));
+          return (c1t * ld(muv, ix2(jv, i, nx)) + c2t) * vt * ld(g.msfvy, ix2(jv, i, nx));
+        };
+        auto FX = [&](int iu) {
+          const double ut = g.cfn * ld(s.u, ix3(nz - 1, j, iu, ny, nx + 1)) + g.cfn1 * ld(s.u, ix3(nz - 2, j, iu, ny, nx + 1));
+          return (c1t * ld(muu, ix2(j, iu, nx + 1)) + c2t) * ut * ld(g.msfux, ix2(j, iu, nx + 1));
+        };
+        auto PTo = [&](int dr, int dc) { return PT(ty + dr, tx + dc); };
+        double adv_y, adv_x;
+        ph_adv_order6(j, i, ny, nx, PTo, FY, FX, adv_y, adv_x);
+        const double msfty_c = ld(g.msfty, c2d);
+        out = out + ((-div_rcp(0.5 * g.rdy, msfty_c, minv)) * adv_y - div_rcp(0.5 * g.rdx, msfty_c, minv) * adv_x);
+      }
     }
     o.ph_tend[cw] = out;
   }
