@@ -85,11 +85,16 @@ typedef struct wrfgpu_step_params {
   /* Kernel tile shapes (no counterpart in the reference; results do not
    * depend on them): levels per block of the level-marching stencil kernels
    * (5, 10 or 25), level lanes of the column kernel (8, 13 or 16) and its
-   * columns per block (16 or 32); 0 selects the built-in defaults (10, 13
+   * columns per block (16 or 32); 0 selects the built-in defaults (10, 16
    * and 32).  wrfgpu_autotune picks them per grid. */
   int march_levels;
   int column_lanes;
   int column_width;
+  /* OperationalNamelist.specified_adv_degrade (operational_mode.py:460; default
+   * off): with specified lateral BCs, WRF's tiered flux orders near the edges
+   * and no horizontal advection of the outermost cells
+   * (flux_advection.py:288-391). */
+  int specified_adv_degrade;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */

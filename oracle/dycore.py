@@ -57,6 +57,7 @@ class Namelist:
     zdamp: float = 5000.0
     hypsometric_opt: int = 1
     h_sca_adv_order: int = 2
+    specified_adv_degrade: bool = False   # operational_mode.py:460 (opt-in)
     scalar_adv_opt: int = 0
     moist_adv_opt: int = 0
     run_boundary: bool = False
@@ -199,6 +200,69 @@ def stage_omega_specified(u, v, mu_total, m, rdx, rdy):
     return rom
 
 
+def _shift0(f, k, axis):
+    """flux_advection.py:257-278: shift by k along axis (value at i is f[i-k]) with zero fill."""
+    n = f.shape[axis]
+    out = np.zeros_like(f)
+    src = [slice(None)] * f.ndim
+    dst = [slice(None)] * f.ndim
+    if k >= 0:
+        src[axis], dst[axis] = slice(0, n - k), slice(k, n)
+    else:
+        src[axis], dst[axis] = slice(-k, n), slice(0, n + k)
+    out[tuple(dst)] = f[tuple(src)]
+    return out
+
+
+def _axis_idx(f, axis):
+    shape = [1] * f.ndim
+    shape[axis] = f.shape[axis]
+    return np.arange(f.shape[axis]).reshape(shape)
+
+
+def specified_flux_faces(f, vel, axis, upstream=False):
+    """flux_advection.py:288-347: tiered order-5 fluxes under specified BCs.
+    Face m (between cells m-1 and m) of an axis of n cells: flux5 on 3..n-3,
+    flux3 (+sign(vel) correction) on 2 and n-2, 2nd order on 1 and n-1 (with
+    the upstream normal-wind rule when ``upstream``), zero on face 0."""
+    q_im3, q_im2, q_im1 = _shift0(f, 3, axis), _shift0(f, 2, axis), _shift0(f, 1, axis)
+    q_ip1, q_ip2 = _shift0(f, -1, axis), _shift0(f, -2, axis)
+    face6 = (37.0 * (f + q_im1) - 8.0 * (q_ip1 + q_im2) + (q_ip2 + q_im3)) / 60.0
+    corr6 = ((q_ip2 - q_im3) - 5.0 * (q_ip1 - q_im2) + 10.0 * (f - q_im1)) / 60.0
+    face5 = face6 - np.sign(vel) * corr6
+    face4 = (7.0 * (f + q_im1) - (q_ip1 + q_im2)) / 12.0
+    corr4 = ((q_ip1 - q_im2) - 3.0 * (f - q_im1)) / 12.0
+    face3 = face4 + np.sign(vel) * corr4
+    face2 = 0.5 * (f + q_im1)
+    n = f.shape[axis]
+    idx = _axis_idx(f, axis)
+    if upstream:
+        low = 0.5 * (f + np.where(f < 0.0, f, q_im1))
+        high = 0.5 * (q_im1 + np.where(q_im1 > 0.0, q_im1, f))
+        face2 = np.where(idx == 1, low, np.where(idx == n - 1, high, face2))
+    five = (idx >= 3) & (idx <= n - 3)
+    three = (idx == 2) | (idx == n - 2)
+    two = (idx == 1) | (idx == n - 1)
+    return vel * np.where(five, face5, np.where(three, face3, np.where(two, face2, 0.0)))
+
+
+def specified_div(fq, axis):
+    """flux_advection.py:350-361: fq(m+1) - fq(m) on cells 1..n-2, zero on the outermost cells."""
+    d = _shift0(fq, -1, axis) - fq
+    idx = _axis_idx(fq, axis)
+    return np.where((idx >= 1) & (idx <= fq.shape[axis] - 2), d, 0.0)
+
+
+def couple_uv_specified(u, v, mu_total, m):
+    """flux_advection.py:364-391: full-face coupled velocities with edge-padded face masses."""
+    mpx = np.pad(mu_total, ((0, 0), (1, 0)), mode="edge")
+    muu = np.concatenate([0.5 * (mpx[:, 1:] + mpx[:, :-1]), mu_total[:, -1:]], axis=1)
+    mpy = np.pad(mu_total, ((1, 0), (0, 0)), mode="edge")
+    muv = np.concatenate([0.5 * (mpy[1:, :] + mpy[:-1, :]), mu_total[-1:, :]], axis=0)
+    c1, c2 = _col(m.c1h), _col(m.c2h)
+    return (c1 * muu[None] + c2) * u / m.msfuy[None], (c1 * muv[None] + c2) * v / m.msfvx[None]
+
+
 def _vflux_scalar(f, rom, fzm, fzp):
     """flux_advection.py:534-562 / 678-711 (order-3 vertical flux, rigid ends)."""
     nz = f.shape[0]
@@ -216,10 +280,14 @@ def _vflux_scalar(f, rom, fzm, fzp):
 def advect_scalar_flux(f, vel, rdx, rdy, rdzw, fzm, fzp):
     """flux_advection.py:482-568 (h5/v3 periodic)."""
     msftx = vel.msftx[None]
-    fqx = vel.ru * flux5_face(f, vel.ru, 2)
-    tend = -msftx * rdx * (np.roll(fqx, -1, 2) - fqx)
-    fqy = vel.rv * flux5_face(f, vel.rv, 1)
-    tend = tend - msftx * rdy * (np.roll(fqy, -1, 1) - fqy)
+    if getattr(vel, "specified", False):  # :512-520
+        tend = -msftx * rdx * specified_div(specified_flux_faces(f, vel.ru, 2), 2)
+        tend = tend - msftx * rdy * specified_div(specified_flux_faces(f, vel.rv, 1), 1)
+    else:
+        fqx = vel.ru * flux5_face(f, vel.ru, 2)
+        tend = -msftx * rdx * (np.roll(fqx, -1, 2) - fqx)
+        fqy = vel.rv * flux5_face(f, vel.rv, 1)
+        tend = tend - msftx * rdy * (np.roll(fqy, -1, 1) - fqy)
     nz = f.shape[0]
     vflux = _vflux_scalar(f, vel.rom, fzm, fzp)
     return tend - _col(rdzw) * (vflux[1:] - vflux[:nz])
@@ -258,18 +326,26 @@ def advect_scalar_flux_limited(f, fo, vel, opt, mut, mu_old, m, rdx, rdy, dt):
     mu_u = c1 * muu[None] + c2
     mu_v = c1 * muv[None] + c2
     dx, dy = 1.0 / rdx, 1.0 / rdy
+    spec = bool(getattr(vel, "specified", False))  # :816-828, 841, 963-968
+    ip1 = (lambda a, ax: _shift0(a, -1, ax)) if spec else (lambda a, ax: np.roll(a, -1, ax))
     fqxl = _flux_upwind_face(fo, vel.ru, mu_u, dx, dt, 2)
     fqyl = _flux_upwind_face(fo, vel.rv, mu_v, dy, dt, 1)
     fqzl = _flux_upwind_face_z(fo, vel.rom, mu_h, rdzw, dt)
-    fqx = vel.ru * flux5_face(f, vel.ru, 2) - fqxl
-    fqy = vel.rv * flux5_face(f, vel.rv, 1) - fqyl
+    if spec:
+        fqxl = np.where(_axis_idx(fqxl, 2) == 0, 0.0, fqxl)
+        fqyl = np.where(_axis_idx(fqyl, 1) == 0, 0.0, fqyl)
+        fqx = specified_flux_faces(f, vel.ru, 2) - fqxl
+        fqy = specified_flux_faces(f, vel.rv, 1) - fqyl
+    else:
+        fqx = vel.ru * flux5_face(f, vel.ru, 2) - fqxl
+        fqy = vel.rv * flux5_face(f, vel.rv, 1) - fqyl
     fqz = _vflux_scalar(f, vel.rom, m.fnm, m.fnp) - fqzl
     mass_old = c1 * mu_old[None] + c2
-    div_low = (msftx * msftx * (rdx * (np.roll(fqxl, -1, 2) - fqxl) + rdy * (np.roll(fqyl, -1, 1) - fqyl))
+    div_low = (msftx * msftx * (rdx * (ip1(fqxl, 2) - fqxl) + rdy * (ip1(fqyl, 1) - fqyl))
                + msftx * _col(rdzw) * (fqzl[1:] - fqzl[:nz]))
     ph_low = mass_old * fo - dt * div_low
-    fqx_ip1 = np.roll(fqx, -1, 2)
-    fqy_jp1 = np.roll(fqy, -1, 1)
+    fqx_ip1 = ip1(fqx, 2)
+    fqy_jp1 = ip1(fqy, 1)
     fqz_kp1, fqz_k = fqz[1:], fqz[:nz]
     pos = lambda a: np.maximum(0.0, a)
     neg = lambda a: np.minimum(0.0, a)
@@ -312,6 +388,10 @@ def advect_scalar_flux_limited(f, fo, vel, opt, mut, mu_old, m, rdx, rdy, dt):
     fx = fqx_lim + fqxl
     fy = fqy_lim + fqyl
     fz = fqz_lim + fqzl
+    if spec:
+        tend = -msftx * rdx * specified_div(fx, 2)
+        tend = tend - msftx * rdy * specified_div(fy, 1)
+        return tend - _col(rdzw) * (fz[1:] - fz[:nz])
     tend = -msftx * rdx * (np.roll(fx, -1, 2) - fx)
     tend = tend - msftx * rdy * (np.roll(fy, -1, 1) - fy)
     return tend - _col(rdzw) * (fz[1:] - fz[:nz])
@@ -357,8 +437,42 @@ def _vdiv_w(w, rom, rdn, top_lid):
     return tend
 
 
+def _advect_u_flux_specified(u, vel, rdx, rdy, m):
+    """flux_advection.py:1150-1182: tiers on the full staggered u (upstream
+    rule on the normal x faces), faces 1..nx-1 updated."""
+    nxs = u.shape[-1]
+    msfux = m.msfux[None]
+    velx = 0.5 * (vel.ru_full + _shift0(vel.ru_full, 1, 2))
+    tend = -msfux * rdx * specified_div(specified_flux_faces(u, velx, 2, upstream=True), 2)
+    rv_pad = np.pad(vel.rv_full, ((0, 0), (0, 0), (1, 1)))
+    vely = (0.5 * (rv_pad[:, :, 1:] + rv_pad[:, :, :-1]))[:, : u.shape[1], :]
+    tend = tend - msfux * rdy * specified_div(specified_flux_faces(u, vely, 1), 1)
+    rom_pad = np.pad(vel.rom, ((0, 0), (0, 0), (1, 1)))
+    tend = tend + _vdiv3(u, 0.5 * (rom_pad[:, :, 1:] + rom_pad[:, :, :-1]), m.rdnw, m.fnm, m.fnp)
+    fi = np.arange(nxs).reshape(1, 1, nxs)
+    return np.where((fi >= 1) & (fi <= nxs - 2), tend, 0.0)
+
+
+def _advect_v_flux_specified(v, vel, rdx, rdy, m):
+    """flux_advection.py:1217-1254: the mirror of the u path (upstream rule on
+    the normal y faces), rows 1..ny-1 updated."""
+    nys = v.shape[-2]
+    msfvy, msfvx = m.msfvy[None], m.msfvx[None]
+    ru_pad = np.pad(vel.ru_full, ((0, 0), (1, 1), (0, 0)))
+    velx = (0.5 * (ru_pad[:, 1:, :] + ru_pad[:, :-1, :]))[:, :, : v.shape[-1]]
+    tend = -msfvy * rdx * specified_div(specified_flux_faces(v, velx, 2), 2)
+    vely = 0.5 * (vel.rv_full + _shift0(vel.rv_full, 1, 1))
+    tend = tend - msfvy * rdy * specified_div(specified_flux_faces(v, vely, 1, upstream=True), 1)
+    rom_pad = np.pad(vel.rom, ((0, 0), (1, 1), (0, 0)))
+    tend = tend + (msfvy / msfvx) * _vdiv3(v, 0.5 * (rom_pad[:, 1:, :] + rom_pad[:, :-1, :]), m.rdnw, m.fnm, m.fnp)
+    ri = np.arange(nys).reshape(1, nys, 1)
+    return np.where((ri >= 1) & (ri <= nys - 2), tend, 0.0)
+
+
 def advect_u_flux(u, vel, rdx, rdy, m):
-    """flux_advection.py:1131-1202 (periodic path)."""
+    """flux_advection.py:1131-1202 (periodic path; specified degrade at :1150-1182)."""
+    if getattr(vel, "specified", False):
+        return _advect_u_flux_specified(u, vel, rdx, rdy, m)
     nx = vel.ru.shape[-1]
     ny = u.shape[1]
     u_f = u[..., :nx]
@@ -375,7 +489,9 @@ def advect_u_flux(u, vel, rdx, rdy, m):
 
 
 def advect_v_flux(v, vel, rdx, rdy, m):
-    """flux_advection.py:1205-1274 (periodic path)."""
+    """flux_advection.py:1205-1274 (periodic path; specified degrade at :1217-1254)."""
+    if getattr(vel, "specified", False):
+        return _advect_v_flux_specified(v, vel, rdx, rdy, m)
     ny = vel.rv.shape[-2]
     v_f = v[:, :ny, :]
     msfvy = vel.msfvy[None]
@@ -402,10 +518,14 @@ def _mass_to_full(f, fzm, fzp):
 
 
 def advect_w_flux(w, vel, rdx, rdy, m, top_lid):
-    """flux_advection.py:1277-1329 (periodic path)."""
+    """flux_advection.py:1277-1329 (periodic path; specified degrade at :1305-1318)."""
     msftx = vel.msftx[None]
     ru_w = _mass_to_full(vel.ru, m.fnm, m.fnp)
     rv_w = _mass_to_full(vel.rv, m.fnm, m.fnp)
+    if getattr(vel, "specified", False):  # :1305-1318
+        tend = -msftx * rdx * specified_div(specified_flux_faces(w, ru_w, 2), 2)
+        tend = tend - msftx * rdy * specified_div(specified_flux_faces(w, rv_w, 1), 1)
+        return tend + _vdiv_w(w, vel.rom, m.rdn, top_lid)
     fqx = ru_w * flux5_face(w, ru_w, 2)
     tend = -msftx * rdx * (np.roll(fqx, -1, 2) - fqx)
     if w.shape[1] > 1:
@@ -1303,6 +1423,9 @@ def rk_scan_step(carry, nl: Namelist, lead_seconds=None):
     for rk_step, dt_rk, dts, nsub in stages:
         s = state
         vel = couple_velocities_periodic(s.u, s.v, s.mu_total, m, rdx, rdy)
+        if nl.specified_adv_degrade and specified:  # operational_mode.py:2464-2475, 2494-2507
+            vel.specified = True
+            vel.ru_full, vel.rv_full = couple_uv_specified(s.u, s.v, s.mu_total, m)
         tend = augment_large_step_tendencies(s, origin, vel, nl, rk_step)
         q_tend = moisture_coupled_tendencies(s, origin, vel, nl, rk_step) if moist else None
         ww_stage = stage_omega_specified(s.u, s.v, s.mu_total, m, rdx, rdy) if (specified or nested) else vel.rom

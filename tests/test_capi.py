@@ -67,6 +67,8 @@ def _params(lib, **kw):
     (dict(precision=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(column_lanes=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
     (dict(column_width=24), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(specified_adv_degrade=2), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    (dict(run_boundary=1, bc_ideal=0, specified_adv_degrade=1, nx=6), _capi.WRFGPU_ERR_BAD_SHAPE),
     (dict(march_levels=7), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
 ])
 def test_validate_rejects(lib, kw, code):

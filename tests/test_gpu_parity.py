@@ -131,6 +131,20 @@ def test_per_step_parity_rhs_ph_order6_specified(cuda_ready, top_lid):
         assert not bad, f"top_lid={top_lid} step {n}: {bad}"
 
 
+@pytest.mark.parametrize("shape,theta_opt,moist_opt", [((40, 18, 12), 0, 1), ((18, 40, 12), 2, 2)])
+def test_per_step_parity_specified_adv_degrade(cuda_ready, shape, theta_opt, moist_opt):
+    """specified_adv_degrade: tiered flux orders near the specified edges and
+    no horizontal advection of the outermost cells in the scalar (plain and
+    limited), u, v and w operators; grids wider than one 32 x 8 tile so the
+    domain edges and the tile edges differ."""
+    nx, ny, nz = shape
+    case = _with_map_factors(cases.real_like_moist(nx, ny, nz, hmax=800.0, specified=True), seed=5)
+    case.controls.update(specified_adv_degrade=True, scalar_adv_opt=theta_opt, moist_adv_opt=moist_opt)
+    for n, e in enumerate(_per_step(case, 2)):
+        bad = {k: v for k, v in e.items() if not v <= _tol(k)}
+        assert not bad, f"{shape} step {n}: {bad}"
+
+
 def test_per_step_parity_map_factors_periodic(cuda_ready):
     case = _with_map_factors(cases.real_like_moist(24, 20, 14, hmax=800.0, specified=False), seed=11)
     for n, e in enumerate(_per_step(case, 2)):

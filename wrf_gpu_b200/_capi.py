@@ -41,7 +41,7 @@ class StepParams(ctypes.Structure):
         ("moist_cqw", _I), ("w_coriolis", _I), ("precision", _I),
         ("cf1", _D), ("cf2", _D), ("cf3", _D), ("p_top", _D),
         ("cfn", _D), ("cfn1", _D),
-        ("march_levels", _I), ("column_lanes", _I), ("column_width", _I),
+        ("march_levels", _I), ("column_lanes", _I), ("column_width", _I), ("specified_adv_degrade", _I),
     ]
 
 

@@ -409,6 +409,10 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13 or 16");
   if (p->column_width != 0 && p->column_width != 16 && p->column_width != 32)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 16 or 32");
+  if (p->specified_adv_degrade != 0 && p->specified_adv_degrade != 1)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "specified_adv_degrade must be 0 or 1");
+  if (spec && p->specified_adv_degrade && (p->nx < 7 || p->ny < 7))
+    return fail(WRFGPU_ERR_BAD_SHAPE, "the specified advection degradation needs nx, ny >= 7");
   return WRFGPU_OK;
 }
 
@@ -543,6 +547,9 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   auto kVface = mixed ? k_vface_tiled<float> : k_vface_tiled<double>;
   // rhs_ph's order<=6 specified-boundary branch (core/rhs_ph.py:281-345)
   const bool ph_order6 = specified && p.h_sca_adv_order >= 4;
+  // specified-boundary advection degradation (operational_mode.py:2464-2475,
+  // 2494-2507; flux_advection.py:288-391): tiered faces, masked divergences
+  const int deg = (specified && p.specified_adv_degrade) ? 1 : 0;
   auto kWface = mixed ? (ph_order6 ? k_wface_tiled<float, true> : k_wface_tiled<float, false>)
                       : (ph_order6 ? k_wface_tiled<double, true> : k_wface_tiled<double, false>);
   // marching kernels for the chosen chunk size (5, 10 or 25 levels)
@@ -575,12 +582,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     UFaceOut uo{w.u_tend, w.u_w, w.cqu};
     PROF("k_uface");
     kUface<<<tgrd(nx + 1, ny, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
-                                                               in->base_u, p.top_lid, p.run_boundary, uo);
+                                                               in->base_u, p.top_lid, p.run_boundary, deg, uo);
     LAUNCH_CHECK("k_uface");
     VFaceOut vo{w.v_tend, w.v_w, w.cqv};
     PROF("k_vface");
     kVface<<<tgrd(nx, ny + 1, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
-                                                               in->base_v, p.top_lid, p.run_boundary, vo);
+                                                               in->base_v, p.top_lid, p.run_boundary, deg, vo);
     LAUNCH_CHECK("k_vface");
     const bool lim_theta = (rk == 3) && (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2);
     const bool lim_moist = moist && (rk == 3) && (p.moist_adv_opt == 1 || p.moist_adv_opt == 2);
@@ -593,12 +600,13 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       const int nfields = 1 + ((moist && !lim_moist) ? 6 : 0);
       const int nchunk = march_nchunk(nz, kc);
       kScalar<<<tgrd(nx, ny, nfields * nchunk), tblk(), 0, stream>>>(
-          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, mo);
+          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, deg, mo);
     }
     LAUNCH_CHECK("k_mass");
     if (lim_theta || lim_moist) {
       LimArgs la;
       la.ru = w.ru; la.rv = w.rv; la.rom = w.rom; la.mut = s.mu_total; la.mu_old = origin.mu_total; la.dt = dt;
+      la.deg = deg;
       set_lim_constants(la, g.rdx, g.rdy);
       if (lim_theta) {
         la.opt = p.scalar_adv_opt;
@@ -632,7 +640,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     PROF("k_wface");
     kWface<<<tgrd(nx, ny, nz + 1), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot,
                                                                w.mub, w.mut, w.muts0, w.muu, w.muv, in->base_w,
-                                                               p.top_lid, p.moist_cqw, p.w_coriolis, wo);
+                                                               p.top_lid, p.moist_cqw, p.w_coriolis, deg, wo);
     LAUNCH_CHECK("k_wface");
     const double x = 0.5 * dts * G * eps1;
     const double cof = x * x;

@@ -150,6 +150,40 @@ __device__ __forceinline__ double vflux3<float>(double vel, double qkm2, double 
   return (double)(v * (flux4 + s * corr));
 }
 
+// flux3 of a horizontal face: flux4 + sign(vel) * correction
+// (flux_advection.py:314-317).
+template <typename F>
+__device__ __forceinline__ double hflux3(double vel, double qm2, double qm1, double q0, double qp1) {
+  const double face4 = div_rcp(7.0 * (q0 + qm1) - (qp1 + qm2), 12.0, R12);
+  const double corr4 = div_rcp((qp1 - qm2) - 3.0 * (q0 - qm1), 12.0, R12);
+  return vel * (face4 + sgn(vel) * corr4);
+}
+template <>
+__device__ __forceinline__ double hflux3<float>(double vel, double qm2, double qm1, double q0, double qp1) {
+  const float v = (float)vel, a2 = (float)qm2, a1 = (float)qm1, b0 = (float)q0, b1 = (float)qp1;
+  const float face4 = (7.0f * (b0 + a1) - (b1 + a2)) * (1.0f / 12.0f);
+  const float corr = ((b1 - a2) - 3.0f * (b0 - a1)) * (1.0f / 12.0f);
+  const float s = (float)((v > 0.0f) - (v < 0.0f));
+  return (double)(v * (face4 + s * corr));
+}
+
+// Flux at face m (between cells m-1 and m) of an axis of n cells under the
+// specified-boundary advection degradation (flux_advection.py:288-347):
+// flux5 on faces 3..n-3, flux3 on 2 and n-2, 2nd order on 1 and n-1 (with
+// the upstream rule for the normal momentum component: the boundary-side
+// value is replaced by the interior one under inflow / outflow), zero on
+// face 0 (and on face n, the wrap of face 0).  Needs n >= 7, so that every
+// tier reads only cells 0..n-1.
+template <typename F>
+__device__ __forceinline__ double hflux_spec(int m, int n, bool upstream, double vel, double qm3, double qm2,
+                                             double qm1, double q0, double qp1, double qp2) {
+  if (m >= 3 && m <= n - 3) return hflux5<F>(vel, qm3, qm2, qm1, q0, qp1, qp2);
+  if (m == 2 || m == n - 2) return hflux3<F>(vel, qm2, qm1, q0, qp1);
+  if (m == 1) return vel * (0.5 * (q0 + ((upstream && q0 < 0.0) ? q0 : qm1)));
+  if (m == n - 1) return vel * (0.5 * (qm1 + ((upstream && qm1 > 0.0) ? qm1 : q0)));
+  return vel * 0.0;
+}
+
 // Dry inverse density from the EOS (acoustic_wrf.py:187-206, qvf = 1).
 __device__ __forceinline__ double inv_density(double theta, double p) {
   return (R_D / P0) * theta * 1.0 * pow(dmax(p, 1.0) / P0, CVPM);

@@ -229,6 +229,7 @@ struct LimArgs {
   double dt;
   int opt;               // 1 PD, 2 mono
   double offset;         // subtracted from both fields (300 for theta, 0 for q)
+  int deg;               // specified-boundary advection degradation (tiered faces, masked divergence)
   // Per-launch constants of the upwind fluxes (set by set_lim_constants):
   // dx = 1/rdx and dy = 1/rdy as the reference forms them, their correctly
   // rounded reciprocals (divisors for div_rcp), 1/dt, dx/dt and dy/dt.

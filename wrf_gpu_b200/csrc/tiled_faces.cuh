@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muu, const double *muus,
                                                            const double *base_u, int top_lid, int run_boundary,
-                                                           UFaceOut o) {
+                                                           int deg, UFaceOut o) {
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<1, 1>;
@@ -96,19 +96,37 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
   const int i = i0 + tx, j = j0 + ty;
-  load_tile<3, 3>(su, s.u + (size_t)k * ny * nxu, nxu, i0, j0, nx, ny, 0.0);
+  // (the specified degradation reads the real east face u(nx): no x wrap)
+  load_tile<3, 3>(su, s.u + (size_t)k * ny * nxu, nxu, i0, j0, deg ? nx + 1 : nx, ny, 0.0);
   load_tile<1, 0>(sru, ru + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
   load_tile<1, 1>(srv, rv + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
   __syncthreads();
   if (i > nx || j >= ny) return;
   const size_t cu = ix3(k, j, i, ny, nxu);
   double tend;
-  if (i < nx) {
+  if (deg && (i == 0 || i == nx)) {
+    tend = 0.0;  // the specified degradation updates u faces 1..nx-1 only (flux_advection.py:1177-1182)
+  } else if (i < nx) {
     auto Q = [&](int r, int cc) { return su[(r + 3) * TQ::W + (cc + 3)]; };
     auto RU = [&](int cc) { return sru[ty * TR::W + (cc + 1)]; };
     auto RV = [&](int r, int cc) { return srv[(r + 1) * TV::W + (cc + 1)]; };
+    // full-face coupled u at the domain-edge faces 0 and nx
+    // (couple_uv_specified, flux_advection.py:364-391: edge-padded face mass)
+    auto ru_edge = [&](int ie) {
+      const double mu_e = (ie == 0) ? 0.5 * (ld(s.mu_total, ix2(j, 0, nx)) + ld(s.mu_total, ix2(j, 0, nx)))
+                                    : ld(s.mu_total, ix2(j, nx - 1, nx));
+      return div_msf((ld(g.c1h, k) * mu_e + ld(g.c2h, k)) * ld(s.u, ix3(k, j, ie, ny, nxu)), g.msfuy, g.rmsfuy,
+                     ix2(j, ie, nxu));
+    };
     auto fqx = [&](int m) {
-      const double vel = 0.5 * (RU(m) + RU(m - 1));
+      double vel = 0.5 * (RU(m) + RU(m - 1));
+      if (deg) {
+        const int gm = i0 + m;
+        if (gm == 1) vel = 0.5 * (RU(m) + ru_edge(0));
+        else if (gm == nx) vel = 0.5 * (ru_edge(nx) + RU(m - 1));
+        return hflux_spec<F>(gm, nx + 1, true, vel, Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1),
+                             Q(ty, m + 2));
+      }
       return hflux5<F>(vel, Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2));
     };
     const double msfux_c = ld(g.msfux, ix2(j, i, nxu));
@@ -116,9 +134,13 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
     if (ny > 1) {
       auto fqy = [&](int r) {
         const double vel = 0.5 * (RV(r, tx) + RV(r, tx - 1));
+        if (deg)
+          return hflux_spec<F>(j0 + r, ny, false, vel, Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx),
+                               Q(r + 1, tx), Q(r + 2, tx));
         return hflux5<F>(vel, Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx));
       };
-      tend = tend - msfux_c * g.rdy * (fqy(ty + 1) - fqy(ty));
+      const bool yin = !deg || (j >= 1 && j <= ny - 2);
+      tend = tend - msfux_c * g.rdy * (yin ? (fqy(ty + 1) - fqy(ty)) : 0.0);
     }
     const int im = wrp(i - 1, nx);
     auto romq = [&](int m) { return 0.5 * (ld(rom, ix3(m, j, i, ny, nx)) + ld(rom, ix3(m, j, im, ny, nx))); };
@@ -204,7 +226,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, 
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muv, const double *muvs,
                                                            const double *base_v, int top_lid, int run_boundary,
-                                                           VFaceOut o) {
+                                                           int deg, VFaceOut o) {
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 1>;
   using TV = Tile<0, 1>;
@@ -215,14 +237,17 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
   const int i = i0 + tx, j = j0 + ty;
-  load_tile<3, 3>(sv, s.v + (size_t)k * nyv * nx, nx, i0, j0, nx, ny, 0.0);
+  // (the specified degradation reads the real north face v(ny): no y wrap)
+  load_tile<3, 3>(sv, s.v + (size_t)k * nyv * nx, nx, i0, j0, nx, deg ? ny + 1 : ny, 0.0);
   load_tile<1, 1>(sru, ru + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
   load_tile<0, 1>(srv, rv + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
   __syncthreads();
   if (i >= nx || j > ny) return;
   const size_t cv = ix3(k, j, i, nyv, nx);
   double tend;
-  if (j < ny) {
+  if (deg && (j == 0 || j == ny)) {
+    tend = 0.0;  // the specified degradation updates v rows 1..ny-1 only (flux_advection.py:1250-1254)
+  } else if (j < ny) {
     auto Q = [&](int r, int cc) { return sv[(r + 3) * TQ::W + (cc + 3)]; };
     auto RU = [&](int r, int cc) { return sru[(r + 1) * TR::W + (cc + 1)]; };
     auto RV = [&](int r) { return srv[(r + 1) * TV::W + tx]; };
@@ -230,11 +255,29 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, 
     const double msfvx_c = ld(g.msfvx, ix2(j, i, nx));
     auto fqx = [&](int m) {
       const double vel = 0.5 * (RU(ty, m) + RU(ty - 1, m));
+      if (deg)
+        return hflux_spec<F>(i0 + m, nx, false, vel, Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m),
+                             Q(ty, m + 1), Q(ty, m + 2));
       return hflux5<F>(vel, Q(ty, m - 3), Q(ty, m - 2), Q(ty, m - 1), Q(ty, m), Q(ty, m + 1), Q(ty, m + 2));
     };
-    tend = -msfvy_c * g.rdx * (fqx(tx + 1) - fqx(tx));
+    const bool xin = !deg || (i >= 1 && i <= nx - 2);
+    tend = -msfvy_c * g.rdx * (xin ? (fqx(tx + 1) - fqx(tx)) : 0.0);
+    // full-face coupled v at the domain-edge rows 0 and ny (flux_advection.py:364-391)
+    auto rv_edge = [&](int je) {
+      const double mu_e = (je == 0) ? 0.5 * (ld(s.mu_total, ix2(0, i, nx)) + ld(s.mu_total, ix2(0, i, nx)))
+                                    : ld(s.mu_total, ix2(ny - 1, i, nx));
+      return div_msf((ld(g.c1h, k) * mu_e + ld(g.c2h, k)) * ld(s.v, ix3(k, je, i, nyv, nx)), g.msfvx, g.rmsfvx,
+                     ix2(je, i, nx));
+    };
     auto fqy = [&](int r) {
-      const double vel = 0.5 * (RV(r) + RV(r - 1));
+      double vel = 0.5 * (RV(r) + RV(r - 1));
+      if (deg) {
+        const int gr = j0 + r;
+        if (gr == 1) vel = 0.5 * (RV(r) + rv_edge(0));
+        else if (gr == ny) vel = 0.5 * (rv_edge(ny) + RV(r - 1));
+        return hflux_spec<F>(gr, ny + 1, true, vel, Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx),
+                             Q(r + 2, tx));
+      }
       return hflux5<F>(vel, Q(r - 3, tx), Q(r - 2, tx), Q(r - 1, tx), Q(r, tx), Q(r + 1, tx), Q(r + 2, tx));
     };
     tend = tend - msfvy_c * g.rdy * (fqy(ty + 1) - fqy(ty));
@@ -363,7 +406,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
                                                            const double *mub, const double *mut, const double *muts0,
                                                            const double *muu, const double *muv,
                                                            const double *base_w, int top_lid, int moist_cqw,
-                                                           int w_coriolis, WFaceOut o) {
+                                                           int w_coriolis, int deg, WFaceOut o) {
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
@@ -419,15 +462,24 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
   const double msftx = ld(g.msftx, c2d);
   auto fqx = [&](int m) {
     const double vel = sru[ty * TR::W + (m + 1)];
+    if (deg)
+      return hflux_spec<F>(i0 + m, nx, false, vel, W_(ty, m - 3), W_(ty, m - 2), W_(ty, m - 1), W_(ty, m),
+                           W_(ty, m + 1), W_(ty, m + 2));
     return hflux5<F>(vel, W_(ty, m - 3), W_(ty, m - 2), W_(ty, m - 1), W_(ty, m), W_(ty, m + 1), W_(ty, m + 2));
   };
-  double adv = -msftx * g.rdx * (fqx(tx + 1) - fqx(tx));
-  if (ny > 1) {
+  // the specified degradation: tiered faces and no horizontal divergence on
+  // the outermost cells (flux_advection.py:1305-1318)
+  const bool xin = !deg || (i >= 1 && i <= nx - 2), yin = !deg || (j >= 1 && j <= ny - 2);
+  double adv = -msftx * g.rdx * (xin ? (fqx(tx + 1) - fqx(tx)) : 0.0);
+  if (ny > 1 || deg) {
     auto fqy = [&](int r) {
       const double vel = srv[(r + 1) * TV::W + tx];
+      if (deg)
+        return hflux_spec<F>(j0 + r, ny, false, vel, W_(r - 3, tx), W_(r - 2, tx), W_(r - 1, tx), W_(r, tx),
+                             W_(r + 1, tx), W_(r + 2, tx));
       return hflux5<F>(vel, W_(r - 3, tx), W_(r - 2, tx), W_(r - 1, tx), W_(r, tx), W_(r + 1, tx), W_(r + 2, tx));
     };
-    adv = adv - msftx * g.rdy * (fqy(ty + 1) - fqy(ty));
+    adv = adv - msftx * g.rdy * (yin ? (fqy(ty + 1) - fqy(ty)) : 0.0);
   }
   {
     auto wc = [&](int kk) { return ld(s.w, ix3(kk, j, i, ny, nx)); };

@@ -79,7 +79,8 @@ __device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int 
 // one face per thread item, into shared memory.  Edge tiles compute a few
 // harmless extra faces from the periodically wrapped staged values.
 template <typename F>
-__device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a, const LimTiles &t, int k) {
+__device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int i0,
+                                                int j0) {
   using TQ = Tile<3, 3>;
   using TO = Tile<1, 1>;
   using TR = Tile<1, 0>;
@@ -101,8 +102,13 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
       const double vel = t.ru[r * TR::W + (m + 1)];
       const double muu = 0.5 * (MT(r, m) + MT(r, m - 1));
       const double mu_u = c1 * muu + c2;
-      const double lo = upw(QO(r, m - 1), QO(r, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
-      const double hi = hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
+      // the specified degradation: tiered high-order faces, no low-order
+      // flux on face 0 (nor on face nx, its wrap)
+      const int gm = i0 + m;
+      const double lo = (a.deg && (gm == 0 || gm == g.nx)) ? 0.0 : upw(QO(r, m - 1), QO(r, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
+      const double hi = a.deg ? hflux_spec<F>(gm, g.nx, false, vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m),
+                                              Q(r, m + 1), Q(r, m + 2))
+                              : hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
       t.fxl[e] = lo;
       t.fxa[e] = hi - lo;
     } else {
@@ -111,8 +117,11 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
       const double vel = t.rv[(r + 1) * TV::W + cc];
       const double muv = 0.5 * (MT(r, cc) + MT(r - 1, cc));
       const double mu_v = c1 * muv + c2;
-      const double lo = upw(QO(r - 1, cc), QO(r, cc), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
-      const double hi = hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc));
+      const int gm = j0 + r;
+      const double lo = (a.deg && (gm == 0 || gm == g.ny)) ? 0.0 : upw(QO(r - 1, cc), QO(r, cc), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
+      const double hi = a.deg ? hflux_spec<F>(gm, g.ny, false, vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc),
+                                              Q(r + 1, cc), Q(r + 2, cc))
+                              : hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc));
       t.fyl[e2] = lo;
       t.fya[e2] = hi - lo;
     }
@@ -260,8 +269,9 @@ __device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a,
   fz0 = fz0 + cf.lz0;
   fz1 = fz1 + cf.lz1;
   const double msftx = ld(g.msftx, ix2(j, i, nx));
-  double tend = -msftx * g.rdx * (fx1 - fx0);
-  tend = tend - msftx * g.rdy * (fy1 - fy0);
+  const bool xin = !a.deg || (i >= 1 && i <= nx - 2), yin = !a.deg || (j >= 1 && j <= ny - 2);
+  double tend = -msftx * g.rdx * (xin ? (fx1 - fx0) : 0.0);
+  tend = tend - msftx * g.rdy * (yin ? (fy1 - fy0) : 0.0);
   tend = tend - ld(g.rdnw, k) * (fz1 - fz0);
   return tend;
 }

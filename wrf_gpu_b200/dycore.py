@@ -258,7 +258,8 @@ class OperationalNamelist:
                   run_boundary=c["run_boundary"], bc_source="ideal" if c["bc_ideal"] else "wrfbdy",
                   boundary_config=bc, w_damping=c["w_damping"], damp_opt=c["damp_opt"], dampcoef=c["dampcoef"],
                   zdamp=c["zdamp"], use_flux_advection=True, scalar_adv_opt=c["scalar_adv_opt"],
-                  moist_adv_opt=c["moist_adv_opt"], moist_cqw=c["moist_cqw"], w_coriolis=c["w_coriolis"])
+                  moist_adv_opt=c["moist_adv_opt"], moist_cqw=c["moist_cqw"], w_coriolis=c["w_coriolis"],
+                  specified_adv_degrade=bool(c.get("specified_adv_degrade", False)))
         kw.update(overrides)
         return cls(**kw)
 
@@ -274,8 +275,6 @@ def _unsupported(nl: OperationalNamelist, physics_tendencies) -> str | None:
         return "explicit diffusion options are not built"
     if nl.specified_bdy_cadence:
         return "specified_bdy_cadence is not built"
-    if nl.specified_adv_degrade:
-        return "specified_adv_degrade is not built"
     if not nl.boundary_config.force_geopotential and nl.run_boundary and nl.bc_source != "ideal":
         return "nested (force_geopotential=False) boundaries are not built"
     if nl.moist_adv_opt and nl.mp_physics in (7, 17, 18, 19, 21, 22, 24, 26, 27, 28, 38):
@@ -308,6 +307,7 @@ def step_params(nl: OperationalNamelist) -> _capi.StepParams:
     p.normal_bdy_relax_strength = -1.0 if s is None else float(s)
     p.moist_cqw, p.w_coriolis = int(bool(nl.moist_cqw)), int(bool(nl.w_coriolis))
     p.precision = _capi.WRFGPU_PRECISION_MIXED if nl.precision == "mixed" else _capi.WRFGPU_PRECISION_FP64
+    p.specified_adv_degrade = 1 if nl.specified_adv_degrade else 0
     m = nl.metrics
     p.cf1, p.cf2, p.cf3, p.p_top = m.cf1, m.cf2, m.cf3, m.p_top
     p.cfn, p.cfn1 = m.cfn()
