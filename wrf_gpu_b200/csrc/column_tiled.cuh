@@ -246,11 +246,9 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
   // ---------------- P5: theta update, t_2ave, wd -> A0, buoy -> A1, coef -> A5 ----------------
   const double muts = valid ? A.muts[c2d] : 1.0;
   const double muave = valid ? A.muave[c2d] : 0.0;
-  // The phase's global stores follow all its loads (a store to global memory
-  // would keep the next level's loads behind it); new t_2ave -> A6.
   if (valid) {
+    for (int k = ty; k <= nz; k += TY) A.ww[M(k)] = S(A3, k);
     cp_async_wait<0>();  // this thread's staged levels
-#pragma unroll 4
     for (int k = ty; k < nz; k += TY) {
       double thw = S(A7, k);
       const double t2ave_old = S(A6, k);
@@ -263,29 +261,24 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
         const double tend = ld(hdiv, M(k)) + ld(g.rdnw, k) * (wdtn_hi - wdtn_lo);
         const double theta_i = thw + msfty * dts * S(A4, k);
         thw = theta_i - dts * msfty * tend;
+        A.theta_w[M(k)] = thw;
         S(A7, k) = thw;
       }
       const double mass_h = ld(g.c1h, k) * muts + ld(g.c2h, k);
       const double half = 0.5 * (eps_p * thw + eps_m * t2ave_old);
       const double t2a = (half + (ld(g.c1h, k) * muave) * T0) / (mass_h * (T0 + T1(k, j, i)));
-      S(A6, k) = t2a;
+      A.t2ave[M(k)] = t2a;
       const double c2a_k = ld(A.c2a, M(k));
       S(A1, k) = c2a_k * ld(A.alt, M(k)) * t2a;
       S(A5, k) = c2a_k * ld(g.rdnw, k) / safe12(ld(g.c1h, k) * mut + ld(g.c2h, k));  // coef(k) for P7
       const double wwm = 0.5 * (S(A3, k + 1) + S(A3, k));
       S(A0, k) = wwm * ld(g.rdnw, k) * (ld(A.pt1, M(k + 1)) - ld(A.pt1, M(k)));
     }
-    for (int k = ty; k <= nz; k += TY) A.ww[M(k)] = S(A3, k);
-    for (int k = ty; k < nz; k += TY) {
-      if (active) A.theta_w[M(k)] = S(A7, k);
-      A.t2ave[M(k)] = S(A6, k);
-    }
   }
   __syncthreads();
   // ---------------- P6: rhs -> A2 (faces 1..nz), old ph -> A4 (faces 0..nz) ----------------
   const double c05gem = 0.5 * G * eps_m;
   if (valid) {
-#pragma unroll 4
     for (int f = ty; f <= nz; f += TY) {
       const double phf = ld(A.ph, M(f));
       S(A4, f) = phf;
@@ -445,10 +438,9 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
     }
   }
   __syncthreads();
-  // ---------------- P10: calc_p_rho with smdiv memory; p -> A0, pm1 -> A1, al -> A3, then stored ----------------
+  // ---------------- P10: calc_p_rho with smdiv memory ----------------
   if (valid) {
     const double mu_work = muts - mut;
-#pragma unroll 4
     for (int k = ty; k < nz; k += TY) {
       const double mass = ld(g.c1h, k) * muts + ld(g.c2h, k);
       const double safe = safe12(mass);
@@ -460,14 +452,9 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
       const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
       const double pp = ld(A.c2a, M(k)) * (altc * (S(A7, k) - mu_term * t1) / (safe * sttr) - al);
       const double pm1 = ld(A.pm1, M(k));
-      S(A0, k) = pp + SMDIV * (pp - pm1);
-      S(A1, k) = pp;
-      S(A3, k) = al;
-    }
-    for (int k = ty; k < nz; k += TY) {
-      A.p[M(k)] = S(A0, k);
-      A.pm1[M(k)] = S(A1, k);
-      A.al[M(k)] = S(A3, k);
+      A.p[M(k)] = pp + SMDIV * (pp - pm1);
+      A.pm1[M(k)] = pp;
+      A.al[M(k)] = al;
     }
   }
 }

@@ -543,20 +543,28 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   // Advective-flux arithmetic: float64 (the reference's), or the mixed
   // variant's FP32 fluxes with float64 accumulation.
   const bool mixed = p.precision == WRFGPU_PRECISION_MIXED;
-  auto kUface = mixed ? k_uface_tiled<float> : k_uface_tiled<double>;
-  auto kVface = mixed ? k_vface_tiled<float> : k_vface_tiled<double>;
   // rhs_ph's order<=6 specified-boundary branch (core/rhs_ph.py:281-345)
   const bool ph_order6 = specified && p.h_sca_adv_order >= 4;
   // specified-boundary advection degradation (operational_mode.py:2464-2475,
-  // 2494-2507; flux_advection.py:288-391): tiered faces, masked divergences
+  // 2494-2507; flux_advection.py:288-391): tiered faces, masked divergences,
+  // a compile-time switch of the advection kernels
   const int deg = (specified && p.specified_adv_degrade) ? 1 : 0;
-  auto kWface = mixed ? (ph_order6 ? k_wface_tiled<float, true> : k_wface_tiled<float, false>)
-                      : (ph_order6 ? k_wface_tiled<double, true> : k_wface_tiled<double, false>);
+  auto kUface = mixed ? (deg ? k_uface_tiled<float, true> : k_uface_tiled<float, false>)
+                      : (deg ? k_uface_tiled<double, true> : k_uface_tiled<double, false>);
+  auto kVface = mixed ? (deg ? k_vface_tiled<float, true> : k_vface_tiled<float, false>)
+                      : (deg ? k_vface_tiled<double, true> : k_vface_tiled<double, false>);
+#define WG_W(F, O) (deg ? k_wface_tiled<F, O, true> : k_wface_tiled<F, O, false>)
+  auto kWface = mixed ? (ph_order6 ? WG_W(float, true) : WG_W(float, false))
+                      : (ph_order6 ? WG_W(double, true) : WG_W(double, false));
+#undef WG_W
   // marching kernels for the chosen chunk size (5, 10 or 25 levels)
-#define WG_PICK_KC(tmpl, ...) \
-  (kc == 5 ? tmpl<__VA_ARGS__, 5> : kc == 25 ? tmpl<__VA_ARGS__, 25> : tmpl<__VA_ARGS__, 10>)
-  auto kScalar = mixed ? WG_PICK_KC(k_scalar_adv_march, float) : WG_PICK_KC(k_scalar_adv_march, double);
-  auto kLimScale = mixed ? WG_PICK_KC(k_lim_march, float) : WG_PICK_KC(k_lim_march, double);
+  // (and for the specified degradation, a compile-time switch of their face fluxes)
+#define WG_PICK_KC(tmpl, F, D) \
+  (kc == 5 ? tmpl<F, 5, D> : kc == 25 ? tmpl<F, 25, D> : tmpl<F, 10, D>)
+#define WG_PICK_KC_DEG(tmpl, F) (deg ? WG_PICK_KC(tmpl, F, true) : WG_PICK_KC(tmpl, F, false))
+  auto kScalar = mixed ? WG_PICK_KC_DEG(k_scalar_adv_march, float) : WG_PICK_KC_DEG(k_scalar_adv_march, double);
+  auto kLimScale = mixed ? WG_PICK_KC_DEG(k_lim_march, float) : WG_PICK_KC_DEG(k_lim_march, double);
+#undef WG_PICK_KC_DEG
 #undef WG_PICK_KC
 
   StateR s = origin;
@@ -582,12 +590,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     UFaceOut uo{w.u_tend, w.u_w, w.cqu};
     PROF("k_uface");
     kUface<<<tgrd(nx + 1, ny, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muu, w.muus,
-                                                               in->base_u, p.top_lid, p.run_boundary, deg, uo);
+                                                               in->base_u, p.top_lid, p.run_boundary, uo);
     LAUNCH_CHECK("k_uface");
     VFaceOut vo{w.v_tend, w.v_w, w.cqv};
     PROF("k_vface");
     kVface<<<tgrd(nx, ny + 1, nz), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, dg, w.muv, w.muvs,
-                                                               in->base_v, p.top_lid, p.run_boundary, deg, vo);
+                                                               in->base_v, p.top_lid, p.run_boundary, vo);
     LAUNCH_CHECK("k_vface");
     const bool lim_theta = (rk == 3) && (p.scalar_adv_opt == 1 || p.scalar_adv_opt == 2);
     const bool lim_moist = moist && (rk == 3) && (p.moist_adv_opt == 1 || p.moist_adv_opt == 2);
@@ -600,7 +608,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       const int nfields = 1 + ((moist && !lim_moist) ? 6 : 0);
       const int nchunk = march_nchunk(nz, kc);
       kScalar<<<tgrd(nx, ny, nfields * nchunk), tblk(), 0, stream>>>(
-          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, deg, mo);
+          g, s, origin, w.ru, w.rv, w.rom, w.mut, w.muts0, in->base_theta, lim_theta ? 0 : 1, nfields, mo);
     }
     LAUNCH_CHECK("k_mass");
     if (lim_theta || lim_moist) {
@@ -640,7 +648,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     PROF("k_wface");
     kWface<<<tgrd(nx, ny, nz + 1), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot,
                                                                w.mub, w.mut, w.muts0, w.muu, w.muv, in->base_w,
-                                                               p.top_lid, p.moist_cqw, p.w_coriolis, deg, wo);
+                                                               p.top_lid, p.moist_cqw, p.w_coriolis, wo);
     LAUNCH_CHECK("k_wface");
     const double x = 0.5 * dts * G * eps1;
     const double cof = x * x;

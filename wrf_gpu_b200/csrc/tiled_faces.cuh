@@ -80,12 +80,13 @@ __device__ __forceinline__ double v_adv_global(const Grid &g, const StateR &s, c
 // ---------------------------------------------------------------------------
 // u faces, tiled advection.  Grid over faces 0..nx.
 // ---------------------------------------------------------------------------
-template <typename F>
+template <typename F, bool DEG>
 __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muu, const double *muus,
                                                            const double *base_u, int top_lid, int run_boundary,
-                                                           int deg, UFaceOut o) {
+                                                           UFaceOut o) {
+  constexpr bool deg = DEG;  // the specified-boundary advection degradation
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<1, 1>;
@@ -221,12 +222,13 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
 // ---------------------------------------------------------------------------
 // v faces, tiled advection.  Grid over faces 0..ny.
 // ---------------------------------------------------------------------------
-template <typename F>
+template <typename F, bool DEG>
 __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muv, const double *muvs,
                                                            const double *base_v, int top_lid, int run_boundary,
-                                                           int deg, VFaceOut o) {
+                                                           VFaceOut o) {
+  constexpr bool deg = DEG;  // the specified-boundary advection degradation
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 1>;
   using TV = Tile<0, 1>;
@@ -399,14 +401,15 @@ __device__ __forceinline__ void ph_adv_order6(int j, int i, int ny, int nx, PTF 
 // ORD6 selects rhs_ph's order<=6 specified-boundary horizontal advection
 // (h_sca_adv_order >= 4 with specified lateral BCs), otherwise order 2.
 // ---------------------------------------------------------------------------
-template <typename F, bool ORD6>
+template <typename F, bool ORD6, bool DEG>
 __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom,
                                                            const double *ww_stage, const double *qtot,
                                                            const double *mub, const double *mut, const double *muts0,
                                                            const double *muu, const double *muv,
                                                            const double *base_w, int top_lid, int moist_cqw,
-                                                           int w_coriolis, int deg, WFaceOut o) {
+                                                           int w_coriolis, WFaceOut o) {
+  constexpr bool deg = DEG;  // the specified-boundary advection degradation
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;

@@ -68,11 +68,11 @@ constexpr int MARCH_KC_CHOICES[] = {5, 10, 25};
 // written, the tendency only when theta is not limited), fields 1..6 the
 // species.
 // ---------------------------------------------------------------------------
-template <typename F, int KC>
+template <typename F, int KC, bool DEG>
 __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s, StateR ref, const double *ru,
                                                                 const double *rv, const double *rom, const double *mut,
                                                                 const double *muts0, const double *base_theta,
-                                                                int theta_plain, int nfields, int deg, MassOut o) {
+                                                                int theta_plain, int nfields, MassOut o) {
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
@@ -137,14 +137,14 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
         if (e < NXF) {
           const int r = e / (TSX + 1), m = e - r * (TSX + 1);
           const double vel = RU[r * TR::W + (m + 1)];
-          sfx[e] = deg ? hflux_spec<F>(i0 + m, nx, false, vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m),
+          sfx[e] = DEG ? hflux_spec<F>(i0 + m, nx, false, vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m),
                                        Q(r, m + 1), Q(r, m + 2))
                        : hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
         } else {
           const int e2 = e - NXF;
           const int r = e2 / TSX, cc = e2 - r * TSX;
           const double vel = RV[(r + 1) * TV::W + cc];
-          sfy[e2] = deg ? hflux_spec<F>(j0 + r, ny, false, vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc),
+          sfy[e2] = DEG ? hflux_spec<F>(j0 + r, ny, false, vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc),
                                         Q(r + 1, cc), Q(r + 2, cc))
                         : hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc));
         }
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s,
       if (valid) {
         // the specified degradation leaves the outermost cells without
         // horizontal flux divergence (flux_advection.py:350-361)
-        const bool xin = !deg || (i >= 1 && i <= nx - 2), yin = !deg || (j >= 1 && j <= ny - 2);
+        const bool xin = !DEG || (i >= 1 && i <= nx - 2), yin = !DEG || (j >= 1 && j <= ny - 2);
         double tend = -msftx * g.rdx * (xin ? (sfx[ty * (TSX + 1) + tx + 1] - sfx[ty * (TSX + 1) + tx]) : 0.0);
         tend = tend - msftx * g.rdy * (yin ? (sfy[(ty + 1) * TSX + tx] - sfy[ty * TSX + tx]) : 0.0);
         const double v_hi = (k + 1 <= nz - 1) ? vflux(k + 1) : 0.0;
@@ -204,7 +204,7 @@ struct LimMarchSmem {
   ZConst zc[2];
 };
 
-template <typename F, int KC>
+template <typename F, int KC, bool DEG>
 __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const double *field,
                                                          const double *field_old, double *s1w, double *s2w,
                                                          LimFaces fo) {
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const
     lim_zconst(g, a, k, sm.zc);
     __syncthreads();
     LimTiles t{sm.q[b], sm.qo[b], sm.ru[b], sm.rv[b], sm.mt, sm.zc, sm.fxl, sm.fxa, sm.fyl, sm.fya};
-    lim_face_fluxes<F>(g, a, t, k, i0, j0);
+    lim_face_fluxes<F, DEG>(g, a, t, k, i0, j0);
     __syncthreads();
     if (valid) {
       CellFluxes cf;

@@ -78,7 +78,7 @@ __device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int 
 // order :678-711 minus low order) fluxes of every x and y face of the tile,
 // one face per thread item, into shared memory.  Edge tiles compute a few
 // harmless extra faces from the periodically wrapped staged values.
-template <typename F>
+template <typename F, bool DEG>
 __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int i0,
                                                 int j0) {
   using TQ = Tile<3, 3>;
@@ -105,8 +105,8 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
       // the specified degradation: tiered high-order faces, no low-order
       // flux on face 0 (nor on face nx, its wrap)
       const int gm = i0 + m;
-      const double lo = (a.deg && (gm == 0 || gm == g.nx)) ? 0.0 : upw(QO(r, m - 1), QO(r, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
-      const double hi = a.deg ? hflux_spec<F>(gm, g.nx, false, vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m),
+      const double lo = (DEG && (gm == 0 || gm == g.nx)) ? 0.0 : upw(QO(r, m - 1), QO(r, m), vel, mu_u, a.dxl, a.rdxl, a.dxl_dt);
+      const double hi = DEG ? hflux_spec<F>(gm, g.nx, false, vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m),
                                               Q(r, m + 1), Q(r, m + 2))
                               : hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
       t.fxl[e] = lo;
@@ -118,8 +118,8 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
       const double muv = 0.5 * (MT(r, cc) + MT(r - 1, cc));
       const double mu_v = c1 * muv + c2;
       const int gm = j0 + r;
-      const double lo = (a.deg && (gm == 0 || gm == g.ny)) ? 0.0 : upw(QO(r - 1, cc), QO(r, cc), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
-      const double hi = a.deg ? hflux_spec<F>(gm, g.ny, false, vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc),
+      const double lo = (DEG && (gm == 0 || gm == g.ny)) ? 0.0 : upw(QO(r - 1, cc), QO(r, cc), vel, mu_v, a.dyl, a.rdyl, a.dyl_dt);
+      const double hi = DEG ? hflux_spec<F>(gm, g.ny, false, vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc),
                                               Q(r + 1, cc), Q(r + 2, cc))
                               : hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc));
       t.fyl[e2] = lo;
