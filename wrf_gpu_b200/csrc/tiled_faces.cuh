@@ -714,29 +714,67 @@ __global__ void __launch_bounds__(256) k_transport_tiled(Grid g, const double *u
     }
   }
   __syncthreads();
-  if (ty == 0 && valid) {
-    double dmdt = D0(0);
-    for (int k = 1; k < nz; ++k) dmdt = dmdt + D0(k);
-    double cum = 0.0;
-    rom[ix3(0, j, i, ny, nx)] = 0.0;
-    for (int k = 0; k < nz - 1; ++k) {
-      const double inc = -(ld(g.dnw, k) * ld(g.c1h, k) * dmdt) - D0(k);
-      cum = (k == 0) ? inc : cum + inc;
-      rom[ix3(k + 1, j, i, ny, nx)] = cum;
+  // Column sums (serial chains over shared memory, loads batched ahead of
+  // the adds), then the level-parallel increments, the serial prefix sum in
+  // place, and the level-parallel stores.  Thread row 0 does rom, row 1 the
+  // specified stage omega.
+  __shared__ double s_dm[2][32];
+  auto serial_sum = [&](auto D) {
+    constexpr int SU = 8;
+    double acc = D(0);
+    int k = 1;
+    for (; k + SU <= nz; k += SU) {
+      double r[SU];
+#pragma unroll
+      for (int u = 0; u < SU; ++u) r[u] = D(k + u);
+#pragma unroll
+      for (int u = 0; u < SU; ++u) acc = acc + r[u];
     }
-    rom[ix3(nz, j, i, ny, nx)] = 0.0;
+    for (; k < nz; ++k) acc = acc + D(k);
+    return acc;
+  };
+  auto serial_prefix = [&](auto D) {  // D(k) <- D(0) + ... + D(k) for k < nz - 1
+    constexpr int SU = 8;
+    double cum = D(0);
+    int k = 1;
+    for (; k + SU <= nz - 1; k += SU) {
+      double r[SU];
+#pragma unroll
+      for (int u = 0; u < SU; ++u) r[u] = D(k + u);
+#pragma unroll
+      for (int u = 0; u < SU; ++u) {
+        cum = cum + r[u];
+        D(k + u) = cum;
+      }
+    }
+    for (; k < nz - 1; ++k) {
+      cum = cum + D(k);
+      D(k) = cum;
+    }
+  };
+  const bool spec = ww_spec != nullptr;
+  if (valid && ty == 0) s_dm[0][tx] = serial_sum(D0);
+  if (valid && ty == 1 && spec) s_dm[1][tx] = serial_sum(D1);
+  __syncthreads();
+  if (valid) {
+    const double dmdt = s_dm[0][tx];
+    const double dm = spec ? s_dm[1][tx] : 0.0;
+    for (int k = ty; k < nz - 1; k += 8) {
+      const double dc = ld(g.dnw, k) * ld(g.c1h, k);
+      D0(k) = -(dc * dmdt) - D0(k);
+      if (spec) D1(k) = -(dc * dm) - D1(k);
+    }
   }
-  if (ty == 1 && valid && ww_spec != nullptr) {
-    double dm = D1(0);
-    for (int k = 1; k < nz; ++k) dm = dm + D1(k);
-    double cm = 0.0;
-    ww_spec[ix3(0, j, i, ny, nx)] = 0.0;
-    for (int k = 0; k < nz - 1; ++k) {
-      const double inc = -(ld(g.dnw, k) * ld(g.c1h, k) * dm) - D1(k);
-      cm = (k == 0) ? inc : cm + inc;
-      ww_spec[ix3(k + 1, j, i, ny, nx)] = cm;
+  __syncthreads();
+  if (valid && ty == 0) serial_prefix(D0);
+  if (valid && ty == 1 && spec) serial_prefix(D1);
+  __syncthreads();
+  if (valid) {
+    for (int f = ty; f <= nz; f += 8) {
+      const double rv_ = (f >= 1 && f <= nz - 1) ? D0(f - 1) : 0.0;
+      rom[ix3(f, j, i, ny, nx)] = rv_;
+      if (spec) ww_spec[ix3(f, j, i, ny, nx)] = (f >= 1 && f <= nz - 1) ? D1(f - 1) : 0.0;
     }
-    ww_spec[ix3(nz, j, i, ny, nx)] = 0.0;
   }
 }
 
