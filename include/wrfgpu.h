@@ -95,6 +95,14 @@ typedef struct wrfgpu_step_params {
    * and no horizontal advection of the outermost cells
    * (flux_advection.py:288-391). */
   int specified_adv_degrade;
+  /* OperationalNamelist.specified_bdy_cadence (operational_mode.py:453;
+   * default off): with specified lateral BCs and a forecast lead, WRF's
+   * relax_bdy_dry tendencies in the relax zone (from the step-start state)
+   * and the ring-0 pins of the tangential winds, mu, theta, ph and the
+   * zero-gradient w every acoustic substep (operational_mode.py:1984-2041,
+   * 2478-2530, 3085-3092; coupling/boundary_apply.py:1148-1340).  Needs the
+   * theta_bdy / ph_bdy / mu_bdy strips. */
+  int specified_bdy_cadence;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */
@@ -121,6 +129,10 @@ typedef struct wrfgpu_step_inputs {
   /* specified lateral boundary strips; NULL unless run_boundary */
   const double *u_bdy, *v_bdy;
   int bdy_ntime, bdy_width, bdy_side_len;
+  /* further strips the specified boundary cadence reads (NULL otherwise):
+   * full theta (nz levels), ph' (nz+1 levels) and mu' (1 level), same
+   * (ntime, 4, width, levels, side_len) layout */
+  const double *theta_bdy, *ph_bdy, *mu_bdy;
 } wrfgpu_step_inputs;
 
 /* Step outputs: the returned OperationalCarry (operational_mode.py:2234-2265). */

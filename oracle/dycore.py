@@ -58,6 +58,7 @@ class Namelist:
     hypsometric_opt: int = 1
     h_sca_adv_order: int = 2
     specified_adv_degrade: bool = False   # operational_mode.py:460 (opt-in)
+    specified_bdy_cadence: bool = False   # operational_mode.py:453 (opt-in)
     scalar_adv_opt: int = 0
     moist_adv_opt: int = 0
     run_boundary: bool = False
@@ -679,7 +680,7 @@ def large_step_coriolis(s, m, specified):
 # large-step tendency assembly: runtime/operational_mode.py:2722-3093, 3162-3316
 # ----------------------------------------------------------------------------
 
-def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step):
+def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_relax=None):
     """operational_mode.py:2722-3093 (flux advection on, diffusion off, physics off)."""
     m = nl.metrics
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
@@ -713,6 +714,9 @@ def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step):
     ru_cor, rv_cor = large_step_coriolis(s, m, bool(nl.run_boundary))
     u_t = u_t + ru_cor
     v_t = v_t + rv_cor
+    if bdy_relax is not None:  # operational_mode.py:3085-3092 (mu at the first stage only)
+        return SimpleNamespace(u=u_t + bdy_relax.ru, v=v_t + bdy_relax.rv, w=w_t, theta=th_t + bdy_relax.t,
+                               mu=(bmu + bdy_relax.mu) if rk_step == 1 else bmu.copy())
     return SimpleNamespace(u=u_t, v=v_t, w=w_t, theta=th_t, mu=bmu.copy())
 
 
@@ -990,6 +994,153 @@ def _strip(forcing, side, b, z_len, side_len):
     return sv[b, :z_len, :side_len]
 
 
+# ---- specified-domain boundary cadence (boundary_apply.py:948-1043, 1148-1340) ----
+SPEC_PLUS_RELAX = 5  # spec_zone + relax_zone of the default boundary configuration
+
+
+def full_ring_target(leaf, z_len, y_len, x_len):
+    """boundary_apply.py:948-969: the leaf's strips written into the outer
+    five rows / columns (W, E, S, N per width index, later writes win)."""
+    t = np.zeros((z_len, y_len, x_len))
+    for b in range(SPEC_PLUS_RELAX):
+        t[:, :, b] = _strip(leaf, "W", b, z_len, y_len)
+        t[:, :, x_len - 1 - b] = _strip(leaf, "E", b, z_len, y_len)
+        t[:, b, :] = _strip(leaf, "S", b, z_len, x_len)
+        t[:, y_len - 1 - b, :] = _strip(leaf, "N", b, z_len, x_len)
+    return t
+
+
+def _wrf_relax_weights(b, dt, spec_zone=1, relax_zone=4):
+    """boundary_apply.py:666-688 (spec_exp 0): dt*fcx, dt*gcx."""
+    loop = b + 1
+    linear = max(0.0, float(spec_zone + relax_zone - loop) / float(relax_zone - 1))
+    fcx = 0.1 / float(dt) * linear * 1.0
+    gcx = 1.0 / float(dt) / 50.0 * linear * 1.0
+    return float(dt) * fcx, float(dt) * gcx
+
+
+def _shift_clamp(v, shift, axis):
+    """boundary_apply.py:577-586."""
+    n = v.shape[axis]
+    idx = np.concatenate(([0], np.arange(n - 1))) if shift == 1 else np.concatenate((np.arange(1, n), [n - 1]))
+    return np.take(v, idx, axis=axis)
+
+
+def _relax_tendency_row(f, t, side, b, fcx, gcx):
+    """boundary_apply.py:972-1006."""
+    if side == "W":
+        cur, te, ti, b0, be, bi = f[:, :, b], f[:, :, b - 1], f[:, :, b + 1], t[:, :, b], t[:, :, b - 1], t[:, :, b + 1]
+    elif side == "E":
+        x = f.shape[2] - 1 - b
+        cur, te, ti, b0, be, bi = f[:, :, x], f[:, :, x + 1], f[:, :, x - 1], t[:, :, x], t[:, :, x + 1], t[:, :, x - 1]
+    elif side == "S":
+        cur, te, ti, b0, be, bi = f[:, b, :], f[:, b - 1, :], f[:, b + 1, :], t[:, b, :], t[:, b - 1, :], t[:, b + 1, :]
+    else:
+        y = f.shape[1] - 1 - b
+        cur, te, ti, b0, be, bi = f[:, y, :], f[:, y + 1, :], f[:, y - 1, :], t[:, y, :], t[:, y + 1, :], t[:, y - 1, :]
+    fls0 = b0 - cur
+    fls1 = _shift_clamp(fls0, +1, 1)
+    fls2 = _shift_clamp(fls0, -1, 1)
+    lap = fls1 + fls2 + (be - te) + (bi - ti) - 4.0 * fls0
+    return float(fcx) * fls0 - float(gcx) * lap
+
+
+def scatter_relax_tendency(f, t, dt_full, spec_zone=1, relax_zone=4):
+    """boundary_apply.py:1009-1043: the relax-zone tendency with WRF's corner trims."""
+    z_len, y_len, x_len = f.shape
+    tend = np.zeros_like(f)
+    for b in range(spec_zone, relax_zone):
+        fcx, gcx = _wrf_relax_weights(b, dt_full, spec_zone, relax_zone)
+        fcx, gcx = fcx / float(dt_full), gcx / float(dt_full)
+        for side in SIDES:
+            row = _relax_tendency_row(f, t, side, b, fcx, gcx)
+            if side in ("W", "E"):
+                col = b if side == "W" else x_len - 1 - b
+                tend[:, b + 1:y_len - b - 1, col] = tend[:, b + 1:y_len - b - 1, col] + row[:, b + 1:y_len - b - 1]
+            else:
+                r = b if side == "S" else y_len - 1 - b
+                tend[:, r, b:x_len - b] = tend[:, r, b:x_len - b] + row[:, b:x_len - b]
+    return tend
+
+
+def specified_relax_dry_tendencies(ref, lead_seconds, m, dt_full, cadence):
+    """boundary_apply.py:1148-1248: relax_bdy_dry from the step-start state,
+    targets at the step-start lead, both sides coupled with the step-start mass."""
+    mu = ref.mu_total
+    muu = 0.5 * (np.concatenate([mu[:, :1], mu], axis=1) + np.concatenate([mu, mu[:, -1:]], axis=1))
+    muv = 0.5 * (np.concatenate([mu[:1, :], mu], axis=0) + np.concatenate([mu, mu[-1:, :]], axis=0))
+    nz, ny, nx = ref.theta.shape
+    lf = lambda leaf: interpolate_boundary_leaf(leaf, lead_seconds, cadence)
+    u_t = full_ring_target(lf(ref.u_bdy), nz, ny, nx + 1)
+    v_t = full_ring_target(lf(ref.v_bdy), nz, ny + 1, nx)
+    t_t = full_ring_target(lf(ref.theta_bdy), nz, ny, nx)
+    ph_t = full_ring_target(lf(ref.ph_bdy), nz + 1, ny, nx)
+    mu_t = full_ring_target(lf(ref.mu_bdy), 1, ny, nx)[0]
+    c1h, c2h, c1f, c2f = _col(m.c1h), _col(m.c2h), _col(m.c1f), _col(m.c2f)
+    mass_u = c1h * muu[None] + c2h
+    mass_v = c1h * muv[None] + c2h
+    mass_h = c1h * mu[None] + c2h
+    mass_f = c1f * mu[None] + c2f
+    r = SimpleNamespace()
+    r.ru = scatter_relax_tendency(mass_u * ref.u / m.msfuy[None], mass_u * u_t / m.msfuy[None], dt_full)
+    r.rv = scatter_relax_tendency(mass_v * ref.v / m.msfvx[None], mass_v * v_t / m.msfvx[None], dt_full)
+    r.t = scatter_relax_tendency(mass_h * ref.theta, mass_h * t_t, dt_full) / m.msfty[None]
+    r.ph = scatter_relax_tendency(mass_f * ref.ph_perturbation, mass_f * ph_t, dt_full) / m.msfty[None]
+    r.mu = scatter_relax_tendency(ref.mu_perturbation[None], mu_t[None], dt_full)[0]
+    return r
+
+
+def tangential_targets(u_strip, v_strip, prep, m):
+    """boundary_apply.py:1251-1296 (spec_zone 1): ring-0 work targets of the
+    tangential winds, u on the S / N rows, v on the W / E columns."""
+    c1h, c2h = _col(m.c1h), _col(m.c2h)
+    mu_cur, mu_stg = c1h * prep.muu[None] + c2h, c1h * prep.muus[None] + c2h
+    mv_cur, mv_stg = c1h * prep.muv[None] + c2h, c1h * prep.muvs[None] + c2h
+    u_save, v_save = prep.u_save, prep.v_save
+    nz, ny, nxu = u_save.shape
+    _, nyv, nx = v_save.shape
+    tu = np.zeros_like(u_save)
+    for rr, side in ((0, "S"), (ny - 1, "N")):
+        st = _strip(u_strip, side, 0, nz, nxu)
+        tu[:, rr, :] = (st * mu_stg[:, rr, :] - u_save[:, rr, :] * mu_cur[:, rr, :]) / m.msfuy[rr, :][None, :]
+    tv = np.zeros_like(v_save)
+    for cc, side in ((0, "W"), (nx - 1, "E")):
+        st = _strip(v_strip, side, 0, nz, nyv)
+        tv[:, :, cc] = (st * mv_stg[:, :, cc] - v_save[:, :, cc] * mv_cur[:, :, cc]) / m.msfvx[:, cc][None, :]
+    return tu, tv
+
+
+def _pin_ring(field, target):
+    """Ring-0 copy (operational acoustic core :902-915, spec_zone 1)."""
+    out = field.copy()
+    out[..., 0, :] = target[..., 0, :]
+    out[..., -1, :] = target[..., -1, :]
+    out[..., :, 0] = target[..., :, 0]
+    out[..., :, -1] = target[..., :, -1]
+    return out
+
+
+def specified_w_zero_grad(w_work, w_save, mut, muts, m):
+    """core/acoustic.py:383-516 (spec_zone 1): the ring-0 work w whose finished
+    physical w equals the nearest interior physical w (S / N rows own corners)."""
+    c1f, c2f = _col(m.c1f), _col(m.c2f)
+    mass_cur = c1f * mut[None] + c2f
+    mass_stage = c1f * muts[None] + c2f
+    msfty = m.msfty
+    phys = (msfty[None] * w_work + w_save * mass_cur) / mass_stage
+    nzp, ny, nx = w_work.shape
+    out = w_work.copy()
+    xi = np.clip(np.arange(nx), 1, nx - 2)
+    work = lambda tgt, j, i: (tgt * mass_stage[:, j, i] - w_save[:, j, i] * mass_cur[:, j, i]) / msfty[j, i]
+    out[:, 0, :] = work(phys[:, 1, xi], 0, slice(None))
+    out[:, ny - 1, :] = work(phys[:, ny - 2, xi], ny - 1, slice(None))
+    rows = np.arange(1, ny - 1)
+    yi = np.clip(rows, 1, ny - 2)
+    out[:, 1:ny - 1, 0] = work(phys[:, yi, 1], slice(1, ny - 1), 0)
+    out[:, 1:ny - 1, nx - 1] = work(phys[:, yi, nx - 2], slice(1, ny - 1), nx - 1)
+    return out
+
+
 def normal_bdy_work_target_u(strip, u_save, mass_cur, mass_stage, msfuy, nzone):
     """boundary_apply.py:729-758."""
     z, y, x = u_save.shape
@@ -1257,8 +1408,22 @@ def acoustic_substep(a, m, nl: Namelist, dts, bdy=None):
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
     _, specified, _ = lateral_flags(nl)
     advance_uv(a, m, dts, rdx, rdy, nl.dx, nl.dy, nl.top_lid, bdy)
+    cad = getattr(a, "cad", None)
+    if cad is not None:  # ring-0 tangential winds (core/acoustic.py:777-785)
+        a.u[:, 0, :] = cad.u_tan[:, 0, :]
+        a.u[:, -1, :] = cad.u_tan[:, -1, :]
+        a.v[:, 1:-1, 0] = cad.v_tan[:, 1:-1, 0]
+        a.v[:, 1:-1, -1] = cad.v_tan[:, 1:-1, -1]
     advance_mu_t(a, m, dts, rdx, rdy, nl.epssm, specified)
+    if cad is not None:  # ring-0 mass and theta pins (core/acoustic.py:902-915)
+        a.mu = _pin_ring(a.mu, cad.mu)
+        a.muts = _pin_ring(a.muts, cad.muts)
+        a.muave = _pin_ring(a.muave, cad.muave)
+        a.theta_work = _pin_ring(a.theta_work, cad.theta)
     advance_w(a, m, nl, dts, rdx, rdy)
+    if cad is not None:  # spec_bdyupdate_ph and zero_grad_bdy w (core/acoustic.py:1059-1090)
+        a.ph = _pin_ring(a.ph, cad.ph_delta)
+        a.w = specified_w_zero_grad(a.w, a.w_save, a.mut, a.muts, m)
     mu_work = a.muts - a.mut
     al, pp = calc_al_p(mu_work, a.muts, a.ph, a.theta_work, a.theta_1, a.c2a, a.alt, m)
     a.p = pp + SMDIV * (pp - a.pm1)
@@ -1270,8 +1435,11 @@ def acoustic_substep(a, m, nl: Namelist, dts, bdy=None):
 # stage / step: runtime/operational_mode.py:1682-2265, 3319-3534
 # ----------------------------------------------------------------------------
 
-def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Namelist, dts, lead_seconds):
-    """operational_mode.py:1682-2166 (no specified cadence, no nested forcing)."""
+def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Namelist, dts, lead_seconds,
+                             bdy_relax=None, dt_rk=0.0):
+    """operational_mode.py:1682-2166 (no nested forcing); with ``bdy_relax``
+    the specified-domain cadence (:1984-2041): the relax ph tendency and the
+    stage-end ring-0 targets."""
     m = nl.metrics
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
     nz, ny, nx = s.theta.shape
@@ -1327,6 +1495,23 @@ def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Nameli
     a.w_save = prep.w_save
     a.rw_tend = rw
     a.php = prep.php
+    a.cad = None
+    if bdy_relax is not None:
+        a.ph_tend = a.ph_tend + bdy_relax.ph
+        lead_stage = lead_seconds + float(dt_rk)
+        lf = lambda leaf: interpolate_boundary_leaf(leaf, lead_stage, nl.update_cadence_s)
+        c1h, c2h = _col(m.c1h), _col(m.c2h)
+        cad = SimpleNamespace()
+        cad.ph_delta = full_ring_target(lf(s.ph_bdy), nz + 1, ny, nx) - prep.ph_save
+        cad.mu = full_ring_target(lf(s.mu_bdy), 1, ny, nx)[0]
+        cad.muts = prep.mub + cad.mu
+        cad.muave = cad.muts - prep.mut
+        th_pin = full_ring_target(lf(s.theta_bdy), nz, ny, nx)
+        mass_pin = c1h * cad.muts[None] + c2h
+        mass_cur = c1h * prep.mut[None] + c2h
+        cad.theta = mass_pin * (th_pin - T0) - mass_cur * prep.t_save
+        cad.u_tan, cad.v_tan = tangential_targets(lf(s.u_bdy), lf(s.v_bdy), prep, m)
+        a.cad = cad
     bdy = None
     if nl.run_boundary and lead_seconds is not None:
         c1h, c2h = _col(m.c1h), _col(m.c2h)
@@ -1417,6 +1602,10 @@ def rk_scan_step(carry, nl: Namelist, lead_seconds=None):
     stages = ((1, dt / 3.0, dt / 3.0, 1), (2, 0.5 * dt, dt / float(ns), max(1, ns // 2)), (3, dt, dt / float(ns), ns))
     _, specified, nested = lateral_flags(nl)
     moist = nl.moist_adv_opt != 0
+    # the specified-domain boundary cadence (operational_mode.py:2478-2530, 3362)
+    bdy_relax = None
+    if nl.specified_bdy_cadence and specified and lead_seconds is not None:
+        bdy_relax = specified_relax_dry_tendencies(origin, lead_seconds, m, dt, nl.update_cadence_s)
     state = origin
     mudf = carry.mudf.copy()
     out = SimpleNamespace()
@@ -1426,12 +1615,13 @@ def rk_scan_step(carry, nl: Namelist, lead_seconds=None):
         if nl.specified_adv_degrade and specified:  # operational_mode.py:2464-2475, 2494-2507
             vel.specified = True
             vel.ru_full, vel.rv_full = couple_uv_specified(s.u, s.v, s.mu_total, m)
-        tend = augment_large_step_tendencies(s, origin, vel, nl, rk_step)
+        tend = augment_large_step_tendencies(s, origin, vel, nl, rk_step, bdy_relax)
         q_tend = moisture_coupled_tendencies(s, origin, vel, nl, rk_step) if moist else None
         ww_stage = stage_omega_specified(s.u, s.v, s.mu_total, m, rdx, rdy) if (specified or nested) else vel.rom
         prep = small_step_prep(s, origin, rk_step, m, ww_stage)
         al0, p0 = calc_al_p(prep.mu_work, prep.muts, prep.ph_work, prep.theta_work, prep.theta_1, prep.c2a, prep.alt, m)
-        a, bdy = acoustic_state_from_prep(s, prep, al0, p0, p0.copy(), tend, mudf, nl, dts, lead_seconds)
+        a, bdy = acoustic_state_from_prep(s, prep, al0, p0, p0.copy(), tend, mudf, nl, dts, lead_seconds,
+                                          bdy_relax, dt_rk)
         a.a, a.alpha, a.gamma = calc_coef_w(prep.mut, m, dts, nl.epssm, nl.top_lid, a.cqw, prep.c2a)
         for _ in range(nsub):
             acoustic_substep(a, m, nl, dts, bdy)

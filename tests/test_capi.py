@@ -120,6 +120,12 @@ def test_launch_count(lib):
     # map-factor reciprocals + 3 stages x (8 stage + 3 finish)
     # + 3 launches per substep x (1 + 3 + 6)
     assert n.value == 1 + 3 * 11 + 3 * 10
+    # specified boundaries (+2 target launches per stage) with the boundary
+    # cadence: + the first stage's mu tendency, one relax launch per stage and
+    # one zero-gradient w launch per substep
+    p = _params(lib, acoustic_substeps=6, run_boundary=1, bc_ideal=0, specified_bdy_cadence=1)
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(n)) == 0
+    assert n.value == (1 + 3 * 13 + 3 * 10) + (1 + 3) + 10
 
 
 def test_null_pointers_rejected_before_any_launch(lib):
@@ -146,7 +152,7 @@ def test_host_shim_rejects_unsupported_namelist():
                              p_top=case.metrics.p_top)
     st = dycore.State.from_host(case.state, device="cpu")
     carry = dycore.initial_operational_carry(st)
-    for kw in (dict(use_flux_advection=False), dict(diff_opt=2), dict(specified_bdy_cadence=True),
+    for kw in (dict(use_flux_advection=False), dict(diff_opt=2),
                dict(const_nu_m2_s=75.0), dict(acoustic_precision_mode="mixed_perturb_fp32")):
         nl = dycore.OperationalNamelist.from_case(case, metrics=m, **kw)
         with pytest.raises(NotImplementedError):

@@ -145,6 +145,19 @@ def test_per_step_parity_specified_adv_degrade(cuda_ready, shape, theta_opt, moi
         assert not bad, f"{shape} step {n}: {bad}"
 
 
+@pytest.mark.parametrize("degrade", [False, True])
+def test_per_step_parity_specified_bdy_cadence(cuda_ready, degrade):
+    """specified_bdy_cadence: relax_bdy_dry tendencies in the relax zone, the
+    ring-0 pins of the tangential winds, mu, theta and ph, and the
+    zero-gradient w, with perturbed boundary leaves that drift in time and
+    non-unit map factors (alone and with the advection degradation)."""
+    case = _with_map_factors(cases.real_like_moist(40, 24, 12, hmax=800.0, specified=True, bdy_noise=True), seed=9)
+    case.controls.update(specified_bdy_cadence=True, specified_adv_degrade=degrade)
+    for n, e in enumerate(_per_step(case, 2)):
+        bad = {k: v for k, v in e.items() if not v <= _tol(k)}
+        assert not bad, f"degrade={degrade} step {n}: {bad}"
+
+
 def test_per_step_parity_map_factors_periodic(cuda_ready):
     case = _with_map_factors(cases.real_like_moist(24, 20, 14, hmax=800.0, specified=False), seed=11)
     for n, e in enumerate(_per_step(case, 2)):

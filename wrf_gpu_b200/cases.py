@@ -137,19 +137,27 @@ def _controls(**kw):
     return base
 
 
-def _boundary_leaves(state, nz, ny, nx, times=2, width=5):
+def _boundary_leaves(state, nz, ny, nx, times=2, width=5, rng=None):
     """Specified boundary strips ``(time, side, width, z, side_len)`` (``contracts/state.py:96-106``)
-    built from the initial edge rows, constant in time."""
+    of u, v, theta (full), ph' (nz+1 levels) and mu' (one level), built from the
+    initial edge rows: constant in time, or with ``rng`` perturbed by seeded
+    noise and drifting between the two time levels (u/v 0.5 m/s, theta 0.3 K,
+    ph' 20 m2/s2, mu' 30 Pa)."""
     side = max(nx + 1, ny + 1)
     out = {}
-    for name, fld in (("u_bdy", state.u), ("v_bdy", state.v)):
-        leaf = np.zeros((times, 4, width, nz, side))
+    specs = (("u_bdy", state.u, 0.5), ("v_bdy", state.v, 0.5), ("theta_bdy", state.theta, 0.3),
+             ("ph_bdy", state.ph_perturbation, 20.0), ("mu_bdy", state.mu_perturbation[None], 30.0))
+    for name, fld, scale in specs:
         zl, yl, xl = fld.shape
+        leaf = np.zeros((times, 4, width, zl, side))
         for b in range(width):
             leaf[:, 0, b, :, :yl] = fld[:, :, b]
             leaf[:, 1, b, :, :yl] = fld[:, :, xl - 1 - b]
             leaf[:, 2, b, :, :xl] = fld[:, b, :]
             leaf[:, 3, b, :, :xl] = fld[:, yl - 1 - b, :]
+        if rng is not None:
+            leaf = leaf + scale * rng.standard_normal(leaf.shape[1:])[None]
+            leaf[1:] = leaf[1:] + 0.5 * scale * rng.standard_normal(leaf[1:].shape)
         out[name] = leaf
     return out
 
@@ -269,11 +277,12 @@ def _qsat(t, p):
 
 def real_like_moist(nx: int = 433, ny: int = 433, nz: int = 50, *, seed: int = 0, dx: float = 1000.0,
                     ztop: float = 20000.0, dt: float = 6.0, ns: int = 6, hmax: float = 3000.0,
-                    specified: bool = True) -> Case:
+                    specified: bool = True, bdy_noise: bool = False) -> Case:
     """Real-like moist synthetic: seeded k^-2 spectral terrain (0..hmax), theta from 295 K
     at the surface with N = 0.011 1/s, seeded 5->20 m/s shear plus N(0, 0.5^2) white noise
     on u/v, qv at 80 % RH decaying with height, lognormal qc/qr in 2-6 km.  Specified
-    lateral boundaries (constant-in-time strips), moist_adv_opt = 1 (positive definite),
+    lateral boundaries (constant-in-time strips; with ``bdy_noise`` seeded
+    perturbed strips that drift in time), moist_adv_opt = 1 (positive definite),
     dt 6 s, 6 acoustic substeps, epssm 0.1, no lid."""
     rng = np.random.default_rng(seed + 1)
     theta_s, nbv = 295.0, 0.011
@@ -307,7 +316,8 @@ def real_like_moist(nx: int = 433, ny: int = 433, nz: int = 50, *, seed: int = 0
     c = _controls(dt_s=dt, acoustic_substeps=ns, epssm=0.1, top_lid=False, moist_adv_opt=1,
                   run_boundary=specified, bc_ideal=not specified)
     if specified:
-        for k, val in _boundary_leaves(s, nz, ny, nx).items():
+        brng = np.random.default_rng(seed + 101) if bdy_noise else None
+        for k, val in _boundary_leaves(s, nz, ny, nx, rng=brng).items():
             setattr(s, k, val)
     return Case("real_like_moist", nx, ny, nz, m, dict(c, dx=dx, dy=dx), s, np.zeros((ny, nx)),
                 notes={"seed": seed, "hmax": hmax})

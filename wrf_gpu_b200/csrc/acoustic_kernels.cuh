@@ -41,6 +41,10 @@ struct BdyArgs {
   // zone_w[d] = min(1, max(0, sub_ratio*0.1*linear(d))) for the relaxation
   // rows d in [spec_zone, relax_zone), filled by set_bdy_weights.
   double zone_w[BDY_MAX_ZONE];
+  // specified boundary cadence: ring-0 tangential wind work pins from the u / v
+  // leaves at the stage-end lead (boundary_apply.py:1251-1296)
+  int cad;
+  BdyLeaf cad_u, cad_v;
 };
 
 inline void set_bdy_weights(BdyArgs &b) {
@@ -209,6 +213,11 @@ __global__ void __launch_bounds__(128, WG_UV_MINB) k_advance_uv(Grid g, Acoustic
       u = u - dts * L.cqu * dpx;
       u = u + c1 * mdu;
       if (wu != 0.0) u = u + wu * (ld(bdy.u_target, cu) - u);
+      if (bdy.cad && (j == 0 || j == ny - 1)) {
+        // tangential u on the S / N rows (core/acoustic.py:777-785)
+        const double ms = c1 * ld(A.muus, fu) + c2, mc = c1 * ld(A.muu, fu) + c2;
+        u = div_msf(strip_at(bdy.cad_u, nz, j == 0 ? 2 : 3, 0, k, i) * ms - ld(A.u_1, cu) * mc, g.msfuy, g.rmsfuy, fu);
+      }
       A.u[cu] = u;
     }
     if (dv) {
@@ -226,6 +235,11 @@ __global__ void __launch_bounds__(128, WG_UV_MINB) k_advance_uv(Grid g, Acoustic
       v = v - dts * L.cqv * dpy;
       v = v + c1 * mdv;
       if (wv != 0.0) v = v + wv * (ld(bdy.v_target, cv) - v);
+      if (bdy.cad && (i == 0 || i == nx - 1) && j >= 1 && j <= ny - 1) {
+        // tangential v on the W / E columns
+        const double ms = c1 * ld(A.muvs, fv) + c2, mc = c1 * ld(A.muv, fv) + c2;
+        v = div_msf(strip_at(bdy.cad_v, nz, i == 0 ? 0 : 1, 0, k, j) * ms - ld(A.v_1, cv) * mc, g.msfvx, g.rmsfvx, fv);
+      }
       A.v[cv] = v;
     }
     pCm = pC0; pWm = pW0; pSm = pS0;
@@ -285,6 +299,13 @@ struct ColArgs {
   int specified, top_lid, w_damping, damp_opt;
   double dampcoef, zdamp;
   double rzdamp;  // 1/zdamp correctly rounded, 0 when zdamp is 0 or its reciprocal overflows
+  // specified boundary cadence: ring-0 pins of mu / muts / muave, the work
+  // theta and the work ph from the leaves at the stage-end lead
+  // (operational_mode.py:1984-2029; core/acoustic.py:902-915, 1059-1068)
+  int cad;
+  BdyLeaf cad_mu, cad_th, cad_ph;
+  const double *ph_save;  // stage ph' (the work ph's reference)
+  const double *mub;      // base dry mass
 };
 
 // (x / zdamp) of the Rayleigh ramp, exact either way.

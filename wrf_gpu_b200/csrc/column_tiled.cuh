@@ -182,6 +182,14 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
     s_mutend[tx] = mu_tend;
     s_scale[tx] = scale;
   }
+  if (ty == 0 && valid && !active && c.cad) {
+    // specified cadence: ring-0 mu', muts and muave pinned to the mu' leaf
+    const double mu_pin = ring_target(c.cad_mu, 1, ny, nx, 0, j, i);
+    const double muts_pin = ld(c.mub, c2d) + mu_pin;
+    A.mu[c2d] = mu_pin;
+    A.muts[c2d] = muts_pin;
+    A.muave[c2d] = muts_pin - mut;
+  }
   __syncthreads();
   // ---------------- P3: ww increments -> A1, ww_1 -> A2, old ww (inactive) -> A3 ----------------
   // P5's per-level inputs are copied asynchronously now, each level by the
@@ -261,6 +269,13 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
         const double tend = ld(hdiv, M(k)) + ld(g.rdnw, k) * (wdtn_hi - wdtn_lo);
         const double theta_i = thw + msfty * dts * S(A4, k);
         thw = theta_i - dts * msfty * tend;
+        A.theta_w[M(k)] = thw;
+        S(A7, k) = thw;
+      } else if (c.cad) {
+        // specified cadence: the ring-0 work theta whose finished theta is the leaf's
+        const double mass_pin = ld(g.c1h, k) * muts + ld(g.c2h, k);
+        const double mass_cur = ld(g.c1h, k) * mut + ld(g.c2h, k);
+        thw = mass_pin * (ring_target(c.cad_th, nz, ny, nx, k, j, i) - T0) - mass_cur * T1(k, j, i);
         A.theta_w[M(k)] = thw;
         S(A7, k) = thw;
       }
@@ -431,6 +446,12 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
         }
         const double mfs = ld(g.c1f, f) * muts + ld(g.c2f, f);
         const double phn = S(A2, f) + msfty * 0.5 * dts * G * eps_p * ws / mfs;
+        S(A4, f) = phn;
+        A.ph[M(f)] = phn;
+      }
+      if (!active && c.cad) {
+        // specified cadence: ring-0 work ph whose finished ph' is the leaf's (spec_bdyupdate_ph)
+        const double phn = ring_target(c.cad_ph, nz + 1, ny, nx, f, j, i) - ld(c.ph_save, M(f));
         S(A4, f) = phn;
         A.ph[M(f)] = phn;
       }

@@ -22,6 +22,7 @@
 #include "tiled_faces.cuh"
 #include "tiled_march.cuh"
 #include "adjoint.cuh"
+#include "bdy_cadence.cuh"
 
 using namespace wg;
 
@@ -79,6 +80,8 @@ struct Work {
   double *rom, *ww_spec, *rw_tend, *ph_tend, *cqw, *w_w, *ph_w, *pt1, *ww, *a, *alpha, *gamma;
   // intermediate states after stages 1 and 2
   StateW st[2];
+  // specified boundary cadence: the first stage's mu tendency (base + relax)
+  double *mu_tend_s1;
 };
 
 bool is_moist(const wrfgpu_step_params &p) { return p.moist_adv_opt != 0; }
@@ -114,6 +117,7 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   w.rw_tend = c.take(d.w); w.ph_tend = c.take(d.w); w.cqw = c.take(d.w); w.w_w = c.take(d.w);
   w.ph_w = c.take(d.w); w.pt1 = c.take(d.w); w.ww = c.take(d.w);
   w.a = c.take(d.w); w.alpha = c.take(d.w); w.gamma = c.take(d.w);
+  w.mu_tend_s1 = (spec && p.specified_bdy_cadence) ? c.take(d.s2) : nullptr;
   for (int s = 0; s < 2; ++s) {
     StateW &S = w.st[s];
     S.u = c.take(d.u); S.v = c.take(d.v); S.w = c.take(d.w); S.theta = c.take(d.m);
@@ -148,19 +152,6 @@ Grid make_grid(const wrfgpu_step_params &p, const wrfgpu_metrics &m, const doubl
 
 // Specified boundary work targets (coupling/boundary_apply.py:729-781) for
 // the normal momentum, from the time-interpolated strips.
-struct BdyLeaf {
-  const double *leaf;
-  int ntime, width, side_len, lo, hi;
-  double alpha;
-};
-
-__device__ __forceinline__ double strip_at(const BdyLeaf &b, int nz, int side, int bb, int k, int t) {
-  bb = bb < 0 ? 0 : (bb > b.width - 1 ? b.width - 1 : bb);
-  auto at = [&](int tt) {
-    return ld(b.leaf, ((((size_t)tt * 4 + side) * b.width + bb) * nz + k) * b.side_len + t);
-  };
-  return at(b.lo) * (1.0 - b.alpha) + at(b.hi) * b.alpha;
-}
 
 __global__ void k_bdy_target_u(Grid g, BdyLeaf b, const double *u_save, const double *muu, const double *muus,
                                int nzone, double *target) {
@@ -262,7 +253,8 @@ ProfState g_prof;
 
 const char *kClassNames[] = {"k_recip_msf", "k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
                              "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_uv",
-                             "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col"};
+                             "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col", "k_spec_relax",
+                             "k_spec_w"};
 constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
 
 int class_of(const char *name) {
@@ -442,6 +434,10 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
     if (bdy) n += 2;
     n += 3 * nsub[s];  // advance_uv, div_h, column
     n += 3;  // finish u, v, col
+    if (p->run_boundary && !p->bc_ideal && p->specified_bdy_cadence) {
+      n += (s == 0) ? 2 : 1;  // [first-stage mu tendency], relax tendencies
+      n += nsub[s];           // zero-gradient w after every column launch
+    }
   }
   *launches = n;
   return WRFGPU_OK;
@@ -480,6 +476,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   if (bdy_active && (in->u_bdy == nullptr || in->v_bdy == nullptr || in->bdy_ntime < 1 || in->bdy_width < 1 ||
                      in->bdy_side_len < (p.nx > p.ny ? p.nx + 1 : p.ny + 1)))
     return fail(WRFGPU_ERR_BAD_SHAPE, "run_boundary needs u_bdy/v_bdy strips (ntime, 4, width, nz, side_len)");
+  // specified boundary cadence (operational_mode.py:2478-2492): on with the
+  // flag, a specified domain and a forecast lead
+  const bool cad = p.run_boundary && !p.bc_ideal && p.specified_bdy_cadence && !std::isnan(lead_seconds);
+  if (cad && (in->theta_bdy == nullptr || in->ph_bdy == nullptr || in->mu_bdy == nullptr || in->bdy_width < 5))
+    return fail(WRFGPU_ERR_BAD_SHAPE,
+                "specified_bdy_cadence needs theta_bdy/ph_bdy/mu_bdy strips (ntime, 4, width >= 5, nz | nz+1 | 1, side_len)");
 
   const Dims d = dims_of(p);
   Carver cv{reinterpret_cast<char *>(workspace), 0, workspace_bytes, false};
@@ -533,6 +535,45 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     a = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
     bl_u = BdyLeaf{in->u_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
     bl_v = BdyLeaf{in->v_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
+  }
+  // a leaf with its time interpolation at one lead (boundary_apply.py:329-345)
+  auto leaf_at = [&](const double *leaf, double lead) {
+    const int mx = in->bdy_ntime - 1;
+    const double li = lead / p.update_cadence_s;
+    int lo = (int)std::floor(li);
+    lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
+    int hi = lo + 1;
+    hi = hi < 0 ? 0 : (hi > mx ? mx : hi);
+    double a = li - (double)lo;
+    a = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
+    return BdyLeaf{leaf, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
+  };
+  RelaxArgs ra{};
+  if (cad) {
+    // relax_bdy_dry from the step-start state at the step-start lead
+    // (boundary_apply.py:1148-1248); per-second weights as the reference
+    // forms them: (dt * fcx) / dt (boundary_apply.py:666-688, 1031-1035)
+    ra.u = in->u; ra.v = in->v; ra.theta = in->theta; ra.ph_pert = in->ph_perturbation;
+    ra.mu_total = in->mu_total; ra.mu_pert = in->mu_perturbation;
+    ra.lu = leaf_at(in->u_bdy, lead_seconds);
+    ra.lv = leaf_at(in->v_bdy, lead_seconds);
+    ra.lt = leaf_at(in->theta_bdy, lead_seconds);
+    ra.lph = leaf_at(in->ph_bdy, lead_seconds);
+    ra.lmu = leaf_at(in->mu_bdy, lead_seconds);
+    for (int b = 0; b < RELAX_B1; ++b) {
+      ra.fcx[b] = 0.0;
+      ra.gcx[b] = 0.0;
+      if (b < RELAX_B0) continue;
+      const double dtf = p.dt;
+      const int loop = b + 1;
+      const double num = (double)(p.spec_zone + p.relax_zone - loop), den = (double)(p.relax_zone - 1);
+      double linear = num / den;
+      linear = linear > 0.0 ? linear : 0.0;
+      const double fcx = 0.1 / dtf * linear * 1.0;
+      const double gcx = 1.0 / dtf / 50.0 * linear * 1.0;
+      ra.fcx[b] = (dtf * fcx) / dtf;
+      ra.gcx[b] = (dtf * gcx) / dtf;
+    }
   }
 
   PROF("k_recip_msf");
@@ -662,8 +703,31 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         g, w.mut, w.muts0, w.mu_work0, w.c2a, w.cqw, w.alt, w.theta_w, w.ph_w, origin.theta, cof, p.top_lid, co);
     LAUNCH_CHECK("k_coef");
 
+    if (cad) {
+      // relax tendencies into this stage's u, v, theta and ph' tendencies, and
+      // (first stage only) the mu' tendency (operational_mode.py:1994-1995, 3085-3092)
+      if (stage == 0) {
+        PROF("k_spec_relax");
+        k_mu_tend_init<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, in->base_mu, w.mu_tend_s1);
+        LAUNCH_CHECK("k_mu_tend_init");
+      }
+      RelaxArgs rs = ra;
+      rs.u_tend = w.u_tend; rs.v_tend = w.v_tend; rs.t_tend = w.t_tend; rs.ph_tend = w.ph_tend;
+      rs.mu_tend = (stage == 0) ? w.mu_tend_s1 : nullptr;
+      const int ring_len = 2 * (nx + 1) + 2 * (ny + 1);
+      PROF("k_spec_relax");
+      k_spec_relax_add<<<dim3((ring_len + 127) / 128, RELAX_B1 - RELAX_B0, 5 * (nz + 1)), 128, 0, stream>>>(g, rs);
+      LAUNCH_CHECK("k_spec_relax_add");
+    }
+    const double lead_stage = lead_seconds + dt_rk[stage];  // stage-end lead of the ring-0 pins
+
     BdyArgs ba{};
     ba.active = bdy_active ? 1 : 0;
+    ba.cad = cad ? 1 : 0;
+    if (cad) {
+      ba.cad_u = leaf_at(in->u_bdy, lead_stage);
+      ba.cad_v = leaf_at(in->v_bdy, lead_stage);
+    }
     if (bdy_active) {
       const int nzone = p.spec_zone + p.relax_zone;
       PROF("k_bdy_target_u");
@@ -689,10 +753,20 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     A.alt = w.alt; A.pb = w.pb; A.c2a = w.c2a; A.cqu = w.cqu; A.cqv = w.cqv; A.cqw = w.cqw; A.php = w.php;
     A.pt1 = w.pt1; A.a = w.a; A.alpha = w.alpha; A.gamma = w.gamma; A.ww_1 = ww_stage;
     A.mut = w.mut; A.muu = w.muu; A.muv = w.muv; A.muus = w.muus; A.muvs = w.muvs;
-    A.mu_tend = in->base_mu;
+    A.mu_tend = (cad && stage == 0) ? w.mu_tend_s1 : in->base_mu;
     A.u_1 = s.u; A.v_1 = s.v; A.w_save = s.w; A.theta_s = s.theta; A.phb0 = w.phb0;
-    ColArgs ca{dts, p.epssm, specified ? 1 : 0, p.top_lid, p.w_damping, p.damp_opt, p.dampcoef, p.zdamp,
-               (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0};
+    ColArgs ca{};
+    ca.dts = dts; ca.epssm = p.epssm; ca.specified = specified ? 1 : 0; ca.top_lid = p.top_lid;
+    ca.w_damping = p.w_damping; ca.damp_opt = p.damp_opt; ca.dampcoef = p.dampcoef; ca.zdamp = p.zdamp;
+    ca.rzdamp = (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0;
+    ca.cad = cad ? 1 : 0;
+    if (cad) {
+      ca.cad_mu = leaf_at(in->mu_bdy, lead_stage);
+      ca.cad_th = leaf_at(in->theta_bdy, lead_stage);
+      ca.cad_ph = leaf_at(in->ph_bdy, lead_stage);
+      ca.ph_save = s.ph_pert;
+      ca.mub = w.mub;
+    }
     const size_t col_smem = column_tiled_smem_bytes(nz, cwidth);
     auto kColumn = (cwidth == 16)
                        ? ((lanes == 8) ? k_column_tiled<16, 8> : (lanes == 16) ? k_column_tiled<16, 16> : k_column_tiled<16, 13>)
@@ -712,6 +786,12 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       kColumn<<<dim3((nx + cwidth - 1) / cwidth, ny, 1), dim3(cwidth, lanes, 1), col_smem, stream>>>(g, A, ca, w.dvdxi,
                                                                                                       w.hdiv);
       LAUNCH_CHECK("k_column");
+      if (cad) {
+        PROF("k_spec_w");
+        const int ring0 = 2 * nx + 2 * (ny - 2);
+        k_spec_w_zero_grad<<<dim3((ring0 + 127) / 128, nz + 1, 1), 128, 0, stream>>>(g, w.w_w, s.w, w.mut, w.muts);
+        LAUNCH_CHECK("k_spec_w_zero_grad");
+      }
     }
 
     PROF("k_finish_u");

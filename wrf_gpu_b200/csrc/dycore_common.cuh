@@ -184,6 +184,40 @@ __device__ __forceinline__ double hflux_spec(int m, int n, bool upstream, double
   return vel * 0.0;
 }
 
+// A specified boundary leaf (time, side W/E/S/N, width, z, side_len)
+// (contracts/state.py:96-106) with its time interpolation at one lead
+// (boundary_apply.py:329-345: lower / upper time index and weight).
+struct BdyLeaf {
+  const double *leaf;
+  int ntime, width, side_len, lo, hi;
+  double alpha;
+};
+
+// Strip value of side `side`, width index bb (clamped, boundary_apply.py:528-549),
+// level k, tangential index t; nz is the leaf's level count.
+__device__ __forceinline__ double strip_at(const BdyLeaf &b, int nz, int side, int bb, int k, int t) {
+  bb = bb < 0 ? 0 : (bb > b.width - 1 ? b.width - 1 : bb);
+  auto at = [&](int tt) {
+    return ld(b.leaf, ((((size_t)tt * 4 + side) * b.width + bb) * nz + k) * b.side_len + t);
+  };
+  return at(b.lo) * (1.0 - b.alpha) + at(b.hi) * b.alpha;
+}
+
+// Value at (k, j, i) of the leaf written into the outer five rows / columns of
+// a (zl, yl, xl) field (boundary_apply.py:948-969: for b = 0..4 the W, E, S, N
+// strips in that order, later writes win); 0 off the ring.
+__device__ __forceinline__ double ring_target(const BdyLeaf &b, int zl, int yl, int xl, int k, int j, int i) {
+  int best = -1, side = 0;
+  for (int bb = 0; bb < 5; ++bb) {
+    if (i == bb) { best = bb; side = 0; }
+    if (i == xl - 1 - bb) { best = bb; side = 1; }
+    if (j == bb) { best = bb; side = 2; }
+    if (j == yl - 1 - bb) { best = bb; side = 3; }
+  }
+  if (best < 0) return 0.0;
+  return strip_at(b, zl, side, best, k, side < 2 ? j : i);
+}
+
 // Dry inverse density from the EOS (acoustic_wrf.py:187-206, qvf = 1).
 __device__ __forceinline__ double inv_density(double theta, double p) {
   return (R_D / P0) * theta * 1.0 * pow(dmax(p, 1.0) / P0, CVPM);

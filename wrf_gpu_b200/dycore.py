@@ -29,6 +29,7 @@ from . import _capi
 
 MOIST = ("qv", "qc", "qr", "qi", "qs", "qg")
 STATE_FIELDS = _capi.STATE_FIELDS
+_LEAVES = ("u_bdy", "v_bdy", "theta_bdy", "ph_bdy", "mu_bdy")
 CARRY_FIELDS = _capi.CARRY_OUT_FIELDS
 METRIC_ARRAYS = _capi.METRIC_FIELDS
 
@@ -115,6 +116,9 @@ class State:
     qg: torch.Tensor | None = None
     u_bdy: torch.Tensor | None = None
     v_bdy: torch.Tensor | None = None
+    theta_bdy: torch.Tensor | None = None
+    ph_bdy: torch.Tensor | None = None
+    mu_bdy: torch.Tensor | None = None
 
     @property
     def p(self):
@@ -259,7 +263,8 @@ class OperationalNamelist:
                   boundary_config=bc, w_damping=c["w_damping"], damp_opt=c["damp_opt"], dampcoef=c["dampcoef"],
                   zdamp=c["zdamp"], use_flux_advection=True, scalar_adv_opt=c["scalar_adv_opt"],
                   moist_adv_opt=c["moist_adv_opt"], moist_cqw=c["moist_cqw"], w_coriolis=c["w_coriolis"],
-                  specified_adv_degrade=bool(c.get("specified_adv_degrade", False)))
+                  specified_adv_degrade=bool(c.get("specified_adv_degrade", False)),
+                  specified_bdy_cadence=bool(c.get("specified_bdy_cadence", False)))
         kw.update(overrides)
         return cls(**kw)
 
@@ -273,8 +278,6 @@ def _unsupported(nl: OperationalNamelist, physics_tendencies) -> str | None:
         return "rk_order must be 3"
     if nl.diff_opt or nl.km_opt or nl.diff_6th_opt or nl.const_nu_m2_s > 0.0:
         return "explicit diffusion options are not built"
-    if nl.specified_bdy_cadence:
-        return "specified_bdy_cadence is not built"
     if not nl.boundary_config.force_geopotential and nl.run_boundary and nl.bc_source != "ideal":
         return "nested (force_geopotential=False) boundaries are not built"
     if nl.moist_adv_opt and nl.mp_physics in (7, 17, 18, 19, 21, 22, 24, 26, 27, 28, 38):
@@ -308,6 +311,7 @@ def step_params(nl: OperationalNamelist) -> _capi.StepParams:
     p.moist_cqw, p.w_coriolis = int(bool(nl.moist_cqw)), int(bool(nl.w_coriolis))
     p.precision = _capi.WRFGPU_PRECISION_MIXED if nl.precision == "mixed" else _capi.WRFGPU_PRECISION_FP64
     p.specified_adv_degrade = 1 if nl.specified_adv_degrade else 0
+    p.specified_bdy_cadence = 1 if nl.specified_bdy_cadence else 0
     m = nl.metrics
     p.cf1, p.cf2, p.cf3, p.p_top = m.cf1, m.cf2, m.cf3, m.p_top
     p.cfn, p.cfn1 = m.cfn()
@@ -336,8 +340,8 @@ class Stepper:
     def alloc_carry(self, like: OperationalCarry) -> OperationalCarry:
         s = like.state
         st = State(**{f_.name: (None if getattr(s, f_.name) is None else torch.empty_like(getattr(s, f_.name)))
-                      for f_ in fields(State) if f_.name not in ("u_bdy", "v_bdy")},
-                   u_bdy=s.u_bdy, v_bdy=s.v_bdy)
+                      for f_ in fields(State) if f_.name not in _LEAVES},
+                   **{n: getattr(s, n) for n in _LEAVES})
         e = lambda t: torch.empty_like(t)
         return OperationalCarry(state=st, t_2ave=e(s.theta), ww=e(s.w), mudf=e(s.mu_total), muave=e(s.mu_total),
                                 muts=e(s.mu_total), ph_tend=e(s.w), u_save=e(s.u), v_save=e(s.v), w_save=e(s.w),
@@ -359,6 +363,8 @@ class Stepper:
         if nl.run_boundary and s.u_bdy is not None:
             ins.u_bdy, ins.v_bdy = _ptr(s.u_bdy), _ptr(s.v_bdy)
             ins.bdy_ntime, _, ins.bdy_width, _, ins.bdy_side_len = s.u_bdy.shape
+            if nl.specified_bdy_cadence and s.theta_bdy is not None:
+                ins.theta_bdy, ins.ph_bdy, ins.mu_bdy = _ptr(s.theta_bdy), _ptr(s.ph_bdy), _ptr(s.mu_bdy)
         outs = _capi.StepOutputs()
         for n in STATE_FIELDS:
             setattr(outs, n, _ptr(getattr(o, n)))
