@@ -103,6 +103,25 @@ typedef struct wrfgpu_step_params {
    * 2478-2530, 3085-3092; coupling/boundary_apply.py:1148-1340).  Needs the
    * theta_bdy / ph_bdy / mu_bdy strips. */
   int specified_bdy_cadence;
+  /* BoundaryConfig.force_geopotential (coupling/boundary_apply.py:110;
+   * default 1).  0 makes a run_boundary, non-ideal domain the nested child
+   * (operational_mode.py:1247-1254): the same non-periodic advance_mu_t,
+   * stage omega and order<=6 rhs_ph as a specified domain, with the
+   * specified-only degradation and cadence off, and the three opt-in nested
+   * forcings below (BoundaryConfig defaults 0, boundary_apply.py:142-144;
+   * operational_mode.py:1906-1968):
+   *   nested_ph_relax  relax-zone ph' tendency from the stage state toward
+   *                    ph_bdy, coupled with c1f*mut+c2f, over msfty, added to
+   *                    the stage ph tendency (boundary_apply.py:1045-1068);
+   *   nested_w_relax   the same for w toward w_bdy into the stage rw
+   *                    tendency (boundary_apply.py:1071-1087);
+   *   nested_ph_spec   the ring-0 ph' pin to ph_bdy every acoustic substep
+   *                    after advance_w (boundary_apply.py:1299-1340).
+   * All three read the strips at the step's lead. */
+  int force_geopotential;
+  int nested_ph_relax;
+  int nested_w_relax;
+  int nested_ph_spec;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */
@@ -133,6 +152,9 @@ typedef struct wrfgpu_step_inputs {
    * full theta (nz levels), ph' (nz+1 levels) and mu' (1 level), same
    * (ntime, 4, width, levels, side_len) layout */
   const double *theta_bdy, *ph_bdy, *mu_bdy;
+  /* w strip (nz+1 levels) the nested w relaxation reads (NULL otherwise);
+   * ph_bdy is also read by the nested ph' relaxation and pin */
+  const double *w_bdy;
 } wrfgpu_step_inputs;
 
 /* Step outputs: the returned OperationalCarry (operational_mode.py:2234-2265). */

@@ -59,6 +59,10 @@ class Namelist:
     h_sca_adv_order: int = 2
     specified_adv_degrade: bool = False   # operational_mode.py:460 (opt-in)
     specified_bdy_cadence: bool = False   # operational_mode.py:453 (opt-in)
+    force_geopotential: bool = True       # BoundaryConfig (boundary_apply.py:110); False = nested child
+    nested_ph_relax: bool = False         # boundary_apply.py:142-144 (opt-in nested forcings)
+    nested_w_relax: bool = False
+    nested_ph_spec: bool = False
     scalar_adv_opt: int = 0
     moist_adv_opt: int = 0
     run_boundary: bool = False
@@ -73,10 +77,12 @@ class Namelist:
 
 
 def lateral_flags(nl: Namelist):
-    """``_acoustic_lateral_bc_flags`` (operational_mode.py:1247-1254); force_geopotential=True."""
+    """``_acoustic_lateral_bc_flags`` (operational_mode.py:1247-1254): periodic,
+    specified, nested; a boundary domain without force_geopotential is nested."""
     if not (nl.run_boundary and not nl.bc_ideal):
         return True, False, False
-    return False, True, False
+    nested = not nl.force_geopotential
+    return False, not nested, nested
 
 
 def copy_state(s: SimpleNamespace) -> SimpleNamespace:
@@ -1090,6 +1096,14 @@ def specified_relax_dry_tendencies(ref, lead_seconds, m, dt_full, cadence):
     return r
 
 
+def nested_relax_tendency(field, target, mut, m, dt_full):
+    """boundary_apply.py:1045-1087: the nested child's relax-zone tendency of a
+    full-level field (ph' or w) toward its full-ring target, both coupled with
+    c1f*mut+c2f, over msfty."""
+    mass_f = _col(m.c1f) * mut[None] + _col(m.c2f)
+    return scatter_relax_tendency(mass_f * field, mass_f * target, float(dt_full)) / m.msfty[None]
+
+
 def tangential_targets(u_strip, v_strip, prep, m):
     """boundary_apply.py:1251-1296 (spec_zone 1): ring-0 work targets of the
     tangential winds, u on the S / N rows, v on the W / E columns."""
@@ -1406,7 +1420,7 @@ def advance_w(a, m, nl: Namelist, dts, rdx, rdy):
 def acoustic_substep(a, m, nl: Namelist, dts, bdy=None):
     """core/acoustic.py:837-1150."""
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
-    _, specified, _ = lateral_flags(nl)
+    _, specified, nested = lateral_flags(nl)
     advance_uv(a, m, dts, rdx, rdy, nl.dx, nl.dy, nl.top_lid, bdy)
     cad = getattr(a, "cad", None)
     if cad is not None:  # ring-0 tangential winds (core/acoustic.py:777-785)
@@ -1414,15 +1428,17 @@ def acoustic_substep(a, m, nl: Namelist, dts, bdy=None):
         a.u[:, -1, :] = cad.u_tan[:, -1, :]
         a.v[:, 1:-1, 0] = cad.v_tan[:, 1:-1, 0]
         a.v[:, 1:-1, -1] = cad.v_tan[:, 1:-1, -1]
-    advance_mu_t(a, m, dts, rdx, rdy, nl.epssm, specified)
+    advance_mu_t(a, m, dts, rdx, rdy, nl.epssm, specified or nested)
     if cad is not None:  # ring-0 mass and theta pins (core/acoustic.py:902-915)
         a.mu = _pin_ring(a.mu, cad.mu)
         a.muts = _pin_ring(a.muts, cad.muts)
         a.muave = _pin_ring(a.muave, cad.muave)
         a.theta_work = _pin_ring(a.theta_work, cad.theta)
     advance_w(a, m, nl, dts, rdx, rdy)
-    if cad is not None:  # spec_bdyupdate_ph and zero_grad_bdy w (core/acoustic.py:1059-1090)
-        a.ph = _pin_ring(a.ph, cad.ph_delta)
+    ph_pin = getattr(a, "ph_pin", None)
+    if ph_pin is not None:  # spec_bdyupdate_ph (core/acoustic.py:1059-1071)
+        a.ph = _pin_ring(a.ph, ph_pin)
+    if cad is not None:  # zero_grad_bdy w (core/acoustic.py:1073-1090)
         a.w = specified_w_zero_grad(a.w, a.w_save, a.mut, a.muts, m)
     mu_work = a.muts - a.mut
     al, pp = calc_al_p(mu_work, a.muts, a.ph, a.theta_work, a.theta_1, a.c2a, a.alt, m)
@@ -1466,7 +1482,7 @@ def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Nameli
         rw[1:nz] = rw[1:nz] + (cor + curv)
     ph_tend = rhs_ph(s.u, s.v, prep.ww_save, s.ph_perturbation, prep.phb, s.w, prep.mut,
                      prep.muu, prep.muv, m, rdx, rdy, nl.top_lid, order=nl.h_sca_adv_order,
-                     specified=lateral_flags(nl)[1])
+                     specified=lateral_flags(nl)[1] or lateral_flags(nl)[2])
     a = SimpleNamespace()
     a.ww = prep.ww_save.copy()
     a.ww_1 = prep.ww_save
@@ -1496,6 +1512,19 @@ def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Nameli
     a.rw_tend = rw
     a.php = prep.php
     a.cad = None
+    a.ph_pin = None
+    if lateral_flags(nl)[2] and lead_seconds is not None:
+        # the nested child's opt-in in-loop forcings (operational_mode.py:1906-1968),
+        # all from the stage state and the strips at the step's lead
+        lf0 = lambda leaf: interpolate_boundary_leaf(leaf, lead_seconds, nl.update_cadence_s)
+        if nl.nested_ph_relax:
+            tgt = full_ring_target(lf0(s.ph_bdy), nz + 1, ny, nx)
+            a.ph_tend = a.ph_tend + nested_relax_tendency(s.ph_perturbation, tgt, prep.mut, m, nl.dt_s)
+        if nl.nested_w_relax:
+            tgt = full_ring_target(lf0(s.w_bdy), nz + 1, ny, nx)
+            a.rw_tend = a.rw_tend + nested_relax_tendency(s.w, tgt, prep.mut, m, nl.dt_s)
+        if nl.nested_ph_spec:  # boundary_apply.py:1299-1340
+            a.ph_pin = full_ring_target(lf0(s.ph_bdy), nz + 1, ny, nx) - prep.ph_save
     if bdy_relax is not None:
         a.ph_tend = a.ph_tend + bdy_relax.ph
         lead_stage = lead_seconds + float(dt_rk)
@@ -1512,6 +1541,7 @@ def acoustic_state_from_prep(s, prep, al0, p0, pm1, tend, carry_mudf, nl: Nameli
         cad.theta = mass_pin * (th_pin - T0) - mass_cur * prep.t_save
         cad.u_tan, cad.v_tan = tangential_targets(lf(s.u_bdy), lf(s.v_bdy), prep, m)
         a.cad = cad
+        a.ph_pin = cad.ph_delta
     bdy = None
     if nl.run_boundary and lead_seconds is not None:
         c1h, c2h = _col(m.c1h), _col(m.c2h)

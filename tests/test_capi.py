@@ -126,6 +126,21 @@ def test_launch_count(lib):
     p = _params(lib, acoustic_substeps=6, run_boundary=1, bc_ideal=0, specified_bdy_cadence=1)
     assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(n)) == 0
     assert n.value == (1 + 3 * 13 + 3 * 10) + (1 + 3) + 10
+    # a nested child (force_geopotential off) ignores the cadence flag; its
+    # relax tendencies add one launch per stage, the ring-0 ph' pin none
+    p = _params(lib, acoustic_substeps=6, run_boundary=1, bc_ideal=0, specified_bdy_cadence=1,
+                force_geopotential=0, nested_ph_relax=1, nested_w_relax=1, nested_ph_spec=1)
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(n)) == 0
+    assert n.value == (1 + 3 * 13 + 3 * 10) + 3
+
+
+def test_params_init_keeps_the_geopotential_forced(lib):
+    # BoundaryConfig defaults: force_geopotential on, the nested forcings off
+    # (coupling/boundary_apply.py:110, 142-144)
+    p = _capi.StepParams()
+    lib.wrfgpu_step_params_init(ctypes.byref(p))
+    assert p.force_geopotential == 1
+    assert p.nested_ph_relax == 0 and p.nested_w_relax == 0 and p.nested_ph_spec == 0
 
 
 def test_null_pointers_rejected_before_any_launch(lib):

@@ -158,6 +158,24 @@ def test_per_step_parity_specified_bdy_cadence(cuda_ready, degrade):
         assert not bad, f"degrade={degrade} step {n}: {bad}"
 
 
+@pytest.mark.parametrize("forcings", [
+    dict(nested_ph_relax=True, nested_ph_spec=True),
+    dict(nested_ph_relax=True, nested_w_relax=True, nested_ph_spec=True),
+    dict(specified_adv_degrade=True, specified_bdy_cadence=True),
+])
+def test_per_step_parity_nested(cuda_ready, forcings):
+    """The nested child (force_geopotential off): the relax-zone ph' / w
+    tendencies from the stage state and the ring-0 ph' pin every substep,
+    with drifting perturbed leaves and non-unit map factors; and a child
+    without forcings, whose specified-only degradation and cadence flags are
+    ignored."""
+    case = _with_map_factors(cases.real_like_moist(40, 24, 12, hmax=800.0, specified=True, bdy_noise=True), seed=5)
+    case.controls.update(force_geopotential=False, **forcings)
+    for n, e in enumerate(_per_step(case, 2)):
+        bad = {k: v for k, v in e.items() if not v <= _tol(k)}
+        assert not bad, f"{forcings} step {n}: {bad}"
+
+
 def test_per_step_parity_map_factors_periodic(cuda_ready):
     case = _with_map_factors(cases.real_like_moist(24, 20, 14, hmax=800.0, specified=False), seed=11)
     for n, e in enumerate(_per_step(case, 2)):

@@ -42,7 +42,8 @@ class StepParams(ctypes.Structure):
         ("cf1", _D), ("cf2", _D), ("cf3", _D), ("p_top", _D),
         ("cfn", _D), ("cfn1", _D),
         ("march_levels", _I), ("column_lanes", _I), ("column_width", _I), ("specified_adv_degrade", _I),
-        ("specified_bdy_cadence", _I),
+        ("specified_bdy_cadence", _I), ("force_geopotential", _I), ("nested_ph_relax", _I),
+        ("nested_w_relax", _I), ("nested_ph_spec", _I),
     ]
 
 
@@ -63,7 +64,7 @@ class StepInputs(ctypes.Structure):
         ("q", _P * 6), ("mudf", _P),
         ("base_u", _P), ("base_v", _P), ("base_w", _P), ("base_theta", _P), ("base_mu", _P),
         ("u_bdy", _P), ("v_bdy", _P), ("bdy_ntime", _I), ("bdy_width", _I), ("bdy_side_len", _I),
-        ("theta_bdy", _P), ("ph_bdy", _P), ("mu_bdy", _P),
+        ("theta_bdy", _P), ("ph_bdy", _P), ("mu_bdy", _P), ("w_bdy", _P),
     ]
 
 

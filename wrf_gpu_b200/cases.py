@@ -139,14 +139,15 @@ def _controls(**kw):
 
 def _boundary_leaves(state, nz, ny, nx, times=2, width=5, rng=None):
     """Specified boundary strips ``(time, side, width, z, side_len)`` (``contracts/state.py:96-106``)
-    of u, v, theta (full), ph' (nz+1 levels) and mu' (one level), built from the
-    initial edge rows: constant in time, or with ``rng`` perturbed by seeded
-    noise and drifting between the two time levels (u/v 0.5 m/s, theta 0.3 K,
-    ph' 20 m2/s2, mu' 30 Pa)."""
+    of u, v, theta (full), ph' (nz+1 levels), mu' (one level) and w (nz+1
+    levels), built from the initial edge rows: constant in time, or with
+    ``rng`` perturbed by seeded noise and drifting between the two time levels
+    (u/v 0.5 m/s, theta 0.3 K, ph' 20 m2/s2, mu' 30 Pa, w 0.2 m/s)."""
     side = max(nx + 1, ny + 1)
     out = {}
     specs = (("u_bdy", state.u, 0.5), ("v_bdy", state.v, 0.5), ("theta_bdy", state.theta, 0.3),
-             ("ph_bdy", state.ph_perturbation, 20.0), ("mu_bdy", state.mu_perturbation[None], 30.0))
+             ("ph_bdy", state.ph_perturbation, 20.0), ("mu_bdy", state.mu_perturbation[None], 30.0),
+             ("w_bdy", state.w, 0.2))
     for name, fld, scale in specs:
         zl, yl, xl = fld.shape
         leaf = np.zeros((times, 4, width, zl, side))

@@ -299,11 +299,16 @@ struct ColArgs {
   int specified, top_lid, w_damping, damp_opt;
   double dampcoef, zdamp;
   double rzdamp;  // 1/zdamp correctly rounded, 0 when zdamp is 0 or its reciprocal overflows
-  // specified boundary cadence: ring-0 pins of mu / muts / muave, the work
-  // theta and the work ph from the leaves at the stage-end lead
-  // (operational_mode.py:1984-2029; core/acoustic.py:902-915, 1059-1068)
+  // specified boundary cadence: ring-0 pins of mu / muts / muave and the work
+  // theta from the leaves at the stage-end lead (operational_mode.py:1984-2029;
+  // core/acoustic.py:902-915)
   int cad;
-  BdyLeaf cad_mu, cad_th, cad_ph;
+  BdyLeaf cad_mu, cad_th;
+  // ring-0 work ph pin after advance_w (spec_bdyupdate_ph, core/acoustic.py:1059-1071):
+  // the cadence's at the stage-end lead, the nested child's at the step's lead
+  // (operational_mode.py:1961-1968)
+  int ph_pin;
+  BdyLeaf cad_ph;
   const double *ph_save;  // stage ph' (the work ph's reference)
   const double *mub;      // base dry mass
 };

@@ -1,13 +1,18 @@
 // The specified-domain boundary cadence (operational namelist
 // specified_bdy_cadence; operational_mode.py:1984-2041, 2478-2530, 3085-3092;
 // coupling/boundary_apply.py:948-1043, 1148-1340; core/acoustic.py:383-516,
-// 777-785, 902-915, 1059-1090).  Everything here touches only the outer five
+// 777-785, 902-915, 1059-1090) and the nested child's in-loop forcings
+// (force_geopotential off; operational_mode.py:1906-1968;
+// boundary_apply.py:1045-1087).  Everything here touches only the outer five
 // rows / columns of the domain, so the kernels run over ring cells only:
 //   * k_spec_relax_add    -- WRF relax_bdy_dry: the relax-zone (rings 1..3)
-//                            tendencies of the coupled u, v, theta, ph' and
-//                            mu' from the step-start state and boundary leaves
-//                            at the step-start lead, added to the stage
-//                            tendencies (mu' into the first stage's only);
+//                            tendencies of the coupled u, v, theta, ph', mu'
+//                            and w toward the boundary leaves, added to the
+//                            stage tendencies.  The cadence relaxes u, v,
+//                            theta, ph' and mu' (mu' into the first stage's
+//                            tendency only) from the step-start state; the
+//                            nested child ph' and / or w from the stage state
+//                            with the stage mass;
 //   * k_spec_w_zero_grad  -- WRF zero_grad_bdy for w, every acoustic substep:
 //                            the ring-0 work w whose finished physical w equals
 //                            the nearest interior physical w.
@@ -21,14 +26,20 @@ namespace wg {
 // Relax-zone rows of the default boundary configuration (spec_zone 1, relax_zone 4).
 constexpr int RELAX_B0 = 1, RELAX_B1 = 4;
 
+// Relaxed fields, in the order of RelaxArgs::fields.
+enum RelaxField { RELAX_U = 0, RELAX_V, RELAX_THETA, RELAX_PH, RELAX_MU, RELAX_W, RELAX_NFIELD };
+
 struct RelaxArgs {
-  // step-start state (the relax reference)
-  const double *u, *v, *theta, *ph_pert, *mu_total, *mu_pert;
-  BdyLeaf lu, lv, lt, lph, lmu;  // leaves at the step-start lead
+  // the relax reference: fields and the total dry mass that couples them
+  const double *u, *v, *theta, *ph_pert, *mu_total, *mu_pert, *w;
+  BdyLeaf lu, lv, lt, lph, lmu, lw;  // leaves at the step's lead
   // per-second weights fcx, gcx of rows b = 1..3 (index b)
   double fcx[RELAX_B1], gcx[RELAX_B1];
   // tendencies the relax terms are added to (mu_tend: the first stage only, else null)
-  double *u_tend, *v_tend, *t_tend, *ph_tend, *mu_tend;
+  double *u_tend, *v_tend, *t_tend, *ph_tend, *mu_tend, *rw_tend;
+  // the relaxed fields of this launch (RelaxField values); blockIdx.z / (nz+1) indexes them
+  int nfield;
+  int fields[RELAX_NFIELD];
 };
 
 // Ring position e of row / column ring b of a (yl, xl) field in WRF's relax
@@ -73,27 +84,29 @@ __device__ __forceinline__ double relax_value(FLS fls, int side, int j, int i, i
   return fcx * f0 - gcx * lap;
 }
 
-// blockIdx.y = ring b - 1, blockIdx.z = field * (nz + 1) + level; x threads
-// over the ring positions.  Fields: 0 u, 1 v, 2 theta, 3 ph', 4 mu'.
+// blockIdx.y = ring b - 1, blockIdx.z = slot * (nz + 1) + level with
+// fields[slot] the relaxed field; x threads over the ring positions.
 __global__ void k_spec_relax_add(Grid g, RelaxArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int b = RELAX_B0 + blockIdx.y;
-  const int field = blockIdx.z / (nz + 1), k = blockIdx.z - field * (nz + 1);
+  const int slot = blockIdx.z / (nz + 1), k = blockIdx.z - slot * (nz + 1);
+  if (slot >= a.nfield) return;
+  const int field = a.fields[slot];
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   int zl, yl, xl;
   switch (field) {
-    case 0: zl = nz; yl = ny; xl = nx + 1; break;
-    case 1: zl = nz; yl = ny + 1; xl = nx; break;
-    case 2: zl = nz; yl = ny; xl = nx; break;
-    case 3: zl = nz + 1; yl = ny; xl = nx; break;
+    case RELAX_U: zl = nz; yl = ny; xl = nx + 1; break;
+    case RELAX_V: zl = nz; yl = ny + 1; xl = nx; break;
+    case RELAX_THETA: zl = nz; yl = ny; xl = nx; break;
+    case RELAX_PH: case RELAX_W: zl = nz + 1; yl = ny; xl = nx; break;
     default: zl = 1; yl = ny; xl = nx; break;
   }
-  if (k >= zl || (field == 4 && a.mu_tend == nullptr)) return;
+  if (k >= zl || (field == RELAX_MU && a.mu_tend == nullptr)) return;
   int j, i, side;
   if (!relax_ring_cell(e, b, yl, xl, j, i, side)) return;
   auto mu = [&](int jj, int ii) { return ld(a.mu_total, ix2(jj, ii, nx)); };
   double val;
-  if (field == 0) {
+  if (field == RELAX_U) {
     const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
     auto fls = [&](int jj, int ii) {
       // face mass of the relax reference (edge-padded face average)
@@ -107,7 +120,7 @@ __global__ void k_spec_relax_add(Grid g, RelaxArgs a) {
     val = 0.0 + relax_value(fls, side, j, i, yl, xl, a.fcx[b], a.gcx[b]);
     double *t = a.u_tend + ix3(k, j, i, ny, nx + 1);
     *t = *t + val;
-  } else if (field == 1) {
+  } else if (field == RELAX_V) {
     const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
     auto fls = [&](int jj, int ii) {
       const double muv = 0.5 * (mu(jj > 0 ? jj - 1 : 0, ii) + mu(jj < ny ? jj : ny - 1, ii));
@@ -120,7 +133,7 @@ __global__ void k_spec_relax_add(Grid g, RelaxArgs a) {
     val = 0.0 + relax_value(fls, side, j, i, yl, xl, a.fcx[b], a.gcx[b]);
     double *t = a.v_tend + ix3(k, j, i, ny + 1, nx);
     *t = *t + val;
-  } else if (field == 2) {
+  } else if (field == RELAX_THETA) {
     const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
     auto fls = [&](int jj, int ii) {
       const double mass = c1 * mu(jj, ii) + c2;
@@ -129,14 +142,18 @@ __global__ void k_spec_relax_add(Grid g, RelaxArgs a) {
     val = div_msf(0.0 + relax_value(fls, side, j, i, yl, xl, a.fcx[b], a.gcx[b]), g.msfty, g.rmsfty, ix2(j, i, nx));
     double *t = a.t_tend + ix3(k, j, i, ny, nx);
     *t = *t + val;
-  } else if (field == 3) {
+  } else if (field == RELAX_PH || field == RELAX_W) {
+    // full-level fields coupled with c1f*mu+c2f (boundary_apply.py:1062-1068, 1081-1087)
+    const bool ph = field == RELAX_PH;
+    const double *fl = ph ? a.ph_pert : a.w;
+    const BdyLeaf &lf = ph ? a.lph : a.lw;
     const double c1 = ld(g.c1f, k), c2 = ld(g.c2f, k);
     auto fls = [&](int jj, int ii) {
       const double mass = c1 * mu(jj, ii) + c2;
-      return mass * ring_target(a.lph, zl, yl, xl, k, jj, ii) - mass * ld(a.ph_pert, ix3(k, jj, ii, ny, nx));
+      return mass * ring_target(lf, zl, yl, xl, k, jj, ii) - mass * ld(fl, ix3(k, jj, ii, ny, nx));
     };
     val = div_msf(0.0 + relax_value(fls, side, j, i, yl, xl, a.fcx[b], a.gcx[b]), g.msfty, g.rmsfty, ix2(j, i, nx));
-    double *t = a.ph_tend + ix3(k, j, i, ny, nx);
+    double *t = (ph ? a.ph_tend : a.rw_tend) + ix3(k, j, i, ny, nx);
     *t = *t + val;
   } else {
     auto fls = [&](int jj, int ii) {
@@ -162,7 +179,7 @@ __global__ void k_mu_tend_init(Grid g, const double *base_mu, double *mu_tend) {
 // corners), blockIdx.y = level 0..nz.
 __global__ void k_spec_w_zero_grad(Grid g, double *w, const double *w_save, const double *mut,
                                    const double *muts) {
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nx = g.nx, ny = g.ny;
   const int f = blockIdx.y;
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   int j, i, js, is;

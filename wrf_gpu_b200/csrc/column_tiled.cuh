@@ -449,8 +449,8 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
         S(A4, f) = phn;
         A.ph[M(f)] = phn;
       }
-      if (!active && c.cad) {
-        // specified cadence: ring-0 work ph whose finished ph' is the leaf's (spec_bdyupdate_ph)
+      if (!active && c.ph_pin) {
+        // ring-0 work ph whose finished ph' is the leaf's (spec_bdyupdate_ph)
         const double phn = ring_target(c.cad_ph, nz + 1, ny, nx, f, j, i) - ld(c.ph_save, M(f));
         S(A4, f) = phn;
         A.ph[M(f)] = phn;

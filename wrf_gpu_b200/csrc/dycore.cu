@@ -117,7 +117,7 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   w.rw_tend = c.take(d.w); w.ph_tend = c.take(d.w); w.cqw = c.take(d.w); w.w_w = c.take(d.w);
   w.ph_w = c.take(d.w); w.pt1 = c.take(d.w); w.ww = c.take(d.w);
   w.a = c.take(d.w); w.alpha = c.take(d.w); w.gamma = c.take(d.w);
-  w.mu_tend_s1 = (spec && p.specified_bdy_cadence) ? c.take(d.s2) : nullptr;
+  w.mu_tend_s1 = (spec && p.specified_bdy_cadence && p.force_geopotential) ? c.take(d.s2) : nullptr;
   for (int s = 0; s < 2; ++s) {
     StateW &S = w.st[s];
     S.u = c.take(d.u); S.v = c.take(d.v); S.w = c.take(d.w); S.theta = c.take(d.m);
@@ -369,6 +369,7 @@ int wrfgpu_step_params_init(wrfgpu_step_params *p) {
   p->relax_zone = 4;
   p->update_cadence_s = 3600.0;
   p->normal_bdy_relax_strength = -1.0;
+  p->force_geopotential = 1;
   p->moist_cqw = 1;
   p->w_coriolis = 1;
   p->precision = WRFGPU_PRECISION_FP64;
@@ -403,7 +404,7 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 16 or 32");
   if (p->specified_adv_degrade != 0 && p->specified_adv_degrade != 1)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "specified_adv_degrade must be 0 or 1");
-  if (spec && p->specified_adv_degrade && (p->nx < 7 || p->ny < 7))
+  if (spec && p->specified_adv_degrade && p->force_geopotential && (p->nx < 7 || p->ny < 7))
     return fail(WRFGPU_ERR_BAD_SHAPE, "the specified advection degradation needs nx, ny >= 7");
   return WRFGPU_OK;
 }
@@ -434,10 +435,12 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
     if (bdy) n += 2;
     n += 3 * nsub[s];  // advance_uv, div_h, column
     n += 3;  // finish u, v, col
-    if (p->run_boundary && !p->bc_ideal && p->specified_bdy_cadence) {
+    if (p->run_boundary && !p->bc_ideal && p->force_geopotential && p->specified_bdy_cadence) {
       n += (s == 0) ? 2 : 1;  // [first-stage mu tendency], relax tendencies
       n += nsub[s];           // zero-gradient w after every column launch
     }
+    if (p->run_boundary && !p->bc_ideal && !p->force_geopotential && (p->nested_ph_relax || p->nested_w_relax))
+      n += 1;  // the nested child's ph' / w relax tendencies
   }
   *launches = n;
   return WRFGPU_OK;
@@ -478,10 +481,20 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     return fail(WRFGPU_ERR_BAD_SHAPE, "run_boundary needs u_bdy/v_bdy strips (ntime, 4, width, nz, side_len)");
   // specified boundary cadence (operational_mode.py:2478-2492): on with the
   // flag, a specified domain and a forecast lead
-  const bool cad = p.run_boundary && !p.bc_ideal && p.specified_bdy_cadence && !std::isnan(lead_seconds);
+  const bool cad = p.run_boundary && !p.bc_ideal && p.force_geopotential && p.specified_bdy_cadence &&
+                   !std::isnan(lead_seconds);
   if (cad && (in->theta_bdy == nullptr || in->ph_bdy == nullptr || in->mu_bdy == nullptr || in->bdy_width < 5))
     return fail(WRFGPU_ERR_BAD_SHAPE,
                 "specified_bdy_cadence needs theta_bdy/ph_bdy/mu_bdy strips (ntime, 4, width >= 5, nz | nz+1 | 1, side_len)");
+  // the nested child's opt-in in-loop forcings (operational_mode.py:1906-1968):
+  // a boundary domain without force_geopotential, with a forecast lead
+  const bool nested = p.run_boundary && !p.bc_ideal && !p.force_geopotential && !std::isnan(lead_seconds);
+  const bool nest_ph_relax = nested && p.nested_ph_relax, nest_w_relax = nested && p.nested_w_relax;
+  const bool nest_ph_pin = nested && p.nested_ph_spec;
+  if ((nest_ph_relax || nest_ph_pin) && (in->ph_bdy == nullptr || in->bdy_width < 5))
+    return fail(WRFGPU_ERR_BAD_SHAPE, "nested_ph_relax / nested_ph_spec need the ph_bdy strip (width >= 5, nz+1 levels)");
+  if (nest_w_relax && (in->w_bdy == nullptr || in->bdy_width < 5))
+    return fail(WRFGPU_ERR_BAD_SHAPE, "nested_w_relax needs the w_bdy strip (width >= 5, nz+1 levels)");
 
   const Dims d = dims_of(p);
   Carver cv{reinterpret_cast<char *>(workspace), 0, workspace_bytes, false};
@@ -549,17 +562,9 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     return BdyLeaf{leaf, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
   };
   RelaxArgs ra{};
-  if (cad) {
-    // relax_bdy_dry from the step-start state at the step-start lead
-    // (boundary_apply.py:1148-1248); per-second weights as the reference
-    // forms them: (dt * fcx) / dt (boundary_apply.py:666-688, 1031-1035)
-    ra.u = in->u; ra.v = in->v; ra.theta = in->theta; ra.ph_pert = in->ph_perturbation;
-    ra.mu_total = in->mu_total; ra.mu_pert = in->mu_perturbation;
-    ra.lu = leaf_at(in->u_bdy, lead_seconds);
-    ra.lv = leaf_at(in->v_bdy, lead_seconds);
-    ra.lt = leaf_at(in->theta_bdy, lead_seconds);
-    ra.lph = leaf_at(in->ph_bdy, lead_seconds);
-    ra.lmu = leaf_at(in->mu_bdy, lead_seconds);
+  if (cad || nest_ph_relax || nest_w_relax) {
+    // per-second weights as the reference forms them: (dt * fcx) / dt
+    // (boundary_apply.py:666-688, 1031-1035)
     for (int b = 0; b < RELAX_B1; ++b) {
       ra.fcx[b] = 0.0;
       ra.gcx[b] = 0.0;
@@ -575,6 +580,20 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       ra.gcx[b] = (dtf * gcx) / dtf;
     }
   }
+  if (cad) {
+    // relax_bdy_dry from the step-start state at the step-start lead
+    // (boundary_apply.py:1148-1248)
+    ra.u = in->u; ra.v = in->v; ra.theta = in->theta; ra.ph_pert = in->ph_perturbation;
+    ra.mu_total = in->mu_total; ra.mu_pert = in->mu_perturbation;
+    ra.lu = leaf_at(in->u_bdy, lead_seconds);
+    ra.lv = leaf_at(in->v_bdy, lead_seconds);
+    ra.lt = leaf_at(in->theta_bdy, lead_seconds);
+    ra.lph = leaf_at(in->ph_bdy, lead_seconds);
+    ra.lmu = leaf_at(in->mu_bdy, lead_seconds);
+    ra.nfield = 5;
+    const int cad_fields[5] = {RELAX_U, RELAX_V, RELAX_THETA, RELAX_PH, RELAX_MU};
+    for (int f = 0; f < 5; ++f) ra.fields[f] = cad_fields[f];
+  }
 
   PROF("k_recip_msf");
   k_recip_msf<<<grd(nx + 1, ny + 1, 1), blk2(), 0, stream>>>(g, w.rmsftx, w.rmsfty, w.rmsfux, w.rmsfuy, w.rmsfvx,
@@ -589,7 +608,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   // specified-boundary advection degradation (operational_mode.py:2464-2475,
   // 2494-2507; flux_advection.py:288-391): tiered faces, masked divergences,
   // a compile-time switch of the advection kernels
-  const int deg = (specified && p.specified_adv_degrade) ? 1 : 0;
+  const int deg = (specified && p.force_geopotential && p.specified_adv_degrade) ? 1 : 0;
   auto kUface = mixed ? (deg ? k_uface_tiled<float, true> : k_uface_tiled<float, false>)
                       : (deg ? k_uface_tiled<double, true> : k_uface_tiled<double, false>);
   auto kVface = mixed ? (deg ? k_vface_tiled<float, true> : k_vface_tiled<float, false>)
@@ -716,7 +735,30 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       rs.mu_tend = (stage == 0) ? w.mu_tend_s1 : nullptr;
       const int ring_len = 2 * (nx + 1) + 2 * (ny + 1);
       PROF("k_spec_relax");
-      k_spec_relax_add<<<dim3((ring_len + 127) / 128, RELAX_B1 - RELAX_B0, 5 * (nz + 1)), 128, 0, stream>>>(g, rs);
+      k_spec_relax_add<<<dim3((ring_len + 127) / 128, RELAX_B1 - RELAX_B0, rs.nfield * (nz + 1)), 128, 0, stream>>>(
+          g, rs);
+      LAUNCH_CHECK("k_spec_relax_add");
+    }
+    if (nest_ph_relax || nest_w_relax) {
+      // the nested child's relax-zone ph' / w tendencies from the stage state,
+      // coupled with the stage mass, leaves at the step's lead, into this
+      // stage's ph and rw tendencies (operational_mode.py:1925-1959)
+      RelaxArgs rn = ra;
+      rn.ph_pert = s.ph_pert; rn.w = s.w; rn.mu_total = w.mut;
+      rn.ph_tend = w.ph_tend; rn.rw_tend = w.rw_tend;
+      rn.nfield = 0;
+      if (nest_ph_relax) {
+        rn.lph = leaf_at(in->ph_bdy, lead_seconds);
+        rn.fields[rn.nfield++] = RELAX_PH;
+      }
+      if (nest_w_relax) {
+        rn.lw = leaf_at(in->w_bdy, lead_seconds);
+        rn.fields[rn.nfield++] = RELAX_W;
+      }
+      const int ring_len = 2 * (nx + 1) + 2 * (ny + 1);
+      PROF("k_spec_relax");
+      k_spec_relax_add<<<dim3((ring_len + 127) / 128, RELAX_B1 - RELAX_B0, rn.nfield * (nz + 1)), 128, 0, stream>>>(
+          g, rn);
       LAUNCH_CHECK("k_spec_relax_add");
     }
     const double lead_stage = lead_seconds + dt_rk[stage];  // stage-end lead of the ring-0 pins
@@ -763,9 +805,13 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     if (cad) {
       ca.cad_mu = leaf_at(in->mu_bdy, lead_stage);
       ca.cad_th = leaf_at(in->theta_bdy, lead_stage);
-      ca.cad_ph = leaf_at(in->ph_bdy, lead_stage);
-      ca.ph_save = s.ph_pert;
       ca.mub = w.mub;
+    }
+    ca.ph_pin = (cad || nest_ph_pin) ? 1 : 0;
+    if (ca.ph_pin) {
+      // the cadence pins to the stage-end lead, the nested child to the step's lead
+      ca.cad_ph = leaf_at(in->ph_bdy, cad ? lead_stage : lead_seconds);
+      ca.ph_save = s.ph_pert;
     }
     const size_t col_smem = column_tiled_smem_bytes(nz, cwidth);
     auto kColumn = (cwidth == 16)

@@ -29,7 +29,7 @@ from . import _capi
 
 MOIST = ("qv", "qc", "qr", "qi", "qs", "qg")
 STATE_FIELDS = _capi.STATE_FIELDS
-_LEAVES = ("u_bdy", "v_bdy", "theta_bdy", "ph_bdy", "mu_bdy")
+_LEAVES = ("u_bdy", "v_bdy", "theta_bdy", "ph_bdy", "mu_bdy", "w_bdy")
 CARRY_FIELDS = _capi.CARRY_OUT_FIELDS
 METRIC_ARRAYS = _capi.METRIC_FIELDS
 
@@ -119,6 +119,7 @@ class State:
     theta_bdy: torch.Tensor | None = None
     ph_bdy: torch.Tensor | None = None
     mu_bdy: torch.Tensor | None = None
+    w_bdy: torch.Tensor | None = None
 
     @property
     def p(self):
@@ -203,6 +204,9 @@ class BoundaryConfig:
     relax_zone: int = 4
     update_cadence_s: float = 3600.0
     force_geopotential: bool = True
+    nested_ph_relax: bool = False
+    nested_w_relax: bool = False
+    nested_ph_spec: bool = False
     normal_bdy_relax_strength: float | None = None
 
 
@@ -255,7 +259,11 @@ class OperationalNamelist:
         m = metrics if metrics is not None else DycoreMetrics.from_host(case.metrics, device)
         bc = BoundaryConfig(spec_zone=c["spec_zone"], relax_zone=c["relax_zone"],
                             update_cadence_s=c["update_cadence_s"],
-                            normal_bdy_relax_strength=c["normal_bdy_relax_strength"])
+                            normal_bdy_relax_strength=c["normal_bdy_relax_strength"],
+                            force_geopotential=bool(c.get("force_geopotential", True)),
+                            nested_ph_relax=bool(c.get("nested_ph_relax", False)),
+                            nested_w_relax=bool(c.get("nested_w_relax", False)),
+                            nested_ph_spec=bool(c.get("nested_ph_spec", False)))
         kw = dict(metrics=m, nx=case.nx, ny=case.ny, nz=case.nz, dx_m=c["dx"], dy_m=c["dy"], dt_s=c["dt_s"],
                   acoustic_substeps=c["acoustic_substeps"], epssm=c["epssm"], hypsometric_opt=c["hypsometric_opt"],
                   h_sca_adv_order=c["h_sca_adv_order"], top_lid=c["top_lid"], run_physics=False,
@@ -278,8 +286,6 @@ def _unsupported(nl: OperationalNamelist, physics_tendencies) -> str | None:
         return "rk_order must be 3"
     if nl.diff_opt or nl.km_opt or nl.diff_6th_opt or nl.const_nu_m2_s > 0.0:
         return "explicit diffusion options are not built"
-    if not nl.boundary_config.force_geopotential and nl.run_boundary and nl.bc_source != "ideal":
-        return "nested (force_geopotential=False) boundaries are not built"
     if nl.moist_adv_opt and nl.mp_physics in (7, 17, 18, 19, 21, 22, 24, 26, 27, 28, 38):
         return "extra advected species of this mp_physics family are not built"
     if nl.acoustic_precision_mode != "fp64_default":
@@ -312,6 +318,10 @@ def step_params(nl: OperationalNamelist) -> _capi.StepParams:
     p.precision = _capi.WRFGPU_PRECISION_MIXED if nl.precision == "mixed" else _capi.WRFGPU_PRECISION_FP64
     p.specified_adv_degrade = 1 if nl.specified_adv_degrade else 0
     p.specified_bdy_cadence = 1 if nl.specified_bdy_cadence else 0
+    bc = nl.boundary_config
+    p.force_geopotential = int(bool(bc.force_geopotential))
+    p.nested_ph_relax, p.nested_w_relax = int(bool(bc.nested_ph_relax)), int(bool(bc.nested_w_relax))
+    p.nested_ph_spec = int(bool(bc.nested_ph_spec))
     m = nl.metrics
     p.cf1, p.cf2, p.cf3, p.p_top = m.cf1, m.cf2, m.cf3, m.p_top
     p.cfn, p.cfn1 = m.cfn()
@@ -365,6 +375,11 @@ class Stepper:
             ins.bdy_ntime, _, ins.bdy_width, _, ins.bdy_side_len = s.u_bdy.shape
             if nl.specified_bdy_cadence and s.theta_bdy is not None:
                 ins.theta_bdy, ins.ph_bdy, ins.mu_bdy = _ptr(s.theta_bdy), _ptr(s.ph_bdy), _ptr(s.mu_bdy)
+            bc = nl.boundary_config
+            if not bc.force_geopotential and (bc.nested_ph_relax or bc.nested_ph_spec) and s.ph_bdy is not None:
+                ins.ph_bdy = _ptr(s.ph_bdy)
+            if not bc.force_geopotential and bc.nested_w_relax and s.w_bdy is not None:
+                ins.w_bdy = _ptr(s.w_bdy)
         outs = _capi.StepOutputs()
         for n in STATE_FIELDS:
             setattr(outs, n, _ptr(getattr(o, n)))
