@@ -251,6 +251,53 @@ int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *params, const wrfg
                                     const double *tend_bar, const double *ru, const double *rv, const double *rom,
                                     double *q_bar, cudaStream_t stream);
 
+/* One acoustic small step on its own (the reference's acoustic_substep_core,
+ * core/acoustic.py:837-1150: advance_uv, advance_mu_t, advance_w with its
+ * Thomas solve, calc_p_rho with smdiv memory), over the evolving work state of
+ * AcousticCoreState (core/acoustic.py:112-292) with the stage constants held
+ * fixed.  Layouts as the step's: u (nz, ny, nx+1), v (nz, ny+1, nx); w, ph, ww
+ * (nz+1, ny, nx); theta_w, t_2ave, p, pm1, al and the stage 3-D constants
+ * (nz, ny, nx), except rw_tend, ph_tend, cqw, pt1, a, alpha, gamma, ww_1 and
+ * w_save (nz+1, ny, nx); 2-D fields (ny, nx); cqu / u_tend / u_1 u-face, cqv /
+ * v_tend / v_1 v-face shaped. */
+typedef struct wrfgpu_acoustic_work {
+  double *u, *v, *w, *ph, *theta_w, *t_2ave, *p, *pm1, *al, *ww; /* 3-D */
+  double *mu, *muts, *muave, *mudf;                              /* 2-D */
+} wrfgpu_acoustic_work;
+
+typedef struct wrfgpu_acoustic_consts {
+  const double *u_tend, *v_tend, *t_tend, *rw_tend, *ph_tend; /* stage tendencies */
+  const double *alt, *pb, *c2a, *cqu, *cqv, *cqw, *php;       /* stage diagnostics */
+  const double *pt1;                                          /* ph_1 + phb (faces) */
+  const double *a, *alpha, *gamma;                            /* calc_coef_w */
+  const double *ww_1;                                         /* stage omega */
+  const double *mut, *muu, *muv;                              /* stage masses */
+  const double *mu_tend;                                      /* NULL = zero */
+  const double *u_1, *v_1, *w_save, *theta;                   /* stage u, v, w, theta */
+  const double *phb0;                                         /* base geopotential, face 0 (ny, nx) */
+} wrfgpu_acoustic_consts;
+
+/* Scratch bytes of wrfgpu_acoustic_substep / _vjp for these params. */
+int wrfgpu_acoustic_workspace_size(const wrfgpu_step_params *params, size_t *bytes);
+
+/* x <- one acoustic substep of length dts from x (in place).  Doubly
+ * periodic domains (run_boundary 0) without the w_damping CFL term. */
+int wrfgpu_acoustic_substep(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                            const wrfgpu_acoustic_consts *consts, wrfgpu_acoustic_work *x, double dts,
+                            void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* Its vector-Jacobian product at x: cot_in = J(x)^T cot_out, J the Jacobian of
+ * wrfgpu_acoustic_substep with respect to the work state, constants fixed
+ * (muave enters no output: its cot_in is zero).  x_out is the substep's
+ * output from x (a stored checkpoint); NULL recomputes it into the
+ * workspace.  cot_out is read only; cot_in must not alias it.  No
+ * counterpart in the reference, which has no differentiation. */
+int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                                const wrfgpu_acoustic_consts *consts, const wrfgpu_acoustic_work *x,
+                                const wrfgpu_acoustic_work *x_out, const wrfgpu_acoustic_work *cot_out,
+                                wrfgpu_acoustic_work *cot_in, double dts, void *workspace, size_t workspace_bytes,
+                                cudaStream_t stream);
+
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 

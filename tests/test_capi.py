@@ -175,3 +175,17 @@ def test_host_shim_rejects_unsupported_namelist():
     nl = dycore.OperationalNamelist.from_case(case, metrics=m)
     with pytest.raises(NotImplementedError):
         dycore.rk_scan_step(carry, nl, physics_tendencies=object())
+
+
+def test_acoustic_substep_rejects_before_any_launch(lib):
+    m, c, x = _capi.Metrics(), _capi.AcousticConsts(), _capi.AcousticWork()
+    for kw, code in ((dict(run_boundary=1), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+                     (dict(w_damping=1), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+                     (dict(), _capi.WRFGPU_ERR_NULL_POINTER)):
+        p = _params(lib, **kw)
+        assert lib.wrfgpu_acoustic_substep(ctypes.byref(p), ctypes.byref(m), ctypes.byref(c), ctypes.byref(x), 1.0,
+                                           None, 0, None) == code
+        assert lib.wrfgpu_acoustic_substep_vjp(ctypes.byref(p), ctypes.byref(m), ctypes.byref(c), ctypes.byref(x),
+                                               None, ctypes.byref(x), ctypes.byref(x), 1.0, None, 0, None) == code
+    n = ctypes.c_size_t(0)
+    assert lib.wrfgpu_acoustic_workspace_size(ctypes.byref(_params(lib)), ctypes.byref(n)) == 0 and n.value > 0

@@ -76,10 +76,26 @@ class StepOutputs(ctypes.Structure):
     _fields_ = [(n, _P) for n in STATE_FIELDS] + [("q", _P * 6)] + [(n, _P) for n in CARRY_OUT_FIELDS]
 
 
+ACOUSTIC_WORK_FIELDS = ("u", "v", "w", "ph", "theta_w", "t_2ave", "p", "pm1", "al", "ww", "mu", "muts", "muave",
+                        "mudf")
+ACOUSTIC_CONST_FIELDS = ("u_tend", "v_tend", "t_tend", "rw_tend", "ph_tend", "alt", "pb", "c2a", "cqu", "cqv", "cqw",
+                         "php", "pt1", "a", "alpha", "gamma", "ww_1", "mut", "muu", "muv", "mu_tend", "u_1", "v_1",
+                         "w_save", "theta", "phb0")
+
+
+class AcousticWork(ctypes.Structure):
+    _fields_ = [(n, _P) for n in ACOUSTIC_WORK_FIELDS]
+
+
+class AcousticConsts(ctypes.Structure):
+    _fields_ = [(n, _P) for n in ACOUSTIC_CONST_FIELDS]
+
+
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
             "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace",
             "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_scalar_advection",
-            "wrfgpu_scalar_advection_adjoint", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_scalar_advection_adjoint", "wrfgpu_acoustic_workspace_size", "wrfgpu_acoustic_substep",
+            "wrfgpu_acoustic_substep_vjp", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version")
 
@@ -122,6 +138,17 @@ def load(path: str | os.PathLike | None = None):
         fn = getattr(lib, name)
         fn.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), _P, _P, _P, _P, _P, _P]
         fn.restype = _I
+    lib.wrfgpu_acoustic_workspace_size.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_size_t)]
+    lib.wrfgpu_acoustic_workspace_size.restype = _I
+    lib.wrfgpu_acoustic_substep.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
+                                            ctypes.POINTER(AcousticConsts), ctypes.POINTER(AcousticWork), _D, _P,
+                                            ctypes.c_size_t, _P]
+    lib.wrfgpu_acoustic_substep.restype = _I
+    lib.wrfgpu_acoustic_substep_vjp.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
+                                                ctypes.POINTER(AcousticConsts), ctypes.POINTER(AcousticWork),
+                                                ctypes.POINTER(AcousticWork), ctypes.POINTER(AcousticWork),
+                                                ctypes.POINTER(AcousticWork), _D, _P, ctypes.c_size_t, _P]
+    lib.wrfgpu_acoustic_substep_vjp.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

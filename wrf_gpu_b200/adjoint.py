@@ -62,3 +62,78 @@ def scalar_advection(q: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: t
     velocities ``ru``, ``rv`` (nz, ny, nx) and ``rom`` (nz+1, ny, nx);
     differentiable with respect to ``q``."""
     return ScalarAdvection.apply(q, ru, rv, rom, _Op(namelist))
+
+
+class AcousticOp:
+    """One acoustic small step (``wrfgpu_acoustic_substep``) and its
+    vector-Jacobian product (``wrfgpu_acoustic_substep_vjp``) for fixed stage
+    constants: the reference's acoustic_substep_core (core/acoustic.py:837-1150)
+    on a doubly periodic domain.  ``consts`` maps the names of
+    ``_capi.ACOUSTIC_CONST_FIELDS`` to device tensors (``mu_tend`` may be
+    absent); they are held for the op's lifetime."""
+
+    def __init__(self, nl: dycore.OperationalNamelist, consts: dict, dts: float, device="cuda"):
+        self.lib = _capi.load()
+        self.nl = nl  # holds the metric tensors the metrics struct points into
+        self.params = dycore.step_params(nl)
+        _capi.check(self.lib.wrfgpu_step_params_validate(ctypes.byref(self.params)))
+        self.metrics = _capi.Metrics(*[dycore._ptr(getattr(nl.metrics, n)) for n in dycore.METRIC_ARRAYS])
+        self.consts_t = {n: t.contiguous() for n, t in consts.items() if t is not None}
+        self.consts = _capi.AcousticConsts(*[dycore._ptr(self.consts_t.get(n)) for n in _capi.ACOUSTIC_CONST_FIELDS])
+        n = ctypes.c_size_t(0)
+        _capi.check(self.lib.wrfgpu_acoustic_workspace_size(ctypes.byref(self.params), ctypes.byref(n)))
+        self.workspace = torch.empty(int(n.value), dtype=torch.uint8, device=device)
+        self.dts = float(dts)
+
+    @staticmethod
+    def _work(ts) -> _capi.AcousticWork:
+        return _capi.AcousticWork(*[dycore._ptr(t) for t in ts])
+
+    def forward_(self, xs) -> None:
+        """Advance the 14 work tensors (``_capi.ACOUSTIC_WORK_FIELDS`` order) one substep in place."""
+        w = self._work(xs)
+        st = torch.cuda.current_stream(xs[0].device)
+        _capi.check(self.lib.wrfgpu_acoustic_substep(
+            ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(self.consts), ctypes.byref(w),
+            self.dts, ctypes.c_void_p(self.workspace.data_ptr()), self.workspace.numel(),
+            ctypes.c_void_p(st.cuda_stream)))
+
+    def vjp(self, xs, cot_out, x_out=None):
+        """Cotangents of the 14 inputs ``xs`` from those of the outputs;
+        ``x_out`` (the substep's outputs from ``xs``) is recomputed if None."""
+        cot_in = [torch.empty_like(t) for t in xs]
+        st = torch.cuda.current_stream(xs[0].device)
+        x, co, ci = self._work(xs), self._work(cot_out), self._work(cot_in)
+        xo = ctypes.byref(self._work(x_out)) if x_out is not None else None
+        _capi.check(self.lib.wrfgpu_acoustic_substep_vjp(
+            ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(self.consts), ctypes.byref(x),
+            xo, ctypes.byref(co), ctypes.byref(ci), self.dts, ctypes.c_void_p(self.workspace.data_ptr()),
+            self.workspace.numel(), ctypes.c_void_p(st.cuda_stream)))
+        return cot_in
+
+
+class AcousticSubstep(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, op: AcousticOp, *xs):
+        x_in = [t.contiguous() for t in xs]
+        out = [t.clone() for t in x_in]
+        op.forward_(out)
+        ctx.op = op
+        ctx.save_for_backward(*x_in, *out)
+        return tuple(out)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        saved = ctx.saved_tensors
+        x_in, x_out = saved[:14], saved[14:]
+        co = [g.contiguous() if g is not None else torch.zeros_like(x) for g, x in zip(grads, x_out)]
+        return (None, *ctx.op.vjp(list(x_in), co, list(x_out)))
+
+
+def acoustic_substep(work: dict, op: AcousticOp) -> dict:
+    """One differentiable acoustic small step of the work state ``work``
+    (``_capi.ACOUSTIC_WORK_FIELDS`` names to tensors); gradients flow to every
+    work field through the hand-written VJP kernels."""
+    names = _capi.ACOUSTIC_WORK_FIELDS
+    outs = AcousticSubstep.apply(op, *[work[n] for n in names])
+    return dict(zip(names, outs))

@@ -1,0 +1,397 @@
+// Vector-Jacobian product of one acoustic small step (advance_uv,
+// advance_mu_t, advance_w, calc_p_rho with smdiv memory; the reference's
+// acoustic_substep_core, core/acoustic.py:837-1150) with respect to its
+// evolving work state, the stage constants held fixed.  Doubly periodic
+// domains, no w_damping CFL term.
+//
+// The step is affine in the work state except through the new muts, which
+// enters the denominators of t_2ave, of the ph update and of calc_p_rho; the
+// reverse pass therefore needs the forward output X' = F(X), which the host
+// computes first with the forward kernels.  Three kernels then run the
+// reverse sweep:
+//   * k_adj_column -- one thread per column, levels in reverse order of the
+//                     forward phases: calc_p_rho + smdiv, the ph finish, the
+//                     Thomas back and forward sweeps, the explicit w, the ph
+//                     predictor, the omega-weighted theta / ph fluxes, t_2ave,
+//                     the theta update, the mass update and the ww prefix.
+//                     Leaves the cotangents of the horizontal theta flux
+//                     divergence and of dvdxi per cell for:
+//   * k_adj_faces  -- the u / v face cotangents gathered from the two cells
+//                     each face bounds (the transpose of k_div_h), plus the
+//                     outputs' own;
+//   * k_adj_uv     -- the transpose of advance_uv: every face scatters its
+//                     pressure-gradient cotangent into p, ph, al, muts and
+//                     mudf with atomic adds (edge-clamped pairs alias).
+#pragma once
+#include "dycore_common.cuh"
+#include "acoustic_kernels.cuh"
+
+namespace wg {
+
+struct AcWork {
+  double *u, *v, *w, *ph, *theta_w, *t2ave, *p, *pm1, *al, *ww, *mu, *muts, *muave, *mudf;
+};
+struct AcWorkR {
+  const double *u, *v, *w, *ph, *theta_w, *t2ave, *p, *pm1, *al, *ww, *mu, *muts, *muave, *mudf;
+};
+
+struct AdjScratch {
+  // mass-level: rdnw*al_bar/safe, theta_w' bar, buoyancy bar, wd bar,
+  // theta flux divergence bar and dvdxi bar; face-level: rhs bar, w bar, ww bar
+  double *gal, *gthw, *gbuoy, *gwd, *gtend, *gdv, *grhs, *gws, *gww;
+};
+
+struct AdjColArgs {
+  AcWorkR x1;  // forward output X' = F(X)
+  AcWorkR co;  // cotangent of X'
+  AcWork ci;   // cotangent of X (written)
+  AdjScratch s;
+  const double *alt, *c2a, *cqw, *theta_s, *pt1, *a, *alpha, *gamma, *mut;
+  ColArgs col;  // dts, epssm, top_lid, damp_opt, dampcoef, zdamp, rzdamp
+};
+
+// One thread per column (i, j).
+__global__ void k_adj_column(Grid g, AdjColArgs q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j >= ny) return;
+  const size_t c2d = ix2(j, i, nx);
+  auto M = [&](int k) { return ix3(k, j, i, ny, nx); };
+  const double dts = q.col.dts, eps_p = 1.0 + q.col.epssm, eps_m = 1.0 - q.col.epssm;
+  const double msfty = ld(g.msfty, c2d), minv = ld(g.rmsfty, c2d);
+  const double mut = ld(q.mut, c2d), muts = ld(q.x1.muts, c2d);
+  auto T1 = [&](int k) { return ld(q.theta_s, M(k)) - T0; };
+  auto coef = [&](int k) {  // advance_w's stage-constant c2a*rdnw/mass_h(mut)
+    return ld(q.c2a, M(k)) * ld(g.rdnw, k) / safe12(ld(g.c1h, k) * mut + ld(g.c2h, k));
+  };
+  double g_muts = 0.0, g_muave = 0.0;
+  const AdjScratch &s = q.s;
+
+  // ---- calc_p_rho with smdiv: p' = pp + SMDIV (pp - pm1), pm1' = pp, al' = al ----
+  for (int k = 0; k < nz; ++k) {
+    const size_t c = M(k);
+    const double gp = ld(q.co.p, c);
+    const double g_pp = (1.0 + SMDIV) * gp + ld(q.co.pm1, c);
+    q.ci.pm1[c] = -SMDIV * gp;
+    const double c2a = ld(q.c2a, c), alt = ld(q.alt, c);
+    const double g_al = ld(q.co.al, c) - c2a * g_pp;
+    const double c1 = ld(g.c1h, k);
+    const double mass = c1 * muts + ld(g.c2h, k);
+    const double safe = safe12(mass);
+    const double t1 = T1(k);
+    const double ttr = T0 + t1;
+    const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
+    const double mu_term = c1 * (muts - mut);
+    const double den = safe * sttr;
+    const double thw = ld(q.x1.theta_w, c), al = ld(q.x1.al, c);
+    const double g_mu_term = -(c2a * alt * t1 / den) * g_pp - (alt / safe) * g_al;
+    const double g_safe = -(c2a * alt * (thw - mu_term * t1) / (safe * den)) * g_pp - (al / safe) * g_al;
+    g_muts += c1 * g_mu_term + (fabs(mass) > 1.0e-12 ? c1 * g_safe : 0.0);
+    s.gal[c] = ld(g.rdnw, k) * g_al / safe;
+    s.gthw[c] = ld(q.co.theta_w, c) + (c2a * alt / den) * g_pp;
+    s.gbuoy[c] = 0.0;
+    s.gwd[c] = 0.0;
+  }
+  // ---- ph finish: ph'(f) = rhs(f) + K ws(f) / (c1f muts + c2f), f >= 1; ph'(0) = ph(0) ----
+  const double K = msfty * 0.5 * dts * G * eps_p;
+  const bool do_damp = (q.col.damp_opt == 3 && q.col.dampcoef > 0.0);
+  double dampmag = 0.0, hbot = 0.0;
+  if (do_damp) {
+    dampmag = dts * q.col.dampcoef;
+    hbot = div_rcp(ld(q.pt1, M(nz)), G, RG) - q.col.zdamp;
+  }
+  q.ci.ph[M(0)] = ld(q.co.ph, M(0)) + s.gal[M(0)];
+  q.ci.w[M(0)] = 0.0;  // the surface w is a stage constant
+  s.grhs[M(0)] = 0.0;
+  for (int f = 1; f <= nz; ++f) {
+    const size_t c = M(f);
+    double g_phn = ld(q.co.ph, c) - s.gal[M(f - 1)];
+    if (f <= nz - 1) g_phn += s.gal[c];
+    const double mfs = ld(g.c1f, f) * muts + ld(g.c2f, f);
+    const double ws = ld(q.x1.w, c);
+    s.grhs[c] = g_phn;
+    q.ci.ph[c] = 0.0;
+    double g_ws = ld(q.co.w, c) + (K / mfs) * g_phn;
+    g_muts += -(K * ws * ld(g.c1f, f) / (mfs * mfs)) * g_phn;
+    if (do_damp) {  // ws_out = (ws - dampwt mf w_save) / (1 + dampwt)
+      const double hk = div_rcp(ld(q.pt1, c), G, RG);
+      const double sv = sin(over_zdamp(0.5 * 3.141592653589793 * (hk - hbot), q.col));
+      const double dampwt = (hk >= hbot) ? dampmag * (sv * sv) : 0.0;
+      g_ws = g_ws / (1.0 + dampwt);
+    }
+    s.gws[c] = g_ws;
+  }
+  // ---- Thomas back substitution ws(f) = wf(f) - gamma(f) ws(f+1), reversed ----
+  {
+    double gprev = 0.0;
+    for (int f = 1; f <= nz; ++f) {
+      const size_t c = M(f);
+      double gws = s.gws[c];
+      if (f >= 2) gws = gws - ld(q.gamma, M(f - 1)) * gprev;
+      s.gws[c] = gws;
+      gprev = gws;
+    }
+  }
+  // ---- forward elimination wf(f) = (wn(f) - a(f) wf(f-1)) alpha(f), reversed ----
+  {
+    double gnext = 0.0;
+    for (int f = nz; f >= 1; --f) {
+      const size_t c = M(f);
+      const double gwf = s.gws[c] + gnext;
+      const double alf = ld(q.alpha, c);
+      s.gws[c] = alf * gwf;  // now the cotangent of the explicit w(f)
+      gnext = -ld(q.a, c) * alf * gwf;
+    }
+  }
+  // ---- explicit w: wn = w + dts rw_tend + tA(rhs, ph) + tB(buoy, muave) ----
+  const double c05dg = 0.5 * dts * G;
+  for (int f = 1; f <= nz - 1; ++f) {
+    const size_t c = M(f);
+    const double gwn = s.gws[c];
+    q.ci.w[c] = gwn;
+    const double Q = minv * ld(q.cqw, c) * (c05dg * ld(g.rdn, f)) * gwn;
+    const double cf = coef(f), cm = coef(f - 1);
+    s.grhs[M(f + 1)] += Q * cf * eps_p;
+    s.grhs[c] -= Q * cf * eps_p + Q * cm * eps_p;
+    s.grhs[M(f - 1)] += Q * cm * eps_p;
+    q.ci.ph[M(f + 1)] += Q * cf * eps_m;
+    q.ci.ph[c] -= Q * cf * eps_m + Q * cm * eps_m;
+    q.ci.ph[M(f - 1)] += Q * cm * eps_m;
+    const double R = dts * G * minv * gwn;
+    s.gbuoy[c] += R * ld(g.rdn, f);
+    s.gbuoy[M(f - 1)] -= R * ld(g.rdn, f);
+    g_muave -= R * ld(g.c1f, f);
+  }
+  double gt2a_top = 0.0;
+  if (!q.col.top_lid) {
+    const size_t c = M(nz);
+    const double gwn = s.gws[c];
+    q.ci.w[c] = gwn;
+    const double gT = minv * gwn;
+    const int km1 = nz - 1;
+    const double mhm = safe12(ld(g.c1h, km1) * mut + ld(g.c2h, km1));
+    const double rdnw_t = ld(g.rdnw, km1);
+    const double CA = -0.5 * dts * G / mhm * (rdnw_t * rdnw_t) * 2.0 * ld(q.c2a, M(km1));
+    s.grhs[c] += CA * eps_p * gT;
+    s.grhs[M(nz - 1)] -= CA * eps_p * gT;
+    q.ci.ph[c] += CA * eps_m * gT;
+    q.ci.ph[M(nz - 1)] -= CA * eps_m * gT;
+    gt2a_top = -dts * G * 2.0 * rdnw_t * ld(q.c2a, M(km1)) * ld(q.alt, M(km1)) * gT;
+    g_muave += -dts * G * ld(g.c1f, nz) * gT;
+  } else {
+    q.ci.w[M(nz)] = 0.0;
+    s.grhs[M(nz)] = 0.0;  // a rigid lid's rhs(nz) is zero
+  }
+  // ---- ph predictor rhs(f) = ph(f) + msfty r(f) / mf(f), r = dts (ph_tend + 0.5 g eps_m w) - dts (fnm wd + fnp wd) ----
+  for (int f = 1; f <= nz; ++f) {
+    const size_t c = M(f);
+    const double grhs = s.grhs[c];
+    q.ci.ph[c] += grhs;
+    const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
+    const double S = msfty * grhs / mf;
+    q.ci.w[c] += S * dts * (0.5 * G * eps_m);
+    if (f < nz) {
+      s.gwd[c] -= S * dts * ld(g.fnm, f);
+      s.gwd[M(f - 1)] -= S * dts * ld(g.fnp, f);
+    }
+  }
+  // ---- wd(k) = 0.5 (ww'(k+1) + ww'(k)) rdnw (pt1(k+1) - pt1(k)) ----
+  for (int f = 0; f <= nz; ++f) s.gww[M(f)] = ld(q.co.ww, M(f));
+  for (int k = 0; k < nz; ++k) {
+    const double cw = 0.5 * ld(g.rdnw, k) * (ld(q.pt1, M(k + 1)) - ld(q.pt1, M(k))) * s.gwd[M(k)];
+    s.gww[M(k + 1)] += cw;
+    s.gww[M(k)] += cw;
+  }
+  // ---- t_2ave' = (0.5 (eps_p thw' + eps_m t2ave) + c1h muave' T0) / ((c1h muts' + c2h) (T0 + t1)) ----
+  for (int k = 0; k < nz; ++k) {
+    const size_t c = M(k);
+    double gt2a = ld(q.co.t2ave, c) + ld(q.c2a, c) * ld(q.alt, c) * s.gbuoy[c];
+    if (k == nz - 1) gt2a += gt2a_top;
+    const double c1 = ld(g.c1h, k);
+    const double mass_h = c1 * muts + ld(g.c2h, k);
+    const double D = mass_h * (T0 + T1(k));
+    const double gn = gt2a / D;
+    s.gthw[c] += 0.5 * eps_p * gn;
+    q.ci.t2ave[c] = 0.5 * eps_m * gn;
+    g_muave += c1 * T0 * gn;
+    g_muts += -(ld(q.x1.t2ave, c) / mass_h) * c1 * gt2a;
+  }
+  // ---- theta: thw' = thw + msfty dts t_tend - dts msfty (hdiv + rdnw (wdtn(k+1) - wdtn(k))) ----
+  for (int k = 0; k < nz; ++k) {
+    const size_t c = M(k);
+    const double gthw = s.gthw[c];
+    q.ci.theta_w[c] = gthw;
+    const double gtend = -dts * msfty * gthw;
+    s.gtend[c] = gtend;
+    const double rdnw = ld(g.rdnw, k);
+    if (k + 1 <= nz - 1)
+      s.gww[M(k + 1)] += rdnw * gtend * (ld(g.fnm, k + 1) * T1(k + 1) + ld(g.fnp, k + 1) * T1(k));
+    if (k >= 1) s.gww[c] -= rdnw * gtend * (ld(g.fnm, k) * T1(k) + ld(g.fnp, k) * T1(k - 1));
+  }
+  // ---- mass update: mu_work' = mu_work + dts (dmdt + mu_tend) ----
+  const double gmu = ld(q.co.mu, c2d);
+  const double g_muts_t = ld(q.co.muts, c2d) + g_muts;
+  const double g_muave_t = ld(q.co.muave, c2d) + g_muave;
+  const double g_mwn = gmu + g_muts_t + 0.5 * eps_p * g_muave_t;
+  const double g_mwo = -gmu + 0.5 * eps_m * g_muave_t + g_mwn;
+  q.ci.mu[c2d] = gmu;
+  q.ci.muts[c2d] = g_mwo;
+  q.ci.muave[c2d] = 0.0;
+  double g_dmdt = dts * g_mwn + ld(q.co.mudf, c2d);
+  // ---- ww'(kk) = ww(0) - sum_{m <= kk} inc(m) - ww_1(kk), kk < nz; ww'(nz) = ww(nz) ----
+  {
+    double S = 0.0;
+    s.gdv[M(nz - 1)] = 0.0;
+    for (int m = nz - 1; m >= 1; --m) {
+      S += s.gww[M(m)];
+      const double ginc = -S;
+      const int k = m - 1;
+      g_dmdt += ld(g.dnw, k) * ld(g.c1h, k) * minv * ginc;
+      s.gdv[M(k)] = ld(g.dnw, k) * minv * ginc;
+    }
+    q.ci.ww[M(0)] = S + s.gww[M(0)];
+    for (int f = 1; f < nz; ++f) q.ci.ww[M(f)] = 0.0;
+    q.ci.ww[M(nz)] = s.gww[M(nz)];
+  }
+  // ---- dmdt = sum_k dnw(k) dvdxi(k) ----
+  for (int k = 0; k < nz; ++k) s.gdv[M(k)] += ld(g.dnw, k) * g_dmdt;
+}
+
+struct AdjFaceArgs {
+  const double *gtend, *gdv, *theta_s;
+  const double *co_u, *co_v;
+  double *ci_u, *ci_v;
+};
+
+// The u / v face cotangents (after advance_uv): the outputs' own plus the
+// transpose of the dvdxi and theta-flux divergence of the two cells a face
+// bounds (k_div_h, doubly periodic).  Index space (nx+1) x (ny+1) x nz.
+__global__ void k_adj_faces(Grid g, AdjFaceArgs q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nxu = nx + 1, nyv = ny + 1;
+  if (i > nx || j > ny) return;
+  auto T1 = [&](int jj, int ii) { return ld(q.theta_s, ix3(k, jj, ii, ny, nx)) - T0; };
+  if (j < ny) {
+    const size_t cu = ix3(k, j, i, ny, nxu);
+    double gu = ld(q.co_u, cu);
+    if (i >= 1) {  // east face of cell i-1
+      const int cc = i - 1;
+      const size_t c = ix3(k, j, cc, ny, nx), c2 = ix2(j, cc, nx);
+      const double msftx = ld(g.msftx, c2), msfty = ld(g.msfty, c2);
+      gu += msftx * msfty * g.rdx * ld(q.gdv, c) +
+            msftx * (0.5 * g.rdx) * (T1(j, wrp(cc + 1, nx)) + T1(j, cc)) * ld(q.gtend, c);
+    }
+    if (i <= nx - 1) {  // west face of cell i
+      const size_t c = ix3(k, j, i, ny, nx), c2 = ix2(j, i, nx);
+      const double msftx = ld(g.msftx, c2), msfty = ld(g.msfty, c2);
+      gu -= msftx * msfty * g.rdx * ld(q.gdv, c) +
+            msftx * (0.5 * g.rdx) * (T1(j, i) + T1(j, wrp(i - 1, nx))) * ld(q.gtend, c);
+    }
+    q.ci_u[cu] = gu;
+  }
+  if (i < nx) {
+    const size_t cv = ix3(k, j, i, nyv, nx);
+    double gv = ld(q.co_v, cv);
+    if (j >= 1) {  // north face of cell j-1
+      const int cj = j - 1;
+      const size_t c = ix3(k, cj, i, ny, nx), c2 = ix2(cj, i, nx);
+      const double msftx = ld(g.msftx, c2), msfty = ld(g.msfty, c2);
+      gv += msftx * msfty * g.rdy * ld(q.gdv, c) +
+            msftx * (0.5 * g.rdy) * (T1(wrp(cj + 1, ny), i) + T1(cj, i)) * ld(q.gtend, c);
+    }
+    if (j <= ny - 1) {  // south face of cell j
+      const size_t c = ix3(k, j, i, ny, nx), c2 = ix2(j, i, nx);
+      const double msftx = ld(g.msftx, c2), msfty = ld(g.msfty, c2);
+      gv -= msftx * msfty * g.rdy * ld(q.gdv, c) +
+            msftx * (0.5 * g.rdy) * (T1(j, i) + T1(wrp(j - 1, ny), i)) * ld(q.gtend, c);
+    }
+    q.ci_v[cv] = gv;
+  }
+}
+
+struct AdjUVArgs {
+  const double *gu, *gv;  // total cotangents of the advanced u, v
+  const double *alt, *pb, *php, *cqu, *cqv, *muu, *muv;
+  double *ci_p, *ci_ph, *ci_al, *ci_muts, *ci_mudf;  // accumulated with atomics
+  double dts;
+  int top_lid;
+};
+
+// Transpose of advance_uv's pressure-gradient and divergence-damping terms
+// (the u / v work values themselves pass through with unit weight).  One
+// thread per (i, j, k) of the (nx+1) x (ny+1) face positions.
+__global__ void k_adj_uv(Grid g, AdjUVArgs q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1, nyv = ny + 1;
+  if (i > nx || j > ny) return;
+  const int ic = min(i, nx - 1), jc = min(j, ny - 1);
+  const int oC = jc * nx + ic, oW = jc * nx + max(i - 1, 0), oS = max(j - 1, 0) * nx + ic;
+  const size_t plane = (size_t)ny * nx;
+  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k), rdnw = ld(g.rdnw, k);
+  auto add_p = [&](int lev, int oa, double v) {
+    atomicAdd(q.ci_p + lev * plane + oa, v);
+    atomicAdd(q.ci_p + lev * plane + oC, v);
+  };
+  // dpn_acoustic of the pair sum ps = p(a) + p(C) at faces k+1 (hi) and k (lo)
+  auto add_dpn = [&](int oa, double g_hi, double g_lo) {
+    if (k + 1 < nz) {
+      add_p(k + 1, oa, 0.5 * ld(g.fnm, k + 1) * g_hi);
+      add_p(k, oa, 0.5 * ld(g.fnp, k + 1) * g_hi);
+    } else if (q.top_lid) {
+      add_p(nz - 1, oa, 0.5 * g.cf1 * g_hi);
+      add_p(nz - 2, oa, 0.5 * g.cf2 * g_hi);
+      add_p(nz - 3, oa, 0.5 * g.cf3 * g_hi);
+    }
+    if (k == 0) {
+      add_p(0, oa, 0.5 * g.cf1 * g_lo);
+      add_p(1, oa, 0.5 * g.cf2 * g_lo);
+      add_p(2, oa, 0.5 * g.cf3 * g_lo);
+    } else {
+      add_p(k, oa, 0.5 * ld(g.fnm, k) * g_lo);
+      add_p(k - 1, oa, 0.5 * ld(g.fnp, k) * g_lo);
+    }
+  };
+  // one face's transpose: a = the W (u) or S (v) mass point, C the other
+  auto face = [&](int oa, double gvel, double cq, double msfr, double mass, double rd, double md_coef) {
+    const double Gx = -q.dts * cq * gvel;
+    const double A1 = msfr * 0.5 * rd * mass * Gx;
+    const size_t ka = k * plane + oa, kc = k * plane + oC;
+    atomicAdd(q.ci_ph + (k + 1) * plane + oC, A1);
+    atomicAdd(q.ci_ph + (k + 1) * plane + oa, -A1);
+    atomicAdd(q.ci_ph + kc, A1);
+    atomicAdd(q.ci_ph + ka, -A1);
+    const double gpt = (ld(q.alt, ka) + ld(q.alt, kc)) * A1;
+    atomicAdd(q.ci_p + kc, gpt);
+    atomicAdd(q.ci_p + ka, -gpt);
+    const double gab = (ld(q.pb, kc) - ld(q.pb, ka)) * A1;
+    atomicAdd(q.ci_al + ka, gab);
+    atomicAdd(q.ci_al + kc, gab);
+    const double B = msfr * rd * (ld(q.php, kc) - ld(q.php, ka)) * Gx;
+    add_dpn(oa, rdnw * B, -rdnw * B);
+    const double gm = -0.5 * c1 * B;
+    atomicAdd(q.ci_muts + oa, gm);
+    atomicAdd(q.ci_muts + oC, gm);
+    const double gmd = c1 * md_coef * gvel;
+    atomicAdd(q.ci_mudf + oC, gmd);
+    atomicAdd(q.ci_mudf + oa, -gmd);
+  };
+  if (j < ny) {
+    const int fu = j * nxu + i;
+    const size_t cu = (size_t)k * ny * nxu + fu;
+    const double msfr = div_msf(ld(g.msfux, fu), g.msfuy, g.rmsfuy, fu);
+    face(oW, ld(q.gu, cu), ld(q.cqu, cu), msfr, c1 * ld(q.muu, fu) + c2, g.rdx, -EMDIV * g.dx * ld(g.rmsfuy, fu));
+  }
+  if (i < nx) {
+    const int fv = j * nx + i;
+    const size_t cv = (size_t)k * nyv * nx + fv;
+    const double msfr = div_msf(ld(g.msfvy, fv), g.msfvx, g.rmsfvx, fv);
+    face(oS, ld(q.gv, cv), ld(q.cqv, cv), msfr, c1 * ld(q.muv, fv) + c2, g.rdy, -EMDIV * g.dy * ld(g.rmsfvx, fv));
+  }
+}
+
+}  // namespace wg

@@ -22,6 +22,7 @@
 #include "tiled_faces.cuh"
 #include "tiled_march.cuh"
 #include "adjoint.cuh"
+#include "acoustic_adjoint.cuh"
 #include "bdy_cadence.cuh"
 
 using namespace wg;
@@ -1087,6 +1088,206 @@ int adv_op_check(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const voi
   return wrfgpu_step_params_validate(p);
 }
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// One acoustic substep on caller-held work state and stage constants, and its
+// vector-Jacobian product.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct AcLayout {
+  double *rmsf[6];
+  double *dvdxi, *hdiv;
+  double *x1[14];  // forward output copy (vjp only), in wrfgpu_acoustic_work order
+  AdjScratch s;
+};
+
+// element counts of the work arrays in wrfgpu_acoustic_work order
+void ac_counts(const Dims &d, size_t n[14]) {
+  const size_t c[14] = {d.u, d.v, d.w, d.w, d.m, d.m, d.m, d.m, d.m, d.w, d.s2, d.s2, d.s2, d.s2};
+  for (int q = 0; q < 14; ++q) n[q] = c[q];
+}
+
+void ac_carve(const wrfgpu_step_params &p, Carver &cv, AcLayout &L) {
+  const Dims d = dims_of(p);
+  L.rmsf[0] = cv.take(d.s2); L.rmsf[1] = cv.take(d.s2);
+  L.rmsf[2] = cv.take(d.su); L.rmsf[3] = cv.take(d.su);
+  L.rmsf[4] = cv.take(d.sv); L.rmsf[5] = cv.take(d.sv);
+  L.dvdxi = cv.take(d.m); L.hdiv = cv.take(d.m);
+  size_t n[14];
+  ac_counts(d, n);
+  for (int q = 0; q < 14; ++q) L.x1[q] = cv.take(n[q]);
+  L.s.gal = cv.take(d.m); L.s.gthw = cv.take(d.m); L.s.gbuoy = cv.take(d.m); L.s.gwd = cv.take(d.m);
+  L.s.gtend = cv.take(d.m); L.s.gdv = cv.take(d.m);
+  L.s.grhs = cv.take(d.w); L.s.gws = cv.take(d.w); L.s.gww = cv.take(d.w);
+}
+
+double *const *work_ptrs(const wrfgpu_acoustic_work &x, double *out[14]) {
+  double *v[14] = {x.u, x.v, x.w, x.ph, x.theta_w, x.t_2ave, x.p, x.pm1, x.al, x.ww, x.mu, x.muts, x.muave, x.mudf};
+  for (int q = 0; q < 14; ++q) out[q] = v[q];
+  return out;
+}
+
+int ac_check(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const wrfgpu_acoustic_consts *c, size_t ws_bytes,
+             const void *ws) {
+  if (p == nullptr || m == nullptr || c == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/metrics/consts is NULL");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  if (p->run_boundary)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "the standalone acoustic substep covers doubly periodic domains only");
+  if (p->w_damping != 0)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "the standalone acoustic substep has no w_damping CFL term");
+  const double *need[] = {c->u_tend, c->v_tend, c->t_tend, c->rw_tend, c->ph_tend, c->alt, c->pb, c->c2a, c->cqu,
+                          c->cqv, c->cqw, c->php, c->pt1, c->a, c->alpha, c->gamma, c->ww_1, c->mut, c->muu,
+                          c->muv, c->u_1, c->v_1, c->w_save, c->theta, c->phb0};
+  for (const double *q : need)
+    if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "a stage constant pointer is NULL (only mu_tend may be)");
+  size_t need_bytes = 0;
+  wrfgpu_acoustic_workspace_size(p, &need_bytes);
+  if (ws == nullptr || ws_bytes < need_bytes)
+    return fail(WRFGPU_ERR_WORKSPACE, "workspace is NULL or smaller than wrfgpu_acoustic_workspace_size()");
+  return WRFGPU_OK;
+}
+
+// Launch one forward substep over the work arrays w[14] (in place).
+int ac_forward(const wrfgpu_step_params &p, const Grid &g, const wrfgpu_acoustic_consts &c, double *const w[14],
+               double dts, const AcLayout &L, cudaStream_t stream) {
+  Acoustic A{};
+  A.u = w[0]; A.v = w[1]; A.w = w[2]; A.ph = w[3]; A.theta_w = w[4]; A.t2ave = w[5]; A.p = w[6]; A.pm1 = w[7];
+  A.al = w[8]; A.ww = w[9]; A.mu = w[10]; A.muts = w[11]; A.muave = w[12]; A.mudf = w[13];
+  A.u_tend = c.u_tend; A.v_tend = c.v_tend; A.t_tend = c.t_tend; A.rw_tend = c.rw_tend; A.ph_tend = c.ph_tend;
+  A.alt = c.alt; A.pb = c.pb; A.c2a = c.c2a; A.cqu = c.cqu; A.cqv = c.cqv; A.cqw = c.cqw; A.php = c.php;
+  A.pt1 = c.pt1; A.a = c.a; A.alpha = c.alpha; A.gamma = c.gamma; A.ww_1 = c.ww_1;
+  A.mut = c.mut; A.muu = c.muu; A.muv = c.muv; A.muus = c.muu; A.muvs = c.muv; A.mu_tend = c.mu_tend;
+  A.u_1 = c.u_1; A.v_1 = c.v_1; A.w_save = c.w_save; A.theta_s = c.theta; A.phb0 = c.phb0;
+  BdyArgs ba{};
+  ColArgs ca{};
+  ca.dts = dts; ca.epssm = p.epssm; ca.specified = 0; ca.top_lid = p.top_lid; ca.w_damping = 0;
+  ca.damp_opt = p.damp_opt; ca.dampcoef = p.dampcoef; ca.zdamp = p.zdamp;
+  ca.rzdamp = (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  k_advance_uv<<<grd(nx + 1, ny + 1, (nz + UV_KC - 1) / UV_KC), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
+  if (int rc = check_launch("k_advance_uv")) return rc;
+  k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, 0, L.dvdxi, L.hdiv);
+  if (int rc = check_launch("k_div_h")) return rc;
+  const size_t smem = column_tiled_smem_bytes(nz, COL_TX);
+  auto kColumn = k_column_tiled<COL_TX, COL_TY>;
+  if (cudaFuncSetAttribute(kColumn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_column_tiled (nz too large)");
+  kColumn<<<dim3((nx + COL_TX - 1) / COL_TX, ny, 1), dim3(COL_TX, COL_TY, 1), smem, stream>>>(g, A, ca, L.dvdxi,
+                                                                                             L.hdiv);
+  return check_launch("k_column_tiled");
+}
+
+Grid ac_grid(const wrfgpu_step_params &p, const wrfgpu_metrics &m, const AcLayout &L) {
+  Grid g = make_grid(p, m, nullptr);
+  g.rmsftx = L.rmsf[0]; g.rmsfty = L.rmsf[1]; g.rmsfux = L.rmsf[2]; g.rmsfuy = L.rmsf[3];
+  g.rmsfvx = L.rmsf[4]; g.rmsfvy = L.rmsf[5];
+  return g;
+}
+
+}  // namespace
+
+extern "C" int wrfgpu_acoustic_workspace_size(const wrfgpu_step_params *p, size_t *bytes) {
+  if (p == nullptr || bytes == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/bytes is NULL");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  Carver cv{nullptr, 0, 0, true};
+  AcLayout L;
+  ac_carve(*p, cv, L);
+  *bytes = cv.off + 256;
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_acoustic_substep(const wrfgpu_step_params *p, const wrfgpu_metrics *m,
+                                       const wrfgpu_acoustic_consts *c, wrfgpu_acoustic_work *x, double dts,
+                                       void *workspace, size_t workspace_bytes, cudaStream_t stream) {
+  int rc = ac_check(p, m, c, workspace_bytes, workspace);
+  if (rc) return rc;
+  if (x == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "work state is NULL");
+  double *w[14];
+  work_ptrs(*x, w);
+  for (double *q : w)
+    if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "a work state pointer is NULL");
+  Carver cv{reinterpret_cast<char *>(workspace), 0, workspace_bytes, false};
+  AcLayout L;
+  ac_carve(*p, cv, L);
+  Grid g = ac_grid(*p, *m, L);
+  k_recip_msf<<<grd(p->nx + 1, p->ny + 1, 1), blk2(), 0, stream>>>(g, L.rmsf[0], L.rmsf[1], L.rmsf[2], L.rmsf[3],
+                                                                 L.rmsf[4], L.rmsf[5]);
+  if ((rc = check_launch("k_recip_msf"))) return rc;
+  if ((rc = ac_forward(*p, g, *c, w, dts, L, stream))) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wrfgpu_metrics *m,
+                                           const wrfgpu_acoustic_consts *c, const wrfgpu_acoustic_work *x,
+                                           const wrfgpu_acoustic_work *x_out, const wrfgpu_acoustic_work *cot_out,
+                                           wrfgpu_acoustic_work *cot_in, double dts, void *workspace,
+                                           size_t workspace_bytes, cudaStream_t stream) {
+  int rc = ac_check(p, m, c, workspace_bytes, workspace);
+  if (rc) return rc;
+  if (x == nullptr || cot_out == nullptr || cot_in == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "work state or cotangent is NULL");
+  double *xin[14], *co[14], *ci[14];
+  work_ptrs(*x, xin);
+  work_ptrs(*cot_out, co);
+  work_ptrs(*cot_in, ci);
+  for (int q = 0; q < 14; ++q)
+    if (xin[q] == nullptr || co[q] == nullptr || ci[q] == nullptr)
+      return fail(WRFGPU_ERR_NULL_POINTER, "a work state or cotangent pointer is NULL");
+  const Dims d = dims_of(*p);
+  Carver cv{reinterpret_cast<char *>(workspace), 0, workspace_bytes, false};
+  AcLayout L;
+  ac_carve(*p, cv, L);
+  Grid g = ac_grid(*p, *m, L);
+  const int nx = p->nx, ny = p->ny, nz = p->nz;
+  k_recip_msf<<<grd(nx + 1, ny + 1, 1), blk2(), 0, stream>>>(g, L.rmsf[0], L.rmsf[1], L.rmsf[2], L.rmsf[3],
+                                                           L.rmsf[4], L.rmsf[5]);
+  if ((rc = check_launch("k_recip_msf"))) return rc;
+  // forward output X' = F(X): the caller's, or recomputed into the workspace
+  size_t n[14];
+  ac_counts(d, n);
+  double *x1[14];
+  if (x_out != nullptr) {
+    work_ptrs(*x_out, x1);
+    for (double *q : x1)
+      if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "an x_out pointer is NULL");
+  } else {
+    for (int q = 0; q < 14; ++q) {
+      x1[q] = L.x1[q];
+      if (cudaMemcpyAsync(L.x1[q], xin[q], n[q] * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+        return fail(WRFGPU_ERR_CUDA, "work state copy failed");
+    }
+    if ((rc = ac_forward(*p, g, *c, L.x1, dts, L, stream))) return rc;
+  }
+  // the atomically accumulated cotangents start from zero
+  for (int q : {6, 8, 13})
+    if (cudaMemsetAsync(ci[q], 0, n[q] * sizeof(double), stream) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "cotangent clear failed");
+  AdjColArgs a{};
+  a.x1 = AcWorkR{x1[0], x1[1], x1[2], x1[3], x1[4], x1[5], x1[6], x1[7], x1[8], x1[9], x1[10], x1[11], x1[12], x1[13]};
+  a.co = AcWorkR{co[0], co[1], co[2], co[3], co[4], co[5], co[6], co[7], co[8], co[9], co[10], co[11], co[12], co[13]};
+  a.ci = AcWork{ci[0], ci[1], ci[2], ci[3], ci[4], ci[5], ci[6], ci[7], ci[8], ci[9], ci[10], ci[11], ci[12], ci[13]};
+  a.s = L.s;
+  a.alt = c->alt; a.c2a = c->c2a; a.cqw = c->cqw; a.theta_s = c->theta; a.pt1 = c->pt1;
+  a.a = c->a; a.alpha = c->alpha; a.gamma = c->gamma; a.mut = c->mut;
+  a.col.dts = dts; a.col.epssm = p->epssm; a.col.top_lid = p->top_lid; a.col.damp_opt = p->damp_opt;
+  a.col.dampcoef = p->dampcoef; a.col.zdamp = p->zdamp;
+  a.col.rzdamp = (p->zdamp != 0.0 && std::isfinite(1.0 / p->zdamp)) ? 1.0 / p->zdamp : 0.0;
+  k_adj_column<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, a);
+  if ((rc = check_launch("k_adj_column"))) return rc;
+  AdjFaceArgs fa{L.s.gtend, L.s.gdv, c->theta, co[0], co[1], ci[0], ci[1]};
+  k_adj_faces<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, fa);
+  if ((rc = check_launch("k_adj_faces"))) return rc;
+  AdjUVArgs ua{ci[0], ci[1], c->alt, c->pb, c->php, c->cqu, c->cqv, c->muu, c->muv,
+               ci[6], ci[3], ci[8], ci[11], ci[13], dts, p->top_lid};
+  k_adj_uv<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, ua);
+  if ((rc = check_launch("k_adj_uv"))) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
 
 extern "C" int wrfgpu_scalar_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
                                        const double *ru, const double *rv, const double *rom, double *tend,
