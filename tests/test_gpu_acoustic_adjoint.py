@@ -216,3 +216,28 @@ def test_vjp_cost_relative_to_forward(cuda_ready):
     print(f"acoustic substep at 433x433x50: forward {t_fwd:.3f} ms, VJP {t_vjp:.3f} ms ({t_vjp / t_fwd:.2f}x) "
           f"recomputing the forward output, {t_st:.3f} ms ({t_st / t_fwd:.2f}x) from the stored one")
     assert t_st <= 3.0 * t_fwd
+
+
+def test_checkpointed_loop_matches_chained_substeps(cuda_ready):
+    case = _case("lid_damped")
+    nl, a, dts, s = _stage(case, 3)
+    op = _op(case, a, s, dts)
+    base = {cn: torch.as_tensor(getattr(a, on).copy(), device="cuda") for cn, on in WORK.items()}
+
+    def loss(y):
+        return (y["w"] ** 2).sum() + 1.0e-4 * (y["theta_w"] ** 2).sum() + 1.0e-2 * (y["p"] ** 2).sum()
+
+    x1 = {n: t.clone().requires_grad_(True) for n, t in base.items()}
+    y1 = x1
+    for _ in range(3):
+        y1 = adjoint.acoustic_substep(y1, op)
+    loss(y1).backward()
+    x2 = {n: t.clone().requires_grad_(True) for n, t in base.items()}
+    y2 = adjoint.acoustic_loop(x2, op, 3)
+    for n in y1:
+        assert torch.equal(y1[n], y2[n]), n
+    loss(y2).backward()
+    for n in x1:
+        g1, g2 = x1[n].grad, x2[n].grad
+        scale = float(g1.abs().max()) or 1.0
+        assert float((g1 - g2).abs().max()) <= 1.0e-12 * scale, n

@@ -1,12 +1,16 @@
-"""Differentiable scalar advection: the CUDA h5/v3 flux-form operator with its
-hand-written adjoint behind ``torch.autograd.Function``.
+"""Hand-written adjoints behind ``torch.autograd.Function``.
 
-``scalar_advection(q, ru, rv, rom, namelist)`` returns the advective
-tendency of ``q`` (``advect_scalar_flux``, dynamics/flux_advection.py:482-568,
-doubly periodic) for fixed transport velocities; ``backward`` applies the
-adjoint kernel (``wrfgpu_scalar_advection_adjoint``) to the incoming
-gradient, so gradients flow to ``q`` (the velocities are treated as
-constants: their gradient is not built).
+* ``scalar_advection(q, ru, rv, rom, namelist)`` returns the advective
+  tendency of ``q`` (``advect_scalar_flux``, dynamics/flux_advection.py:482-568,
+  doubly periodic) for fixed transport velocities; ``backward`` applies the
+  adjoint kernel (``wrfgpu_scalar_advection_adjoint``) to the incoming
+  gradient, so gradients flow to ``q`` (the velocities are treated as
+  constants: their gradient is not built).
+* ``acoustic_substep(work, op)`` / ``acoustic_loop(work, op, nsub)``: one or
+  ``nsub`` acoustic small steps (acoustic_substep_core, core/acoustic.py:
+  837-1150) of the evolving work state for fixed stage constants, with the
+  VJP kernels of ``wrfgpu_acoustic_substep_vjp`` in the backward pass; the
+  loop keeps one checkpoint and recomputes its substeps.
 """
 
 from __future__ import annotations
@@ -128,6 +132,44 @@ class AcousticSubstep(torch.autograd.Function):
         x_in, x_out = saved[:14], saved[14:]
         co = [g.contiguous() if g is not None else torch.zeros_like(x) for g, x in zip(grads, x_out)]
         return (None, *ctx.op.vjp(list(x_in), co, list(x_out)))
+
+
+class AcousticLoop(torch.autograd.Function):
+    """``nsub`` acoustic substeps behind one checkpoint: the forward keeps only
+    the loop's input state; the backward recomputes the substep states from it
+    (one forward pass) and applies the substep VJPs in reverse, each with its
+    stored forward output."""
+
+    @staticmethod
+    def forward(ctx, op: AcousticOp, nsub: int, *xs):
+        x0 = [t.contiguous() for t in xs]
+        cur = [t.clone() for t in x0]
+        for _ in range(nsub):
+            op.forward_(cur)
+        ctx.op, ctx.nsub = op, nsub
+        ctx.save_for_backward(*x0)
+        return tuple(cur)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        x0 = list(ctx.saved_tensors)
+        states = [x0]
+        for _ in range(ctx.nsub):
+            nxt = [t.clone() for t in states[-1]]
+            ctx.op.forward_(nxt)
+            states.append(nxt)
+        co = [g.contiguous() if g is not None else torch.zeros_like(x) for g, x in zip(grads, states[-1])]
+        for n in range(ctx.nsub - 1, -1, -1):
+            co = ctx.op.vjp(states[n], co, states[n + 1])
+        return (None, None, *co)
+
+
+def acoustic_loop(work: dict, op: AcousticOp, nsub: int) -> dict:
+    """``nsub`` differentiable acoustic small steps with the loop input as the
+    only stored state (substeps recomputed in the backward pass)."""
+    names = _capi.ACOUSTIC_WORK_FIELDS
+    outs = AcousticLoop.apply(op, int(nsub), *[work[n] for n in names])
+    return dict(zip(names, outs))
 
 
 def acoustic_substep(work: dict, op: AcousticOp) -> dict:

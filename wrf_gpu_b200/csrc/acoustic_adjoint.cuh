@@ -36,9 +36,9 @@ struct AcWorkR {
 };
 
 struct AdjScratch {
-  // mass-level: rdnw*al_bar/safe, theta_w' bar, buoyancy bar, wd bar,
-  // theta flux divergence bar and dvdxi bar; face-level: rhs bar, w bar, ww bar
-  double *gal, *gthw, *gbuoy, *gwd, *gtend, *gdv, *grhs, *gws, *gww;
+  // mass-level: theta_w' bar (calc_p_rho part), theta flux divergence bar and
+  // dvdxi bar; face-level: rhs bar (ph finish part), w bar, ww bar
+  double *gthw, *gtend, *gdv, *grhs, *gws, *gww;
 };
 
 struct AdjColArgs {
@@ -50,14 +50,23 @@ struct AdjColArgs {
   ColArgs col;  // dts, epssm, top_lid, damp_opt, dampcoef, zdamp, rzdamp
 };
 
-// One thread per column (i, j).
+// One thread per column (i, j), three passes over the levels:
+//   1 (up)   calc_p_rho + smdiv, the ph finish, the Thomas back substitution;
+//   2 (down) the Thomas forward elimination, the explicit w, the ph predictor
+//            one face behind it, the omega-weighted wd, t_2ave and theta;
+//   3        the mass update, the ww prefix and the column sum of dvdxi.
+// Pass 2 keeps the cotangents still collecting contributions (rhs, ph and w
+// of faces m+1 and m, the buoyancy of level m, wd of level m+1) in registers
+// and finishes each as soon as its last contributor has run.
 __global__ void k_adj_column(Grid g, AdjColArgs q) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   if (i >= nx || j >= ny) return;
   const size_t c2d = ix2(j, i, nx);
-  auto M = [&](int k) { return ix3(k, j, i, ny, nx); };
+  const size_t plane = (size_t)ny * nx;
+  const size_t base = (size_t)j * nx + i;
+  auto M = [&](int k) { return (size_t)k * plane + base; };
   const double dts = q.col.dts, eps_p = 1.0 + q.col.epssm, eps_m = 1.0 - q.col.epssm;
   const double msfty = ld(g.msfty, c2d), minv = ld(g.rmsfty, c2d);
   const double mut = ld(q.mut, c2d), muts = ld(q.x1.muts, c2d);
@@ -65,35 +74,15 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
   auto coef = [&](int k) {  // advance_w's stage-constant c2a*rdnw/mass_h(mut)
     return ld(q.c2a, M(k)) * ld(g.rdnw, k) / safe12(ld(g.c1h, k) * mut + ld(g.c2h, k));
   };
+  double *__restrict__ s_thw = q.s.gthw;
+  double *__restrict__ s_rhs = q.s.grhs;
+  double *__restrict__ s_ws = q.s.gws;
+  double *__restrict__ s_ww = q.s.gww;
+  double *__restrict__ s_tend = q.s.gtend;
+  double *__restrict__ s_dv = q.s.gdv;
   double g_muts = 0.0, g_muave = 0.0;
-  const AdjScratch &s = q.s;
 
-  // ---- calc_p_rho with smdiv: p' = pp + SMDIV (pp - pm1), pm1' = pp, al' = al ----
-  for (int k = 0; k < nz; ++k) {
-    const size_t c = M(k);
-    const double gp = ld(q.co.p, c);
-    const double g_pp = (1.0 + SMDIV) * gp + ld(q.co.pm1, c);
-    q.ci.pm1[c] = -SMDIV * gp;
-    const double c2a = ld(q.c2a, c), alt = ld(q.alt, c);
-    const double g_al = ld(q.co.al, c) - c2a * g_pp;
-    const double c1 = ld(g.c1h, k);
-    const double mass = c1 * muts + ld(g.c2h, k);
-    const double safe = safe12(mass);
-    const double t1 = T1(k);
-    const double ttr = T0 + t1;
-    const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
-    const double mu_term = c1 * (muts - mut);
-    const double den = safe * sttr;
-    const double thw = ld(q.x1.theta_w, c), al = ld(q.x1.al, c);
-    const double g_mu_term = -(c2a * alt * t1 / den) * g_pp - (alt / safe) * g_al;
-    const double g_safe = -(c2a * alt * (thw - mu_term * t1) / (safe * den)) * g_pp - (al / safe) * g_al;
-    g_muts += c1 * g_mu_term + (fabs(mass) > 1.0e-12 ? c1 * g_safe : 0.0);
-    s.gal[c] = ld(g.rdnw, k) * g_al / safe;
-    s.gthw[c] = ld(q.co.theta_w, c) + (c2a * alt / den) * g_pp;
-    s.gbuoy[c] = 0.0;
-    s.gwd[c] = 0.0;
-  }
-  // ---- ph finish: ph'(f) = rhs(f) + K ws(f) / (c1f muts + c2f), f >= 1; ph'(0) = ph(0) ----
+  // ================= pass 1 (faces f = 0..nz, level k = f) =================
   const double K = msfty * 0.5 * dts * G * eps_p;
   const bool do_damp = (q.col.damp_opt == 3 && q.col.dampcoef > 0.0);
   double dampmag = 0.0, hbot = 0.0;
@@ -101,161 +90,193 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     dampmag = dts * q.col.dampcoef;
     hbot = div_rcp(ld(q.pt1, M(nz)), G, RG) - q.col.zdamp;
   }
-  q.ci.ph[M(0)] = ld(q.co.ph, M(0)) + s.gal[M(0)];
-  q.ci.w[M(0)] = 0.0;  // the surface w is a stage constant
-  s.grhs[M(0)] = 0.0;
-  for (int f = 1; f <= nz; ++f) {
-    const size_t c = M(f);
-    double g_phn = ld(q.co.ph, c) - s.gal[M(f - 1)];
-    if (f <= nz - 1) g_phn += s.gal[c];
-    const double mfs = ld(g.c1f, f) * muts + ld(g.c2f, f);
-    const double ws = ld(q.x1.w, c);
-    s.grhs[c] = g_phn;
-    q.ci.ph[c] = 0.0;
-    double g_ws = ld(q.co.w, c) + (K / mfs) * g_phn;
-    g_muts += -(K * ws * ld(g.c1f, f) / (mfs * mfs)) * g_phn;
-    if (do_damp) {  // ws_out = (ws - dampwt mf w_save) / (1 + dampwt)
-      const double hk = div_rcp(ld(q.pt1, c), G, RG);
-      const double sv = sin(over_zdamp(0.5 * 3.141592653589793 * (hk - hbot), q.col));
-      const double dampwt = (hk >= hbot) ? dampmag * (sv * sv) : 0.0;
-      g_ws = g_ws / (1.0 + dampwt);
-    }
-    s.gws[c] = g_ws;
-  }
-  // ---- Thomas back substitution ws(f) = wf(f) - gamma(f) ws(f+1), reversed ----
-  {
-    double gprev = 0.0;
-    for (int f = 1; f <= nz; ++f) {
-      const size_t c = M(f);
-      double gws = s.gws[c];
-      if (f >= 2) gws = gws - ld(q.gamma, M(f - 1)) * gprev;
-      s.gws[c] = gws;
-      gprev = gws;
-    }
-  }
-  // ---- forward elimination wf(f) = (wn(f) - a(f) wf(f-1)) alpha(f), reversed ----
-  {
-    double gnext = 0.0;
-    for (int f = nz; f >= 1; --f) {
-      const size_t c = M(f);
-      const double gwf = s.gws[c] + gnext;
-      const double alf = ld(q.alpha, c);
-      s.gws[c] = alf * gwf;  // now the cotangent of the explicit w(f)
-      gnext = -ld(q.a, c) * alf * gwf;
-    }
-  }
-  // ---- explicit w: wn = w + dts rw_tend + tA(rhs, ph) + tB(buoy, muave) ----
-  const double c05dg = 0.5 * dts * G;
-  for (int f = 1; f <= nz - 1; ++f) {
-    const size_t c = M(f);
-    const double gwn = s.gws[c];
-    q.ci.w[c] = gwn;
-    const double Q = minv * ld(q.cqw, c) * (c05dg * ld(g.rdn, f)) * gwn;
-    const double cf = coef(f), cm = coef(f - 1);
-    s.grhs[M(f + 1)] += Q * cf * eps_p;
-    s.grhs[c] -= Q * cf * eps_p + Q * cm * eps_p;
-    s.grhs[M(f - 1)] += Q * cm * eps_p;
-    q.ci.ph[M(f + 1)] += Q * cf * eps_m;
-    q.ci.ph[c] -= Q * cf * eps_m + Q * cm * eps_m;
-    q.ci.ph[M(f - 1)] += Q * cm * eps_m;
-    const double R = dts * G * minv * gwn;
-    s.gbuoy[c] += R * ld(g.rdn, f);
-    s.gbuoy[M(f - 1)] -= R * ld(g.rdn, f);
-    g_muave -= R * ld(g.c1f, f);
-  }
-  double gt2a_top = 0.0;
-  if (!q.col.top_lid) {
-    const size_t c = M(nz);
-    const double gwn = s.gws[c];
-    q.ci.w[c] = gwn;
-    const double gT = minv * gwn;
-    const int km1 = nz - 1;
-    const double mhm = safe12(ld(g.c1h, km1) * mut + ld(g.c2h, km1));
-    const double rdnw_t = ld(g.rdnw, km1);
-    const double CA = -0.5 * dts * G / mhm * (rdnw_t * rdnw_t) * 2.0 * ld(q.c2a, M(km1));
-    s.grhs[c] += CA * eps_p * gT;
-    s.grhs[M(nz - 1)] -= CA * eps_p * gT;
-    q.ci.ph[c] += CA * eps_m * gT;
-    q.ci.ph[M(nz - 1)] -= CA * eps_m * gT;
-    gt2a_top = -dts * G * 2.0 * rdnw_t * ld(q.c2a, M(km1)) * ld(q.alt, M(km1)) * gT;
-    g_muave += -dts * G * ld(g.c1f, nz) * gT;
-  } else {
-    q.ci.w[M(nz)] = 0.0;
-    s.grhs[M(nz)] = 0.0;  // a rigid lid's rhs(nz) is zero
-  }
-  // ---- ph predictor rhs(f) = ph(f) + msfty r(f) / mf(f), r = dts (ph_tend + 0.5 g eps_m w) - dts (fnm wd + fnp wd) ----
-  for (int f = 1; f <= nz; ++f) {
-    const size_t c = M(f);
-    const double grhs = s.grhs[c];
-    q.ci.ph[c] += grhs;
-    const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
-    const double S = msfty * grhs / mf;
-    q.ci.w[c] += S * dts * (0.5 * G * eps_m);
+  double gal_prev = 0.0, gws_prev = 0.0, ph0 = 0.0;
+  for (int f = 0; f <= nz; ++f) {
+    // calc_p_rho with smdiv at level f: p' = pp + SMDIV (pp - pm1), pm1' = pp, al' = al
+    double gal = 0.0;
     if (f < nz) {
-      s.gwd[c] -= S * dts * ld(g.fnm, f);
-      s.gwd[M(f - 1)] -= S * dts * ld(g.fnp, f);
+      const size_t c = M(f);
+      const double gp = ld(q.co.p, c);
+      const double g_pp = (1.0 + SMDIV) * gp + ld(q.co.pm1, c);
+      q.ci.pm1[c] = -SMDIV * gp;
+      const double c2a = ld(q.c2a, c), alt = ld(q.alt, c);
+      const double g_al = ld(q.co.al, c) - c2a * g_pp;
+      const double c1 = ld(g.c1h, f);
+      const double mass = c1 * muts + ld(g.c2h, f);
+      const double safe = safe12(mass);
+      const double t1 = T1(f);
+      const double ttr = T0 + t1;
+      const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
+      const double mu_term = c1 * (muts - mut);
+      const double den = safe * sttr;
+      const double thw = ld(q.x1.theta_w, c), al = ld(q.x1.al, c);
+      const double g_mu_term = -(c2a * alt * t1 / den) * g_pp - (alt / safe) * g_al;
+      const double g_safe = -(c2a * alt * (thw - mu_term * t1) / (safe * den)) * g_pp - (al / safe) * g_al;
+      g_muts += c1 * g_mu_term + (fabs(mass) > 1.0e-12 ? c1 * g_safe : 0.0);
+      gal = ld(g.rdnw, f) * g_al / safe;  // al(f) = ... - rdnw (ph'(f+1) - ph'(f)) / safe
+      s_thw[c] = ld(q.co.theta_w, c) + (c2a * alt / den) * g_pp;
     }
+    const size_t c = M(f);
+    s_ww[c] = ld(q.co.ww, c);
+    if (f == 0) {
+      ph0 = ld(q.co.ph, c) + gal;  // ph'(0) = ph(0)
+    } else {
+      // ph finish: ph'(f) = rhs(f) + K ws(f) / (c1f muts + c2f)
+      const double g_phn = ld(q.co.ph, c) - gal_prev + gal;
+      const double mfs = ld(g.c1f, f) * muts + ld(g.c2f, f);
+      s_rhs[c] = g_phn;
+      double g_ws = ld(q.co.w, c) + (K / mfs) * g_phn;
+      g_muts += -(K * ld(q.x1.w, c) * ld(g.c1f, f) / (mfs * mfs)) * g_phn;
+      if (do_damp) {  // ws_out = (ws - dampwt mf w_save) / (1 + dampwt)
+        const double hk = div_rcp(ld(q.pt1, c), G, RG);
+        const double sv = sin(over_zdamp(0.5 * 3.141592653589793 * (hk - hbot), q.col));
+        const double dampwt = (hk >= hbot) ? dampmag * (sv * sv) : 0.0;
+        g_ws = g_ws / (1.0 + dampwt);
+      }
+      // Thomas back substitution ws(f-1) = wf(f-1) - gamma(f-1) ws(f), reversed
+      if (f >= 2) g_ws = g_ws - ld(q.gamma, M(f - 1)) * gws_prev;
+      s_ws[c] = g_ws;
+      gws_prev = g_ws;
+    }
+    gal_prev = gal;
   }
-  // ---- wd(k) = 0.5 (ww'(k+1) + ww'(k)) rdnw (pt1(k+1) - pt1(k)) ----
-  for (int f = 0; f <= nz; ++f) s.gww[M(f)] = ld(q.co.ww, M(f));
-  for (int k = 0; k < nz; ++k) {
-    const double cw = 0.5 * ld(g.rdnw, k) * (ld(q.pt1, M(k + 1)) - ld(q.pt1, M(k))) * s.gwd[M(k)];
-    s.gww[M(k + 1)] += cw;
-    s.gww[M(k)] += cw;
-  }
-  // ---- t_2ave' = (0.5 (eps_p thw' + eps_m t2ave) + c1h muave' T0) / ((c1h muts' + c2h) (T0 + t1)) ----
-  for (int k = 0; k < nz; ++k) {
+
+  // ================= pass 2 (faces m = nz..1) =================
+  const double c05dg = 0.5 * dts * G;
+  const double wfac = dts * (0.5 * G * eps_m);
+  // the ph predictor of face f: rhs(f) = ph(f) + msfty r / mf, r = dts (ph_tend + 0.5 g eps_m w)
+  // - dts (fnm wd(f) + fnp wd(f-1)); returns the wd(f) (fnm) and wd(f-1) (fnp) cotangent parts
+  auto predictor = [&](int f, double grhs, double &gph, double &gw, double &gwd_f, double &gwd_fm1) {
+    if (f == nz && q.col.top_lid) grhs = 0.0;  // a rigid lid's rhs(nz) is zero
+    gph += grhs;
+    const double S = msfty * grhs / (ld(g.c1f, f) * mut + ld(g.c2f, f));
+    gw += S * wfac;
+    gwd_f = (f < nz) ? -(S * dts * ld(g.fnm, f)) : 0.0;
+    gwd_fm1 = (f < nz) ? -(S * dts * ld(g.fnp, f)) : 0.0;
+  };
+  // wd(k) = 0.5 (ww'(k+1) + ww'(k)) rdnw (pt1(k+1) - pt1(k))
+  auto wd_rev = [&](int k, double gwd) {
+    const double cw = 0.5 * ld(g.rdnw, k) * (ld(q.pt1, M(k + 1)) - ld(q.pt1, M(k))) * gwd;
+    s_ww[M(k + 1)] += cw;
+    s_ww[M(k)] += cw;
+  };
+  // t_2ave' and theta at level k (after its buoyancy cotangent is complete)
+  auto t2a_theta = [&](int k, double gbuoy, double gt2a_extra) {
     const size_t c = M(k);
-    double gt2a = ld(q.co.t2ave, c) + ld(q.c2a, c) * ld(q.alt, c) * s.gbuoy[c];
-    if (k == nz - 1) gt2a += gt2a_top;
+    const double gt2a = ld(q.co.t2ave, c) + ld(q.c2a, c) * ld(q.alt, c) * gbuoy + gt2a_extra;
     const double c1 = ld(g.c1h, k);
     const double mass_h = c1 * muts + ld(g.c2h, k);
-    const double D = mass_h * (T0 + T1(k));
-    const double gn = gt2a / D;
-    s.gthw[c] += 0.5 * eps_p * gn;
+    const double t1 = T1(k);
+    const double gn = gt2a / (mass_h * (T0 + t1));
+    const double gthw = s_thw[c] + 0.5 * eps_p * gn;
     q.ci.t2ave[c] = 0.5 * eps_m * gn;
     g_muave += c1 * T0 * gn;
     g_muts += -(ld(q.x1.t2ave, c) / mass_h) * c1 * gt2a;
-  }
-  // ---- theta: thw' = thw + msfty dts t_tend - dts msfty (hdiv + rdnw (wdtn(k+1) - wdtn(k))) ----
-  for (int k = 0; k < nz; ++k) {
-    const size_t c = M(k);
-    const double gthw = s.gthw[c];
+    // theta: thw' = thw + msfty dts t_tend - dts msfty (hdiv + rdnw (wdtn(k+1) - wdtn(k)))
     q.ci.theta_w[c] = gthw;
     const double gtend = -dts * msfty * gthw;
-    s.gtend[c] = gtend;
+    s_tend[c] = gtend;
     const double rdnw = ld(g.rdnw, k);
-    if (k + 1 <= nz - 1)
-      s.gww[M(k + 1)] += rdnw * gtend * (ld(g.fnm, k + 1) * T1(k + 1) + ld(g.fnp, k + 1) * T1(k));
-    if (k >= 1) s.gww[c] -= rdnw * gtend * (ld(g.fnm, k) * T1(k) + ld(g.fnp, k) * T1(k - 1));
+    if (k + 1 <= nz - 1) s_ww[M(k + 1)] += rdnw * gtend * (ld(g.fnm, k + 1) * T1(k + 1) + ld(g.fnp, k + 1) * t1);
+    if (k >= 1) s_ww[c] -= rdnw * gtend * (ld(g.fnm, k) * t1 + ld(g.fnp, k) * T1(k - 1));
+  };
+  double gnext = 0.0;
+  double R_hi = 0.0, R_mid = s_rhs[M(nz)];  // rhs cotangents of faces m+1, m
+  double P_hi = 0.0, P_mid = 0.0;           // ph cotangents of faces m+1, m
+  double W_hi = 0.0;                        // w cotangent of face m+1
+  double B_mid = 0.0;                       // buoyancy cotangent of level m
+  double D_hi = 0.0;                        // wd cotangent of level m+1 (from face m+2)
+  double gt2a_top = 0.0;
+  for (int m = nz; m >= 1; --m) {
+    const size_t c = M(m);
+    // Thomas forward elimination wf(m) = (wn(m) - a(m) wf(m-1)) alpha(m), reversed
+    const double gwf = s_ws[c] + gnext;
+    const double alf = ld(q.alpha, c);
+    const double gwn = alf * gwf;
+    gnext = -ld(q.a, c) * alf * gwf;
+    double R_lo = (m - 1 >= 1) ? s_rhs[M(m - 1)] : 0.0;
+    double P_lo = (m - 1 == 0) ? ph0 : 0.0;
+    double B_lo = 0.0;
+    double W_mid = 0.0;
+    if (m <= nz - 1) {  // explicit w: wn = w + dts rw_tend + tA(rhs, ph) + tB(buoy, muave)
+      W_mid = gwn;
+      const double Q = minv * ld(q.cqw, c) * (c05dg * ld(g.rdn, m)) * gwn;
+      const double cf = coef(m), cm = coef(m - 1);
+      R_hi += Q * cf * eps_p;
+      R_mid -= Q * cf * eps_p + Q * cm * eps_p;
+      R_lo += Q * cm * eps_p;
+      P_hi += Q * cf * eps_m;
+      P_mid -= Q * cf * eps_m + Q * cm * eps_m;
+      P_lo += Q * cm * eps_m;
+      const double R = dts * G * minv * gwn;
+      B_mid += R * ld(g.rdn, m);
+      B_lo -= R * ld(g.rdn, m);
+      g_muave -= R * ld(g.c1f, m);
+    } else if (!q.col.top_lid) {  // the open top face
+      W_mid = gwn;
+      const double gT = minv * gwn;
+      const int km1 = nz - 1;
+      const double mhm = safe12(ld(g.c1h, km1) * mut + ld(g.c2h, km1));
+      const double rdnw_t = ld(g.rdnw, km1);
+      const double CA = -0.5 * dts * G / mhm * (rdnw_t * rdnw_t) * 2.0 * ld(q.c2a, M(km1));
+      R_mid += CA * eps_p * gT;
+      R_lo -= CA * eps_p * gT;
+      P_mid += CA * eps_m * gT;
+      P_lo -= CA * eps_m * gT;
+      gt2a_top = -dts * G * 2.0 * rdnw_t * ld(q.c2a, M(km1)) * ld(q.alt, M(km1)) * gT;
+      g_muave += -dts * G * ld(g.c1f, nz) * gT;
+    }
+    if (m + 1 <= nz) {  // face m+1 has all its contributions
+      double gwd_f, gwd_fm1;
+      predictor(m + 1, R_hi, P_hi, W_hi, gwd_f, gwd_fm1);
+      q.ci.ph[M(m + 1)] = P_hi;
+      q.ci.w[M(m + 1)] = W_hi;
+      if (m + 1 <= nz - 1) wd_rev(m + 1, D_hi + gwd_f);
+      D_hi = gwd_fm1;
+    }
+    if (m <= nz - 1) t2a_theta(m, B_mid, (m == nz - 1) ? gt2a_top : 0.0);
+    R_hi = R_mid; R_mid = R_lo;
+    P_hi = P_mid; P_mid = P_lo;
+    W_hi = W_mid;
+    B_mid = B_lo;
   }
-  // ---- mass update: mu_work' = mu_work + dts (dmdt + mu_tend) ----
+  {  // face 1, level 0 and face 0
+    double gwd_f, gwd_fm1;
+    predictor(1, R_hi, P_hi, W_hi, gwd_f, gwd_fm1);
+    q.ci.ph[M(1)] = P_hi;
+    q.ci.w[M(1)] = W_hi;
+    if (1 <= nz - 1) wd_rev(1, D_hi + gwd_f);
+    wd_rev(0, gwd_fm1);
+    q.ci.ph[M(0)] = P_mid;
+    q.ci.w[M(0)] = 0.0;  // the surface w is a stage constant
+    t2a_theta(0, B_mid, (nz - 1 == 0) ? gt2a_top : 0.0);
+  }
+
+  // ================= pass 3: mass update, ww prefix, dvdxi sum =================
   const double gmu = ld(q.co.mu, c2d);
   const double g_muts_t = ld(q.co.muts, c2d) + g_muts;
   const double g_muave_t = ld(q.co.muave, c2d) + g_muave;
-  const double g_mwn = gmu + g_muts_t + 0.5 * eps_p * g_muave_t;
+  const double g_mwn = gmu + g_muts_t + 0.5 * eps_p * g_muave_t;  // mu_work' = mu_work + dts (dmdt + mu_tend)
   const double g_mwo = -gmu + 0.5 * eps_m * g_muave_t + g_mwn;
   q.ci.mu[c2d] = gmu;
   q.ci.muts[c2d] = g_mwo;
   q.ci.muave[c2d] = 0.0;
   double g_dmdt = dts * g_mwn + ld(q.co.mudf, c2d);
-  // ---- ww'(kk) = ww(0) - sum_{m <= kk} inc(m) - ww_1(kk), kk < nz; ww'(nz) = ww(nz) ----
-  {
-    double S = 0.0;
-    s.gdv[M(nz - 1)] = 0.0;
-    for (int m = nz - 1; m >= 1; --m) {
-      S += s.gww[M(m)];
-      const double ginc = -S;
-      const int k = m - 1;
-      g_dmdt += ld(g.dnw, k) * ld(g.c1h, k) * minv * ginc;
-      s.gdv[M(k)] = ld(g.dnw, k) * minv * ginc;
-    }
-    q.ci.ww[M(0)] = S + s.gww[M(0)];
-    for (int f = 1; f < nz; ++f) q.ci.ww[M(f)] = 0.0;
-    q.ci.ww[M(nz)] = s.gww[M(nz)];
+  // ww'(kk) = ww(0) - sum_{m <= kk} inc(m) - ww_1(kk), kk < nz; ww'(nz) = ww(nz)
+  double S = 0.0;
+  s_dv[M(nz - 1)] = 0.0;
+  for (int m = nz - 1; m >= 1; --m) {
+    S += s_ww[M(m)];
+    const int k = m - 1;
+    const double ginc = -S;
+    g_dmdt += ld(g.dnw, k) * ld(g.c1h, k) * minv * ginc;
+    s_dv[M(k)] = ld(g.dnw, k) * minv * ginc;
+    q.ci.ww[M(m)] = 0.0;
   }
-  // ---- dmdt = sum_k dnw(k) dvdxi(k) ----
-  for (int k = 0; k < nz; ++k) s.gdv[M(k)] += ld(g.dnw, k) * g_dmdt;
+  q.ci.ww[M(0)] = S + s_ww[M(0)];
+  q.ci.ww[M(nz)] = s_ww[M(nz)];
+  // dmdt = sum_k dnw(k) dvdxi(k)
+  for (int k = 0; k < nz; ++k) s_dv[M(k)] += ld(g.dnw, k) * g_dmdt;
 }
 
 struct AdjFaceArgs {

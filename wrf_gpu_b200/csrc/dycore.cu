@@ -1117,8 +1117,7 @@ void ac_carve(const wrfgpu_step_params &p, Carver &cv, AcLayout &L) {
   size_t n[14];
   ac_counts(d, n);
   for (int q = 0; q < 14; ++q) L.x1[q] = cv.take(n[q]);
-  L.s.gal = cv.take(d.m); L.s.gthw = cv.take(d.m); L.s.gbuoy = cv.take(d.m); L.s.gwd = cv.take(d.m);
-  L.s.gtend = cv.take(d.m); L.s.gdv = cv.take(d.m);
+  L.s.gthw = cv.take(d.m); L.s.gtend = cv.take(d.m); L.s.gdv = cv.take(d.m);
   L.s.grhs = cv.take(d.w); L.s.gws = cv.take(d.w); L.s.gww = cv.take(d.w);
 }
 
