@@ -20,7 +20,9 @@ step, copy out) is reported beside it.
 
 Prints ONE JSON line (rank 0).  Beside the float64 step it also times the
 mixed-precision variant (FP32 advective fluxes, float64 accumulation) on the
-same input and reports it under "mixed" (skip with --no-mixed).  ``--impl reference`` times the reference
+same input and reports it under "mixed" (skip with --no-mixed), and the
+cost of the two hand-written adjoints against their forwards at the same grid
+under "adjoint" (skip with --no-adjoint).  ``--impl reference`` times the reference
 algorithm's CPU implementation available here -- the NumPy restatement in
 ``oracle/`` (JAX, the reference's own runtime, is not installed) -- on the
 host cores, on bounded 64 x 64 x 50 samples of the same workload.
@@ -419,7 +421,75 @@ def run_gpu(args, rank, world, local_rank):
                                       "serial_ms_per_step": serial_ms / k_e2e,
                                       "serial_value": world * cells * nsub * k_e2e / (serial_ms / 1000.0)},
                 launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed,
+                adjoint=adjoint_ratios(case, dev) if not args.no_adjoint else None,
                 tuned={"march_levels": tuned[0], "column_lanes": tuned[1], "column_width": tuned[2]})
+
+
+def adjoint_ratios(case, dev, reps=10):
+    """Adjoint / forward cost of the two hand-written adjoints at the workload's
+    grid (doubly periodic operators): the acoustic substep's VJP against one
+    forward substep, and the scalar-advection adjoint against its forward.
+    Operator inputs are synthesised from the workload state (timing does not
+    depend on the values): the stage's transport velocities, masses, pressure
+    and geopotential, unit moisture factors and a uniform tridiagonal
+    factorisation."""
+    import torch
+    from wrf_gpu_b200 import adjoint, dycore
+    nl = dycore.OperationalNamelist.from_case(case, device=dev, run_boundary=False, bc_source="ideal")
+    st = dycore.State.from_host(case.state, device=dev)
+    nz, ny, nx = st.theta.shape
+    z = lambda *s: torch.zeros(s, dtype=torch.float64, device=dev)
+    full = lambda v, *s: torch.full(s, v, dtype=torch.float64, device=dev)
+    mu = st.mu_total
+    muu = torch.cat([mu[:, :1], 0.5 * (mu[:, 1:] + mu[:, :-1]), mu[:, -1:]], dim=1).contiguous()
+    muv = torch.cat([mu[:1], 0.5 * (mu[1:] + mu[:-1]), mu[-1:]], dim=0).contiguous()
+    ph = st.ph_total
+    consts = {"u_tend": z(nz, ny, nx + 1), "v_tend": z(nz, ny + 1, nx), "t_tend": z(nz, ny, nx),
+              "rw_tend": z(nz + 1, ny, nx), "ph_tend": z(nz + 1, ny, nx), "alt": full(1.1, nz, ny, nx),
+              "pb": (st.p_total - st.p_perturbation).contiguous(), "c2a": full(1.3e5, nz, ny, nx),
+              "cqu": full(1.0, nz, ny, nx + 1), "cqv": full(1.0, nz, ny + 1, nx), "cqw": full(1.0, nz + 1, ny, nx),
+              "php": (0.5 * (ph[1:] + ph[:-1])).contiguous(), "pt1": ph.contiguous(),
+              "a": full(-0.1, nz + 1, ny, nx), "alpha": full(0.9, nz + 1, ny, nx), "gamma": full(-0.1, nz + 1, ny, nx),
+              "ww_1": z(nz + 1, ny, nx), "mut": mu.contiguous(), "muu": muu, "muv": muv,
+              "u_1": st.u, "v_1": st.v, "w_save": st.w, "theta": st.theta,
+              "phb0": (st.ph_total[0] - st.ph_perturbation[0]).contiguous()}
+    op = adjoint.AcousticOp(nl, consts, float(nl.dt_s) / float(nl.acoustic_substeps), device=dev)
+    x = [z(nz, ny, nx + 1), z(nz, ny + 1, nx), z(nz + 1, ny, nx), z(nz + 1, ny, nx), z(nz, ny, nx), z(nz, ny, nx),
+         st.p_perturbation.clone(), st.p_perturbation.clone(), z(nz, ny, nx), z(nz + 1, ny, nx),
+         st.mu_perturbation.clone(), mu.clone(), z(ny, nx), z(ny, nx)]
+    co = [torch.randn_like(t) for t in x]
+    xo = [t.clone() for t in x]
+    op.forward_(xo)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    xs = [t.clone() for t in x]
+    f_ms = timed(lambda: op.forward_(xs))
+    vs_ms = timed(lambda: op.vjp(x, co, xo))
+    vr_ms = timed(lambda: op.vjp(x, co))
+    aop = adjoint._Op(nl)
+    q = st.theta.clone()
+    ru, rv = torch.randn_like(q) * 5.0e4, torch.randn_like(q) * 5.0e4
+    rom = torch.randn(nz + 1, ny, nx, dtype=torch.float64, device=dev) * 1.0e3
+    tend = torch.empty_like(q)
+    af = timed(lambda: aop.apply("wrfgpu_scalar_advection", q, ru, rv, rom, tend))
+    ab = timed(lambda: aop.apply("wrfgpu_scalar_advection_adjoint", q, ru, rv, rom, tend))
+    del op, aop
+    return {"acoustic_substep": {"forward_ms": f_ms, "vjp_stored_ms": vs_ms, "vjp_recompute_ms": vr_ms,
+                                 "ratio_stored": vs_ms / f_ms, "ratio_recompute": vr_ms / f_ms,
+                                 "note": "VJP from a stored checkpoint of the substep output / recomputing it"},
+            "scalar_advection": {"forward_ms": af, "adjoint_ms": ab, "ratio": ab / af},
+            "data": "operator inputs synthesised from the workload state"}
 
 
 def run_batched(args):
@@ -489,6 +559,7 @@ def main():
     ap.add_argument("--nz", type=int, default=NZ)
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--no-mixed", action="store_true", help="skip timing the mixed-precision variant")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip timing the adjoints against their forwards")
     ap.add_argument("--no-tune", action="store_true", help="skip the tile-shape tuner (built-in defaults)")
     ap.add_argument("--workload", choices=("moist433", "batched"), default="moist433",
                     help="batched: the nest + ensemble set advanced by the batched call (1 GPU)")
@@ -546,7 +617,7 @@ def main():
                            "parallelism": f"replicas x{world}", "cuda_graph": True, "tile_shapes": r["tuned"]},
                 "e2e": r["e2e"], "roofline": r["roofline"], "whole_step_roofline": r["whole_step_roofline"],
                 "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": r["launches"],
-                "kernels": r["kernels"], "finite": r["finite"], "mixed": r["mixed"]}
+                "kernels": r["kernels"], "finite": r["finite"], "mixed": r["mixed"], "adjoint": r["adjoint"]}
         print(json.dumps(line))
     return 0
 

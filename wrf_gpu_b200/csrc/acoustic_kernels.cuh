@@ -102,6 +102,8 @@ constexpr int UV_KC = WG_UV_KC;
 #define WG_UV_MINB 1
 #endif
 
+// PIN: compile in the boundary cadence's ring-0 tangential wind pins.
+template <bool PIN = false>
 __global__ void __launch_bounds__(128, WG_UV_MINB) k_advance_uv(Grid g, Acoustic A, double dts, int top_lid, BdyArgs bdy) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(128, WG_UV_MINB) k_advance_uv(Grid g, Acoustic
       u = u - dts * L.cqu * dpx;
       u = u + c1 * mdu;
       if (wu != 0.0) u = u + wu * (ld(bdy.u_target, cu) - u);
-      if (bdy.cad && (j == 0 || j == ny - 1)) {
+      if (PIN && bdy.cad && (j == 0 || j == ny - 1)) {
         // tangential u on the S / N rows (core/acoustic.py:777-785)
         const double ms = c1 * ld(A.muus, fu) + c2, mc = c1 * ld(A.muu, fu) + c2;
         u = div_msf(strip_at(bdy.cad_u, nz, j == 0 ? 2 : 3, 0, k, i) * ms - ld(A.u_1, cu) * mc, g.msfuy, g.rmsfuy, fu);
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(128, WG_UV_MINB) k_advance_uv(Grid g, Acoustic
       v = v - dts * L.cqv * dpy;
       v = v + c1 * mdv;
       if (wv != 0.0) v = v + wv * (ld(bdy.v_target, cv) - v);
-      if (bdy.cad && (i == 0 || i == nx - 1) && j >= 1 && j <= ny - 1) {
+      if (PIN && bdy.cad && (i == 0 || i == nx - 1) && j >= 1 && j <= ny - 1) {
         // tangential v on the W / E columns
         const double ms = c1 * ld(A.muvs, fv) + c2, mc = c1 * ld(A.muv, fv) + c2;
         v = div_msf(strip_at(bdy.cad_v, nz, i == 0 ? 0 : 1, 0, k, j) * ms - ld(A.v_1, cv) * mc, g.msfvx, g.rmsfvx, fv);

@@ -95,7 +95,10 @@ __device__ __forceinline__ void column_prefetch(const Grid &g, const Acoustic &A
 
 inline size_t column_tiled_smem_bytes(int nz, int tx) { return (size_t)COL_NARR * (nz + 1) * tx * sizeof(double); }
 
-template <int TX, int TY>
+// PIN: compile in the boundary cadence's ring-0 pins of mu / muts / muave and
+// the work theta, and the ring-0 ph pin (cadence and nested child); off, the
+// kernel carries no trace of them.
+template <int TX, int TY, bool PIN = false>
 __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, Acoustic A, ColArgs c,
                                                                          const double *dvdxi, const double *hdiv) {
   static_assert(TX == 16 || TX == 32, "a column block is 16 or 32 columns wide");
@@ -182,7 +185,7 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
     s_mutend[tx] = mu_tend;
     s_scale[tx] = scale;
   }
-  if (ty == 0 && valid && !active && c.cad) {
+  if (PIN && ty == 0 && valid && !active && c.cad) {
     // specified cadence: ring-0 mu', muts and muave pinned to the mu' leaf
     const double mu_pin = ring_target(c.cad_mu, 1, ny, nx, 0, j, i);
     const double muts_pin = ld(c.mub, c2d) + mu_pin;
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
         thw = theta_i - dts * msfty * tend;
         A.theta_w[M(k)] = thw;
         S(A7, k) = thw;
-      } else if (c.cad) {
+      } else if (PIN && c.cad) {
         // specified cadence: the ring-0 work theta whose finished theta is the leaf's
         const double mass_pin = ld(g.c1h, k) * muts + ld(g.c2h, k);
         const double mass_cur = ld(g.c1h, k) * mut + ld(g.c2h, k);
@@ -449,7 +452,7 @@ __global__ void __launch_bounds__(TX * TY, col_minb(TX)) k_column_tiled(Grid g, 
         S(A4, f) = phn;
         A.ph[M(f)] = phn;
       }
-      if (!active && c.ph_pin) {
+      if (PIN && !active && c.ph_pin) {
         // ring-0 work ph whose finished ph' is the leaf's (spec_bdyupdate_ph)
         const double phn = ring_target(c.cad_ph, nz + 1, ny, nx, f, j, i) - ld(c.ph_save, M(f));
         S(A4, f) = phn;

@@ -815,15 +815,19 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       ca.ph_save = s.ph_pert;
     }
     const size_t col_smem = column_tiled_smem_bytes(nz, cwidth);
-    auto kColumn = (cwidth == 16)
-                       ? ((lanes == 8) ? k_column_tiled<16, 8> : (lanes == 16) ? k_column_tiled<16, 16> : k_column_tiled<16, 13>)
-                       : ((lanes == 8) ? k_column_tiled<32, 8> : (lanes == 16) ? k_column_tiled<32, 16> : k_column_tiled<32, 13>);
+    // the ring-0 pins are compiled into their own instantiations
+    const bool pins = cad || nest_ph_pin;
+#define WG_COL(TX, TY) (pins ? k_column_tiled<TX, TY, true> : k_column_tiled<TX, TY, false>)
+    auto kColumn = (cwidth == 16) ? ((lanes == 8) ? WG_COL(16, 8) : (lanes == 16) ? WG_COL(16, 16) : WG_COL(16, 13))
+                                  : ((lanes == 8) ? WG_COL(32, 8) : (lanes == 16) ? WG_COL(32, 16) : WG_COL(32, 13));
+#undef WG_COL
+    auto kAdvanceUV = cad ? k_advance_uv<true> : k_advance_uv<false>;
     if (stage == 0 && cudaFuncSetAttribute(kColumn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) !=
                           cudaSuccess)
       return fail(WRFGPU_ERR_CUDA, "cannot reserve shared memory for k_column_tiled (nz too large)");
     for (int it = 0; it < nsub[stage]; ++it) {
       PROF("k_advance_uv");
-      k_advance_uv<<<grd(nx + 1, ny + 1, (nz + UV_KC - 1) / UV_KC), blk2(), 0, stream>>>(g, A, dts, p.top_lid,
+      kAdvanceUV<<<grd(nx + 1, ny + 1, (nz + UV_KC - 1) / UV_KC), blk2(), 0, stream>>>(g, A, dts, p.top_lid,
                                                                                               ba);
       LAUNCH_CHECK("k_advance_uv");
       PROF("k_div_h");
@@ -1165,7 +1169,7 @@ int ac_forward(const wrfgpu_step_params &p, const Grid &g, const wrfgpu_acoustic
   ca.damp_opt = p.damp_opt; ca.dampcoef = p.dampcoef; ca.zdamp = p.zdamp;
   ca.rzdamp = (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
-  k_advance_uv<<<grd(nx + 1, ny + 1, (nz + UV_KC - 1) / UV_KC), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
+  k_advance_uv<false><<<grd(nx + 1, ny + 1, (nz + UV_KC - 1) / UV_KC), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
   if (int rc = check_launch("k_advance_uv")) return rc;
   k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, 0, L.dvdxi, L.hdiv);
   if (int rc = check_launch("k_div_h")) return rc;
