@@ -275,20 +275,27 @@ typedef struct wrfgpu_acoustic_consts {
   const double *mu_tend;                                      /* NULL = zero */
   const double *u_1, *v_1, *w_save, *theta;                   /* stage u, v, w, theta */
   const double *phb0;                                         /* base geopotential, face 0 (ny, nx) */
+  /* run_boundary: the stage's normal-wind work targets, u- / v-face shaped
+   * (coupling/boundary_apply.py:729-781), blended into the relax zone every
+   * substep; NULL otherwise */
+  const double *u_target, *v_target;
 } wrfgpu_acoustic_consts;
 
 /* Scratch bytes of wrfgpu_acoustic_substep / _vjp for these params. */
 int wrfgpu_acoustic_workspace_size(const wrfgpu_step_params *params, size_t *bytes);
 
-/* x <- one acoustic substep of length dts from x (in place).  Doubly
- * periodic domains (run_boundary 0) without the w_damping CFL term. */
+/* x <- one acoustic substep of length dts from x (in place), on doubly
+ * periodic or specified / nested domains (the boundary relaxation toward
+ * u_target / v_target, advance_mu_t's frozen ring and drain limiter), without
+ * the boundary cadence's ring-0 pins and without the w_damping CFL term. */
 int wrfgpu_acoustic_substep(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
                             const wrfgpu_acoustic_consts *consts, wrfgpu_acoustic_work *x, double dts,
                             void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* Its vector-Jacobian product at x: cot_in = J(x)^T cot_out, J the Jacobian of
  * wrfgpu_acoustic_substep with respect to the work state, constants fixed
- * (muave enters no output: its cot_in is zero).  x_out is the substep's
+ * and the drain limiter's scale held at its forward value (muave enters no
+ * output of an updated column: its cot_in is zero there).  x_out is the substep's
  * output from x (a stored checkpoint); NULL recomputes it into the
  * workspace.  cot_out is read only; cot_in must not alias it.  No
  * counterpart in the reference, which has no differentiation. */

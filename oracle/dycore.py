@@ -1679,23 +1679,28 @@ def rk_scan_step(carry, nl: Namelist, lead_seconds=None):
     return out
 
 
-def stage_acoustic_state(carry, nl: Namelist, rk_step: int = 3):
+def stage_acoustic_state(carry, nl: Namelist, rk_step: int = 3, lead_seconds=None):
     """The acoustic work state and stage constants that ``rk_scan_step`` hands
     its small-step loop (operational_mode.py:1682-2166), for RK stage
     ``rk_step`` entered from ``carry.state`` (used as both the stage and the
-    step-start state), on a doubly periodic domain.  Returns ``(a, dts, s)``:
-    ``a`` as ``acoustic_substep`` takes it, the substep length and the stage
-    state.  Test infrastructure for the substep operator and its adjoint."""
+    step-start state), without the specified-domain cadence and the nested
+    forcings.  Returns ``(a, dts, s, bdy)``: ``a`` as ``acoustic_substep``
+    takes it, the substep length, the stage state and the boundary relaxation
+    (None unless run_boundary with a lead).  Test infrastructure for the
+    substep operator and its adjoint."""
     m = nl.metrics
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
     s = copy_state(carry.state)
     dt = float(nl.dt_s)
     ns = int(nl.acoustic_substeps)
     dt_rk, dts = {1: (dt / 3.0, dt / 3.0), 2: (0.5 * dt, dt / float(ns)), 3: (dt, dt / float(ns))}[rk_step]
+    _, specified, nested = lateral_flags(nl)
     vel = couple_velocities_periodic(s.u, s.v, s.mu_total, m, rdx, rdy)
     tend = augment_large_step_tendencies(s, s, vel, nl, rk_step, None)
-    prep = small_step_prep(s, s, rk_step, m, vel.rom)
+    ww_stage = stage_omega_specified(s.u, s.v, s.mu_total, m, rdx, rdy) if (specified or nested) else vel.rom
+    prep = small_step_prep(s, s, rk_step, m, ww_stage)
     al0, p0 = calc_al_p(prep.mu_work, prep.muts, prep.ph_work, prep.theta_work, prep.theta_1, prep.c2a, prep.alt, m)
-    a, _ = acoustic_state_from_prep(s, prep, al0, p0, p0.copy(), tend, carry.mudf, nl, dts, None, None, dt_rk)
+    a, bdy = acoustic_state_from_prep(s, prep, al0, p0, p0.copy(), tend, carry.mudf, nl, dts, lead_seconds, None,
+                                      dt_rk)
     a.a, a.alpha, a.gamma = calc_coef_w(prep.mut, m, dts, nl.epssm, nl.top_lid, a.cqw, prep.c2a)
-    return a, dts, s
+    return a, dts, s, bdy

@@ -179,7 +179,7 @@ def test_host_shim_rejects_unsupported_namelist():
 
 def test_acoustic_substep_rejects_before_any_launch(lib):
     m, c, x = _capi.Metrics(), _capi.AcousticConsts(), _capi.AcousticWork()
-    for kw, code in ((dict(run_boundary=1), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
+    for kw, code in ((dict(run_boundary=1), _capi.WRFGPU_ERR_NULL_POINTER),
                      (dict(w_damping=1), _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG),
                      (dict(), _capi.WRFGPU_ERR_NULL_POINTER)):
         p = _params(lib, **kw)

@@ -80,7 +80,7 @@ ACOUSTIC_WORK_FIELDS = ("u", "v", "w", "ph", "theta_w", "t_2ave", "p", "pm1", "a
                         "mudf")
 ACOUSTIC_CONST_FIELDS = ("u_tend", "v_tend", "t_tend", "rw_tend", "ph_tend", "alt", "pb", "c2a", "cqu", "cqv", "cqw",
                          "php", "pt1", "a", "alpha", "gamma", "ww_1", "mut", "muu", "muv", "mu_tend", "u_1", "v_1",
-                         "w_save", "theta", "phb0")
+                         "w_save", "theta", "phb0", "u_target", "v_target")
 
 
 class AcousticWork(ctypes.Structure):

@@ -72,7 +72,8 @@ class AcousticOp:
     """One acoustic small step (``wrfgpu_acoustic_substep``) and its
     vector-Jacobian product (``wrfgpu_acoustic_substep_vjp``) for fixed stage
     constants: the reference's acoustic_substep_core (core/acoustic.py:837-1150)
-    on a doubly periodic domain.  ``consts`` maps the names of
+    on a doubly periodic or specified domain (``u_target`` / ``v_target``
+    given with run_boundary).  ``consts`` maps the names of
     ``_capi.ACOUSTIC_CONST_FIELDS`` to device tensors (``mu_tend`` may be
     absent); they are held for the op's lifetime."""
 

@@ -1,8 +1,9 @@
 // Vector-Jacobian product of one acoustic small step (advance_uv,
 // advance_mu_t, advance_w, calc_p_rho with smdiv memory; the reference's
 // acoustic_substep_core, core/acoustic.py:837-1150) with respect to its
-// evolving work state, the stage constants held fixed.  Doubly periodic
-// domains, no w_damping CFL term.
+// evolving work state, the stage constants held fixed.  Doubly periodic or
+// specified domains (the frozen ring, the drain limiter with its scale held
+// at the forward value, the relax-zone blend), no w_damping CFL term.
 //
 // The step is affine in the work state except through the new muts, which
 // enters the denominators of t_2ave, of the ph update and of calc_p_rho; the
@@ -42,6 +43,10 @@ struct AdjScratch {
 };
 
 struct AdjColArgs {
+  const double *x0_muts;  // input muts (the drain limiter's mu_work_old)
+  const double *dvdxi;    // forward dvdxi (specified: the drain limiter's dmdt)
+  const double *mu_tend;  // nullable
+  int specified;
   AcWorkR x1;  // forward output X' = F(X)
   AcWorkR co;  // cotangent of X'
   AcWork ci;   // cotangent of X (written)
@@ -70,6 +75,8 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
   const double dts = q.col.dts, eps_p = 1.0 + q.col.epssm, eps_m = 1.0 - q.col.epssm;
   const double msfty = ld(g.msfty, c2d), minv = ld(g.rmsfty, c2d);
   const double mut = ld(q.mut, c2d), muts = ld(q.x1.muts, c2d);
+  // specified domains advance mass, omega and theta on the interior columns only
+  const bool active = !q.specified || (j >= 1 && j <= ny - 2 && i >= 1 && i <= nx - 2);
   auto T1 = [&](int k) { return ld(q.theta_s, M(k)) - T0; };
   auto coef = [&](int k) {  // advance_w's stage-constant c2a*rdnw/mass_h(mut)
     return ld(q.c2a, M(k)) * ld(g.rdnw, k) / safe12(ld(g.c1h, k) * mut + ld(g.c2h, k));
@@ -174,8 +181,9 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     g_muts += -(ld(q.x1.t2ave, c) / mass_h) * c1 * gt2a;
     // theta: thw' = thw + msfty dts t_tend - dts msfty (hdiv + rdnw (wdtn(k+1) - wdtn(k)))
     q.ci.theta_w[c] = gthw;
-    const double gtend = -dts * msfty * gthw;
+    const double gtend = active ? -dts * msfty * gthw : 0.0;  // a frozen column keeps its theta
     s_tend[c] = gtend;
+    if (!active) return;
     const double rdnw = ld(g.rdnw, k);
     if (k + 1 <= nz - 1) s_ww[M(k + 1)] += rdnw * gtend * (ld(g.fnm, k + 1) * T1(k + 1) + ld(g.fnp, k + 1) * t1);
     if (k >= 1) s_ww[c] -= rdnw * gtend * (ld(g.fnm, k) * t1 + ld(g.fnp, k) * T1(k - 1));
@@ -256,6 +264,34 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
   const double gmu = ld(q.co.mu, c2d);
   const double g_muts_t = ld(q.co.muts, c2d) + g_muts;
   const double g_muave_t = ld(q.co.muave, c2d) + g_muave;
+  if (!active) {  // mu, muts, muave, mudf and ww pass through unchanged
+    q.ci.mu[c2d] = gmu;
+    q.ci.muts[c2d] = g_muts_t;
+    q.ci.muave[c2d] = g_muave_t;
+    q.ci.mudf[c2d] = ld(q.co.mudf, c2d);
+    for (int f = 0; f <= nz; ++f) q.ci.ww[M(f)] = s_ww[M(f)];
+    for (int k = 0; k < nz; ++k) s_dv[M(k)] = 0.0;
+    return;
+  }
+  // the drain limiter's scale (dynamics/mu_t_advance.py:295-451), held fixed
+  double scale = 1.0;
+  if (q.specified) {
+    double dmdt = 0.0;
+    for (int k = 0; k < nz; ++k) {
+      const double tk = ld(g.dnw, k) * ld(q.dvdxi, M(k));
+      dmdt = (k == 0) ? tk : dmdt + tk;
+    }
+    const double mu_tend = (q.mu_tend != nullptr) ? ld(q.mu_tend, c2d) : 0.0;
+    const double mu_work_old = ld(q.x0_muts, c2d) - mut;
+    const double floor_ = dmax(MIN_MUTS_PA, MIN_MUTS_FRACTION * mut);
+    const double muts_old = mut + mu_work_old;
+    const double raw = dts * (dmdt + mu_tend);
+    const double allowed = dmax(muts_old - floor_, 0.0);
+    const double loss = -raw;
+    const bool finite = isfinite(raw) && isfinite(muts_old);
+    scale = (finite && (loss > allowed)) ? allowed / dmax(loss, 1.0) : (finite ? 1.0 : 0.0);
+    scale = dmin(dmax(scale, 0.0), 1.0);
+  }
   const double g_mwn = gmu + g_muts_t + 0.5 * eps_p * g_muave_t;  // mu_work' = mu_work + dts (dmdt + mu_tend)
   const double g_mwo = -gmu + 0.5 * eps_m * g_muave_t + g_mwn;
   q.ci.mu[c2d] = gmu;
@@ -270,12 +306,13 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     const int k = m - 1;
     const double ginc = -S;
     g_dmdt += ld(g.dnw, k) * ld(g.c1h, k) * minv * ginc;
-    s_dv[M(k)] = ld(g.dnw, k) * minv * ginc;
+    s_dv[M(k)] = scale * (ld(g.dnw, k) * minv * ginc);
     q.ci.ww[M(m)] = 0.0;
   }
   q.ci.ww[M(0)] = S + s_ww[M(0)];
   q.ci.ww[M(nz)] = s_ww[M(nz)];
   // dmdt = sum_k dnw(k) dvdxi(k)
+  g_dmdt = scale * g_dmdt;
   for (int k = 0; k < nz; ++k) s_dv[M(k)] += ld(g.dnw, k) * g_dmdt;
 }
 
@@ -283,6 +320,7 @@ struct AdjFaceArgs {
   const double *gtend, *gdv, *theta_s;
   const double *co_u, *co_v;
   double *ci_u, *ci_v;
+  BdyArgs bdy;  // relax-zone weights (active on specified domains)
 };
 
 // The u / v face cotangents (after advance_uv): the outputs' own plus the
@@ -311,6 +349,8 @@ __global__ void k_adj_faces(Grid g, AdjFaceArgs q) {
       gu -= msftx * msfty * g.rdx * ld(q.gdv, c) +
             msftx * (0.5 * g.rdx) * (T1(j, i) + T1(j, wrp(i - 1, nx))) * ld(q.gtend, c);
     }
+    // the relax-zone blend u' = u + wu (target - u)
+    if (q.bdy.active) gu = gu - relax_weight_u(j, i, ny, nxu, q.bdy) * gu;
     q.ci_u[cu] = gu;
   }
   if (i < nx) {
@@ -329,6 +369,7 @@ __global__ void k_adj_faces(Grid g, AdjFaceArgs q) {
       gv -= msftx * msfty * g.rdy * ld(q.gdv, c) +
             msftx * (0.5 * g.rdy) * (T1(j, i) + T1(wrp(j - 1, ny), i)) * ld(q.gtend, c);
     }
+    if (q.bdy.active) gv = gv - relax_weight_v(j, i, nyv, nx, q.bdy) * gv;
     q.ci_v[cv] = gv;
   }
 }

@@ -1136,8 +1136,8 @@ int ac_check(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const wrfgpu_
   if (p == nullptr || m == nullptr || c == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/metrics/consts is NULL");
   int rc = wrfgpu_step_params_validate(p);
   if (rc) return rc;
-  if (p->run_boundary)
-    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "the standalone acoustic substep covers doubly periodic domains only");
+  if (p->run_boundary && (c->u_target == nullptr || c->v_target == nullptr))
+    return fail(WRFGPU_ERR_NULL_POINTER, "run_boundary needs the u_target / v_target work targets");
   if (p->w_damping != 0)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "the standalone acoustic substep has no w_damping CFL term");
   const double *need[] = {c->u_tend, c->v_tend, c->t_tend, c->rw_tend, c->ph_tend, c->alt, c->pb, c->c2a, c->cqu,
@@ -1152,9 +1152,7 @@ int ac_check(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const wrfgpu_
   return WRFGPU_OK;
 }
 
-// Launch one forward substep over the work arrays w[14] (in place).
-int ac_forward(const wrfgpu_step_params &p, const Grid &g, const wrfgpu_acoustic_consts &c, double *const w[14],
-               double dts, const AcLayout &L, cudaStream_t stream) {
+Acoustic ac_state(const wrfgpu_acoustic_consts &c, double *const w[14]) {
   Acoustic A{};
   A.u = w[0]; A.v = w[1]; A.w = w[2]; A.ph = w[3]; A.theta_w = w[4]; A.t2ave = w[5]; A.p = w[6]; A.pm1 = w[7];
   A.al = w[8]; A.ww = w[9]; A.mu = w[10]; A.muts = w[11]; A.muave = w[12]; A.mudf = w[13];
@@ -1163,15 +1161,39 @@ int ac_forward(const wrfgpu_step_params &p, const Grid &g, const wrfgpu_acoustic
   A.pt1 = c.pt1; A.a = c.a; A.alpha = c.alpha; A.gamma = c.gamma; A.ww_1 = c.ww_1;
   A.mut = c.mut; A.muu = c.muu; A.muv = c.muv; A.muus = c.muu; A.muvs = c.muv; A.mu_tend = c.mu_tend;
   A.u_1 = c.u_1; A.v_1 = c.v_1; A.w_save = c.w_save; A.theta_s = c.theta; A.phb0 = c.phb0;
+  return A;
+}
+
+// The boundary relaxation of one substep (as the step sets it up).
+BdyArgs ac_bdy(const wrfgpu_step_params &p, const wrfgpu_acoustic_consts &c, double dts) {
   BdyArgs ba{};
+  ba.active = p.run_boundary ? 1 : 0;
+  if (ba.active) {
+    const double strength = (p.normal_bdy_relax_strength < 0.0) ? 20.0 : p.normal_bdy_relax_strength;
+    ba.u_target = c.u_target;
+    ba.v_target = c.v_target;
+    ba.sub_ratio = strength * (p.dt != 0.0 ? dts / p.dt : 0.0);
+    ba.spec_zone = 1;
+    ba.relax_zone = 4;
+    set_bdy_weights(ba);
+  }
+  return ba;
+}
+
+// Launch one forward substep over the work arrays w[14] (in place).
+int ac_forward(const wrfgpu_step_params &p, const Grid &g, const wrfgpu_acoustic_consts &c, double *const w[14],
+               double dts, const AcLayout &L, cudaStream_t stream) {
+  Acoustic A = ac_state(c, w);
+  const int specified = (p.run_boundary && !p.bc_ideal) ? 1 : 0;
+  BdyArgs ba = ac_bdy(p, c, dts);
   ColArgs ca{};
-  ca.dts = dts; ca.epssm = p.epssm; ca.specified = 0; ca.top_lid = p.top_lid; ca.w_damping = 0;
+  ca.dts = dts; ca.epssm = p.epssm; ca.specified = specified; ca.top_lid = p.top_lid; ca.w_damping = 0;
   ca.damp_opt = p.damp_opt; ca.dampcoef = p.dampcoef; ca.zdamp = p.zdamp;
   ca.rzdamp = (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   k_advance_uv<false><<<grd(nx + 1, ny + 1, (nz + UV_KC - 1) / UV_KC), blk2(), 0, stream>>>(g, A, dts, p.top_lid, ba);
   if (int rc = check_launch("k_advance_uv")) return rc;
-  k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, 0, L.dvdxi, L.hdiv);
+  k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, specified, L.dvdxi, L.hdiv);
   if (int rc = check_launch("k_div_h")) return rc;
   const size_t smem = column_tiled_smem_bytes(nz, COL_TX);
   auto kColumn = k_column_tiled<COL_TX, COL_TY>;
@@ -1265,11 +1287,21 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
     }
     if ((rc = ac_forward(*p, g, *c, L.x1, dts, L, stream))) return rc;
   }
+  const int specified = (p->run_boundary && !p->bc_ideal) ? 1 : 0;
+  if (specified && x_out != nullptr) {  // the forward dvdxi (the drain limiter's input) from the stored output
+    Acoustic A = ac_state(*c, x1);
+    k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, 1, L.dvdxi, L.hdiv);
+    if ((rc = check_launch("k_div_h"))) return rc;
+  }
   // the atomically accumulated cotangents start from zero
   for (int q : {6, 8, 13})
     if (cudaMemsetAsync(ci[q], 0, n[q] * sizeof(double), stream) != cudaSuccess)
       return fail(WRFGPU_ERR_CUDA, "cotangent clear failed");
   AdjColArgs a{};
+  a.x0_muts = xin[11];
+  a.dvdxi = L.dvdxi;
+  a.mu_tend = c->mu_tend;
+  a.specified = specified;
   a.x1 = AcWorkR{x1[0], x1[1], x1[2], x1[3], x1[4], x1[5], x1[6], x1[7], x1[8], x1[9], x1[10], x1[11], x1[12], x1[13]};
   a.co = AcWorkR{co[0], co[1], co[2], co[3], co[4], co[5], co[6], co[7], co[8], co[9], co[10], co[11], co[12], co[13]};
   a.ci = AcWork{ci[0], ci[1], ci[2], ci[3], ci[4], ci[5], ci[6], ci[7], ci[8], ci[9], ci[10], ci[11], ci[12], ci[13]};
@@ -1281,7 +1313,7 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
   a.col.rzdamp = (p->zdamp != 0.0 && std::isfinite(1.0 / p->zdamp)) ? 1.0 / p->zdamp : 0.0;
   k_adj_column<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, a);
   if ((rc = check_launch("k_adj_column"))) return rc;
-  AdjFaceArgs fa{L.s.gtend, L.s.gdv, c->theta, co[0], co[1], ci[0], ci[1]};
+  AdjFaceArgs fa{L.s.gtend, L.s.gdv, c->theta, co[0], co[1], ci[0], ci[1], ac_bdy(*p, *c, dts)};
   k_adj_faces<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, fa);
   if ((rc = check_launch("k_adj_faces"))) return rc;
   AdjUVArgs ua{ci[0], ci[1], c->alt, c->pb, c->php, c->cqu, c->cqv, c->muu, c->muv,
