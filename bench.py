@@ -170,6 +170,24 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(ms, dist=None, device="cpu"):
+    """The largest of each rank's duration, returned on every rank (ranks
+    are replicas: the job takes as long as its slowest rank)."""
+    if dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(ms, world, cells, nsub, steps):
+    """Whole-job cell-substeps/s of `world` replicas each advancing `cells`
+    cells through `steps` RK3 steps of `nsub` substeps in `ms` (the max over
+    ranks)."""
+    return world * cells * nsub * steps / (ms / 1000.0)
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     from wrf_gpu_b200 import build, cases, dycore, perfmodel, _capi
@@ -222,14 +240,11 @@ def run_gpu(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_per_step = ms / args.steps
-    value = world * cells * nsub * args.steps / (ms / 1000.0)
+    value = replica_throughput(ms, world, cells, nsub, args.steps)
 
     # per-kernel timing over a second, instrumented region of the same steps
     _capi.profile_enable(True, max_records=stp.launches_per_step * args.steps + 16)
@@ -281,11 +296,7 @@ def run_gpu(args, rank, world, local_rank):
             h.copy_(t, non_blocking=True)
 
     def _max_over_ranks(ms):
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ms, dist, dev)
 
     # (a) serial: copy in, step, copy out on one stream
     for _ in range(max(1, min(args.warmup, 2))):
@@ -355,7 +366,7 @@ def run_gpu(args, rank, world, local_rank):
     g1 = torch.cuda.Event(enable_timing=True)
     streamed(k_e2e, g0, g1)
     e2e_ms = _max_over_ranks(g0.elapsed_time(g1))
-    e2e_value = world * cells * nsub * k_e2e / (e2e_ms / 1000.0)
+    e2e_value = replica_throughput(e2e_ms, world, cells, nsub, k_e2e)
     del graph_b, bufs
     out_ok = bool(torch.isfinite(out.state.w).all().item() and torch.isfinite(out.state.theta).all().item())
     del graph
@@ -396,17 +407,13 @@ def run_gpu(args, rank, world, local_rank):
             graph_m.replay()
         g1.record(stream)
         torch.cuda.synchronize(dev)
-        ms_m = g0.elapsed_time(g1)
-        if dist is not None:
-            t = torch.tensor([ms_m], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_m = float(t.item())
+        ms_m = max_over_ranks(g0.elapsed_time(g1), dist, dev)
         # one-step difference from the float64 step on this workload
         diff = {}
         for f in ("u", "v", "w", "theta"):
             a, b = getattr(out_m.state, f), getattr(out.state, f)
             diff[f] = float((a - b).abs().max().item() / max(b.abs().max().item(), 1e-300))
-        mixed = {"value": world * cells * nsub * args.steps / (ms_m / 1000.0), "unit": METRIC,
+        mixed = {"value": replica_throughput(ms_m, world, cells, nsub, args.steps), "unit": METRIC,
                  "ms_per_step": ms_m / args.steps, "dtype": "f32 fluxes / f64 accumulation",
                  "rel_diff_vs_fp64_one_step": diff,
                  "stated_error": "<= 1e-5 relative max-abs on u, v, w, theta after 60 steps vs the float64 oracle "
@@ -419,7 +426,7 @@ def run_gpu(args, rank, world, local_rank):
                                                 "whole output state device->host (pinned); double-buffered so "
                                                 "copies overlap compute on separate streams",
                                       "serial_ms_per_step": serial_ms / k_e2e,
-                                      "serial_value": world * cells * nsub * k_e2e / (serial_ms / 1000.0)},
+                                      "serial_value": replica_throughput(serial_ms, world, cells, nsub, k_e2e)},
                 launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed,
                 adjoint=adjoint_ratios(case, dev) if not args.no_adjoint else None,
                 tuned={"march_levels": tuned[0], "column_lanes": tuned[1], "column_width": tuned[2]})
