@@ -122,6 +122,13 @@ typedef struct wrfgpu_step_params {
   int nested_ph_relax;
   int nested_w_relax;
   int nested_ph_spec;
+  /* 1: the step merges the caller's RK1-fixed physics tendencies
+   * (_rk_scan_step's physics_tendencies, a DryPhysicsTendencies,
+   * dynamics/core/rk_addtend_dry.py:103-124) into every RK stage's
+   * tendencies as rk_addtend_dry does (rk_addtend_dry.py:490-546;
+   * operational_mode.py:3062-3075); the bundle's arrays are the inputs'
+   * physics pointers (NULL = zero).  0 (default): no bundle. */
+  int physics;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */
@@ -155,6 +162,14 @@ typedef struct wrfgpu_step_inputs {
   /* w strip (nz+1 levels) the nested w relaxation reads (NULL otherwise);
    * ph_bdy is also read by the nested ph' relaxation and pin */
   const double *w_bdy;
+  /* DryPhysicsTendencies leaves (params.physics = 1; each NULL = zero):
+   * ru_tendf (u-face), rv_tendf (v-face), rw_tendf, ph_tendf (nz+1), t_tendf,
+   * h_diabatic (mass), mu_tendf (ny, nx), and the boundary tendencies added
+   * at the first RK stage only, phys_u_save ... phys_t_save.  ph_tendf and
+   * phys_ph_save enter no output: the ph tendency of this path is rhs_ph's
+   * (operational_mode.py:3083-3084). */
+  const double *ru_tendf, *rv_tendf, *rw_tendf, *ph_tendf, *t_tendf, *mu_tendf, *h_diabatic;
+  const double *phys_u_save, *phys_v_save, *phys_w_save, *phys_ph_save, *phys_t_save;
 } wrfgpu_step_inputs;
 
 /* Step outputs: the returned OperationalCarry (operational_mode.py:2234-2265). */

@@ -686,8 +686,30 @@ def large_step_coriolis(s, m, specified):
 # large-step tendency assembly: runtime/operational_mode.py:2722-3093, 3162-3316
 # ----------------------------------------------------------------------------
 
-def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_relax=None):
-    """operational_mode.py:2722-3093 (flux advection on, diffusion off, physics off)."""
+def rk_addtend_dry(t, physics, rk_step, m, mut):
+    """core/rk_addtend_dry.py:490-546: the RK1-fixed physics tendencies merged
+    into one stage's tendencies (u, v, w coupled by their map factors, theta
+    with the diabatic heating coupled by the full column mass ``mut``; the
+    rk_step 1 boundary saves added first).  ``physics`` has the attributes of
+    DryPhysicsTendencies (None = zero); ph has no consumer on this path."""
+    z = lambda ref, c: np.zeros_like(ref) if c is None else c
+    ru, rv, rw = z(t.u, physics.ru_tendf), z(t.v, physics.rv_tendf), z(t.w, physics.rw_tendf)
+    tt, mt = z(t.theta, physics.t_tendf), z(t.mu, physics.mu_tendf)
+    if rk_step == 1:
+        ru = ru + z(t.u, physics.u_save) * m.msfuy[None]
+        rv = rv + z(t.v, physics.v_save) * m.msfvx[None]
+        rw = rw + z(t.w, physics.w_save) * m.msfty[None]
+        tt = tt + z(t.theta, physics.t_save)
+    mass_h = _col(m.c1h) * mut[None] + _col(m.c2h)
+    h = z(t.theta, physics.h_diabatic)
+    return SimpleNamespace(u=t.u + ru / m.msfuy[None], v=t.v + rv * (1.0 / m.msfvx)[None],
+                           w=t.w + rw / m.msfty[None],
+                           theta=t.theta + tt / m.msfty[None] + mass_h * h / m.msfty[None], mu=t.mu + mt)
+
+
+def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_relax=None, physics=None):
+    """operational_mode.py:2722-3093 (flux advection on, diffusion off), with
+    the physics merge (:3062-3075) when ``physics`` is given."""
     m = nl.metrics
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
     c1h, c2h, c1f, c2f = _col(m.c1h), _col(m.c2h), _col(m.c1f), _col(m.c2f)
@@ -720,6 +742,10 @@ def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_rel
     ru_cor, rv_cor = large_step_coriolis(s, m, bool(nl.run_boundary))
     u_t = u_t + ru_cor
     v_t = v_t + rv_cor
+    if physics is not None:
+        mg = rk_addtend_dry(SimpleNamespace(u=u_t, v=v_t, w=w_t, theta=th_t, mu=bmu), physics, rk_step, m,
+                            s.mu_total)
+        u_t, v_t, w_t, th_t, bmu = mg.u, mg.v, mg.w, mg.theta, mg.mu
     if bdy_relax is not None:  # operational_mode.py:3085-3092 (mu at the first stage only)
         return SimpleNamespace(u=u_t + bdy_relax.ru, v=v_t + bdy_relax.rv, w=w_t, theta=th_t + bdy_relax.t,
                                mu=(bmu + bdy_relax.mu) if rk_step == 1 else bmu.copy())
@@ -1618,11 +1644,13 @@ def small_step_finish_and_refresh(s, prep, a, nl: Namelist):
     return n
 
 
-def rk_scan_step(carry, nl: Namelist, lead_seconds=None):
+def rk_scan_step(carry, nl: Namelist, lead_seconds=None, physics=None):
     """``_rk_scan_step`` (operational_mode.py:3319-3534).
 
     ``carry`` is a SimpleNamespace with ``state`` and ``mudf``; the returned
     carry adds t_2ave, ww, mudf, muave, muts, ph_tend and the *_save family.
+    ``physics`` (DryPhysicsTendencies attributes) is merged into every stage's
+    tendencies by ``rk_addtend_dry``.
     """
     m = nl.metrics
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
@@ -1645,7 +1673,7 @@ def rk_scan_step(carry, nl: Namelist, lead_seconds=None):
         if nl.specified_adv_degrade and specified:  # operational_mode.py:2464-2475, 2494-2507
             vel.specified = True
             vel.ru_full, vel.rv_full = couple_uv_specified(s.u, s.v, s.mu_total, m)
-        tend = augment_large_step_tendencies(s, origin, vel, nl, rk_step, bdy_relax)
+        tend = augment_large_step_tendencies(s, origin, vel, nl, rk_step, bdy_relax, physics)
         q_tend = moisture_coupled_tendencies(s, origin, vel, nl, rk_step) if moist else None
         ww_stage = stage_omega_specified(s.u, s.v, s.mu_total, m, rdx, rdy) if (specified or nested) else vel.rom
         prep = small_step_prep(s, origin, rk_step, m, ww_stage)

@@ -19,11 +19,11 @@ def oracle_namelist(case):
     return D.Namelist(metrics=case.metrics, **case.controls)
 
 
-def oracle_steps(case, nsteps, lead0=0.0):
+def oracle_steps(case, nsteps, lead0=0.0, physics=None):
     nl = oracle_namelist(case)
     carry = SimpleNamespace(state=D.copy_state(case.state), mudf=case.mudf.copy())
     for i in range(nsteps):
-        carry = D.rk_scan_step(carry, nl, lead_seconds=lead0 + i * nl.dt_s)
+        carry = D.rk_scan_step(carry, nl, lead_seconds=lead0 + i * nl.dt_s, physics=physics)
     return carry
 
 

@@ -134,6 +134,16 @@ def test_launch_count(lib):
     assert n.value == (1 + 3 * 13 + 3 * 10) + 3
 
 
+def test_launch_count_with_physics(lib):
+    n0, n1 = ctypes.c_int(0), ctypes.c_int(0)
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(_params(lib, acoustic_substeps=6)), ctypes.byref(n0)) == 0
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(_params(lib, acoustic_substeps=6, physics=1)),
+                                        ctypes.byref(n1)) == 0
+    # the mu tendency once per step, the u / v / theta merge once per stage
+    assert n1.value == n0.value + 1 + 3
+    assert lib.wrfgpu_step_params_validate(ctypes.byref(_params(lib, physics=2))) == _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG
+
+
 def test_params_init_keeps_the_geopotential_forced(lib):
     # BoundaryConfig defaults: force_geopotential on, the nested forcings off
     # (coupling/boundary_apply.py:110, 142-144)
@@ -172,9 +182,6 @@ def test_host_shim_rejects_unsupported_namelist():
         nl = dycore.OperationalNamelist.from_case(case, metrics=m, **kw)
         with pytest.raises(NotImplementedError):
             dycore.rk_scan_step(carry, nl)
-    nl = dycore.OperationalNamelist.from_case(case, metrics=m)
-    with pytest.raises(NotImplementedError):
-        dycore.rk_scan_step(carry, nl, physics_tendencies=object())
 
 
 def test_acoustic_substep_rejects_before_any_launch(lib):

@@ -35,25 +35,29 @@ def _tol(k):
     return DIAG_TOL if k in DIAG else TOL
 
 
-def _gpu_one_step(case, state, mudf, lead):
+def _gpu_one_step(case, state, mudf, lead, physics=None):
     c = SimpleNamespace(**vars(case))
     c.state = state
     c.mudf = mudf
     nl = dycore.OperationalNamelist.from_case(case)
     carry = dycore.carry_from_case(c)
-    out = dycore.rk_scan_step(carry, nl, lead_seconds=lead)
+    phys = None
+    if physics is not None:
+        phys = SimpleNamespace(**{k: (None if v is None else torch.as_tensor(v, device="cuda"))
+                                  for k, v in vars(physics).items()})
+    out = dycore.rk_scan_step(carry, nl, lead_seconds=lead, physics_tendencies=phys)
     torch.cuda.synchronize()
     return out
 
 
-def _per_step(case, nsteps):
+def _per_step(case, nsteps, physics=None):
     nl = P.oracle_namelist(case)
     carry = SimpleNamespace(state=D.copy_state(case.state), mudf=case.mudf.copy())
     worst = []
     for n in range(nsteps):
         lead = n * nl.dt_s
-        ora = D.rk_scan_step(carry, nl, lead_seconds=lead)
-        gpu = _gpu_one_step(case, carry.state, carry.mudf, lead)
+        ora = D.rk_scan_step(carry, nl, lead_seconds=lead, physics=physics)
+        gpu = _gpu_one_step(case, carry.state, carry.mudf, lead, physics)
         worst.append(P.compare(gpu, ora))
         carry = SimpleNamespace(state=ora.state, mudf=ora.mudf)
     return worst
@@ -174,6 +178,29 @@ def test_per_step_parity_nested(cuda_ready, forcings):
     for n, e in enumerate(_per_step(case, 2)):
         bad = {k: v for k, v in e.items() if not v <= _tol(k)}
         assert not bad, f"{forcings} step {n}: {bad}"
+
+
+@pytest.mark.parametrize("kind,leaves", [
+    ("periodic", "all"), ("specified", "all"), ("specified", "saves_only"), ("cadence", "all")])
+def test_per_step_parity_physics_tendencies(cuda_ready, kind, leaves):
+    """rk_addtend_dry: a DryPhysicsTendencies bundle merged into every stage
+    (the boundary saves at the first stage only; h_diabatic coupled by the
+    stage mass), with non-unit map factors; a bundle of saves only leaves the
+    tendf lanes at zero."""
+    from tests.test_oracle_physics_merge import physics_bundle
+    specified = kind != "periodic"
+    case = _with_map_factors(cases.real_like_moist(28, 22, 12, hmax=800.0, specified=specified,
+                                                   bdy_noise=specified), seed=21)
+    if kind == "cadence":
+        case.controls.update(specified_bdy_cadence=True)
+    nz, ny, nx = case.state.theta.shape
+    phys = physics_bundle(nz, ny, nx, 17)
+    if leaves == "saves_only":
+        for f in ("ru_tendf", "rv_tendf", "rw_tendf", "t_tendf", "mu_tendf", "h_diabatic"):
+            setattr(phys, f, None)
+    for n, e in enumerate(_per_step(case, 2, phys)):
+        bad = {k: v for k, v in e.items() if not v <= _tol(k)}
+        assert not bad, f"{kind}/{leaves} step {n}: {bad}"
 
 
 def test_per_step_parity_map_factors_periodic(cuda_ready):

@@ -43,7 +43,7 @@ class StepParams(ctypes.Structure):
         ("cfn", _D), ("cfn1", _D),
         ("march_levels", _I), ("column_lanes", _I), ("column_width", _I), ("specified_adv_degrade", _I),
         ("specified_bdy_cadence", _I), ("force_geopotential", _I), ("nested_ph_relax", _I),
-        ("nested_w_relax", _I), ("nested_ph_spec", _I),
+        ("nested_w_relax", _I), ("nested_ph_spec", _I), ("physics", _I),
     ]
 
 
@@ -59,13 +59,20 @@ STATE_FIELDS = ("u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total",
                 "mu_total", "mu_perturbation")
 
 
+# DryPhysicsTendencies leaves (dynamics/core/rk_addtend_dry.py:103-124) and their C input names
+PHYSICS_LEAVES = ("ru_tendf", "rv_tendf", "rw_tendf", "ph_tendf", "t_tendf", "mu_tendf", "h_diabatic", "u_save",
+                  "v_save", "w_save", "ph_save", "t_save")
+PHYSICS_FIELDS = ("ru_tendf", "rv_tendf", "rw_tendf", "ph_tendf", "t_tendf", "mu_tendf", "h_diabatic", "phys_u_save",
+                  "phys_v_save", "phys_w_save", "phys_ph_save", "phys_t_save")
+
+
 class StepInputs(ctypes.Structure):
     _fields_ = [(n, _P) for n in STATE_FIELDS] + [
         ("q", _P * 6), ("mudf", _P),
         ("base_u", _P), ("base_v", _P), ("base_w", _P), ("base_theta", _P), ("base_mu", _P),
         ("u_bdy", _P), ("v_bdy", _P), ("bdy_ntime", _I), ("bdy_width", _I), ("bdy_side_len", _I),
         ("theta_bdy", _P), ("ph_bdy", _P), ("mu_bdy", _P), ("w_bdy", _P),
-    ]
+    ] + [(n, _P) for n in PHYSICS_FIELDS]
 
 
 CARRY_OUT_FIELDS = ("t_2ave", "ww", "mudf", "muave", "muts", "ph_tend", "u_save", "v_save", "w_save", "t_save",

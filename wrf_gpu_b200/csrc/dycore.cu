@@ -24,6 +24,7 @@
 #include "adjoint.cuh"
 #include "acoustic_adjoint.cuh"
 #include "bdy_cadence.cuh"
+#include "physics_merge.cuh"
 
 using namespace wg;
 
@@ -81,6 +82,7 @@ struct Work {
   double *rom, *ww_spec, *rw_tend, *ph_tend, *cqw, *w_w, *ph_w, *pt1, *ww, *a, *alpha, *gamma;
   // intermediate states after stages 1 and 2
   StateW st[2];
+  double *mu_tend_phys;  // physics: the stages' mu tendency (base + mu_tendf)
   // specified boundary cadence: the first stage's mu tendency (base + relax)
   double *mu_tend_s1;
 };
@@ -119,6 +121,7 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   w.ph_w = c.take(d.w); w.pt1 = c.take(d.w); w.ww = c.take(d.w);
   w.a = c.take(d.w); w.alpha = c.take(d.w); w.gamma = c.take(d.w);
   w.mu_tend_s1 = (spec && p.specified_bdy_cadence && p.force_geopotential) ? c.take(d.s2) : nullptr;
+  w.mu_tend_phys = p.physics ? c.take(d.s2) : nullptr;
   for (int s = 0; s < 2; ++s) {
     StateW &S = w.st[s];
     S.u = c.take(d.u); S.v = c.take(d.v); S.w = c.take(d.w); S.theta = c.take(d.m);
@@ -255,7 +258,7 @@ ProfState g_prof;
 const char *kClassNames[] = {"k_recip_msf", "k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
                              "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_uv",
                              "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col", "k_spec_relax",
-                             "k_spec_w"};
+                             "k_spec_w", "k_phys"};
 constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
 
 int class_of(const char *name) {
@@ -403,6 +406,7 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13 or 16");
   if (p->column_width != 0 && p->column_width != 16 && p->column_width != 32)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 16 or 32");
+  if (p->physics != 0 && p->physics != 1) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "physics must be 0 or 1");
   if (p->specified_adv_degrade != 0 && p->specified_adv_degrade != 1)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "specified_adv_degrade must be 0 or 1");
   if (spec && p->specified_adv_degrade && p->force_geopotential && (p->nx < 7 || p->ny < 7))
@@ -428,7 +432,7 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
   const int ns = p->acoustic_substeps;
   const int nsub[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
   const bool bdy = p->run_boundary != 0;
-  int n = 1;  // map-factor reciprocals
+  int n = 1 + (p->physics ? 1 : 0);  // map-factor reciprocals [, the physics mu tendency]
   for (int s = 0; s < 3; ++s) {
     n += 8;  // mass2d, transport, diag, uface, vface, mass, wface, coef
     if (s == 2 && (p->scalar_adv_opt == 1 || p->scalar_adv_opt == 2)) n += 2;
@@ -436,6 +440,7 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
     if (bdy) n += 2;
     n += 3 * nsub[s];  // advance_uv, div_h, column
     n += 3;  // finish u, v, col
+    if (p->physics) n += 1;  // the physics merge of u, v, theta
     if (p->run_boundary && !p->bc_ideal && p->force_geopotential && p->specified_bdy_cadence) {
       n += (s == 0) ? 2 : 1;  // [first-stage mu tendency], relax tendencies
       n += nsub[s];           // zero-gradient w after every column launch
@@ -600,6 +605,17 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   k_recip_msf<<<grd(nx + 1, ny + 1, 1), blk2(), 0, stream>>>(g, w.rmsftx, w.rmsfty, w.rmsfux, w.rmsfuy, w.rmsfvx,
                                                              w.rmsfvy);
   LAUNCH_CHECK("k_recip_msf");
+  // the stages' mu tendency: the base tendency, plus the physics mu_tendf
+  const double *base_mu = in->base_mu;
+  if (p.physics) {
+    PROF("k_phys");
+    k_phys_mu<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, in->base_mu, in->mu_tendf, w.mu_tend_phys);
+    LAUNCH_CHECK("k_phys_mu");
+    base_mu = w.mu_tend_phys;
+  }
+  PhysArgs phys{in->ru_tendf, in->rv_tendf, in->rw_tendf, in->t_tendf, in->mu_tendf, in->h_diabatic,
+                in->phys_u_save, in->phys_v_save, in->phys_w_save, in->phys_t_save, 0};
+  if (!p.physics) phys = PhysArgs{};
 
   // Advective-flux arithmetic: float64 (the reference's), or the mixed
   // variant's FP32 fluxes with float64 accumulation.
@@ -709,7 +725,8 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     PROF("k_wface");
     kWface<<<tgrd(nx, ny, nz + 1), tblk(), 0, stream>>>(g, s, origin, w.ru, w.rv, w.rom, ww_stage, w.qtot,
                                                                w.mub, w.mut, w.muts0, w.muu, w.muv, in->base_w,
-                                                               p.top_lid, p.moist_cqw, p.w_coriolis, wo);
+                                                               p.top_lid, p.moist_cqw, p.w_coriolis, wo,
+                                                               PhysW{phys.rw_tendf, phys.w_save, stage == 0 ? 1 : 0});
     LAUNCH_CHECK("k_wface");
     const double x = 0.5 * dts * G * eps1;
     const double cof = x * x;
@@ -723,12 +740,20 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         g, w.mut, w.muts0, w.mu_work0, w.c2a, w.cqw, w.alt, w.theta_w, w.ph_w, origin.theta, cof, p.top_lid, co);
     LAUNCH_CHECK("k_coef");
 
+    if (p.physics) {
+      // rk_addtend_dry: the physics tendencies into this stage's u, v, theta (w: in k_wface)
+      PhysArgs ps = phys;
+      ps.rk1 = (stage == 0) ? 1 : 0;
+      PROF("k_phys");
+      k_phys_merge<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, ps, s.mu_total, w.u_tend, w.v_tend, w.t_tend);
+      LAUNCH_CHECK("k_phys_merge");
+    }
     if (cad) {
       // relax tendencies into this stage's u, v, theta and ph' tendencies, and
       // (first stage only) the mu' tendency (operational_mode.py:1994-1995, 3085-3092)
       if (stage == 0) {
         PROF("k_spec_relax");
-        k_mu_tend_init<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, in->base_mu, w.mu_tend_s1);
+        k_mu_tend_init<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, base_mu, w.mu_tend_s1);
         LAUNCH_CHECK("k_mu_tend_init");
       }
       RelaxArgs rs = ra;
@@ -796,7 +821,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     A.alt = w.alt; A.pb = w.pb; A.c2a = w.c2a; A.cqu = w.cqu; A.cqv = w.cqv; A.cqw = w.cqw; A.php = w.php;
     A.pt1 = w.pt1; A.a = w.a; A.alpha = w.alpha; A.gamma = w.gamma; A.ww_1 = ww_stage;
     A.mut = w.mut; A.muu = w.muu; A.muv = w.muv; A.muus = w.muus; A.muvs = w.muvs;
-    A.mu_tend = (cad && stage == 0) ? w.mu_tend_s1 : in->base_mu;
+    A.mu_tend = (cad && stage == 0) ? w.mu_tend_s1 : base_mu;
     A.u_1 = s.u; A.v_1 = s.v; A.w_save = s.w; A.theta_s = s.theta; A.phb0 = w.phb0;
     ColArgs ca{};
     ca.dts = dts; ca.epssm = p.epssm; ca.specified = specified ? 1 : 0; ca.top_lid = p.top_lid;

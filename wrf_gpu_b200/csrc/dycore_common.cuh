@@ -45,6 +45,12 @@ struct Grid {
   double cfn, cfn1;  // top-face extrapolation weights (rk_addtend_dry.py:282-288)
 };
 
+// The physics merge's w leaves (rk_addtend_dry; NULL = zero) for the w-face kernel.
+struct PhysW {
+  const double *rw_tendf, *w_save;
+  int rk1;
+};
+
 // A read-only view of a model state (the reference State leaves the step uses).
 struct StateR {
   const double *u, *v, *w, *theta, *p_total, *p_pert, *ph_total, *ph_pert, *mu_total, *mu_pert;

@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
                                                            const double *mub, const double *mut, const double *muts0,
                                                            const double *muu, const double *muv,
                                                            const double *base_w, int top_lid, int moist_cqw,
-                                                           int w_coriolis, WFaceOut o) {
+                                                           int w_coriolis, WFaceOut o, PhysW pw) {
   constexpr bool deg = DEG;  // the specified-boundary advection degradation
   using TQ = Tile<3, 3>;
   using TR = Tile<1, 0>;
@@ -505,6 +505,12 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, 
     w_t = ld(base_w, cw) * mass_f + adv;
   } else {
     w_t = adv;
+  }
+  if (pw.rw_tendf != nullptr || (pw.rk1 && pw.w_save != nullptr)) {
+    // rk_addtend_dry (rk_addtend_dry.py:490-546): w += (rw_tendf + [rk1] w_save msfty) / msfty
+    double r = (pw.rw_tendf != nullptr) ? ld(pw.rw_tendf, cw) : 0.0;
+    if (pw.rk1 && pw.w_save != nullptr) r = r + ld(pw.w_save, cw) * ld(g.msfty, c2d);
+    w_t = w_t + div_msf(r, g.msfty, g.rmsfty, c2d);
   }
   const double mub_c = ld(mub, c2d), mut_c = ld(mut, c2d);
   const double mu_prime = mut_c - mub_c;

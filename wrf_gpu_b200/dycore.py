@@ -290,8 +290,6 @@ def _unsupported(nl: OperationalNamelist, physics_tendencies) -> str | None:
         return "extra advected species of this mp_physics family are not built"
     if nl.acoustic_precision_mode != "fp64_default":
         return "acoustic_precision_mode other than fp64_default is not built"
-    if physics_tendencies is not None:
-        return "physics_tendencies (rk_addtend_dry merge) is not built"
     return None
 
 
@@ -331,13 +329,15 @@ def step_params(nl: OperationalNamelist) -> _capi.StepParams:
 class Stepper:
     """Prepared step for one namelist: params, metrics struct, workspace."""
 
-    def __init__(self, nl: OperationalNamelist, device="cuda"):
+    def __init__(self, nl: OperationalNamelist, device="cuda", physics: bool = False):
         reason = _unsupported(nl, None)
         if reason:
             raise NotImplementedError(reason)
         self.lib = _capi.load()
         self.nl = nl
         self.params = step_params(nl)
+        # a DryPhysicsTendencies bundle is merged into every stage (rk_addtend_dry)
+        self.params.physics = 1 if physics else 0
         _capi.check(self.lib.wrfgpu_step_params_validate(ctypes.byref(self.params)))
         nbytes = ctypes.c_size_t(0)
         _capi.check(self.lib.wrfgpu_step_workspace_size(ctypes.byref(self.params), ctypes.byref(nbytes)))
@@ -357,10 +357,17 @@ class Stepper:
                                 muts=e(s.mu_total), ph_tend=e(s.w), u_save=e(s.u), v_save=e(s.v), w_save=e(s.w),
                                 t_save=e(s.theta), ph_save=e(s.w), mu_save=e(s.mu_total), ww_save=e(s.w))
 
-    def _structs(self, carry: OperationalCarry, out: OperationalCarry):
-        """C input/output structs for one step from ``carry`` into ``out``."""
+    def _structs(self, carry: OperationalCarry, out: OperationalCarry, physics=None):
+        """C input/output structs for one step from ``carry`` into ``out``
+        (``physics``: a DryPhysicsTendencies-like bundle of device tensors,
+        None leaves = zero; only for a stepper built with ``physics=True``)."""
         s, o, nl = carry.state, out.state, self.nl
+        if physics is not None and not self.params.physics:
+            raise ValueError("physics tendencies given to a stepper built without physics=True")
         ins = _capi.StepInputs()
+        if physics is not None:
+            for leaf, field in zip(_capi.PHYSICS_LEAVES, _capi.PHYSICS_FIELDS):
+                setattr(ins, field, _ptr(getattr(physics, leaf, None)))
         for n in STATE_FIELDS:
             setattr(ins, n, _ptr(getattr(s, n)))
         have_q = s.qv is not None
@@ -389,9 +396,11 @@ class Stepper:
             setattr(outs, n, _ptr(getattr(out, n)))
         return ins, outs
 
-    def step_into(self, carry: OperationalCarry, out: OperationalCarry, lead_seconds=None, stream=None) -> None:
-        """Enqueue one step from ``carry`` into the preallocated ``out`` (no sync)."""
-        ins, outs = self._structs(carry, out)
+    def step_into(self, carry: OperationalCarry, out: OperationalCarry, lead_seconds=None, stream=None,
+                  physics=None) -> None:
+        """Enqueue one step from ``carry`` into the preallocated ``out`` (no sync);
+        ``physics`` as in ``rk_scan_step``."""
+        ins, outs = self._structs(carry, out, physics)
         lead = float("nan") if lead_seconds is None else float(lead_seconds)
         st = torch.cuda.current_stream() if stream is None else stream
         rc = self.lib.wrfgpu_rk3_step(ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(ins),
@@ -441,7 +450,7 @@ class BatchStepper:
         _capi.check(self.lib.wrfgpu_rk3_step_batched(n, P, M, I, O, L, W, B, ctypes.c_void_p(st.cuda_stream)))
 
 
-_STEPPERS: dict[int, Stepper] = {}
+_STEPPERS: dict[tuple, Stepper] = {}
 
 
 @dataclass
@@ -459,19 +468,25 @@ def rk_scan_step(carry: OperationalCarry, namelist: OperationalNamelist, *, debu
 
     Returns a new ``OperationalCarry``; ``carry`` is not modified.  The step is
     enqueued on the current CUDA stream and is not synchronised.
+    ``physics_tendencies`` is a DryPhysicsTendencies-like bundle
+    (dynamics/core/rk_addtend_dry.py:103-124: ru_tendf, rv_tendf, rw_tendf,
+    ph_tendf, t_tendf, mu_tendf, h_diabatic, u_save, v_save, w_save, ph_save,
+    t_save; float64 CUDA tensors, absent or None leaves are zero) merged into
+    every RK stage as rk_addtend_dry does.
     """
     reason = _unsupported(namelist, physics_tendencies)
     if reason:
         raise NotImplementedError(reason)
-    key = id(namelist)
+    with_physics = physics_tendencies is not None
+    key = (id(namelist), with_physics)
     stp = _STEPPERS.get(key)
     if stp is None or stp.nl is not namelist:
-        stp = Stepper(namelist, device=carry.state.u.device)
+        stp = Stepper(namelist, device=carry.state.u.device, physics=with_physics)
         _STEPPERS[key] = stp
     if carry.mudf is None:
         carry = carry.replace(mudf=torch.zeros_like(carry.state.mu_total))
     out = stp.alloc_carry(carry)
-    stp.step_into(carry, out, lead_seconds=lead_seconds)
+    stp.step_into(carry, out, lead_seconds=lead_seconds, physics=physics_tendencies)
     out.base_state = carry.base_state
     if debug:
         print("wrfgpu rk3 step: 3 stages, substeps", 1, max(1, namelist.acoustic_substeps // 2),
