@@ -203,6 +203,18 @@ def test_per_step_parity_physics_tendencies(cuda_ready, kind, leaves):
         assert not bad, f"{kind}/{leaves} step {n}: {bad}"
 
 
+@pytest.mark.parametrize("nx,ny,nz,specified", [(5, 3, 4, False), (33, 9, 7, False), (1, 6, 5, False),
+                                                 (7, 7, 5, True)])
+def test_per_step_parity_edge_shapes(cuda_ready, nx, ny, nz, specified):
+    """Grids smaller than one tile or column block, widths off every tile
+    multiple, the minimum 4 levels, a one-column-wide periodic slab and the
+    smallest specified domain that holds the five-row boundary strips."""
+    case = cases.real_like_moist(nx, ny, nz, hmax=300.0, specified=specified)
+    for n, e in enumerate(_per_step(case, 2)):
+        bad = {k: v for k, v in e.items() if not v <= _tol(k)}
+        assert not bad, f"{(nx, ny, nz, specified)} step {n}: {bad}"
+
+
 def test_per_step_parity_map_factors_periodic(cuda_ready):
     case = _with_map_factors(cases.real_like_moist(24, 20, 14, hmax=800.0, specified=False), seed=11)
     for n, e in enumerate(_per_step(case, 2)):
