@@ -307,18 +307,26 @@ int wrfgpu_acoustic_substep(const wrfgpu_step_params *params, const wrfgpu_metri
                             const wrfgpu_acoustic_consts *consts, wrfgpu_acoustic_work *x, double dts,
                             void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* Cotangents of the stage tendencies the substep reads (wrfgpu_acoustic_consts
+ * u_tend .. ph_tend, mu_tend), shaped like them; a NULL member is not
+ * computed. */
+typedef struct wrfgpu_acoustic_tend_cot {
+  double *u_tend, *v_tend, *t_tend, *rw_tend, *ph_tend, *mu_tend;
+} wrfgpu_acoustic_tend_cot;
+
 /* Its vector-Jacobian product at x: cot_in = J(x)^T cot_out, J the Jacobian of
  * wrfgpu_acoustic_substep with respect to the work state, constants fixed
  * and the drain limiter's scale held at its forward value (muave enters no
  * output of an updated column: its cot_in is zero there).  x_out is the substep's
  * output from x (a stored checkpoint); NULL recomputes it into the
- * workspace.  cot_out is read only; cot_in must not alias it.  No
+ * workspace.  cot_tend (may be NULL) receives the cotangents of the stage
+ * tendencies.  cot_out is read only; cot_in must not alias it.  No
  * counterpart in the reference, which has no differentiation. */
 int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
                                 const wrfgpu_acoustic_consts *consts, const wrfgpu_acoustic_work *x,
                                 const wrfgpu_acoustic_work *x_out, const wrfgpu_acoustic_work *cot_out,
-                                wrfgpu_acoustic_work *cot_in, double dts, void *workspace, size_t workspace_bytes,
-                                cudaStream_t stream);
+                                wrfgpu_acoustic_work *cot_in, wrfgpu_acoustic_tend_cot *cot_tend, double dts,
+                                void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);

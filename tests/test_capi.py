@@ -193,6 +193,7 @@ def test_acoustic_substep_rejects_before_any_launch(lib):
         assert lib.wrfgpu_acoustic_substep(ctypes.byref(p), ctypes.byref(m), ctypes.byref(c), ctypes.byref(x), 1.0,
                                            None, 0, None) == code
         assert lib.wrfgpu_acoustic_substep_vjp(ctypes.byref(p), ctypes.byref(m), ctypes.byref(c), ctypes.byref(x),
-                                               None, ctypes.byref(x), ctypes.byref(x), 1.0, None, 0, None) == code
+                                               None, ctypes.byref(x), ctypes.byref(x), None, 1.0, None, 0,
+                                               None) == code
     n = ctypes.c_size_t(0)
     assert lib.wrfgpu_acoustic_workspace_size(ctypes.byref(_params(lib)), ctypes.byref(n)) == 0 and n.value > 0

@@ -251,3 +251,47 @@ def test_checkpointed_loop_matches_chained_substeps(cuda_ready):
         g1, g2 = x1[n].grad, x2[n].grad
         scale = float(g1.abs().max()) or 1.0
         assert float((g1 - g2).abs().max()) <= 1.0e-12 * scale, n
+
+
+# C tendency-cotangent names -> oracle attribute names
+TENDS = {"u_tend": "u_tend", "v_tend": "v_tend", "t_tend": "theta_tend", "rw_tend": "rw_tend", "ph_tend": "ph_tend",
+         "mu_tend": "mu_tend"}
+
+
+@pytest.mark.parametrize("kind", ["moist_periodic", "lid_damped", "moist_specified"])
+def test_substep_vjp_tendency_cotangents(cuda_ready, kind):
+    """The cotangents of the stage tendencies against central differences of
+    the oracle's substep in each tendency (all together and one at a time)."""
+    case = _case(kind)
+    nl, a, dts, s = _stage(case, 3)
+    x = {cn: getattr(a, on).copy() for cn, on in WORK.items()}
+    op = _op(case, a, s, dts)
+    rng = np.random.default_rng(99)
+    y = _oracle_step(nl, a, dts, x)
+    spread = lambda f: float(np.std(f)) + 1.0e-3 * (float(np.max(np.abs(f))) + 1.0)
+    cot = {n: rng.standard_normal(y[n].shape) / spread(y[n]) for n in y}
+    ts = [torch.as_tensor(x[n], device="cuda") for n in _capi.ACOUSTIC_WORK_FIELDS]
+    cs = [torch.as_tensor(cot[n], device="cuda") for n in _capi.ACOUSTIC_WORK_FIELDS]
+    _, tc = op.vjp(ts, cs, tendencies=True)
+    torch.cuda.synchronize()
+    tc = {n: t.cpu().numpy() for n, t in tc.items()}
+    d = {n: rng.standard_normal(np.shape(getattr(a, on))) * spread(np.asarray(getattr(a, on)) + 1.0)
+         for n, on in TENDS.items()}
+    h = 1.0e-3
+
+    def jd(dd):
+        def step(sign):
+            b = D.copy_state(a)
+            for n, on in TENDS.items():
+                setattr(b, on, np.asarray(getattr(a, on)) + sign * h * dd[n])
+            return _oracle_step(nl, b, dts, x)
+        fp, fm = step(1.0), step(-1.0)
+        return {n: (fp[n] - fm[n]) / (2.0 * h) for n in fp}
+
+    floor = 8.0 * np.finfo(np.float64).eps / (2.0 * h) * sum(float(np.sum(np.abs(cot[n] * y[n]))) for n in y)
+    lhs, rhs = _dot(cot, jd(d)), sum(float(np.sum(tc[n] * d[n])) for n in d)
+    assert abs(lhs - rhs) <= 1.0e-8 * (abs(lhs) + abs(rhs)) + floor, (lhs, rhs)
+    for n in TENDS:
+        dn = {m: (d[m] if m == n else np.zeros_like(d[m])) for m in d}
+        lhs, rhs = _dot(cot, jd(dn)), float(np.sum(tc[n] * d[n]))
+        assert abs(lhs - rhs) <= 1.0e-8 * (abs(lhs) + abs(rhs)) + floor, (n, lhs, rhs, floor)

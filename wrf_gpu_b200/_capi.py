@@ -98,6 +98,13 @@ class AcousticConsts(ctypes.Structure):
     _fields_ = [(n, _P) for n in ACOUSTIC_CONST_FIELDS]
 
 
+ACOUSTIC_TEND_FIELDS = ("u_tend", "v_tend", "t_tend", "rw_tend", "ph_tend", "mu_tend")
+
+
+class AcousticTendCot(ctypes.Structure):
+    _fields_ = [(n, _P) for n in ACOUSTIC_TEND_FIELDS]
+
+
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
             "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace",
             "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_scalar_advection",
@@ -154,7 +161,8 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_acoustic_substep_vjp.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
                                                 ctypes.POINTER(AcousticConsts), ctypes.POINTER(AcousticWork),
                                                 ctypes.POINTER(AcousticWork), ctypes.POINTER(AcousticWork),
-                                                ctypes.POINTER(AcousticWork), _D, _P, ctypes.c_size_t, _P]
+                                                ctypes.POINTER(AcousticWork), ctypes.POINTER(AcousticTendCot), _D,
+                                                _P, ctypes.c_size_t, _P]
     lib.wrfgpu_acoustic_substep_vjp.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I

@@ -103,18 +103,25 @@ class AcousticOp:
             self.dts, ctypes.c_void_p(self.workspace.data_ptr()), self.workspace.numel(),
             ctypes.c_void_p(st.cuda_stream)))
 
-    def vjp(self, xs, cot_out, x_out=None):
+    def vjp(self, xs, cot_out, x_out=None, tendencies=False):
         """Cotangents of the 14 inputs ``xs`` from those of the outputs;
-        ``x_out`` (the substep's outputs from ``xs``) is recomputed if None."""
+        ``x_out`` (the substep's outputs from ``xs``) is recomputed if None.
+        With ``tendencies``, also returns the cotangents of the stage
+        tendencies (a dict over ``_capi.ACOUSTIC_TEND_FIELDS``)."""
         cot_in = [torch.empty_like(t) for t in xs]
         st = torch.cuda.current_stream(xs[0].device)
         x, co, ci = self._work(xs), self._work(cot_out), self._work(cot_in)
         xo = ctypes.byref(self._work(x_out)) if x_out is not None else None
+        tend, tc = None, None
+        if tendencies:
+            tend = {n: torch.empty_like(self.consts_t[n]) if n in self.consts_t
+                    else torch.empty_like(self.consts_t["mut"]) for n in _capi.ACOUSTIC_TEND_FIELDS}
+            tc = ctypes.byref(_capi.AcousticTendCot(*[dycore._ptr(tend[n]) for n in _capi.ACOUSTIC_TEND_FIELDS]))
         _capi.check(self.lib.wrfgpu_acoustic_substep_vjp(
             ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(self.consts), ctypes.byref(x),
-            xo, ctypes.byref(co), ctypes.byref(ci), self.dts, ctypes.c_void_p(self.workspace.data_ptr()),
+            xo, ctypes.byref(co), ctypes.byref(ci), tc, self.dts, ctypes.c_void_p(self.workspace.data_ptr()),
             self.workspace.numel(), ctypes.c_void_p(st.cuda_stream)))
-        return cot_in
+        return (cot_in, tend) if tendencies else cot_in
 
 
 class AcousticSubstep(torch.autograd.Function):

@@ -42,7 +42,13 @@ struct AdjScratch {
   double *gthw, *gtend, *gdv, *grhs, *gws, *gww;
 };
 
+// Cotangents of the stage tendencies (each nullable).
+struct AdjTend {
+  double *u_tend, *v_tend, *t_tend, *rw_tend, *ph_tend, *mu_tend;
+};
+
 struct AdjColArgs {
+  AdjTend tc;             // tendency cotangents out
   const double *x0_muts;  // input muts (the drain limiter's mu_work_old)
   const double *dvdxi;    // forward dvdxi (specified: the drain limiter's dmdt)
   const double *mu_tend;  // nullable
@@ -158,6 +164,7 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     gph += grhs;
     const double S = msfty * grhs / (ld(g.c1f, f) * mut + ld(g.c2f, f));
     gw += S * wfac;
+    if (q.tc.ph_tend != nullptr) q.tc.ph_tend[M(f)] = dts * S;
     gwd_f = (f < nz) ? -(S * dts * ld(g.fnm, f)) : 0.0;
     gwd_fm1 = (f < nz) ? -(S * dts * ld(g.fnp, f)) : 0.0;
   };
@@ -183,6 +190,7 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     q.ci.theta_w[c] = gthw;
     const double gtend = active ? -dts * msfty * gthw : 0.0;  // a frozen column keeps its theta
     s_tend[c] = gtend;
+    if (q.tc.t_tend != nullptr) q.tc.t_tend[c] = active ? msfty * dts * gthw : 0.0;
     if (!active) return;
     const double rdnw = ld(g.rdnw, k);
     if (k + 1 <= nz - 1) s_ww[M(k + 1)] += rdnw * gtend * (ld(g.fnm, k + 1) * T1(k + 1) + ld(g.fnp, k + 1) * t1);
@@ -206,6 +214,7 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     double P_lo = (m - 1 == 0) ? ph0 : 0.0;
     double B_lo = 0.0;
     double W_mid = 0.0;
+    if (q.tc.rw_tend != nullptr) q.tc.rw_tend[c] = (m <= nz - 1 || !q.col.top_lid) ? dts * gwn : 0.0;
     if (m <= nz - 1) {  // explicit w: wn = w + dts rw_tend + tA(rhs, ph) + tB(buoy, muave)
       W_mid = gwn;
       const double Q = minv * ld(q.cqw, c) * (c05dg * ld(g.rdn, m)) * gwn;
@@ -257,6 +266,8 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     wd_rev(0, gwd_fm1);
     q.ci.ph[M(0)] = P_mid;
     q.ci.w[M(0)] = 0.0;  // the surface w is a stage constant
+    if (q.tc.rw_tend != nullptr) q.tc.rw_tend[M(0)] = 0.0;
+    if (q.tc.ph_tend != nullptr) q.tc.ph_tend[M(0)] = 0.0;
     t2a_theta(0, B_mid, (nz - 1 == 0) ? gt2a_top : 0.0);
   }
 
@@ -271,6 +282,7 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
     q.ci.mudf[c2d] = ld(q.co.mudf, c2d);
     for (int f = 0; f <= nz; ++f) q.ci.ww[M(f)] = s_ww[M(f)];
     for (int k = 0; k < nz; ++k) s_dv[M(k)] = 0.0;
+    if (q.tc.mu_tend != nullptr) q.tc.mu_tend[c2d] = 0.0;
     return;
   }
   // the drain limiter's scale (dynamics/mu_t_advance.py:295-451), held fixed
@@ -313,6 +325,8 @@ __global__ void k_adj_column(Grid g, AdjColArgs q) {
   q.ci.ww[M(nz)] = s_ww[M(nz)];
   // dmdt = sum_k dnw(k) dvdxi(k)
   g_dmdt = scale * g_dmdt;
+  // mu_tend enters as dmdt does: (dmdt + mu_tend) scale and c1h dmdt + c1h mu_tend
+  if (q.tc.mu_tend != nullptr) q.tc.mu_tend[c2d] = g_dmdt;
   for (int k = 0; k < nz; ++k) s_dv[M(k)] += ld(g.dnw, k) * g_dmdt;
 }
 
@@ -375,6 +389,7 @@ __global__ void k_adj_faces(Grid g, AdjFaceArgs q) {
 }
 
 struct AdjUVArgs {
+  double *gu_tend, *gv_tend;  // u_tend / v_tend cotangents out (nullable)
   const double *gu, *gv;  // total cotangents of the advanced u, v
   const double *alt, *pb, *php, *cqu, *cqv, *muu, *muv;
   double *ci_p, *ci_ph, *ci_al, *ci_muts, *ci_mudf;  // accumulated with atomics
@@ -447,12 +462,14 @@ __global__ void k_adj_uv(Grid g, AdjUVArgs q) {
     const size_t cu = (size_t)k * ny * nxu + fu;
     const double msfr = div_msf(ld(g.msfux, fu), g.msfuy, g.rmsfuy, fu);
     face(oW, ld(q.gu, cu), ld(q.cqu, cu), msfr, c1 * ld(q.muu, fu) + c2, g.rdx, -EMDIV * g.dx * ld(g.rmsfuy, fu));
+    if (q.gu_tend != nullptr) q.gu_tend[cu] = q.dts * ld(q.gu, cu);
   }
   if (i < nx) {
     const int fv = j * nx + i;
     const size_t cv = (size_t)k * nyv * nx + fv;
     const double msfr = div_msf(ld(g.msfvy, fv), g.msfvx, g.rmsfvx, fv);
     face(oS, ld(q.gv, cv), ld(q.cqv, cv), msfr, c1 * ld(q.muv, fv) + c2, g.rdy, -EMDIV * g.dy * ld(g.rmsfvx, fv));
+    if (q.gv_tend != nullptr) q.gv_tend[cv] = q.dts * ld(q.gv, cv);
   }
 }
 

@@ -1274,8 +1274,9 @@ extern "C" int wrfgpu_acoustic_substep(const wrfgpu_step_params *p, const wrfgpu
 extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wrfgpu_metrics *m,
                                            const wrfgpu_acoustic_consts *c, const wrfgpu_acoustic_work *x,
                                            const wrfgpu_acoustic_work *x_out, const wrfgpu_acoustic_work *cot_out,
-                                           wrfgpu_acoustic_work *cot_in, double dts, void *workspace,
-                                           size_t workspace_bytes, cudaStream_t stream) {
+                                           wrfgpu_acoustic_work *cot_in, wrfgpu_acoustic_tend_cot *cot_tend,
+                                           double dts, void *workspace, size_t workspace_bytes,
+                                           cudaStream_t stream) {
   int rc = ac_check(p, m, c, workspace_bytes, workspace);
   if (rc) return rc;
   if (x == nullptr || cot_out == nullptr || cot_in == nullptr)
@@ -1323,6 +1324,9 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
     if (cudaMemsetAsync(ci[q], 0, n[q] * sizeof(double), stream) != cudaSuccess)
       return fail(WRFGPU_ERR_CUDA, "cotangent clear failed");
   AdjColArgs a{};
+  if (cot_tend != nullptr)
+    a.tc = AdjTend{cot_tend->u_tend, cot_tend->v_tend, cot_tend->t_tend, cot_tend->rw_tend, cot_tend->ph_tend,
+                   cot_tend->mu_tend};
   a.x0_muts = xin[11];
   a.dvdxi = L.dvdxi;
   a.mu_tend = c->mu_tend;
@@ -1341,7 +1345,8 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
   AdjFaceArgs fa{L.s.gtend, L.s.gdv, c->theta, co[0], co[1], ci[0], ci[1], ac_bdy(*p, *c, dts)};
   k_adj_faces<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, fa);
   if ((rc = check_launch("k_adj_faces"))) return rc;
-  AdjUVArgs ua{ci[0], ci[1], c->alt, c->pb, c->php, c->cqu, c->cqv, c->muu, c->muv,
+  AdjUVArgs ua{cot_tend != nullptr ? cot_tend->u_tend : nullptr, cot_tend != nullptr ? cot_tend->v_tend : nullptr,
+               ci[0], ci[1], c->alt, c->pb, c->php, c->cqu, c->cqv, c->muu, c->muv,
                ci[6], ci[3], ci[8], ci[11], ci[13], dts, p->top_lid};
   k_adj_uv<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, ua);
   if ((rc = check_launch("k_adj_uv"))) return rc;
