@@ -1732,3 +1732,112 @@ def stage_acoustic_state(carry, nl: Namelist, rk_step: int = 3, lead_seconds=Non
                                       dt_rk)
     a.a, a.alpha, a.gamma = calc_coef_w(prep.mut, m, dts, nl.epssm, nl.top_lid, a.cqw, prep.c2a)
     return a, dts, s, bdy
+
+
+# ---- end-of-step lateral boundaries (coupling/boundary_apply.py:154-326, 503-663) ----
+
+def _relax_row(field, forcing, side, b, z_len, side_len, wf, wg):
+    """boundary_apply.py:589-640: the relaxed row b of one side, from the
+    unmodified field and the leaf strips b-1, b, b+1 (tangential clamp)."""
+    if side == "W":
+        cur, te, ti = field[:, :, b], field[:, :, b - 1], field[:, :, b + 1]
+    elif side == "E":
+        x = field.shape[2] - 1 - b
+        cur, te, ti = field[:, :, x], field[:, :, x + 1], field[:, :, x - 1]
+    elif side == "S":
+        cur, te, ti = field[:, b, :], field[:, b - 1, :], field[:, b + 1, :]
+    else:
+        y = field.shape[1] - 1 - b
+        cur, te, ti = field[:, y, :], field[:, y + 1, :], field[:, y - 1, :]
+    fls0 = _strip(forcing, side, b, z_len, side_len) - cur
+    fls1 = _shift_clamp(fls0, +1, 1)
+    fls2 = _shift_clamp(fls0, -1, 1)
+    fls3 = _strip(forcing, side, b - 1, z_len, side_len) - te
+    fls4 = _strip(forcing, side, b + 1, z_len, side_len) - ti
+    lap = fls1 + fls2 + fls3 + fls4 - 4.0 * fls0
+    return cur + wf * fls0 - wg * lap
+
+
+def _apply_side_spec(field, forcing, side, spec_zone=1):
+    """boundary_apply.py:556-570: the outer spec_zone rows set to the strips."""
+    z_len, y_len, x_len = field.shape
+    out = field.copy()
+    for b in range(spec_zone):
+        if side == "W":
+            out[:, :, b] = _strip(forcing, side, b, z_len, y_len)
+        elif side == "E":
+            out[:, :, x_len - 1 - b] = _strip(forcing, side, b, z_len, y_len)
+        elif side == "S":
+            out[:, b, :] = _strip(forcing, side, b, z_len, x_len)
+        else:
+            out[:, y_len - 1 - b, :] = _strip(forcing, side, b, z_len, x_len)
+    return out
+
+
+def lbc_apply_3d(field, leaf, lead_seconds, dt_s, cadence, spec_zone=1, relax_zone=4):
+    """boundary_apply.py:503-525 (+ :622-663): every side's relax rows from the
+    unmodified field (W / E columns trimmed to rows [b+1, y_len-b-2], S / N
+    rows to columns [b, x_len-b-1]), then the spec rows (W, E, S, N)."""
+    forcing = interpolate_boundary_leaf(leaf, lead_seconds, cadence)
+    z_len, y_len, x_len = field.shape
+    out = field.copy()
+    for side in SIDES:
+        for b in range(spec_zone, relax_zone):
+            wf, wg = _wrf_relax_weights(b, dt_s, spec_zone, relax_zone)
+            if side in ("W", "E"):
+                row = _relax_row(field, forcing, side, b, z_len, y_len, wf, wg)
+                col = b if side == "W" else x_len - 1 - b
+                out[:, b + 1:y_len - b - 1, col] = row[:, b + 1:y_len - b - 1]
+            else:
+                row = _relax_row(field, forcing, side, b, z_len, x_len, wf, wg)
+                r = b if side == "S" else y_len - 1 - b
+                out[:, r, b:x_len - b] = row[:, b:x_len - b]
+    for side in SIDES:
+        out = _apply_side_spec(out, forcing, side, spec_zone)
+    return out
+
+
+def lbc_apply_3d_spec_only(field, leaf, lead_seconds, cadence, spec_zone=1):
+    """boundary_apply.py:154-167: the spec rows only."""
+    forcing = interpolate_boundary_leaf(leaf, lead_seconds, cadence)
+    out = field
+    for side in SIDES:
+        out = _apply_side_spec(out, forcing, side, spec_zone)
+    return out
+
+
+def apply_lateral_boundaries(s, lead_seconds, dt_s, nl: Namelist, dry_spec_only=False):
+    """``apply_lateral_boundaries`` (coupling/boundary_apply.py:170-326) on an
+    oracle state carrying the ``*_bdy`` leaves (u, v, w, theta, qv..qg, p, pb,
+    mu, mub, ph, phb); the moisture leaves are optional (absent: untouched)."""
+    cad = nl.update_cadence_s
+    a3 = lambda f, leaf: lbc_apply_3d(f, leaf, lead_seconds, dt_s, cad, nl.spec_zone, nl.relax_zone)
+    s3 = lambda f, leaf: lbc_apply_3d_spec_only(f, leaf, lead_seconds, cad, nl.spec_zone)
+    n = copy_state(s)
+    for q in MOIST_SPECIES:
+        leaf = getattr(s, q + "_bdy", None)
+        if leaf is not None:
+            setattr(n, q, np.maximum(a3(getattr(s, q), leaf), 0.0))
+    mub0 = (s.mu_total - s.mu_perturbation)[None]
+    phb0 = s.ph_total - s.ph_perturbation
+    if dry_spec_only:
+        n.u, n.v, n.theta = s3(s.u, s.u_bdy), s3(s.v, s.v_bdy), s3(s.theta, s.theta_bdy)
+        mu_p = s3(s.mu_perturbation[None], s.mu_bdy)[0]
+        mub = s3(mub0, s.mub_bdy)[0]
+        ph_p = s3(s.ph_perturbation, s.ph_bdy)
+        phb = s3(phb0, s.phb_bdy)
+        n.ph_total, n.ph_perturbation = phb + ph_p, ph_p
+        n.mu_total, n.mu_perturbation = mub + mu_p, mu_p
+        return n
+    n.u, n.v, n.w, n.theta = a3(s.u, s.u_bdy), a3(s.v, s.v_bdy), a3(s.w, s.w_bdy), a3(s.theta, s.theta_bdy)
+    p_p = a3(s.p_perturbation, s.p_bdy)
+    pb = a3(s.p_total - s.p_perturbation, s.pb_bdy)
+    mu_p = a3(s.mu_perturbation[None], s.mu_bdy)[0]
+    mub = a3(mub0, s.mub_bdy)[0]
+    if nl.force_geopotential:
+        ph_p = a3(s.ph_perturbation, s.ph_bdy)
+        phb = a3(phb0, s.phb_bdy)
+        n.ph_total, n.ph_perturbation = phb + ph_p, ph_p
+    n.p_total, n.p_perturbation = pb + p_p, p_p
+    n.mu_total, n.mu_perturbation = mub + mu_p, mu_p
+    return n
