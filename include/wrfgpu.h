@@ -328,6 +328,34 @@ int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *params, const wrfgpu_m
                                 wrfgpu_acoustic_work *cot_in, wrfgpu_acoustic_tend_cot *cot_tend, double dts,
                                 void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* Boundary strips of the end-of-step lateral boundary pass, each
+ * (ntime, 4, width, levels, side_len) like u_bdy (sides W, E, S, N): u, v,
+ * theta, the six moisture species (nz levels), w, ph' and phb (nz+1), p' and
+ * pb (nz), mu' and mub (1 level).  A NULL moisture strip leaves that species
+ * untouched. */
+typedef struct wrfgpu_lbc_leaves {
+  const double *u, *v, *w, *theta;
+  const double *q[WRFGPU_NMOIST];
+  const double *p, *pb, *mu, *mub, *ph, *phb;
+  int ntime, width, side_len;
+} wrfgpu_lbc_leaves;
+
+/* The end-of-step lateral boundary pass of a forecast step, replacing
+ * apply_lateral_boundaries(state, lead_seconds, dt_s, boundary_config,
+ * metrics, dry_spec_only=...) (coupling/boundary_apply.py:170-326): the
+ * state `in` (its 10 state leaves and moisture) with the strips at
+ * lead_seconds into `out` (the same leaves; out's carry pointers are not
+ * used; out must not alias in).  Full pass: u, v, w, theta, p', pb, mu', mub
+ * and (params.force_geopotential) ph', phb relaxed in the relax zone and set
+ * in the outer row (totals rebuilt as base + perturbation), moisture relaxed
+ * and clipped at zero.  dry_spec_only = 1 (the specified boundary cadence's
+ * pass): u, v, theta, mu', mub, ph', phb set in the outer row only, w and p
+ * untouched, moisture as in the full pass.  Reads params nx, ny, nz, dt,
+ * update_cadence_s, spec_zone = 1, relax_zone = 4, force_geopotential. */
+int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *params, const wrfgpu_step_inputs *in,
+                                    const wrfgpu_lbc_leaves *leaves, const wrfgpu_step_outputs *out,
+                                    double lead_seconds, int dry_spec_only, cudaStream_t stream);
+
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 

@@ -197,3 +197,13 @@ def test_acoustic_substep_rejects_before_any_launch(lib):
                                                None) == code
     n = ctypes.c_size_t(0)
     assert lib.wrfgpu_acoustic_workspace_size(ctypes.byref(_params(lib)), ctypes.byref(n)) == 0 and n.value > 0
+
+
+def test_lateral_boundary_pass_rejects_before_any_launch(lib):
+    ins, outs, lv = _capi.StepInputs(), _capi.StepOutputs(), _capi.LbcLeaves()
+    assert lib.wrfgpu_apply_lateral_boundaries(ctypes.byref(_params(lib)), ctypes.byref(ins), ctypes.byref(lv),
+                                               ctypes.byref(outs), 0.0, 0, None) == _capi.WRFGPU_ERR_NULL_POINTER
+    assert lib.wrfgpu_apply_lateral_boundaries(ctypes.byref(_params(lib)), ctypes.byref(ins), ctypes.byref(lv),
+                                               ctypes.byref(outs), float("nan"), 0,
+                                               None) == _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG
+    assert lib.wrfgpu_apply_lateral_boundaries(None, None, None, None, 0.0, 0, None) == _capi.WRFGPU_ERR_NULL_POINTER

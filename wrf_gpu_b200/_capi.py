@@ -105,11 +105,16 @@ class AcousticTendCot(ctypes.Structure):
     _fields_ = [(n, _P) for n in ACOUSTIC_TEND_FIELDS]
 
 
+class LbcLeaves(ctypes.Structure):
+    _fields_ = [("u", _P), ("v", _P), ("w", _P), ("theta", _P), ("q", _P * 6), ("p", _P), ("pb", _P), ("mu", _P),
+                ("mub", _P), ("ph", _P), ("phb", _P), ("ntime", _I), ("width", _I), ("side_len", _I)]
+
+
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
             "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace",
             "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_scalar_advection",
             "wrfgpu_scalar_advection_adjoint", "wrfgpu_acoustic_workspace_size", "wrfgpu_acoustic_substep",
-            "wrfgpu_acoustic_substep_vjp", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_acoustic_substep_vjp", "wrfgpu_apply_lateral_boundaries", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version")
 
@@ -164,6 +169,10 @@ def load(path: str | os.PathLike | None = None):
                                                 ctypes.POINTER(AcousticWork), ctypes.POINTER(AcousticTendCot), _D,
                                                 _P, ctypes.c_size_t, _P]
     lib.wrfgpu_acoustic_substep_vjp.restype = _I
+    lib.wrfgpu_apply_lateral_boundaries.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(StepInputs),
+                                                    ctypes.POINTER(LbcLeaves), ctypes.POINTER(StepOutputs), _D, _I,
+                                                    _P]
+    lib.wrfgpu_apply_lateral_boundaries.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

@@ -25,6 +25,7 @@
 #include "acoustic_adjoint.cuh"
 #include "bdy_cadence.cuh"
 #include "physics_merge.cuh"
+#include "lbc.cuh"
 
 using namespace wg;
 
@@ -1350,6 +1351,109 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
                ci[6], ci[3], ci[8], ci[11], ci[13], dts, p->top_lid};
   k_adj_uv<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, ua);
   if ((rc = check_launch("k_adj_uv"))) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The end-of-step lateral boundary pass.
+// ---------------------------------------------------------------------------
+extern "C" int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *p, const wrfgpu_step_inputs *in,
+                                               const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out,
+                                               double lead_seconds, int dry_spec_only, cudaStream_t stream) {
+  if (p == nullptr || in == nullptr || lv == nullptr || out == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "params/inputs/leaves/outputs is NULL");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  if (p->spec_zone != 1 || p->relax_zone != 4)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "boundary zones other than spec_zone=1, relax_zone=4 are not built");
+  if (!std::isfinite(lead_seconds)) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "lead_seconds must be finite");
+  const double *req_in[] = {in->u, in->v, in->w, in->theta, in->p_total, in->p_perturbation, in->ph_total,
+                            in->ph_perturbation, in->mu_total, in->mu_perturbation};
+  double *req_out[] = {out->u, out->v, out->w, out->theta, out->p_total, out->p_perturbation, out->ph_total,
+                       out->ph_perturbation, out->mu_total, out->mu_perturbation};
+  for (int k = 0; k < 10; ++k)
+    if (req_in[k] == nullptr || req_out[k] == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "a state pointer is NULL");
+  const bool geo = p->force_geopotential != 0;
+  const double *need[] = {lv->u, lv->v, lv->theta, lv->mu, lv->mub, lv->ph, lv->phb};
+  for (const double *q : need)
+    if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "the u, v, theta, mu, mub, ph and phb strips are needed");
+  if (!dry_spec_only && (lv->w == nullptr || lv->p == nullptr || lv->pb == nullptr))
+    return fail(WRFGPU_ERR_NULL_POINTER, "the full pass needs the w, p and pb strips");
+  if (lv->ntime < 1 || lv->width < 1 || lv->side_len < (p->nx > p->ny ? p->nx + 1 : p->ny + 1))
+    return fail(WRFGPU_ERR_BAD_SHAPE, "strips must be (ntime >= 1, 4, width >= 1, levels, side_len >= max(nx, ny) + 1)");
+  for (int s = 0; s < 6; ++s)
+    if (lv->q[s] != nullptr && (in->q[s] == nullptr || out->q[s] == nullptr))
+      return fail(WRFGPU_ERR_NULL_POINTER, "a forced moisture species needs its input and output");
+  const int nx = p->nx, ny = p->ny, nz = p->nz;
+  // strips at the lead (boundary_apply.py:329-345)
+  const int mx = lv->ntime - 1;
+  const double li = lead_seconds / p->update_cadence_s;
+  int lo = (int)std::floor(li);
+  lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
+  int hi = lo + 1 > mx ? mx : lo + 1;
+  double al = li - (double)lo;
+  al = al < 0.0 ? 0.0 : (al > 1.0 ? 1.0 : al);
+  auto leaf = [&](const double *x) { return BdyLeaf{x, lv->ntime, lv->width, lv->side_len, lo, hi, al}; };
+  // dt*fcx, dt*gcx of the relax rows (boundary_apply.py:666-688, spec_exp 0)
+  LbcJob base{};
+  for (int b = 1; b <= 3; ++b) {
+    const double dt = p->dt;
+    const double linear = (double)(p->spec_zone + p->relax_zone - (b + 1)) / (double)(p->relax_zone - 1);
+    const double fcx = 0.1 / dt * (linear > 0.0 ? linear : 0.0) * 1.0;
+    const double gcx = 1.0 / dt / 50.0 * (linear > 0.0 ? linear : 0.0) * 1.0;
+    base.wf[b] = dt * fcx;
+    base.wg[b] = dt * gcx;
+  }
+  auto run = [&](const double *x, const double *x2, double *o, double *o2, const double *l1, const double *l2, int zl,
+                 int yl, int xl, int relax, int clamp) -> int {
+    LbcJob a = base;
+    a.x = x; a.x2 = x2; a.out = o; a.out2 = o2;
+    a.leaf = leaf(l1);
+    a.leaf2 = leaf(l2 != nullptr ? l2 : l1);
+    a.zl = zl; a.yl = yl; a.xl = xl;
+    a.relax = relax; a.clamp = clamp;
+    k_lbc_field<<<grd(xl, yl, zl), blk2(), 0, stream>>>(a);
+    return check_launch("k_lbc_field");
+  };
+  auto copy = [&](double *o, const double *x, size_t n) -> int {
+    if (cudaMemcpyAsync(o, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "boundary pass copy failed");
+    return WRFGPU_OK;
+  };
+  const Dims d = dims_of(*p);
+  const int full = dry_spec_only ? 0 : 1;
+  if ((rc = run(in->u, nullptr, out->u, nullptr, lv->u, nullptr, nz, ny, nx + 1, full, 0))) return rc;
+  if ((rc = run(in->v, nullptr, out->v, nullptr, lv->v, nullptr, nz, ny + 1, nx, full, 0))) return rc;
+  if ((rc = run(in->theta, nullptr, out->theta, nullptr, lv->theta, nullptr, nz, ny, nx, full, 0))) return rc;
+  if (full) {
+    if ((rc = run(in->w, nullptr, out->w, nullptr, lv->w, nullptr, nz + 1, ny, nx, 1, 0))) return rc;
+    if ((rc = run(in->p_total, in->p_perturbation, out->p_total, out->p_perturbation, lv->p, lv->pb, nz, ny, nx, 1,
+                  0)))
+      return rc;
+  } else {  // the cadence's pass forces neither w nor p
+    if ((rc = copy(out->w, in->w, d.w)) || (rc = copy(out->p_total, in->p_total, d.m)) ||
+        (rc = copy(out->p_perturbation, in->p_perturbation, d.m)))
+      return rc;
+  }
+  if ((rc = run(in->mu_total, in->mu_perturbation, out->mu_total, out->mu_perturbation, lv->mu, lv->mub, 1, ny, nx,
+                full, 0)))
+    return rc;
+  if (geo || dry_spec_only) {
+    if ((rc = run(in->ph_total, in->ph_perturbation, out->ph_total, out->ph_perturbation, lv->ph, lv->phb, nz + 1, ny,
+                  nx, full, 0)))
+      return rc;
+  } else {  // the nested child's geopotential is left to the dynamics
+    if ((rc = copy(out->ph_total, in->ph_total, d.w)) || (rc = copy(out->ph_perturbation, in->ph_perturbation, d.w)))
+      return rc;
+  }
+  for (int s = 0; s < 6; ++s) {
+    if (lv->q[s] != nullptr) {
+      if ((rc = run(in->q[s], nullptr, out->q[s], nullptr, lv->q[s], nullptr, nz, ny, nx, 1, 1))) return rc;
+    } else if (in->q[s] != nullptr && out->q[s] != nullptr && (rc = copy(out->q[s], in->q[s], d.m))) {
+      return rc;
+    }
+  }
   g_last_error.clear();
   return WRFGPU_OK;
 }

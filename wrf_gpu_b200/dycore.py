@@ -29,7 +29,8 @@ from . import _capi
 
 MOIST = ("qv", "qc", "qr", "qi", "qs", "qg")
 STATE_FIELDS = _capi.STATE_FIELDS
-_LEAVES = ("u_bdy", "v_bdy", "theta_bdy", "ph_bdy", "mu_bdy", "w_bdy")
+_LEAVES = ("u_bdy", "v_bdy", "theta_bdy", "ph_bdy", "mu_bdy", "w_bdy", "qv_bdy", "qc_bdy", "qr_bdy", "qi_bdy",
+           "qs_bdy", "qg_bdy", "p_bdy", "pb_bdy", "mub_bdy", "phb_bdy")
 CARRY_FIELDS = _capi.CARRY_OUT_FIELDS
 METRIC_ARRAYS = _capi.METRIC_FIELDS
 
@@ -120,6 +121,17 @@ class State:
     ph_bdy: torch.Tensor | None = None
     mu_bdy: torch.Tensor | None = None
     w_bdy: torch.Tensor | None = None
+    # further strips of the end-of-step lateral boundary pass
+    qv_bdy: torch.Tensor | None = None
+    qc_bdy: torch.Tensor | None = None
+    qr_bdy: torch.Tensor | None = None
+    qi_bdy: torch.Tensor | None = None
+    qs_bdy: torch.Tensor | None = None
+    qg_bdy: torch.Tensor | None = None
+    p_bdy: torch.Tensor | None = None
+    pb_bdy: torch.Tensor | None = None
+    mub_bdy: torch.Tensor | None = None
+    phb_bdy: torch.Tensor | None = None
 
     @property
     def p(self):
@@ -500,3 +512,51 @@ def carry_from_case(case, device="cuda") -> OperationalCarry:
     st = State.from_host(case.state, device)
     c = initial_operational_carry(st)
     return c.replace(mudf=_dev(case.mudf, device))
+
+
+def apply_lateral_boundaries(state: State, lead_seconds, dt_s: float, config: BoundaryConfig | None = None,
+                             metrics=None, *, dry_spec_only: bool = False) -> State:
+    """Drop-in for ``apply_lateral_boundaries`` (coupling/boundary_apply.py:170-326),
+    the forecast step's end-of-step lateral boundary pass, through
+    ``wrfgpu_apply_lateral_boundaries``: the state's ``*_bdy`` strips at
+    ``lead_seconds`` relax the boundary band and set the outer row (or, with
+    ``dry_spec_only``, set the outer row only).  Returns a new State (the
+    strips carried over); enqueued on the current stream, not synchronised.
+    ``metrics`` is accepted for the reference's signature and not needed."""
+    del metrics
+    cfg = BoundaryConfig() if config is None else config
+    lib = _capi.load()
+    nz, ny, nx = state.theta.shape
+    p = _capi.StepParams()
+    lib.wrfgpu_step_params_init(ctypes.byref(p))
+    p.nx, p.ny, p.nz, p.dx, p.dy, p.dt = nx, ny, nz, 1.0, 1.0, float(dt_s)
+    p.spec_zone, p.relax_zone = int(cfg.spec_zone), int(cfg.relax_zone)
+    p.update_cadence_s = float(cfg.update_cadence_s)
+    p.force_geopotential = int(bool(cfg.force_geopotential))
+    out = State(**{f_.name: (torch.empty_like(getattr(state, f_.name)) if getattr(state, f_.name) is not None
+                             and f_.name not in _LEAVES else getattr(state, f_.name)) for f_ in fields(State)})
+    ins, outs = _capi.StepInputs(), _capi.StepOutputs()
+    for n in STATE_FIELDS:
+        setattr(ins, n, _ptr(getattr(state, n)))
+        setattr(outs, n, _ptr(getattr(out, n)))
+    for k_, n in enumerate(MOIST):
+        ins.q[k_], outs.q[k_] = _ptr(getattr(state, n)), _ptr(getattr(out, n))
+    lv = _capi.LbcLeaves()
+    lv.u, lv.v, lv.w, lv.theta = _ptr(state.u_bdy), _ptr(state.v_bdy), _ptr(state.w_bdy), _ptr(state.theta_bdy)
+    for k_, n in enumerate(MOIST):
+        lv.q[k_] = _ptr(getattr(state, n + "_bdy"))
+    lv.p, lv.pb, lv.mu, lv.mub = _ptr(state.p_bdy), _ptr(state.pb_bdy), _ptr(state.mu_bdy), _ptr(state.mub_bdy)
+    lv.ph, lv.phb = _ptr(state.ph_bdy), _ptr(state.phb_bdy)
+    lv.ntime, _, lv.width, _, lv.side_len = state.u_bdy.shape
+    levels = dict(w_bdy=nz + 1, ph_bdy=nz + 1, phb_bdy=nz + 1, mu_bdy=1, mub_bdy=1)
+    for n in _LEAVES:
+        t = getattr(state, n)
+        if t is not None and tuple(t.shape) != (lv.ntime, 4, lv.width, levels.get(n, nz), lv.side_len):
+            raise ValueError(f"{n} has shape {tuple(t.shape)}, expected "
+                             f"{(lv.ntime, 4, lv.width, levels.get(n, nz), lv.side_len)}")
+    lead = float(lead_seconds)
+    st = torch.cuda.current_stream(state.u.device)
+    _capi.check(lib.wrfgpu_apply_lateral_boundaries(ctypes.byref(p), ctypes.byref(ins), ctypes.byref(lv),
+                                                     ctypes.byref(outs), lead, int(bool(dry_spec_only)),
+                                                     ctypes.c_void_p(st.cuda_stream)))
+    return out
