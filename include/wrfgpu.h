@@ -356,6 +356,41 @@ int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *params, const wrfg
                                     const wrfgpu_lbc_leaves *leaves, const wrfgpu_step_outputs *out,
                                     double lead_seconds, int dry_spec_only, cudaStream_t stream);
 
+/* The theta limiter's record (the dict of
+ * _positive_definite_theta_increment_limiter, runtime/operational_mode.py:
+ * 1444-1454): offending cells, the first one as [x, y, z] ([-1, -1, -1] when
+ * none), and the mass-weighted theta integral before and after. */
+typedef struct wrfgpu_theta_limiter_diag {
+  int limited_cell_count;
+  int first_limited_cell_xyz[3];
+  double mass_before, mass_after, mass_residual;
+} wrfgpu_theta_limiter_diag;
+
+/* Workspace bytes of wrfgpu_step_epilogue for these params. */
+int wrfgpu_step_epilogue_workspace_size(const wrfgpu_step_params *params, size_t *bytes);
+
+/* The forecast step after _rk_scan_step, without physics, replacing
+ * runtime/operational_mode.py:4950-4983 of
+ * _physics_boundary_step_with_limiter_diagnostics: `next` is the step's
+ * output state, `origin` the step-start state (physical_origin), `out` the
+ * new state (must not alias `next` or `origin`).
+ * Guards on (disable_guards = 0): the theta increment limiter weighted by
+ * next's mu_total, the dry-mass guard and the mixing-ratio guard of every
+ * moisture species against origin (_limit_guarded_dynamics_state_with_
+ * diagnostics, _valid_mixing_ratio); then, when params.run_boundary, the
+ * end-of-step boundary pass (as wrfgpu_apply_lateral_boundaries, with
+ * dry_spec_only = the specified boundary cadence is active) followed by the
+ * finite guard of u, v, w, theta, p, p', ph, ph', the mixing-ratio guard of
+ * qv and the dry-mass guard, all against origin.  Guards off: the boundary
+ * pass alone (or a copy).  `leaves` is read only when params.run_boundary.
+ * `diag` (device memory, may be NULL) receives the limiter's record (the
+ * empty record with guards off).  Enqueued on `stream`; allocates nothing. */
+int wrfgpu_step_epilogue(const wrfgpu_step_params *params, const wrfgpu_step_inputs *origin,
+                         const wrfgpu_step_inputs *next, const wrfgpu_lbc_leaves *leaves,
+                         const wrfgpu_step_outputs *out, double lead_seconds, int disable_guards,
+                         wrfgpu_theta_limiter_diag *diag, void *workspace, size_t workspace_bytes,
+                         cudaStream_t stream);
+
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 

@@ -1841,3 +1841,144 @@ def apply_lateral_boundaries(s, lead_seconds, dt_s, nl: Namelist, dry_spec_only=
     n.p_total, n.p_perturbation = pb + p_p, p_p
     n.mu_total, n.mu_perturbation = mub + mu_p, mu_p
     return n
+
+
+# ----------------------------------------------------------------------------
+# post-step guards (runtime/operational_mode.py:1300-1520, 4950-4983)
+# ----------------------------------------------------------------------------
+
+THETA_LIMITER_MIN_K = 0.0     # operational_mode.py:180
+THETA_LIMITER_MAX_K = 1000.0  # operational_mode.py:198
+MIXING_RATIO_MAX = 0.05       # operational_mode.py:1300
+
+
+def valid_mixing_ratio(candidate, origin, upper=MIXING_RATIO_MAX):
+    """``_valid_mixing_ratio`` (operational_mode.py:1300-1306)."""
+    c = np.asarray(candidate, dtype=np.float64)
+    with np.errstate(invalid="ignore"):
+        ok = np.isfinite(c) & (c >= 0.0) & (c <= upper)
+    return np.where(ok, c, origin)
+
+
+def finite_or_origin(candidate, origin):
+    """``_finite_or_origin`` (operational_mode.py:1309-1314)."""
+    c = np.asarray(candidate, dtype=np.float64)
+    return np.where(np.isfinite(c), c, origin)
+
+
+def theta_mass_weights(theta, mu_total):
+    """``_theta_mass_weights`` (operational_mode.py:1317-1323)."""
+    m = np.asarray(mu_total, dtype=np.float64)
+    with np.errstate(invalid="ignore"):
+        m = np.where(np.isfinite(m) & (m > 0.0), m, 0.0)
+    return np.broadcast_to(m[None], np.shape(theta))
+
+
+def first_limited_cell_xyz(mask):
+    """``_first_limited_cell_xyz`` (operational_mode.py:1342-1357): the first
+    True cell in (z, y, x) order as [x, y, z], or [-1, -1, -1]."""
+    flat = np.flatnonzero(np.ravel(mask))
+    if flat.size == 0:
+        return np.array([-1, -1, -1], dtype=np.int32)
+    z, rem = divmod(int(flat[0]), mask.shape[1] * mask.shape[2])
+    y, x = divmod(rem, mask.shape[2])
+    return np.array([x, y, z], dtype=np.int32)
+
+
+def empty_theta_limiter_diagnostics():
+    """``_empty_theta_limiter_diagnostics`` (operational_mode.py:1374-1384)."""
+    return {"theta_limited_cell_count": 0, "theta_first_limited_cell_xyz": np.array([-1, -1, -1], dtype=np.int32),
+            "theta_mass_before": 0.0, "theta_mass_after": 0.0, "theta_mass_residual": 0.0}
+
+
+def theta_increment_limiter(candidate, origin, mass, minimum_k=THETA_LIMITER_MIN_K, maximum_k=THETA_LIMITER_MAX_K,
+                            lower_bound=None, upper_bound=None):
+    """``_positive_definite_theta_increment_limiter`` (operational_mode.py:
+    1387-1455): offending cells (non-finite, above ``upper`` or below
+    ``lower``) keep the RK direction with the increment scaled into the
+    interval; the removed mass-weighted increment is spread over every cell in
+    proportion to its room, so the domain integral of theta * mass is kept."""
+    c = np.asarray(candidate, dtype=np.float64)
+    o = np.asarray(origin, dtype=np.float64)
+    m = np.asarray(mass, dtype=np.float64)
+    lower = np.float64(minimum_k)
+    upper = np.float64(maximum_k)
+    if lower_bound is not None:
+        lower = np.maximum(lower, np.asarray(lower_bound, dtype=np.float64))
+    if upper_bound is not None:
+        upper = np.minimum(upper, np.asarray(upper_bound, dtype=np.float64))
+    upper = np.maximum(upper, lower)
+    mid = 0.5 * (lower + upper)
+    safe_o = np.where(np.isfinite(o), o, mid)
+    safe_o = np.minimum(np.maximum(safe_o, lower), upper)
+    fc = np.where(np.isfinite(c), c, safe_o)
+    raw = fc - safe_o
+    mask = ~np.isfinite(c) | (fc > upper) | (fc < lower)
+    pos, neg = raw > 0.0, raw < 0.0
+    ua = (upper - safe_o) / np.where(pos, raw, 1.0)
+    la = (lower - safe_o) / np.where(neg, raw, -1.0)
+    alpha = np.where(pos, ua, np.where(neg, la, 1.0))
+    alpha = np.where(mask, np.minimum(np.maximum(alpha, 0.0), 1.0), 1.0)
+    lim0 = safe_o + alpha * raw
+    target = np.sum(fc * m)
+    mass0 = np.sum(lim0 * m)
+    residual = target - mass0
+    room = np.where(residual >= 0.0, upper - lim0, lim0 - lower)
+    cap = np.sum(room * m)
+    frac = min(abs(residual) / cap, 1.0) if cap > 0.0 else 0.0
+    lim = lim0 + np.sign(residual) * frac * room
+    lim = np.minimum(np.maximum(lim, lower), upper)
+    after = np.sum(lim * m)
+    diag = {"theta_limited_cell_count": int(mask.sum()), "theta_first_limited_cell_xyz": first_limited_cell_xyz(mask),
+            "theta_mass_before": float(target), "theta_mass_after": float(after),
+            "theta_mass_residual": float(after - target)}
+    return lim, diag
+
+
+def limit_guarded_mass_state(candidate, origin):
+    """``_limit_guarded_mass_state`` (operational_mode.py:1458-1470): dry mass
+    that is non-finite or below 1 Pa falls back to the origin's (total and
+    perturbation together)."""
+    mt, mp = np.asarray(candidate.mu_total), np.asarray(candidate.mu_perturbation)
+    with np.errstate(invalid="ignore"):
+        ok = np.isfinite(mt) & np.isfinite(mp) & (mt >= 1.0)
+    n = copy_state(candidate)
+    n.mu_total = np.where(ok, mt, origin.mu_total)
+    n.mu_perturbation = np.where(ok, mp, origin.mu_perturbation)
+    return n
+
+
+def limit_guarded_dynamics_state(candidate, origin):
+    """``_limit_guarded_dynamics_state_with_diagnostics`` (operational_mode.py:
+    1473-1512): the theta limiter weighted by the candidate's column mass, then
+    the dry-mass guard."""
+    mass = theta_mass_weights(candidate.theta, candidate.mu_total)
+    theta, diag = theta_increment_limiter(candidate.theta, origin.theta, mass)
+    n = copy_state(candidate)
+    n.theta = theta
+    return limit_guarded_mass_state(n, origin), diag
+
+
+def step_epilogue(next_state, origin, lead_seconds, dt_s, nl, run_boundary, disable_guards=False,
+                  dry_spec_only=False):
+    """The forecast step after ``_rk_scan_step`` without physics
+    (operational_mode.py:4950-4983): the dynamics guards (theta limiter,
+    dry-mass guard, every moisture species checked against the origin), the
+    end-of-step lateral boundary pass, then the finite / mixing-ratio /
+    dry-mass guards of the bounded state.  Returns (state, diagnostics)."""
+    s, diag = next_state, empty_theta_limiter_diagnostics()
+    if not disable_guards:
+        s, diag = limit_guarded_dynamics_state(s, origin)
+        for q in MOIST_SPECIES:
+            setattr(s, q, valid_mixing_ratio(getattr(s, q), getattr(origin, q)))
+    if run_boundary:
+        b = apply_lateral_boundaries(s, lead_seconds, dt_s, nl, dry_spec_only=dry_spec_only)
+        if disable_guards:
+            s = b
+        else:
+            s = copy_state(b)
+            for f in ("u", "v", "w", "theta", "p_total", "ph_total", "p_perturbation", "ph_perturbation"):
+                setattr(s, f, finite_or_origin(getattr(b, f), getattr(origin, f)))
+            s.qv = valid_mixing_ratio(b.qv, origin.qv)
+            s = limit_guarded_mass_state(s, origin)
+    return s, diag

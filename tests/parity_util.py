@@ -53,3 +53,17 @@ def compare(gpu_carry, ora_carry, keys_state=STATE_KEYS, keys_carry=CARRY_KEYS):
             continue
         out[k] = rel_err(g.cpu().numpy(), o)
     return out
+
+
+def attach_lbc_leaves(s, rng, moist=("qv", "qc", "qr")):
+    """Drifting random strips (2 times) for the leaves a real-like case does
+    not carry (p, pb, mub, phb) and for ``moist`` (a few negatives, for the
+    clip); shapes (2, 4, 5, levels, side_len)."""
+    nz = s.theta.shape[0]
+    side = s.u_bdy.shape[-1]
+    leaf = lambda z, mean, sc: mean + sc * rng.standard_normal((2, 4, 5, z, side))
+    s.p_bdy, s.pb_bdy = leaf(nz, 0.0, 40.0), leaf(nz, 5.0e4, 100.0)
+    s.mub_bdy, s.phb_bdy = leaf(1, 9.0e4, 50.0), leaf(nz + 1, 2.0e4, 20.0)
+    for q in moist:
+        setattr(s, q + "_bdy", np.abs(leaf(nz, 1.0e-3, 1.0e-3)) - 2.0e-4)
+    return s

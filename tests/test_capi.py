@@ -207,3 +207,14 @@ def test_lateral_boundary_pass_rejects_before_any_launch(lib):
                                                ctypes.byref(outs), float("nan"), 0,
                                                None) == _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG
     assert lib.wrfgpu_apply_lateral_boundaries(None, None, None, None, 0.0, 0, None) == _capi.WRFGPU_ERR_NULL_POINTER
+
+
+def test_step_epilogue_rejects_before_any_launch(lib):
+    p = _params(lib)
+    n = ctypes.c_size_t(0)
+    assert lib.wrfgpu_step_epilogue_workspace_size(ctypes.byref(p), ctypes.byref(n)) == 0 and n.value > 0
+    ins, org, outs = _capi.StepInputs(), _capi.StepInputs(), _capi.StepOutputs()
+    assert lib.wrfgpu_step_epilogue(None, None, None, None, None, 0.0, 0, None, None, 0,
+                                    None) == _capi.WRFGPU_ERR_NULL_POINTER
+    assert lib.wrfgpu_step_epilogue(ctypes.byref(p), ctypes.byref(org), ctypes.byref(ins), None, ctypes.byref(outs),
+                                    0.0, 0, None, None, 0, None) == _capi.WRFGPU_ERR_NULL_POINTER

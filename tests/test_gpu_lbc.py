@@ -27,18 +27,11 @@ def _state(seed=8):
     case = cases.real_like_moist(30, 22, 10, hmax=800.0, specified=True, bdy_noise=True)
     s = D.copy_state(case.state)
     rng = np.random.default_rng(seed)
-    nz, ny, nx = s.theta.shape
-    side = s.u_bdy.shape[-1]
     for f, sc in (("u", 0.5), ("v", 0.5), ("w", 0.1), ("theta", 0.3), ("p_perturbation", 30.0),
                   ("ph_perturbation", 5.0)):
         setattr(s, f, getattr(s, f) + sc * rng.standard_normal(getattr(s, f).shape))
     s.mu_perturbation = s.mu_perturbation + 20.0 * rng.standard_normal(s.mu_perturbation.shape)
-    leaf = lambda z, mean, sc: mean + sc * rng.standard_normal((2, 4, 5, z, side))
-    s.p_bdy, s.pb_bdy = leaf(nz, 0.0, 40.0), leaf(nz, 5.0e4, 100.0)
-    s.mub_bdy, s.phb_bdy = leaf(1, 9.0e4, 50.0), leaf(nz + 1, 2.0e4, 20.0)
-    for q in ("qv", "qc", "qr"):
-        setattr(s, q + "_bdy", np.abs(leaf(nz, 1.0e-3, 1.0e-3)) - 2.0e-4)  # a few negatives for the clip
-    return case, s
+    return case, P.attach_lbc_leaves(s, rng)
 
 
 @pytest.mark.parametrize("geo,spec_only", [(True, False), (False, False), (True, True)])

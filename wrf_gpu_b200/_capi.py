@@ -110,11 +110,16 @@ class LbcLeaves(ctypes.Structure):
                 ("mub", _P), ("ph", _P), ("phb", _P), ("ntime", _I), ("width", _I), ("side_len", _I)]
 
 
+# wrfgpu_theta_limiter_diag: 4 int32 (count, x, y, z) then 3 float64 (mass before, after, residual)
+THETA_DIAG_BYTES = 40
+
+
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
             "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace",
             "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_scalar_advection",
             "wrfgpu_scalar_advection_adjoint", "wrfgpu_acoustic_workspace_size", "wrfgpu_acoustic_substep",
-            "wrfgpu_acoustic_substep_vjp", "wrfgpu_apply_lateral_boundaries", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_acoustic_substep_vjp", "wrfgpu_apply_lateral_boundaries",
+            "wrfgpu_step_epilogue_workspace_size", "wrfgpu_step_epilogue", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version")
 
@@ -173,6 +178,12 @@ def load(path: str | os.PathLike | None = None):
                                                     ctypes.POINTER(LbcLeaves), ctypes.POINTER(StepOutputs), _D, _I,
                                                     _P]
     lib.wrfgpu_apply_lateral_boundaries.restype = _I
+    lib.wrfgpu_step_epilogue_workspace_size.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_size_t)]
+    lib.wrfgpu_step_epilogue_workspace_size.restype = _I
+    lib.wrfgpu_step_epilogue.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(StepInputs),
+                                         ctypes.POINTER(StepInputs), ctypes.POINTER(LbcLeaves),
+                                         ctypes.POINTER(StepOutputs), _D, _I, _P, _P, ctypes.c_size_t, _P]
+    lib.wrfgpu_step_epilogue.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

@@ -1358,43 +1358,63 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
 // ---------------------------------------------------------------------------
 // The end-of-step lateral boundary pass.
 // ---------------------------------------------------------------------------
-extern "C" int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *p, const wrfgpu_step_inputs *in,
-                                               const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out,
-                                               double lead_seconds, int dry_spec_only, cudaStream_t stream) {
-  if (p == nullptr || in == nullptr || lv == nullptr || out == nullptr)
-    return fail(WRFGPU_ERR_NULL_POINTER, "params/inputs/leaves/outputs is NULL");
+namespace {
+
+// The state and strip checks shared by the boundary pass and the epilogue.
+int epilogue_check(const wrfgpu_step_params *p, const wrfgpu_step_inputs *in, const wrfgpu_lbc_leaves *lv,
+                   const wrfgpu_step_outputs *out, bool boundary, bool spec_only, double lead_seconds) {
   int rc = wrfgpu_step_params_validate(p);
   if (rc) return rc;
-  if (p->spec_zone != 1 || p->relax_zone != 4)
+  if (boundary && (p->spec_zone != 1 || p->relax_zone != 4))
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "boundary zones other than spec_zone=1, relax_zone=4 are not built");
-  if (!std::isfinite(lead_seconds)) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "lead_seconds must be finite");
+  if (boundary && !std::isfinite(lead_seconds))
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "lead_seconds must be finite");
   const double *req_in[] = {in->u, in->v, in->w, in->theta, in->p_total, in->p_perturbation, in->ph_total,
                             in->ph_perturbation, in->mu_total, in->mu_perturbation};
   double *req_out[] = {out->u, out->v, out->w, out->theta, out->p_total, out->p_perturbation, out->ph_total,
                        out->ph_perturbation, out->mu_total, out->mu_perturbation};
-  for (int k = 0; k < 10; ++k)
+  for (int k = 0; k < 10; ++k) {
     if (req_in[k] == nullptr || req_out[k] == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "a state pointer is NULL");
-  const bool geo = p->force_geopotential != 0;
+    if ((const double *)req_out[k] == req_in[k]) return fail(WRFGPU_ERR_BAD_SHAPE, "out must not alias the input state");
+  }
+  for (int s = 0; s < 6; ++s)
+    if ((in->q[s] == nullptr) != (out->q[s] == nullptr))
+      return fail(WRFGPU_ERR_NULL_POINTER, "a moisture species needs both its input and its output");
+  if (!boundary) return WRFGPU_OK;
+  if (lv == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "the boundary pass needs the strips");
   const double *need[] = {lv->u, lv->v, lv->theta, lv->mu, lv->mub, lv->ph, lv->phb};
   for (const double *q : need)
     if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "the u, v, theta, mu, mub, ph and phb strips are needed");
-  if (!dry_spec_only && (lv->w == nullptr || lv->p == nullptr || lv->pb == nullptr))
+  if (!spec_only && (lv->w == nullptr || lv->p == nullptr || lv->pb == nullptr))
     return fail(WRFGPU_ERR_NULL_POINTER, "the full pass needs the w, p and pb strips");
   if (lv->ntime < 1 || lv->width < 1 || lv->side_len < (p->nx > p->ny ? p->nx + 1 : p->ny + 1))
     return fail(WRFGPU_ERR_BAD_SHAPE, "strips must be (ntime >= 1, 4, width >= 1, levels, side_len >= max(nx, ny) + 1)");
   for (int s = 0; s < 6; ++s)
-    if (lv->q[s] != nullptr && (in->q[s] == nullptr || out->q[s] == nullptr))
+    if (lv->q[s] != nullptr && in->q[s] == nullptr)
       return fail(WRFGPU_ERR_NULL_POINTER, "a forced moisture species needs its input and output");
+  return WRFGPU_OK;
+}
+
+// One launch per field (or a copy where nothing touches it): the boundary
+// pass (when `boundary`) with the guards fused before and after it (when
+// `guards`; `gs` / `after` are the theta limiter's scalars and partials).
+int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, const wrfgpu_step_inputs *in,
+                    const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out, double lead_seconds, bool guards,
+                    bool boundary, bool spec_only, const GuardScalars *gs, double *after, cudaStream_t stream) {
   const int nx = p->nx, ny = p->ny, nz = p->nz;
-  // strips at the lead (boundary_apply.py:329-345)
-  const int mx = lv->ntime - 1;
-  const double li = lead_seconds / p->update_cadence_s;
-  int lo = (int)std::floor(li);
-  lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
-  int hi = lo + 1 > mx ? mx : lo + 1;
-  double al = li - (double)lo;
-  al = al < 0.0 ? 0.0 : (al > 1.0 ? 1.0 : al);
-  auto leaf = [&](const double *x) { return BdyLeaf{x, lv->ntime, lv->width, lv->side_len, lo, hi, al}; };
+  BdyLeaf nolf{};
+  auto leaf = [&](const double *x) -> BdyLeaf {
+    if (!boundary || x == nullptr) return nolf;
+    // strips at the lead (boundary_apply.py:329-345)
+    const int mx = lv->ntime - 1;
+    const double li = lead_seconds / p->update_cadence_s;
+    int lo = (int)std::floor(li);
+    lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
+    const int hi = lo + 1 > mx ? mx : lo + 1;
+    double al = li - (double)lo;
+    al = al < 0.0 ? 0.0 : (al > 1.0 ? 1.0 : al);
+    return BdyLeaf{x, lv->ntime, lv->width, lv->side_len, lo, hi, al};
+  };
   // dt*fcx, dt*gcx of the relax rows (boundary_apply.py:666-688, spec_exp 0)
   LbcJob base{};
   for (int b = 1; b <= 3; ++b) {
@@ -1405,54 +1425,173 @@ extern "C" int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *p, cons
     base.wf[b] = dt * fcx;
     base.wg[b] = dt * gcx;
   }
-  auto run = [&](const double *x, const double *x2, double *o, double *o2, const double *l1, const double *l2, int zl,
-                 int yl, int xl, int relax, int clamp) -> int {
+  const int ring = boundary ? (spec_only ? 1 : 2) : 0;
+  const int post_fin = (guards && boundary) ? GUARD_FINITE : GUARD_NONE;
+  auto copy = [&](double *o, const double *x, size_t n) -> int {
+    if (o == x) return WRFGPU_OK;
+    if (cudaMemcpyAsync(o, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "epilogue copy failed");
+    return WRFGPU_OK;
+  };
+  // one field: x (x2: a pair's perturbation) into o (o2), levels zl, extent yl x xl
+  auto run = [&](const double *x, const double *x2, double *o, double *o2, const double *o_org, const double *o_org2,
+                 const double *l1, const double *l2, int zl, int yl, int xl, int rg, int pre, int post,
+                 int clamp) -> int {
+    const size_t n = (size_t)zl * yl * xl;
+    if (rg == 0 && pre == GUARD_NONE && post == GUARD_NONE) {
+      int rc = copy(o, x, n);
+      if (!rc && x2 != nullptr) rc = copy(o2, x2, n);
+      return rc;
+    }
     LbcJob a = base;
     a.x = x; a.x2 = x2; a.out = o; a.out2 = o2;
     a.leaf = leaf(l1);
     a.leaf2 = leaf(l2 != nullptr ? l2 : l1);
     a.zl = zl; a.yl = yl; a.xl = xl;
-    a.relax = relax; a.clamp = clamp;
+    a.ring = rg; a.clamp = clamp;
+    a.pre = pre; a.post = post;
+    a.org = o_org; a.org2 = o_org2;
+    a.mu_next = in->mu_total;
+    a.gs = gs;
+    a.after = after;
     k_lbc_field<<<grd(xl, yl, zl), blk2(), 0, stream>>>(a);
     return check_launch("k_lbc_field");
   };
-  auto copy = [&](double *o, const double *x, size_t n) -> int {
-    if (cudaMemcpyAsync(o, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
-      return fail(WRFGPU_ERR_CUDA, "boundary pass copy failed");
-    return WRFGPU_OK;
-  };
-  const Dims d = dims_of(*p);
-  const int full = dry_spec_only ? 0 : 1;
-  if ((rc = run(in->u, nullptr, out->u, nullptr, lv->u, nullptr, nz, ny, nx + 1, full, 0))) return rc;
-  if ((rc = run(in->v, nullptr, out->v, nullptr, lv->v, nullptr, nz, ny + 1, nx, full, 0))) return rc;
-  if ((rc = run(in->theta, nullptr, out->theta, nullptr, lv->theta, nullptr, nz, ny, nx, full, 0))) return rc;
-  if (full) {
-    if ((rc = run(in->w, nullptr, out->w, nullptr, lv->w, nullptr, nz + 1, ny, nx, 1, 0))) return rc;
-    if ((rc = run(in->p_total, in->p_perturbation, out->p_total, out->p_perturbation, lv->p, lv->pb, nz, ny, nx, 1,
-                  0)))
-      return rc;
-  } else {  // the cadence's pass forces neither w nor p
-    if ((rc = copy(out->w, in->w, d.w)) || (rc = copy(out->p_total, in->p_total, d.m)) ||
-        (rc = copy(out->p_perturbation, in->p_perturbation, d.m)))
-      return rc;
-  }
-  if ((rc = run(in->mu_total, in->mu_perturbation, out->mu_total, out->mu_perturbation, lv->mu, lv->mub, 1, ny, nx,
-                full, 0)))
+  const bool geo = p->force_geopotential != 0;
+  const wrfgpu_step_inputs *O = org;
+  const double *nul = nullptr;
+  int rc;
+  if ((rc = run(in->u, nul, out->u, nullptr, O ? O->u : nul, nul, lv ? lv->u : nul, nul, nz, ny, nx + 1, ring,
+                GUARD_NONE, post_fin, 0)))
     return rc;
-  if (geo || dry_spec_only) {
-    if ((rc = run(in->ph_total, in->ph_perturbation, out->ph_total, out->ph_perturbation, lv->ph, lv->phb, nz + 1, ny,
-                  nx, full, 0)))
-      return rc;
-  } else {  // the nested child's geopotential is left to the dynamics
-    if ((rc = copy(out->ph_total, in->ph_total, d.w)) || (rc = copy(out->ph_perturbation, in->ph_perturbation, d.w)))
+  if ((rc = run(in->v, nul, out->v, nullptr, O ? O->v : nul, nul, lv ? lv->v : nul, nul, nz, ny + 1, nx, ring,
+                GUARD_NONE, post_fin, 0)))
+    return rc;
+  // WRF's specified cadence leaves w and p to the step (boundary_apply.py:217-220, 290)
+  const int ring_wp = spec_only ? 0 : ring;
+  if ((rc = run(in->w, nul, out->w, nullptr, O ? O->w : nul, nul, lv ? lv->w : nul, nul, nz + 1, ny, nx, ring_wp,
+                GUARD_NONE, post_fin, 0)))
+    return rc;
+  if ((rc = run(in->theta, nul, out->theta, nullptr, O ? O->theta : nul, nul, lv ? lv->theta : nul, nul, nz, ny, nx,
+                ring, guards ? GUARD_THETA : GUARD_NONE, post_fin, 0)))
+    return rc;
+  if ((rc = run(in->p_total, in->p_perturbation, out->p_total, out->p_perturbation, O ? O->p_total : nul,
+                O ? O->p_perturbation : nul, lv ? lv->p : nul, lv ? lv->pb : nul, nz, ny, nx, ring_wp, GUARD_NONE,
+                post_fin, 0)))
+    return rc;
+  if ((rc = run(in->mu_total, in->mu_perturbation, out->mu_total, out->mu_perturbation, O ? O->mu_total : nul,
+                O ? O->mu_perturbation : nul, lv ? lv->mu : nul, lv ? lv->mub : nul, 1, ny, nx, ring,
+                guards ? GUARD_MASS : GUARD_NONE, (guards && boundary) ? GUARD_MASS : GUARD_NONE, 0)))
+    return rc;
+  // the nested child's geopotential is left to the dynamics (boundary_apply.py:270-307)
+  const int ring_ph = (geo || spec_only) ? ring : 0;
+  if ((rc = run(in->ph_total, in->ph_perturbation, out->ph_total, out->ph_perturbation, O ? O->ph_total : nul,
+                O ? O->ph_perturbation : nul, lv ? lv->ph : nul, lv ? lv->phb : nul, nz + 1, ny, nx, ring_ph,
+                GUARD_NONE, post_fin, 0)))
+    return rc;
+  for (int s = 0; s < 6; ++s) {
+    if (in->q[s] == nullptr) continue;
+    const bool forced = boundary && lv->q[s] != nullptr;
+    const int post = (s == 0 && guards && boundary) ? GUARD_RATIO : GUARD_NONE;
+    if ((rc = run(in->q[s], nul, out->q[s], nullptr, O ? O->q[s] : nul, nul, forced ? lv->q[s] : nul, nul, nz, ny, nx,
+                  forced ? 2 : 0, guards ? GUARD_RATIO : GUARD_NONE, post, forced ? 1 : 0)))
       return rc;
   }
-  for (int s = 0; s < 6; ++s) {
-    if (lv->q[s] != nullptr) {
-      if ((rc = run(in->q[s], nullptr, out->q[s], nullptr, lv->q[s], nullptr, nz, ny, nx, 1, 1))) return rc;
-    } else if (in->q[s] != nullptr && out->q[s] != nullptr && (rc = copy(out->q[s], in->q[s], d.m))) {
-      return rc;
-    }
+  return WRFGPU_OK;
+}
+
+// Workspace layout of wrfgpu_step_epilogue.
+struct EpilogueWs {
+  size_t scalars, partials, after, total;
+  int nparts, nafter;
+};
+
+EpilogueWs epilogue_ws(const wrfgpu_step_params &p) {
+  EpilogueWs w{};
+  const long long n = (long long)p.nz * p.ny * p.nx;
+  const long long want = (n + GUARD_THREADS - 1) / GUARD_THREADS;
+  w.nparts = (int)(want < 148 * 8 ? (want < 1 ? 1 : want) : 148 * 8);
+  const dim3 g = grd(p.nx, p.ny, p.nz);
+  w.nafter = (int)(g.x * g.y * g.z);
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  w.scalars = 0;
+  w.partials = up(sizeof(GuardScalars));
+  w.after = w.partials + up((size_t)w.nparts * sizeof(GuardPartial));
+  w.total = w.after + up((size_t)w.nafter * sizeof(double));
+  return w;
+}
+
+}  // namespace
+
+extern "C" int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *p, const wrfgpu_step_inputs *in,
+                                               const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out,
+                                               double lead_seconds, int dry_spec_only, cudaStream_t stream) {
+  if (p == nullptr || in == nullptr || lv == nullptr || out == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "params/inputs/leaves/outputs is NULL");
+  int rc = epilogue_check(p, in, lv, out, true, dry_spec_only != 0, lead_seconds);
+  if (rc) return rc;
+  rc = epilogue_fields(p, nullptr, in, lv, out, lead_seconds, false, true, dry_spec_only != 0, nullptr, nullptr,
+                       stream);
+  if (rc) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_step_epilogue_workspace_size(const wrfgpu_step_params *p, size_t *bytes) {
+  if (p == nullptr || bytes == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/bytes is NULL");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  *bytes = epilogue_ws(*p).total;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_step_epilogue(const wrfgpu_step_params *p, const wrfgpu_step_inputs *origin,
+                                    const wrfgpu_step_inputs *next, const wrfgpu_lbc_leaves *lv,
+                                    const wrfgpu_step_outputs *out, double lead_seconds, int disable_guards,
+                                    wrfgpu_theta_limiter_diag *diag, void *ws, size_t ws_bytes, cudaStream_t stream) {
+  if (p == nullptr || next == nullptr || out == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/next/out is NULL");
+  const bool guards = disable_guards == 0;
+  const bool boundary = p->run_boundary != 0;
+  // _specified_bdy_cadence_active (operational_mode.py:2478-2491)
+  const bool spec_only = boundary && !p->bc_ideal && p->force_geopotential && p->specified_bdy_cadence;
+  int rc = epilogue_check(p, next, lv, out, boundary, spec_only, lead_seconds);
+  if (rc) return rc;
+  if (guards) {
+    if (origin == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "the guards need the origin state");
+    const double *req[] = {origin->u, origin->v, origin->w, origin->theta, origin->p_total, origin->p_perturbation,
+                           origin->ph_total, origin->ph_perturbation, origin->mu_total, origin->mu_perturbation};
+    for (const double *q : req)
+      if (q == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "an origin state pointer is NULL");
+    for (int s = 0; s < 6; ++s)
+      if (next->q[s] != nullptr && origin->q[s] == nullptr)
+        return fail(WRFGPU_ERR_NULL_POINTER, "a guarded moisture species needs its origin");
+  }
+  const EpilogueWs w = epilogue_ws(*p);
+  if (guards && (ws == nullptr || ws_bytes < w.total || ((uintptr_t)ws & 255) != 0))
+    return fail(WRFGPU_ERR_WORKSPACE, "workspace is NULL, too small or not 256-byte aligned");
+  GuardScalars *gs = nullptr;
+  double *after = nullptr;
+  if (guards) {
+    char *base = (char *)ws;
+    gs = (GuardScalars *)(base + w.scalars);
+    GuardPartial *part = (GuardPartial *)(base + w.partials);
+    after = (double *)(base + w.after);
+    k_guard_reduce<<<w.nparts, GUARD_THREADS, 0, stream>>>(next->theta, origin->theta, next->mu_total, p->nz, p->ny,
+                                                           p->nx, part);
+    if ((rc = check_launch("k_guard_reduce"))) return rc;
+    k_guard_finalize<<<1, GUARD_THREADS, 0, stream>>>(part, w.nparts, gs);
+    if ((rc = check_launch("k_guard_finalize"))) return rc;
+  }
+  rc = epilogue_fields(p, guards ? origin : nullptr, next, lv, out, lead_seconds, guards, boundary, spec_only, gs,
+                       after, stream);
+  if (rc) return rc;
+  if (diag != nullptr) {
+    if (guards)
+      k_guard_diag<<<1, GUARD_THREADS, 0, stream>>>(after, w.nafter, gs, p->ny, p->nx, diag);
+    else
+      k_guard_diag_empty<<<1, 1, 0, stream>>>(diag);
+    if ((rc = check_launch("k_guard_diag"))) return rc;
   }
   g_last_error.clear();
   return WRFGPU_OK;

@@ -246,6 +246,7 @@ class OperationalNamelist:
     run_physics: bool = True
     run_boundary: bool = True
     bc_source: str = "ideal"
+    disable_guards: bool = False
     boundary_config: BoundaryConfig = field(default_factory=BoundaryConfig)
     use_vertical_solver: bool = True
     w_damping: int = 0
@@ -514,6 +515,46 @@ def carry_from_case(case, device="cuda") -> OperationalCarry:
     return c.replace(mudf=_dev(case.mudf, device))
 
 
+def _state_structs(state: State):
+    """The state's leaves as a wrfgpu_step_inputs, and a fresh State (the
+    strips carried over) with its wrfgpu_step_outputs."""
+    out = State(**{f_.name: (torch.empty_like(getattr(state, f_.name)) if getattr(state, f_.name) is not None
+                             and f_.name not in _LEAVES else getattr(state, f_.name)) for f_ in fields(State)})
+    outs = _capi.StepOutputs()
+    for n in STATE_FIELDS:
+        setattr(outs, n, _ptr(getattr(out, n)))
+    for k_, n in enumerate(MOIST):
+        outs.q[k_] = _ptr(getattr(out, n))
+    return _inputs_struct(state), out, outs
+
+
+def _inputs_struct(state: State) -> _capi.StepInputs:
+    ins = _capi.StepInputs()
+    for n in STATE_FIELDS:
+        setattr(ins, n, _ptr(getattr(state, n)))
+    for k_, n in enumerate(MOIST):
+        ins.q[k_] = _ptr(getattr(state, n))
+    return ins
+
+
+def _leaves_struct(state: State) -> _capi.LbcLeaves:
+    nz = state.theta.shape[0]
+    lv = _capi.LbcLeaves()
+    lv.u, lv.v, lv.w, lv.theta = _ptr(state.u_bdy), _ptr(state.v_bdy), _ptr(state.w_bdy), _ptr(state.theta_bdy)
+    for k_, n in enumerate(MOIST):
+        lv.q[k_] = _ptr(getattr(state, n + "_bdy"))
+    lv.p, lv.pb, lv.mu, lv.mub = _ptr(state.p_bdy), _ptr(state.pb_bdy), _ptr(state.mu_bdy), _ptr(state.mub_bdy)
+    lv.ph, lv.phb = _ptr(state.ph_bdy), _ptr(state.phb_bdy)
+    lv.ntime, _, lv.width, _, lv.side_len = state.u_bdy.shape
+    levels = dict(w_bdy=nz + 1, ph_bdy=nz + 1, phb_bdy=nz + 1, mu_bdy=1, mub_bdy=1)
+    for n in _LEAVES:
+        t = getattr(state, n)
+        if t is not None and tuple(t.shape) != (lv.ntime, 4, lv.width, levels.get(n, nz), lv.side_len):
+            raise ValueError(f"{n} has shape {tuple(t.shape)}, expected "
+                             f"{(lv.ntime, 4, lv.width, levels.get(n, nz), lv.side_len)}")
+    return lv
+
+
 def apply_lateral_boundaries(state: State, lead_seconds, dt_s: float, config: BoundaryConfig | None = None,
                              metrics=None, *, dry_spec_only: bool = False) -> State:
     """Drop-in for ``apply_lateral_boundaries`` (coupling/boundary_apply.py:170-326),
@@ -533,30 +574,48 @@ def apply_lateral_boundaries(state: State, lead_seconds, dt_s: float, config: Bo
     p.spec_zone, p.relax_zone = int(cfg.spec_zone), int(cfg.relax_zone)
     p.update_cadence_s = float(cfg.update_cadence_s)
     p.force_geopotential = int(bool(cfg.force_geopotential))
-    out = State(**{f_.name: (torch.empty_like(getattr(state, f_.name)) if getattr(state, f_.name) is not None
-                             and f_.name not in _LEAVES else getattr(state, f_.name)) for f_ in fields(State)})
-    ins, outs = _capi.StepInputs(), _capi.StepOutputs()
-    for n in STATE_FIELDS:
-        setattr(ins, n, _ptr(getattr(state, n)))
-        setattr(outs, n, _ptr(getattr(out, n)))
-    for k_, n in enumerate(MOIST):
-        ins.q[k_], outs.q[k_] = _ptr(getattr(state, n)), _ptr(getattr(out, n))
-    lv = _capi.LbcLeaves()
-    lv.u, lv.v, lv.w, lv.theta = _ptr(state.u_bdy), _ptr(state.v_bdy), _ptr(state.w_bdy), _ptr(state.theta_bdy)
-    for k_, n in enumerate(MOIST):
-        lv.q[k_] = _ptr(getattr(state, n + "_bdy"))
-    lv.p, lv.pb, lv.mu, lv.mub = _ptr(state.p_bdy), _ptr(state.pb_bdy), _ptr(state.mu_bdy), _ptr(state.mub_bdy)
-    lv.ph, lv.phb = _ptr(state.ph_bdy), _ptr(state.phb_bdy)
-    lv.ntime, _, lv.width, _, lv.side_len = state.u_bdy.shape
-    levels = dict(w_bdy=nz + 1, ph_bdy=nz + 1, phb_bdy=nz + 1, mu_bdy=1, mub_bdy=1)
-    for n in _LEAVES:
-        t = getattr(state, n)
-        if t is not None and tuple(t.shape) != (lv.ntime, 4, lv.width, levels.get(n, nz), lv.side_len):
-            raise ValueError(f"{n} has shape {tuple(t.shape)}, expected "
-                             f"{(lv.ntime, 4, lv.width, levels.get(n, nz), lv.side_len)}")
-    lead = float(lead_seconds)
+    ins, out, outs = _state_structs(state)
+    lv = _leaves_struct(state)
     st = torch.cuda.current_stream(state.u.device)
     _capi.check(lib.wrfgpu_apply_lateral_boundaries(ctypes.byref(p), ctypes.byref(ins), ctypes.byref(lv),
-                                                     ctypes.byref(outs), lead, int(bool(dry_spec_only)),
-                                                     ctypes.c_void_p(st.cuda_stream)))
+                                                     ctypes.byref(outs), float(lead_seconds),
+                                                     int(bool(dry_spec_only)), ctypes.c_void_p(st.cuda_stream)))
     return out
+
+
+def theta_limiter_diagnostics(raw: torch.Tensor) -> dict:
+    """The limiter record (``wrfgpu_theta_limiter_diag``, 40 bytes on the
+    device) as the reference's dict of device scalars
+    (operational_mode.py:1444-1454)."""
+    ints, dbl = raw[:16].view(torch.int32), raw[16:].view(torch.float64)
+    return {"theta_limited_cell_count": ints[0], "theta_first_limited_cell_xyz": ints[1:4],
+            "theta_mass_before": dbl[0], "theta_mass_after": dbl[1], "theta_mass_residual": dbl[2]}
+
+
+def step_epilogue(next_state: State, origin: State, lead_seconds, nl: OperationalNamelist):
+    """The forecast step after ``_rk_scan_step`` without physics
+    (runtime/operational_mode.py:4950-4983), through ``wrfgpu_step_epilogue``:
+    unless ``nl.disable_guards``, the theta increment limiter, dry-mass and
+    mixing-ratio guards against ``origin`` (the step-start state); with
+    ``nl.run_boundary`` the end-of-step lateral boundary pass (ring 0 only
+    when the specified boundary cadence is active) and the guards of the
+    bounded state.  Returns (State, limiter diagnostics); enqueued on the
+    current stream, not synchronised."""
+    lib = _capi.load()
+    p = step_params(nl)
+    dev = next_state.u.device
+    n = ctypes.c_size_t(0)
+    _capi.check(lib.wrfgpu_step_epilogue_workspace_size(ctypes.byref(p), ctypes.byref(n)))
+    ws = torch.empty(n.value + 256, dtype=torch.uint8, device=dev)
+    wsp = (ws.data_ptr() + 255) // 256 * 256
+    raw = torch.empty(_capi.THETA_DIAG_BYTES, dtype=torch.uint8, device=dev)
+    ins, out, outs = _state_structs(next_state)
+    org = _inputs_struct(origin)
+    lv = _leaves_struct(next_state) if nl.run_boundary else None
+    st = torch.cuda.current_stream(dev)
+    _capi.check(lib.wrfgpu_step_epilogue(ctypes.byref(p), ctypes.byref(org), ctypes.byref(ins),
+                                         None if lv is None else ctypes.byref(lv), ctypes.byref(outs),
+                                         float(lead_seconds), int(bool(nl.disable_guards)),
+                                         ctypes.c_void_p(raw.data_ptr()), ctypes.c_void_p(wsp), n.value,
+                                         ctypes.c_void_p(st.cuda_stream)))
+    return out, theta_limiter_diagnostics(raw)
