@@ -22,7 +22,9 @@ Prints ONE JSON line (rank 0).  Beside the float64 step it also times the
 mixed-precision variant (FP32 advective fluxes, float64 accumulation) on the
 same input and reports it under "mixed" (skip with --no-mixed), and the
 cost of the two hand-written adjoints against their forwards at the same grid
-under "adjoint" (skip with --no-adjoint).  ``--impl reference`` times the reference
+under "adjoint" (skip with --no-adjoint), and the step epilogue (guards and
+the end-of-step lateral boundary pass) under "epilogue" (skip with
+--no-epilogue).  ``--impl reference`` times the reference
 algorithm's CPU implementation available here -- the NumPy restatement in
 ``oracle/`` (JAX, the reference's own runtime, is not installed) -- on the
 host cores, on bounded 64 x 64 x 50 samples of the same workload.
@@ -429,6 +431,7 @@ def run_gpu(args, rank, world, local_rank):
                                       "serial_value": replica_throughput(serial_ms, world, cells, nsub, k_e2e)},
                 launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed,
                 adjoint=adjoint_ratios(case, dev) if not args.no_adjoint else None,
+                epilogue=epilogue_cost(case, dev) if not args.no_epilogue else None,
                 tuned={"march_levels": tuned[0], "column_lanes": tuned[1], "column_width": tuned[2]})
 
 
@@ -499,6 +502,67 @@ def adjoint_ratios(case, dev, reps=10):
             "data": "operator inputs synthesised from the workload state"}
 
 
+def epilogue_cost(case, dev, reps=20):
+    """The step epilogue (guards, full end-of-step boundary pass, guards of the
+    bounded state; ``wrfgpu_step_epilogue``) on the workload's state, timed
+    with CUDA events over ``reps`` calls.  The strips the workload does not
+    carry (p, pb, mub, phb, qv) are synthesised from its own (timing does not
+    depend on the values).  Algorithmic bytes: every state field (u, v, w,
+    theta, p and p', ph and ph', mu and mu', six species) read once and
+    written once, plus the limiter's reduction pass (theta, origin theta and
+    mu_total) and the origin theta read again where theta is written; the
+    guards' origin reads on offending cells and the strips (0.2 % of it) are
+    not counted."""
+    import ctypes
+
+    import torch
+    from wrf_gpu_b200 import _capi, dycore
+    st = dycore.State.from_host(case.state, device=dev)
+    nz, ny, nx = st.theta.shape
+    tb = st.theta_bdy
+    st.p_bdy, st.pb_bdy, st.qv_bdy = torch.zeros_like(tb), torch.full_like(tb, 5.0e4), torch.full_like(tb, 1.0e-3)
+    st.mub_bdy, st.phb_bdy = torch.full_like(st.mu_bdy, 9.0e4), torch.full_like(st.ph_bdy, 2.0e4)
+    nl = dycore.OperationalNamelist.from_case(case, device=dev, run_boundary=True, bc_source="wrfbdy",
+                                              specified_bdy_cadence=False)
+    lib = _capi.load()
+    p = dycore.step_params(nl)
+    n = ctypes.c_size_t(0)
+    _capi.check(lib.wrfgpu_step_epilogue_workspace_size(ctypes.byref(p), ctypes.byref(n)))
+    ws = torch.empty(n.value + 256, dtype=torch.uint8, device=dev)
+    wsp = ctypes.c_void_p((ws.data_ptr() + 255) // 256 * 256)
+    raw = torch.empty(_capi.THETA_DIAG_BYTES, dtype=torch.uint8, device=dev)
+    ins, out, outs = dycore._state_structs(st)
+    org = dycore._inputs_struct(st)
+    lv = dycore._leaves_struct(st)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    call = lambda: _capi.check(lib.wrfgpu_step_epilogue(ctypes.byref(p), ctypes.byref(org), ctypes.byref(ins),
+                                                        ctypes.byref(lv), ctypes.byref(outs), 1800.0, 0,
+                                                        ctypes.c_void_p(raw.data_ptr()), wsp, n.value, sp))
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / reps
+    m = nz * ny * nx
+    sizes = (nz * ny * (nx + 1) + nz * (ny + 1) * nx + (nz + 1) * ny * nx + m + 2 * m + 2 * ny * nx
+             + 2 * (nz + 1) * ny * nx + 6 * m)
+    nbytes = 8 * (2 * sizes + 3 * m + 2 * ny * nx)
+    peak, src = _peaks()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    diag = dycore.theta_limiter_diagnostics(raw)
+    # launches: the limiter's reduction and scalars, every field's elementwise part, every ring band, the record
+    return {"ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs, "peak_gbs": peak, "peak_source": src,
+            "frac": gbs / peak, "launches": 5, "limited_cells": int(diag["theta_limited_cell_count"]),
+            "what": "guards + full end-of-step lateral boundary pass + guards of the bounded state "
+                    "(operational_mode.py:4950-4983 without physics), one call per rep, inputs larger than L2"}
+
+
 def run_batched(args):
     """Batched-domains workload (nests and ensemble members in one call):
     a 3-level nest 150x150x45 (dx 9 km, dt 54 s), 301x301x45 (3 km, 18 s),
@@ -567,6 +631,7 @@ def main():
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--no-mixed", action="store_true", help="skip timing the mixed-precision variant")
     ap.add_argument("--no-adjoint", action="store_true", help="skip timing the adjoints against their forwards")
+    ap.add_argument("--no-epilogue", action="store_true", help="skip timing the step epilogue (guards + boundary pass)")
     ap.add_argument("--no-tune", action="store_true", help="skip the tile-shape tuner (built-in defaults)")
     ap.add_argument("--workload", choices=("moist433", "batched"), default="moist433",
                     help="batched: the nest + ensemble set advanced by the batched call (1 GPU)")
@@ -624,7 +689,8 @@ def main():
                            "parallelism": f"replicas x{world}", "cuda_graph": True, "tile_shapes": r["tuned"]},
                 "e2e": r["e2e"], "roofline": r["roofline"], "whole_step_roofline": r["whole_step_roofline"],
                 "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": r["launches"],
-                "kernels": r["kernels"], "finite": r["finite"], "mixed": r["mixed"], "adjoint": r["adjoint"]}
+                "kernels": r["kernels"], "finite": r["finite"], "mixed": r["mixed"], "adjoint": r["adjoint"],
+                "epilogue": r["epilogue"]}
         print(json.dumps(line))
     return 0
 

@@ -1400,7 +1400,8 @@ int epilogue_check(const wrfgpu_step_params *p, const wrfgpu_step_inputs *in, co
 // `guards`; `gs` / `after` are the theta limiter's scalars and partials).
 int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, const wrfgpu_step_inputs *in,
                     const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out, double lead_seconds, bool guards,
-                    bool boundary, bool spec_only, const GuardScalars *gs, double *after, cudaStream_t stream) {
+                    bool boundary, bool spec_only, const GuardScalars *gs, double *after, int *theta_slots,
+                    cudaStream_t stream) {
   const int nx = p->nx, ny = p->ny, nz = p->nz;
   BdyLeaf nolf{};
   auto leaf = [&](const double *x) -> BdyLeaf {
@@ -1426,6 +1427,8 @@ int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, 
     base.wg[b] = dt * gcx;
   }
   const int ring = boundary ? (spec_only ? 1 : 2) : 0;
+  // the field jobs, launched together at the end: the elementwise parts, then the ring bands
+  LbcBatch inner{}, rings{};
   const int post_fin = (guards && boundary) ? GUARD_FINITE : GUARD_NONE;
   auto copy = [&](double *o, const double *x, size_t n) -> int {
     if (o == x) return WRFGPU_OK;
@@ -1454,8 +1457,31 @@ int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, 
     a.mu_next = in->mu_total;
     a.gs = gs;
     a.after = after;
-    k_lbc_field<<<grd(xl, yl, zl), blk2(), 0, stream>>>(a);
-    return check_launch("k_lbc_field");
+    a.all_ring = (rg && (xl < 8 || yl < 8)) ? 1 : 0;
+    int inner_blocks = 0;
+    if (!a.all_ring) {
+      const dim3 g = grd(xl, yl, (zl + LBC_KZ - 1) / LBC_KZ);
+      const int q = inner.njobs++;
+      inner.job[q] = a;
+      inner.gx[q] = (int)g.x;
+      inner.gy[q] = (int)g.y;
+      inner.slot0[q] = 0;
+      inner_blocks = (int)(g.x * g.y * g.z);
+      inner.start[q + 1] = inner.start[q] + inner_blocks;
+    }
+    int ring_blocks = 0;
+    if (rg) {
+      const int gx = (ring_cells(xl, yl, a.all_ring) + LBC_RING_THREADS - 1) / LBC_RING_THREADS;
+      const int q = rings.njobs++;
+      rings.job[q] = a;
+      rings.gx[q] = gx;
+      rings.gy[q] = zl;
+      rings.slot0[q] = inner_blocks;
+      ring_blocks = gx * zl;
+      rings.start[q + 1] = rings.start[q] + ring_blocks;
+    }
+    if (pre == GUARD_THETA) *theta_slots = inner_blocks + ring_blocks;
+    return WRFGPU_OK;
   };
   const bool geo = p->force_geopotential != 0;
   const wrfgpu_step_inputs *O = org;
@@ -1497,6 +1523,14 @@ int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, 
                   forced ? 2 : 0, guards ? GUARD_RATIO : GUARD_NONE, post, forced ? 1 : 0)))
       return rc;
   }
+  if (inner.njobs > 0) {
+    k_lbc_fields<<<inner.start[inner.njobs], blk2(), 0, stream>>>(inner);
+    if ((rc = check_launch("k_lbc_fields"))) return rc;
+  }
+  if (rings.njobs > 0) {
+    k_lbc_rings<<<rings.start[rings.njobs], dim3(LBC_RING_THREADS, 1, 1), 0, stream>>>(rings);
+    if ((rc = check_launch("k_lbc_rings"))) return rc;
+  }
   return WRFGPU_OK;
 }
 
@@ -1511,8 +1545,10 @@ EpilogueWs epilogue_ws(const wrfgpu_step_params &p) {
   const long long n = (long long)p.nz * p.ny * p.nx;
   const long long want = (n + GUARD_THREADS - 1) / GUARD_THREADS;
   w.nparts = (int)(want < 148 * 8 ? (want < 1 ? 1 : want) : 148 * 8);
-  const dim3 g = grd(p.nx, p.ny, p.nz);
-  w.nafter = (int)(g.x * g.y * g.z);
+  // the theta job's blocks: the elementwise kernel's and the ring band's (at most)
+  const dim3 g = grd(p.nx, p.ny, (p.nz + LBC_KZ - 1) / LBC_KZ);
+  const int rb = (ring_cells(p.nx, p.ny, 1) + LBC_RING_THREADS - 1) / LBC_RING_THREADS;
+  w.nafter = (int)(g.x * g.y * g.z) + rb * p.nz;
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   w.scalars = 0;
   w.partials = up(sizeof(GuardScalars));
@@ -1530,8 +1566,9 @@ extern "C" int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *p, cons
     return fail(WRFGPU_ERR_NULL_POINTER, "params/inputs/leaves/outputs is NULL");
   int rc = epilogue_check(p, in, lv, out, true, dry_spec_only != 0, lead_seconds);
   if (rc) return rc;
+  int slots = 0;
   rc = epilogue_fields(p, nullptr, in, lv, out, lead_seconds, false, true, dry_spec_only != 0, nullptr, nullptr,
-                       stream);
+                       &slots, stream);
   if (rc) return rc;
   g_last_error.clear();
   return WRFGPU_OK;
@@ -1583,12 +1620,13 @@ extern "C" int wrfgpu_step_epilogue(const wrfgpu_step_params *p, const wrfgpu_st
     k_guard_finalize<<<1, GUARD_THREADS, 0, stream>>>(part, w.nparts, gs);
     if ((rc = check_launch("k_guard_finalize"))) return rc;
   }
+  int slots = 0;
   rc = epilogue_fields(p, guards ? origin : nullptr, next, lv, out, lead_seconds, guards, boundary, spec_only, gs,
-                       after, stream);
+                       after, &slots, stream);
   if (rc) return rc;
   if (diag != nullptr) {
     if (guards)
-      k_guard_diag<<<1, GUARD_THREADS, 0, stream>>>(after, w.nafter, gs, p->ny, p->nx, diag);
+      k_guard_diag<<<1, GUARD_THREADS, 0, stream>>>(after, slots, gs, p->ny, p->nx, diag);
     else
       k_guard_diag_empty<<<1, 1, 0, stream>>>(diag);
     if ((rc = check_launch("k_guard_diag"))) return rc;

@@ -27,6 +27,7 @@ struct LbcJob {
   int ring;          // 0: no boundary pass, 1: ring 0 only (the specified cadence's pass), 2: ring 0 + relax rows
   int clamp;         // clip the bounded value at zero (moisture)
   double wf[4], wg[4];  // dt*fcx, dt*gcx of rows 1..3
+  int all_ring;      // grids under 8 x 8: the ring kernel covers every cell, the elementwise one none
   int pre, post;     // GUARD_* before / after the boundary pass
   const double *org, *org2;  // the origin state's field (a pair: total, perturbation)
   const double *mu_next;     // the step output's mu_total (GUARD_THETA's mass weight)
@@ -84,91 +85,13 @@ __device__ __forceinline__ double lbc_value(const LbcJob &a, const BdyLeaf &lf, 
   return cur + a.wf[b] * fls0 - a.wg[b] * lap;
 }
 
-template <typename FLD>
-__device__ __forceinline__ double bounded(const LbcJob &a, const BdyLeaf &lf, FLD F, int k, int j, int i) {
-  return a.ring ? lbc_value(a, lf, F, k, j, i) : F(j, i);
-}
-
-// Index space xl x yl x zl, blocks of LBC_THREADS threads.
 constexpr int LBC_THREADS = 128;
-__global__ void __launch_bounds__(LBC_THREADS) k_lbc_field(LbcJob a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  const bool in = i < a.xl && j < a.yl;
-  const size_t plane = (size_t)a.yl * a.xl;
-  const size_t c = k * plane + (size_t)j * a.xl + i;
-  const auto at = [&](int jj, int ii) { return k * plane + (size_t)jj * a.xl + ii; };
-  if (a.x2 == nullptr) {
-    if (a.pre == GUARD_THETA) {
-      const GuardScalars gs = *a.gs;
-      auto F = [&](int jj, int ii) { return guard_theta(ld(a.x, at(jj, ii)), ld(a.org, at(jj, ii)), gs); };
-      double own = 0.0;
-      if (in) {
-        own = F(j, i) * guard_mass(ld(a.mu_next, (size_t)j * a.xl + i));
-        double v = bounded(a, a.leaf, F, k, j, i);
-        if (a.post == GUARD_FINITE && !isfinite(v)) v = ld(a.org, c);
-        a.out[c] = v;
-      }
-      __shared__ double sh[LBC_THREADS / 32];
-      const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-      // block_sum indexes warps by threadIdx.x: give it the flat thread index
-      double s = own;
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if ((tid & 31) == 0) sh[tid >> 5] = s;
-      __syncthreads();
-      if (tid == 0) {
-        double t = 0.0;
-        for (int w = 0; w < LBC_THREADS / 32; ++w) t += sh[w];
-        a.after[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
-      }
-      return;
-    }
-    if (!in) return;
-    double v;
-    if (a.pre == GUARD_RATIO) {
-      auto F = [&](int jj, int ii) {
-        const double q = ld(a.x, at(jj, ii));
-        return valid_ratio(q) ? q : ld(a.org, at(jj, ii));
-      };
-      v = bounded(a, a.leaf, F, k, j, i);
-    } else {
-      auto F = [&](int jj, int ii) { return ld(a.x, at(jj, ii)); };
-      v = bounded(a, a.leaf, F, k, j, i);
-    }
-    if (a.clamp && v < 0.0) v = 0.0;  // jnp.maximum(v, 0): NaN stays NaN
-    if (a.post == GUARD_FINITE && !isfinite(v)) v = ld(a.org, c);
-    if (a.post == GUARD_RATIO && !valid_ratio(v)) v = ld(a.org, c);
-    a.out[c] = v;
-    return;
-  }
-  if (!in) return;
-  double pert, base;
-  if (a.pre == GUARD_MASS) {  // the dry-mass guard: total and perturbation from one source
-    auto ok = [&](int jj, int ii) { return valid_mu(ld(a.x, at(jj, ii)), ld(a.x2, at(jj, ii))); };
-    auto P = [&](int jj, int ii) { return ok(jj, ii) ? ld(a.x2, at(jj, ii)) : ld(a.org2, at(jj, ii)); };
-    auto B = [&](int jj, int ii) {
-      const size_t cc = at(jj, ii);
-      return ok(jj, ii) ? ld(a.x, cc) - ld(a.x2, cc) : ld(a.org, cc) - ld(a.org2, cc);
-    };
-    pert = bounded(a, a.leaf, P, k, j, i);
-    base = bounded(a, a.leaf2, B, k, j, i);
-  } else {
-    auto P = [&](int jj, int ii) { return ld(a.x2, at(jj, ii)); };
-    auto B = [&](int jj, int ii) {
-      const size_t cc = at(jj, ii);
-      return ld(a.x, cc) - ld(a.x2, cc);
-    };
-    pert = bounded(a, a.leaf, P, k, j, i);
-    base = bounded(a, a.leaf2, B, k, j, i);
-  }
-  // the boundary pass rebuilds every total as base + perturbation; without it
-  // the (guarded) total is kept as it is
-  double tot = base + pert;
-  if (!a.ring) {
-    const bool keep = a.pre != GUARD_MASS || valid_mu(ld(a.x, c), ld(a.x2, c));
-    tot = keep ? ld(a.x, c) : ld(a.org, c);
-  }
+constexpr int LBC_RING_THREADS = 128;
+constexpr int LBC_THREADS_MAX = 128;
+constexpr int LBC_KZ = 4;
+
+// The post guards of a written pair (total, perturbation), then the stores.
+__device__ __forceinline__ void post_pair(const LbcJob &a, double tot, double pert, size_t c) {
   if (a.post == GUARD_FINITE) {
     if (!isfinite(tot)) tot = ld(a.org, c);
     if (!isfinite(pert)) pert = ld(a.org2, c);
@@ -178,6 +101,189 @@ __global__ void __launch_bounds__(LBC_THREADS) k_lbc_field(LbcJob a) {
   }
   a.out[c] = tot;
   a.out2[c] = pert;
+}
+
+// The post guard of one written value.
+__device__ __forceinline__ double post_single(const LbcJob &a, double v, size_t c) {
+  if (a.post == GUARD_FINITE && !isfinite(v)) v = ld(a.org, c);
+  if (a.post == GUARD_RATIO && !valid_ratio(v)) v = ld(a.org, c);
+  return v;
+}
+
+// The per-block partial of sum(limited theta * mass) (GUARD_THETA jobs);
+// `own` is this thread's sum of the limited theta over its levels, `m` its
+// column's mass weight.
+__device__ __forceinline__ void theta_partial(const LbcJob &a, double own, double m, size_t slot) {
+  __shared__ double sh[LBC_THREADS_MAX / 32];
+  double s = own * m;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nt = blockDim.x * blockDim.y;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((tid & 31) == 0) sh[tid >> 5] = s;
+  __syncthreads();
+  if (tid == 0) {
+    double tsum = 0.0;
+    for (int w = 0; w < nt / 32; ++w) tsum += sh[w];
+    a.after[slot] = tsum;
+  }
+}
+
+// The elementwise part: index space xl x yl x ceil(zl / LBC_KZ), each thread
+// LBC_KZ levels of one column with all loads issued first.  With the
+// boundary pass the 4-wide ring band is left to lbc_ring.
+__device__ __forceinline__ void lbc_field(const LbcJob &a, int bx, int by, int bz, size_t slot) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k0 = bz * LBC_KZ;
+  const int xl = a.xl, yl = a.yl;
+  const bool in = i < xl && j < yl && (!a.ring || (i >= 4 && i < xl - 4 && j >= 4 && j < yl - 4));
+  const size_t plane = (size_t)yl * xl;
+  const size_t c0 = (size_t)k0 * plane + (size_t)j * xl + i;
+  const int nk = a.zl - k0 < LBC_KZ ? a.zl - k0 : LBC_KZ;
+  const bool th = a.pre == GUARD_THETA;
+  double own = 0.0;
+  if (in && a.x2 == nullptr) {
+    double xv[LBC_KZ], ov[LBC_KZ];
+#pragma unroll
+    for (int t = 0; t < LBC_KZ; ++t)
+      if (t < nk) {
+        xv[t] = ld(a.x, c0 + t * plane);
+        ov[t] = th ? ld(a.org, c0 + t * plane) : 0.0;
+      }
+    GuardScalars gs{};
+    if (th) gs = *a.gs;
+#pragma unroll
+    for (int t = 0; t < LBC_KZ; ++t) {
+      if (t >= nk) break;
+      const size_t c = c0 + t * plane;
+      double v = xv[t];
+      if (th) v = guard_theta(v, ov[t], gs);
+      else if (a.pre == GUARD_RATIO && !valid_ratio(v)) v = ld(a.org, c);
+      own += v;
+      if (a.clamp && v < 0.0) v = 0.0;  // jnp.maximum(v, 0): NaN stays NaN
+      a.out[c] = post_single(a, v, c);
+    }
+  } else if (in) {
+    // a pair: the boundary pass rebuilds every total as base + perturbation;
+    // without it the (guarded) total is kept as it is
+    double tv[LBC_KZ], pv[LBC_KZ];
+#pragma unroll
+    for (int t = 0; t < LBC_KZ; ++t)
+      if (t < nk) {
+        tv[t] = ld(a.x, c0 + t * plane);
+        pv[t] = ld(a.x2, c0 + t * plane);
+      }
+#pragma unroll
+    for (int t = 0; t < LBC_KZ; ++t) {
+      if (t >= nk) break;
+      const size_t c = c0 + t * plane;
+      double tot = tv[t], pert = pv[t];
+      if (a.pre == GUARD_MASS && !valid_mu(tot, pert)) {
+        tot = ld(a.org, c);
+        pert = ld(a.org2, c);
+      }
+      if (a.ring) tot = (tot - pert) + pert;
+      post_pair(a, tot, pert, c);
+    }
+  }
+  if (th) theta_partial(a, own, in ? guard_mass(ld(a.mu_next, (size_t)j * xl + i)) : 0.0, slot);
+}
+
+// Cells of the 4-wide ring band per level: rows 0..3 and yl-4..yl-1 (all
+// columns), then columns 0..3 and xl-4..xl-1 of rows 4..yl-5 (xl, yl >= 8);
+// every cell when all_ring.
+__host__ __device__ inline int ring_cells(int xl, int yl, int all_ring) {
+  return all_ring ? xl * yl : 8 * xl + 8 * (yl - 8);
+}
+
+// The stencil part: index space ring_cells x zl, one thread per band cell.
+__device__ __forceinline__ void lbc_ring(const LbcJob &a, int bx, int k, size_t slot) {
+  const int xl = a.xl, yl = a.yl;
+  const int r = bx * blockDim.x + threadIdx.x;
+  const int nb = ring_cells(xl, yl, a.all_ring);
+  int i = 0, j = 0;
+  const bool in = r < nb;
+  if (in) {
+    if (a.all_ring) {
+      j = r / xl;
+      i = r - j * xl;
+    } else if (r < 8 * xl) {
+      const int row = r / xl;
+      i = r - row * xl;
+      j = row < 4 ? row : yl - 8 + row;
+    } else {
+      const int q = r - 8 * xl, h = yl - 8;
+      const int col = q / h;
+      j = 4 + (q - col * h);
+      i = col < 4 ? col : xl - 8 + col;
+    }
+  }
+  const size_t plane = (size_t)yl * xl;
+  const auto at = [&](int jj, int ii) { return (size_t)k * plane + (size_t)jj * xl + ii; };
+  const bool th = a.pre == GUARD_THETA;
+  double own = 0.0;
+  if (in && a.x2 == nullptr) {
+    GuardScalars gs{};
+    if (th) gs = *a.gs;
+    auto F = [&](int jj, int ii) {
+      const size_t cc = at(jj, ii);
+      const double x = ld(a.x, cc);
+      if (th) return guard_theta(x, ld(a.org, cc), gs);
+      if (a.pre == GUARD_RATIO && !valid_ratio(x)) return ld(a.org, cc);
+      return x;
+    };
+    own = F(j, i);
+    double v = lbc_value(a, a.leaf, F, k, j, i);
+    if (a.clamp && v < 0.0) v = 0.0;
+    a.out[at(j, i)] = post_single(a, v, at(j, i));
+  } else if (in) {
+    auto ok = [&](int jj, int ii) {
+      return a.pre != GUARD_MASS || valid_mu(ld(a.x, at(jj, ii)), ld(a.x2, at(jj, ii)));
+    };
+    auto P = [&](int jj, int ii) { return ok(jj, ii) ? ld(a.x2, at(jj, ii)) : ld(a.org2, at(jj, ii)); };
+    auto B = [&](int jj, int ii) {
+      const size_t cc = at(jj, ii);
+      return ok(jj, ii) ? ld(a.x, cc) - ld(a.x2, cc) : ld(a.org, cc) - ld(a.org2, cc);
+    };
+    double pert = lbc_value(a, a.leaf, P, k, j, i);
+    double tot = lbc_value(a, a.leaf2, B, k, j, i) + pert;
+    post_pair(a, tot, pert, at(j, i));
+  }
+  if (th) theta_partial(a, own, in ? guard_mass(ld(a.mu_next, (size_t)j * xl + i)) : 0.0, slot);
+}
+
+// Every field of one epilogue in one launch: job q owns the blocks
+// [start[q], start[q+1]) of the flattened grid, laid out as its own
+// gx x gy x gz grid (gz levels for the ring kernel, level chunks for the
+// elementwise one).  The theta job's partial of block b goes to slot
+// slot0[q] + (b - start[q]).
+constexpr int LBC_MAX_JOBS = 16;
+struct LbcBatch {
+  LbcJob job[LBC_MAX_JOBS];
+  int start[LBC_MAX_JOBS + 1];
+  int gx[LBC_MAX_JOBS], gy[LBC_MAX_JOBS];
+  int slot0[LBC_MAX_JOBS];
+  int njobs;
+};
+
+__device__ __forceinline__ int batch_job(const LbcBatch &b, int blk) {
+  int q = 0;
+  while (q + 1 < b.njobs && blk >= b.start[q + 1]) ++q;
+  return q;
+}
+
+__global__ void __launch_bounds__(LBC_THREADS) k_lbc_fields(const __grid_constant__ LbcBatch b) {
+  const int q = batch_job(b, blockIdx.x);
+  const int l = blockIdx.x - b.start[q];
+  const int gx = b.gx[q], gy = b.gy[q];
+  lbc_field(b.job[q], l % gx, (l / gx) % gy, l / (gx * gy), (size_t)b.slot0[q] + l);
+}
+
+__global__ void __launch_bounds__(LBC_RING_THREADS) k_lbc_rings(const __grid_constant__ LbcBatch b) {
+  const int q = batch_job(b, blockIdx.x);
+  const int l = blockIdx.x - b.start[q];
+  const int gx = b.gx[q];
+  lbc_ring(b.job[q], l % gx, l / gx, (size_t)b.slot0[q] + l);
 }
 
 }  // namespace wg
