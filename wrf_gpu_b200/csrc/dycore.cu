@@ -1429,6 +1429,10 @@ int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, 
   const int ring = boundary ? (spec_only ? 1 : 2) : 0;
   // the field jobs, launched together at the end: the elementwise parts, then the ring bands
   LbcBatch inner{}, rings{};
+  // shared x / y grids: the widest field (nx + 1 by ny + 1); the ring band of the largest field
+  const dim3 inner_grid = grd(nx + 1, ny + 1, 1);
+  const bool small = nx + 1 < 8 || ny + 1 < 8;
+  const int ring_gx = (ring_cells(nx + 1, ny + 1, small ? 1 : 0) + LBC_RING_THREADS - 1) / LBC_RING_THREADS;
   const int post_fin = (guards && boundary) ? GUARD_FINITE : GUARD_NONE;
   auto copy = [&](double *o, const double *x, size_t n) -> int {
     if (o == x) return WRFGPU_OK;
@@ -1460,25 +1464,20 @@ int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, 
     a.all_ring = (rg && (xl < 8 || yl < 8)) ? 1 : 0;
     int inner_blocks = 0;
     if (!a.all_ring) {
-      const dim3 g = grd(xl, yl, (zl + LBC_KZ - 1) / LBC_KZ);
       const int q = inner.njobs++;
       inner.job[q] = a;
-      inner.gx[q] = (int)g.x;
-      inner.gy[q] = (int)g.y;
       inner.slot0[q] = 0;
-      inner_blocks = (int)(g.x * g.y * g.z);
-      inner.start[q + 1] = inner.start[q] + inner_blocks;
+      inner_blocks = (int)(inner_grid.x * inner_grid.y);
     }
     int ring_blocks = 0;
     if (rg) {
-      const int gx = (ring_cells(xl, yl, a.all_ring) + LBC_RING_THREADS - 1) / LBC_RING_THREADS;
+      if (ring_cells(xl, yl, a.all_ring) > ring_gx * LBC_RING_THREADS)
+        return fail(WRFGPU_ERR_BAD_SHAPE, "a field's ring band exceeds the shared ring grid");
       const int q = rings.njobs++;
       rings.job[q] = a;
-      rings.gx[q] = gx;
-      rings.gy[q] = zl;
       rings.slot0[q] = inner_blocks;
-      ring_blocks = gx * zl;
-      rings.start[q + 1] = rings.start[q] + ring_blocks;
+      rings.start[q + 1] = rings.start[q] + zl;
+      ring_blocks = ring_gx * zl;
     }
     if (pre == GUARD_THETA) *theta_slots = inner_blocks + ring_blocks;
     return WRFGPU_OK;
@@ -1524,11 +1523,11 @@ int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, 
       return rc;
   }
   if (inner.njobs > 0) {
-    k_lbc_fields<<<inner.start[inner.njobs], blk2(), 0, stream>>>(inner);
+    k_lbc_fields<<<dim3(inner_grid.x, inner_grid.y, inner.njobs), blk2(), 0, stream>>>(inner);
     if ((rc = check_launch("k_lbc_fields"))) return rc;
   }
   if (rings.njobs > 0) {
-    k_lbc_rings<<<rings.start[rings.njobs], dim3(LBC_RING_THREADS, 1, 1), 0, stream>>>(rings);
+    k_lbc_rings<<<dim3(ring_gx, rings.start[rings.njobs], 1), dim3(LBC_RING_THREADS, 1, 1), 0, stream>>>(rings);
     if ((rc = check_launch("k_lbc_rings"))) return rc;
   }
   return WRFGPU_OK;
@@ -1546,8 +1545,8 @@ EpilogueWs epilogue_ws(const wrfgpu_step_params &p) {
   const long long want = (n + GUARD_THREADS - 1) / GUARD_THREADS;
   w.nparts = (int)(want < 148 * 8 ? (want < 1 ? 1 : want) : 148 * 8);
   // the theta job's blocks: the elementwise kernel's and the ring band's (at most)
-  const dim3 g = grd(p.nx, p.ny, (p.nz + LBC_KZ - 1) / LBC_KZ);
-  const int rb = (ring_cells(p.nx, p.ny, 1) + LBC_RING_THREADS - 1) / LBC_RING_THREADS;
+  const dim3 g = grd(p.nx + 1, p.ny + 1, 1);
+  const int rb = (ring_cells(p.nx + 1, p.ny + 1, 1) + LBC_RING_THREADS - 1) / LBC_RING_THREADS;
   w.nafter = (int)(g.x * g.y * g.z) + rb * p.nz;
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   w.scalars = 0;

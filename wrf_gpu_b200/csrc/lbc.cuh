@@ -128,70 +128,79 @@ __device__ __forceinline__ void theta_partial(const LbcJob &a, double own, doubl
   }
 }
 
-// The elementwise part: index space xl x yl x ceil(zl / LBC_KZ), each thread
-// LBC_KZ levels of one column with all loads issued first.  With the
+// The elementwise part: index space xl x yl, each thread one column in
+// chunks of LBC_KZ levels with each chunk's loads issued first.  With the
 // boundary pass the 4-wide ring band is left to lbc_ring.
-__device__ __forceinline__ void lbc_field(const LbcJob &a, int bx, int by, int bz, size_t slot) {
+__device__ __forceinline__ void lbc_field(const LbcJob &a, int bx, int by, size_t slot) {
   const int i = bx * blockDim.x + threadIdx.x;
   const int j = by * blockDim.y + threadIdx.y;
-  const int k0 = bz * LBC_KZ;
-  const int xl = a.xl, yl = a.yl;
+  const int xl = a.xl, yl = a.yl, zl = a.zl;
   const bool in = i < xl && j < yl && (!a.ring || (i >= 4 && i < xl - 4 && j >= 4 && j < yl - 4));
   const size_t plane = (size_t)yl * xl;
-  const size_t c0 = (size_t)k0 * plane + (size_t)j * xl + i;
-  const int nk = a.zl - k0 < LBC_KZ ? a.zl - k0 : LBC_KZ;
   const bool th = a.pre == GUARD_THETA;
   double own = 0.0;
   if (in && a.x2 == nullptr) {
-    double xv[LBC_KZ], ov[LBC_KZ];
-#pragma unroll
-    for (int t = 0; t < LBC_KZ; ++t)
-      if (t < nk) {
-        xv[t] = ld(a.x, c0 + t * plane);
-        ov[t] = th ? ld(a.org, c0 + t * plane) : 0.0;
-      }
+    const double *x = a.x + (size_t)j * xl + i;
+    const double *org = a.org + (size_t)j * xl + i;
+    double *out = a.out + (size_t)j * xl + i;
     GuardScalars gs{};
     if (th) gs = *a.gs;
+    for (int k0 = 0; k0 < zl; k0 += LBC_KZ) {
+      const int nk = zl - k0 < LBC_KZ ? zl - k0 : LBC_KZ;
+      double xv[LBC_KZ], ov[LBC_KZ];
 #pragma unroll
-    for (int t = 0; t < LBC_KZ; ++t) {
-      if (t >= nk) break;
-      const size_t c = c0 + t * plane;
-      double v = xv[t];
-      if (th) v = guard_theta(v, ov[t], gs);
-      else if (a.pre == GUARD_RATIO && !valid_ratio(v)) v = ld(a.org, c);
-      own += v;
-      if (a.clamp && v < 0.0) v = 0.0;  // jnp.maximum(v, 0): NaN stays NaN
-      a.out[c] = post_single(a, v, c);
+      for (int t = 0; t < LBC_KZ; ++t)
+        if (t < nk) {
+          xv[t] = ld(x, (size_t)(k0 + t) * plane);
+          ov[t] = th ? ld(org, (size_t)(k0 + t) * plane) : 0.0;
+        }
+#pragma unroll
+      for (int t = 0; t < LBC_KZ; ++t) {
+        if (t >= nk) break;
+        const size_t c = (size_t)(k0 + t) * plane;
+        double v = xv[t];
+        if (th) v = guard_theta(v, ov[t], gs);
+        else if (a.pre == GUARD_RATIO && !valid_ratio(v)) v = ld(org, c);
+        own += v;
+        if (a.clamp && v < 0.0) v = 0.0;  // jnp.maximum(v, 0): NaN stays NaN
+        if (a.post == GUARD_FINITE && !isfinite(v)) v = ld(org, c);
+        if (a.post == GUARD_RATIO && !valid_ratio(v)) v = ld(org, c);
+        out[c] = v;
+      }
     }
   } else if (in) {
     // a pair: the boundary pass rebuilds every total as base + perturbation;
     // without it the (guarded) total is kept as it is
-    double tv[LBC_KZ], pv[LBC_KZ];
+    const size_t c0 = (size_t)j * xl + i;
+    for (int k0 = 0; k0 < zl; k0 += LBC_KZ) {
+      const int nk = zl - k0 < LBC_KZ ? zl - k0 : LBC_KZ;
+      double tv[LBC_KZ], pv[LBC_KZ];
 #pragma unroll
-    for (int t = 0; t < LBC_KZ; ++t)
-      if (t < nk) {
-        tv[t] = ld(a.x, c0 + t * plane);
-        pv[t] = ld(a.x2, c0 + t * plane);
-      }
+      for (int t = 0; t < LBC_KZ; ++t)
+        if (t < nk) {
+          tv[t] = ld(a.x, c0 + (size_t)(k0 + t) * plane);
+          pv[t] = ld(a.x2, c0 + (size_t)(k0 + t) * plane);
+        }
 #pragma unroll
-    for (int t = 0; t < LBC_KZ; ++t) {
-      if (t >= nk) break;
-      const size_t c = c0 + t * plane;
-      double tot = tv[t], pert = pv[t];
-      if (a.pre == GUARD_MASS && !valid_mu(tot, pert)) {
-        tot = ld(a.org, c);
-        pert = ld(a.org2, c);
+      for (int t = 0; t < LBC_KZ; ++t) {
+        if (t >= nk) break;
+        const size_t c = c0 + (size_t)(k0 + t) * plane;
+        double tot = tv[t], pert = pv[t];
+        if (a.pre == GUARD_MASS && !valid_mu(tot, pert)) {
+          tot = ld(a.org, c);
+          pert = ld(a.org2, c);
+        }
+        if (a.ring) tot = (tot - pert) + pert;
+        post_pair(a, tot, pert, c);
       }
-      if (a.ring) tot = (tot - pert) + pert;
-      post_pair(a, tot, pert, c);
     }
   }
   if (th) theta_partial(a, own, in ? guard_mass(ld(a.mu_next, (size_t)j * xl + i)) : 0.0, slot);
 }
 
 // Cells of the 4-wide ring band per level: rows 0..3 and yl-4..yl-1 (all
-// columns), then columns 0..3 and xl-4..xl-1 of rows 4..yl-5 (xl, yl >= 8);
-// every cell when all_ring.
+// columns), then columns 0..3 and xl-4..xl-1 of rows 4..yl-5, row by row
+// (xl, yl >= 8); every cell when all_ring.
 __host__ __device__ inline int ring_cells(int xl, int yl, int all_ring) {
   return all_ring ? xl * yl : 8 * xl + 8 * (yl - 8);
 }
@@ -211,10 +220,10 @@ __device__ __forceinline__ void lbc_ring(const LbcJob &a, int bx, int k, size_t 
       const int row = r / xl;
       i = r - row * xl;
       j = row < 4 ? row : yl - 8 + row;
-    } else {
-      const int q = r - 8 * xl, h = yl - 8;
-      const int col = q / h;
-      j = 4 + (q - col * h);
+    } else {  // eight band columns of one row per 8 threads (two 32-byte runs)
+      const int q = r - 8 * xl;
+      const int col = q & 7;
+      j = 4 + (q >> 3);
       i = col < 4 ? col : xl - 8 + col;
     }
   }
@@ -252,16 +261,15 @@ __device__ __forceinline__ void lbc_ring(const LbcJob &a, int bx, int k, size_t 
   if (th) theta_partial(a, own, in ? guard_mass(ld(a.mu_next, (size_t)j * xl + i)) : 0.0, slot);
 }
 
-// Every field of one epilogue in one launch: job q owns the blocks
-// [start[q], start[q+1]) of the flattened grid, laid out as its own
-// gx x gy x gz grid (gz levels for the ring kernel, level chunks for the
-// elementwise one).  The theta job's partial of block b goes to slot
-// slot0[q] + (b - start[q]).
+// Every field of one epilogue in one launch.  All jobs share the x / y grid
+// (sized for the widest field; threads past a field's extent idle);
+// blockIdx.z is the job of the elementwise kernel, and the ring kernel's
+// blockIdx.y is flattened over the jobs' levels: job q owns [start[q], start[q+1]).  The theta
+// job's partial of a block goes to slot slot0[q] + its index within the job.
 constexpr int LBC_MAX_JOBS = 16;
 struct LbcBatch {
   LbcJob job[LBC_MAX_JOBS];
   int start[LBC_MAX_JOBS + 1];
-  int gx[LBC_MAX_JOBS], gy[LBC_MAX_JOBS];
   int slot0[LBC_MAX_JOBS];
   int njobs;
 };
@@ -272,18 +280,15 @@ __device__ __forceinline__ int batch_job(const LbcBatch &b, int blk) {
   return q;
 }
 
-__global__ void __launch_bounds__(LBC_THREADS) k_lbc_fields(const __grid_constant__ LbcBatch b) {
-  const int q = batch_job(b, blockIdx.x);
-  const int l = blockIdx.x - b.start[q];
-  const int gx = b.gx[q], gy = b.gy[q];
-  lbc_field(b.job[q], l % gx, (l / gx) % gy, l / (gx * gy), (size_t)b.slot0[q] + l);
+__global__ void __launch_bounds__(LBC_THREADS, 8) k_lbc_fields(const __grid_constant__ LbcBatch b) {
+  const int q = blockIdx.z;
+  lbc_field(b.job[q], blockIdx.x, blockIdx.y, (size_t)b.slot0[q] + (size_t)blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 __global__ void __launch_bounds__(LBC_RING_THREADS) k_lbc_rings(const __grid_constant__ LbcBatch b) {
-  const int q = batch_job(b, blockIdx.x);
-  const int l = blockIdx.x - b.start[q];
-  const int gx = b.gx[q];
-  lbc_ring(b.job[q], l % gx, l / gx, (size_t)b.slot0[q] + l);
+  const int q = batch_job(b, blockIdx.y);
+  const int k = blockIdx.y - b.start[q];
+  lbc_ring(b.job[q], blockIdx.x, k, (size_t)b.slot0[q] + (size_t)k * gridDim.x + blockIdx.x);
 }
 
 }  // namespace wg
