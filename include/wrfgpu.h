@@ -129,6 +129,13 @@ typedef struct wrfgpu_step_params {
    * operational_mode.py:3062-3075); the bundle's arrays are the inputs'
    * physics pointers (NULL = zero).  0 (default): no bundle. */
   int physics;
+  /* 6th-order numerical diffusion (diff_6th_opt, operational_mode.py:
+   * 2870-2876; dynamics/explicit_diffusion.py:160-226): 0 (default) off, 1 or
+   * 2 add the monotonic filter of u, v, w, theta, coupled by their dry-air
+   * mass, to every stage's tendencies with coefficient
+   * diff_6th_factor * 0.015625 / (2 dt) (default factor 0.12). */
+  int diff_6th_opt;
+  double diff_6th_factor;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */

@@ -73,6 +73,8 @@ class Namelist:
     normal_bdy_relax_strength: float | None = None
     moist_cqw: bool = True          # GPUWRF_MOIST_CQW default (operational_mode.py:219)
     w_coriolis: bool = True         # GPUWRF_W_CORIOLIS default (operational_mode.py:1793)
+    diff_6th_opt: int = 0           # operational_mode.py:491 (0 off; 1 and 2 apply the monotonic filter)
+    diff_6th_factor: float = 0.12   # operational_mode.py:492
     base_tend: dict | None = None   # namelist.tendencies u/v/w/theta/mu (zero when None)
 
 
@@ -707,6 +709,38 @@ def rk_addtend_dry(t, physics, rk_step, m, mut):
                            theta=t.theta + tt / m.msfty[None] + mass_h * h / m.msfty[None], mu=t.mu + mt)
 
 
+def dflux6(f, axis):
+    """``_dflux6`` (dynamics/explicit_diffusion.py:160-180): the 6th-order
+    diffusive fluxes at the left (p0) and right (p1) faces of every cell and
+    the matching first differences, neighbours wrapped along ``axis``."""
+    r = lambda n: np.roll(f, n, axis=axis)
+    fm3, fm2, fm1, fp1, fp2, fp3 = r(3), r(2), r(1), r(-1), r(-2), r(-3)
+    p0 = 10.0 * (f - fm1) - 5.0 * (fp1 - fm2) + (fp2 - fm3)
+    p1 = 10.0 * (fp1 - f) - 5.0 * (fp2 - fm1) + (fp3 - fm2)
+    return p0, p1, f - fm1, fp1 - f
+
+
+def sixth_axis(f, axis, coef):
+    """``_sixth_axis`` (explicit_diffusion.py:183-197) with the monotonic
+    limiter on (the stage passes the default): fluxes that point up-gradient
+    are zeroed."""
+    p0, p1, g0, g1 = dflux6(f, axis)
+    p0 = np.where(p0 * g0 <= 0.0, 0.0, p0)
+    p1 = np.where(p1 * g1 <= 0.0, 0.0, p1)
+    return coef * (p1 - p0)
+
+
+def sixth_order_diffusion_tendency(f, dt, factor):
+    """``sixth_order_diffusion_tendency`` (explicit_diffusion.py:200-226): the
+    uncoupled filter tendency along x, plus along y when the field has more
+    than one row; coefficient factor * 0.015625 / (2 dt)."""
+    coef = float(factor) * 0.015625 / (2.0 * float(dt))
+    t = sixth_axis(f, 2, coef)
+    if f.shape[1] > 1:
+        t = t + sixth_axis(f, 1, coef)
+    return t
+
+
 def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_relax=None, physics=None):
     """operational_mode.py:2722-3093 (flux advection on, diffusion off), with
     the physics merge (:3062-3075) when ``physics`` is given."""
@@ -736,6 +770,12 @@ def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_rel
     else:
         adv = advect_scalar_flux(s.theta - T0, vel, rdx, rdy, m.rdnw, m.fnm, m.fnp)
     th_t = bth * mass_h + adv
+    if nl.diff_6th_opt != 0:  # operational_mode.py:2870-2876
+        f6 = nl.diff_6th_factor
+        u_t = u_t + mass_u * sixth_order_diffusion_tendency(s.u, nl.dt_s, f6)
+        v_t = v_t + mass_v * sixth_order_diffusion_tendency(s.v, nl.dt_s, f6)
+        w_t = w_t + mass_f * sixth_order_diffusion_tendency(s.w, nl.dt_s, f6)
+        th_t = th_t + mass_h * sixth_order_diffusion_tendency(s.theta, nl.dt_s, f6)
     ru_pgf, rv_pgf = large_step_horizontal_pgf(s, m, rdx, rdy, nl.top_lid, nl.hypsometric_opt)
     u_t = u_t + ru_pgf
     v_t = v_t + rv_pgf

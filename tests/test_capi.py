@@ -218,3 +218,16 @@ def test_step_epilogue_rejects_before_any_launch(lib):
                                     None) == _capi.WRFGPU_ERR_NULL_POINTER
     assert lib.wrfgpu_step_epilogue(ctypes.byref(p), ctypes.byref(org), ctypes.byref(ins), None, ctypes.byref(outs),
                                     0.0, 0, None, None, 0, None) == _capi.WRFGPU_ERR_NULL_POINTER
+
+
+def test_sixth_order_diffusion_params(lib):
+    p = _capi.StepParams()
+    lib.wrfgpu_step_params_init(ctypes.byref(p))
+    assert p.diff_6th_opt == 0 and p.diff_6th_factor == 0.12  # operational_mode.py:491-492
+    n0, n1 = ctypes.c_int(0), ctypes.c_int(0)
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(_params(lib)), ctypes.byref(n0)) == 0
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(_params(lib, diff_6th_opt=2)), ctypes.byref(n1)) == 0
+    assert n1.value == n0.value + 3  # one filter launch per stage
+    for kw in (dict(diff_6th_opt=3), dict(diff_6th_opt=1, diff_6th_factor=float("nan"))):
+        assert lib.wrfgpu_step_params_validate(ctypes.byref(_params(lib, **kw))) == \
+            _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG

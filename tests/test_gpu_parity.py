@@ -306,3 +306,15 @@ def test_full_size_properties(cuda_ready):
     out_s = dycore.rk_scan_step(dycore.carry_from_case(case_s), nl_s, lead_seconds=0.0)
     torch.cuda.synchronize()
     assert torch.isfinite(out_s.state.w).all() and torch.isfinite(out_s.state.theta).all()
+
+
+@pytest.mark.parametrize("specified,factor,shape", [(False, 0.12, (24, 20, 14)), (True, 0.12, (24, 20, 14)),
+                                                    (False, 0.5, (33, 9, 7))])
+def test_per_step_parity_sixth_order_diffusion(cuda_ready, specified, factor, shape):
+    """diff_6th_opt: the monotonic 6th-order filter of u, v, w, theta added to
+    every stage's coupled tendencies (operational_mode.py:2870-2876)."""
+    case = cases.real_like_moist(*shape, hmax=800.0, specified=specified)
+    case.controls.update(diff_6th_opt=2, diff_6th_factor=factor)
+    for n, errs in enumerate(_per_step(case, 2 if specified else 3)):
+        bad = {k: v for k, v in errs.items() if not v <= _tol(k)}
+        assert not bad, f"step {n}: {bad}"

@@ -44,6 +44,7 @@ class StepParams(ctypes.Structure):
         ("march_levels", _I), ("column_lanes", _I), ("column_width", _I), ("specified_adv_degrade", _I),
         ("specified_bdy_cadence", _I), ("force_geopotential", _I), ("nested_ph_relax", _I),
         ("nested_w_relax", _I), ("nested_ph_spec", _I), ("physics", _I),
+        ("diff_6th_opt", _I), ("diff_6th_factor", _D),
     ]
 
 

@@ -26,6 +26,7 @@
 #include "bdy_cadence.cuh"
 #include "physics_merge.cuh"
 #include "lbc.cuh"
+#include "diffusion.cuh"
 
 using namespace wg;
 
@@ -259,7 +260,7 @@ ProfState g_prof;
 const char *kClassNames[] = {"k_recip_msf", "k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
                              "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_uv",
                              "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col", "k_spec_relax",
-                             "k_spec_w", "k_phys"};
+                             "k_spec_w", "k_phys", "k_diff6"};
 constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
 
 int class_of(const char *name) {
@@ -375,6 +376,7 @@ int wrfgpu_step_params_init(wrfgpu_step_params *p) {
   p->update_cadence_s = 3600.0;
   p->normal_bdy_relax_strength = -1.0;
   p->force_geopotential = 1;
+  p->diff_6th_factor = 0.12;  // operational_mode.py:492
   p->moist_cqw = 1;
   p->w_coriolis = 1;
   p->precision = WRFGPU_PRECISION_FP64;
@@ -408,6 +410,10 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
   if (p->column_width != 0 && p->column_width != 16 && p->column_width != 32)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 16 or 32");
   if (p->physics != 0 && p->physics != 1) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "physics must be 0 or 1");
+  if (p->diff_6th_opt < 0 || p->diff_6th_opt > 2)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "diff_6th_opt must be 0, 1 or 2");
+  if (p->diff_6th_opt && !(std::isfinite(p->diff_6th_factor) && p->diff_6th_factor >= 0.0))
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "diff_6th_factor must be finite and non-negative");
   if (p->specified_adv_degrade != 0 && p->specified_adv_degrade != 1)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "specified_adv_degrade must be 0 or 1");
   if (spec && p->specified_adv_degrade && p->force_geopotential && (p->nx < 7 || p->ny < 7))
@@ -442,6 +448,7 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
     n += 3 * nsub[s];  // advance_uv, div_h, column
     n += 3;  // finish u, v, col
     if (p->physics) n += 1;  // the physics merge of u, v, theta
+    if (p->diff_6th_opt) n += 1;  // the 6th-order filter of u, v, w, theta
     if (p->run_boundary && !p->bc_ideal && p->force_geopotential && p->specified_bdy_cadence) {
       n += (s == 0) ? 2 : 1;  // [first-stage mu tendency], relax tendencies
       n += nsub[s];           // zero-gradient w after every column launch
@@ -741,6 +748,16 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
         g, w.mut, w.muts0, w.mu_work0, w.c2a, w.cqw, w.alt, w.theta_w, w.ph_w, origin.theta, cof, p.top_lid, co);
     LAUNCH_CHECK("k_coef");
 
+    if (p.diff_6th_opt) {
+      // the 6th-order filter of the stage state into its coupled tendencies
+      // (operational_mode.py:2870-2876), ahead of the physics merge
+      Diff6Args da{s.u, s.v, s.w, s.theta, s.mu_total, w.u_tend, w.v_tend, w.rw_tend, w.t_tend,
+                   p.diff_6th_factor * 0.015625 / (2.0 * p.dt)};
+      PROF("k_diff6");
+      k_diff6<<<dim3((nx + 1 + D6_TX - 1) / D6_TX, (ny + 1 + D6_TY - 1) / D6_TY, nz + 1), dim3(D6_TX, D6_TY, 1), 0,
+                stream>>>(g, da);
+      LAUNCH_CHECK("k_diff6");
+    }
     if (p.physics) {
       // rk_addtend_dry: the physics tendencies into this stage's u, v, theta (w: in k_wface)
       PhysArgs ps = phys;

@@ -256,6 +256,7 @@ class OperationalNamelist:
     diff_opt: int = 0
     km_opt: int = 0
     diff_6th_opt: int = 0
+    diff_6th_factor: float = 0.12
     const_nu_m2_s: float = 0.0
     use_flux_advection: bool = False
     scalar_adv_opt: int = 0
@@ -285,7 +286,8 @@ class OperationalNamelist:
                   zdamp=c["zdamp"], use_flux_advection=True, scalar_adv_opt=c["scalar_adv_opt"],
                   moist_adv_opt=c["moist_adv_opt"], moist_cqw=c["moist_cqw"], w_coriolis=c["w_coriolis"],
                   specified_adv_degrade=bool(c.get("specified_adv_degrade", False)),
-                  specified_bdy_cadence=bool(c.get("specified_bdy_cadence", False)))
+                  specified_bdy_cadence=bool(c.get("specified_bdy_cadence", False)),
+                  diff_6th_opt=int(c.get("diff_6th_opt", 0)), diff_6th_factor=float(c.get("diff_6th_factor", 0.12)))
         kw.update(overrides)
         return cls(**kw)
 
@@ -297,7 +299,7 @@ def _unsupported(nl: OperationalNamelist, physics_tendencies) -> str | None:
         return "use_vertical_solver=False is not built"
     if nl.rk_order != 3:
         return "rk_order must be 3"
-    if nl.diff_opt or nl.km_opt or nl.diff_6th_opt or nl.const_nu_m2_s > 0.0:
+    if nl.diff_opt or nl.km_opt or nl.const_nu_m2_s > 0.0:
         return "explicit diffusion options are not built"
     if nl.moist_adv_opt and nl.mp_physics in (7, 17, 18, 19, 21, 22, 24, 26, 27, 28, 38):
         return "extra advected species of this mp_physics family are not built"
@@ -333,6 +335,7 @@ def step_params(nl: OperationalNamelist) -> _capi.StepParams:
     p.force_geopotential = int(bool(bc.force_geopotential))
     p.nested_ph_relax, p.nested_w_relax = int(bool(bc.nested_ph_relax)), int(bool(bc.nested_w_relax))
     p.nested_ph_spec = int(bool(bc.nested_ph_spec))
+    p.diff_6th_opt, p.diff_6th_factor = int(nl.diff_6th_opt), float(nl.diff_6th_factor)
     m = nl.metrics
     p.cf1, p.cf2, p.cf3, p.p_top = m.cf1, m.cf2, m.cf3, m.p_top
     p.cfn, p.cfn1 = m.cfn()
