@@ -208,6 +208,22 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *params, const wrfgpu_metrics *metr
                     double lead_seconds, void *workspace, size_t workspace_bytes,
                     cudaStream_t stream);
 
+/* One RK3 step with the forecast clock on the device: lead_seconds_dev points
+ * to one double (seconds at step start, device memory) that the kernels
+ * read when they interpolate boundary strips in time.  Replaces the same
+ * _rk_scan_step call as it sits in the reference's jitted loop, where
+ * lead_seconds is a traced value (runtime/operational_mode.py:4929-4945,
+ * lead_seconds = step_index * dt inside fori_loop; interpolate_boundary_leaf
+ * takes it as an array, coupling/boundary_apply.py:329-345).  The lead is
+ * always present (the NaN = None form is wrfgpu_rk3_step's); results are
+ * identical to wrfgpu_rk3_step with the same value on the host, and one
+ * captured CUDA graph of this call can be replayed for successive steps by
+ * updating the device value alone. */
+int wrfgpu_rk3_step_device_lead(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                                const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
+                                const double *lead_seconds_dev, void *workspace, size_t workspace_bytes,
+                                cudaStream_t stream);
+
 /* Size of the workspace that the library itself holds for
  * wrfgpu_rk3_step_static_workspace: 32 MiB per GPU, reserved in every
  * process that loads the library, on every GPU it runs on, until exit. */
@@ -224,7 +240,10 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *params, const wrfgpu_metrics *metr
  *   - Grids whose wrfgpu_step_workspace_size() exceeds
  *     WRFGPU_STATIC_WORKSPACE_BYTES are rejected with WRFGPU_ERR_WORKSPACE.
  *   - The first call on a GPU looks up the array's device address (with that
- *     GPU current); make that first call before any stream capture.
+ *     GPU current); make that first call before any stream capture.  The
+ *     address is kept for the life of the process and does not survive a
+ *     cudaDeviceReset of that GPU: do not call this entry point on a device
+ *     after resetting it.
  *   - Nothing in the array needs to start at zero: the step writes every
  *     scratch value before reading it, and clears or copies mudf itself.
  *   - Every call on one GPU shares the one array, which keeps the previous
@@ -397,6 +416,17 @@ int wrfgpu_step_epilogue(const wrfgpu_step_params *params, const wrfgpu_step_inp
                          const wrfgpu_step_outputs *out, double lead_seconds, int disable_guards,
                          wrfgpu_theta_limiter_diag *diag, void *workspace, size_t workspace_bytes,
                          cudaStream_t stream);
+
+/* wrfgpu_step_epilogue with the forecast clock on the device (one double at
+ * lead_seconds_dev, seconds), read by the boundary pass's kernels: the
+ * reference passes the traced lead_seconds of its jitted loop to
+ * apply_lateral_boundaries (runtime/operational_mode.py:4966-4969).  Results
+ * are identical to wrfgpu_step_epilogue with the same value on the host. */
+int wrfgpu_step_epilogue_device_lead(const wrfgpu_step_params *params, const wrfgpu_step_inputs *origin,
+                                     const wrfgpu_step_inputs *next, const wrfgpu_lbc_leaves *leaves,
+                                     const wrfgpu_step_outputs *out, const double *lead_seconds_dev,
+                                     int disable_guards, wrfgpu_theta_limiter_diag *diag, void *workspace,
+                                     size_t workspace_bytes, cudaStream_t stream);
 
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);

@@ -231,3 +231,24 @@ def test_sixth_order_diffusion_params(lib):
     for kw in (dict(diff_6th_opt=3), dict(diff_6th_opt=1, diff_6th_factor=float("nan"))):
         assert lib.wrfgpu_step_params_validate(ctypes.byref(_params(lib, **kw))) == \
             _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG
+
+
+def test_torch_op_is_registered_with_a_fake_implementation():
+    """torch.ops.wrfgpu.rk3_step exists and propagates shapes on meta tensors
+    (its fake implementation): 16 state leaves, then the 13 carry outputs."""
+    import torch
+
+    from wrf_gpu_b200 import torch_ops
+
+    nz, ny, nx = 5, 4, 6
+    m = lambda *s: torch.empty(*s, dtype=torch.float64, device="meta")
+    shapes = dict(u=(nz, ny, nx + 1), v=(nz, ny + 1, nx), w=(nz + 1, ny, nx), ph_total=(nz + 1, ny, nx),
+                  ph_perturbation=(nz + 1, ny, nx), mu_total=(ny, nx), mu_perturbation=(ny, nx))
+    fields = [m(*shapes.get(n, (nz, ny, nx))) for n in torch_ops.STEP_FIELDS]
+    res = torch.ops.wrfgpu.rk3_step(fields, [], fields[8], None, 0)
+    assert len(res) == len(torch_ops.STEP_FIELDS) + len(torch_ops.CARRY_OUT)
+    for f, r in zip(fields, res):
+        assert r.shape == f.shape and r.dtype == torch.float64
+    carry = dict(zip(torch_ops.CARRY_OUT, res[len(fields):]))
+    assert carry["ww"].shape == (nz + 1, ny, nx) and carry["mudf"].shape == (ny, nx)
+    assert carry["u_save"].shape == (nz, ny, nx + 1)

@@ -116,11 +116,11 @@ THETA_DIAG_BYTES = 40
 
 
 EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_step_workspace_size",
-            "wrfgpu_rk3_step", "wrfgpu_rk3_step_static_workspace",
+            "wrfgpu_rk3_step", "wrfgpu_rk3_step_device_lead", "wrfgpu_rk3_step_static_workspace",
             "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_scalar_advection",
             "wrfgpu_scalar_advection_adjoint", "wrfgpu_acoustic_workspace_size", "wrfgpu_acoustic_substep",
             "wrfgpu_acoustic_substep_vjp", "wrfgpu_apply_lateral_boundaries",
-            "wrfgpu_step_epilogue_workspace_size", "wrfgpu_step_epilogue", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
+            "wrfgpu_step_epilogue_workspace_size", "wrfgpu_step_epilogue", "wrfgpu_step_epilogue_device_lead", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version")
 
@@ -149,6 +149,10 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_rk3_step.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), ctypes.POINTER(StepInputs),
                                     ctypes.POINTER(StepOutputs), _D, _P, ctypes.c_size_t, _P]
     lib.wrfgpu_rk3_step.restype = _I
+    lib.wrfgpu_rk3_step_device_lead.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
+                                                ctypes.POINTER(StepInputs), ctypes.POINTER(StepOutputs), _P, _P,
+                                                ctypes.c_size_t, _P]
+    lib.wrfgpu_rk3_step_device_lead.restype = _I
     lib.wrfgpu_rk3_step_static_workspace.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
                                                      ctypes.POINTER(StepInputs), ctypes.POINTER(StepOutputs), _D, _P]
     lib.wrfgpu_rk3_step_static_workspace.restype = _I
@@ -185,6 +189,11 @@ def load(path: str | os.PathLike | None = None):
                                          ctypes.POINTER(StepInputs), ctypes.POINTER(LbcLeaves),
                                          ctypes.POINTER(StepOutputs), _D, _I, _P, _P, ctypes.c_size_t, _P]
     lib.wrfgpu_step_epilogue.restype = _I
+    lib.wrfgpu_step_epilogue_device_lead.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(StepInputs),
+                                                     ctypes.POINTER(StepInputs), ctypes.POINTER(LbcLeaves),
+                                                     ctypes.POINTER(StepOutputs), _P, _I, _P, _P, ctypes.c_size_t,
+                                                     _P]
+    lib.wrfgpu_step_epilogue_device_lead.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

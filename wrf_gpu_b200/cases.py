@@ -137,17 +137,25 @@ def _controls(**kw):
     return base
 
 
-def _boundary_leaves(state, nz, ny, nx, times=2, width=5, rng=None):
+def _boundary_leaves(state, nz, ny, nx, times=2, width=5, rng=None, full=False):
     """Specified boundary strips ``(time, side, width, z, side_len)`` (``contracts/state.py:96-106``)
     of u, v, theta (full), ph' (nz+1 levels), mu' (one level) and w (nz+1
     levels), built from the initial edge rows: constant in time, or with
     ``rng`` perturbed by seeded noise and drifting between the two time levels
-    (u/v 0.5 m/s, theta 0.3 K, ph' 20 m2/s2, mu' 30 Pa, w 0.2 m/s)."""
+    (u/v 0.5 m/s, theta 0.3 K, ph' 20 m2/s2, mu' 30 Pa, w 0.2 m/s).  With
+    ``full`` also the strips the end-of-step lateral boundary pass reads
+    (``coupling/boundary_apply.py:170-326``): p', pb, mub, phb and the six
+    mixing ratios, from the same edge rows (unperturbed)."""
     side = max(nx + 1, ny + 1)
     out = {}
     specs = (("u_bdy", state.u, 0.5), ("v_bdy", state.v, 0.5), ("theta_bdy", state.theta, 0.3),
              ("ph_bdy", state.ph_perturbation, 20.0), ("mu_bdy", state.mu_perturbation[None], 30.0),
              ("w_bdy", state.w, 0.2))
+    if full:
+        specs = specs + (("p_bdy", state.p_perturbation, 0.0), ("pb_bdy", state.p_total - state.p_perturbation, 0.0),
+                         ("mub_bdy", (state.mu_total - state.mu_perturbation)[None], 0.0),
+                         ("phb_bdy", state.ph_total - state.ph_perturbation, 0.0)) + \
+            tuple((q + "_bdy", getattr(state, q), 0.0) for q in MOIST)
     for name, fld, scale in specs:
         zl, yl, xl = fld.shape
         leaf = np.zeros((times, 4, width, zl, side))
@@ -156,7 +164,7 @@ def _boundary_leaves(state, nz, ny, nx, times=2, width=5, rng=None):
             leaf[:, 1, b, :, :yl] = fld[:, :, xl - 1 - b]
             leaf[:, 2, b, :, :xl] = fld[:, b, :]
             leaf[:, 3, b, :, :xl] = fld[:, yl - 1 - b, :]
-        if rng is not None:
+        if rng is not None and scale > 0.0:
             leaf = leaf + scale * rng.standard_normal(leaf.shape[1:])[None]
             leaf[1:] = leaf[1:] + 0.5 * scale * rng.standard_normal(leaf[1:].shape)
         out[name] = leaf
@@ -357,34 +365,50 @@ def mountain_wave(nx: int = 256, ny: int = 256, nz: int = 50, *, dx: float = 200
     return Case("mountain_wave", nx, ny, nz, m, dict(c, dx=dx, dy=dx), s, np.zeros((ny, nx)))
 
 
-def crop(case: Case, nx: int, ny: int) -> Case:
-    """Sub-window of a case (periodic wrap of the staggered edge faces), for small parity runs."""
+def crop(case: Case, nx: int, ny: int, j0: int = 0, i0: int = 0, *, full_leaves: bool = False) -> Case:
+    """Sub-window ``[j0:j0+ny, i0:i0+nx]`` of a case (periodic wrap of the
+    staggered edge faces), for parity runs on windows of a full-size case.  A
+    case with boundary strips gets constant strips rebuilt from the window's
+    edge rows (``full_leaves``: also the strips of the end-of-step boundary
+    pass)."""
     s = case.state
     m = case.metrics
     n = SimpleNamespace()
+    jy, ix = slice(j0, j0 + ny), slice(i0, i0 + nx)
+    if j0 + ny > case.ny or i0 + nx > case.nx or j0 < 0 or i0 < 0:
+        raise ValueError("crop window outside the case")
     for k, vv in vars(s).items():
-        if k in ("u_bdy", "v_bdy"):
+        if k.endswith("_bdy"):
             continue
         if k == "u":
-            a = vv[:, :ny, :nx + 1].copy()
+            a = vv[:, jy, i0:i0 + nx + 1].copy()
             a[:, :, nx] = a[:, :, 0]
         elif k == "v":
-            a = vv[:, :ny + 1, :nx].copy()
+            a = vv[:, j0:j0 + ny + 1, ix].copy()
             a[:, ny, :] = a[:, 0, :]
         elif vv.ndim == 3:
-            a = vv[:, :ny, :nx].copy()
+            a = vv[:, jy, ix].copy()
         else:
-            a = vv[:ny, :nx].copy()
+            a = vv[jy, ix].copy()
         setattr(n, k, a)
     mm = SimpleNamespace(**vars(m))
     for k in ("msftx", "msfty", "f", "e", "sina", "cosa"):
-        setattr(mm, k, getattr(m, k)[:ny, :nx].copy())
+        setattr(mm, k, getattr(m, k)[jy, ix].copy())
     for k in ("msfux", "msfuy"):
-        setattr(mm, k, getattr(m, k)[:ny, :nx + 1].copy())
+        setattr(mm, k, getattr(m, k)[jy, i0:i0 + nx + 1].copy())
     for k in ("msfvx", "msfvy"):
-        setattr(mm, k, getattr(m, k)[:ny + 1, :nx].copy())
-    if hasattr(s, "u_bdy"):
-        for kk, val in _boundary_leaves(n, case.nz, ny, nx).items():
+        setattr(mm, k, getattr(m, k)[j0:j0 + ny + 1, ix].copy())
+    if hasattr(s, "u_bdy") or full_leaves:
+        for kk, val in _boundary_leaves(n, case.nz, ny, nx, full=full_leaves).items():
             setattr(n, kk, val)
     return Case(case.name + f"_crop{nx}x{ny}", nx, ny, case.nz, mm, dict(case.controls), n,
-                case.mudf[:ny, :nx].copy(), notes=dict(case.notes))
+                case.mudf[jy, ix].copy(), notes=dict(case.notes, crop=(j0, i0)))
+
+
+def with_full_leaves(case: Case, rng=None) -> Case:
+    """The case with every boundary strip the end-of-step lateral boundary
+    pass reads, built from its initial edge rows (``rng``: the dynamic strips
+    perturbed and drifting in time as ``_boundary_leaves`` does)."""
+    for kk, val in _boundary_leaves(case.state, case.nz, case.ny, case.nx, rng=rng, full=True).items():
+        setattr(case.state, kk, val)
+    return case

@@ -39,7 +39,13 @@ constexpr int COL_NARR = 8;
 // Column widths and level-lane counts the column kernel is instantiated for
 // (the tuner's choices).  A 16-column block holds half the shared memory of a
 // 32-column one, so twice as many blocks are resident per SM.
-constexpr int COL_TX_CHOICES[] = {32, 16};
+constexpr int COL_TX_CHOICES[] = {32, 16, 1};
+// Width of the default column kernel: 1 selects the one-thread-per-column
+// streaming kernel (column_stream.cuh), 16 or 32 this level-parallel one.
+#ifndef WG_COL_DEFAULT_WIDTH
+#define WG_COL_DEFAULT_WIDTH 32
+#endif
+constexpr int COL_DEFAULT_WIDTH = WG_COL_DEFAULT_WIDTH;
 constexpr int COL_TY_CHOICES[] = {8, 13, 16};
 constexpr int col_minb(int tx) { return tx == 16 ? 2 * WG_COL_MINB : WG_COL_MINB; }
 // Levels per software-pipelined batch of the serial recurrences: the batch's

@@ -18,6 +18,7 @@
 #include "acoustic_kernels.cuh"
 #include "finish_kernels.cuh"
 #include "column_tiled.cuh"
+#include "column_stream.cuh"
 #include "tiled_stencils.cuh"
 #include "tiled_faces.cuh"
 #include "tiled_march.cuh"
@@ -407,8 +408,8 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "march_levels must be 0, 5, 10 or 25");
   if (p->column_lanes != 0 && p->column_lanes != 8 && p->column_lanes != 13 && p->column_lanes != 16)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13 or 16");
-  if (p->column_width != 0 && p->column_width != 16 && p->column_width != 32)
-    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 16 or 32");
+  if (p->column_width != 0 && p->column_width != 1 && p->column_width != 16 && p->column_width != 32)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 1, 16 or 32");
   if (p->physics != 0 && p->physics != 1) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "physics must be 0 or 1");
   if (p->diff_6th_opt < 0 || p->diff_6th_opt > 2)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "diff_6th_opt must be 0, 1 or 2");
@@ -460,9 +461,17 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
   return WRFGPU_OK;
 }
 
-int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const wrfgpu_step_inputs *in,
-                    const wrfgpu_step_outputs *out, double lead_seconds, void *workspace, size_t workspace_bytes,
-                    cudaStream_t stream) {
+}  // extern "C"
+
+namespace {
+
+// The RK3 step.  The forecast lead is `lead_seconds` (host; NaN = no lead:
+// boundary forcing off), or with `lead_dev` set a device-resident lead read
+// by the kernels that interpolate boundary strips in time (`lead_seconds` is
+// then only a non-NaN flag).
+int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const wrfgpu_step_inputs *in,
+                  const wrfgpu_step_outputs *out, double lead_seconds, const double *lead_dev, void *workspace,
+                  size_t workspace_bytes, cudaStream_t stream) {
   if (pp == nullptr || mm == nullptr || in == nullptr || out == nullptr)
     return fail(WRFGPU_ERR_NULL_POINTER, "params/metrics/inputs/outputs is NULL");
   int rc = wrfgpu_step_params_validate(pp);
@@ -523,7 +532,8 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   const int ns = p.acoustic_substeps;
   const int kc = (p.march_levels == 5 || p.march_levels == 25) ? p.march_levels : MARCH_KC;
   const int lanes = (p.column_lanes > 0) ? p.column_lanes : COL_TY;
-  const int cwidth = (p.column_width > 0) ? p.column_width : COL_TX;
+  const int cwidth = (p.column_width > 0) ? p.column_width : COL_DEFAULT_WIDTH;
+  const bool col_stream = cwidth == 1;  // one thread per column (column_stream.cuh)
   const double dt_rk[3] = {dt / 3.0, 0.5 * dt, dt};
   const double dts_rk[3] = {dt / 3.0, dt / (double)ns, dt / (double)ns};
   const int nsub[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
@@ -550,31 +560,25 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   }
 
   const double eps1 = 1.0 + p.epssm;
+  // a leaf with its time interpolation at the step's lead plus `off` seconds
+  // (boundary_apply.py:329-345): resolved here, or by the kernels from the
+  // device lead
+  auto leaf_at_off = [&](const double *leaf, double off) {
+    BdyLeaf b{leaf, in->bdy_ntime, in->bdy_width, in->bdy_side_len, 0, 0, 0.0, nullptr, 0.0, p.update_cadence_s};
+    if (lead_dev != nullptr) {
+      b.lead = lead_dev;
+      b.lead_off = off;
+    } else {
+      leaf_time_weights(off == 0.0 ? lead_seconds : lead_seconds + off, p.update_cadence_s, in->bdy_ntime, b.lo,
+                        b.hi, b.alpha);
+    }
+    return b;
+  };
   BdyLeaf bl_u{}, bl_v{};
   if (bdy_active) {
-    const int mx = in->bdy_ntime - 1;
-    const double li = lead_seconds / p.update_cadence_s;
-    int lo = (int)std::floor(li);
-    lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
-    int hi = lo + 1;
-    hi = hi < 0 ? 0 : (hi > mx ? mx : hi);
-    double a = li - (double)lo;
-    a = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
-    bl_u = BdyLeaf{in->u_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
-    bl_v = BdyLeaf{in->v_bdy, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
+    bl_u = leaf_at_off(in->u_bdy, 0.0);
+    bl_v = leaf_at_off(in->v_bdy, 0.0);
   }
-  // a leaf with its time interpolation at one lead (boundary_apply.py:329-345)
-  auto leaf_at = [&](const double *leaf, double lead) {
-    const int mx = in->bdy_ntime - 1;
-    const double li = lead / p.update_cadence_s;
-    int lo = (int)std::floor(li);
-    lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
-    int hi = lo + 1;
-    hi = hi < 0 ? 0 : (hi > mx ? mx : hi);
-    double a = li - (double)lo;
-    a = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
-    return BdyLeaf{leaf, in->bdy_ntime, in->bdy_width, in->bdy_side_len, lo, hi, a};
-  };
   RelaxArgs ra{};
   if (cad || nest_ph_relax || nest_w_relax) {
     // per-second weights as the reference forms them: (dt * fcx) / dt
@@ -599,11 +603,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     // (boundary_apply.py:1148-1248)
     ra.u = in->u; ra.v = in->v; ra.theta = in->theta; ra.ph_pert = in->ph_perturbation;
     ra.mu_total = in->mu_total; ra.mu_pert = in->mu_perturbation;
-    ra.lu = leaf_at(in->u_bdy, lead_seconds);
-    ra.lv = leaf_at(in->v_bdy, lead_seconds);
-    ra.lt = leaf_at(in->theta_bdy, lead_seconds);
-    ra.lph = leaf_at(in->ph_bdy, lead_seconds);
-    ra.lmu = leaf_at(in->mu_bdy, lead_seconds);
+    ra.lu = leaf_at_off(in->u_bdy, 0.0);
+    ra.lv = leaf_at_off(in->v_bdy, 0.0);
+    ra.lt = leaf_at_off(in->theta_bdy, 0.0);
+    ra.lph = leaf_at_off(in->ph_bdy, 0.0);
+    ra.lmu = leaf_at_off(in->mu_bdy, 0.0);
     ra.nfield = 5;
     const int cad_fields[5] = {RELAX_U, RELAX_V, RELAX_THETA, RELAX_PH, RELAX_MU};
     for (int f = 0; f < 5; ++f) ra.fields[f] = cad_fields[f];
@@ -792,11 +796,11 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       rn.ph_tend = w.ph_tend; rn.rw_tend = w.rw_tend;
       rn.nfield = 0;
       if (nest_ph_relax) {
-        rn.lph = leaf_at(in->ph_bdy, lead_seconds);
+        rn.lph = leaf_at_off(in->ph_bdy, 0.0);
         rn.fields[rn.nfield++] = RELAX_PH;
       }
       if (nest_w_relax) {
-        rn.lw = leaf_at(in->w_bdy, lead_seconds);
+        rn.lw = leaf_at_off(in->w_bdy, 0.0);
         rn.fields[rn.nfield++] = RELAX_W;
       }
       const int ring_len = 2 * (nx + 1) + 2 * (ny + 1);
@@ -805,14 +809,14 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
           g, rn);
       LAUNCH_CHECK("k_spec_relax_add");
     }
-    const double lead_stage = lead_seconds + dt_rk[stage];  // stage-end lead of the ring-0 pins
+    // the ring-0 pins interpolate the strips at the stage-end lead, lead + dt_rk[stage]
 
     BdyArgs ba{};
     ba.active = bdy_active ? 1 : 0;
     ba.cad = cad ? 1 : 0;
     if (cad) {
-      ba.cad_u = leaf_at(in->u_bdy, lead_stage);
-      ba.cad_v = leaf_at(in->v_bdy, lead_stage);
+      ba.cad_u = leaf_at_off(in->u_bdy, dt_rk[stage]);
+      ba.cad_v = leaf_at_off(in->v_bdy, dt_rk[stage]);
     }
     if (bdy_active) {
       const int nzone = p.spec_zone + p.relax_zone;
@@ -847,23 +851,27 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
     ca.rzdamp = (p.zdamp != 0.0 && std::isfinite(1.0 / p.zdamp)) ? 1.0 / p.zdamp : 0.0;
     ca.cad = cad ? 1 : 0;
     if (cad) {
-      ca.cad_mu = leaf_at(in->mu_bdy, lead_stage);
-      ca.cad_th = leaf_at(in->theta_bdy, lead_stage);
+      ca.cad_mu = leaf_at_off(in->mu_bdy, dt_rk[stage]);
+      ca.cad_th = leaf_at_off(in->theta_bdy, dt_rk[stage]);
       ca.mub = w.mub;
     }
     ca.ph_pin = (cad || nest_ph_pin) ? 1 : 0;
     if (ca.ph_pin) {
       // the cadence pins to the stage-end lead, the nested child to the step's lead
-      ca.cad_ph = leaf_at(in->ph_bdy, cad ? lead_stage : lead_seconds);
+      ca.cad_ph = leaf_at_off(in->ph_bdy, cad ? dt_rk[stage] : 0.0);
       ca.ph_save = s.ph_pert;
     }
-    const size_t col_smem = column_tiled_smem_bytes(nz, cwidth);
+    const size_t col_smem = col_stream ? column_stream_smem_bytes(nz) : column_tiled_smem_bytes(nz, cwidth);
     // the ring-0 pins are compiled into their own instantiations
     const bool pins = cad || nest_ph_pin;
 #define WG_COL(TX, TY) (pins ? k_column_tiled<TX, TY, true> : k_column_tiled<TX, TY, false>)
-    auto kColumn = (cwidth == 16) ? ((lanes == 8) ? WG_COL(16, 8) : (lanes == 16) ? WG_COL(16, 16) : WG_COL(16, 13))
-                                  : ((lanes == 8) ? WG_COL(32, 8) : (lanes == 16) ? WG_COL(32, 16) : WG_COL(32, 13));
+    auto kColumn = col_stream ? (pins ? k_column_stream<true> : k_column_stream<false>)
+                   : (cwidth == 16) ? ((lanes == 8) ? WG_COL(16, 8) : (lanes == 16) ? WG_COL(16, 16) : WG_COL(16, 13))
+                                    : ((lanes == 8) ? WG_COL(32, 8) : (lanes == 16) ? WG_COL(32, 16) : WG_COL(32, 13));
 #undef WG_COL
+    const dim3 col_grid = col_stream ? dim3((nx + 31) / 32, (ny + CS_WARPS - 1) / CS_WARPS, 1)
+                                     : dim3((nx + cwidth - 1) / cwidth, ny, 1);
+    const dim3 col_block = col_stream ? dim3(32, CS_WARPS, 1) : dim3(cwidth, lanes, 1);
     auto kAdvanceUV = cad ? k_advance_uv<true> : k_advance_uv<false>;
     if (stage == 0 && cudaFuncSetAttribute(kColumn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem) !=
                           cudaSuccess)
@@ -877,8 +885,7 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
       k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, specified ? 1 : 0, w.dvdxi, w.hdiv);
       LAUNCH_CHECK("k_div_h");
       PROF("k_column");
-      kColumn<<<dim3((nx + cwidth - 1) / cwidth, ny, 1), dim3(cwidth, lanes, 1), col_smem, stream>>>(g, A, ca, w.dvdxi,
-                                                                                                      w.hdiv);
+      kColumn<<<col_grid, col_block, col_smem, stream>>>(g, A, ca, w.dvdxi, w.hdiv);
       LAUNCH_CHECK("k_column");
       if (cad) {
         PROF("k_spec_w");
@@ -930,6 +937,24 @@ int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, cons
   return WRFGPU_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int wrfgpu_rk3_step(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const wrfgpu_step_inputs *in,
+                    const wrfgpu_step_outputs *out, double lead_seconds, void *workspace, size_t workspace_bytes,
+                    cudaStream_t stream) {
+  return rk3_step_impl(pp, mm, in, out, lead_seconds, nullptr, workspace, workspace_bytes, stream);
+}
+
+int wrfgpu_rk3_step_device_lead(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm,
+                                const wrfgpu_step_inputs *in, const wrfgpu_step_outputs *out,
+                                const double *lead_seconds_dev, void *workspace, size_t workspace_bytes,
+                                cudaStream_t stream) {
+  if (lead_seconds_dev == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "lead_seconds_dev is NULL");
+  return rk3_step_impl(pp, mm, in, out, 0.0, lead_seconds_dev, workspace, workspace_bytes, stream);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -943,6 +968,12 @@ static __device__ __align__(256) unsigned char g_static_workspace[WRFGPU_STATIC_
 namespace {
 constexpr int kMaxStaticDevices = 64;
 std::mutex g_static_ws_mutex;
+// Device address of the array per device ordinal, looked up on the first call
+// and kept for the life of the process.  It belongs to the device context that
+// was current then: after cudaDeviceReset (or anything else that destroys and
+// recreates the primary context) the module is loaded again and this cached
+// address is stale, so a process that resets a device must not call the
+// static-workspace step on it afterwards.
 void *g_static_ws_addr[kMaxStaticDevices] = {};
 }  // namespace
 
@@ -1089,10 +1120,12 @@ extern "C" int wrfgpu_autotune(wrfgpu_step_params *pp, const wrfgpu_metrics *mm,
   };
   wrfgpu_step_params best = *pp;
   float best_ms = 1e30f;
-  // column block shapes first (march levels at the default), then march levels
+  // column block shapes first (march levels at the default), then march levels;
+  // width 1 is the one-thread-per-column kernel (its lane count is unused)
   for (int cw : COL_TX_CHOICES) {
     for (int l : COL_TY_CHOICES) {
       if (rc) break;
+      if (cw == 1 && l != COL_TY_CHOICES[0]) continue;
       wrfgpu_step_params p = *pp;
       p.column_width = cw;
       p.column_lanes = l;
@@ -1416,22 +1449,18 @@ int epilogue_check(const wrfgpu_step_params *p, const wrfgpu_step_inputs *in, co
 // pass (when `boundary`) with the guards fused before and after it (when
 // `guards`; `gs` / `after` are the theta limiter's scalars and partials).
 int epilogue_fields(const wrfgpu_step_params *p, const wrfgpu_step_inputs *org, const wrfgpu_step_inputs *in,
-                    const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out, double lead_seconds, bool guards,
-                    bool boundary, bool spec_only, const GuardScalars *gs, double *after, int *theta_slots,
-                    cudaStream_t stream) {
+                    const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out, double lead_seconds,
+                    const double *lead_dev, bool guards, bool boundary, bool spec_only, const GuardScalars *gs,
+                    double *after, int *theta_slots, cudaStream_t stream) {
   const int nx = p->nx, ny = p->ny, nz = p->nz;
   BdyLeaf nolf{};
   auto leaf = [&](const double *x) -> BdyLeaf {
     if (!boundary || x == nullptr) return nolf;
-    // strips at the lead (boundary_apply.py:329-345)
-    const int mx = lv->ntime - 1;
-    const double li = lead_seconds / p->update_cadence_s;
-    int lo = (int)std::floor(li);
-    lo = lo < 0 ? 0 : (lo > mx ? mx : lo);
-    const int hi = lo + 1 > mx ? mx : lo + 1;
-    double al = li - (double)lo;
-    al = al < 0.0 ? 0.0 : (al > 1.0 ? 1.0 : al);
-    return BdyLeaf{x, lv->ntime, lv->width, lv->side_len, lo, hi, al};
+    // strips at the lead (boundary_apply.py:329-345), on the host or read
+    // from the device lead by the kernels
+    BdyLeaf b{x, lv->ntime, lv->width, lv->side_len, 0, 0, 0.0, lead_dev, 0.0, p->update_cadence_s};
+    if (lead_dev == nullptr) leaf_time_weights(lead_seconds, p->update_cadence_s, lv->ntime, b.lo, b.hi, b.alpha);
+    return b;
   };
   // dt*fcx, dt*gcx of the relax rows (boundary_apply.py:666-688, spec_exp 0)
   LbcJob base{};
@@ -1583,8 +1612,8 @@ extern "C" int wrfgpu_apply_lateral_boundaries(const wrfgpu_step_params *p, cons
   int rc = epilogue_check(p, in, lv, out, true, dry_spec_only != 0, lead_seconds);
   if (rc) return rc;
   int slots = 0;
-  rc = epilogue_fields(p, nullptr, in, lv, out, lead_seconds, false, true, dry_spec_only != 0, nullptr, nullptr,
-                       &slots, stream);
+  rc = epilogue_fields(p, nullptr, in, lv, out, lead_seconds, nullptr, false, true, dry_spec_only != 0, nullptr,
+                       nullptr, &slots, stream);
   if (rc) return rc;
   g_last_error.clear();
   return WRFGPU_OK;
@@ -1599,10 +1628,14 @@ extern "C" int wrfgpu_step_epilogue_workspace_size(const wrfgpu_step_params *p, 
   return WRFGPU_OK;
 }
 
-extern "C" int wrfgpu_step_epilogue(const wrfgpu_step_params *p, const wrfgpu_step_inputs *origin,
-                                    const wrfgpu_step_inputs *next, const wrfgpu_lbc_leaves *lv,
-                                    const wrfgpu_step_outputs *out, double lead_seconds, int disable_guards,
-                                    wrfgpu_theta_limiter_diag *diag, void *ws, size_t ws_bytes, cudaStream_t stream) {
+namespace {
+
+// The step epilogue at a host lead, or (lead_dev set) at a device-resident
+// lead that the boundary kernels read.
+int step_epilogue_impl(const wrfgpu_step_params *p, const wrfgpu_step_inputs *origin, const wrfgpu_step_inputs *next,
+                       const wrfgpu_lbc_leaves *lv, const wrfgpu_step_outputs *out, double lead_seconds,
+                       const double *lead_dev, int disable_guards, wrfgpu_theta_limiter_diag *diag, void *ws,
+                       size_t ws_bytes, cudaStream_t stream) {
   if (p == nullptr || next == nullptr || out == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "params/next/out is NULL");
   const bool guards = disable_guards == 0;
   const bool boundary = p->run_boundary != 0;
@@ -1637,8 +1670,8 @@ extern "C" int wrfgpu_step_epilogue(const wrfgpu_step_params *p, const wrfgpu_st
     if ((rc = check_launch("k_guard_finalize"))) return rc;
   }
   int slots = 0;
-  rc = epilogue_fields(p, guards ? origin : nullptr, next, lv, out, lead_seconds, guards, boundary, spec_only, gs,
-                       after, &slots, stream);
+  rc = epilogue_fields(p, guards ? origin : nullptr, next, lv, out, lead_seconds, lead_dev, guards, boundary,
+                       spec_only, gs, after, &slots, stream);
   if (rc) return rc;
   if (diag != nullptr) {
     if (guards)
@@ -1649,6 +1682,26 @@ extern "C" int wrfgpu_step_epilogue(const wrfgpu_step_params *p, const wrfgpu_st
   }
   g_last_error.clear();
   return WRFGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int wrfgpu_step_epilogue(const wrfgpu_step_params *p, const wrfgpu_step_inputs *origin,
+                                    const wrfgpu_step_inputs *next, const wrfgpu_lbc_leaves *lv,
+                                    const wrfgpu_step_outputs *out, double lead_seconds, int disable_guards,
+                                    wrfgpu_theta_limiter_diag *diag, void *ws, size_t ws_bytes, cudaStream_t stream) {
+  return step_epilogue_impl(p, origin, next, lv, out, lead_seconds, nullptr, disable_guards, diag, ws, ws_bytes,
+                            stream);
+}
+
+extern "C" int wrfgpu_step_epilogue_device_lead(const wrfgpu_step_params *p, const wrfgpu_step_inputs *origin,
+                                                const wrfgpu_step_inputs *next, const wrfgpu_lbc_leaves *lv,
+                                                const wrfgpu_step_outputs *out, const double *lead_seconds_dev,
+                                                int disable_guards, wrfgpu_theta_limiter_diag *diag, void *ws,
+                                                size_t ws_bytes, cudaStream_t stream) {
+  if (lead_seconds_dev == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "lead_seconds_dev is NULL");
+  return step_epilogue_impl(p, origin, next, lv, out, 0.0, lead_seconds_dev, disable_guards, diag, ws, ws_bytes,
+                            stream);
 }
 
 extern "C" int wrfgpu_scalar_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,

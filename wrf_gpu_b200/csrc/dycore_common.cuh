@@ -193,20 +193,44 @@ __device__ __forceinline__ double hflux_spec(int m, int n, bool upstream, double
 // A specified boundary leaf (time, side W/E/S/N, width, z, side_len)
 // (contracts/state.py:96-106) with its time interpolation at one lead
 // (boundary_apply.py:329-345: lower / upper time index and weight).
+// A boundary leaf (time, side, width, levels, side_len) and its time
+// interpolation at one lead (boundary_apply.py:329-345): (lo, hi, alpha)
+// resolved on the host, or -- when `lead` is set -- on the device from the
+// forecast clock *lead + lead_off, so a step can run with a device-resident
+// lead (a traced clock, or one graph replayed with a changing lead).
 struct BdyLeaf {
   const double *leaf;
   int ntime, width, side_len, lo, hi;
   double alpha;
+  const double *lead;  // device lead in seconds, or nullptr
+  double lead_off;     // seconds added to *lead (a stage-end lead)
+  double cadence;      // the strips' update cadence in seconds
 };
+
+// (lo, hi, alpha) of a leaf at lead L: the reference's clipped floor index of
+// L / cadence and its clipped fraction.
+__host__ __device__ __forceinline__ void leaf_time_weights(double L, double cadence, int ntime, int &lo, int &hi,
+                                                           double &alpha) {
+  const int mx = ntime - 1;
+  const double li = L / cadence;
+  const double fl = floor(li);
+  lo = fl < 0.0 ? 0 : (fl > (double)mx ? mx : (int)fl);
+  hi = lo + 1 > mx ? mx : lo + 1;
+  double a = li - (double)lo;
+  alpha = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
+}
 
 // Strip value of side `side`, width index bb (clamped, boundary_apply.py:528-549),
 // level k, tangential index t; nz is the leaf's level count.
 __device__ __forceinline__ double strip_at(const BdyLeaf &b, int nz, int side, int bb, int k, int t) {
   bb = bb < 0 ? 0 : (bb > b.width - 1 ? b.width - 1 : bb);
+  int lo = b.lo, hi = b.hi;
+  double alpha = b.alpha;
+  if (b.lead != nullptr) leaf_time_weights(*b.lead + b.lead_off, b.cadence, b.ntime, lo, hi, alpha);
   auto at = [&](int tt) {
     return ld(b.leaf, ((((size_t)tt * 4 + side) * b.width + bb) * nz + k) * b.side_len + t);
   };
-  return at(b.lo) * (1.0 - b.alpha) + at(b.hi) * b.alpha;
+  return at(lo) * (1.0 - alpha) + at(hi) * alpha;
 }
 
 // Value at (k, j, i) of the leaf written into the outer five rows / columns of

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+from collections import OrderedDict
 from dataclasses import dataclass, field, fields, replace
 from typing import Any
 
@@ -345,19 +346,24 @@ def step_params(nl: OperationalNamelist) -> _capi.StepParams:
 class Stepper:
     """Prepared step for one namelist: params, metrics struct, workspace."""
 
-    def __init__(self, nl: OperationalNamelist, device="cuda", physics: bool = False):
+    def __init__(self, nl: OperationalNamelist, device="cuda", physics: bool = False, own_workspace: bool = True):
         reason = _unsupported(nl, None)
         if reason:
             raise NotImplementedError(reason)
         self.lib = _capi.load()
         self.nl = nl
+        self.device = torch.device(device)
         self.params = step_params(nl)
         # a DryPhysicsTendencies bundle is merged into every stage (rk_addtend_dry)
         self.params.physics = 1 if physics else 0
         _capi.check(self.lib.wrfgpu_step_params_validate(ctypes.byref(self.params)))
         nbytes = ctypes.c_size_t(0)
         _capi.check(self.lib.wrfgpu_step_workspace_size(ctypes.byref(self.params), ctypes.byref(nbytes)))
-        self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8, device=device)
+        self.workspace_bytes = int(nbytes.value)
+        # without an own workspace, every step_into takes one from torch's
+        # caching allocator on the launching stream (stream-ordered reuse)
+        self.workspace = (torch.empty(self.workspace_bytes, dtype=torch.uint8, device=device)
+                          if own_workspace else None)
         self.metrics = _capi.Metrics(*[_ptr(getattr(nl.metrics, n)) for n in METRIC_ARRAYS])
         n = ctypes.c_int(0)
         _capi.check(self.lib.wrfgpu_step_launch_count(ctypes.byref(self.params), ctypes.byref(n)))
@@ -415,13 +421,23 @@ class Stepper:
     def step_into(self, carry: OperationalCarry, out: OperationalCarry, lead_seconds=None, stream=None,
                   physics=None) -> None:
         """Enqueue one step from ``carry`` into the preallocated ``out`` (no sync);
-        ``physics`` as in ``rk_scan_step``."""
+        ``physics`` as in ``rk_scan_step``.  ``lead_seconds``: None, a float,
+        or a one-element float64 tensor on the device (the traced-clock form:
+        the kernels read it, so no host value is needed)."""
         ins, outs = self._structs(carry, out, physics)
-        lead = float("nan") if lead_seconds is None else float(lead_seconds)
-        st = torch.cuda.current_stream() if stream is None else stream
-        rc = self.lib.wrfgpu_rk3_step(ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(ins),
-                                      ctypes.byref(outs), lead, ctypes.c_void_p(self.workspace.data_ptr()),
-                                      ctypes.c_size_t(self.workspace.numel()), ctypes.c_void_p(st.cuda_stream))
+        st = torch.cuda.current_stream(self.device) if stream is None else stream
+        ws = self.workspace
+        if ws is None:
+            with torch.cuda.stream(st):
+                ws = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=self.device)
+        args = (ctypes.byref(self.params), ctypes.byref(self.metrics), ctypes.byref(ins), ctypes.byref(outs))
+        tail = (ctypes.c_void_p(ws.data_ptr()), ctypes.c_size_t(ws.numel()), ctypes.c_void_p(st.cuda_stream))
+        if isinstance(lead_seconds, torch.Tensor):
+            lead_dev = _device_lead(lead_seconds, self.device)
+            rc = self.lib.wrfgpu_rk3_step_device_lead(*args, ctypes.c_void_p(lead_dev.data_ptr()), *tail)
+        else:
+            lead = float("nan") if lead_seconds is None else float(lead_seconds)
+            rc = self.lib.wrfgpu_rk3_step(*args, lead, *tail)
         _capi.check(rc)
 
     def autotune(self, carry: OperationalCarry, out: OperationalCarry, stream=None) -> tuple[int, int, int]:
@@ -466,7 +482,47 @@ class BatchStepper:
         _capi.check(self.lib.wrfgpu_rk3_step_batched(n, P, M, I, O, L, W, B, ctypes.c_void_p(st.cuda_stream)))
 
 
-_STEPPERS: dict[tuple, Stepper] = {}
+def _same_device(a, b) -> bool:
+    a, b = torch.device(a), torch.device(b)
+    if a.type != b.type:
+        return False
+    cur = torch.cuda.current_device() if a.type == "cuda" else 0
+    return (cur if a.index is None else a.index) == (cur if b.index is None else b.index)
+
+
+def _device_lead(t: torch.Tensor, device) -> torch.Tensor:
+    if t.numel() != 1 or t.dtype != torch.float64 or not _same_device(t.device, device):
+        raise ValueError("a device lead_seconds must be one float64 element on the step's device")
+    return t.reshape(1)
+
+
+# Prepared steps (params and metric pointers, no workspace) of recent
+# namelists, keyed by their content so that a caller who builds a new
+# namelist per call (the reference's ``namelist.replace(...)`` idiom) reuses
+# them; bounded, least recently used evicted first.
+_PLANS: "OrderedDict[tuple, Stepper]" = OrderedDict()
+_PLAN_CAPACITY = 8
+
+
+def _plan_key(nl: OperationalNamelist, physics: bool, device) -> tuple:
+    p = step_params(nl)
+    m = nl.metrics
+    ptrs = tuple(getattr(m, n).data_ptr() for n in METRIC_ARRAYS)
+    return bytes(ctypes.string_at(ctypes.addressof(p), ctypes.sizeof(p))), ptrs, bool(physics), str(device)
+
+
+def _plan_for(nl: OperationalNamelist, physics: bool, device) -> Stepper:
+    key = _plan_key(nl, physics, device)
+    stp = _PLANS.get(key)
+    if stp is None:
+        stp = Stepper(nl, device=device, physics=physics, own_workspace=False)
+        _PLANS[key] = stp
+        while len(_PLANS) > _PLAN_CAPACITY:
+            _PLANS.popitem(last=False)
+    else:
+        _PLANS.move_to_end(key)
+        stp.nl = nl  # the base tendencies are read from the namelist at call time
+    return stp
 
 
 @dataclass
@@ -483,7 +539,12 @@ def rk_scan_step(carry: OperationalCarry, namelist: OperationalNamelist, *, debu
     """Drop-in for ``_rk_scan_step`` (runtime/operational_mode.py:3319-3534).
 
     Returns a new ``OperationalCarry``; ``carry`` is not modified.  The step is
-    enqueued on the current CUDA stream and is not synchronised.
+    enqueued on the current CUDA stream and is not synchronised; its scratch
+    comes from torch's caching allocator on that stream, so calls on
+    different streams never share a workspace.  ``lead_seconds`` is None, a
+    float, or a one-element float64 device tensor (the reference's traced
+    clock: the kernels read it, so the call can sit in a captured graph whose
+    replays advance the clock on the device).
     ``physics_tendencies`` is a DryPhysicsTendencies-like bundle
     (dynamics/core/rk_addtend_dry.py:103-124: ru_tendf, rv_tendf, rw_tendf,
     ph_tendf, t_tendf, mu_tendf, h_diabatic, u_save, v_save, w_save, ph_save,
@@ -494,11 +555,7 @@ def rk_scan_step(carry: OperationalCarry, namelist: OperationalNamelist, *, debu
     if reason:
         raise NotImplementedError(reason)
     with_physics = physics_tendencies is not None
-    key = (id(namelist), with_physics)
-    stp = _STEPPERS.get(key)
-    if stp is None or stp.nl is not namelist:
-        stp = Stepper(namelist, device=carry.state.u.device, physics=with_physics)
-        _STEPPERS[key] = stp
+    stp = _plan_for(namelist, with_physics, carry.state.u.device)
     if carry.mudf is None:
         carry = carry.replace(mudf=torch.zeros_like(carry.state.mu_total))
     out = stp.alloc_carry(carry)
@@ -602,8 +659,9 @@ def step_epilogue(next_state: State, origin: State, lead_seconds, nl: Operationa
     mixing-ratio guards against ``origin`` (the step-start state); with
     ``nl.run_boundary`` the end-of-step lateral boundary pass (ring 0 only
     when the specified boundary cadence is active) and the guards of the
-    bounded state.  Returns (State, limiter diagnostics); enqueued on the
-    current stream, not synchronised."""
+    bounded state.  ``lead_seconds`` is a float or a one-element float64
+    device tensor (read by the boundary kernels).  Returns (State, limiter
+    diagnostics); enqueued on the current stream, not synchronised."""
     lib = _capi.load()
     p = step_params(nl)
     dev = next_state.u.device
@@ -616,9 +674,33 @@ def step_epilogue(next_state: State, origin: State, lead_seconds, nl: Operationa
     org = _inputs_struct(origin)
     lv = _leaves_struct(next_state) if nl.run_boundary else None
     st = torch.cuda.current_stream(dev)
-    _capi.check(lib.wrfgpu_step_epilogue(ctypes.byref(p), ctypes.byref(org), ctypes.byref(ins),
-                                         None if lv is None else ctypes.byref(lv), ctypes.byref(outs),
-                                         float(lead_seconds), int(bool(nl.disable_guards)),
-                                         ctypes.c_void_p(raw.data_ptr()), ctypes.c_void_p(wsp), n.value,
-                                         ctypes.c_void_p(st.cuda_stream)))
+    head = (ctypes.byref(p), ctypes.byref(org), ctypes.byref(ins), None if lv is None else ctypes.byref(lv),
+            ctypes.byref(outs))
+    tail = (int(bool(nl.disable_guards)), ctypes.c_void_p(raw.data_ptr()), ctypes.c_void_p(wsp), n.value,
+            ctypes.c_void_p(st.cuda_stream))
+    if isinstance(lead_seconds, torch.Tensor):
+        lead_dev = _device_lead(lead_seconds, dev)
+        _capi.check(lib.wrfgpu_step_epilogue_device_lead(*head, ctypes.c_void_p(lead_dev.data_ptr()), *tail))
+    else:
+        _capi.check(lib.wrfgpu_step_epilogue(*head, float(lead_seconds), *tail))
     return out, theta_limiter_diagnostics(raw)
+
+
+def forecast_step(carry: OperationalCarry, namelist: OperationalNamelist, step_index, *, debug: bool = False):
+    """One forecast step without physics, as the reference's
+    ``_physics_boundary_step_with_limiter_diagnostics``
+    (runtime/operational_mode.py:4915-4993) runs it with physics off: the
+    clock ``lead_seconds = step_index * dt``, ``rk_scan_step`` at that lead,
+    then the post-step guards and the end-of-step lateral boundary pass
+    (``step_epilogue``; ring 0 only under the specified boundary cadence).
+    ``step_index`` is an int or a one-element float64 device tensor (then the
+    lead is formed on the device and the step reads it there).  Returns the
+    new carry and the theta limiter's diagnostics; not synchronised."""
+    if isinstance(step_index, torch.Tensor):
+        lead = (step_index.to(torch.float64) * float(namelist.dt_s)).reshape(1)
+    else:
+        lead = float(step_index) * float(namelist.dt_s)
+    origin = carry.state
+    nxt = rk_scan_step(carry, namelist, debug=debug, lead_seconds=lead)
+    state, diag = step_epilogue(nxt.state, origin, lead, namelist)
+    return nxt.replace(state=state), diag
