@@ -136,6 +136,23 @@ typedef struct wrfgpu_step_params {
    * diff_6th_factor * 0.015625 / (2 dt) (default factor 0.12). */
   int diff_6th_opt;
   double diff_6th_factor;
+  /* Second-order explicit diffusion (operational_mode.py:2878-2960), added
+   * to every stage's coupled u, v, w, theta tendencies after the 6th-order
+   * filter:
+   *   diff_opt = 1 with km_opt = 4: WRF's 2-D Smagorinsky horizontal
+   *     diffusion on coordinate surfaces (the real-data default), eddy
+   *     viscosity c_s^2 l^2 |D| capped at 10 l, l = sqrt(dx dy), heat
+   *     diffusivity xkmh / prandtl (dynamics/explicit_diffusion.py:960-1365);
+   *     c_s is OperationalNamelist.c_s (default 0.25);
+   *   const_nu_m2_s > 0: constant-K diffusion in the mass-conservative flux
+   *     form, horizontal and vertical (explicit_diffusion.py:282-331).
+   * Other diff_opt / km_opt pairs select nothing in the reference except
+   * diff_opt = 2 with km_opt 2, 3 or 5 (the TKE / 3-D Smagorinsky closures),
+   * which are rejected as not built. */
+  int diff_opt;
+  int km_opt;
+  double c_s;
+  double const_nu_m2_s;
 } wrfgpu_step_params;
 
 /* DycoreMetrics device arrays (contracts/grid.py:66-126). */

@@ -75,6 +75,10 @@ class Namelist:
     w_coriolis: bool = True         # GPUWRF_W_CORIOLIS default (operational_mode.py:1793)
     diff_6th_opt: int = 0           # operational_mode.py:491 (0 off; 1 and 2 apply the monotonic filter)
     diff_6th_factor: float = 0.12   # operational_mode.py:492
+    diff_opt: int = 0               # operational_mode.py:475 (1 with km_opt 4: 2-D Smagorinsky)
+    km_opt: int = 0                 # operational_mode.py:476
+    c_s: float = 0.25               # operational_mode.py:482 (explicit_diffusion.py:957 C_S_DEFAULT)
+    const_nu_m2_s: float = 0.0      # operational_mode.py:494 (> 0: constant-K diffusion)
     base_tend: dict | None = None   # namelist.tendencies u/v/w/theta/mu (zero when None)
 
 
@@ -741,8 +745,117 @@ def sixth_order_diffusion_tendency(f, dt, factor):
     return t
 
 
+PRANDTL = 1.0 / 3.0  # explicit_diffusion.py:956
+
+
+def horizontal_deformation_2d(u, v, dx, dy):
+    """``horizontal_deformation_2d`` (explicit_diffusion.py:960-1113) as the
+    stage calls it (operational_mode.py:2950: no metric arguments, so the map
+    factors are one and the zx / zy slope terms multiply zero): D11 = 2 du/dx
+    and D22 = 2 dv/dy on mass cells, D12 = du/dy + dv/dx on the cell's SW
+    corner; u and v without their wrap faces, neighbours rolled."""
+    nx = u.shape[2] - 1
+    ny = v.shape[1] - 1
+    um = u[:, :, :nx]
+    vm = v[:, :ny, :]
+    d11 = 2.0 * ((np.roll(um, -1, axis=2) - um) / dx)
+    d22 = 2.0 * ((np.roll(vm, -1, axis=1) - vm) / dy)
+    dudy = (um - np.roll(um, 1, axis=1)) / dy
+    dvdx = (vm - np.roll(vm, 1, axis=2)) / dx
+    return d11, d22, dudy + dvdx
+
+
+def smag2d_horizontal_km(d11, d22, d12, dx, dy, c_s):
+    """``smag2d_horizontal_km`` (explicit_diffusion.py:1116-1212), unit map
+    factors, no slope reduction: the four-corner D12 average, def2, the
+    mixing length sqrt(dx dy), xkmh = c_s^2 l^2 sqrt(def2) capped at 10 l,
+    xkhh = xkmh / prandtl."""
+    nw = np.roll(d12, -1, axis=1)
+    se = np.roll(d12, -1, axis=2)
+    ne = np.roll(np.roll(d12, -1, axis=1), -1, axis=2)
+    tmp = 0.25 * (d12 + nw + se + ne)
+    def2 = 0.25 * (d11 - d22) * (d11 - d22) + tmp * tmp
+    mlen_h = np.sqrt((dx / 1.0) * (dy / 1.0))
+    xkmh = c_s * c_s * mlen_h * mlen_h * np.sqrt(def2)
+    xkmh = np.minimum(xkmh, 10.0 * mlen_h)
+    return xkmh, xkmh / PRANDTL
+
+
+def hdiff_coord(field, k, mass, dx, dy):
+    """``_hdiff_coord_scalar`` (explicit_diffusion.py:1233-1284): the
+    mass-coupled variable-K flux divergence along coordinate surfaces, face K
+    and face mass the averages of the two cells, neighbours rolled; the y part
+    only for fields with more than one row."""
+    rdx, rdy = 1.0 / dx, 1.0 / dy
+    r = lambda a, n, ax: np.roll(a, n, axis=ax)
+    mkrdxp = 0.5 * (r(k, -1, 2) + k) * (0.5 * (r(mass, -1, 2) + mass)) * rdx
+    mkrdxm = 0.5 * (k + r(k, 1, 2)) * (0.5 * (mass + r(mass, 1, 2))) * rdx
+    tend = rdx * (mkrdxp * (r(field, -1, 2) - field) - mkrdxm * (field - r(field, 1, 2)))
+    if field.shape[1] > 1:
+        mkrdyp = 0.5 * (r(k, -1, 1) + k) * (0.5 * (r(mass, -1, 1) + mass)) * rdy
+        mkrdym = 0.5 * (k + r(k, 1, 1)) * (0.5 * (mass + r(mass, 1, 1))) * rdy
+        tend = tend + rdy * (mkrdyp * (r(field, -1, 1) - field) - mkrdym * (field - r(field, 1, 1)))
+    return tend
+
+
+def k_to_w_levels(k):
+    """``_xkmhd_to_w_levels`` (explicit_diffusion.py:1215-1230)."""
+    nz = k.shape[0]
+    out = np.zeros((nz + 1,) + k.shape[1:])
+    out[1:nz] = 0.5 * (k[1:nz] + k[0:nz - 1])
+    out[0] = k[0]
+    out[nz] = k[nz - 1]
+    return out
+
+
+def smagorinsky_2d_tendencies(s, mass_u, mass_v, mass_h, mass_f, dx, dy, c_s):
+    """The diff_opt=1 / km_opt=4 block of the stage (operational_mode.py:
+    2946-2960): coupled u, v, w, theta tendencies (theta as the perturbation
+    from 300 K, with xkhh; momentum with xkmh on each field's own stagger,
+    wrap faces repeated)."""
+    d11, d22, d12 = horizontal_deformation_2d(s.u, s.v, dx, dy)
+    xkmh, xkhh = smag2d_horizontal_km(d11, d22, d12, dx, dy, c_s)
+    nz, ny, nx = s.theta.shape
+    th = hdiff_coord(s.theta - T0, xkhh, mass_h, dx, dy)
+    du = hdiff_coord(s.u[:, :, :nx], xkmh, mass_u[:, :, :nx], dx, dy)
+    dv = hdiff_coord(s.v[:, :ny, :], xkmh, mass_v[:, :ny, :], dx, dy)
+    dw = hdiff_coord(s.w, k_to_w_levels(xkmh), mass_f, dx, dy)
+    du = np.concatenate((du, du[:, :, :1]), axis=2)
+    dv = np.concatenate((dv, dv[:, :1, :]), axis=1)
+    return du, dv, dw, th
+
+
+def const_k_diffusion(field, mass, nu, dx, dy, dz):
+    """``conservative_constant_k_diffusion_tendency`` (explicit_diffusion.py:
+    282-331): d/dx_j(mass K d field/dx_j), periodic rolls over the field's
+    own extent horizontally, zero flux through the bottom and top faces."""
+    r = lambda a, n, ax: np.roll(a, n, axis=ax)
+    tend = np.zeros_like(field)
+    mass_xf = 0.5 * (mass + r(mass, -1, 2))
+    fx = mass_xf * nu * (r(field, -1, 2) - field) / dx
+    tend = tend + (fx - r(fx, 1, 2)) / dx
+    if field.shape[1] > 1:
+        mass_yf = 0.5 * (mass + r(mass, -1, 1))
+        fy = mass_yf * nu * (r(field, -1, 1) - field) / dy
+        tend = tend + (fy - r(fy, 1, 1)) / dy
+    nz = field.shape[0]
+    if nz > 2:
+        mass_zf = 0.5 * (mass[:-1] + mass[1:])
+        flux = np.zeros((nz + 1,) + field.shape[1:])
+        flux[1:nz] = mass_zf * nu * (field[1:] - field[:-1]) / dz
+        tend = tend + (flux[1:] - flux[:nz]) / dz
+    return tend
+
+
+def const_k_dz(ph_total):
+    """The stage's mean physical layer depth for the constant-K vertical term
+    (operational_mode.py:2757-2758): max(mean(diff(ph)/g), 1)."""
+    return max(float(np.mean((ph_total[1:] - ph_total[:-1]) / G)), 1.0)
+
+
 def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_relax=None, physics=None):
-    """operational_mode.py:2722-3093 (flux advection on, diffusion off), with
+    """operational_mode.py:2722-3093 (flux advection on; the 6th-order filter,
+    constant-K and 2-D Smagorinsky diffusion when selected), with
     the physics merge (:3062-3075) when ``physics`` is given."""
     m = nl.metrics
     rdx, rdy = 1.0 / nl.dx, 1.0 / nl.dy
@@ -776,6 +889,18 @@ def augment_large_step_tendencies(s, origin, vel, nl: Namelist, rk_step, bdy_rel
         v_t = v_t + mass_v * sixth_order_diffusion_tendency(s.v, nl.dt_s, f6)
         w_t = w_t + mass_f * sixth_order_diffusion_tendency(s.w, nl.dt_s, f6)
         th_t = th_t + mass_h * sixth_order_diffusion_tendency(s.theta, nl.dt_s, f6)
+    if nl.const_nu_m2_s > 0.0:  # operational_mode.py:2878-2929 (scalar flux-divergence form)
+        nu, dz = float(nl.const_nu_m2_s), const_k_dz(s.ph_total)
+        th_t = th_t + const_k_diffusion(s.theta, mass_h, nu, nl.dx, nl.dy, dz)
+        u_t = u_t + const_k_diffusion(s.u, mass_u, nu, nl.dx, nl.dy, dz)
+        v_t = v_t + const_k_diffusion(s.v, mass_v, nu, nl.dx, nl.dy, dz)
+        w_t = w_t + const_k_diffusion(s.w, mass_f, nu, nl.dx, nl.dy, dz)
+    if nl.diff_opt == 1 and nl.km_opt == 4:  # operational_mode.py:2946-2960
+        du, dv, dw, dth = smagorinsky_2d_tendencies(s, mass_u, mass_v, mass_h, mass_f, nl.dx, nl.dy, nl.c_s)
+        th_t = th_t + dth
+        u_t = u_t + du
+        v_t = v_t + dv
+        w_t = w_t + dw
     ru_pgf, rv_pgf = large_step_horizontal_pgf(s, m, rdx, rdy, nl.top_lid, nl.hypsometric_opt)
     u_t = u_t + ru_pgf
     v_t = v_t + rv_pgf

@@ -177,8 +177,9 @@ def test_host_shim_rejects_unsupported_namelist():
                              p_top=case.metrics.p_top)
     st = dycore.State.from_host(case.state, device="cpu")
     carry = dycore.initial_operational_carry(st)
-    for kw in (dict(use_flux_advection=False), dict(diff_opt=2),
-               dict(const_nu_m2_s=75.0), dict(acoustic_precision_mode="mixed_perturb_fp32")):
+    for kw in (dict(use_flux_advection=False), dict(diff_opt=2, km_opt=2), dict(diff_opt=2, km_opt=5),
+               dict(const_nu_m2_s=75.0, use_deformation_momentum_diffusion=True),
+               dict(acoustic_precision_mode="mixed_perturb_fp32")):
         nl = dycore.OperationalNamelist.from_case(case, metrics=m, **kw)
         with pytest.raises(NotImplementedError):
             dycore.rk_scan_step(carry, nl)
@@ -252,3 +253,34 @@ def test_torch_op_is_registered_with_a_fake_implementation():
     carry = dict(zip(torch_ops.CARRY_OUT, res[len(fields):]))
     assert carry["ww"].shape == (nz + 1, ny, nx) and carry["mudf"].shape == (ny, nx)
     assert carry["u_save"].shape == (nz, ny, nx + 1)
+
+
+def test_diffusion_closure_params(lib):
+    """diff_opt / km_opt / c_s / const_nu_m2_s: defaults are the reference's,
+    the built closures validate and add their launches, the TKE / 3-D
+    Smagorinsky pairs are rejected before any launch."""
+    p = _capi.StepParams()
+    lib.wrfgpu_step_params_init(ctypes.byref(p))
+    assert (p.diff_opt, p.km_opt, p.c_s, p.const_nu_m2_s) == (0, 0, 0.25, 0.0)
+    p.nx, p.ny, p.nz, p.dx, p.dy, p.dt = 16, 12, 8, 1000.0, 1000.0, 6.0
+    base = ctypes.c_int(0)
+    assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(base)) == 0
+    ws0 = ctypes.c_size_t(0)
+    assert lib.wrfgpu_step_workspace_size(ctypes.byref(p), ctypes.byref(ws0)) == 0
+    for kw, extra in ((dict(diff_opt=1, km_opt=4), 2 * 3), (dict(const_nu_m2_s=75.0), 3 * 3),
+                      (dict(diff_opt=1, km_opt=4, const_nu_m2_s=75.0), 5 * 3), (dict(diff_opt=1, km_opt=1), 0),
+                      (dict(diff_opt=2, km_opt=1), 0)):
+        q = _capi.StepParams.from_buffer_copy(p)
+        for k, v in kw.items():
+            setattr(q, k, v)
+        assert lib.wrfgpu_step_params_validate(ctypes.byref(q)) == 0, kw
+        n = ctypes.c_int(0)
+        assert lib.wrfgpu_step_launch_count(ctypes.byref(q), ctypes.byref(n)) == 0
+        assert n.value == base.value + extra, kw
+        ws = ctypes.c_size_t(0)
+        assert lib.wrfgpu_step_workspace_size(ctypes.byref(q), ctypes.byref(ws)) == 0
+        assert (ws.value > ws0.value) == (extra > 0), kw
+    for km in (2, 3, 5):
+        q = _capi.StepParams.from_buffer_copy(p)
+        q.diff_opt, q.km_opt = 2, km
+        assert lib.wrfgpu_step_params_validate(ctypes.byref(q)) == _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG

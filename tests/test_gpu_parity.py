@@ -318,3 +318,22 @@ def test_per_step_parity_sixth_order_diffusion(cuda_ready, specified, factor, sh
     for n, errs in enumerate(_per_step(case, 2 if specified else 3)):
         bad = {k: v for k, v in errs.items() if not v <= _tol(k)}
         assert not bad, f"step {n}: {bad}"
+
+
+@pytest.mark.parametrize("specified,kw,shape", [
+    (False, dict(diff_opt=1, km_opt=4), (24, 20, 14)),
+    (True, dict(diff_opt=1, km_opt=4), (24, 20, 14)),
+    (False, dict(const_nu_m2_s=75.0), (24, 20, 14)),
+    (True, dict(const_nu_m2_s=75.0, diff_opt=1, km_opt=4, diff_6th_opt=2), (33, 9, 7)),
+    (False, dict(diff_opt=1, km_opt=4, c_s=0.5), (5, 1, 6)),
+])
+def test_per_step_parity_explicit_diffusion(cuda_ready, specified, kw, shape):
+    """The stage's second-order closures (operational_mode.py:2878-2960): the
+    2-D Smagorinsky horizontal diffusion (diff_opt=1, km_opt=4) and the
+    constant-K flux form (const_nu_m2_s), alone and together with the
+    6th-order filter, on a one-row slab too."""
+    case = cases.real_like_moist(*shape, hmax=800.0, specified=specified)
+    case.controls.update(kw)
+    for n, errs in enumerate(_per_step(case, 2)):
+        bad = {k: v for k, v in errs.items() if not v <= _tol(k)}
+        assert not bad, f"{kw} step {n}: {bad}"

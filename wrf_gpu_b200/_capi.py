@@ -45,6 +45,7 @@ class StepParams(ctypes.Structure):
         ("specified_bdy_cadence", _I), ("force_geopotential", _I), ("nested_ph_relax", _I),
         ("nested_w_relax", _I), ("nested_ph_spec", _I), ("physics", _I),
         ("diff_6th_opt", _I), ("diff_6th_factor", _D),
+        ("diff_opt", _I), ("km_opt", _I), ("c_s", _D), ("const_nu_m2_s", _D),
     ]
 
 

@@ -28,6 +28,7 @@
 #include "physics_merge.cuh"
 #include "lbc.cuh"
 #include "diffusion.cuh"
+#include "explicit_diffusion.cuh"
 
 using namespace wg;
 
@@ -86,11 +87,16 @@ struct Work {
   // intermediate states after stages 1 and 2
   StateW st[2];
   double *mu_tend_phys;  // physics: the stages' mu tendency (base + mu_tendf)
+  double *xkmh;          // Smagorinsky eddy viscosity (mass cells)
+  double *dz_part, *dz;  // constant K: per-row layer-depth sums and the mean
   // specified boundary cadence: the first stage's mu tendency (base + relax)
   double *mu_tend_s1;
 };
 
 bool is_moist(const wrfgpu_step_params &p) { return p.moist_adv_opt != 0; }
+// the stage's second-order diffusion closures (operational_mode.py:2878-2960)
+bool smag_on(const wrfgpu_step_params &p) { return p.diff_opt == 1 && p.km_opt == 4; }
+bool constk_on(const wrfgpu_step_params &p) { return p.const_nu_m2_s > 0.0; }
 
 void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   const Dims d = dims_of(p);
@@ -125,6 +131,9 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   w.a = c.take(d.w); w.alpha = c.take(d.w); w.gamma = c.take(d.w);
   w.mu_tend_s1 = (spec && p.specified_bdy_cadence && p.force_geopotential) ? c.take(d.s2) : nullptr;
   w.mu_tend_phys = p.physics ? c.take(d.s2) : nullptr;
+  w.xkmh = smag_on(p) ? c.take(d.m) : nullptr;
+  w.dz_part = constk_on(p) ? c.take((size_t)p.ny) : nullptr;
+  w.dz = constk_on(p) ? c.take(1) : nullptr;
   for (int s = 0; s < 2; ++s) {
     StateW &S = w.st[s];
     S.u = c.take(d.u); S.v = c.take(d.v); S.w = c.take(d.w); S.theta = c.take(d.m);
@@ -261,7 +270,7 @@ ProfState g_prof;
 const char *kClassNames[] = {"k_recip_msf", "k_mass2d", "k_transport", "k_diag", "k_uface", "k_vface", "k_mass", "k_lim_scale",
                              "k_lim_tend", "k_wface", "k_coef", "k_bdy_target_u", "k_bdy_target_v", "k_advance_uv",
                              "k_div_h", "k_column", "k_finish_u", "k_finish_v", "k_finish_col", "k_spec_relax",
-                             "k_spec_w", "k_phys", "k_diff6"};
+                             "k_spec_w", "k_phys", "k_diff6", "k_constk", "k_smag"};
 constexpr int kNumClasses = sizeof(kClassNames) / sizeof(kClassNames[0]);
 
 int class_of(const char *name) {
@@ -378,6 +387,7 @@ int wrfgpu_step_params_init(wrfgpu_step_params *p) {
   p->normal_bdy_relax_strength = -1.0;
   p->force_geopotential = 1;
   p->diff_6th_factor = 0.12;  // operational_mode.py:492
+  p->c_s = 0.25;              // operational_mode.py:482
   p->moist_cqw = 1;
   p->w_coriolis = 1;
   p->precision = WRFGPU_PRECISION_FP64;
@@ -415,6 +425,13 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "diff_6th_opt must be 0, 1 or 2");
   if (p->diff_6th_opt && !(std::isfinite(p->diff_6th_factor) && p->diff_6th_factor >= 0.0))
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "diff_6th_factor must be finite and non-negative");
+  if (p->diff_opt == 2 && (p->km_opt == 2 || p->km_opt == 3 || p->km_opt == 5))
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG,
+                "diff_opt=2 with km_opt 2/3/5 (TKE / 3-D Smagorinsky closures) is not built");
+  if (p->diff_opt == 1 && p->km_opt == 4 && !(std::isfinite(p->c_s) && p->c_s >= 0.0))
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "c_s must be finite and non-negative");
+  if (!std::isfinite(p->const_nu_m2_s))
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "const_nu_m2_s must be finite");
   if (p->specified_adv_degrade != 0 && p->specified_adv_degrade != 1)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "specified_adv_degrade must be 0 or 1");
   if (spec && p->specified_adv_degrade && p->force_geopotential && (p->nx < 7 || p->ny < 7))
@@ -450,6 +467,8 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
     n += 3;  // finish u, v, col
     if (p->physics) n += 1;  // the physics merge of u, v, theta
     if (p->diff_6th_opt) n += 1;  // the 6th-order filter of u, v, w, theta
+    if (constk_on(*p)) n += 3;    // constant K: layer-depth partials, mean, tendencies
+    if (smag_on(*p)) n += 2;      // Smagorinsky: eddy viscosity, tendencies
     if (p->run_boundary && !p->bc_ideal && p->force_geopotential && p->specified_bdy_cadence) {
       n += (s == 0) ? 2 : 1;  // [first-stage mu tendency], relax tendencies
       n += nsub[s];           // zero-gradient w after every column launch
@@ -761,6 +780,32 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
       k_diff6<<<dim3((nx + 1 + D6_TX - 1) / D6_TX, (ny + 1 + D6_TY - 1) / D6_TY, nz + 1), dim3(D6_TX, D6_TY, 1), 0,
                 stream>>>(g, da);
       LAUNCH_CHECK("k_diff6");
+    }
+    if (constk_on(p) || smag_on(p)) {
+      DiffArgs xa{s.u, s.v, s.w, s.theta, s.mu_total, w.u_tend, w.v_tend, w.rw_tend, w.t_tend,
+                  w.xkmh, p.c_s, p.const_nu_m2_s, w.dz};
+      const dim3 agrid = grd(nx + 1, ny + 1, nz + 1);
+      if (constk_on(p)) {
+        // constant K (operational_mode.py:2878-2929), the stage's mean layer depth first
+        PROF("k_constk");
+        k_dz_partial<<<ny, DZ_THREADS, 0, stream>>>(g, s.ph_total, w.dz_part);
+        LAUNCH_CHECK("k_dz_partial");
+        PROF("k_constk");
+        k_dz_final<<<1, 32, 0, stream>>>(g, w.dz_part, w.dz);
+        LAUNCH_CHECK("k_dz_final");
+        PROF("k_constk");
+        k_constk_apply<<<agrid, blk2(), 0, stream>>>(g, xa);
+        LAUNCH_CHECK("k_constk_apply");
+      }
+      if (smag_on(p)) {
+        // 2-D Smagorinsky (operational_mode.py:2946-2960)
+        PROF("k_smag");
+        k_smag_km<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, xa, w.xkmh);
+        LAUNCH_CHECK("k_smag_km");
+        PROF("k_smag");
+        k_smag_apply<<<agrid, blk2(), 0, stream>>>(g, xa);
+        LAUNCH_CHECK("k_smag_apply");
+      }
     }
     if (p.physics) {
       // rk_addtend_dry: the physics tendencies into this stage's u, v, theta (w: in k_wface)

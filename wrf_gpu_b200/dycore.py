@@ -258,7 +258,9 @@ class OperationalNamelist:
     km_opt: int = 0
     diff_6th_opt: int = 0
     diff_6th_factor: float = 0.12
+    c_s: float = 0.25
     const_nu_m2_s: float = 0.0
+    use_deformation_momentum_diffusion: bool = False
     use_flux_advection: bool = False
     scalar_adv_opt: int = 0
     moist_adv_opt: int = 0
@@ -288,7 +290,9 @@ class OperationalNamelist:
                   moist_adv_opt=c["moist_adv_opt"], moist_cqw=c["moist_cqw"], w_coriolis=c["w_coriolis"],
                   specified_adv_degrade=bool(c.get("specified_adv_degrade", False)),
                   specified_bdy_cadence=bool(c.get("specified_bdy_cadence", False)),
-                  diff_6th_opt=int(c.get("diff_6th_opt", 0)), diff_6th_factor=float(c.get("diff_6th_factor", 0.12)))
+                  diff_6th_opt=int(c.get("diff_6th_opt", 0)), diff_6th_factor=float(c.get("diff_6th_factor", 0.12)),
+                  diff_opt=int(c.get("diff_opt", 0)), km_opt=int(c.get("km_opt", 0)), c_s=float(c.get("c_s", 0.25)),
+                  const_nu_m2_s=float(c.get("const_nu_m2_s", 0.0)))
         kw.update(overrides)
         return cls(**kw)
 
@@ -300,8 +304,10 @@ def _unsupported(nl: OperationalNamelist, physics_tendencies) -> str | None:
         return "use_vertical_solver=False is not built"
     if nl.rk_order != 3:
         return "rk_order must be 3"
-    if nl.diff_opt or nl.km_opt or nl.const_nu_m2_s > 0.0:
-        return "explicit diffusion options are not built"
+    if int(nl.diff_opt) == 2 and int(nl.km_opt) in (2, 3, 5):
+        return "diff_opt=2 with km_opt 2/3/5 (TKE / 3-D Smagorinsky closures) is not built"
+    if nl.const_nu_m2_s > 0.0 and nl.use_deformation_momentum_diffusion:
+        return "the deformation-tensor momentum form of the constant-K diffusion is not built"
     if nl.moist_adv_opt and nl.mp_physics in (7, 17, 18, 19, 21, 22, 24, 26, 27, 28, 38):
         return "extra advected species of this mp_physics family are not built"
     if nl.acoustic_precision_mode != "fp64_default":
@@ -337,6 +343,8 @@ def step_params(nl: OperationalNamelist) -> _capi.StepParams:
     p.nested_ph_relax, p.nested_w_relax = int(bool(bc.nested_ph_relax)), int(bool(bc.nested_w_relax))
     p.nested_ph_spec = int(bool(bc.nested_ph_spec))
     p.diff_6th_opt, p.diff_6th_factor = int(nl.diff_6th_opt), float(nl.diff_6th_factor)
+    p.diff_opt, p.km_opt, p.c_s = int(nl.diff_opt), int(nl.km_opt), float(nl.c_s)
+    p.const_nu_m2_s = float(nl.const_nu_m2_s)
     m = nl.metrics
     p.cf1, p.cf2, p.cf3, p.p_top = m.cf1, m.cf2, m.cf3, m.p_top
     p.cfn, p.cfn1 = m.cfn()
