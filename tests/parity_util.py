@@ -67,3 +67,17 @@ def attach_lbc_leaves(s, rng, moist=("qv", "qc", "qr")):
     for q in moist:
         setattr(s, q + "_bdy", np.abs(leaf(nz, 1.0e-3, 1.0e-3)) - 2.0e-4)
     return s
+
+
+def compare_oracles(a, b, keys_state=STATE_KEYS, keys_carry=CARRY_KEYS):
+    """``compare`` for two oracle carries (host arrays on both sides)."""
+    out = {}
+    for k in keys_state:
+        x, y = getattr(a.state, k, None), getattr(b.state, k, None)
+        if x is not None and y is not None:
+            out[k] = rel_err(x, y)
+    for k in keys_carry:
+        x, y = getattr(a, k, None), getattr(b, k, None)
+        if x is not None and y is not None:
+            out[k] = rel_err(x, y)
+    return out

@@ -75,13 +75,28 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
     const double muts_in = ldw(A.muts, c2d);
     const double mu_in = ldw(A.mu, c2d);
     mu_tend = (A.mu_tend != nullptr) ? ld(A.mu_tend, c2d) : 0.0;
-    double d0 = ld(dvdxi, M(0)), d1 = (nz > 1) ? ld(dvdxi, M(1)) : 0.0;
-    for (int k = 0; k < nz; ++k) {
-      const double d2 = (k + 2 < nz) ? ld(dvdxi, M(k + 2)) : 0.0;
-      const double t = ld(g.dnw, k) * d0;
-      dmdt = (k == 0) ? t : dmdt + t;
-      d0 = d1;
-      d1 = d2;
+    // the column sum in level order, its loads batched SB levels ahead
+    constexpr int SB = 8;
+    double ba[SB], bb[SB];
+    auto ldb = [&](int k0, double *b) {
+#pragma unroll
+      for (int u = 0; u < SB; ++u) b[u] = (k0 + u < nz) ? ld(dvdxi, M(k0 + u)) : 0.0;
+    };
+    auto acc = [&](int k0, const double *b) {
+#pragma unroll
+      for (int u = 0; u < SB; ++u) {
+        if (k0 + u < nz) {
+          const double t = ld(g.dnw, k0 + u) * b[u];
+          dmdt = (k0 + u == 0) ? t : dmdt + t;
+        }
+      }
+    };
+    ldb(0, ba);
+    for (int k0 = 0; k0 < nz; k0 += 2 * SB) {
+      ldb(k0 + SB, bb);
+      acc(k0, ba);
+      ldb(k0 + 2 * SB, ba);
+      acc(k0 + SB, bb);
     }
     const double mu_work_old = muts_in - mut;
     const double mu_save = mu_in - mu_work_old;
@@ -178,7 +193,7 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
       v.alt = ld(A.alt, o);
     }
   };
-  In cur, nx1, nx2;
+  In cur, nx1;
   load(0, cur);
   load(1, nx1);
 
@@ -200,7 +215,9 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
   double t2a_m1 = 0.0, c2a_m1 = 0.0, alt_m1 = 0.0;                            // level k-1 (top face)
   double wf_prev = 0.0;                 // forward-eliminated w at face k-2
 
-  for (int k = 0; k <= nz; ++k) {
+  // one iteration; the three input buffers rotate by unrolling the loop
+  // three ways (a register copy of a buffer would wait for its loads)
+  auto step2 = [&](int k, In &cur, const In &nx1, In &nx2) {
     if (k + 2 <= nz) load(k + 2, nx2);
     // --- ww at face k+1 (advance_mu_t's ww prefix, mu_t_advance.py:229-237) ---
     double ww_k1 = 0.0;
@@ -307,8 +324,12 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
       t2a_m1 = t2a_k; c2a_m1 = cur.c2a; alt_m1 = cur.alt;
     }
     ww_k = ww_k1;
-    cur = nx1;
-    nx1 = nx2;
+  };
+  In b2;
+  for (int k = 0; k <= nz; k += 3) {
+    step2(k, cur, nx1, b2);
+    if (k + 1 <= nz) step2(k + 1, nx1, b2, cur);
+    if (k + 2 <= nz) step2(k + 2, b2, cur, nx1);
   }
   // --- face nz: the top explicit w and its forward elimination ---
   {
@@ -339,54 +360,44 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
   const double mu_work = muts - mut;
   double ws_next = 0.0;    // undamped back-substituted w at face f+1
   double phn_up = 0.0;     // final phi at face f+1
-  // face-f inputs one face ahead (downward): gamma, pt1, w_save
-  auto ldg3 = [&](int f, double &gm, double &pt, double &wsv) {
-    gm = (f >= 1 && f <= nz - 1) ? ld(A.gamma, M(f)) : 0.0;
-    pt = (do_damp && f >= 1) ? ld(A.pt1, M(f)) : 0.0;
-    wsv = (do_damp && f >= 1) ? ld(A.w_save, M(f)) : 0.0;
+  // face-f inputs of the back substitution and damping, and level-f inputs
+  // of calc_p_rho, loaded two faces ahead (downward)
+  struct In3 {
+    double gm, pt, wsv, thw, alt, c2a, th, pm1;
   };
-  // level-f inputs of calc_p_rho, one level ahead
-  auto ldp = [&](int k, double &thw, double &alt, double &c2a, double &th, double &pm1) {
-    if (k >= 0 && k < nz) {
-      const size_t o = M(k);
-      thw = ldw(A.theta_w, o);
-      alt = ld(A.alt, o);
-      c2a = ld(A.c2a, o);
-      th = ld(A.theta_s, o) - T0;
-      pm1 = ldw(A.pm1, o);
+  auto load3 = [&](int f, In3 &v) {
+    const size_t o = M(f);
+    v.gm = (f >= 1 && f <= nz - 1) ? ld(A.gamma, o) : 0.0;
+    v.pt = (do_damp && f >= 1) ? ld(A.pt1, o) : 0.0;
+    v.wsv = (do_damp && f >= 1) ? ld(A.w_save, o) : 0.0;
+    if (f < nz) {
+      v.thw = ldw(A.theta_w, o);
+      v.alt = ld(A.alt, o);
+      v.c2a = ld(A.c2a, o);
+      v.th = ld(A.theta_s, o) - T0;
+      v.pm1 = ldw(A.pm1, o);
     }
   };
-  double gm0, pt0, wsv0, gm1, pt1v, wsv1;
-  ldg3(nz, gm0, pt0, wsv0);
-  ldg3(nz - 1, gm1, pt1v, wsv1);
-  double p_thw = 0.0, p_alt = 0.0, p_c2a = 0.0, p_th = 0.0, p_pm1 = 0.0;
-  double q_thw = 0.0, q_alt = 0.0, q_c2a = 0.0, q_th = 0.0, q_pm1 = 0.0;
-  ldp(nz - 1, p_thw, p_alt, p_c2a, p_th, p_pm1);
-  ldp(nz - 2, q_thw, q_alt, q_c2a, q_th, q_pm1);
-  for (int f = nz; f >= 0; --f) {
-    double gm2 = 0.0, pt2 = 0.0, wsv2 = 0.0;
-    if (f - 2 >= 0) ldg3(f - 2, gm2, pt2, wsv2);
-    // calc_p_rho consumes level f this iteration and level f-2 two later
-    double r_thw = 0.0, r_alt = 0.0, r_c2a = 0.0, r_th = 0.0, r_pm1 = 0.0;
-    if (f <= nz - 1 && f - 2 >= 0) ldp(f - 2, r_thw, r_alt, r_c2a, r_th, r_pm1);
+  auto step3 = [&](int f, const In3 &cur, In3 &nx2) {
+    if (f - 2 >= 0) load3(f - 2, nx2);
     // back substitution (undamped), core/advance_w.py:583-592
     double ws;
     if (f == nz || f == 0) {
       ws = WF(f);
     } else {
-      ws = WF(f) - gm0 * ws_next;
+      ws = WF(f) - cur.gm * ws_next;
     }
     ws_next = ws;
     // P9: damping, w and phi out
     double phn;
     if (f >= 1) {
       if (do_damp) {
-        const double hk = div_rcp(pt0, G, RG);
+        const double hk = div_rcp(cur.pt, G, RG);
         const double sv = sin(over_zdamp(0.5 * 3.141592653589793 * (hk - hbot), c));
         const double ramp = sv * sv;
         const double dampwt = (hk >= hbot) ? dampmag * ramp : 0.0;
         const double mf = ld(g.c1f, f) * mut + ld(g.c2f, f);
-        ws = (ws - dampwt * mf * wsv0) / (1.0 + dampwt);
+        ws = (ws - dampwt * mf * cur.wsv) / (1.0 + dampwt);
       }
       const double mfs = ld(g.c1f, f) * muts + ld(g.c2f, f);
       phn = RHS(f) + msfty * 0.5 * dts * G * eps_p * ws / mfs;
@@ -405,22 +416,25 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
       const double mass = ld(g.c1h, k) * muts + ld(g.c2h, k);
       const double safe = safe12(mass);
       const double mu_term = ld(g.c1h, k) * mu_work;
-      const double altc = p_alt;
+      const double altc = cur.alt;
       const double al = -(altc * mu_term + ld(g.rdnw, k) * (phn_up - phn)) / safe;
-      const double t1 = p_th;
+      const double t1 = cur.th;
       const double ttr = T0 + t1;
       const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
-      const double pp = p_c2a * (altc * (p_thw - mu_term * t1) / (safe * sttr) - al);
-      const double pm1 = p_pm1;
-      A.p[M(k)] = pp + SMDIV * (pp - pm1);
+      const double pp = cur.c2a * (altc * (cur.thw - mu_term * t1) / (safe * sttr) - al);
+      A.p[M(k)] = pp + SMDIV * (pp - cur.pm1);
       A.pm1[M(k)] = pp;
       A.al[M(k)] = al;
-      p_thw = q_thw; p_alt = q_alt; p_c2a = q_c2a; p_th = q_th; p_pm1 = q_pm1;
-      q_thw = r_thw; q_alt = r_alt; q_c2a = r_c2a; q_th = r_th; q_pm1 = r_pm1;
     }
     phn_up = phn;
-    gm0 = gm1; pt0 = pt1v; wsv0 = wsv1;
-    gm1 = gm2; pt1v = pt2; wsv1 = wsv2;
+  };
+  In3 x0, x1, x2;
+  load3(nz, x0);
+  load3(nz - 1, x1);
+  for (int f = nz; f >= 0; f -= 3) {
+    step3(f, x0, x2);
+    if (f - 1 >= 0) step3(f - 1, x1, x0);
+    if (f - 2 >= 0) step3(f - 2, x2, x1);
   }
 }
 
