@@ -445,6 +445,64 @@ int wrfgpu_step_epilogue_device_lead(const wrfgpu_step_params *params, const wrf
                                      int disable_guards, wrfgpu_theta_limiter_diag *diag, void *workspace,
                                      size_t workspace_bytes, cudaStream_t stream);
 
+/* ------------------------------------------------------------------------
+ * Nest coupling around the step (a nested child's boundary leaves from its
+ * parent, and the child's feedback onto the parent).
+ * ------------------------------------------------------------------------ */
+
+/* Static parent -> child bilinear gather of one staggering (device arrays):
+ * per child row the floor / ceil parent rows y0, y1 and the weight wy toward
+ * y1, per child column x0, x1, wx (nesting/interp.py:68-190, built on the host
+ * with the WRF sint cell-centered or the node-aligned registration). */
+typedef struct wrfgpu_nest_interp {
+  const int *y0, *y1, *x0, *x1;   /* (child_ny), (child_nx) */
+  const double *wy, *wx;
+  int child_ny, child_nx;         /* child extent of this staggering */
+  int parent_ny, parent_nx;       /* parent extent of this staggering */
+} wrfgpu_nest_interp;
+
+/* A parent field (nz, parent_ny, parent_nx) interpolated onto the whole child
+ * grid (nz, child_ny, child_nx): rows first, then columns.  Replaces
+ * interp_sint_linear / interp_bilinear (nesting/interp.py:248-314) and
+ * interp_parent_field_to_child (nesting/boundary_construction.py:454-468). */
+int wrfgpu_nest_interp_field(const wrfgpu_nest_interp *w, const double *parent, int nz, double *child_out,
+                             cudaStream_t stream);
+
+/* One two-time child boundary leaf (2, 4, width, leaf_z, leaf_side): time 0
+ * the child field's own ring, time 1 the parent interpolated to the same ring
+ * cells (w = NULL: the child's own ring again, as for the base leaves); W / E
+ * columns and S / N rows from the domain edge inward, zero beyond the field's
+ * extent (side_len = the strips' tangential length) or the leaf's.  One call
+ * per leaf replaces build_child_boundary_package
+ * (nesting/boundary_construction.py:360-451: field_sides_3d/_2d, _fit and the
+ * two-time stack). */
+int wrfgpu_nest_ring_leaf(const wrfgpu_nest_interp *w, const double *parent, const double *child, int nz,
+                          int child_ny, int child_nx, int width, int side_len, int leaf_z, int leaf_side,
+                          double *leaf, cudaStream_t stream);
+
+/* WRF copy_fcn feedback plan of one staggering (device index arrays) and its
+ * sm121 smoother interior (coupling/boundary_feedback.py:170-319). */
+typedef struct wrfgpu_nest_feedback_plan {
+  const int *parent_lin;          /* (npts) parent linear index in a (psn, pwe) plane */
+  const int *child_lin;           /* (npts, stencil) child donors in a (csn, cwe) plane */
+  int npts, stencil, pwe, psn, cwe, csn;
+  int i_lo, i_hi, j_lo, j_hi;     /* sm121 interior, 0-based half-open */
+  int smooth;                     /* smooth_option != 0 */
+} wrfgpu_nest_feedback_plan;
+
+/* out = parent with the overlap points set to the mean of their child donors,
+ * then (plan->smooth) the sm121 1-2-1 smoother over the interior; nz levels
+ * of (psn, pwe); scratch is one field of the same size (used by the
+ * smoother); out may alias parent.  Replaces apply_feedback + sm121_smooth
+ * (coupling/boundary_feedback.py:400-494). */
+int wrfgpu_nest_feedback(const wrfgpu_nest_feedback_plan *plan, const double *parent, const double *child, int nz,
+                         double *out, double *scratch, cudaStream_t stream);
+
+/* out_total = (parent_total - parent_pert) + new_pert over n elements: the
+ * totals rebuilt after feedback (coupling/boundary_feedback.py:557-568). */
+int wrfgpu_nest_rebuild_total(const double *parent_total, const double *parent_pert, const double *new_pert,
+                              size_t n, double *out_total, cudaStream_t stream);
+
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 

@@ -112,6 +112,16 @@ class LbcLeaves(ctypes.Structure):
                 ("mub", _P), ("ph", _P), ("phb", _P), ("ntime", _I), ("width", _I), ("side_len", _I)]
 
 
+class NestInterp(ctypes.Structure):
+    _fields_ = [("y0", _P), ("y1", _P), ("x0", _P), ("x1", _P), ("wy", _P), ("wx", _P), ("child_ny", _I),
+                ("child_nx", _I), ("parent_ny", _I), ("parent_nx", _I)]
+
+
+class NestFeedbackPlan(ctypes.Structure):
+    _fields_ = [("parent_lin", _P), ("child_lin", _P), ("npts", _I), ("stencil", _I), ("pwe", _I), ("psn", _I),
+                ("cwe", _I), ("csn", _I), ("i_lo", _I), ("i_hi", _I), ("j_lo", _I), ("j_hi", _I), ("smooth", _I)]
+
+
 # wrfgpu_theta_limiter_diag: 4 int32 (count, x, y, z) then 3 float64 (mass before, after, residual)
 THETA_DIAG_BYTES = 40
 
@@ -123,7 +133,8 @@ EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_st
             "wrfgpu_acoustic_substep_vjp", "wrfgpu_apply_lateral_boundaries",
             "wrfgpu_step_epilogue_workspace_size", "wrfgpu_step_epilogue", "wrfgpu_step_epilogue_device_lead", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
-            "wrfgpu_version")
+            "wrfgpu_version", "wrfgpu_nest_interp_field", "wrfgpu_nest_ring_leaf", "wrfgpu_nest_feedback",
+            "wrfgpu_nest_rebuild_total")
 
 _lib = None
 
@@ -195,6 +206,14 @@ def load(path: str | os.PathLike | None = None):
                                                      ctypes.POINTER(StepOutputs), _P, _I, _P, _P, ctypes.c_size_t,
                                                      _P]
     lib.wrfgpu_step_epilogue_device_lead.restype = _I
+    lib.wrfgpu_nest_interp_field.argtypes = [ctypes.POINTER(NestInterp), _P, _I, _P, _P]
+    lib.wrfgpu_nest_interp_field.restype = _I
+    lib.wrfgpu_nest_ring_leaf.argtypes = [ctypes.POINTER(NestInterp), _P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P]
+    lib.wrfgpu_nest_ring_leaf.restype = _I
+    lib.wrfgpu_nest_feedback.argtypes = [ctypes.POINTER(NestFeedbackPlan), _P, _P, _I, _P, _P, _P]
+    lib.wrfgpu_nest_feedback.restype = _I
+    lib.wrfgpu_nest_rebuild_total.argtypes = [_P, _P, _P, ctypes.c_size_t, _P, _P]
+    lib.wrfgpu_nest_rebuild_total.restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

@@ -29,6 +29,7 @@
 #include "lbc.cuh"
 #include "diffusion.cuh"
 #include "explicit_diffusion.cuh"
+#include "nesting.cuh"
 
 using namespace wg;
 
@@ -1771,6 +1772,124 @@ extern "C" int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *p, cons
   AdvOpArgs a{ru, rv, rom};
   k_scalar_adv_adj<<<grd(p->nx, p->ny, p->nz), blk2(), 0, stream>>>(g, a, tend_bar, q_bar);
   if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_adj launch failed");
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Nest coupling: parent -> child interpolation and boundary leaves, child ->
+// parent feedback (nesting.cuh).
+// ---------------------------------------------------------------------------
+namespace {
+
+int nest_interp_check(const wrfgpu_nest_interp *w) {
+  if (w == nullptr || w->y0 == nullptr || w->y1 == nullptr || w->x0 == nullptr || w->x1 == nullptr ||
+      w->wy == nullptr || w->wx == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "interpolation weights are NULL");
+  if (w->child_ny < 1 || w->child_nx < 1 || w->parent_ny < 1 || w->parent_nx < 1)
+    return fail(WRFGPU_ERR_BAD_SHAPE, "interpolation extents must be >= 1");
+  return WRFGPU_OK;
+}
+
+NestInterp nest_interp_of(const wrfgpu_nest_interp *w) {
+  return NestInterp{w->y0, w->y1, w->x0, w->x1, w->wy, w->wx, w->child_ny, w->child_nx, w->parent_ny, w->parent_nx};
+}
+
+}  // namespace
+
+extern "C" int wrfgpu_nest_interp_field(const wrfgpu_nest_interp *w, const double *parent, int nz, double *child_out,
+                                        cudaStream_t stream) {
+  int rc = nest_interp_check(w);
+  if (rc) return rc;
+  if (parent == nullptr || child_out == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "parent/child_out is NULL");
+  if (nz < 1 || nz > 65535) return fail(WRFGPU_ERR_BAD_SHAPE, "nz must be in 1..65535");
+  const NestInterp ni = nest_interp_of(w);
+  k_nest_interp<<<dim3((ni.cnx + 31) / 32, (ni.cny + 3) / 4, nz), dim3(32, 4, 1), 0, stream>>>(ni, parent, child_out);
+  if ((rc = check_launch("k_nest_interp"))) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_nest_ring_leaf(const wrfgpu_nest_interp *w, const double *parent, const double *child,
+                                     int nz, int child_ny, int child_nx, int width, int side_len, int leaf_z,
+                                     int leaf_side, double *leaf, cudaStream_t stream) {
+  if (child == nullptr || leaf == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "child/leaf is NULL");
+  if (w != nullptr) {
+    int rc = nest_interp_check(w);
+    if (rc) return rc;
+    if (parent == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "parent is NULL");
+    if (w->child_ny != child_ny || w->child_nx != child_nx)
+      return fail(WRFGPU_ERR_BAD_SHAPE, "the weights' child extent differs from the child field's");
+  }
+  if (nz < 1 || child_ny < 1 || child_nx < 1 || width < 1 || side_len < 1 || leaf_z < 1 || leaf_side < 1 ||
+      4 * width > 65535 || 2 * leaf_z > 65535)
+    return fail(WRFGPU_ERR_BAD_SHAPE, "bad ring-leaf extents");
+  NestRingJob a{};
+  if (w != nullptr) a.w = nest_interp_of(w);
+  a.w.cny = child_ny;
+  a.w.cnx = child_nx;
+  a.interp = w != nullptr ? 1 : 0;
+  a.parent = parent;
+  a.child = child;
+  a.nzf = nz;
+  a.width = width;
+  a.side_len = side_len;
+  a.lz = leaf_z;
+  a.lside = leaf_side;
+  a.leaf = leaf;
+  k_nest_ring_leaf<<<dim3((leaf_side + 127) / 128, 4 * width, 2 * leaf_z), 128, 0, stream>>>(a);
+  int rc = check_launch("k_nest_ring_leaf");
+  if (rc) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_nest_feedback(const wrfgpu_nest_feedback_plan *plan, const double *parent, const double *child,
+                                    int nz, double *out, double *scratch, cudaStream_t stream) {
+  if (plan == nullptr || parent == nullptr || child == nullptr || out == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "plan/parent/child/out is NULL");
+  if (plan->npts > 0 && (plan->parent_lin == nullptr || plan->child_lin == nullptr))
+    return fail(WRFGPU_ERR_NULL_POINTER, "the plan's index arrays are NULL");
+  if (nz < 1 || nz > 65535 || plan->npts < 0 || plan->stencil < 1 || plan->pwe < 1 || plan->psn < 1 ||
+      plan->cwe < 1 || plan->csn < 1)
+    return fail(WRFGPU_ERR_BAD_SHAPE, "bad feedback extents");
+  const bool smooth = plan->smooth != 0 && plan->i_hi > plan->i_lo && plan->j_hi > plan->j_lo;
+  if (smooth && scratch == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "the smoother needs a scratch field");
+  if (smooth && (plan->i_lo < 1 || plan->j_lo < 1 || plan->i_hi > plan->pwe - 1 || plan->j_hi > plan->psn - 1))
+    return fail(WRFGPU_ERR_BAD_SHAPE, "the smoother interior needs a one-cell halo inside the parent field");
+  const size_t n = (size_t)nz * plan->psn * plan->pwe;
+  if (out != parent && cudaMemcpyAsync(out, parent, n * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+    return fail(WRFGPU_ERR_CUDA, "feedback copy failed");
+  int rc;
+  if (plan->npts > 0) {
+    NestFeedback f{plan->parent_lin, plan->child_lin, plan->npts, plan->stencil, plan->pwe, plan->psn, plan->cwe,
+                   plan->csn};
+    k_nest_feedback<<<dim3((plan->npts + 127) / 128, nz, 1), 128, 0, stream>>>(f, child, out);
+    if ((rc = check_launch("k_nest_feedback"))) return rc;
+  }
+  if (smooth) {
+    if (cudaMemcpyAsync(scratch, out, n * sizeof(double), cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return fail(WRFGPU_ERR_CUDA, "smoother copy failed");
+    const dim3 grid((plan->i_hi - plan->i_lo + 31) / 32, (plan->j_hi - plan->j_lo + 3) / 4, nz);
+    k_sm121_j<<<grid, dim3(32, 4, 1), 0, stream>>>(out, scratch, plan->psn, plan->pwe, plan->i_lo, plan->i_hi,
+                                                   plan->j_lo, plan->j_hi);
+    if ((rc = check_launch("k_sm121_j"))) return rc;
+    k_sm121_i<<<grid, dim3(32, 4, 1), 0, stream>>>(scratch, out, plan->psn, plan->pwe, plan->i_lo, plan->i_hi,
+                                                   plan->j_lo, plan->j_hi);
+    if ((rc = check_launch("k_sm121_i"))) return rc;
+  }
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_nest_rebuild_total(const double *parent_total, const double *parent_pert,
+                                         const double *new_pert, size_t n, double *out_total, cudaStream_t stream) {
+  if (parent_total == nullptr || parent_pert == nullptr || new_pert == nullptr || out_total == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "a total-rebuild pointer is NULL");
+  if (n == 0) return WRFGPU_OK;
+  k_nest_total<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(parent_total, parent_pert, new_pert, n, out_total);
+  int rc = check_launch("k_nest_total");
+  if (rc) return rc;
   g_last_error.clear();
   return WRFGPU_OK;
 }
