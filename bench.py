@@ -618,6 +618,25 @@ def run_batched(args):
     return 0
 
 
+def run_profile_target(args):
+    """A few plain RK3 steps of the workload (the target of ncu captures)."""
+    import torch
+    from wrf_gpu_b200 import build, cases, dycore
+    build.build()
+    case = cases.real_like_moist(args.nx, args.ny, args.nz, specified=not args.periodic)
+    case.controls["diff_6th_opt"] = args.diff_6th
+    nl = dycore.OperationalNamelist.from_case(case, precision=args.precision)
+    stp = dycore.Stepper(nl)
+    stp.params.column_width = args.column_width
+    carry = dycore.carry_from_case(case)
+    out = stp.alloc_carry(carry)
+    for _ in range(args.profile_steps):
+        stp.step_into(carry, out, lead_seconds=0.0)
+    torch.cuda.synchronize()
+    print("ok", float(out.state.w.abs().max().item()))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -635,6 +654,12 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the tile-shape tuner (built-in defaults)")
     ap.add_argument("--workload", choices=("moist433", "batched"), default="moist433",
                     help="batched: the nest + ensemble set advanced by the batched call (1 GPU)")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling target: run this many plain steps of the workload (no timing, no JSON) and exit")
+    ap.add_argument("--periodic", action="store_true", help="with --profile-steps: doubly periodic boundaries")
+    ap.add_argument("--diff-6th", type=int, default=0, help="with --profile-steps: diff_6th_opt of the step")
+    ap.add_argument("--column-width", type=int, default=0,
+                    help="with --profile-steps: column kernel (0 default, 1 one thread per column, 16 / 32 tiled)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -643,6 +668,8 @@ def main():
 
     if args.workload == "batched" and args.impl == "ours":
         return run_batched(args)
+    if args.profile_steps > 0:
+        return run_profile_target(args)
 
     if args.impl == "reference":
         if rank != 0:

@@ -11,8 +11,10 @@
 //                  whose loads are in flight;
 //   sweep 3 (down) Thomas back substitution, Rayleigh damping, w and phi
 //                  out, and calc_p_rho one level behind.
-// Inputs of level k+2 are loaded while level k is computed, so every thread
-// keeps two levels of ~20 loads in flight with no block barrier anywhere;
+// The inputs of each iteration are loaded several iterations ahead into a
+// ring of register buffers (3 levels up, 4 faces down, the column sum 8-16
+// levels), so every thread keeps dozens of loads in flight with no block
+// barrier anywhere;
 // the forward-elimination result and the phi predictor of each face are
 // parked in warp-private shared memory for sweep 3 (2 (nz+1) doubles per
 // column).  A warp owns 32 adjacent columns of one row, so every load and
@@ -166,15 +168,14 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
   // t_2ave / buoyancy / coef / wd of level k, the phi predictor of face k,
   // then the explicit w and the forward elimination of face k-1.
   // ------------------------------------------------------------------
-  // per-level inputs, loaded two levels ahead
+  // per-iteration inputs: iteration k reads face k, level k and the three
+  // values of k+1 its stencils reach (ww_1, theta, pt1), loaded LA2 = 3
+  // iterations ahead into a ring of four buffers
   struct In {
-    double ww1, dv, th, hd, thw, ttend, t2o, c2a, alt, pt1, ph, pht, w, rwt, cqw, a, alpha;
+    double dv, hd, thw, ttend, t2o, c2a, alt, ph, pht, w, rwt, cqw, a, alpha, ww1n, thn, pt1n;
   };
   auto load = [&](int k, In &v) {
-    // face quantities (k <= nz) and level quantities (k < nz)
     const size_t o = M(k);
-    v.ww1 = ld(A.ww_1, o);
-    v.pt1 = ld(A.pt1, o);
     v.ph = ldw(A.ph, o);
     v.pht = ld(A.ph_tend, o);
     v.w = ldw(A.w, o);
@@ -183,26 +184,33 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
     v.a = ld(A.a, o);
     v.alpha = ld(A.alpha, o);
     if (k < nz) {
+      const size_t o1 = M(k + 1);
       v.dv = active ? ld(dvdxi, o) : 0.0;
-      v.th = ld(A.theta_s, o) - T0;
       v.hd = active ? ld(hdiv, o) : 0.0;
       v.thw = ldw(A.theta_w, o);
       v.ttend = ld(A.t_tend, o);
       v.t2o = ldw(A.t2ave, o);
       v.c2a = ld(A.c2a, o);
       v.alt = ld(A.alt, o);
+      v.ww1n = ld(A.ww_1, o1);
+      v.pt1n = ld(A.pt1, o1);
+      v.thn = (k + 1 < nz) ? ld(A.theta_s, o1) - T0 : 0.0;
     }
   };
-  In cur, nx1;
-  load(0, cur);
-  load(1, nx1);
+  In b0, b1, b2, b3;
+  load(0, b0);
+  load(1, b1);
+  load(2, b2);
+  const double ww1_0 = ld(A.ww_1, M(0));
+  double th_k = ld(A.theta_s, M(0)) - T0;  // theta' at level k (the window)
+  double pt1_k = ld(A.pt1, M(0));          // pt1 at face k
 
   const double c05gem = 0.5 * G * eps_m;
   const double c05dg = 0.5 * dts * G;
   const double dtsg = dts * G;
   // ww prefix state: ww at faces k and k+1, the running sum `prev`
   double prev = ww_bot;
-  double ww_k = active ? (ww_bot - cur.ww1) : ww_bot;  // face 0 (inactive: old ww)
+  double ww_k = active ? (ww_bot - ww1_0) : ww_bot;  // face 0 (inactive: old ww)
   // windows of the level / face quantities the later stencils read
   double thm1 = 0.0;                    // T1 at level k-1
   double wd_m1 = 0.0;                   // wd at level k-1
@@ -215,10 +223,10 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
   double t2a_m1 = 0.0, c2a_m1 = 0.0, alt_m1 = 0.0;                            // level k-1 (top face)
   double wf_prev = 0.0;                 // forward-eliminated w at face k-2
 
-  // one iteration; the three input buffers rotate by unrolling the loop
-  // three ways (a register copy of a buffer would wait for its loads)
-  auto step2 = [&](int k, In &cur, const In &nx1, In &nx2) {
-    if (k + 2 <= nz) load(k + 2, nx2);
+  // one iteration; the four input buffers rotate by unrolling the loop four
+  // ways (a register copy of a buffer would wait for its loads)
+  auto step2 = [&](int k, const In &cur, In &nx3) {
+    if (k + 3 <= nz) load(k + 3, nx3);
     // --- ww at face k+1 (advance_mu_t's ww prefix, mu_t_advance.py:229-237) ---
     double ww_k1 = 0.0;
     if (k + 1 <= nz) {
@@ -233,7 +241,7 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
         const double inc =
             div_rcp(ld(g.dnw, kl) * (ld(g.c1h, kl) * dmdt + dv + ld(g.c1h, kl) * mu_tend), msfty, minv);
         const double cc = prev - inc;
-        ww_k1 = cc - nx1.ww1;
+        ww_k1 = cc - cur.ww1n;
         prev = cc;
       }
     }
@@ -242,8 +250,7 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
     // --- level k: theta update, t_2ave, buoyancy, coef, wd (P5) ---
     double wd_k = 0.0, coef_k = 0.0, buoy_k = 0.0, t2a_k = 0.0;
     if (k < nz) {
-      const double th_k = cur.th;
-      const double th_p1 = (k + 1 < nz) ? nx1.th : 0.0;
+      const double th_p1 = (k + 1 < nz) ? cur.thn : 0.0;
       double thw = cur.thw;
       if (active) {
         const double wdtn_hi = (k + 1 <= nz - 1) ? ww_k1 * (ld(g.fnm, k + 1) * th_p1 + ld(g.fnp, k + 1) * th_k) : 0.0;
@@ -266,7 +273,7 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
       buoy_k = cur.c2a * cur.alt * t2a_k;
       coef_k = cur.c2a * ld(g.rdnw, k) / safe12(ld(g.c1h, k) * mut + ld(g.c2h, k));
       const double wwm = 0.5 * (ww_k1 + ww_k);
-      wd_k = wwm * ld(g.rdnw, k) * (nx1.pt1 - cur.pt1);
+      wd_k = wwm * ld(g.rdnw, k) * (cur.pt1n - pt1_k);
     }
 
     // --- face k: the phi predictor (P6) ---
@@ -312,7 +319,11 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
     }
 
     // --- slide the windows ---
-    thm1 = (k < nz) ? cur.th : thm1;
+    if (k < nz) {
+      thm1 = th_k;
+      th_k = cur.thn;
+      pt1_k = cur.pt1n;
+    }
     wd_m1 = wd_k;
     coef_m2 = coef_m1; coef_m1 = coef_k;
     buoy_m2 = buoy_m1; buoy_m1 = buoy_k;
@@ -325,11 +336,11 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
     }
     ww_k = ww_k1;
   };
-  In b2;
-  for (int k = 0; k <= nz; k += 3) {
-    step2(k, cur, nx1, b2);
-    if (k + 1 <= nz) step2(k + 1, nx1, b2, cur);
-    if (k + 2 <= nz) step2(k + 2, b2, cur, nx1);
+  for (int k = 0; k <= nz; k += 4) {
+    step2(k, b0, b3);
+    if (k + 1 <= nz) step2(k + 1, b1, b0);
+    if (k + 2 <= nz) step2(k + 2, b2, b1);
+    if (k + 3 <= nz) step2(k + 3, b3, b2);
   }
   // --- face nz: the top explicit w and its forward elimination ---
   {
@@ -361,7 +372,7 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
   double ws_next = 0.0;    // undamped back-substituted w at face f+1
   double phn_up = 0.0;     // final phi at face f+1
   // face-f inputs of the back substitution and damping, and level-f inputs
-  // of calc_p_rho, loaded two faces ahead (downward)
+  // of calc_p_rho, loaded four faces ahead (downward) into a ring of five
   struct In3 {
     double gm, pt, wsv, thw, alt, c2a, th, pm1;
   };
@@ -378,8 +389,8 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
       v.pm1 = ldw(A.pm1, o);
     }
   };
-  auto step3 = [&](int f, const In3 &cur, In3 &nx2) {
-    if (f - 2 >= 0) load3(f - 2, nx2);
+  auto step3 = [&](int f, const In3 &cur, In3 &nx4) {
+    if (f - 4 >= 0) load3(f - 4, nx4);
     // back substitution (undamped), core/advance_w.py:583-592
     double ws;
     if (f == nz || f == 0) {
@@ -428,13 +439,17 @@ __global__ void __launch_bounds__(32 * CS_WARPS, 2) k_column_stream(Grid g, Acou
     }
     phn_up = phn;
   };
-  In3 x0, x1, x2;
+  In3 x0, x1, x2, x3, x4;
   load3(nz, x0);
   load3(nz - 1, x1);
-  for (int f = nz; f >= 0; f -= 3) {
-    step3(f, x0, x2);
+  load3(nz - 2, x2);
+  load3(nz - 3, x3);
+  for (int f = nz; f >= 0; f -= 5) {
+    step3(f, x0, x4);
     if (f - 1 >= 0) step3(f - 1, x1, x0);
     if (f - 2 >= 0) step3(f - 2, x2, x1);
+    if (f - 3 >= 0) step3(f - 3, x3, x2);
+    if (f - 4 >= 0) step3(f - 4, x4, x3);
   }
 }
 
