@@ -469,16 +469,18 @@ int wrfgpu_nest_interp_field(const wrfgpu_nest_interp *w, const double *parent, 
                              cudaStream_t stream);
 
 /* One two-time child boundary leaf (2, 4, width, leaf_z, leaf_side): time 0
- * the child field's own ring, time 1 the parent interpolated to the same ring
- * cells (w = NULL: the child's own ring again, as for the base leaves); W / E
+ * the child field's own ring (with child_sub set: of child - child_sub, a
+ * base state from a total and its perturbation), time 1 the parent
+ * interpolated to the same ring cells (w = NULL: the time-0 ring again, as
+ * for the base leaves); W / E
  * columns and S / N rows from the domain edge inward, zero beyond the field's
  * extent (side_len = the strips' tangential length) or the leaf's.  One call
  * per leaf replaces build_child_boundary_package
  * (nesting/boundary_construction.py:360-451: field_sides_3d/_2d, _fit and the
  * two-time stack). */
-int wrfgpu_nest_ring_leaf(const wrfgpu_nest_interp *w, const double *parent, const double *child, int nz,
-                          int child_ny, int child_nx, int width, int side_len, int leaf_z, int leaf_side,
-                          double *leaf, cudaStream_t stream);
+int wrfgpu_nest_ring_leaf(const wrfgpu_nest_interp *w, const double *parent, const double *child,
+                          const double *child_sub, int nz, int child_ny, int child_nx, int width, int side_len,
+                          int leaf_z, int leaf_side, double *leaf, cudaStream_t stream);
 
 /* WRF copy_fcn feedback plan of one staggering (device index arrays) and its
  * sm121 smoother interior (coupling/boundary_feedback.py:170-319). */

@@ -208,7 +208,8 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_step_epilogue_device_lead.restype = _I
     lib.wrfgpu_nest_interp_field.argtypes = [ctypes.POINTER(NestInterp), _P, _I, _P, _P]
     lib.wrfgpu_nest_interp_field.restype = _I
-    lib.wrfgpu_nest_ring_leaf.argtypes = [ctypes.POINTER(NestInterp), _P, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P]
+    lib.wrfgpu_nest_ring_leaf.argtypes = [ctypes.POINTER(NestInterp), _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _P,
+                                          _P]
     lib.wrfgpu_nest_ring_leaf.restype = _I
     lib.wrfgpu_nest_feedback.argtypes = [ctypes.POINTER(NestFeedbackPlan), _P, _P, _I, _P, _P, _P]
     lib.wrfgpu_nest_feedback.restype = _I

@@ -1811,8 +1811,8 @@ extern "C" int wrfgpu_nest_interp_field(const wrfgpu_nest_interp *w, const doubl
 }
 
 extern "C" int wrfgpu_nest_ring_leaf(const wrfgpu_nest_interp *w, const double *parent, const double *child,
-                                     int nz, int child_ny, int child_nx, int width, int side_len, int leaf_z,
-                                     int leaf_side, double *leaf, cudaStream_t stream) {
+                                     const double *child_sub, int nz, int child_ny, int child_nx, int width,
+                                     int side_len, int leaf_z, int leaf_side, double *leaf, cudaStream_t stream) {
   if (child == nullptr || leaf == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "child/leaf is NULL");
   if (w != nullptr) {
     int rc = nest_interp_check(w);
@@ -1831,6 +1831,7 @@ extern "C" int wrfgpu_nest_ring_leaf(const wrfgpu_nest_interp *w, const double *
   a.interp = w != nullptr ? 1 : 0;
   a.parent = parent;
   a.child = child;
+  a.child_sub = child_sub;
   a.nzf = nz;
   a.width = width;
   a.side_len = side_len;

@@ -54,6 +54,7 @@ struct NestRingJob {
   int interp;             // 1: time 1 from the parent; 0: time 1 = time 0
   const double *parent;
   const double *child;    // (nzf, cny, cnx)
+  const double *child_sub;  // nullable: the ring of child - child_sub (a base = total - perturbation)
   int nzf;                // levels of the field
   int width, side_len;    // strip geometry (field_sides_3d)
   int lz, lside;          // leaf extents (the fit)
@@ -82,8 +83,11 @@ __global__ void k_nest_ring_leaf(NestRingJob a) {
     }
   }
   if (jj >= 0) {
-    v = (t == 1 && a.interp) ? nest_gather(a.w, a.parent, z, jj, ii)
-                             : __ldg(a.child + ((size_t)z * cny + jj) * cnx + ii);
+    const size_t e = ((size_t)z * cny + jj) * cnx + ii;
+    if (t == 1 && a.interp)
+      v = nest_gather(a.w, a.parent, z, jj, ii);
+    else
+      v = a.child_sub != nullptr ? __ldg(a.child + e) - __ldg(a.child_sub + e) : __ldg(a.child + e);
   }
   a.leaf[((((size_t)t * 4 + side) * a.width + b) * a.lz + z) * a.lside + q] = v;
 }

@@ -30,7 +30,7 @@ the current CUDA stream.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, fields, replace
+from dataclasses import dataclass, replace
 
 import numpy as np
 import torch
@@ -139,36 +139,36 @@ def build_child_boundary_package(child_state: State, parent_state: State, weight
     side_len = int(max(child_state.u_bdy.shape[-1], child_state.v_bdy.shape[-1]))
     lib = _capi.load()
     st = torch.cuda.current_stream(child_state.u.device)
-    child_phb = child_state.ph_total - child_state.ph_perturbation
-    child_pb = child_state.p_total - child_state.p_perturbation
-    child_mub = child_state.mu_total - child_state.mu_perturbation
-    jobs = {  # leaf: (child field, parent field or None, weights)
-        "u_bdy": (child_state.u, parent_state.u, weights.u),
-        "v_bdy": (child_state.v, parent_state.v, weights.v),
-        "w_bdy": (child_state.w, parent_state.w, weights.mass),
-        "theta_bdy": (child_state.theta, parent_state.theta, weights.mass),
-        "qv_bdy": (child_state.qv, parent_state.qv, weights.mass),
-        "ph_bdy": (child_state.ph_perturbation, parent_state.ph_perturbation, weights.mass),
-        "phb_bdy": (child_phb, None, None),
-        "p_bdy": (child_state.p_perturbation, parent_state.p_perturbation, weights.mass),
-        "pb_bdy": (child_pb, None, None),
-        "mu_bdy": (child_state.mu_perturbation, parent_state.mu_perturbation, weights.mass),
-        "mub_bdy": (child_mub, None, None),
+    cs = child_state
+    jobs = {  # leaf: (child field, subtracted child field or None, parent field or None, weights)
+        "u_bdy": (cs.u, None, parent_state.u, weights.u),
+        "v_bdy": (cs.v, None, parent_state.v, weights.v),
+        "w_bdy": (cs.w, None, parent_state.w, weights.mass),
+        "theta_bdy": (cs.theta, None, parent_state.theta, weights.mass),
+        "qv_bdy": (cs.qv, None, parent_state.qv, weights.mass),
+        "ph_bdy": (cs.ph_perturbation, None, parent_state.ph_perturbation, weights.mass),
+        "phb_bdy": (cs.ph_total, cs.ph_perturbation, None, None),  # the child's own base
+        "p_bdy": (cs.p_perturbation, None, parent_state.p_perturbation, weights.mass),
+        "pb_bdy": (cs.p_total, cs.p_perturbation, None, None),
+        "mu_bdy": (cs.mu_perturbation, None, parent_state.mu_perturbation, weights.mass),
+        "mub_bdy": (cs.mu_total, cs.mu_perturbation, None, None),
     }
     new = {}
-    for name, (cf, pf, wt) in jobs.items():
+    for name, (cf, csub, pf, wt) in jobs.items():
         old = getattr(child_state, name)
         if old is None:
             raise ValueError(f"the child state has no {name} leaf to fit the package to")
         lz, lside = int(old.shape[-2]), int(old.shape[-1])
         c3 = (cf if cf.dim() == 3 else cf.unsqueeze(0)).contiguous()
+        s3 = None if csub is None else (csub if csub.dim() == 3 else csub.unsqueeze(0)).contiguous()
         leaf = torch.empty((2, 4, w, lz, lside), dtype=torch.float64, device=cf.device)
         if pf is not None:
             p3 = (pf if pf.dim() == 3 else pf.unsqueeze(0)).contiguous()
             wp = ctypes.byref(wt.c_struct())
         else:
             p3, wp = None, None
-        _capi.check(lib.wrfgpu_nest_ring_leaf(wp, None if p3 is None else _ptr(p3), _ptr(c3), int(c3.shape[0]),
+        _capi.check(lib.wrfgpu_nest_ring_leaf(wp, None if p3 is None else _ptr(p3), _ptr(c3),
+                                              None if s3 is None else _ptr(s3), int(c3.shape[0]),
                                               int(c3.shape[1]), int(c3.shape[2]), w, side_len, lz, lside,
                                               _ptr(leaf), ctypes.c_void_p(st.cuda_stream)))
         new[name] = leaf
@@ -314,3 +314,91 @@ def apply_state_feedback(parent: State, child: State, weights: StateFeedbackWeig
         if pv is not None and cv is not None:
             up[q] = fb(pv, cv, weights.mass)
     return replace(parent, **up)
+
+
+# ---------------------------------------------------------------------------
+# The nest tower: WRF's integrate recursion on the device
+# ---------------------------------------------------------------------------
+
+@dataclass(frozen=True)
+class NestEdge:
+    """Static parent -> child geometry of one tower edge
+    (nesting/scheduler.py:49-62): the space / time ratio and the 1-based
+    origin of the child in the parent grid."""
+
+    parent: str
+    child: str
+    parent_grid_ratio: int
+    i_parent_start: int
+    j_parent_start: int
+
+
+class NestTower:
+    """A nested tower advanced the way WRF's ``integrate`` recursion does
+    (frame/module_integrate.F:408-435 as nesting/scheduler.py:191-224
+    restates it): per own step of a domain, (1) advance it one forecast step
+    (``dycore.forecast_step``: RK3 step, guards, end-of-step boundary pass),
+    (2) build every child's two-time boundary package from the just-advanced
+    domain, (3) recurse into each child for ``parent_grid_ratio`` own steps,
+    (4) with ``feedback`` write the child back onto the parent
+    (``apply_state_feedback``).  Every domain's forecast clock inside its
+    parent's step is ``local_step * dt`` (local_step 1-based), so a child's
+    strips (update cadence = its parent's dt) are interpolated from the old
+    ring at 0 to the parent's new state at the parent's step end.
+
+    ``namelists[name]``: each domain's namelist; a child must be a nested
+    boundary domain (run_boundary, non-ideal source, force_geopotential off)
+    with dt = parent dt / ratio and update_cadence_s = parent dt.
+    ``grids[name]``: mass-grid extents (``nx``, ``ny``)."""
+
+    def __init__(self, order, edges, namelists, grids, *, registration: str = "sint", feedback: bool = False,
+                 bdy_width: int = 5, smooth_option: int = 1, device="cuda"):
+        self.order = list(order)
+        self.edges: dict[str, list[NestEdge]] = {}
+        for e in edges:
+            self.edges.setdefault(e.parent, []).append(e)
+        self.namelists = dict(namelists)
+        self.feedback = bool(feedback)
+        self.bdy_width = int(bdy_width)
+        self.force_w, self.fb_w = {}, {}
+        for e in edges:
+            pn, cn = self.namelists[e.parent], self.namelists[e.child]
+            r = int(e.parent_grid_ratio)
+            bc = cn.boundary_config
+            if not (cn.run_boundary and cn.bc_source != "ideal" and not bc.force_geopotential):
+                raise ValueError(f"{e.child}: a nest child must be a nested boundary domain "
+                                 "(run_boundary, non-ideal bc_source, force_geopotential off)")
+            if abs(cn.dt_s * r - pn.dt_s) > 1e-9 * pn.dt_s:
+                raise ValueError(f"{e.child}: dt_s must be the parent's dt_s / parent_grid_ratio")
+            if abs(bc.update_cadence_s - pn.dt_s) > 1e-9 * pn.dt_s:
+                raise ValueError(f"{e.child}: update_cadence_s must be the parent's dt_s")
+            c = dict(parent_grid_ratio=r, i_parent_start=e.i_parent_start, j_parent_start=e.j_parent_start,
+                     parent_grid=grids[e.parent], child_grid=grids[e.child])
+            self.force_w[e.child] = build_nest_force_weights(registration=registration, device=device, **c)
+            if self.feedback:
+                self.fb_w[e.child] = build_state_feedback_weights(smooth_option=smooth_option, device=device, **c)
+
+    def run(self, carries: dict, root_steps: int, root: str | None = None) -> dict:
+        """Advance the tower ``root_steps`` steps of its root; returns the new
+        carries (``carries`` itself is not modified)."""
+        from .dycore import forecast_step
+
+        out = dict(carries)
+        root = root or self.order[0]
+
+        def integrate(name: str, n_steps: int) -> None:
+            children = self.edges.get(name, [])
+            for local in range(1, int(n_steps) + 1):
+                out[name], _ = forecast_step(out[name], self.namelists[name], local)
+                for e in children:
+                    pkg = build_child_boundary_package(out[e.child].state, out[name].state, self.force_w[e.child],
+                                                       bdy_width=self.bdy_width)
+                    out[e.child] = out[e.child].replace(state=pkg)
+                for e in children:
+                    integrate(e.child, int(e.parent_grid_ratio))
+                    if self.feedback:
+                        fed = apply_state_feedback(out[name].state, out[e.child].state, self.fb_w[e.child])
+                        out[name] = out[name].replace(state=fed)
+
+        integrate(root, int(root_steps))
+        return out
