@@ -130,8 +130,9 @@ typedef struct wrfgpu_step_params {
    * physics pointers (NULL = zero).  0 (default): no bundle. */
   int physics;
   /* 6th-order numerical diffusion (diff_6th_opt, operational_mode.py:
-   * 2870-2876; dynamics/explicit_diffusion.py:160-226): 0 (default) off, 1 or
-   * 2 add the monotonic filter of u, v, w, theta, coupled by their dry-air
+   * 2870-2876; dynamics/explicit_diffusion.py:160-226): 0 (default) off, any
+   * other value (the reference tests int(diff_6th_opt) != 0) adds the
+   * monotonic filter of u, v, w, theta, coupled by their dry-air
    * mass, to every stage's tendencies with coefficient
    * diff_6th_factor * 0.015625 / (2 dt) (default factor 0.12). */
   int diff_6th_opt;

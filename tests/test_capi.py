@@ -229,9 +229,13 @@ def test_sixth_order_diffusion_params(lib):
     assert lib.wrfgpu_step_launch_count(ctypes.byref(_params(lib)), ctypes.byref(n0)) == 0
     assert lib.wrfgpu_step_launch_count(ctypes.byref(_params(lib, diff_6th_opt=2)), ctypes.byref(n1)) == 0
     assert n1.value == n0.value + 3  # one filter launch per stage
-    for kw in (dict(diff_6th_opt=3), dict(diff_6th_opt=1, diff_6th_factor=float("nan"))):
-        assert lib.wrfgpu_step_params_validate(ctypes.byref(_params(lib, **kw))) == \
-            _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG
+    # any nonzero diff_6th_opt switches the filter on, as the reference's int(opt) != 0
+    for opt in (3, -1):
+        assert lib.wrfgpu_step_params_validate(ctypes.byref(_params(lib, diff_6th_opt=opt))) == 0
+        assert lib.wrfgpu_step_launch_count(ctypes.byref(_params(lib, diff_6th_opt=opt)), ctypes.byref(n1)) == 0
+        assert n1.value == n0.value + 3
+    assert lib.wrfgpu_step_params_validate(ctypes.byref(_params(lib, diff_6th_opt=1, diff_6th_factor=float("nan")))) \
+        == _capi.WRFGPU_ERR_UNSUPPORTED_CONFIG
 
 
 def test_torch_op_is_registered_with_a_fake_implementation():

@@ -309,10 +309,13 @@ def test_full_size_properties(cuda_ready):
 
 
 @pytest.mark.parametrize("specified,factor,shape", [(False, 0.12, (24, 20, 14)), (True, 0.12, (24, 20, 14)),
-                                                    (False, 0.5, (33, 9, 7))])
+                                                    (False, 0.5, (33, 9, 7)), (False, 0.5, (24, 1, 8)),
+                                                    (False, 0.5, (24, 2, 8))])
 def test_per_step_parity_sixth_order_diffusion(cuda_ready, specified, factor, shape):
     """diff_6th_opt: the monotonic 6th-order filter of u, v, w, theta added to
-    every stage's coupled tendencies (operational_mode.py:2870-2876)."""
+    every stage's coupled tendencies (operational_mode.py:2870-2876); the
+    one-row slab (only v, with its two rows, is filtered along y) and a two-row
+    grid exercise the short-axis wrap."""
     case = cases.real_like_moist(*shape, hmax=800.0, specified=specified)
     case.controls.update(diff_6th_opt=2, diff_6th_factor=factor)
     for n, errs in enumerate(_per_step(case, 2 if specified else 3)):

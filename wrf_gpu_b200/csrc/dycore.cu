@@ -422,8 +422,6 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
   if (p->column_width != 0 && p->column_width != 1 && p->column_width != 16 && p->column_width != 32)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 1, 16 or 32");
   if (p->physics != 0 && p->physics != 1) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "physics must be 0 or 1");
-  if (p->diff_6th_opt < 0 || p->diff_6th_opt > 2)
-    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "diff_6th_opt must be 0, 1 or 2");
   if (p->diff_6th_opt && !(std::isfinite(p->diff_6th_factor) && p->diff_6th_factor >= 0.0))
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "diff_6th_factor must be finite and non-negative");
   if (p->diff_opt == 2 && (p->km_opt == 2 || p->km_opt == 3 || p->km_opt == 5))
