@@ -418,8 +418,12 @@ def run_gpu(args, rank, world, local_rank):
         mixed = {"value": replica_throughput(ms_m, world, cells, nsub, args.steps), "unit": METRIC,
                  "ms_per_step": ms_m / args.steps, "dtype": "f32 fluxes / f64 accumulation",
                  "rel_diff_vs_fp64_one_step": diff,
-                 "stated_error": "<= 1e-5 relative max-abs on u, v, w, theta after 60 steps vs the float64 oracle "
-                                 "(tests/test_gpu_mixed.py)"}
+                 "error_60_steps": (mixed_sixty_step_error(args.nx, args.ny, args.nz, dev)
+                                    if rank == 0 and world == 1 and not args.no_mixed60 else None),
+                 "stated_error": "60 forecast steps of this workload (specified-boundary cadence, step + "
+                                 "end-of-step boundary pass): within 2x the float64 trajectory's own one-ulp "
+                                 "spread per field, max-abs and rms (tests/test_gpu_mixed.py); <= 1e-5 on "
+                                 "u, v, w, theta after 60 steps of the smooth 3-D warm bubble vs the oracle"}
         del graph_m
     return dict(value=value, ms_per_step=ms_per_step, clocks=clk, roofline=roof, whole_step_roofline=whole,
                 kernels=kernels, e2e={"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
@@ -433,6 +437,38 @@ def run_gpu(args, rank, world, local_rank):
                 adjoint=adjoint_ratios(case, dev) if not args.no_adjoint else None,
                 epilogue=epilogue_cost(case, dev) if not args.no_epilogue else None,
                 tuned={"march_levels": tuned[0], "column_lanes": tuned[1], "column_width": tuned[2]})
+
+
+def mixed_sixty_step_error(nx, ny, nz, dev, nsteps=60):
+    """The mixed variant's difference from the float64 trajectory after 60
+    forecast steps of the workload under the WRF specified-boundary cadence
+    (RK3 step + guards + end-of-step boundary pass each step), with the
+    float64 trajectory's own spread when its initial theta moves by one ulp
+    (this moist flow amplifies any rounding difference), relative max-abs and
+    rms on u, v, w, theta."""
+    import torch
+    from wrf_gpu_b200 import cases, dycore
+
+    def run(precision, ulp=False):
+        case = cases.with_full_leaves(cases.real_like_moist(nx, ny, nz))
+        case.controls["specified_bdy_cadence"] = True
+        if ulp:
+            case.state.theta = np.nextafter(case.state.theta, np.inf)
+        nl = dycore.OperationalNamelist.from_case(case, device=dev, precision=precision)
+        c = dycore.carry_from_case(case, device=dev)
+        for n in range(nsteps):
+            c, _ = dycore.forecast_step(c, nl, n)
+        torch.cuda.synchronize(dev)
+        return {f: getattr(c.state, f).cpu().numpy() for f in ("u", "v", "w", "theta")}
+
+    ref, mix, ulp = run("fp64"), run("mixed"), run("fp64", ulp=True)
+    mx = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    rms = lambda a, b: float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b * b)), 1e-300))
+    return {"steps": nsteps, "max_abs": {f: mx(mix[f], ref[f]) for f in ref},
+            "rms": {f: rms(mix[f], ref[f]) for f in ref},
+            "fp64_one_ulp_spread_max_abs": {f: mx(ulp[f], ref[f]) for f in ref},
+            "fp64_one_ulp_spread_rms": {f: rms(ulp[f], ref[f]) for f in ref},
+            "finite": bool(all(np.isfinite(v).all() for v in ref.values()))}
 
 
 def adjoint_ratios(case, dev, reps=10):
@@ -649,6 +685,8 @@ def main():
     ap.add_argument("--nz", type=int, default=NZ)
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--no-mixed", action="store_true", help="skip timing the mixed-precision variant")
+    ap.add_argument("--no-mixed60", action="store_true",
+                    help="skip the mixed variant's 60-step error against the float64 trajectory")
     ap.add_argument("--no-adjoint", action="store_true", help="skip timing the adjoints against their forwards")
     ap.add_argument("--no-epilogue", action="store_true", help="skip timing the step epilogue (guards + boundary pass)")
     ap.add_argument("--no-tune", action="store_true", help="skip the tile-shape tuner (built-in defaults)")
