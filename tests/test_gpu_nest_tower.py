@@ -66,20 +66,34 @@ def oracle_tower(parent, child, parent_steps, feedback):
     return st
 
 
+# The child starts from its own state and adjusts to the parent's boundary
+# package, which amplifies rounding differences: the oracle tower itself moves
+# by up to ~1e-6 relative (child w) when both domains' initial theta moves by
+# one ulp.  The bound is therefore per field 10x that one-ulp spread (1e-10
+# where the spread is smaller).
+TOWER_FACTOR, TOWER_FLOOR = 10.0, 1.0e-10
+
+
 @pytest.mark.parametrize("feedback", [False, True])
 def test_nest_tower_matches_oracle(cuda_ready, feedback):
     parent, child = tower_cases()
     want = oracle_tower(parent, child, 2, feedback)
+    parent_u, child_u = tower_cases()
+    parent_u.state.theta = np.nextafter(parent_u.state.theta, np.inf)
+    child_u.state.theta = np.nextafter(child_u.state.theta, np.inf)
+    spread_run = oracle_tower(parent_u, child_u, 2, feedback)
     nls = {"p": dycore.OperationalNamelist.from_case(parent), "c": dycore.OperationalNamelist.from_case(child)}
     grids = {"p": SimpleNamespace(nx=PNX, ny=PNY), "c": SimpleNamespace(nx=CNX, ny=CNY)}
     tower = nesting.NestTower(["p", "c"], [nesting.NestEdge("p", "c", RATIO, IPOS, JPOS)], nls, grids,
                               feedback=feedback)
     got = tower.run({"p": dycore.carry_from_case(parent), "c": dycore.carry_from_case(child)}, 2)
     torch.cuda.synchronize()
+    fields = ("u", "v", "w", "theta", "p_perturbation", "ph_perturbation", "mu_perturbation", "qv")
     for name in ("p", "c"):
-        errs = {f: P.rel_err(getattr(got[name].state, f).cpu().numpy(), getattr(want[name].state, f))
-                for f in ("u", "v", "w", "theta", "p_perturbation", "ph_perturbation", "mu_perturbation", "qv")}
-        print(name, "feedback" if feedback else "one-way", {k: f"{v:.1e}" for k, v in errs.items()})
+        errs = {f: P.rel_err(getattr(got[name].state, f).cpu().numpy(), getattr(want[name].state, f)) for f in fields}
+        spread = {f: P.rel_err(getattr(spread_run[name].state, f), getattr(want[name].state, f)) for f in fields}
+        print(name, "feedback" if feedback else "one-way", {k: f"{v:.1e}" for k, v in errs.items()},
+              "one-ulp spread", {k: f"{v:.1e}" for k, v in spread.items()})
         assert all(np.isfinite(getattr(want[name].state, f)).all() for f in errs)
-        bad = {k: v for k, v in errs.items() if not v <= 1e-10}
+        bad = {k: (v, spread[k]) for k, v in errs.items() if not v <= max(TOWER_FACTOR * spread[k], TOWER_FLOOR)}
         assert not bad, (name, bad)
