@@ -18,6 +18,39 @@ namespace wg {
 #define WG_FACE_MINB 4
 #endif
 
+// Staged inputs of the u faces' large-step PGF (rk_addtend_dry.py:232-362):
+// for the block's rows and the mass points i0-1 .. i0+TSX-1 (clamped into
+// the domain, the faces' l = max(i-1, 0) and r = min(i, nx-1)), alt, al, pb,
+// php and qtot at level k, ph' at levels k and k+1, p' at the three levels
+// lev0 .. lev0+2 that dpn at faces k and k+1 reads, and mu', mu.
+constexpr int PGF_W = TSX + 1;
+enum { PGF_ALT, PGF_AL, PGF_PB, PGF_PHP, PGF_QT, PGF_PH0, PGF_PH1, PGF_P0, PGF_P1, PGF_P2, PGF_MUP, PGF_MUT,
+       PGF_U_N };
+
+__device__ __forceinline__ void load_pgf_u(const Grid &g, const StateR &s, const Diag &d, int k, int lev0, int i0,
+                                           int j0, double (*spg)[TSY][PGF_W]) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  for (int e = threadIdx.y * TSX + threadIdx.x; e < TSY * PGF_W; e += TSX * TSY) {
+    const int r = e / PGF_W, cc = e - r * PGF_W;
+    const int jj = j0 + r;
+    if (jj >= ny) continue;
+    int ic = i0 - 1 + cc;
+    ic = ic < 0 ? 0 : (ic > nx - 1 ? nx - 1 : ic);
+    auto L3 = [&](const double *a, int kk) { return ld(a, ix3(kk, jj, ic, ny, nx)); };
+    spg[PGF_ALT][r][cc] = L3(d.alt_raw, k);
+    spg[PGF_AL][r][cc] = L3(d.al_ls, k);
+    spg[PGF_PB][r][cc] = L3(d.pb, k);
+    spg[PGF_PHP][r][cc] = L3(d.php_ls, k);
+    spg[PGF_QT][r][cc] = L3(d.qtot, k);
+    spg[PGF_PH0][r][cc] = L3(s.ph_pert, k);
+    spg[PGF_PH1][r][cc] = L3(s.ph_pert, k + 1);
+    for (int q = 0; q < 3; ++q)
+      if (lev0 + q < nz) spg[PGF_P0 + q][r][cc] = L3(s.p_pert, lev0 + q);
+    spg[PGF_MUP][r][cc] = ld(s.mu_pert, ix2(jj, ic, nx));
+    spg[PGF_MUT][r][cc] = ld(s.mu_total, ix2(jj, ic, nx));
+  }
+}
+
 // Advection of u at collapsed face ii from global loads (the periodic wrap face).
 template <typename F>
 __device__ __forceinline__ double u_adv_global(const Grid &g, const StateR &s, const double *ru, const double *rv,
@@ -93,14 +126,20 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
   __shared__ double su[TQ::N];
   __shared__ double sru[TR::N];
   __shared__ double srv[TV::N];
+  // the large-step PGF's mass-point inputs of the block's faces (PGF_U_*),
+  // staged with the advection tiles so their loads are in flight together
+  __shared__ double spg[PGF_U_N][TSY][PGF_W];
   const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
   const int i = i0 + tx, j = j0 + ty;
+  // levels of the p' staged for dpn at faces k and k+1
+  const int lev0 = k == 0 ? 0 : k - 1;
   // (the specified degradation reads the real east face u(nx): no x wrap)
   load_tile<3, 3>(su, s.u + (size_t)k * ny * nxu, nxu, i0, j0, deg ? nx + 1 : nx, ny, 0.0);
   load_tile<1, 0>(sru, ru + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
   load_tile<1, 1>(srv, rv + (size_t)k * ny * nx, nx, i0, j0, nx, ny, 0.0);
+  load_pgf_u(g, s, d, k, lev0, i0, j0, spg);
   __syncthreads();
   if (i > nx || j >= ny) return;
   const size_t cu = ix3(k, j, i, ny, nxu);
@@ -164,21 +203,23 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
     u_t = tend;
   }
   {
-    auto P = [&](const double *a, int kk, int ic) { return ld(a, ix3(kk, j, ic, ny, nx)); };
-    const double ph_term = (P(s.ph_pert, k + 1, r) - P(s.ph_pert, k + 1, l)) + (P(s.ph_pert, k, r) - P(s.ph_pert, k, l));
-    const double p_term = (P(d.alt_raw, k, l) + P(d.alt_raw, k, r)) * (P(s.p_pert, k, r) - P(s.p_pert, k, l));
-    const double pb_term = (P(d.al_ls, k, l) + P(d.al_ls, k, r)) * (P(d.pb, k, r) - P(d.pb, k, l));
-    const double mp_l = ld(s.mu_pert, ix2(j, l, nx)), mp_r = ld(s.mu_pert, ix2(j, r, nx));
-    const double mt_l = (ld(s.mu_total, ix2(j, l, nx)) - mp_l) + mp_l;
-    const double mt_r = (ld(s.mu_total, ix2(j, r, nx)) - mp_r) + mp_r;
+    // staged values at the mass point ic (l or r) of this thread's row
+    auto S = [&](int slot, int ic) { return spg[slot][ty][ic - i0 + 1]; };
+    const double ph_term = (S(PGF_PH1, r) - S(PGF_PH1, l)) + (S(PGF_PH0, r) - S(PGF_PH0, l));
+    const int pk = PGF_P0 + (k - lev0);
+    const double p_term = (S(PGF_ALT, l) + S(PGF_ALT, r)) * (S(pk, r) - S(pk, l));
+    const double pb_term = (S(PGF_AL, l) + S(PGF_AL, r)) * (S(PGF_PB, r) - S(PGF_PB, l));
+    const double mp_l = S(PGF_MUP, l), mp_r = S(PGF_MUP, r);
+    const double mt_l = (S(PGF_MUT, l) - mp_l) + mp_l;
+    const double mt_r = (S(PGF_MUT, r) - mp_r) + mp_r;
     const double mass_u = c1 * (0.5 * (mt_l + mt_r)) + c2;
     const double msf_u = div_msf(ld(g.msfux, ix2(j, i, nxu)), g.msfuy, g.rmsfuy, ix2(j, i, nxu));
     double dpx = msf_u * 0.5 * g.rdx * mass_u * (ph_term + p_term + pb_term);
-    auto ps = [&](int m) { return P(s.p_pert, m, l) + P(s.p_pert, m, r); };
+    auto ps = [&](int m) { return S(PGF_P0 + (m - lev0), l) + S(PGF_P0 + (m - lev0), r); };
     const double bracket = ld(g.rdnw, k) * (dpn_large(g, k + 1, top_lid, ps) - dpn_large(g, k, top_lid, ps)) -
                            0.5 * (c1 * (mp_l + mp_r));
-    dpx = dpx + msf_u * g.rdx * (P(d.php_ls, k, r) - P(d.php_ls, k, l)) * bracket;
-    const double cqu = 1.0 / (1.0 + 0.5 * (P(d.qtot, k, l) + P(d.qtot, k, r)));
+    dpx = dpx + msf_u * g.rdx * (S(PGF_PHP, r) - S(PGF_PHP, l)) * bracket;
+    const double cqu = 1.0 / (1.0 + 0.5 * (S(PGF_QT, l) + S(PGF_QT, r)));
     u_t = u_t + (-cqu) * dpx;
     o.cqu[cu] = cqu;
   }
