@@ -654,6 +654,96 @@ def run_batched(args):
     return 0
 
 
+def run_sharded(args, rank, world, local_rank):
+    """The workload split into y slabs (``wrf_gpu_b200.sharding``): with
+    ``--shard`` under torchrun one slab per rank, halo blocks swapped over
+    NCCL after each step (strong scaling of the one domain); with
+    ``--slabs K`` on one GPU, K slabs driven from one process (the halo
+    hand-over is a pack / unpack on the device), which measures what a
+    slab step and the exchange's packing cost.  Timed: whole RK3 steps of
+    every slab plus the exchange; the exchange alone is timed beside it."""
+    import torch
+    from wrf_gpu_b200 import build, cases, dycore, perfmodel, sharding
+    build.build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nx, ny, nz = args.nx, args.ny, args.nz
+    case = cases.real_like_moist(nx, ny, nz, seed=0)
+    nl = dycore.OperationalNamelist.from_case(case, device=dev)
+    carry = dycore.carry_from_case(case, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        drv = sharding.DistributedSlab(nl, boundary_pass=True)
+        slabs = [drv.slab]
+        nslab = world
+    else:
+        drv = sharding.SlabRing(nl, max(1, args.slabs), boundary_pass=True)
+        slabs = drv.slabs
+        nslab = len(slabs)
+    drv.load(carry)
+    nsub = perfmodel.substeps_per_step(nl.acoustic_substeps)
+    dt = nl.dt_s
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the same forecast steps on the whole domain (RK3 step + end-of-step boundary pass), for the
+    # cost of the halo rows
+    whole_ms = None
+    if world == 1:
+        from dataclasses import replace as _replace
+        nl_pass = _replace(nl, disable_guards=True)
+        c = carry
+        for i in range(args.warmup + args.steps):
+            if i == args.warmup:
+                e0.record(stream)
+            nxt = dycore.rk_scan_step(c, nl, lead_seconds=(i + 1) * dt)
+            st, _ = dycore.step_epilogue(nxt.state, c.state, (i + 1) * dt, nl_pass)
+            c = nxt.replace(state=st)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        whole_ms = e0.elapsed_time(e1) / args.steps
+        del c, nxt
+    del carry
+    for i in range(args.warmup):
+        drv.step((i + 1) * dt)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    e0.record(stream)
+    for i in range(args.steps):
+        drv.step((args.warmup + i + 1) * dt)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    # the exchange alone: pack every slab's send blocks and unpack them into its neighbours
+    e0.record(stream)
+    for i in range(args.steps):
+        drv.exchange()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ex_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev) / args.steps
+    L = slabs[0].layout
+    send_bytes = sum(b.numel() * 8 for b in slabs[0].pack())
+    finite = bool(all(torch.isfinite(s.carry.state.w).all().item() for s in slabs))
+    if dist is not None:
+        dist.barrier()
+    line = {"metric": METRIC, "value": nx * ny * nz * nsub * args.steps / (ms / 1000.0), "unit": METRIC,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "none", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": _workload_name(nx, ny, nz, "fp64"), "nx": nx, "ny": ny, "nz": nz,
+                       "parallelism": f"y-slabs x{nslab}" + (" over NCCL" if world > 1 else " in one process"),
+                       "halo_rows": L.halo, "rows_per_slab": L.n_local, "owned_rows": L.own,
+                       "stepped_over_owned": round(L.n_local * nslab / ny, 3)},
+            "exchange": {"ms_per_step": ex_ms, "bytes_sent_per_slab_step": send_bytes,
+                         "what": "pack + unpack" + (" + NCCL send/recv" if world > 1 else " (no transfer)")},
+            "step": "RK3 step + end-of-step lateral boundary pass per slab, forecast leads",
+            "whole_domain_ms_per_step": whole_ms, "finite": finite}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def run_profile_target(args):
     """A few plain RK3 steps of the workload (the target of ncu captures)."""
     import torch
@@ -698,6 +788,10 @@ def main():
     ap.add_argument("--diff-6th", type=int, default=0, help="with --profile-steps: diff_6th_opt of the step")
     ap.add_argument("--column-width", type=int, default=0,
                     help="with --profile-steps: column kernel (0 default, 1 one thread per column, 16 / 32 tiled)")
+    ap.add_argument("--shard", action="store_true",
+                    help="under torchrun: one y slab of the workload per rank, halos swapped over NCCL")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="one GPU: the workload as this many y slabs driven from one process")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -732,6 +826,13 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    if args.shard or args.slabs > 0:
+        rc = run_sharded(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return rc
     r = run_gpu(args, rank, world, local_rank)
     cpu = None
     if rank == 0:

@@ -506,6 +506,39 @@ int wrfgpu_nest_feedback(const wrfgpu_nest_feedback_plan *plan, const double *pa
 int wrfgpu_nest_rebuild_total(const double *parent_total, const double *parent_pert, const double *new_pert,
                               size_t n, double *out_total, cudaStream_t stream);
 
+/* ---- y-slab decomposition: row copies ------------------------------------
+ * The multi-GPU form of the step (wrf_gpu_b200/sharding.py) gives each rank
+ * a slab of rows plus halo rows and, after each step, exchanges the halo
+ * blocks of the fields the next step reads.  These entries move those rows;
+ * they replace the reference's x-halo refresh by lax.ppermute
+ * (runtime/sharding.py:800-866) and its partition / merge of the state
+ * (runtime/sharding.py:515-590, 768-798). */
+
+/* Rows [src_j0, src_j0 + nrows) of every level of src (nz, src_ny, nx) copied
+ * into rows [dst_j0, dst_j0 + nrows) of dst (nz, dst_ny, nx). */
+int wrfgpu_copy_rows(const double *src, int nz, int src_ny, int src_j0, double *dst, int dst_ny, int dst_j0,
+                     int nrows, int nx, cudaStream_t stream);
+
+/* One block of rows of one array: rows [row0, row0 + nrows) of every level
+ * of field (nz, ny, nx), stored in a packed buffer from element offset on as
+ * (nz, nrows, nx). */
+typedef struct wrfgpu_row_block {
+  double *field;
+  int nz, ny, nx;
+  int row0, nrows;
+  long long offset;
+} wrfgpu_row_block;
+
+#define WRFGPU_MAX_ROW_BLOCKS 40
+
+/* Every block's rows copied into buffer (buffer_elems doubles), one launch. */
+int wrfgpu_rows_pack(const wrfgpu_row_block *blocks, int nblocks, double *buffer, long long buffer_elems,
+                     cudaStream_t stream);
+
+/* The inverse: every block's rows written from buffer, one launch. */
+int wrfgpu_rows_unpack(const wrfgpu_row_block *blocks, int nblocks, const double *buffer, long long buffer_elems,
+                       cudaStream_t stream);
+
 /* Number of kernel launches one wrfgpu_rk3_step issues for these params. */
 int wrfgpu_step_launch_count(const wrfgpu_step_params *params, int *launches);
 

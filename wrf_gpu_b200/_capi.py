@@ -122,6 +122,16 @@ class NestFeedbackPlan(ctypes.Structure):
                 ("cwe", _I), ("csn", _I), ("i_lo", _I), ("i_hi", _I), ("j_lo", _I), ("j_hi", _I), ("smooth", _I)]
 
 
+class RowBlock(ctypes.Structure):
+    """``wrfgpu_row_block``: rows [row0, row0 + nrows) of a (nz, ny, nx) array,
+    packed at element ``offset`` of a buffer."""
+    _fields_ = [("field", _P), ("nz", _I), ("ny", _I), ("nx", _I), ("row0", _I), ("nrows", _I),
+                ("offset", ctypes.c_longlong)]
+
+
+MAX_ROW_BLOCKS = 40
+
+
 # wrfgpu_theta_limiter_diag: 4 int32 (count, x, y, z) then 3 float64 (mass before, after, residual)
 THETA_DIAG_BYTES = 40
 
@@ -134,7 +144,8 @@ EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_st
             "wrfgpu_step_epilogue_workspace_size", "wrfgpu_step_epilogue", "wrfgpu_step_epilogue_device_lead", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
             "wrfgpu_profile_class_count", "wrfgpu_profile_class_name", "wrfgpu_last_error_string",
             "wrfgpu_version", "wrfgpu_nest_interp_field", "wrfgpu_nest_ring_leaf", "wrfgpu_nest_feedback",
-            "wrfgpu_nest_rebuild_total")
+            "wrfgpu_nest_rebuild_total", "wrfgpu_copy_rows",
+            "wrfgpu_rows_pack", "wrfgpu_rows_unpack")
 
 _lib = None
 
@@ -215,6 +226,11 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_nest_feedback.restype = _I
     lib.wrfgpu_nest_rebuild_total.argtypes = [_P, _P, _P, ctypes.c_size_t, _P, _P]
     lib.wrfgpu_nest_rebuild_total.restype = _I
+    lib.wrfgpu_copy_rows.argtypes = [_P, _I, _I, _I, _P, _I, _I, _I, _I, _P]
+    lib.wrfgpu_copy_rows.restype = _I
+    for name in ("wrfgpu_rows_pack", "wrfgpu_rows_unpack"):
+        getattr(lib, name).argtypes = [ctypes.POINTER(RowBlock), _I, _P, ctypes.c_longlong, _P]
+        getattr(lib, name).restype = _I
     lib.wrfgpu_profile_enable.argtypes = [_I, _I]
     lib.wrfgpu_profile_enable.restype = _I
     lib.wrfgpu_profile_read.argtypes = [ctypes.POINTER(_D), ctypes.POINTER(_I), _I, ctypes.POINTER(_I)]

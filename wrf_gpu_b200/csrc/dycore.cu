@@ -1892,3 +1892,110 @@ extern "C" int wrfgpu_nest_rebuild_total(const double *parent_total, const doubl
   g_last_error.clear();
   return WRFGPU_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Row copies of the y-slab decomposition (wrf_gpu_b200/sharding.py): rows of
+// every level of (nz, ny, nx) arrays copied array to array (scatter / gather
+// of a slab), or packed into / unpacked from one contiguous buffer (the halo
+// blocks a rank sends and receives after each step).  One thread per element,
+// consecutive threads along a row: coalesced on both sides.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void k_copy_rows(const double *src, int src_ny, int src_j0, double *dst, int dst_ny, int dst_j0,
+                            int nrows, int nx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  const int z = blockIdx.z;
+  if (i >= nx) return;
+  dst[((size_t)z * dst_ny + dst_j0 + r) * nx + i] = __ldg(src + ((size_t)z * src_ny + src_j0 + r) * nx + i);
+}
+
+struct RowBlocks {
+  wrfgpu_row_block b[WRFGPU_MAX_ROW_BLOCKS];
+};
+
+constexpr int ROWS_THREADS = 256;
+
+// Index space (chunks of ROWS_THREADS elements, blocks): element e of block
+// blockIdx.y is (z, r, i) of its rows, at buffer[offset + e].
+template <bool PACK>
+__global__ void __launch_bounds__(ROWS_THREADS) k_rows_pack(RowBlocks B, double *buffer) {
+  const wrfgpu_row_block &blk = B.b[blockIdx.y];
+  const long long per_level = (long long)blk.nrows * blk.nx;
+  const long long n = per_level * blk.nz;
+  for (long long e = (long long)blockIdx.x * ROWS_THREADS + threadIdx.x; e < n;
+       e += (long long)gridDim.x * ROWS_THREADS) {
+    const long long z = e / per_level, rem = e - z * per_level;
+    const long long r = rem / blk.nx, i = rem - r * blk.nx;
+    const size_t f = ((size_t)z * blk.ny + blk.row0 + r) * blk.nx + i;
+    if (PACK)
+      buffer[blk.offset + e] = __ldg(blk.field + f);
+    else
+      blk.field[f] = __ldg(buffer + blk.offset + e);
+  }
+}
+
+int rows_blocks(const wrfgpu_row_block *blocks, int nblocks, long long buffer_elems, RowBlocks &B, long long &most) {
+  if (blocks == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "blocks is NULL");
+  if (nblocks < 0 || nblocks > WRFGPU_MAX_ROW_BLOCKS) return fail(WRFGPU_ERR_BAD_SHAPE, "nblocks out of range");
+  most = 0;
+  for (int k = 0; k < nblocks; ++k) {
+    const wrfgpu_row_block &b = blocks[k];
+    if (b.field == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "a row block's field is NULL");
+    if (b.nz < 1 || b.ny < 1 || b.nx < 1 || b.nrows < 0 || b.row0 < 0 || b.row0 + b.nrows > b.ny)
+      return fail(WRFGPU_ERR_BAD_SHAPE, "a row block's rows lie outside its field");
+    const long long n = (long long)b.nz * b.nrows * b.nx;
+    if (b.offset < 0 || b.offset + n > buffer_elems)
+      return fail(WRFGPU_ERR_BAD_SHAPE, "a row block lies outside the buffer");
+    B.b[k] = b;
+    most = n > most ? n : most;
+  }
+  return WRFGPU_OK;
+}
+
+template <bool PACK>
+int rows_pack_impl(const wrfgpu_row_block *blocks, int nblocks, double *buffer, long long buffer_elems,
+                   cudaStream_t stream) {
+  if (buffer == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "buffer is NULL");
+  RowBlocks B;
+  long long most = 0;
+  int rc = rows_blocks(blocks, nblocks, buffer_elems, B, most);
+  if (rc) return rc;
+  if (nblocks == 0 || most == 0) return WRFGPU_OK;
+  long long chunks = (most + ROWS_THREADS - 1) / ROWS_THREADS;
+  // a few elements per thread on large blocks; the grid stays a few waves of the SMs
+  const long long cap = 148LL * 16;
+  const int gx = (int)(chunks < cap ? chunks : cap);
+  k_rows_pack<PACK><<<dim3(gx, nblocks), ROWS_THREADS, 0, stream>>>(B, buffer);
+  rc = check_launch(PACK ? "k_rows_pack" : "k_rows_unpack");
+  if (rc) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+}  // namespace
+
+extern "C" int wrfgpu_copy_rows(const double *src, int nz, int src_ny, int src_j0, double *dst, int dst_ny,
+                                int dst_j0, int nrows, int nx, cudaStream_t stream) {
+  if (src == nullptr || dst == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "src/dst is NULL");
+  if (nz < 1 || nz > 65535 || nx < 1 || nrows < 0 || nrows > 65535 || src_ny < 1 || dst_ny < 1)
+    return fail(WRFGPU_ERR_BAD_SHAPE, "bad row-copy extents");
+  if (dst_j0 < 0 || dst_j0 + nrows > dst_ny || src_j0 < 0 || src_j0 + nrows > src_ny)
+    return fail(WRFGPU_ERR_BAD_SHAPE, "rows out of range");
+  if (nrows == 0) return WRFGPU_OK;
+  k_copy_rows<<<dim3((nx + 127) / 128, nrows, nz), 128, 0, stream>>>(src, src_ny, src_j0, dst, dst_ny, dst_j0, nrows,
+                                                                      nx);
+  int rc = check_launch("k_copy_rows");
+  if (rc) return rc;
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_rows_pack(const wrfgpu_row_block *blocks, int nblocks, double *buffer,
+                                long long buffer_elems, cudaStream_t stream) {
+  return rows_pack_impl<true>(blocks, nblocks, buffer, buffer_elems, stream);
+}
+
+extern "C" int wrfgpu_rows_unpack(const wrfgpu_row_block *blocks, int nblocks, const double *buffer,
+                                  long long buffer_elems, cudaStream_t stream) {
+  return rows_pack_impl<false>(blocks, nblocks, const_cast<double *>(buffer), buffer_elems, stream);
+}
