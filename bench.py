@@ -668,7 +668,8 @@ def run_sharded(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     nx, ny, nz = args.nx, args.ny, args.nz
-    case = cases.real_like_moist(nx, ny, nz, seed=0)
+    # every strip of the end-of-step boundary pass, from the initial edge rows
+    case = cases.with_full_leaves(cases.real_like_moist(nx, ny, nz, seed=0))
     nl = dycore.OperationalNamelist.from_case(case, device=dev)
     carry = dycore.carry_from_case(case, device=dev)
     stream = torch.cuda.current_stream(dev)
