@@ -98,8 +98,9 @@ __device__ __forceinline__ double relax_weight_v(int j, int i, int y_len, int x_
 #endif
 constexpr int UV_KC = WG_UV_KC;
 // resident 128-thread blocks per SM requested from the register allocator
+// (4: 128 registers; timed at 433 x 433 x 50 against 1 (164 registers) and 5)
 #ifndef WG_UV_MINB
-#define WG_UV_MINB 1
+#define WG_UV_MINB 4
 #endif
 
 // PIN: compile in the boundary cadence's ring-0 tangential wind pins.

@@ -14,8 +14,17 @@
 namespace wg {
 
 // Resident blocks per SM requested for the face kernels (register budget).
-#ifndef WG_FACE_MINB
-#define WG_FACE_MINB 4
+// (per kernel; chosen by timing each at 433 x 433 x 50: fewer registers and
+// more resident warps hide more of the tile loads' latency, up to the point
+// where spills cost more than the warps gain)
+#ifndef WG_UFACE_MINB
+#define WG_UFACE_MINB 5
+#endif
+#ifndef WG_VFACE_MINB
+#define WG_VFACE_MINB 6
+#endif
+#ifndef WG_WFACE_MINB
+#define WG_WFACE_MINB 5
 #endif
 
 // Staged inputs of the u faces' large-step PGF (rk_addtend_dry.py:232-362):
@@ -114,7 +123,7 @@ __device__ __forceinline__ double v_adv_global(const Grid &g, const StateR &s, c
 // u faces, tiled advection.  Grid over faces 0..nx.
 // ---------------------------------------------------------------------------
 template <typename F, bool DEG>
-__global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+__global__ void __launch_bounds__(TSX *TSY, WG_UFACE_MINB) k_uface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muu, const double *muus,
                                                            const double *base_u, int top_lid, int run_boundary,
@@ -264,7 +273,7 @@ __global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_uface_tiled(Grid g, 
 // v faces, tiled advection.  Grid over faces 0..ny.
 // ---------------------------------------------------------------------------
 template <typename F, bool DEG>
-__global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_vface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+__global__ void __launch_bounds__(TSX *TSY, WG_VFACE_MINB) k_vface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom, Diag d,
                                                            const double *muv, const double *muvs,
                                                            const double *base_v, int top_lid, int run_boundary,
@@ -443,7 +452,7 @@ __device__ __forceinline__ void ph_adv_order6(int j, int i, int ny, int nx, PTF 
 // (h_sca_adv_order >= 4 with specified lateral BCs), otherwise order 2.
 // ---------------------------------------------------------------------------
 template <typename F, bool ORD6, bool DEG>
-__global__ void __launch_bounds__(TSX *TSY, WG_FACE_MINB) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
+__global__ void __launch_bounds__(TSX *TSY, WG_WFACE_MINB) k_wface_tiled(Grid g, StateR s, StateR ref, const double *ru,
                                                            const double *rv, const double *rom,
                                                            const double *ww_stage, const double *qtot,
                                                            const double *mub, const double *mut, const double *muts0,

@@ -55,6 +55,26 @@ __device__ __forceinline__ P pick6(const P (&p)[6], int n) {
   return r;
 }
 
+// Resident 256-thread blocks per SM requested from the register allocator
+// (timed at 433 x 433 x 50: 6 for the scalar advection, 4 for the limiter's
+// scale pass; unset: no request).
+#ifndef WG_SCALAR_MINB
+#define WG_SCALAR_MINB 6
+#endif
+#ifndef WG_LIM_MINB
+#define WG_LIM_MINB 4
+#endif
+#ifdef WG_SCALAR_MINB
+#define WG_SCALAR_BOUNDS __launch_bounds__(TSX * TSY, WG_SCALAR_MINB)
+#else
+#define WG_SCALAR_BOUNDS __launch_bounds__(TSX * TSY)
+#endif
+#ifdef WG_LIM_MINB
+#define WG_LIM_BOUNDS __launch_bounds__(TSX * TSY, WG_LIM_MINB)
+#else
+#define WG_LIM_BOUNDS __launch_bounds__(TSX * TSY)
+#endif
+
 // Levels per marching block: the kernels are instantiated for these chunk
 // sizes (compile-time loop bounds); the default and the tuner's choices.
 constexpr int MARCH_KC = 10;
@@ -69,7 +89,7 @@ constexpr int MARCH_KC_CHOICES[] = {5, 10, 25};
 // species.
 // ---------------------------------------------------------------------------
 template <typename F, int KC, bool DEG>
-__global__ void __launch_bounds__(TSX *TSY) k_scalar_adv_march(Grid g, StateR s, StateR ref, const double *ru,
+__global__ void WG_SCALAR_BOUNDS k_scalar_adv_march(Grid g, StateR s, StateR ref, const double *ru,
                                                                 const double *rv, const double *rom, const double *mut,
                                                                 const double *muts0, const double *base_theta,
                                                                 int theta_plain, int nfields, MassOut o) {
@@ -205,7 +225,7 @@ struct LimMarchSmem {
 };
 
 template <typename F, int KC, bool DEG>
-__global__ void __launch_bounds__(TSX *TSY) k_lim_march(Grid g, LimArgs a, const double *field,
+__global__ void WG_LIM_BOUNDS k_lim_march(Grid g, LimArgs a, const double *field,
                                                          const double *field_old, double *s1w, double *s2w,
                                                          LimFaces fo) {
   __shared__ LimMarchSmem sm;
