@@ -279,7 +279,12 @@ struct CoefOut {
 constexpr int COEF_TY = 8;
 inline size_t coef_smem_bytes(int nz) { return (size_t)3 * (nz + 1) * 32 * sizeof(double); }
 
-__global__ void __launch_bounds__(32 * COEF_TY) k_coef(Grid g, const double *mut, const double *muts0,
+#ifdef WG_COEF_MINB
+#define WG_COEF_BOUNDS __launch_bounds__(32 * COEF_TY, WG_COEF_MINB)
+#else
+#define WG_COEF_BOUNDS __launch_bounds__(32 * COEF_TY)
+#endif
+__global__ void WG_COEF_BOUNDS k_coef(Grid g, const double *mut, const double *muts0,
                                                        const double *mu_work0, const double *c2a, const double *cqw,
                                                        const double *alt, const double *theta_w, const double *ph_w,
                                                        const double *ref_theta, double cof, int top_lid, CoefOut o) {

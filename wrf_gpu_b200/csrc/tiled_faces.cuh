@@ -709,7 +709,12 @@ __global__ void __launch_bounds__(TSX *TSY, WG_WFACE_MINB) k_wface_tiled(Grid g,
 // ---------------------------------------------------------------------------
 inline size_t transport_smem_bytes(int nz) { return (size_t)2 * nz * 32 * sizeof(double); }
 
-__global__ void __launch_bounds__(256) k_transport_tiled(Grid g, const double *u, const double *v,
+#ifdef WG_TRANSPORT_MINB
+#define WG_TRANSPORT_BOUNDS __launch_bounds__(256, WG_TRANSPORT_MINB)
+#else
+#define WG_TRANSPORT_BOUNDS __launch_bounds__(256)
+#endif
+__global__ void WG_TRANSPORT_BOUNDS k_transport_tiled(Grid g, const double *u, const double *v,
                                                           const double *mu_total, double *ru, double *rv, double *rom,
                                                           double *ww_spec) {
   extern __shared__ double sm[];
