@@ -264,3 +264,21 @@ def test_limiter_3d_with_y_flow_and_distinct_old_field(opt):
     args = (f, fo, ru, rv, rom, mu, c1, c2, 1.0, 1.0, rdzw, fzm, fzp, 0.4, opt)
     want, got = wrf_limited_tendency(*args), _oracle(*args)
     assert np.max(np.abs(got - want)) < 1e-12
+
+
+@pytest.mark.parametrize("opt", [1, 2])
+def test_limited_coupled_tendency_conserves_mass(opt):
+    """The reference's moisture-conservation property
+    (tests/dynamics/test_moisture_advection_operational.py:153-166): on a
+    periodic domain with uniform layers, the coupled limited tendency sums to
+    zero relative to the sum of its magnitudes (1e-12)."""
+    rng = np.random.default_rng(11)
+    nz, ny, nx = 6, 10, 12
+    f = _blob(nz, ny, nx) + 0.05 * rng.random((nz, ny, nx))
+    fo = np.clip(f + 0.02 * rng.standard_normal((nz, ny, nx)), 0.0, None)
+    ru, rom = _xz_stream_flow(nz, ny, nx, 0.25)
+    rv = np.full((nz, ny, nx), 0.3)
+    mu = 1.0 + 0.1 * rng.random((ny, nx))
+    c1, c2, rdzw, fzm, fzp = _unit(nz)
+    tend = _oracle(f, fo, ru, rv, rom, mu, c1, c2, 1.0, 1.0, rdzw, fzm, fzp, 0.4, opt)
+    assert abs(tend.sum()) / np.abs(tend).sum() < 1e-12
