@@ -20,9 +20,11 @@
 //   * k_adj_faces  -- the u / v face cotangents gathered from the two cells
 //                     each face bounds (the transpose of k_div_h), plus the
 //                     outputs' own;
-//   * k_adj_uv     -- the transpose of advance_uv: every face scatters its
-//                     pressure-gradient cotangent into p, ph, al, muts and
-//                     mudf with atomic adds (edge-clamped pairs alias).
+//   * k_adj_uv_faces, k_adj_uv_cells -- the transpose of advance_uv: every
+//                     face forms its pressure-gradient weights, then every
+//                     column gathers its four faces' shares into p, ph, al,
+//                     muts and mudf in a fixed order (edge-clamped pairs
+//                     alias), so the cotangents are the same on every run.
 #pragma once
 #include "dycore_common.cuh"
 #include "acoustic_kernels.cuh"
@@ -40,6 +42,7 @@ struct AdjScratch {
   // mass-level: theta_w' bar (calc_p_rho part), theta flux divergence bar and
   // dvdxi bar; face-level: rhs bar (ph finish part), w bar, ww bar
   double *gthw, *gtend, *gdv, *grhs, *gws, *gww;
+  double *fu[3], *fv[3];  // advance_uv transpose: per-face A1, B, mudf weight
 };
 
 // Cotangents of the stage tendencies (each nullable).
@@ -69,7 +72,13 @@ struct AdjColArgs {
 // Pass 2 keeps the cotangents still collecting contributions (rhs, ph and w
 // of faces m+1 and m, the buoyancy of level m, wd of level m+1) in registers
 // and finishes each as soon as its last contributor has run.
-__global__ void k_adj_column(Grid g, AdjColArgs q) {
+// 6 resident 128-thread blocks per SM requested (85 registers): timed at
+// 433 x 433 x 50, 1.96 vs 2.34 ms per VJP without the request (127 registers).
+#ifndef WG_ADJCOL_MINB
+#define WG_ADJCOL_MINB 6
+#endif
+#define WG_ADJCOL_BOUNDS __launch_bounds__(128, WG_ADJCOL_MINB)
+__global__ void WG_ADJCOL_BOUNDS k_adj_column(Grid g, AdjColArgs q) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -392,85 +401,131 @@ struct AdjUVArgs {
   double *gu_tend, *gv_tend;  // u_tend / v_tend cotangents out (nullable)
   const double *gu, *gv;  // total cotangents of the advanced u, v
   const double *alt, *pb, *php, *cqu, *cqv, *muu, *muv;
-  double *ci_p, *ci_ph, *ci_al, *ci_muts, *ci_mudf;  // accumulated with atomics
+  double *ci_p, *ci_ph, *ci_al, *ci_muts, *ci_mudf;  // accumulated (p, al, mudf from zero)
+  double *fu[3], *fv[3];  // per-face A1, B and the mudf weight (u faces, v faces)
   double dts;
   int top_lid;
 };
 
 // Transpose of advance_uv's pressure-gradient and divergence-damping terms
-// (the u / v work values themselves pass through with unit weight).  One
-// thread per (i, j, k) of the (nx+1) x (ny+1) face positions.
-__global__ void k_adj_uv(Grid g, AdjUVArgs q) {
+// (the u / v work values themselves pass through with unit weight), in two
+// passes so that every cotangent is summed in a fixed order: k_adj_uv_faces
+// forms each face's three scalars -- A1 (the ph and p weight), B (the dpn
+// weight) and the mudf weight -- and k_adj_uv_cells gathers them per cell.
+// A face at position f of a row has the mass points a = max(f-1, 0) and
+// C = min(f, n-1) (the edge faces' pairs alias), and in the forward update
+// reads ph and p' through a difference C - a, al, pb and muts through a
+// sum, and p' through the pair sums of dpn at up to three levels.
+__global__ void k_adj_uv_faces(Grid g, AdjUVArgs q) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1, nyv = ny + 1;
+  const int nx = g.nx, ny = g.ny, nxu = nx + 1, nyv = ny + 1;
   if (i > nx || j > ny) return;
   const int ic = min(i, nx - 1), jc = min(j, ny - 1);
   const int oC = jc * nx + ic, oW = jc * nx + max(i - 1, 0), oS = max(j - 1, 0) * nx + ic;
   const size_t plane = (size_t)ny * nx;
-  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k), rdnw = ld(g.rdnw, k);
-  auto add_p = [&](int lev, int oa, double v) {
-    atomicAdd(q.ci_p + lev * plane + oa, v);
-    atomicAdd(q.ci_p + lev * plane + oC, v);
-  };
-  // dpn_acoustic of the pair sum ps = p(a) + p(C) at faces k+1 (hi) and k (lo)
-  auto add_dpn = [&](int oa, double g_hi, double g_lo) {
-    if (k + 1 < nz) {
-      add_p(k + 1, oa, 0.5 * ld(g.fnm, k + 1) * g_hi);
-      add_p(k, oa, 0.5 * ld(g.fnp, k + 1) * g_hi);
-    } else if (q.top_lid) {
-      add_p(nz - 1, oa, 0.5 * g.cf1 * g_hi);
-      add_p(nz - 2, oa, 0.5 * g.cf2 * g_hi);
-      add_p(nz - 3, oa, 0.5 * g.cf3 * g_hi);
-    }
-    if (k == 0) {
-      add_p(0, oa, 0.5 * g.cf1 * g_lo);
-      add_p(1, oa, 0.5 * g.cf2 * g_lo);
-      add_p(2, oa, 0.5 * g.cf3 * g_lo);
-    } else {
-      add_p(k, oa, 0.5 * ld(g.fnm, k) * g_lo);
-      add_p(k - 1, oa, 0.5 * ld(g.fnp, k) * g_lo);
-    }
-  };
-  // one face's transpose: a = the W (u) or S (v) mass point, C the other
-  auto face = [&](int oa, double gvel, double cq, double msfr, double mass, double rd, double md_coef) {
+  const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
+  auto face = [&](int oa, double gvel, double cq, double msfr, double mass, double rd, double md_coef, double *const *f,
+                  size_t cf) {
     const double Gx = -q.dts * cq * gvel;
-    const double A1 = msfr * 0.5 * rd * mass * Gx;
-    const size_t ka = k * plane + oa, kc = k * plane + oC;
-    atomicAdd(q.ci_ph + (k + 1) * plane + oC, A1);
-    atomicAdd(q.ci_ph + (k + 1) * plane + oa, -A1);
-    atomicAdd(q.ci_ph + kc, A1);
-    atomicAdd(q.ci_ph + ka, -A1);
-    const double gpt = (ld(q.alt, ka) + ld(q.alt, kc)) * A1;
-    atomicAdd(q.ci_p + kc, gpt);
-    atomicAdd(q.ci_p + ka, -gpt);
-    const double gab = (ld(q.pb, kc) - ld(q.pb, ka)) * A1;
-    atomicAdd(q.ci_al + ka, gab);
-    atomicAdd(q.ci_al + kc, gab);
-    const double B = msfr * rd * (ld(q.php, kc) - ld(q.php, ka)) * Gx;
-    add_dpn(oa, rdnw * B, -rdnw * B);
-    const double gm = -0.5 * c1 * B;
-    atomicAdd(q.ci_muts + oa, gm);
-    atomicAdd(q.ci_muts + oC, gm);
-    const double gmd = c1 * md_coef * gvel;
-    atomicAdd(q.ci_mudf + oC, gmd);
-    atomicAdd(q.ci_mudf + oa, -gmd);
+    f[0][cf] = msfr * 0.5 * rd * mass * Gx;
+    f[1][cf] = msfr * rd * (ld(q.php, k * plane + oC) - ld(q.php, k * plane + oa)) * Gx;
+    f[2][cf] = c1 * md_coef * gvel;
   };
   if (j < ny) {
     const int fu = j * nxu + i;
     const size_t cu = (size_t)k * ny * nxu + fu;
     const double msfr = div_msf(ld(g.msfux, fu), g.msfuy, g.rmsfuy, fu);
-    face(oW, ld(q.gu, cu), ld(q.cqu, cu), msfr, c1 * ld(q.muu, fu) + c2, g.rdx, -EMDIV * g.dx * ld(g.rmsfuy, fu));
+    face(oW, ld(q.gu, cu), ld(q.cqu, cu), msfr, c1 * ld(q.muu, fu) + c2, g.rdx, -EMDIV * g.dx * ld(g.rmsfuy, fu), q.fu,
+         cu);
     if (q.gu_tend != nullptr) q.gu_tend[cu] = q.dts * ld(q.gu, cu);
   }
   if (i < nx) {
     const int fv = j * nx + i;
     const size_t cv = (size_t)k * nyv * nx + fv;
     const double msfr = div_msf(ld(g.msfvy, fv), g.msfvx, g.rmsfvx, fv);
-    face(oS, ld(q.gv, cv), ld(q.cqv, cv), msfr, c1 * ld(q.muv, fv) + c2, g.rdy, -EMDIV * g.dy * ld(g.rmsfvx, fv));
+    face(oS, ld(q.gv, cv), ld(q.cqv, cv), msfr, c1 * ld(q.muv, fv) + c2, g.rdy, -EMDIV * g.dy * ld(g.rmsfvx, fv), q.fv,
+         cv);
     if (q.gv_tend != nullptr) q.gv_tend[cv] = q.dts * ld(q.gv, cv);
   }
+}
+
+// One thread per column (i, j): the cell's share of its four faces' scalars,
+// level by level.  For each face, d = [cell is C] - [cell is a] weighs the
+// difference terms and s = [cell is C] + [cell is a] the sum terms (2 or 0
+// at an aliased edge face).
+__global__ void k_adj_uv_cells(Grid g, AdjUVArgs q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1, nyv = ny + 1;
+  if (i >= nx || j >= ny) return;
+  const size_t plane = (size_t)ny * nx;
+  const size_t c2d = (size_t)j * nx + i;
+  // the four faces: u at i (W) and i+1 (E), v at j (S) and j+1 (N)
+  const size_t fo[4] = {(size_t)j * nxu + i, (size_t)j * nxu + i + 1, (size_t)j * nx + i, (size_t)(j + 1) * nx + i};
+  const size_t fplane[4] = {(size_t)ny * nxu, (size_t)ny * nxu, (size_t)nyv * nx, (size_t)nyv * nx};
+  const double dw[4] = {i == 0 ? 0.0 : 1.0, i == nx - 1 ? 0.0 : -1.0, j == 0 ? 0.0 : 1.0, j == ny - 1 ? 0.0 : -1.0};
+  const double sw[4] = {i == 0 ? 2.0 : 1.0, i == nx - 1 ? 2.0 : 1.0, j == 0 ? 2.0 : 1.0, j == ny - 1 ? 2.0 : 1.0};
+  // the other mass point of each face's pair (for the alt / pb terms)
+  const size_t other[4] = {(size_t)j * nx + max(i - 1, 0), (size_t)j * nx + min(i + 1, nx - 1),
+                           (size_t)max(j - 1, 0) * nx + i, (size_t)min(j + 1, ny - 1) * nx + i};
+  auto F = [&](int n, int comp, int k) {
+    const double *const *f = n < 2 ? q.fu : q.fv;
+    return ld(f[comp], (size_t)k * fplane[n] + fo[n]);
+  };
+  // sum-weighted B of the four faces at level k (the pair sums of dpn)
+  auto Bs = [&](int k) {
+    double b = 0.0;
+    for (int n = 0; n < 4; ++n) b = b + sw[n] * F(n, 1, k);
+    return b;
+  };
+  double muts = 0.0, mudf = 0.0;
+  for (int kk = 0; kk <= nz; ++kk) {
+    const size_t c = (size_t)kk * plane + c2d;
+    // ph: face levels kk (its lower face) and kk - 1 (its upper face)
+    double gph = 0.0;
+    for (int k = kk - 1; k <= kk; ++k) {
+      if (k < 0 || k >= nz) continue;
+      for (int n = 0; n < 4; ++n) gph = gph + dw[n] * F(n, 0, k);
+    }
+    q.ci_ph[c] += gph;
+    if (kk == nz) break;
+    const double c1 = ld(g.c1h, kk);
+    double gp = 0.0, gal = 0.0;
+    for (int n = 0; n < 4; ++n) {
+      const double A1 = F(n, 0, kk);
+      const double alt_c = ld(q.alt, c), alt_o = ld(q.alt, (size_t)kk * plane + other[n]);
+      const double pb_c = ld(q.pb, c), pb_o = ld(q.pb, (size_t)kk * plane + other[n]);
+      // a face whose C is this cell: + (alt_a + alt_C) A1; whose a is: - (...)
+      gp = gp + dw[n] * ((alt_o + alt_c) * A1);
+      // al: (pb_C - pb_a) A1 to both points (this cell is C of the W / S
+      // face and a of the E / N face)
+      const double pdiff = (n == 0 || n == 2) ? (pb_c - pb_o) : (pb_o - pb_c);
+      gal = gal + sw[n] * (pdiff * A1);
+      muts = muts + sw[n] * (-0.5 * c1 * F(n, 1, kk));
+      mudf = mudf + dw[n] * F(n, 2, kk);
+    }
+    // dpn: the pair-sum weights reaching level kk from face levels kk - 1 .. kk + 1
+    const double rd_k = ld(g.rdnw, kk);
+    if (kk + 1 < nz) gp = gp + 0.5 * ld(g.fnp, kk + 1) * (rd_k * Bs(kk));
+    if (kk >= 1) gp = gp + 0.5 * ld(g.fnm, kk) * (-rd_k * Bs(kk));
+    else gp = gp + 0.5 * g.cf1 * (-rd_k * Bs(0));
+    if (kk >= 1) gp = gp + 0.5 * ld(g.fnm, kk) * (ld(g.rdnw, kk - 1) * Bs(kk - 1));
+    if (kk + 1 <= nz - 1) gp = gp + 0.5 * ld(g.fnp, kk + 1) * (-ld(g.rdnw, kk + 1) * Bs(kk + 1));
+    if (kk == 1) gp = gp + 0.5 * g.cf2 * (-ld(g.rdnw, 0) * Bs(0));
+    if (kk == 2) gp = gp + 0.5 * g.cf3 * (-ld(g.rdnw, 0) * Bs(0));
+    if (q.top_lid) {
+      const double rt = ld(g.rdnw, nz - 1);
+      if (kk == nz - 1) gp = gp + 0.5 * g.cf1 * (rt * Bs(nz - 1));
+      if (kk == nz - 2) gp = gp + 0.5 * g.cf2 * (rt * Bs(nz - 1));
+      if (kk == nz - 3) gp = gp + 0.5 * g.cf3 * (rt * Bs(nz - 1));
+    }
+    q.ci_p[c] += gp;
+    q.ci_al[c] += gal;
+  }
+  q.ci_muts[c2d] += muts;
+  q.ci_mudf[c2d] += mudf;
 }
 
 }  // namespace wg

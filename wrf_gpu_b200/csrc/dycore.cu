@@ -670,7 +670,10 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
   (kc == 5 ? tmpl<F, 5, D> : kc == 25 ? tmpl<F, 25, D> : tmpl<F, 10, D>)
 #define WG_PICK_KC_DEG(tmpl, F) (deg ? WG_PICK_KC(tmpl, F, true) : WG_PICK_KC(tmpl, F, false))
   auto kScalar = mixed ? WG_PICK_KC_DEG(k_scalar_adv_march, float) : WG_PICK_KC_DEG(k_scalar_adv_march, double);
-  auto kLimScale = mixed ? WG_PICK_KC_DEG(k_lim_march, float) : WG_PICK_KC_DEG(k_lim_march, double);
+  // the limiter's scale pass in each precision (the mixed variant stores its
+  // face fluxes and scales as float32)
+  auto kLimScaleF = WG_PICK_KC_DEG(k_lim_march, float);
+  auto kLimScaleD = WG_PICK_KC_DEG(k_lim_march, double);
 #undef WG_PICK_KC_DEG
 #undef WG_PICK_KC
 
@@ -709,7 +712,10 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
     MassOut mo;
     mo.t_tend = w.t_tend;
     mo.theta_w = w.theta_w;
-    for (int q = 0; q < 6; ++q) mo.q_tend[q] = w.qtend[q];
+    for (int q = 0; q < 6; ++q) {
+      mo.q_tend[q] = w.qtend[q];
+      mo.q_tend32[q] = reinterpret_cast<float *>(w.qtend[q]);
+    }
     PROF("k_mass");
     {
       const int nfields = 1 + ((moist && !lim_moist) ? 6 : 0);
@@ -723,16 +729,33 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
       la.ru = w.ru; la.rv = w.rv; la.rom = w.rom; la.mut = s.mu_total; la.mu_old = origin.mu_total; la.dt = dt;
       la.deg = deg;
       set_lim_constants(la, g.rdx, g.rdy);
+      // float32 views of the same scratch for the mixed variant
+      LimFacesT<float> limf32{reinterpret_cast<float *>(w.limf.lx), reinterpret_cast<float *>(w.limf.ax),
+                              reinterpret_cast<float *>(w.limf.ly), reinterpret_cast<float *>(w.limf.ay),
+                              reinterpret_cast<float *>(w.limf.lz), reinterpret_cast<float *>(w.limf.az)};
+      float *s1f = reinterpret_cast<float *>(w.s1), *s2f = reinterpret_cast<float *>(w.s2);
+      const dim3 lim_grid = tgrd(nx, ny, march_nchunk(nz, kc));
+      auto scale_pass = [&](const double *fld, const double *fld_old) {
+        if (mixed)
+          kLimScaleF<<<lim_grid, tblk(), 0, stream>>>(g, la, fld, fld_old, s1f, s2f, limf32);
+        else
+          kLimScaleD<<<lim_grid, tblk(), 0, stream>>>(g, la, fld, fld_old, w.s1, w.s2, w.limf);
+      };
       if (lim_theta) {
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
         PROF("k_lim_scale");
-        kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(g, la, s.theta, origin.theta, w.s1,
-                                                                                  w.s2, w.limf);
+        scale_pass(s.theta, origin.theta);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
-        k_lim_tend_faces<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, w.limf, w.s1, w.s2, in->base_theta,
-                                                                 s.mu_total, w.t_tend);
+        // theta's tendency stays float64 (the acoustic loop reads it)
+        if (mixed)
+          k_lim_tend_faces<float, double><<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, limf32, s1f, s2f,
+                                                                                in->base_theta, s.mu_total, w.t_tend);
+        else
+          k_lim_tend_faces<double, double><<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, w.limf, w.s1, w.s2,
+                                                                                 in->base_theta, s.mu_total,
+                                                                                 w.t_tend);
         LAUNCH_CHECK("k_lim_tend");
       }
       if (lim_moist) {
@@ -740,12 +763,15 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
         la.offset = 0.0;
         for (int q = 0; q < 6; ++q) {
           PROF("k_lim_scale");
-          kLimScale<<<tgrd(nx, ny, march_nchunk(nz, kc)), tblk(), 0, stream>>>(g, la, s.q[q], origin.q[q], w.s1,
-                                                                                    w.s2, w.limf);
+          scale_pass(s.q[q], origin.q[q]);
           LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
-          k_lim_tend_faces<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, w.limf, w.s1, w.s2, nullptr, s.mu_total,
-                                                                   w.qtend[q]);
+          if (mixed)
+            k_lim_tend_faces<float, float><<<grd(nx, ny, nz), blk2(), 0, stream>>>(
+                g, la, limf32, s1f, s2f, nullptr, s.mu_total, reinterpret_cast<float *>(w.qtend[q]));
+          else
+            k_lim_tend_faces<double, double><<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, w.limf, w.s1, w.s2,
+                                                                                   nullptr, s.mu_total, w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
         }
       }
@@ -948,7 +974,11 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
     FinishArgs fa;
     fa.w_w = w.w_w; fa.ph_w = w.ph_w; fa.theta_w = w.theta_w; fa.p_ac = w.p; fa.mu_ac = w.mu; fa.muts_ac = w.muts;
     fa.t2ave = w.t2ave; fa.ww_ac = w.ww; fa.mut = w.mut; fa.ww_stage = ww_stage;
-    for (int q = 0; q < 6; ++q) fa.q_tend[q] = w.qtend[q];
+    for (int q = 0; q < 6; ++q) {
+      fa.q_tend[q] = w.qtend[q];
+      fa.q_tend32[q] = reinterpret_cast<const float *>(w.qtend[q]);
+    }
+    fa.q32 = mixed ? 1 : 0;
     fa.dt_rk = dt_rk[stage];
     fa.hyps = p.hypsometric_opt;
     fa.moist = moist ? 1 : 0;
@@ -1243,6 +1273,10 @@ void ac_carve(const wrfgpu_step_params &p, Carver &cv, AcLayout &L) {
   for (int q = 0; q < 14; ++q) L.x1[q] = cv.take(n[q]);
   L.s.gthw = cv.take(d.m); L.s.gtend = cv.take(d.m); L.s.gdv = cv.take(d.m);
   L.s.grhs = cv.take(d.w); L.s.gws = cv.take(d.w); L.s.gww = cv.take(d.w);
+  for (int n = 0; n < 3; ++n) {
+    L.s.fu[n] = cv.take(d.u);
+    L.s.fv[n] = cv.take(d.v);
+  }
 }
 
 double *const *work_ptrs(const wrfgpu_acoustic_work &x, double *out[14]) {
@@ -1414,7 +1448,7 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
     k_div_h<<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, A, 1, L.dvdxi, L.hdiv);
     if ((rc = check_launch("k_div_h"))) return rc;
   }
-  // the atomically accumulated cotangents start from zero
+  // the cotangents the advance_uv transpose accumulates into start from zero
   for (int q : {6, 8, 13})
     if (cudaMemsetAsync(ci[q], 0, n[q] * sizeof(double), stream) != cudaSuccess)
       return fail(WRFGPU_ERR_CUDA, "cotangent clear failed");
@@ -1440,11 +1474,22 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
   AdjFaceArgs fa{L.s.gtend, L.s.gdv, c->theta, co[0], co[1], ci[0], ci[1], ac_bdy(*p, *c, dts)};
   k_adj_faces<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, fa);
   if ((rc = check_launch("k_adj_faces"))) return rc;
-  AdjUVArgs ua{cot_tend != nullptr ? cot_tend->u_tend : nullptr, cot_tend != nullptr ? cot_tend->v_tend : nullptr,
-               ci[0], ci[1], c->alt, c->pb, c->php, c->cqu, c->cqv, c->muu, c->muv,
-               ci[6], ci[3], ci[8], ci[11], ci[13], dts, p->top_lid};
-  k_adj_uv<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, ua);
-  if ((rc = check_launch("k_adj_uv"))) return rc;
+  AdjUVArgs ua{};
+  ua.gu_tend = cot_tend != nullptr ? cot_tend->u_tend : nullptr;
+  ua.gv_tend = cot_tend != nullptr ? cot_tend->v_tend : nullptr;
+  ua.gu = ci[0]; ua.gv = ci[1];
+  ua.alt = c->alt; ua.pb = c->pb; ua.php = c->php; ua.cqu = c->cqu; ua.cqv = c->cqv; ua.muu = c->muu; ua.muv = c->muv;
+  ua.ci_p = ci[6]; ua.ci_ph = ci[3]; ua.ci_al = ci[8]; ua.ci_muts = ci[11]; ua.ci_mudf = ci[13];
+  for (int n = 0; n < 3; ++n) {
+    ua.fu[n] = L.s.fu[n];
+    ua.fv[n] = L.s.fv[n];
+  }
+  ua.dts = dts;
+  ua.top_lid = p->top_lid;
+  k_adj_uv_faces<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, ua);
+  if ((rc = check_launch("k_adj_uv_faces"))) return rc;
+  k_adj_uv_cells<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, ua);
+  if ((rc = check_launch("k_adj_uv_cells"))) return rc;
   g_last_error.clear();
   return WRFGPU_OK;
 }

@@ -80,6 +80,8 @@ __device__ __forceinline__ int wrp(int i, int n) {
 __device__ __forceinline__ double sgn(double x) { return (double)((x > 0.0) - (x < 0.0)); }
 
 __device__ __forceinline__ double ld(const double *p, size_t i) { return __ldg(p + i); }
+// a float32 intermediate of the mixed-precision variant, widened exactly
+__device__ __forceinline__ double ld(const float *p, size_t i) { return (double)__ldg(p + i); }
 
 // jnp.maximum / jnp.minimum semantics are not needed for NaN here; plain compares.
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }

@@ -47,6 +47,8 @@ struct FinishArgs {
   const double *w_w, *ph_w, *theta_w, *p_ac, *mu_ac, *muts_ac, *t2ave, *ww_ac;
   const double *mut, *ww_stage;
   const double *q_tend[6];
+  const float *q_tend32[6];  // the mixed variant's float32 species tendencies (q32)
+  int q32;
   double dt_rk;
   int hyps, moist;
   // carry outputs (nullable: written on the final stage only)
@@ -136,7 +138,8 @@ __global__ void k_finish_cells(Grid g, StateR s, StateR origin, FinishArgs a, St
     const double mass_new = c1 * mu_total_out + c2;
     const double inv = 1.0 / mass_new;
     for (int sp = 0; sp < 6; ++sp) {
-      o.q[sp][M(k)] = (mass_old * ld(origin.q[sp], M(k)) + a.dt_rk * ld(a.q_tend[sp], M(k))) * inv;
+      const double qt = a.q32 ? ld(a.q_tend32[sp], M(k)) : ld(a.q_tend[sp], M(k));
+      o.q[sp][M(k)] = (mass_old * ld(origin.q[sp], M(k)) + a.dt_rk * qt) * inv;
     }
   } else if (o.q[0] != nullptr && s.q[0] != nullptr) {
     for (int sp = 0; sp < 6; ++sp) o.q[sp][M(k)] = ld(s.q[sp], M(k));

@@ -214,6 +214,17 @@ struct VFaceOut {
 struct MassOut {
   double *t_tend, *theta_w;
   double *q_tend[6];
+  float *q_tend32[6];  // the mixed variant's float32 species tendencies
+};
+template <typename F>
+struct MassOutQ;
+template <>
+struct MassOutQ<double> {
+  __device__ static double *const (&get(const MassOut &o))[6] { return o.q_tend; }
+};
+template <>
+struct MassOutQ<float> {
+  __device__ static float *const (&get(const MassOut &o))[6] { return o.q_tend32; }
 };
 
 // ---------------------------------------------------------------------------

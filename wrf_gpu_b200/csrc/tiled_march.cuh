@@ -111,7 +111,8 @@ __global__ void WG_SCALAR_BOUNDS k_scalar_adv_march(Grid g, StateR s, StateR ref
   const int i = i0 + tx, j = j0 + ty;
   const bool valid = i < nx && j < ny;
   const double *fld = (field == 0) ? s.theta : pick6(s.q, field - 1);
-  double *q_out = (field == 0) ? nullptr : pick6(o.q_tend, field - 1);
+  // the species' tendencies are stored as F (float32 in the mixed variant)
+  F *q_out = (field == 0) ? nullptr : pick6(MassOutQ<F>::get(o), field - 1);
   const double sub = (field == 0) ? T0 : 0.0;
   const bool advect = (field > 0) || theta_plain;
   const size_t plane = (size_t)ny * nx;
@@ -198,7 +199,7 @@ __global__ void WG_SCALAR_BOUNDS k_scalar_adv_march(Grid g, StateR s, StateR ref
         const double mass_cur = c1 * ld(mut, c2d) + c2;
         o.theta_w[c] = mass_ref * (ld(ref.theta, c) - T0) - mass_cur * (ld(s.theta, c) - T0);
       } else {
-        q_out[c] = adv;
+        q_out[c] = (F)adv;
       }
     }
     __syncthreads();  // sq/sru/srv[b] and sfx/sfy are reused next level
@@ -226,8 +227,8 @@ struct LimMarchSmem {
 
 template <typename F, int KC, bool DEG>
 __global__ void WG_LIM_BOUNDS k_lim_march(Grid g, LimArgs a, const double *field,
-                                                         const double *field_old, double *s1w, double *s2w,
-                                                         LimFaces fo) {
+                                                         const double *field_old, F *s1w, F *s2w,
+                                                         LimFacesT<F> fo) {
   __shared__ LimMarchSmem sm;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -278,14 +279,14 @@ __global__ void WG_LIM_BOUNDS k_lim_march(Grid g, LimArgs a, const double *field
       const size_t c = (size_t)k * plane + ix2(j, i, nx);
       double r1, r2;
       lim_cell_scales(g, a, t, k, j, i, field_old, cf, r1, r2);
-      s1w[c] = r1;
-      if (a.opt == 2) s2w[c] = r2;  // the PD tendency reads s1 only
-      fo.lx[c] = cf.lx0;
-      fo.ax[c] = cf.ax0;
-      fo.ly[c] = cf.ly0;
-      fo.ay[c] = cf.ay0;
-      fo.lz[c] = cf.lz0;
-      fo.az[c] = cf.az0;
+      s1w[c] = (F)r1;
+      if (a.opt == 2) s2w[c] = (F)r2;  // the PD tendency reads s1 only
+      fo.lx[c] = (F)cf.lx0;
+      fo.ax[c] = (F)cf.ax0;
+      fo.ly[c] = (F)cf.ly0;
+      fo.ay[c] = (F)cf.ay0;
+      fo.lz[c] = (F)cf.lz0;
+      fo.az[c] = (F)cf.az0;
     }
     __syncthreads();  // staged tiles of buffer b, face fluxes and zc are reused next level
   }

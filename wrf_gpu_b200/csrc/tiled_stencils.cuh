@@ -218,17 +218,21 @@ __device__ __forceinline__ void lim_cell_scales(const Grid &g, const LimArgs &a,
 // instead of recomputing them; the east / north / top faces of a cell are the
 // west / south / bottom faces of its neighbours (the top face of level nz-1
 // carries no flux).
-struct LimFaces {
-  double *lx, *ax, *ly, *ay, *lz, *az;
+// Stored as T: float64, or float32 in the mixed-precision variant (whose
+// advective fluxes are FP32 quantities).
+template <typename T>
+struct LimFacesT {
+  T *lx, *ax, *ly, *ay, *lz, *az;
 };
+using LimFaces = LimFacesT<double>;
 
 // Limited tendency at cell (k, j, i) (flux_advection.py:937-1000) from its
 // face fluxes; S1(dr, dc) / S2(dr, dc) return the scales at the horizontal
 // neighbour (j + dr, i + dc) of level k, s1 / s2 are the scale arrays (for the
 // levels above and below).
-template <typename SA1, typename SA2>
+template <typename SA1, typename SA2, typename T>
 __device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a, SA1 S1, SA2 S2, int k, int j, int i,
-                                                const double *s1, const double *s2, const CellFluxes &cf) {
+                                                const T *s1, const T *s2, const CellFluxes &cf) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   auto S1k = [&](int kk) { return ld(s1, ix3(kk, j, i, ny, nx)); };
   auto S2k = [&](int kk) { return ld(s2, ix3(kk, j, i, ny, nx)); };
@@ -278,8 +282,11 @@ __device__ __forceinline__ double lim_cell_tend(const Grid &g, const LimArgs &a,
 
 // The limiter's tendency pass, one thread per cell, from the face fluxes and
 // scales the scale pass stored.
-__global__ void k_lim_tend_faces(Grid g, LimArgs a, LimFaces fc, const double *s1, const double *s2,
-                                 const double *base, const double *mu_total_stage, double *tend_out) {
+// T: the storage type of the face fluxes and scales; TO: of the tendency
+// (float64 for theta, T for the moisture species).
+template <typename T, typename TO>
+__global__ void k_lim_tend_faces(Grid g, LimArgs a, LimFacesT<T> fc, const T *s1, const T *s2,
+                                 const double *base, const double *mu_total_stage, TO *tend_out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -304,9 +311,9 @@ __global__ void k_lim_tend_faces(Grid g, LimArgs a, LimFaces fc, const double *s
   const double tend = lim_cell_tend(g, a, S1, S2, k, j, i, s1, s2, cf);
   if (base != nullptr) {
     const double mass_h = ld(g.c1h, k) * ld(mu_total_stage, ix2(j, i, nx)) + ld(g.c2h, k);
-    tend_out[c] = ld(base, c) * mass_h + tend;
+    tend_out[c] = (TO)(ld(base, c) * mass_h + tend);
   } else {
-    tend_out[c] = tend;
+    tend_out[c] = (TO)tend;
   }
 }
 
