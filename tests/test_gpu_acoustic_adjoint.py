@@ -227,6 +227,7 @@ def test_vjp_cost_relative_to_forward(cuda_ready):
     print(f"acoustic substep at 433x433x50: forward {t_fwd:.3f} ms, VJP {t_vjp:.3f} ms ({t_vjp / t_fwd:.2f}x) "
           f"recomputing the forward output, {t_st:.3f} ms ({t_st / t_fwd:.2f}x) from the stored one")
     assert t_st <= 3.0 * t_fwd
+    assert t_vjp <= 3.0 * t_fwd  # the checkpointing mode: forward recomputed inside the VJP
 
 
 def test_checkpointed_loop_matches_chained_substeps(cuda_ready):

@@ -451,79 +451,105 @@ __global__ void k_adj_uv_faces(Grid g, AdjUVArgs q) {
   }
 }
 
-// One thread per column (i, j): the cell's share of its four faces' scalars,
-// level by level.  For each face, d = [cell is C] - [cell is a] weighs the
-// difference terms and s = [cell is C] + [cell is a] the sum terms (2 or 0
-// at an aliased edge face).
+// The geometry of a cell's four faces (u at i and i+1, v at j and j+1): their
+// offsets and planes in the per-face arrays, the difference weights d =
+// [cell is C] - [cell is a] and sum weights s = [cell is C] + [cell is a]
+// (2 or 0 at an aliased edge face), and the other mass point of each pair.
+struct CellFaces {
+  size_t fo[4], fplane[4], other[4];
+  double dw[4], sw[4];
+  __device__ CellFaces(int i, int j, int nx, int ny) {
+    const int nxu = nx + 1, nyv = ny + 1;
+    fo[0] = (size_t)j * nxu + i; fo[1] = (size_t)j * nxu + i + 1;
+    fo[2] = (size_t)j * nx + i; fo[3] = (size_t)(j + 1) * nx + i;
+    fplane[0] = fplane[1] = (size_t)ny * nxu;
+    fplane[2] = fplane[3] = (size_t)nyv * nx;
+    other[0] = (size_t)j * nx + max(i - 1, 0); other[1] = (size_t)j * nx + min(i + 1, nx - 1);
+    other[2] = (size_t)max(j - 1, 0) * nx + i; other[3] = (size_t)min(j + 1, ny - 1) * nx + i;
+    dw[0] = i == 0 ? 0.0 : 1.0; dw[1] = i == nx - 1 ? 0.0 : -1.0;
+    dw[2] = j == 0 ? 0.0 : 1.0; dw[3] = j == ny - 1 ? 0.0 : -1.0;
+    sw[0] = i == 0 ? 2.0 : 1.0; sw[1] = i == nx - 1 ? 2.0 : 1.0;
+    sw[2] = j == 0 ? 2.0 : 1.0; sw[3] = j == ny - 1 ? 2.0 : 1.0;
+  }
+  __device__ double F(const AdjUVArgs &q, int n, int comp, int k) const {
+    const double *const *f = n < 2 ? q.fu : q.fv;
+    return ld(f[comp], (size_t)k * fplane[n] + fo[n]);
+  }
+};
+
+// One thread per cell (i, j, kk), kk = 0..nz: the cell's share of its four
+// faces' A1 and B in ph, p and al, summed in a fixed order.
 __global__ void k_adj_uv_cells(Grid g, AdjUVArgs q) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1, nyv = ny + 1;
+  const int kk = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
   if (i >= nx || j >= ny) return;
   const size_t plane = (size_t)ny * nx;
-  const size_t c2d = (size_t)j * nx + i;
-  // the four faces: u at i (W) and i+1 (E), v at j (S) and j+1 (N)
-  const size_t fo[4] = {(size_t)j * nxu + i, (size_t)j * nxu + i + 1, (size_t)j * nx + i, (size_t)(j + 1) * nx + i};
-  const size_t fplane[4] = {(size_t)ny * nxu, (size_t)ny * nxu, (size_t)nyv * nx, (size_t)nyv * nx};
-  const double dw[4] = {i == 0 ? 0.0 : 1.0, i == nx - 1 ? 0.0 : -1.0, j == 0 ? 0.0 : 1.0, j == ny - 1 ? 0.0 : -1.0};
-  const double sw[4] = {i == 0 ? 2.0 : 1.0, i == nx - 1 ? 2.0 : 1.0, j == 0 ? 2.0 : 1.0, j == ny - 1 ? 2.0 : 1.0};
-  // the other mass point of each face's pair (for the alt / pb terms)
-  const size_t other[4] = {(size_t)j * nx + max(i - 1, 0), (size_t)j * nx + min(i + 1, nx - 1),
-                           (size_t)max(j - 1, 0) * nx + i, (size_t)min(j + 1, ny - 1) * nx + i};
-  auto F = [&](int n, int comp, int k) {
-    const double *const *f = n < 2 ? q.fu : q.fv;
-    return ld(f[comp], (size_t)k * fplane[n] + fo[n]);
-  };
+  const size_t c = (size_t)kk * plane + (size_t)j * nx + i;
+  const CellFaces cf(i, j, nx, ny);
+  // ph: face levels kk (its lower face) and kk - 1 (its upper face)
+  double gph = 0.0;
+  for (int k = kk - 1; k <= kk; ++k) {
+    if (k < 0 || k >= nz) continue;
+    for (int n = 0; n < 4; ++n) gph = gph + cf.dw[n] * cf.F(q, n, 0, k);
+  }
+  q.ci_ph[c] += gph;
+  if (kk == nz) return;
   // sum-weighted B of the four faces at level k (the pair sums of dpn)
   auto Bs = [&](int k) {
     double b = 0.0;
-    for (int n = 0; n < 4; ++n) b = b + sw[n] * F(n, 1, k);
+    for (int n = 0; n < 4; ++n) b = b + cf.sw[n] * cf.F(q, n, 1, k);
     return b;
   };
-  double muts = 0.0, mudf = 0.0;
-  for (int kk = 0; kk <= nz; ++kk) {
-    const size_t c = (size_t)kk * plane + c2d;
-    // ph: face levels kk (its lower face) and kk - 1 (its upper face)
-    double gph = 0.0;
-    for (int k = kk - 1; k <= kk; ++k) {
-      if (k < 0 || k >= nz) continue;
-      for (int n = 0; n < 4; ++n) gph = gph + dw[n] * F(n, 0, k);
-    }
-    q.ci_ph[c] += gph;
-    if (kk == nz) break;
-    const double c1 = ld(g.c1h, kk);
-    double gp = 0.0, gal = 0.0;
-    for (int n = 0; n < 4; ++n) {
-      const double A1 = F(n, 0, kk);
-      const double alt_c = ld(q.alt, c), alt_o = ld(q.alt, (size_t)kk * plane + other[n]);
-      const double pb_c = ld(q.pb, c), pb_o = ld(q.pb, (size_t)kk * plane + other[n]);
-      // a face whose C is this cell: + (alt_a + alt_C) A1; whose a is: - (...)
-      gp = gp + dw[n] * ((alt_o + alt_c) * A1);
-      // al: (pb_C - pb_a) A1 to both points (this cell is C of the W / S
-      // face and a of the E / N face)
-      const double pdiff = (n == 0 || n == 2) ? (pb_c - pb_o) : (pb_o - pb_c);
-      gal = gal + sw[n] * (pdiff * A1);
-      muts = muts + sw[n] * (-0.5 * c1 * F(n, 1, kk));
-      mudf = mudf + dw[n] * F(n, 2, kk);
-    }
-    // dpn: the pair-sum weights reaching level kk from face levels kk - 1 .. kk + 1
-    const double rd_k = ld(g.rdnw, kk);
-    if (kk + 1 < nz) gp = gp + 0.5 * ld(g.fnp, kk + 1) * (rd_k * Bs(kk));
-    if (kk >= 1) gp = gp + 0.5 * ld(g.fnm, kk) * (-rd_k * Bs(kk));
-    else gp = gp + 0.5 * g.cf1 * (-rd_k * Bs(0));
-    if (kk >= 1) gp = gp + 0.5 * ld(g.fnm, kk) * (ld(g.rdnw, kk - 1) * Bs(kk - 1));
-    if (kk + 1 <= nz - 1) gp = gp + 0.5 * ld(g.fnp, kk + 1) * (-ld(g.rdnw, kk + 1) * Bs(kk + 1));
-    if (kk == 1) gp = gp + 0.5 * g.cf2 * (-ld(g.rdnw, 0) * Bs(0));
-    if (kk == 2) gp = gp + 0.5 * g.cf3 * (-ld(g.rdnw, 0) * Bs(0));
-    if (q.top_lid) {
-      const double rt = ld(g.rdnw, nz - 1);
-      if (kk == nz - 1) gp = gp + 0.5 * g.cf1 * (rt * Bs(nz - 1));
-      if (kk == nz - 2) gp = gp + 0.5 * g.cf2 * (rt * Bs(nz - 1));
-      if (kk == nz - 3) gp = gp + 0.5 * g.cf3 * (rt * Bs(nz - 1));
-    }
-    q.ci_p[c] += gp;
-    q.ci_al[c] += gal;
+  double gp = 0.0, gal = 0.0;
+  const double alt_c = ld(q.alt, c), pb_c = ld(q.pb, c);
+  for (int n = 0; n < 4; ++n) {
+    const double A1 = cf.F(q, n, 0, kk);
+    const size_t o = (size_t)kk * plane + cf.other[n];
+    // p: + (alt_a + alt_C) A1 to C, - to a
+    gp = gp + cf.dw[n] * ((ld(q.alt, o) + alt_c) * A1);
+    // al: (pb_C - pb_a) A1 to both points (this cell is C of the W / S face
+    // and a of the E / N face)
+    const double pdiff = (n == 0 || n == 2) ? (pb_c - ld(q.pb, o)) : (ld(q.pb, o) - pb_c);
+    gal = gal + cf.sw[n] * (pdiff * A1);
   }
+  // dpn: the pair-sum weights reaching level kk from face levels kk - 1 .. kk + 1
+  const double rd_k = ld(g.rdnw, kk);
+  if (kk + 1 < nz) gp = gp + 0.5 * ld(g.fnp, kk + 1) * (rd_k * Bs(kk));
+  if (kk >= 1) gp = gp + 0.5 * ld(g.fnm, kk) * (-rd_k * Bs(kk));
+  else gp = gp + 0.5 * g.cf1 * (-rd_k * Bs(0));
+  if (kk >= 1) gp = gp + 0.5 * ld(g.fnm, kk) * (ld(g.rdnw, kk - 1) * Bs(kk - 1));
+  if (kk + 1 <= nz - 1) gp = gp + 0.5 * ld(g.fnp, kk + 1) * (-ld(g.rdnw, kk + 1) * Bs(kk + 1));
+  if (kk == 1) gp = gp + 0.5 * g.cf2 * (-ld(g.rdnw, 0) * Bs(0));
+  if (kk == 2) gp = gp + 0.5 * g.cf3 * (-ld(g.rdnw, 0) * Bs(0));
+  if (q.top_lid) {
+    const double rt = ld(g.rdnw, nz - 1);
+    if (kk == nz - 1) gp = gp + 0.5 * g.cf1 * (rt * Bs(nz - 1));
+    if (kk == nz - 2) gp = gp + 0.5 * g.cf2 * (rt * Bs(nz - 1));
+    if (kk == nz - 3) gp = gp + 0.5 * g.cf3 * (rt * Bs(nz - 1));
+  }
+  q.ci_p[c] += gp;
+  q.ci_al[c] += gal;
+}
+
+// One thread per column (i, j): the column sums of the four faces' muts and
+// mudf shares, level by level.
+__global__ void k_adj_uv_cols(Grid g, AdjUVArgs q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j >= ny) return;
+  const CellFaces cf(i, j, nx, ny);
+  double muts = 0.0, mudf = 0.0;
+  for (int k = 0; k < nz; ++k) {
+    const double c1 = ld(g.c1h, k);
+    for (int n = 0; n < 4; ++n) {
+      muts = muts + cf.sw[n] * (-0.5 * c1 * cf.F(q, n, 1, k));
+      mudf = mudf + cf.dw[n] * cf.F(q, n, 2, k);
+    }
+  }
+  const size_t c2d = (size_t)j * nx + i;
   q.ci_muts[c2d] += muts;
   q.ci_mudf[c2d] += mudf;
 }

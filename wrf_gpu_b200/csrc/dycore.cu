@@ -1488,8 +1488,10 @@ extern "C" int wrfgpu_acoustic_substep_vjp(const wrfgpu_step_params *p, const wr
   ua.top_lid = p->top_lid;
   k_adj_uv_faces<<<grd(nx + 1, ny + 1, nz), blk2(), 0, stream>>>(g, ua);
   if ((rc = check_launch("k_adj_uv_faces"))) return rc;
-  k_adj_uv_cells<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, ua);
+  k_adj_uv_cells<<<grd(nx, ny, nz + 1), blk2(), 0, stream>>>(g, ua);
   if ((rc = check_launch("k_adj_uv_cells"))) return rc;
+  k_adj_uv_cols<<<grd(nx, ny, 1), blk2(), 0, stream>>>(g, ua);
+  if ((rc = check_launch("k_adj_uv_cols"))) return rc;
   g_last_error.clear();
   return WRFGPU_OK;
 }
