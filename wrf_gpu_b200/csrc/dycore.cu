@@ -11,6 +11,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <algorithm>
 
 #include "../../include/wrfgpu.h"
 #include "dycore_common.cuh"
@@ -1089,7 +1090,10 @@ extern "C" int wrfgpu_rk3_step_static_workspace(const wrfgpu_step_params *pp, co
 // Batched step: members forked onto a per-device pool of library streams.
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int kPoolStreams = 8;
+#ifndef WG_POOL_STREAMS
+#define WG_POOL_STREAMS 8
+#endif
+constexpr int kPoolStreams = WG_POOL_STREAMS;
 constexpr int kMaxPoolDevices = 64;
 struct StreamPool {
   cudaStream_t s[kPoolStreams];
@@ -1150,9 +1154,22 @@ extern "C" int wrfgpu_rk3_step_batched(int n, const wrfgpu_step_params *params, 
     if (cudaStreamWaitEvent(pool->s[k], pool->fork, 0) != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "fork wait failed");
   int first_err = WRFGPU_OK;
   std::string first_msg;
+  // members to streams, largest first onto the least loaded stream (cells)
+  std::vector<int> order(n), stream_of(n);
+  for (int m = 0; m < n; ++m) order[m] = m;
+  auto cells = [&](int m) { return (double)params[m].nx * params[m].ny * params[m].nz; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cells(a) > cells(b); });
+  std::vector<double> load(used, 0.0);
+  for (int m : order) {
+    int best = 0;
+    for (int k = 1; k < used; ++k)
+      if (load[k] < load[best]) best = k;
+    stream_of[m] = best;
+    load[best] += cells(m);
+  }
   for (int m = 0; m < n; ++m) {
     rc = wrfgpu_rk3_step(&params[m], &metrics[m], &in[m], &out[m], lead_seconds[m], workspace[m], workspace_bytes[m],
-                         pool->s[m % kPoolStreams]);
+                         pool->s[stream_of[m]]);
     if (rc && first_err == WRFGPU_OK) {
       first_err = rc;
       first_msg = "member " + std::to_string(m) + ": " + g_last_error;
