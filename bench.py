@@ -11,8 +11,11 @@ aggregate, so no L2 flush is needed).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 ``e2e`` is the same step through the C ABI with host buffers: every step
-copies its whole input state from pinned host memory to the device and its
-whole output state back, inside the timed region; the device input and output
+copies its whole input state (and the boundary strips) from pinned host
+memory to the device and reads the advanced state and mudf -- everything the
+next step reads -- back, inside the timed region (the variant that also reads
+back the carry's diagnostic leaves is reported beside it as
+``e2e.full_carry``); the device input and output
 sets are double-buffered so that step n+1's input copy and step n's output
 copy overlap step n's compute on their own streams, as a caller streaming
 cases through the GPU would run it.  The one-stream serial figure (copy in,
@@ -281,13 +284,19 @@ def run_gpu(args, rank, world, local_rank):
               "mu_perturbation", "qv", "qc", "qr", "qi", "qs", "qg", "u_bdy", "v_bdy"):
         host_in[f] = getattr(carry.state, f).cpu().pin_memory()
     host_in["mudf"] = carry.mudf.cpu().pin_memory()
-    out_tensors = [getattr(out.state, f) for f in ("u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total",
-                                                   "ph_perturbation", "mu_total", "mu_perturbation", "qv", "qc",
-                                                   "qr", "qi", "qs", "qg")]
-    out_tensors += [getattr(out, f) for f in _capi.CARRY_OUT_FIELDS]
-    host_out = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in out_tensors]
+    state_fields = ("u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total", "ph_perturbation", "mu_total",
+                    "mu_perturbation", "qv", "qc", "qr", "qi", "qs", "qg")
+    # read back every step: the advanced state and mudf -- what the next step
+    # reads; the carry's diagnostic leaves (t_2ave, ww, muave, muts, ph_tend,
+    # the saves) are read back too in the full-carry variant reported beside it
+    diag_fields = tuple(f for f in _capi.CARRY_OUT_FIELDS if f != "mudf")
+    out_tensors = [getattr(out.state, f) for f in state_fields] + [out.mudf]
+    out_full = out_tensors + [getattr(out, f) for f in diag_fields]
+    host_full = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in out_full]
+    host_out = host_full[:len(out_tensors)]
     h2d = sum(t.numel() * 8 for t in host_in.values())
     d2h = sum(t.numel() * 8 for t in host_out)
+    d2h_full = sum(t.numel() * 8 for t in host_full)
 
     def e2e_step():
         for f, h in host_in.items():
@@ -324,14 +333,14 @@ def run_gpu(args, rank, world, local_rank):
     with torch.cuda.graph(graph_b):
         stp.step_into(carry_b, out_b, lead_seconds=0.0)
     torch.cuda.synchronize(dev)
-    bufs = [(carry, out_tensors, graph), (carry_b, [getattr(out_b.state, f) for f in (
-        "u", "v", "w", "theta", "p_total", "p_perturbation", "ph_total", "ph_perturbation", "mu_total",
-        "mu_perturbation", "qv", "qc", "qr", "qi", "qs", "qg")] + [getattr(out_b, f) for f in _capi.CARRY_OUT_FIELDS],
-        graph_b)]
+    out_full_b = [getattr(out_b.state, f) for f in state_fields] + [out_b.mudf] + [getattr(out_b, f)
+                                                                                 for f in diag_fields]
+    bufs = [(carry, out_full, graph), (carry_b, out_full_b, graph_b)]
     s_in = torch.cuda.Stream(dev)
     s_out = torch.cuda.Stream(dev)
 
-    def streamed(nsteps, t0=None, t1=None):
+    def streamed(nsteps, t0=None, t1=None, full=False):
+        nout = len(host_full) if full else len(host_out)
         torch.cuda.synchronize(dev)
         if t0 is not None:
             t0.record(s_in)
@@ -354,7 +363,7 @@ def run_gpu(args, rank, world, local_rank):
             st_ev.record(stream)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(st_ev)
-                for h, t in zip(host_out, ob):
+                for h, t in zip(host_full[:nout], ob[:nout]):
                     h.copy_(t, non_blocking=True)
                 out_ev = torch.cuda.Event()
                 out_ev.record(s_out)
@@ -369,6 +378,8 @@ def run_gpu(args, rank, world, local_rank):
     streamed(k_e2e, g0, g1)
     e2e_ms = _max_over_ranks(g0.elapsed_time(g1))
     e2e_value = replica_throughput(e2e_ms, world, cells, nsub, k_e2e)
+    streamed(k_e2e, g0, g1, full=True)
+    full_ms = _max_over_ranks(g0.elapsed_time(g1))
     del graph_b, bufs
     out_ok = bool(torch.isfinite(out.state.w).all().item() and torch.isfinite(out.state.theta).all().item())
     del graph
@@ -428,9 +439,17 @@ def run_gpu(args, rank, world, local_rank):
     return dict(value=value, ms_per_step=ms_per_step, clocks=clk, roofline=roof, whole_step_roofline=whole,
                 kernels=kernels, e2e={"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                                       "d2h_bytes_per_step": d2h, "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e,
-                                      "copies": "every step copies its whole input state host->device and its "
-                                                "whole output state device->host (pinned); double-buffered so "
+                                      "copies": "every step copies its whole input state and strips "
+                                                "host->device and reads back the advanced state and mudf (the "
+                                                "next step's inputs) device->host, pinned; double-buffered so "
                                                 "copies overlap compute on separate streams",
+                                      "full_carry": {"d2h_bytes_per_step": d2h_full,
+                                                     "ms_per_step": full_ms / k_e2e,
+                                                     "value": replica_throughput(full_ms, world, cells, nsub,
+                                                                                 k_e2e),
+                                                     "what": "the same with the carry's diagnostic leaves "
+                                                             "(t_2ave, ww, muave, muts, ph_tend, saves) read "
+                                                             "back too"},
                                       "serial_ms_per_step": serial_ms / k_e2e,
                                       "serial_value": replica_throughput(serial_ms, world, cells, nsub, k_e2e)},
                 launches=stp.launches_per_step * args.steps, finite=out_ok, mixed=mixed,
