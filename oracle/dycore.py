@@ -593,23 +593,39 @@ def large_step_horizontal_pgf(s, m, rdx, rdy, top_lid, hyps):
     ph, p_abs, al, alt, php = absolute_diagnostics(s, m, hyps)
     pb = s.p_total - s.p_perturbation
     mub = s.mu_total - s.mu_perturbation
-    mu_pert = s.mu_perturbation
     cqu, cqv = moisture_coupling_factors(s)
+    return pgf_from_fields(ph, p_abs, pb, al, alt, php, mub + s.mu_perturbation, s.mu_perturbation, cqu, cqv, m,
+                           rdx, rdy, top_lid)
+
+
+def pgf_dpn(ps, m, top_lid):
+    """Face values of a pair sum of pressures for the large-step PGF
+    (rk_addtend_dry.py:289-316): half the cf1/cf2/cf3 extrapolation at the
+    surface, half the fnm/fnp interpolation inside, the cfn/cfn1 one at a
+    rigid lid's top (zero otherwise)."""
+    cfn, cfn1 = _cfn(m)
+    nz = ps.shape[0]
+    dpn = np.zeros((nz + 1,) + ps.shape[1:])
+    dpn[0] = 0.5 * (m.cf1 * ps[0] + m.cf2 * ps[1] + m.cf3 * ps[2])
+    dpn[1:nz] = 0.5 * (_col(m.fnm[1:]) * ps[1:] + _col(m.fnp[1:]) * ps[:-1])
+    if top_lid:
+        dpn[nz] = 0.5 * (cfn * ps[-1] + cfn1 * ps[-2])
+    return dpn
+
+
+def pgf_from_fields(ph, p_abs, pb, al, alt, php, mu_total, mu_pert, cqu, cqv, m, rdx, rdy, top_lid,
+                    non_hydrostatic=True):
+    """The large-step horizontal pressure gradient from its fields
+    (rk_addtend_dry.py:233-362; the same terms as acoustic_wrf.py's
+    horizontal_pressure_gradient): per u face 0.5 rdx mass_u msf_u times the
+    geopotential difference summed over the two adjacent w levels, plus
+    (alt_l + alt_r)(p_r - p_l) and (al_l + al_r)(pb_r - pb_l), then (when
+    ``non_hydrostatic``) rdx msf_u (php_r - php_l)(rdnw (dpn(k+1) - dpn(k)) -
+    0.5 c1 (mu'_l + mu'_r)); returns (-cqu dpx, -cqv dpy)."""
     c1h, c2h, rdnw = _col(m.c1h), _col(m.c2h), _col(m.rdnw)
     msf_u = (m.msfux / m.msfuy)[None]
     msf_v = (m.msfvy / m.msfvx)[None]
-    mu_total = mub + mu_pert
-    cfn, cfn1 = _cfn(m)
-
-    def dpn_faces(ps):
-        nz = ps.shape[0]
-        dpn = np.zeros((nz + 1,) + ps.shape[1:])
-        dpn[0] = 0.5 * (m.cf1 * ps[0] + m.cf2 * ps[1] + m.cf3 * ps[2])
-        dpn[1:nz] = 0.5 * (_col(m.fnm[1:]) * ps[1:] + _col(m.fnp[1:]) * ps[:-1])
-        if top_lid:
-            dpn[nz] = 0.5 * (cfn * ps[-1] + cfn1 * ps[-2])
-        return dpn
-
+    dpn_faces = lambda ps: pgf_dpn(ps, m, top_lid)
     ph_l, ph_r = xpair(ph)
     p_l, p_r = xpair(p_abs)
     pb_l, pb_r = xpair(pb)
@@ -620,11 +636,12 @@ def large_step_horizontal_pgf(s, m, rdx, rdy, top_lid, hyps):
     mass_u = c1h * muu[None] + c2h
     dpx = msf_u * 0.5 * rdx * mass_u * (((ph_r[1:] - ph_l[1:]) + (ph_r[:-1] - ph_l[:-1]))
                                         + (alt_l + alt_r) * (p_r - p_l) + (al_l + al_r) * (pb_r - pb_l))
-    php_l, php_r = xpair(php)
-    dpn = dpn_faces(p_l + p_r)
-    mu_l, mu_r = xpair(mu_pert)
-    bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_l + mu_r)[None])
-    dpx = dpx + msf_u * rdx * (php_r - php_l) * bracket
+    if non_hydrostatic:
+        php_l, php_r = xpair(php)
+        dpn = dpn_faces(p_l + p_r)
+        mu_l, mu_r = xpair(mu_pert)
+        bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_l + mu_r)[None])
+        dpx = dpx + msf_u * rdx * (php_r - php_l) * bracket
 
     ph_s, ph_n = ypair(ph)
     p_s, p_n = ypair(p_abs)
@@ -636,11 +653,12 @@ def large_step_horizontal_pgf(s, m, rdx, rdy, top_lid, hyps):
     mass_v = c1h * muv[None] + c2h
     dpy = msf_v * 0.5 * rdy * mass_v * (((ph_n[1:] - ph_s[1:]) + (ph_n[:-1] - ph_s[:-1]))
                                         + (alt_s + alt_n) * (p_n - p_s) + (al_s + al_n) * (pb_n - pb_s))
-    php_s, php_n = ypair(php)
-    dpn = dpn_faces(p_s + p_n)
-    mu_s, mu_n = ypair(mu_pert)
-    bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_s + mu_n)[None])
-    dpy = dpy + msf_v * rdy * (php_n - php_s) * bracket
+    if non_hydrostatic:
+        php_s, php_n = ypair(php)
+        dpn = dpn_faces(p_s + p_n)
+        mu_s, mu_n = ypair(mu_pert)
+        bracket = rdnw * (dpn[1:] - dpn[:-1]) - 0.5 * (c1h * (mu_s + mu_n)[None])
+        dpy = dpy + msf_v * rdy * (php_n - php_s) * bracket
     return -cqu * dpx, -cqv * dpy
 
 
