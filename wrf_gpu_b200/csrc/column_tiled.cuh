@@ -51,7 +51,10 @@ constexpr int col_minb(int tx) { return tx == 16 ? 2 * WG_COL_MINB : WG_COL_MINB
 // Levels per software-pipelined batch of the serial recurrences: the batch's
 // shared-memory operands are loaded before its first store, so the loads
 // overlap instead of each waiting behind the previous level's store.
-constexpr int COL_SU = 8;
+#ifndef WG_COL_SU
+#define WG_COL_SU 8
+#endif
+constexpr int COL_SU = WG_COL_SU;
 
 // Bulk L2 prefetch of the rows (levels 0..nz) this column block will read.
 // group 0: advance_mu_t / theta / t_2ave inputs; group 1: advance_w and
