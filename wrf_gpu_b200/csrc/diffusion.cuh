@@ -50,47 +50,87 @@ __device__ __forceinline__ double sixth_at(const double (*tile)[D6_W], int yl, d
   return t;
 }
 
-// Index space (nx+1) x (ny+1) x (nz+1) in D6_TX x D6_TY blocks: the u, v, w
-// and theta cells at (k, j, i).  The four fields' tiles (3-cell wrapped halo)
-// are loaded together, then filtered from shared memory.
+// Levels per block of k_diff6: the next level's four tiles are copied
+// (cp.async, 8-byte) while the current level is filtered.
+constexpr int D6_KC = 4;
+constexpr int D6_NS = (D6_R * D6_W + D6_TX * D6_TY - 1) / (D6_TX * D6_TY);
+
+// Index space (nx+1) x (ny+1) x ceil((nz+1) / D6_KC) in D6_TX x D6_TY blocks:
+// the u, v, w and theta cells at (k, j, i) for the block's D6_KC levels.  The
+// four fields' tiles (3-cell wrapped halo) of a level are staged together,
+// double-buffered across levels, then filtered from shared memory.
 __global__ void __launch_bounds__(D6_TX * D6_TY) k_diff6(Grid g, Diff6Args a) {
-  __shared__ double tile[4][D6_R][D6_W];
+  __shared__ double tile[2][4][D6_R][D6_W];
   const int i0 = blockIdx.x * D6_TX, j0 = blockIdx.y * D6_TY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-  const int k = blockIdx.z;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const bool mass_level = k < nz;  // u, v, theta live on nz levels, w on nz + 1 (uniform over the block)
+  const int k0 = blockIdx.z * D6_KC, k1 = min(nz + 1, k0 + D6_KC);
   const int tid = threadIdx.y * D6_TX + threadIdx.x;
-  const size_t pu = (size_t)k * (nx + 1) * ny, pv = (size_t)k * nx * (ny + 1), pm = (size_t)k * nx * ny;
-  for (int e = tid; e < D6_R * D6_W; e += D6_TX * D6_TY) {
-    const int r = e / D6_W, q = e - r * D6_W;
-    const int jm = wrap(j0 - D6_H + r, ny), jv = wrap(j0 - D6_H + r, ny + 1);
-    const int im = wrap(i0 - D6_H + q, nx), iu = wrap(i0 - D6_H + q, nx + 1);
-    tile[2][r][q] = ld(a.w, pm + (size_t)jm * nx + im);
-    if (mass_level) {
-      tile[0][r][q] = ld(a.u, pu + (size_t)jm * (nx + 1) + iu);
-      tile[1][r][q] = ld(a.v, pv + (size_t)jv * nx + im);
-      tile[3][r][q] = ld(a.theta, pm + (size_t)jm * nx + im);
+  // this thread's tile elements and their wrapped in-plane offsets (mass / w,
+  // u and v planes), resolved once for all levels
+  int om[D6_NS], ou[D6_NS], ov[D6_NS];
+#pragma unroll
+  for (int n = 0; n < D6_NS; ++n) {
+    const int e = tid + n * D6_TX * D6_TY;
+    om[n] = ou[n] = ov[n] = -1;
+    if (e < D6_R * D6_W) {
+      const int r = e / D6_W, q = e - r * D6_W;
+      const int jm = wrap(j0 - D6_H + r, ny), jv = wrap(j0 - D6_H + r, ny + 1);
+      const int im = wrap(i0 - D6_H + q, nx), iu = wrap(i0 - D6_H + q, nx + 1);
+      om[n] = jm * nx + im;
+      ou[n] = jm * (nx + 1) + iu;
+      ov[n] = jv * nx + im;
     }
   }
-  __syncthreads();
+  auto issue = [&](int k, int b) {
+    const bool mass_level = k < nz;
+    const size_t pu = (size_t)k * (nx + 1) * ny, pv = (size_t)k * nx * (ny + 1), pm = (size_t)k * nx * ny;
+    double *t = &tile[b][0][0][0];
+    constexpr int TN = D6_R * D6_W;
+#pragma unroll
+    for (int n = 0; n < D6_NS; ++n) {
+      if (om[n] < 0) continue;
+      const int e = tid + n * D6_TX * D6_TY;
+      cp_async8(t + 2 * TN + e, a.w + pm + om[n]);
+      if (mass_level) {
+        cp_async8(t + e, a.u + pu + ou[n]);
+        cp_async8(t + TN + e, a.v + pv + ov[n]);
+        cp_async8(t + 3 * TN + e, a.theta + pm + om[n]);
+      }
+    }
+    cp_async_commit();
+  };
   auto mu = [&](int jj, int ii) { return ld(a.mu, (size_t)jj * nx + ii); };
-  if (mass_level && i <= nx && j < ny) {  // u faces: mass_u from the edge-padded x average of mu
-    const double muu = i == 0 ? mu(j, 0) : (i == nx ? mu(j, nx - 1) : 0.5 * (mu(j, i - 1) + mu(j, i)));
-    const size_t c = pu + (size_t)j * (nx + 1) + i;
-    a.u_tend[c] = a.u_tend[c] + (ld(g.c1h, k) * muu + ld(g.c2h, k)) * sixth_at(tile[0], ny, a.coef);
-  }
-  if (mass_level && i < nx && j <= ny) {  // v faces
-    const double muv = j == 0 ? mu(0, i) : (j == ny ? mu(ny - 1, i) : 0.5 * (mu(j - 1, i) + mu(j, i)));
-    const size_t c = pv + (size_t)j * nx + i;
-    a.v_tend[c] = a.v_tend[c] + (ld(g.c1h, k) * muv + ld(g.c2h, k)) * sixth_at(tile[1], ny + 1, a.coef);
-  }
-  if (i < nx && j < ny) {
-    const double mt = mu(j, i);
-    const size_t c = pm + (size_t)j * nx + i;
-    a.w_tend[c] = a.w_tend[c] + (ld(g.c1f, k) * mt + ld(g.c2f, k)) * sixth_at(tile[2], ny, a.coef);
-    if (mass_level)
-      a.t_tend[c] = a.t_tend[c] + (ld(g.c1h, k) * mt + ld(g.c2h, k)) * sixth_at(tile[3], ny, a.coef);
+  issue(k0, 0);
+  for (int k = k0; k < k1; ++k) {
+    const int b = (k - k0) & 1;
+    if (k + 1 < k1) {
+      issue(k + 1, b ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const bool mass_level = k < nz;  // u, v, theta live on nz levels, w on nz + 1 (uniform over the block)
+    const size_t pu = (size_t)k * (nx + 1) * ny, pv = (size_t)k * nx * (ny + 1), pm = (size_t)k * nx * ny;
+    if (mass_level && i <= nx && j < ny) {  // u faces: mass_u from the edge-padded x average of mu
+      const double muu = i == 0 ? mu(j, 0) : (i == nx ? mu(j, nx - 1) : 0.5 * (mu(j, i - 1) + mu(j, i)));
+      const size_t c = pu + (size_t)j * (nx + 1) + i;
+      a.u_tend[c] = a.u_tend[c] + (ld(g.c1h, k) * muu + ld(g.c2h, k)) * sixth_at(tile[b][0], ny, a.coef);
+    }
+    if (mass_level && i < nx && j <= ny) {  // v faces
+      const double muv = j == 0 ? mu(0, i) : (j == ny ? mu(ny - 1, i) : 0.5 * (mu(j - 1, i) + mu(j, i)));
+      const size_t c = pv + (size_t)j * nx + i;
+      a.v_tend[c] = a.v_tend[c] + (ld(g.c1h, k) * muv + ld(g.c2h, k)) * sixth_at(tile[b][1], ny + 1, a.coef);
+    }
+    if (i < nx && j < ny) {
+      const double mt = mu(j, i);
+      const size_t c = pm + (size_t)j * nx + i;
+      a.w_tend[c] = a.w_tend[c] + (ld(g.c1f, k) * mt + ld(g.c2f, k)) * sixth_at(tile[b][2], ny, a.coef);
+      if (mass_level)
+        a.t_tend[c] = a.t_tend[c] + (ld(g.c1h, k) * mt + ld(g.c2h, k)) * sixth_at(tile[b][3], ny, a.coef);
+    }
+    __syncthreads();  // buffer b is refilled two levels on
   }
 }
 

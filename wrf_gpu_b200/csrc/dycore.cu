@@ -803,8 +803,8 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
       Diff6Args da{s.u, s.v, s.w, s.theta, s.mu_total, w.u_tend, w.v_tend, w.rw_tend, w.t_tend,
                    p.diff_6th_factor * 0.015625 / (2.0 * p.dt)};
       PROF("k_diff6");
-      k_diff6<<<dim3((nx + 1 + D6_TX - 1) / D6_TX, (ny + 1 + D6_TY - 1) / D6_TY, nz + 1), dim3(D6_TX, D6_TY, 1), 0,
-                stream>>>(g, da);
+      k_diff6<<<dim3((nx + 1 + D6_TX - 1) / D6_TX, (ny + 1 + D6_TY - 1) / D6_TY, (nz + 1 + D6_KC - 1) / D6_KC),
+                dim3(D6_TX, D6_TY, 1), 0, stream>>>(g, da);
       LAUNCH_CHECK("k_diff6");
     }
     if (constk_on(p) || smag_on(p)) {
