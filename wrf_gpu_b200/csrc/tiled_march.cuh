@@ -10,6 +10,7 @@
 // carried up the march: face k+1 of level k is face k of level k+1.
 // Arithmetic keeps the reference's expression order.
 #pragma once
+#include <type_traits>
 #include "dycore_common.cuh"
 #include "stage_kernels.cuh"
 #include "tiled_stencils.cuh"
@@ -153,23 +154,34 @@ __global__ void WG_SCALAR_BOUNDS k_scalar_adv_march(Grid g, StateR s, StateR ref
       const double *Qt = sq[b];
       const double *RU = sru[b];
       const double *RV = srv[b];
-      auto Q = [&](int r, int cc) { return Qt[(r + 3) * TQ::W + (cc + 3)] - sub; };
-      for (int e = ty * TSX + tx; e < NXF + NYF; e += TSX * TSY) {
-        if (e < NXF) {
-          const int r = e / (TSX + 1), m = e - r * (TSX + 1);
-          const double vel = RU[r * TR::W + (m + 1)];
-          sfx[e] = DEG ? hflux_spec<F>(i0 + m, nx, false, vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m),
-                                       Q(r, m + 1), Q(r, m + 2))
-                       : hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
-        } else {
-          const int e2 = e - NXF;
-          const int r = e2 / TSX, cc = e2 - r * TSX;
-          const double vel = RV[(r + 1) * TV::W + cc];
-          sfy[e2] = DEG ? hflux_spec<F>(j0 + r, ny, false, vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc),
-                                        Q(r + 1, cc), Q(r + 2, cc))
-                        : hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc), Q(r + 2, cc));
+      // SUB: theta's tiles less T0; the species' offset is 0 and x - 0.0 == x
+      auto faces = [&](auto SUB) {
+        auto Q = [&](int r, int cc) {
+          const double x = Qt[(r + 3) * TQ::W + (cc + 3)];
+          return decltype(SUB)::value ? x - sub : x;
+        };
+        for (int e = ty * TSX + tx; e < NXF + NYF; e += TSX * TSY) {
+          if (e < NXF) {
+            const int r = e / (TSX + 1), m = e - r * (TSX + 1);
+            const double vel = RU[r * TR::W + (m + 1)];
+            sfx[e] = DEG ? hflux_spec<F>(i0 + m, nx, false, vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m),
+                                         Q(r, m + 1), Q(r, m + 2))
+                         : hflux5<F>(vel, Q(r, m - 3), Q(r, m - 2), Q(r, m - 1), Q(r, m), Q(r, m + 1), Q(r, m + 2));
+          } else {
+            const int e2 = e - NXF;
+            const int r = e2 / TSX, cc = e2 - r * TSX;
+            const double vel = RV[(r + 1) * TV::W + cc];
+            sfy[e2] = DEG ? hflux_spec<F>(j0 + r, ny, false, vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc),
+                                          Q(r, cc), Q(r + 1, cc), Q(r + 2, cc))
+                          : hflux5<F>(vel, Q(r - 3, cc), Q(r - 2, cc), Q(r - 1, cc), Q(r, cc), Q(r + 1, cc),
+                                      Q(r + 2, cc));
+          }
         }
-      }
+      };
+      if (field == 0)
+        faces(std::true_type{});
+      else
+        faces(std::false_type{});
       __syncthreads();
       if (valid) {
         // the specified degradation leaves the outermost cells without
