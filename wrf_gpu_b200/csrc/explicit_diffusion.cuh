@@ -28,6 +28,7 @@
 namespace wg {
 
 constexpr double PRANDTL = 1.0 / 3.0;  // explicit_diffusion.py:956
+constexpr double RPRANDTL = 1.0 / PRANDTL;  // its correctly rounded reciprocal, for div_rcp
 
 __device__ __forceinline__ int roll_idx(int q, int n) { return q < 0 ? q + n : (q >= n ? q - n : q); }
 
@@ -54,13 +55,14 @@ __global__ void k_smag_km(Grid g, DiffArgs a, double *xkmh) {
   auto V = [&](int jj, int ii) { return ld(a.v, ix3(k, jj, ii, ny + 1, nx)); };  // core v: jj < ny
   const int ie = roll_idx(i + 1, nx), jn = roll_idx(j + 1, ny);
   // D11 = 2 du/dx, D22 = 2 dv/dy at the cell (explicit_diffusion.py:1033-1057)
-  const double d11 = 2.0 * ((U(j, ie) - U(j, i)) / g.dx);
-  const double d22 = 2.0 * ((V(jn, i) - V(j, i)) / g.dy);
+  // every x / dx and x / dy is an exact div_rcp with g.rdx = 1/dx, g.rdy = 1/dy
+  const double d11 = 2.0 * div_rcp(U(j, ie) - U(j, i), g.dx, g.rdx);
+  const double d22 = 2.0 * div_rcp(V(jn, i) - V(j, i), g.dy, g.rdy);
   // D12 = du/dy + dv/dx on the SW corner (ic, jc) of a cell (:1059-1112)
   auto d12 = [&](int jc, int ic) {
     const int js = roll_idx(jc - 1, ny), iw = roll_idx(ic - 1, nx);
-    const double dudy = (U(jc, ic) - U(js, ic)) / g.dy;
-    const double dvdx = (V(jc, ic) - V(jc, iw)) / g.dx;
+    const double dudy = div_rcp(U(jc, ic) - U(js, ic), g.dy, g.rdy);
+    const double dvdx = div_rcp(V(jc, ic) - V(jc, iw), g.dx, g.rdx);
     return dudy + dvdx;
   };
   // four-corner average, SW + NW + SE + NE (:1173-1177)
@@ -146,7 +148,7 @@ __global__ void k_smag_apply(Grid g, DiffArgs a) {
     if (k < nz) {
       // theta as the perturbation from 300 K, with xkhh = xkmh / prandtl
       auto FT = [&](int jj, int ii) { return ld(a.theta, ix3(k, jj, ii, ny, nx)) - T0; };
-      auto KH = [&](int jj, int ii) { return KM(k, jj, ii) / PRANDTL; };
+      auto KH = [&](int jj, int ii) { return div_rcp(KM(k, jj, ii), PRANDTL, RPRANDTL); };
       auto MH = [&](int jj, int ii) { return c1h * ld(a.mu, ix2(jj, ii, nx)) + c2h; };
       a.t_tend[c] = a.t_tend[c] + hdiff_point(g, j, i, ny, nx, FT, KH, MH);
     }
@@ -166,7 +168,7 @@ __global__ void __launch_bounds__(DZ_THREADS) k_dz_partial(Grid g, const double 
   double acc = 0.0;
   for (int e = threadIdx.x; e < nz * nx; e += DZ_THREADS) {
     const int k = e / nx, i = e - k * nx;
-    acc += (ld(ph_total, ix3(k + 1, j, i, ny, nx)) - ld(ph_total, ix3(k, j, i, ny, nx))) / G;
+    acc += div_rcp(ld(ph_total, ix3(k + 1, j, i, ny, nx)) - ld(ph_total, ix3(k, j, i, ny, nx)), G, RG);
   }
   s[threadIdx.x] = acc;
   __syncthreads();
@@ -189,23 +191,25 @@ __global__ void k_dz_final(Grid g, const double *partial, double *dz) {
 // (ny_f, nx_f) extent and nz_f levels (zero flux through the bottom and top).
 template <typename FF, typename FM>
 __device__ __forceinline__ double constk_point(const Grid &g, int k, int j, int i, int nz_f, int ny_f, int nx_f,
-                                               double nu, double dz, FF F, FM Ms) {
+                                               double nu, double dz, double rdz, FF F, FM Ms) {
   const int ie = roll_idx(i + 1, nx_f), iw = roll_idx(i - 1, nx_f);
   const double fc = F(k, j, i), mc = Ms(k, j, i);
   // x fluxes at the faces i+1/2 and i-1/2
-  const double fxp = 0.5 * (mc + Ms(k, j, ie)) * nu * (F(k, j, ie) - fc) / g.dx;
-  const double fxm = 0.5 * (Ms(k, j, iw) + mc) * nu * (fc - F(k, j, iw)) / g.dx;
-  double tend = 0.0 + (fxp - fxm) / g.dx;
+  // x / dx, x / dy, x / dz as exact div_rcp (rdz = 1/dz computed once)
+  const double fxp = div_rcp(0.5 * (mc + Ms(k, j, ie)) * nu * (F(k, j, ie) - fc), g.dx, g.rdx);
+  const double fxm = div_rcp(0.5 * (Ms(k, j, iw) + mc) * nu * (fc - F(k, j, iw)), g.dx, g.rdx);
+  double tend = 0.0 + div_rcp(fxp - fxm, g.dx, g.rdx);
   if (ny_f > 1) {
     const int jn = roll_idx(j + 1, ny_f), js = roll_idx(j - 1, ny_f);
-    const double fyp = 0.5 * (mc + Ms(k, jn, i)) * nu * (F(k, jn, i) - fc) / g.dy;
-    const double fym = 0.5 * (Ms(k, js, i) + mc) * nu * (fc - F(k, js, i)) / g.dy;
-    tend = tend + (fyp - fym) / g.dy;
+    const double fyp = div_rcp(0.5 * (mc + Ms(k, jn, i)) * nu * (F(k, jn, i) - fc), g.dy, g.rdy);
+    const double fym = div_rcp(0.5 * (Ms(k, js, i) + mc) * nu * (fc - F(k, js, i)), g.dy, g.rdy);
+    tend = tend + div_rcp(fyp - fym, g.dy, g.rdy);
   }
   if (nz_f > 2) {
-    const double ftop = (k + 1 <= nz_f - 1) ? 0.5 * (mc + Ms(k + 1, j, i)) * nu * (F(k + 1, j, i) - fc) / dz : 0.0;
-    const double fbot = (k >= 1) ? 0.5 * (Ms(k - 1, j, i) + mc) * nu * (fc - F(k - 1, j, i)) / dz : 0.0;
-    tend = tend + (ftop - fbot) / dz;
+    const double ftop =
+        (k + 1 <= nz_f - 1) ? div_rcp(0.5 * (mc + Ms(k + 1, j, i)) * nu * (F(k + 1, j, i) - fc), dz, rdz) : 0.0;
+    const double fbot = (k >= 1) ? div_rcp(0.5 * (Ms(k - 1, j, i) + mc) * nu * (fc - F(k - 1, j, i)), dz, rdz) : 0.0;
+    tend = tend + div_rcp(ftop - fbot, dz, rdz);
   }
   return tend;
 }
@@ -218,27 +222,28 @@ __global__ void k_constk_apply(Grid g, DiffArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nxu = nx + 1, nyv = ny + 1;
   if (i > nx || j > ny) return;
   const double dz = a.dz[0], nu = a.nu;
+  const double rdz = 1.0 / dz;
   if (k < nz && j < ny) {
     auto F = [&](int kk, int jj, int ii) { return ld(a.u, ix3(kk, jj, ii, ny, nxu)); };
     auto Ms = [&](int kk, int jj, int ii) { return ld(g.c1h, kk) * mu_u_face(a.mu, jj, ii, nx) + ld(g.c2h, kk); };
     const size_t c = ix3(k, j, i, ny, nxu);
-    a.u_tend[c] = a.u_tend[c] + constk_point(g, k, j, i, nz, ny, nxu, nu, dz, F, Ms);
+    a.u_tend[c] = a.u_tend[c] + constk_point(g, k, j, i, nz, ny, nxu, nu, dz, rdz, F, Ms);
   }
   if (k < nz && i < nx) {
     auto F = [&](int kk, int jj, int ii) { return ld(a.v, ix3(kk, jj, ii, nyv, nx)); };
     auto Ms = [&](int kk, int jj, int ii) { return ld(g.c1h, kk) * mu_v_face(a.mu, jj, ii, nx, ny) + ld(g.c2h, kk); };
     const size_t c = ix3(k, j, i, nyv, nx);
-    a.v_tend[c] = a.v_tend[c] + constk_point(g, k, j, i, nz, nyv, nx, nu, dz, F, Ms);
+    a.v_tend[c] = a.v_tend[c] + constk_point(g, k, j, i, nz, nyv, nx, nu, dz, rdz, F, Ms);
   }
   if (i < nx && j < ny) {
     auto FW = [&](int kk, int jj, int ii) { return ld(a.w, ix3(kk, jj, ii, ny, nx)); };
     auto MF = [&](int kk, int jj, int ii) { return ld(g.c1f, kk) * ld(a.mu, ix2(jj, ii, nx)) + ld(g.c2f, kk); };
     const size_t c = ix3(k, j, i, ny, nx);
-    a.w_tend[c] = a.w_tend[c] + constk_point(g, k, j, i, nz + 1, ny, nx, nu, dz, FW, MF);
+    a.w_tend[c] = a.w_tend[c] + constk_point(g, k, j, i, nz + 1, ny, nx, nu, dz, rdz, FW, MF);
     if (k < nz) {
       auto FT = [&](int kk, int jj, int ii) { return ld(a.theta, ix3(kk, jj, ii, ny, nx)); };
       auto MH = [&](int kk, int jj, int ii) { return ld(g.c1h, kk) * ld(a.mu, ix2(jj, ii, nx)) + ld(g.c2h, kk); };
-      a.t_tend[c] = a.t_tend[c] + constk_point(g, k, j, i, nz, ny, nx, nu, dz, FT, MH);
+      a.t_tend[c] = a.t_tend[c] + constk_point(g, k, j, i, nz, ny, nx, nu, dz, rdz, FT, MH);
     }
   }
 }

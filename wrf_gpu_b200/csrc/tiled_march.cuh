@@ -279,7 +279,10 @@ __global__ void WG_LIM_BOUNDS k_lim_march(Grid g, LimArgs a, const double *field
     lim_zconst(g, a, k, sm.zc);
     __syncthreads();
     LimTiles t{sm.q[b], sm.qo[b], sm.ru[b], sm.rv[b], sm.mt, sm.zc, sm.fxl, sm.fxa, sm.fyl, sm.fya};
-    lim_face_fluxes<F, DEG>(g, a, t, k, i0, j0);
+    if (__double_as_longlong(a.offset) == 0)
+      lim_face_fluxes<F, DEG, false>(g, a, t, k, i0, j0);
+    else
+      lim_face_fluxes<F, DEG, true>(g, a, t, k, i0, j0);
     __syncthreads();
     if (valid) {
       CellFluxes cf;

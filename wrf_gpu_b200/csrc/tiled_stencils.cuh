@@ -77,8 +77,10 @@ __device__ __forceinline__ void lim_zconst(const Grid &g, const LimArgs &a, int 
 // Low-order upwind (flux_advection.py:614-675) and antidiffusive (high
 // order :678-711 minus low order) fluxes of every x and y face of the tile,
 // one face per thread item, into shared memory.  Edge tiles compute a few
-// harmless extra faces from the periodically wrapped staged values.
-template <typename F, bool DEG>
+// harmless extra faces from the periodically wrapped staged values.  SUB
+// false: the field's offset is +0.0 and the staged values are read as they
+// are (x - 0.0 == x bit for bit).
+template <typename F, bool DEG, bool SUB = true>
 __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a, const LimTiles &t, int k, int i0,
                                                 int j0) {
   using TQ = Tile<3, 3>;
@@ -86,8 +88,14 @@ __device__ __forceinline__ void lim_face_fluxes(const Grid &g, const LimArgs &a,
   using TR = Tile<1, 0>;
   using TV = Tile<0, 1>;
   const double c1 = ld(g.c1h, k), c2 = ld(g.c2h, k);
-  auto Q = [&](int r, int cc) { return t.q[(r + 3) * TQ::W + (cc + 3)] - a.offset; };
-  auto QO = [&](int r, int cc) { return t.qo[(r + 1) * TO::W + (cc + 1)] - a.offset; };
+  auto Q = [&](int r, int cc) {
+    const double x = t.q[(r + 3) * TQ::W + (cc + 3)];
+    return SUB ? x - a.offset : x;
+  };
+  auto QO = [&](int r, int cc) {
+    const double x = t.qo[(r + 1) * TO::W + (cc + 1)];
+    return SUB ? x - a.offset : x;
+  };
   auto MT = [&](int r, int cc) { return t.mt[(r + 1) * TO::W + (cc + 1)]; };
   // cr = vel*dt/dxy/mu_face and mu_face*(dxy/dt)*(...) with the constant
   // divisions done by div_rcp / per-launch constants (same bits).
