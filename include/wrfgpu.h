@@ -310,6 +310,18 @@ int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *params, const wrfg
                                     const double *tend_bar, const double *ru, const double *rv, const double *rom,
                                     double *q_bar, cudaStream_t stream);
 
+/* The full vector-Jacobian product at (q, ru, rv, rom): q_bar (as
+ * wrfgpu_scalar_advection_adjoint) and the velocities' cotangents ru_bar,
+ * rv_bar (nz, ny, nx) and rom_bar (nz+1, ny, nx; zero on the bottom and top
+ * faces), so that <tend_bar, dL> = <q_bar, dq> + <ru_bar, d ru> +
+ * <rv_bar, d rv> + <rom_bar, d rom>, the upwind switches held at their
+ * forward sign (the operator is bilinear in q and the velocities away from
+ * zero velocities).  One launch; any output may be NULL (not computed), not
+ * all four. */
+int wrfgpu_scalar_advection_vjp(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const double *q,
+                                const double *tend_bar, const double *ru, const double *rv, const double *rom,
+                                double *q_bar, double *ru_bar, double *rv_bar, double *rom_bar, cudaStream_t stream);
+
 /* One acoustic small step on its own (the reference's acoustic_substep_core,
  * core/acoustic.py:837-1150: advance_uv, advance_mu_t, advance_w with its
  * Thomas solve, calc_p_rho with smdiv memory), over the evolving work state of

@@ -2,10 +2,11 @@
 
 * ``scalar_advection(q, ru, rv, rom, namelist)`` returns the advective
   tendency of ``q`` (``advect_scalar_flux``, dynamics/flux_advection.py:482-568,
-  doubly periodic) for fixed transport velocities; ``backward`` applies the
-  adjoint kernel (``wrfgpu_scalar_advection_adjoint``) to the incoming
-  gradient, so gradients flow to ``q`` (the velocities are treated as
-  constants: their gradient is not built).
+  doubly periodic); ``backward`` applies the adjoint kernels to the incoming
+  gradient: ``wrfgpu_scalar_advection_adjoint`` when only ``q`` needs one,
+  ``wrfgpu_scalar_advection_vjp`` (one launch) when the transport velocities
+  ``ru``, ``rv``, ``rom`` do too (the operator is bilinear; the upwind
+  switches are held at their forward sign).
 * ``acoustic_substep(work, op)`` / ``acoustic_loop(work, op, nsub)``: one or
   ``nsub`` acoustic small steps (acoustic_substep_core, core/acoustic.py:
   837-1150) of the evolving work state for fixed stage constants, with the
@@ -46,25 +47,34 @@ class ScalarAdvection(torch.autograd.Function):
         q, ru, rv, rom = (t.contiguous() for t in (q, ru, rv, rom))
         tend = torch.empty_like(q)
         op.apply("wrfgpu_scalar_advection", q, ru, rv, rom, tend)
-        ctx.save_for_backward(ru, rv, rom)
+        ctx.save_for_backward(q, ru, rv, rom)
         ctx.op = op
         return tend
 
     @staticmethod
     def backward(ctx, tend_bar):
-        ru, rv, rom = ctx.saved_tensors
-        if any(ctx.needs_input_grad[1:4]):
-            raise NotImplementedError("gradients with respect to the transport velocities are not built")
-        q_bar = torch.empty_like(tend_bar)
-        ctx.op.apply("wrfgpu_scalar_advection_adjoint", tend_bar.contiguous(), ru, rv, rom, q_bar)
-        return q_bar, None, None, None, None
+        q, ru, rv, rom = ctx.saved_tensors
+        tend_bar = tend_bar.contiguous()
+        need = ctx.needs_input_grad[:4]
+        if not need[1] and not need[2] and not need[3]:
+            q_bar = torch.empty_like(tend_bar)
+            ctx.op.apply("wrfgpu_scalar_advection_adjoint", tend_bar, ru, rv, rom, q_bar)
+            return q_bar, None, None, None, None
+        # the cotangents of q and of the velocities in one launch
+        outs = [torch.empty_like(t) if n else None for t, n in zip((q, ru, rv, rom), need)]
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)
+        st = torch.cuda.current_stream(q.device)
+        _capi.check(_capi.load().wrfgpu_scalar_advection_vjp(
+            ctypes.byref(ctx.op.params), ctypes.byref(ctx.op.metrics), ptr(q), ptr(tend_bar), ptr(ru), ptr(rv),
+            ptr(rom), *map(ptr, outs), ctypes.c_void_p(st.cuda_stream)))
+        return (*outs, None)
 
 
 def scalar_advection(q: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: torch.Tensor,
                      namelist: dycore.OperationalNamelist) -> torch.Tensor:
     """Flux-form advective tendency of ``q`` (nz, ny, nx) for transport
     velocities ``ru``, ``rv`` (nz, ny, nx) and ``rom`` (nz+1, ny, nx);
-    differentiable with respect to ``q``."""
+    differentiable with respect to ``q`` and the velocities."""
     return ScalarAdvection.apply(q, ru, rv, rom, _Op(namelist))
 
 

@@ -129,4 +129,99 @@ __global__ void k_scalar_adv_adj(Grid g, AdvOpArgs v, const double *lam, double 
   qbar[ix3(k, j, i, ny, nx)] = acc;
 }
 
+// The full vector-Jacobian product.  tend is bilinear in (q, vel): with the
+// upwind signs frozen each face flux is F_f = vel_f h_f(q), so besides
+// q_bar (as k_scalar_adv_adj)
+//   velbar_f = Fbar_f h_f(q),   h_f = flux5 / flux3 of the face's stencil
+//   (the second-order face value at m = 1 and nz-1),
+//   Fbar_x(i) = rdx (msftx(i) lam(i) - msftx(i-1) lam(i-1)), likewise y,
+//   Fbar_z(m) = rdnw(m) lam(m) - rdnw(m-1) lam(m-1).
+// Index space (nx, ny, nz+1): q_bar, ru_bar, rv_bar at cell (k, j, i) and
+// the west / south face of it for k < nz, rom_bar at w face (k, j, i) (zero
+// at k = 0 and nz, whose fluxes are zero).  Outputs given as NULL are
+// skipped; the shared loads (lam, msftx, the velocities) are made once.
+__global__ void k_scalar_adv_vjp(Grid g, AdvOpArgs v, const double *q, const double *lam, double *q_bar,
+                                 double *ru_bar, double *rv_bar, double *rom_bar) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j >= ny) return;
+  auto Q = [&](int jj, int ii) { return ld(q, ix3(k, wrp(jj, ny), wrp(ii, nx), ny, nx)); };
+  if (k < nz) {
+    double acc = 0.0;
+    {
+      double ml[7];
+#pragma unroll
+      for (int t = -3; t <= 3; ++t) {
+        const int ii = wrp(i + t, nx);
+        ml[t + 3] = ld(g.msftx, ix2(j, ii, nx)) * ld(lam, ix3(k, j, ii, ny, nx));
+      }
+      double vel0 = 0.0;
+#pragma unroll
+      for (int t = -2; t <= 3; ++t) {
+        const double vel = ld(v.ru, ix3(k, j, wrp(i + t, nx), ny, nx));
+        if (t == 0) vel0 = vel;
+        acc += vel * w5(3 - t, sgn(vel)) * (g.rdx * (ml[t + 3] - ml[t + 2]));
+      }
+      if (ru_bar != nullptr)
+        ru_bar[ix3(k, j, i, ny, nx)] =
+            g.rdx * (ml[3] - ml[2]) * flux5(Q(j, i - 3), Q(j, i - 2), Q(j, i - 1), Q(j, i), Q(j, i + 1), Q(j, i + 2), vel0);
+    }
+    {
+      double ml[7];
+#pragma unroll
+      for (int t = -3; t <= 3; ++t) {
+        const int jj = wrp(j + t, ny);
+        ml[t + 3] = ld(g.msftx, ix2(jj, i, nx)) * ld(lam, ix3(k, jj, i, ny, nx));
+      }
+      double vel0 = 0.0;
+#pragma unroll
+      for (int t = -2; t <= 3; ++t) {
+        const double vel = ld(v.rv, ix3(k, wrp(j + t, ny), i, ny, nx));
+        if (t == 0) vel0 = vel;
+        acc += vel * w5(3 - t, sgn(vel)) * (g.rdy * (ml[t + 3] - ml[t + 2]));
+      }
+      if (rv_bar != nullptr)
+        rv_bar[ix3(k, j, i, ny, nx)] =
+            g.rdy * (ml[3] - ml[2]) * flux5(Q(j - 3, i), Q(j - 2, i), Q(j - 1, i), Q(j, i), Q(j + 1, i), Q(j + 2, i), vel0);
+    }
+    if (q_bar != nullptr) {
+      auto Lz = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
+#pragma unroll
+      for (int t = -1; t <= 2; ++t) {
+        const int m = k + t;
+        if (m < 1 || m > nz - 1) continue;
+        const double rom = ld(v.rom, ix3(m, j, i, ny, nx));
+        double wk = 0.0;
+        if (m == 1 || m == nz - 1) {
+          if (t == 0) wk = ld(g.fnm, m);
+          else if (t == 1) wk = ld(g.fnp, m);
+        } else {
+          wk = w3(2 - t, sgn(-rom));
+        }
+        acc += rom * wk * (ld(g.rdnw, m) * Lz(m) - ld(g.rdnw, m - 1) * Lz(m - 1));
+      }
+      q_bar[ix3(k, j, i, ny, nx)] = acc;
+    }
+  }
+  if (rom_bar != nullptr) {
+    double r = 0.0;
+    if (k >= 1 && k <= nz - 1) {
+      auto qc = [&](int kk) { return ld(q, ix3(kk, j, i, ny, nx)); };
+      auto L = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
+      const double rom = ld(v.rom, ix3(k, j, i, ny, nx));
+      double h;
+      if (k == 1 || k == nz - 1) {
+        h = ld(g.fnm, k) * qc(k) + ld(g.fnp, k) * qc(k - 1);
+      } else {
+        const double s = sgn(-rom);
+        h = w3(0, s) * qc(k - 2) + w3(1, s) * qc(k - 1) + w3(2, s) * qc(k) + w3(3, s) * qc(k + 1);
+      }
+      r = (ld(g.rdnw, k) * L(k) - ld(g.rdnw, k - 1) * L(k - 1)) * h;
+    }
+    rom_bar[ix3(k, j, i, ny, nx)] = r;
+  }
+}
+
 }  // namespace wg

@@ -1838,6 +1838,23 @@ extern "C" int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *p, cons
   return WRFGPU_OK;
 }
 
+extern "C" int wrfgpu_scalar_advection_vjp(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
+                                           const double *tend_bar, const double *ru, const double *rv,
+                                           const double *rom, double *q_bar, double *ru_bar, double *rv_bar,
+                                           double *rom_bar, cudaStream_t stream) {
+  int rc = adv_op_check(p, m, q, ru, rv, rom, tend_bar);
+  if (rc) return rc;
+  if (q_bar == nullptr && ru_bar == nullptr && rv_bar == nullptr && rom_bar == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "q_bar, ru_bar, rv_bar and rom_bar are all NULL");
+  Grid g = make_grid(*p, *m, nullptr);
+  AdvOpArgs a{ru, rv, rom};
+  const int nzl = p->nz + (rom_bar != nullptr ? 1 : 0);
+  k_scalar_adv_vjp<<<grd(p->nx, p->ny, nzl), blk2(), 0, stream>>>(g, a, q, tend_bar, q_bar, ru_bar, rv_bar, rom_bar);
+  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_vjp launch failed");
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Nest coupling: parent -> child interpolation and boundary leaves, child ->
 // parent feedback (nesting.cuh).
