@@ -1,11 +1,12 @@
 // Flux-form scalar advection operator (h5/v3, periodic) and its hand-written
-// adjoint with respect to the advected field.
+// adjoints with respect to the advected field and the transport velocities.
 //
 // For fixed transport velocities (ru, rv at the cells' west / south faces,
 // rom at the w faces) the tendency tend = L(ru, rv, rom) q of
 // flux_advection.py:482-568 is linear in q: the upwind switch sign(vel)
-// depends on the velocity only.  k_scalar_adv_op applies L; k_scalar_adv_adj
-// applies its transpose L^T to a tendency-space vector lambda:
+// depends on the velocity only.  k_scalar_adv_op applies L; k_scalar_adv_vjp
+// applies its transpose L^T to a tendency-space vector lambda (and forms the
+// velocities' cotangents, below):
 //
 //   face flux   F_f = vel_f * sum_m w_m(sign vel_f) q(stencil_f, m)
 //   tendency    tend(c) = -msftx rdx (Fx(c+1) - Fx(c)) - msftx rdy (Fy(c+1) - Fy(c))
@@ -21,6 +22,7 @@
 #pragma once
 #include "dycore_common.cuh"
 #include "stage_kernels.cuh"
+#include "tiled_stencils.cuh"
 
 namespace wg {
 
@@ -54,158 +56,135 @@ __global__ void k_scalar_adv_op(Grid g, AdvOpArgs v, const double *q, double *te
   tend[ix3(k, j, i, ny, nx)] = t - ld(g.rdnw, k) * (v1 - v0);
 }
 
-// flux5 weight of stencil position m (0..5 = q-3..q+2) for upwind sign s.
+// flux5 weight of stencil position m (0..5 = q-3..q+2) for upwind sign s,
+// and the flux3 weight of position m (0..3 = q(m-2)..q(m+1)) for
+// s' = sign(-vel).  s takes the values -1, 0, 1 only, so every weight is one
+// of three constants folded at compile time (the same quotients a runtime
+// division gives); the loops that call these unroll m.
+__host__ __device__ constexpr double w5c(int m, double s) {
+  return m == 0 ? (1.0 + s) / 60.0
+       : m == 1 ? (-8.0 - 5.0 * s) / 60.0
+       : m == 2 ? (37.0 + 10.0 * s) / 60.0
+       : m == 3 ? (37.0 - 10.0 * s) / 60.0
+       : m == 4 ? (-8.0 + 5.0 * s) / 60.0
+                : (1.0 - s) / 60.0;
+}
+__host__ __device__ constexpr double w3c(int m, double s) {
+  return m == 0 ? (-1.0 - s) / 12.0 : m == 1 ? (7.0 + 3.0 * s) / 12.0 : m == 2 ? (7.0 - 3.0 * s) / 12.0 : (-1.0 + s) / 12.0;
+}
+template <int M>
+__device__ __forceinline__ double w5(double s) {
+  constexpr double p = w5c(M, 1.0), z = w5c(M, 0.0), n = w5c(M, -1.0);
+  return s > 0.0 ? p : (s < 0.0 ? n : z);
+}
 __device__ __forceinline__ double w5(int m, double s) {
   switch (m) {
-    case 0: return (1.0 + s) / 60.0;
-    case 1: return (-8.0 - 5.0 * s) / 60.0;
-    case 2: return (37.0 + 10.0 * s) / 60.0;
-    case 3: return (37.0 - 10.0 * s) / 60.0;
-    case 4: return (-8.0 + 5.0 * s) / 60.0;
-    default: return (1.0 - s) / 60.0;
+    case 0: return w5<0>(s);
+    case 1: return w5<1>(s);
+    case 2: return w5<2>(s);
+    case 3: return w5<3>(s);
+    case 4: return w5<4>(s);
+    default: return w5<5>(s);
   }
 }
-// flux3 weight of stencil position m (0..3 = q(m-2)..q(m+1)) for s' = sign(-vel).
+template <int M>
+__device__ __forceinline__ double w3(double s) {
+  constexpr double p = w3c(M, 1.0), z = w3c(M, 0.0), n = w3c(M, -1.0);
+  return s > 0.0 ? p : (s < 0.0 ? n : z);
+}
 __device__ __forceinline__ double w3(int m, double s) {
   switch (m) {
-    case 0: return (-1.0 - s) / 12.0;
-    case 1: return (7.0 + 3.0 * s) / 12.0;
-    case 2: return (7.0 - 3.0 * s) / 12.0;
-    default: return (-1.0 + s) / 12.0;
+    case 0: return w3<0>(s);
+    case 1: return w3<1>(s);
+    case 2: return w3<2>(s);
+    default: return w3<3>(s);
   }
-}
-
-__global__ void k_scalar_adv_adj(Grid g, AdvOpArgs v, const double *lam, double *qbar) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  if (i >= nx || j >= ny) return;
-  double acc = 0.0;
-  // x faces ii = i-2 .. i+3 (west faces of cells ii); this cell is stencil
-  // position 3 - t of face ii = i + t.  ml[t+3] = msftx * lambda at cell i+t.
-  {
-    double ml[7];
-#pragma unroll
-    for (int t = -3; t <= 3; ++t) {
-      const int ii = wrp(i + t, nx);
-      ml[t + 3] = ld(g.msftx, ix2(j, ii, nx)) * ld(lam, ix3(k, j, ii, ny, nx));
-    }
-#pragma unroll
-    for (int t = -2; t <= 3; ++t) {
-      const double vel = ld(v.ru, ix3(k, j, wrp(i + t, nx), ny, nx));
-      acc += vel * w5(3 - t, sgn(vel)) * (g.rdx * (ml[t + 3] - ml[t + 2]));
-    }
-  }
-  {
-    double ml[7];
-#pragma unroll
-    for (int t = -3; t <= 3; ++t) {
-      const int jj = wrp(j + t, ny);
-      ml[t + 3] = ld(g.msftx, ix2(jj, i, nx)) * ld(lam, ix3(k, jj, i, ny, nx));
-    }
-#pragma unroll
-    for (int t = -2; t <= 3; ++t) {
-      const double vel = ld(v.rv, ix3(k, wrp(j + t, ny), i, ny, nx));
-      acc += vel * w5(3 - t, sgn(vel)) * (g.rdy * (ml[t + 3] - ml[t + 2]));
-    }
-  }
-  // z faces m = 1 .. nz-1 whose stencil holds level k
-  auto Lz = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
-#pragma unroll
-  for (int t = -1; t <= 2; ++t) {
-    const int m = k + t;
-    if (m < 1 || m > nz - 1) continue;
-    const double rom = ld(v.rom, ix3(m, j, i, ny, nx));
-    double wk = 0.0;
-    if (m == 1 || m == nz - 1) {
-      if (t == 0) wk = ld(g.fnm, m);
-      else if (t == 1) wk = ld(g.fnp, m);
-    } else {
-      wk = w3(2 - t, sgn(-rom));  // stencil q(m-2) .. q(m+1): level k is position 2 - t
-    }
-    acc += rom * wk * (ld(g.rdnw, m) * Lz(m) - ld(g.rdnw, m - 1) * Lz(m - 1));
-  }
-  qbar[ix3(k, j, i, ny, nx)] = acc;
 }
 
 // The full vector-Jacobian product.  tend is bilinear in (q, vel): with the
-// upwind signs frozen each face flux is F_f = vel_f h_f(q), so besides
-// q_bar (as k_scalar_adv_adj)
-//   velbar_f = Fbar_f h_f(q),   h_f = flux5 / flux3 of the face's stencil
-//   (the second-order face value at m = 1 and nz-1),
+// upwind signs frozen each face flux is F_f = vel_f h_f(q), so
 //   Fbar_x(i) = rdx (msftx(i) lam(i) - msftx(i-1) lam(i-1)), likewise y,
-//   Fbar_z(m) = rdnw(m) lam(m) - rdnw(m-1) lam(m-1).
-// Index space (nx, ny, nz+1): q_bar, ru_bar, rv_bar at cell (k, j, i) and
-// the west / south face of it for k < nz, rom_bar at w face (k, j, i) (zero
-// at k = 0 and nz, whose fluxes are zero).  Outputs given as NULL are
-// skipped; the shared loads (lam, msftx, the velocities) are made once.
-__global__ void k_scalar_adv_vjp(Grid g, AdvOpArgs v, const double *q, const double *lam, double *q_bar,
-                                 double *ru_bar, double *rv_bar, double *rom_bar) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+//   Fbar_z(m) = rdnw(m) lam(m) - rdnw(m-1) lam(m-1),
+//   q_bar(c)  = sum over the faces whose stencil holds c of
+//               vel_f w_m(sign vel_f) Fbar_f            (a gather, no atomics)
+//   velbar_f  = Fbar_f h_f(q),   h_f = flux5 / flux3 of the face's stencil
+//               (the second-order face value at m = 1 and nz-1).
+// One 32 x 8 block per tile and level: the level's msftx*lam, ru, rv (and,
+// for the velocity cotangents, q) plane tiles are staged in shared memory
+// with their periodic halos, the vertical stencils read the column.  q_bar,
+// ru_bar, rv_bar at cell (k, j, i) and its west / south face for k < nz,
+// rom_bar at w face (k, j, i) (zero at k = 0 and nz, whose fluxes are zero).
+// Outputs given as NULL are skipped.
+__global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs v, const double *q,
+                                                               const double *lam, double *q_bar, double *ru_bar,
+                                                               double *rv_bar, double *rom_bar) {
+  using TM = Tile<3, 3>;  // msftx * lam
+  using TU = Tile<3, 0>;  // ru: west faces of cells i0-3 .. i0+34
+  using TV = Tile<0, 3>;  // rv: south faces of rows j0-3 .. j0+10
+  __shared__ double sml[TM::N], sru[TU::N], srv[TV::N], sq[TM::N];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  if (i >= nx || j >= ny) return;
-  auto Q = [&](int jj, int ii) { return ld(q, ix3(k, wrp(jj, ny), wrp(ii, nx), ny, nx)); };
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY, k = blockIdx.z;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool valid = i < nx && j < ny;
   if (k < nz) {
-    double acc = 0.0;
-    {
-      double ml[7];
-#pragma unroll
-      for (int t = -3; t <= 3; ++t) {
-        const int ii = wrp(i + t, nx);
-        ml[t + 3] = ld(g.msftx, ix2(j, ii, nx)) * ld(lam, ix3(k, j, ii, ny, nx));
-      }
-      double vel0 = 0.0;
+    const size_t kp = (size_t)k * ny * nx;
+    for (int e = ty * TSX + tx; e < TM::N; e += TSX * TSY) {
+      const int r = e / TM::W, c = e - r * TM::W;
+      const int jj = wrp(j0 - 3 + r, ny), ii = wrp(i0 - 3 + c, nx);
+      sml[e] = ld(g.msftx, ix2(jj, ii, nx)) * ld(lam, kp + ix2(jj, ii, nx));
+    }
+    load_tile<3, 0>(sru, v.ru + kp, nx, i0, j0, nx, ny, 0.0);
+    load_tile<0, 3>(srv, v.rv + kp, nx, i0, j0, nx, ny, 0.0);
+    if (ru_bar != nullptr || rv_bar != nullptr) load_tile<3, 3>(sq, q + kp, nx, i0, j0, nx, ny, 0.0);
+    __syncthreads();
+    if (valid) {
+      auto ML = [&](int r, int cc) { return sml[(r + 3) * TM::W + (cc + 3)]; };
+      auto RU = [&](int cc) { return sru[ty * TU::W + (cc + 3)]; };
+      auto RV = [&](int r) { return srv[(r + 3) * TV::W + tx]; };
+      auto Q = [&](int r, int cc) { return sq[(r + 3) * TM::W + (cc + 3)]; };
+      double acc = 0.0;
+      // x faces of cells i-2 .. i+3 whose stencils hold this cell (position 3 - t)
 #pragma unroll
       for (int t = -2; t <= 3; ++t) {
-        const double vel = ld(v.ru, ix3(k, j, wrp(i + t, nx), ny, nx));
-        if (t == 0) vel0 = vel;
-        acc += vel * w5(3 - t, sgn(vel)) * (g.rdx * (ml[t + 3] - ml[t + 2]));
+        const double vel = RU(tx + t);
+        acc += vel * w5(3 - t, sgn(vel)) * (g.rdx * (ML(ty, tx + t) - ML(ty, tx + t - 1)));
       }
       if (ru_bar != nullptr)
-        ru_bar[ix3(k, j, i, ny, nx)] =
-            g.rdx * (ml[3] - ml[2]) * flux5(Q(j, i - 3), Q(j, i - 2), Q(j, i - 1), Q(j, i), Q(j, i + 1), Q(j, i + 2), vel0);
-    }
-    {
-      double ml[7];
-#pragma unroll
-      for (int t = -3; t <= 3; ++t) {
-        const int jj = wrp(j + t, ny);
-        ml[t + 3] = ld(g.msftx, ix2(jj, i, nx)) * ld(lam, ix3(k, jj, i, ny, nx));
-      }
-      double vel0 = 0.0;
+        ru_bar[kp + ix2(j, i, nx)] = g.rdx * (ML(ty, tx) - ML(ty, tx - 1)) *
+                                     flux5(Q(ty, tx - 3), Q(ty, tx - 2), Q(ty, tx - 1), Q(ty, tx), Q(ty, tx + 1),
+                                           Q(ty, tx + 2), RU(tx));
 #pragma unroll
       for (int t = -2; t <= 3; ++t) {
-        const double vel = ld(v.rv, ix3(k, wrp(j + t, ny), i, ny, nx));
-        if (t == 0) vel0 = vel;
-        acc += vel * w5(3 - t, sgn(vel)) * (g.rdy * (ml[t + 3] - ml[t + 2]));
+        const double vel = RV(ty + t);
+        acc += vel * w5(3 - t, sgn(vel)) * (g.rdy * (ML(ty + t, tx) - ML(ty + t - 1, tx)));
       }
       if (rv_bar != nullptr)
-        rv_bar[ix3(k, j, i, ny, nx)] =
-            g.rdy * (ml[3] - ml[2]) * flux5(Q(j - 3, i), Q(j - 2, i), Q(j - 1, i), Q(j, i), Q(j + 1, i), Q(j + 2, i), vel0);
-    }
-    if (q_bar != nullptr) {
-      auto Lz = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
+        rv_bar[kp + ix2(j, i, nx)] = g.rdy * (ML(ty, tx) - ML(ty - 1, tx)) *
+                                     flux5(Q(ty - 3, tx), Q(ty - 2, tx), Q(ty - 1, tx), Q(ty, tx), Q(ty + 1, tx),
+                                           Q(ty + 2, tx), RV(ty));
+      if (q_bar != nullptr) {
+        // z faces m = k-1 .. k+2 whose stencils hold level k
+        auto Lz = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
 #pragma unroll
-      for (int t = -1; t <= 2; ++t) {
-        const int m = k + t;
-        if (m < 1 || m > nz - 1) continue;
-        const double rom = ld(v.rom, ix3(m, j, i, ny, nx));
-        double wk = 0.0;
-        if (m == 1 || m == nz - 1) {
-          if (t == 0) wk = ld(g.fnm, m);
-          else if (t == 1) wk = ld(g.fnp, m);
-        } else {
-          wk = w3(2 - t, sgn(-rom));
+        for (int t = -1; t <= 2; ++t) {
+          const int m = k + t;
+          if (m < 1 || m > nz - 1) continue;
+          const double rom = ld(v.rom, ix3(m, j, i, ny, nx));
+          double wk = 0.0;
+          if (m == 1 || m == nz - 1) {
+            if (t == 0) wk = ld(g.fnm, m);
+            else if (t == 1) wk = ld(g.fnp, m);
+          } else {
+            wk = w3(2 - t, sgn(-rom));  // stencil q(m-2) .. q(m+1): level k is position 2 - t
+          }
+          acc += rom * wk * (ld(g.rdnw, m) * Lz(m) - ld(g.rdnw, m - 1) * Lz(m - 1));
         }
-        acc += rom * wk * (ld(g.rdnw, m) * Lz(m) - ld(g.rdnw, m - 1) * Lz(m - 1));
+        q_bar[kp + ix2(j, i, nx)] = acc;
       }
-      q_bar[ix3(k, j, i, ny, nx)] = acc;
     }
   }
-  if (rom_bar != nullptr) {
+  if (rom_bar != nullptr && valid) {
     double r = 0.0;
     if (k >= 1 && k <= nz - 1) {
       auto qc = [&](int kk) { return ld(q, ix3(kk, j, i, ny, nx)); };

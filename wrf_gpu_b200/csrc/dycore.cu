@@ -1832,8 +1832,10 @@ extern "C" int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *p, cons
   if (rc) return rc;
   Grid g = make_grid(*p, *m, nullptr);
   AdvOpArgs a{ru, rv, rom};
-  k_scalar_adv_adj<<<grd(p->nx, p->ny, p->nz), blk2(), 0, stream>>>(g, a, tend_bar, q_bar);
-  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_adj launch failed");
+  // the VJP kernel with only the field's cotangent (q is not read)
+  k_scalar_adv_vjp<<<tgrd(p->nx, p->ny, p->nz), tblk(), 0, stream>>>(g, a, tend_bar, tend_bar, q_bar, nullptr,
+                                                                     nullptr, nullptr);
+  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_vjp launch failed");
   g_last_error.clear();
   return WRFGPU_OK;
 }
@@ -1849,7 +1851,8 @@ extern "C" int wrfgpu_scalar_advection_vjp(const wrfgpu_step_params *p, const wr
   Grid g = make_grid(*p, *m, nullptr);
   AdvOpArgs a{ru, rv, rom};
   const int nzl = p->nz + (rom_bar != nullptr ? 1 : 0);
-  k_scalar_adv_vjp<<<grd(p->nx, p->ny, nzl), blk2(), 0, stream>>>(g, a, q, tend_bar, q_bar, ru_bar, rv_bar, rom_bar);
+  k_scalar_adv_vjp<<<tgrd(p->nx, p->ny, nzl), tblk(), 0, stream>>>(g, a, q, tend_bar, q_bar, ru_bar, rv_bar,
+                                                                     rom_bar);
   if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_vjp launch failed");
   g_last_error.clear();
   return WRFGPU_OK;
