@@ -131,12 +131,15 @@ __global__ void WG_ADJCOL_BOUNDS k_adj_column(Grid g, AdjColArgs q) {
       const double sttr = fabs(ttr) > 1.0e-6 ? ttr : 1.0e-6;
       const double mu_term = c1 * (muts - mut);
       const double den = safe * sttr;
+      // the sweep is serial per column: one reciprocal per divisor instead
+      // of six divisions on its dependency chain
+      const double rsafe = 1.0 / safe, rden = 1.0 / den;
       const double thw = ld(q.x1.theta_w, c), al = ld(q.x1.al, c);
-      const double g_mu_term = -(c2a * alt * t1 / den) * g_pp - (alt / safe) * g_al;
-      const double g_safe = -(c2a * alt * (thw - mu_term * t1) / (safe * den)) * g_pp - (al / safe) * g_al;
+      const double g_mu_term = -(c2a * alt * t1 * rden) * g_pp - (alt * rsafe) * g_al;
+      const double g_safe = -(c2a * alt * (thw - mu_term * t1) * (rsafe * rden)) * g_pp - (al * rsafe) * g_al;
       g_muts += c1 * g_mu_term + (fabs(mass) > 1.0e-12 ? c1 * g_safe : 0.0);
-      gal = ld(g.rdnw, f) * g_al / safe;  // al(f) = ... - rdnw (ph'(f+1) - ph'(f)) / safe
-      s_thw[c] = ld(q.co.theta_w, c) + (c2a * alt / den) * g_pp;
+      gal = ld(g.rdnw, f) * g_al * rsafe;  // al(f) = ... - rdnw (ph'(f+1) - ph'(f)) / safe
+      s_thw[c] = ld(q.co.theta_w, c) + (c2a * alt * rden) * g_pp;
     }
     const size_t c = M(f);
     s_ww[c] = ld(q.co.ww, c);
@@ -146,9 +149,10 @@ __global__ void WG_ADJCOL_BOUNDS k_adj_column(Grid g, AdjColArgs q) {
       // ph finish: ph'(f) = rhs(f) + K ws(f) / (c1f muts + c2f)
       const double g_phn = ld(q.co.ph, c) - gal_prev + gal;
       const double mfs = ld(g.c1f, f) * muts + ld(g.c2f, f);
+      const double rmfs = 1.0 / mfs;
       s_rhs[c] = g_phn;
-      double g_ws = ld(q.co.w, c) + (K / mfs) * g_phn;
-      g_muts += -(K * ld(q.x1.w, c) * ld(g.c1f, f) / (mfs * mfs)) * g_phn;
+      double g_ws = ld(q.co.w, c) + (K * rmfs) * g_phn;
+      g_muts += -(K * ld(q.x1.w, c) * ld(g.c1f, f) * (rmfs * rmfs)) * g_phn;
       if (do_damp) {  // ws_out = (ws - dampwt mf w_save) / (1 + dampwt)
         const double hk = div_rcp(ld(q.pt1, c), G, RG);
         const double sv = sin(over_zdamp(0.5 * 3.141592653589793 * (hk - hbot), q.col));
@@ -190,11 +194,12 @@ __global__ void WG_ADJCOL_BOUNDS k_adj_column(Grid g, AdjColArgs q) {
     const double c1 = ld(g.c1h, k);
     const double mass_h = c1 * muts + ld(g.c2h, k);
     const double t1 = T1(k);
-    const double gn = gt2a / (mass_h * (T0 + t1));
+    const double rd = 1.0 / (mass_h * (T0 + t1));
+    const double gn = gt2a * rd;
     const double gthw = s_thw[c] + 0.5 * eps_p * gn;
     q.ci.t2ave[c] = 0.5 * eps_m * gn;
     g_muave += c1 * T0 * gn;
-    g_muts += -(ld(q.x1.t2ave, c) / mass_h) * c1 * gt2a;
+    g_muts += -(ld(q.x1.t2ave, c) * (T0 + t1) * rd) * c1 * gt2a;  // t2ave / mass_h
     // theta: thw' = thw + msfty dts t_tend - dts msfty (hdiv + rdnw (wdtn(k+1) - wdtn(k)))
     q.ci.theta_w[c] = gthw;
     const double gtend = active ? -dts * msfty * gthw : 0.0;  // a frozen column keeps its theta
@@ -212,6 +217,7 @@ __global__ void WG_ADJCOL_BOUNDS k_adj_column(Grid g, AdjColArgs q) {
   double B_mid = 0.0;                       // buoyancy cotangent of level m
   double D_hi = 0.0;                        // wd cotangent of level m+1 (from face m+2)
   double gt2a_top = 0.0;
+  double coef_lo = 0.0;  // coef(m) of the next (lower) face, carried down
   for (int m = nz; m >= 1; --m) {
     const size_t c = M(m);
     // Thomas forward elimination wf(m) = (wn(m) - a(m) wf(m-1)) alpha(m), reversed
@@ -227,7 +233,8 @@ __global__ void WG_ADJCOL_BOUNDS k_adj_column(Grid g, AdjColArgs q) {
     if (m <= nz - 1) {  // explicit w: wn = w + dts rw_tend + tA(rhs, ph) + tB(buoy, muave)
       W_mid = gwn;
       const double Q = minv * ld(q.cqw, c) * (c05dg * ld(g.rdn, m)) * gwn;
-      const double cf = coef(m), cm = coef(m - 1);
+      const double cf = (m == nz - 1) ? coef(m) : coef_lo, cm = coef(m - 1);
+      coef_lo = cm;
       R_hi += Q * cf * eps_p;
       R_mid -= Q * cf * eps_p + Q * cm * eps_p;
       R_lo += Q * cm * eps_p;
