@@ -322,6 +322,26 @@ int wrfgpu_scalar_advection_vjp(const wrfgpu_step_params *params, const wrfgpu_m
                                 const double *tend_bar, const double *ru, const double *rv, const double *rom,
                                 double *q_bar, double *ru_bar, double *rv_bar, double *rom_bar, cudaStream_t stream);
 
+/* The same flux-form operator with its map-factor weights given: tend =
+ * -hfac rdx (Fx(i+1) - Fx(i)) - hfac rdy (Fy(j+1) - Fy(j)) + vfac (-rdnw
+ * (Fz(k+1) - Fz(k))) for a field q (nz, ny, nx) doubly periodic on its own
+ * extent, hfac and vfac (ny, nx).  hfac NULL is metrics->msftx and vfac NULL
+ * is 1 (wrfgpu_scalar_advection).  The periodic momentum advection is this
+ * operator on the core faces with face-averaged transport velocities:
+ * advect_u_flux (dynamics/flux_advection.py:1131-1202) with hfac = msfux and
+ * vfac NULL, advect_v_flux (:1205-1274) with hfac = msfvy and vfac = msfvy /
+ * msfvx, the averages and the wrap face formed by the caller. */
+int wrfgpu_flux_advection(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const double *q,
+                          const double *ru, const double *rv, const double *rom, const double *hfac,
+                          const double *vfac, double *tend, cudaStream_t stream);
+
+/* Its vector-Jacobian product (as wrfgpu_scalar_advection_vjp, with the same
+ * hfac / vfac); q may be NULL when only q_bar is asked for. */
+int wrfgpu_flux_advection_vjp(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const double *q,
+                              const double *tend_bar, const double *ru, const double *rv, const double *rom,
+                              const double *hfac, const double *vfac, double *q_bar, double *ru_bar,
+                              double *rv_bar, double *rom_bar, cudaStream_t stream);
+
 /* One acoustic small step on its own (the reference's acoustic_substep_core,
  * core/acoustic.py:837-1150: advance_uv, advance_mu_t, advance_w with its
  * Thomas solve, calc_p_rho with smdiv memory), over the evolving work state of

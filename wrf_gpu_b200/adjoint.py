@@ -2,11 +2,12 @@
 
 * ``scalar_advection(q, ru, rv, rom, namelist)`` returns the advective
   tendency of ``q`` (``advect_scalar_flux``, dynamics/flux_advection.py:482-568,
-  doubly periodic); ``backward`` applies the adjoint kernels to the incoming
-  gradient: ``wrfgpu_scalar_advection_adjoint`` when only ``q`` needs one,
-  ``wrfgpu_scalar_advection_vjp`` (one launch) when the transport velocities
-  ``ru``, ``rv``, ``rom`` do too (the operator is bilinear; the upwind
-  switches are held at their forward sign).
+  doubly periodic), ``advect_u`` / ``advect_v`` those of the momentum
+  components (``advect_u_flux`` / ``advect_v_flux``, :1131-1274, periodic);
+  ``backward`` applies the hand-written VJP kernel
+  (``wrfgpu_flux_advection_vjp``, one launch) for the advected field and the
+  transport velocities ``ru``, ``rv``, ``rom`` (the operator is bilinear; the
+  upwind switches are held at their forward sign).
 * ``acoustic_substep(work, op)`` / ``acoustic_loop(work, op, nsub)``: one or
   ``nsub`` acoustic small steps (acoustic_substep_core, core/acoustic.py:
   837-1150) of the evolving work state for fixed stage constants, with the
@@ -41,33 +42,39 @@ class _Op:
                                           ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
 
 
-class ScalarAdvection(torch.autograd.Function):
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr() if t is not None else None)
+
+
+class FluxAdvection(torch.autograd.Function):
+    """The flux-form advection operator ``wrfgpu_flux_advection`` with its
+    map-factor weights ``hfac`` / ``vfac`` (constants, not differentiated)."""
+
     @staticmethod
-    def forward(ctx, q, ru, rv, rom, op: _Op):
+    def forward(ctx, q, ru, rv, rom, op: _Op, hfac, vfac):
         q, ru, rv, rom = (t.contiguous() for t in (q, ru, rv, rom))
         tend = torch.empty_like(q)
-        op.apply("wrfgpu_scalar_advection", q, ru, rv, rom, tend)
+        st = torch.cuda.current_stream(q.device)
+        _capi.check(_capi.load().wrfgpu_flux_advection(
+            ctypes.byref(op.params), ctypes.byref(op.metrics), _ptr(q), _ptr(ru), _ptr(rv), _ptr(rom), _ptr(hfac),
+            _ptr(vfac), _ptr(tend), ctypes.c_void_p(st.cuda_stream)))
         ctx.save_for_backward(q, ru, rv, rom)
-        ctx.op = op
+        ctx.op, ctx.hfac, ctx.vfac = op, hfac, vfac
         return tend
 
     @staticmethod
     def backward(ctx, tend_bar):
         q, ru, rv, rom = ctx.saved_tensors
-        tend_bar = tend_bar.contiguous()
         need = ctx.needs_input_grad[:4]
-        if not need[1] and not need[2] and not need[3]:
-            q_bar = torch.empty_like(tend_bar)
-            ctx.op.apply("wrfgpu_scalar_advection_adjoint", tend_bar, ru, rv, rom, q_bar)
-            return q_bar, None, None, None, None
-        # the cotangents of q and of the velocities in one launch
         outs = [torch.empty_like(t) if n else None for t, n in zip((q, ru, rv, rom), need)]
-        ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)
-        st = torch.cuda.current_stream(q.device)
-        _capi.check(_capi.load().wrfgpu_scalar_advection_vjp(
-            ctypes.byref(ctx.op.params), ctypes.byref(ctx.op.metrics), ptr(q), ptr(tend_bar), ptr(ru), ptr(rv),
-            ptr(rom), *map(ptr, outs), ctypes.c_void_p(st.cuda_stream)))
-        return (*outs, None)
+        if any(o is not None for o in outs):
+            # the field's and the velocities' cotangents in one launch
+            st = torch.cuda.current_stream(q.device)
+            _capi.check(_capi.load().wrfgpu_flux_advection_vjp(
+                ctypes.byref(ctx.op.params), ctypes.byref(ctx.op.metrics), _ptr(q), _ptr(tend_bar.contiguous()),
+                _ptr(ru), _ptr(rv), _ptr(rom), _ptr(ctx.hfac), _ptr(ctx.vfac), *map(_ptr, outs),
+                ctypes.c_void_p(st.cuda_stream)))
+        return (*outs, None, None, None)
 
 
 def scalar_advection(q: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: torch.Tensor,
@@ -75,7 +82,41 @@ def scalar_advection(q: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: t
     """Flux-form advective tendency of ``q`` (nz, ny, nx) for transport
     velocities ``ru``, ``rv`` (nz, ny, nx) and ``rom`` (nz+1, ny, nx);
     differentiable with respect to ``q`` and the velocities."""
-    return ScalarAdvection.apply(q, ru, rv, rom, _Op(namelist))
+    return FluxAdvection.apply(q, ru, rv, rom, _Op(namelist), None, None)
+
+
+def advect_u(u: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: torch.Tensor,
+             namelist: dycore.OperationalNamelist) -> torch.Tensor:
+    """advect_u_flux (dynamics/flux_advection.py:1131-1202), doubly periodic:
+    the advective tendency of u (nz, ny, nx+1) for the transport velocities
+    ru, rv (nz, ny, nx) and rom (nz+1, ny, nx) -- the operator on u's core
+    faces with the velocities averaged to them and the map factor msfux; the
+    wrap face repeats face 0.  Differentiable with respect to u (its wrap
+    face does not enter) and the velocities."""
+    m = namelist.metrics
+    nx = ru.shape[-1]
+    velx = 0.5 * (ru + torch.roll(ru, 1, -1))
+    vely = 0.5 * (rv + torch.roll(rv, 1, -1))
+    velz = 0.5 * (rom + torch.roll(rom, 1, -1))
+    tend = FluxAdvection.apply(u[..., :nx], velx, vely, velz, _Op(namelist), m.msfux[:, :nx].contiguous(), None)
+    return torch.cat((tend, tend[:, :, :1]), dim=2)
+
+
+def advect_v(v: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: torch.Tensor,
+             namelist: dycore.OperationalNamelist) -> torch.Tensor:
+    """advect_v_flux (dynamics/flux_advection.py:1205-1274), doubly periodic:
+    the advective tendency of v (nz, ny+1, nx) -- the operator on v's core
+    faces with the velocities averaged to them, the map factor msfvy and the
+    vertical term scaled by msfvy / msfvx; the wrap row repeats row 0."""
+    m = namelist.metrics
+    ny = rv.shape[-2]
+    velx = 0.5 * (ru + torch.roll(ru, 1, -2))
+    vely = 0.5 * (rv + torch.roll(rv, 1, -2))
+    velz = 0.5 * (rom + torch.roll(rom, 1, -2))
+    hfac = m.msfvy[:ny].contiguous()
+    vfac = (m.msfvy[:ny] / m.msfvx[:ny]).contiguous()
+    tend = FluxAdvection.apply(v[:, :ny, :], velx, vely, velz, _Op(namelist), hfac, vfac)
+    return torch.cat((tend, tend[:, :1, :]), dim=1)
 
 
 class AcousticOp:

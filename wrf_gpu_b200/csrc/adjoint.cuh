@@ -28,6 +28,10 @@ namespace wg {
 
 struct AdvOpArgs {
   const double *ru, *rv, *rom;  // (nz, ny, nx), (nz, ny, nx), (nz+1, ny, nx)
+  // (ny, nx) factors of the horizontal and the vertical flux divergence: the
+  // scalar's msftx and 1 (vfac NULL); msfux and 1 for u's core faces;
+  // msfvy and msfvy / msfvx for v's (flux_advection.py:1131-1274)
+  const double *hfac, *vfac;
 };
 
 __global__ void k_scalar_adv_op(Grid g, AdvOpArgs v, const double *q, double *tend) {
@@ -47,13 +51,16 @@ __global__ void k_scalar_adv_op(Grid g, AdvOpArgs v, const double *q, double *te
     return hflux5<double>(vel, Q(k, jj - 3, i), Q(k, jj - 2, i), Q(k, jj - 1, i), Q(k, jj, i), Q(k, jj + 1, i),
                           Q(k, jj + 2, i));
   };
-  const double msftx = ld(g.msftx, ix2(j, i, nx));
-  double t = -msftx * g.rdx * (fx(i + 1) - fx(i));
-  t = t - msftx * g.rdy * (fy(j + 1) - fy(j));
+  const double hf = ld(v.hfac, ix2(j, i, nx));
+  double t = -hf * g.rdx * (fx(i + 1) - fx(i));
+  t = t - hf * g.rdy * (fy(j + 1) - fy(j));
   auto qc = [&](int kk) { return ld(q, ix3(kk, j, i, ny, nx)); };
   const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, ld(v.rom, ix3(k + 1, j, i, ny, nx)), qc) : 0.0;
   const double v0 = (k >= 1) ? vflux3_at(g, k, ld(v.rom, ix3(k, j, i, ny, nx)), qc) : 0.0;
-  tend[ix3(k, j, i, ny, nx)] = t - ld(g.rdnw, k) * (v1 - v0);
+  if (v.vfac == nullptr)
+    tend[ix3(k, j, i, ny, nx)] = t - ld(g.rdnw, k) * (v1 - v0);
+  else
+    tend[ix3(k, j, i, ny, nx)] = t + ld(v.vfac, ix2(j, i, nx)) * (-(ld(g.rdnw, k) * (v1 - v0)));
 }
 
 // flux5 weight of stencil position m (0..5 = q-3..q+2) for upwind sign s,
@@ -103,13 +110,13 @@ __device__ __forceinline__ double w3(int m, double s) {
 
 // The full vector-Jacobian product.  tend is bilinear in (q, vel): with the
 // upwind signs frozen each face flux is F_f = vel_f h_f(q), so
-//   Fbar_x(i) = rdx (msftx(i) lam(i) - msftx(i-1) lam(i-1)), likewise y,
-//   Fbar_z(m) = rdnw(m) lam(m) - rdnw(m-1) lam(m-1),
+//   Fbar_x(i) = rdx (hfac(i) lam(i) - hfac(i-1) lam(i-1)), likewise y,
+//   Fbar_z(m) = vfac (rdnw(m) lam(m) - rdnw(m-1) lam(m-1)),
 //   q_bar(c)  = sum over the faces whose stencil holds c of
 //               vel_f w_m(sign vel_f) Fbar_f            (a gather, no atomics)
 //   velbar_f  = Fbar_f h_f(q),   h_f = flux5 / flux3 of the face's stencil
 //               (the second-order face value at m = 1 and nz-1).
-// One 32 x 8 block per tile and level: the level's msftx*lam, ru, rv (and,
+// One 32 x 8 block per tile and level: the level's hfac*lam, ru, rv (and,
 // for the velocity cotangents, q) plane tiles are staged in shared memory
 // with their periodic halos, the vertical stencils read the column.  q_bar,
 // ru_bar, rv_bar at cell (k, j, i) and its west / south face for k < nz,
@@ -118,7 +125,7 @@ __device__ __forceinline__ double w3(int m, double s) {
 __global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs v, const double *q,
                                                                const double *lam, double *q_bar, double *ru_bar,
                                                                double *rv_bar, double *rom_bar) {
-  using TM = Tile<3, 3>;  // msftx * lam
+  using TM = Tile<3, 3>;  // hfac * lam
   using TU = Tile<3, 0>;  // ru: west faces of cells i0-3 .. i0+34
   using TV = Tile<0, 3>;  // rv: south faces of rows j0-3 .. j0+10
   __shared__ double sml[TM::N], sru[TU::N], srv[TV::N], sq[TM::N];
@@ -132,7 +139,7 @@ __global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs 
     for (int e = ty * TSX + tx; e < TM::N; e += TSX * TSY) {
       const int r = e / TM::W, c = e - r * TM::W;
       const int jj = wrp(j0 - 3 + r, ny), ii = wrp(i0 - 3 + c, nx);
-      sml[e] = ld(g.msftx, ix2(jj, ii, nx)) * ld(lam, kp + ix2(jj, ii, nx));
+      sml[e] = ld(v.hfac, ix2(jj, ii, nx)) * ld(lam, kp + ix2(jj, ii, nx));
     }
     load_tile<3, 0>(sru, v.ru + kp, nx, i0, j0, nx, ny, 0.0);
     load_tile<0, 3>(srv, v.rv + kp, nx, i0, j0, nx, ny, 0.0);
@@ -165,7 +172,8 @@ __global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs 
                                            Q(ty + 2, tx), RV(ty));
       if (q_bar != nullptr) {
         // z faces m = k-1 .. k+2 whose stencils hold level k
-        auto Lz = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
+        const double vf = v.vfac != nullptr ? ld(v.vfac, ix2(j, i, nx)) : 1.0;
+        auto Lz = [&](int kk) { return vf * ld(lam, ix3(kk, j, i, ny, nx)); };
 #pragma unroll
         for (int t = -1; t <= 2; ++t) {
           const int m = k + t;
@@ -188,7 +196,8 @@ __global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs 
     double r = 0.0;
     if (k >= 1 && k <= nz - 1) {
       auto qc = [&](int kk) { return ld(q, ix3(kk, j, i, ny, nx)); };
-      auto L = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
+      const double vf = v.vfac != nullptr ? ld(v.vfac, ix2(j, i, nx)) : 1.0;
+      auto L = [&](int kk) { return vf * ld(lam, ix3(kk, j, i, ny, nx)); };
       const double rom = ld(v.rom, ix3(k, j, i, ny, nx));
       double h;
       if (k == 1 || k == nz - 1) {

@@ -1812,50 +1812,57 @@ extern "C" int wrfgpu_step_epilogue_device_lead(const wrfgpu_step_params *p, con
                             stream);
 }
 
-extern "C" int wrfgpu_scalar_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
-                                       const double *ru, const double *rv, const double *rom, double *tend,
-                                       cudaStream_t stream) {
+extern "C" int wrfgpu_flux_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
+                                     const double *ru, const double *rv, const double *rom, const double *hfac,
+                                     const double *vfac, double *tend, cudaStream_t stream) {
   int rc = adv_op_check(p, m, q, ru, rv, rom, tend);
   if (rc) return rc;
   Grid g = make_grid(*p, *m, nullptr);
-  AdvOpArgs a{ru, rv, rom};
+  AdvOpArgs a{ru, rv, rom, hfac != nullptr ? hfac : m->msftx, vfac};
   k_scalar_adv_op<<<grd(p->nx, p->ny, p->nz), blk2(), 0, stream>>>(g, a, q, tend);
   if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_op launch failed");
   g_last_error.clear();
   return WRFGPU_OK;
 }
 
-extern "C" int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *p, const wrfgpu_metrics *m,
-                                               const double *tend_bar, const double *ru, const double *rv,
-                                               const double *rom, double *q_bar, cudaStream_t stream) {
-  int rc = adv_op_check(p, m, tend_bar, ru, rv, rom, q_bar);
+extern "C" int wrfgpu_flux_advection_vjp(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
+                                         const double *tend_bar, const double *ru, const double *rv,
+                                         const double *rom, const double *hfac, const double *vfac, double *q_bar,
+                                         double *ru_bar, double *rv_bar, double *rom_bar, cudaStream_t stream) {
+  const bool vel = ru_bar != nullptr || rv_bar != nullptr || rom_bar != nullptr;
+  // q is read only for the velocities' cotangents
+  int rc = adv_op_check(p, m, vel ? q : tend_bar, ru, rv, rom, tend_bar);
   if (rc) return rc;
+  if (q_bar == nullptr && !vel) return fail(WRFGPU_ERR_NULL_POINTER, "q_bar, ru_bar, rv_bar and rom_bar are all NULL");
   Grid g = make_grid(*p, *m, nullptr);
-  AdvOpArgs a{ru, rv, rom};
-  // the VJP kernel with only the field's cotangent (q is not read)
-  k_scalar_adv_vjp<<<tgrd(p->nx, p->ny, p->nz), tblk(), 0, stream>>>(g, a, tend_bar, tend_bar, q_bar, nullptr,
-                                                                     nullptr, nullptr);
+  AdvOpArgs a{ru, rv, rom, hfac != nullptr ? hfac : m->msftx, vfac};
+  const int nzl = p->nz + (rom_bar != nullptr ? 1 : 0);
+  k_scalar_adv_vjp<<<tgrd(p->nx, p->ny, nzl), tblk(), 0, stream>>>(g, a, vel ? q : tend_bar, tend_bar, q_bar, ru_bar,
+                                                                     rv_bar, rom_bar);
   if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_vjp launch failed");
   g_last_error.clear();
   return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_scalar_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
+                                       const double *ru, const double *rv, const double *rom, double *tend,
+                                       cudaStream_t stream) {
+  return wrfgpu_flux_advection(p, m, q, ru, rv, rom, nullptr, nullptr, tend, stream);
+}
+
+extern "C" int wrfgpu_scalar_advection_adjoint(const wrfgpu_step_params *p, const wrfgpu_metrics *m,
+                                               const double *tend_bar, const double *ru, const double *rv,
+                                               const double *rom, double *q_bar, cudaStream_t stream) {
+  return wrfgpu_flux_advection_vjp(p, m, nullptr, tend_bar, ru, rv, rom, nullptr, nullptr, q_bar, nullptr, nullptr,
+                                   nullptr, stream);
 }
 
 extern "C" int wrfgpu_scalar_advection_vjp(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
                                            const double *tend_bar, const double *ru, const double *rv,
                                            const double *rom, double *q_bar, double *ru_bar, double *rv_bar,
                                            double *rom_bar, cudaStream_t stream) {
-  int rc = adv_op_check(p, m, q, ru, rv, rom, tend_bar);
-  if (rc) return rc;
-  if (q_bar == nullptr && ru_bar == nullptr && rv_bar == nullptr && rom_bar == nullptr)
-    return fail(WRFGPU_ERR_NULL_POINTER, "q_bar, ru_bar, rv_bar and rom_bar are all NULL");
-  Grid g = make_grid(*p, *m, nullptr);
-  AdvOpArgs a{ru, rv, rom};
-  const int nzl = p->nz + (rom_bar != nullptr ? 1 : 0);
-  k_scalar_adv_vjp<<<tgrd(p->nx, p->ny, nzl), tblk(), 0, stream>>>(g, a, q, tend_bar, q_bar, ru_bar, rv_bar,
-                                                                     rom_bar);
-  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_vjp launch failed");
-  g_last_error.clear();
-  return WRFGPU_OK;
+  return wrfgpu_flux_advection_vjp(p, m, q, tend_bar, ru, rv, rom, nullptr, nullptr, q_bar, ru_bar, rv_bar, rom_bar,
+                                   stream);
 }
 
 // ---------------------------------------------------------------------------
