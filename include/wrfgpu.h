@@ -336,11 +336,27 @@ int wrfgpu_flux_advection(const wrfgpu_step_params *params, const wrfgpu_metrics
                           const double *vfac, double *tend, cudaStream_t stream);
 
 /* Its vector-Jacobian product (as wrfgpu_scalar_advection_vjp, with the same
- * hfac / vfac); q may be NULL when only q_bar is asked for. */
+ * hfac / vfac); q may be NULL when only q_bar is asked for.  In both, rom
+ * NULL leaves the vertical flux out (the horizontal part of w's advection,
+ * params.nz then being w's level count). */
 int wrfgpu_flux_advection_vjp(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const double *q,
                               const double *tend_bar, const double *ru, const double *rv, const double *rom,
                               const double *hfac, const double *vfac, double *q_bar, double *ru_bar,
                               double *rv_bar, double *rom_bar, cudaStream_t stream);
+
+/* The vertical flux divergence of w (nz+1, ny, nx) by the omega rom
+ * (nz+1, ny, nx): advect_w_flux's _vdiv_w part (dynamics/flux_advection.py:
+ * 1410-1482; the horizontal part is wrfgpu_flux_advection on w's levels with
+ * the velocities interpolated to them and rom NULL).  Reads params nx, ny,
+ * nz (mass levels), top_lid and metrics rdn. */
+int wrfgpu_w_vertical_advection(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics, const double *w,
+                                const double *rom, double *tend, cudaStream_t stream);
+
+/* Its vector-Jacobian product: w_bar and rom_bar (either may be NULL) for a
+ * cotangent tend_bar, the upwind switches held at their forward signs. */
+int wrfgpu_w_vertical_advection_vjp(const wrfgpu_step_params *params, const wrfgpu_metrics *metrics,
+                                    const double *w, const double *rom, const double *tend_bar, double *w_bar,
+                                    double *rom_bar, cudaStream_t stream);
 
 /* One acoustic small step on its own (the reference's acoustic_substep_core,
  * core/acoustic.py:837-1150: advance_uv, advance_mu_t, advance_w with its

@@ -1,13 +1,17 @@
 """Momentum advection operators and their hand-written adjoints.
 
-``adjoint.advect_u`` / ``adjoint.advect_v`` are the reference's periodic
-advect_u_flux / advect_v_flux (dynamics/flux_advection.py:1131-1274): the
-flux-form operator of the CUDA library (``wrfgpu_flux_advection``) on the
-core faces, with the transport velocities averaged to them and the map
-factors msfux, msfvy (and msfvy / msfvx on v's vertical term).
+``adjoint.advect_u`` / ``adjoint.advect_v`` / ``adjoint.advect_w`` are the
+reference's periodic advect_u_flux / advect_v_flux / advect_w_flux
+(dynamics/flux_advection.py:1131-1329): the flux-form operator of the CUDA
+library (``wrfgpu_flux_advection``) on the core faces, with the transport
+velocities averaged to them and the map factors msfux, msfvy (and msfvy /
+msfvx on v's vertical term); for w the same operator over w's levels with
+the velocities interpolated to them, plus w's own vertical flux divergence
+(``wrfgpu_w_vertical_advection``).
 
-* forward: against the oracle's advect_u_flux / advect_v_flux on random
-  fields, map factors and velocities, 1e-12 relative max-abs;
+* forward: against the oracle's advect_u_flux / advect_v_flux /
+  advect_w_flux (rigid lid and open top) on random fields, map factors and
+  velocities, 1e-12 relative max-abs;
 * adjoint: the operator is bilinear in the advected component and the
   velocities (the upwind switches are fixed by the velocities' signs), so
   with the face-averaged velocities kept away from zero, the directional
@@ -122,3 +126,49 @@ def test_momentum_advection_vjp(cuda_ready, comp):
         fd = (inner(*plus) - inner(*minus)) / (2 * h)
         ad = float((grads[which] * _dev(d)).sum())
         assert abs(fd - ad) <= 1.0e-10 * max(abs(ad), 1e-300), (comp, which, fd, ad)
+
+
+@pytest.mark.parametrize("top_lid", [True, False])
+def test_w_advection_matches_oracle_and_vjp(cuda_ready, top_lid):
+    """advect_w: the horizontal operator on w's levels plus w's vertical flux
+    divergence (rigid lid and open top), against the oracle's advect_w_flux
+    at 1e-12, and its VJP against central differences along w and each
+    velocity (1e-10) with the dot-product identity in w (1e-12)."""
+    nx, ny, nz = 24, 20, 12
+    case, nl, m, _, _, ru, rv, rom, rng = _setup(nx, ny, nz, seed=4)
+    nl.top_lid = top_lid
+    w = rng.standard_normal((nz + 1, ny, nx))
+    vel = _oracle_vel(m, ru, rv, rom, nx, ny)
+    rdx, rdy = 1.0 / case.controls["dx"], 1.0 / case.controls["dy"]
+    ora = D.advect_w_flux(w, vel, rdx, rdy, m, top_lid)
+    xs = [_dev(a).requires_grad_(True) for a in (w, ru, rv, rom)]
+    y = adjoint.advect_w(*xs, nl)
+    got = y.detach().cpu().numpy()
+    err = np.abs(got - ora).max() / np.abs(ora).max()
+    assert err <= 1.0e-12, err
+
+    lam = rng.standard_normal(w.shape)
+    LAM = _dev(lam)
+    grads = torch.autograd.grad(y, xs, grad_outputs=LAM)
+    lhs = float((y.detach() * LAM).sum())
+    rhs = float((grads[0] * xs[0].detach()).sum())
+    assert abs(lhs - rhs) <= 1.0e-12 * abs(lhs), (lhs, rhs)
+
+    def inner(*args):
+        return float((adjoint.advect_w(*map(_dev, args), nl) * LAM).sum())
+
+    base = [w, ru, rv, rom]
+    steps = [1.0, 200.0, 200.0, 5.0]
+    for which in range(4):
+        d = rng.standard_normal(base[which].shape)
+        if which == 3:
+            d[0] = 0.0
+            d[-1] = 0.0
+        h = steps[which]
+        plus = [b.copy() for b in base]
+        minus = [b.copy() for b in base]
+        plus[which] = plus[which] + h * d
+        minus[which] = minus[which] - h * d
+        fd = (inner(*plus) - inner(*minus)) / (2 * h)
+        ad = float((grads[which] * _dev(d)).sum())
+        assert abs(fd - ad) <= 1.0e-10 * max(abs(ad), 1e-300), (which, fd, ad)

@@ -140,7 +140,7 @@ EXPORTED = ("wrfgpu_step_params_init", "wrfgpu_step_params_validate", "wrfgpu_st
             "wrfgpu_rk3_step", "wrfgpu_rk3_step_device_lead", "wrfgpu_rk3_step_static_workspace",
             "wrfgpu_rk3_step_batched", "wrfgpu_autotune", "wrfgpu_scalar_advection",
             "wrfgpu_scalar_advection_adjoint", "wrfgpu_scalar_advection_vjp", "wrfgpu_flux_advection",
-            "wrfgpu_flux_advection_vjp",
+            "wrfgpu_flux_advection_vjp", "wrfgpu_w_vertical_advection", "wrfgpu_w_vertical_advection_vjp",
             "wrfgpu_acoustic_workspace_size", "wrfgpu_acoustic_substep",
             "wrfgpu_acoustic_substep_vjp", "wrfgpu_apply_lateral_boundaries",
             "wrfgpu_step_epilogue_workspace_size", "wrfgpu_step_epilogue", "wrfgpu_step_epilogue_device_lead", "wrfgpu_step_launch_count", "wrfgpu_profile_enable", "wrfgpu_profile_read",
@@ -201,6 +201,11 @@ def load(path: str | os.PathLike | None = None):
     lib.wrfgpu_flux_advection_vjp.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
                                               _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
     lib.wrfgpu_flux_advection_vjp.restype = _I
+    lib.wrfgpu_w_vertical_advection.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics), _P, _P, _P, _P]
+    lib.wrfgpu_w_vertical_advection.restype = _I
+    lib.wrfgpu_w_vertical_advection_vjp.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),
+                                                    _P, _P, _P, _P, _P, _P]
+    lib.wrfgpu_w_vertical_advection_vjp.restype = _I
     lib.wrfgpu_acoustic_workspace_size.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_size_t)]
     lib.wrfgpu_acoustic_workspace_size.restype = _I
     lib.wrfgpu_acoustic_substep.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(Metrics),

@@ -2,12 +2,14 @@
 
 * ``scalar_advection(q, ru, rv, rom, namelist)`` returns the advective
   tendency of ``q`` (``advect_scalar_flux``, dynamics/flux_advection.py:482-568,
-  doubly periodic), ``advect_u`` / ``advect_v`` those of the momentum
-  components (``advect_u_flux`` / ``advect_v_flux``, :1131-1274, periodic);
+  doubly periodic), ``advect_u`` / ``advect_v`` / ``advect_w`` those of the
+  momentum components (``advect_u_flux`` / ``advect_v_flux`` /
+  ``advect_w_flux``, :1131-1329, periodic);
   ``backward`` applies the hand-written VJP kernel
   (``wrfgpu_flux_advection_vjp``, one launch) for the advected field and the
   transport velocities ``ru``, ``rv``, ``rom`` (the operator is bilinear; the
-  upwind switches are held at their forward sign).
+  upwind switches are held at their forward sign), with w's vertical part
+  through ``wrfgpu_w_vertical_advection_vjp``.
 * ``acoustic_substep(work, op)`` / ``acoustic_loop(work, op, nsub)``: one or
   ``nsub`` acoustic small steps (acoustic_substep_core, core/acoustic.py:
   837-1150) of the evolving work state for fixed stage constants, with the
@@ -52,7 +54,8 @@ class FluxAdvection(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, q, ru, rv, rom, op: _Op, hfac, vfac):
-        q, ru, rv, rom = (t.contiguous() for t in (q, ru, rv, rom))
+        # rom None: the horizontal flux divergence alone
+        q, ru, rv, rom = (t.contiguous() if t is not None else None for t in (q, ru, rv, rom))
         tend = torch.empty_like(q)
         st = torch.cuda.current_stream(q.device)
         _capi.check(_capi.load().wrfgpu_flux_advection(
@@ -117,6 +120,57 @@ def advect_v(v: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: torch.Ten
     vfac = (m.msfvy[:ny] / m.msfvx[:ny]).contiguous()
     tend = FluxAdvection.apply(v[:, :ny, :], velx, vely, velz, _Op(namelist), hfac, vfac)
     return torch.cat((tend, tend[:, :1, :]), dim=1)
+
+
+class _WVertical(torch.autograd.Function):
+    """The vertical flux divergence of w (``wrfgpu_w_vertical_advection``)
+    and its VJP (``wrfgpu_w_vertical_advection_vjp``)."""
+
+    @staticmethod
+    def forward(ctx, w, rom, op: _Op):
+        w, rom = w.contiguous(), rom.contiguous()
+        tend = torch.empty_like(w)
+        st = torch.cuda.current_stream(w.device)
+        _capi.check(_capi.load().wrfgpu_w_vertical_advection(
+            ctypes.byref(op.params), ctypes.byref(op.metrics), _ptr(w), _ptr(rom), _ptr(tend),
+            ctypes.c_void_p(st.cuda_stream)))
+        ctx.save_for_backward(w, rom)
+        ctx.op = op
+        return tend
+
+    @staticmethod
+    def backward(ctx, tend_bar):
+        w, rom = ctx.saved_tensors
+        outs = [torch.empty_like(t) if n else None for t, n in zip((w, rom), ctx.needs_input_grad[:2])]
+        if any(o is not None for o in outs):
+            st = torch.cuda.current_stream(w.device)
+            _capi.check(_capi.load().wrfgpu_w_vertical_advection_vjp(
+                ctypes.byref(ctx.op.params), ctypes.byref(ctx.op.metrics), _ptr(w), _ptr(rom),
+                _ptr(tend_bar.contiguous()), *map(_ptr, outs), ctypes.c_void_p(st.cuda_stream)))
+        return (*outs, None)
+
+
+def _mass_to_full(f, fnm, fnp):
+    """flux_advection.py:1332-1352: a mass-level field on the w levels."""
+    inner = fnm[1:, None, None] * f[1:] + fnp[1:, None, None] * f[:-1]
+    return torch.cat((f[:1], inner, f[-1:]), dim=0)
+
+
+def advect_w(w: torch.Tensor, ru: torch.Tensor, rv: torch.Tensor, rom: torch.Tensor,
+             namelist: dycore.OperationalNamelist) -> torch.Tensor:
+    """advect_w_flux (dynamics/flux_advection.py:1277-1329), doubly periodic:
+    the advective tendency of w (nz+1, ny, nx) -- the horizontal flux
+    operator on w's levels with ru, rv interpolated to them (map factor
+    msftx) plus w's own vertical flux divergence by rom (namelist.top_lid).
+    Differentiable with respect to w and the velocities."""
+    m = namelist.metrics
+    nz = ru.shape[0]
+    fnm, fnp = m.fnm[:nz], m.fnp[:nz]
+    ru_w, rv_w = _mass_to_full(ru, fnm, fnp), _mass_to_full(rv, fnm, fnp)
+    op_w = _Op(namelist)
+    op_w.params.nz = nz + 1  # the horizontal operator over w's levels
+    tend_h = FluxAdvection.apply(w, ru_w, rv_w, None, op_w, m.msftx.contiguous(), None)
+    return tend_h + _WVertical.apply(w, rom, _Op(namelist))
 
 
 class AcousticOp:

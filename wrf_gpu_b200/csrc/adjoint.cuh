@@ -54,6 +54,10 @@ __global__ void k_scalar_adv_op(Grid g, AdvOpArgs v, const double *q, double *te
   const double hf = ld(v.hfac, ix2(j, i, nx));
   double t = -hf * g.rdx * (fx(i + 1) - fx(i));
   t = t - hf * g.rdy * (fy(j + 1) - fy(j));
+  if (v.rom == nullptr) {  // the horizontal flux divergence alone
+    tend[ix3(k, j, i, ny, nx)] = t;
+    return;
+  }
   auto qc = [&](int kk) { return ld(q, ix3(kk, j, i, ny, nx)); };
   const double v1 = (k + 1 <= nz - 1) ? vflux3_at(g, k + 1, ld(v.rom, ix3(k + 1, j, i, ny, nx)), qc) : 0.0;
   const double v0 = (k >= 1) ? vflux3_at(g, k, ld(v.rom, ix3(k, j, i, ny, nx)), qc) : 0.0;
@@ -170,7 +174,8 @@ __global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs 
         rv_bar[kp + ix2(j, i, nx)] = g.rdy * (ML(ty, tx) - ML(ty - 1, tx)) *
                                      flux5(Q(ty - 3, tx), Q(ty - 2, tx), Q(ty - 1, tx), Q(ty, tx), Q(ty + 1, tx),
                                            Q(ty + 2, tx), RV(ty));
-      if (q_bar != nullptr) {
+      if (q_bar != nullptr && v.rom == nullptr) q_bar[kp + ix2(j, i, nx)] = acc;
+      if (q_bar != nullptr && v.rom != nullptr) {
         // z faces m = k-1 .. k+2 whose stencils hold level k
         const double vf = v.vfac != nullptr ? ld(v.vfac, ix2(j, i, nx)) : 1.0;
         auto Lz = [&](int kk) { return vf * ld(lam, ix3(kk, j, i, ny, nx)); };
@@ -192,7 +197,7 @@ __global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs 
       }
     }
   }
-  if (rom_bar != nullptr && valid) {
+  if (rom_bar != nullptr && v.rom != nullptr && valid) {
     double r = 0.0;
     if (k >= 1 && k <= nz - 1) {
       auto qc = [&](int kk) { return ld(q, ix3(kk, j, i, ny, nx)); };
@@ -209,6 +214,105 @@ __global__ void __launch_bounds__(TSX * TSY) k_scalar_adv_vjp(Grid g, AdvOpArgs 
       r = (ld(g.rdnw, k) * L(k) - ld(g.rdnw, k - 1) * L(k - 1)) * h;
     }
     rom_bar[ix3(k, j, i, ny, nx)] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The vertical flux divergence of w (flux_advection.py:1410-1482, the
+// oracle's _vdiv_w) on its nz+1 levels: vel(k) = (rom(k) + rom(k-1)) / 2,
+// face values flux3 with the -sign(vel) correction for k = 2..nz-1 and
+// (w(k) + w(k-1)) / 2 at k = 1 and, without a rigid lid, at k = nz;
+// tend(k) = -rdn(k) (vflux(k+1) - vflux(k)) for k = 1..nz-1 and, without a
+// lid, tend(nz) = 2 rdn(nz-1) vflux(nz).  Index space (nx, ny, nz+1).
+// ---------------------------------------------------------------------------
+struct WColumn {
+  const double *w, *rom;  // (nz+1, ny, nx) each
+  int top_lid;
+};
+
+__device__ __forceinline__ double wvel(const Grid &g, const WColumn &c, int k, int j, int i) {
+  return 0.5 * (ld(c.rom, ix3(k, j, i, g.ny, g.nx)) + ld(c.rom, ix3(k - 1, j, i, g.ny, g.nx)));
+}
+// vflux(k) / vel(k): the face value of w at w-level face k (0 where there is no flux)
+__device__ __forceinline__ double wface(const Grid &g, const WColumn &c, int k, int j, int i, double vel) {
+  const int nz = g.nz;
+  auto W = [&](int kk) { return ld(c.w, ix3(kk, j, i, g.ny, g.nx)); };
+  if (k == 1) return 0.5 * (W(1) + W(0));
+  if (k >= 2 && k <= nz - 1) {
+    const double flux4 = div_rcp(7.0 * (W(k) + W(k - 1)) - (W(k + 1) + W(k - 2)), 12.0, R12);
+    const double corr = div_rcp((W(k + 1) - W(k - 2)) - 3.0 * (W(k) - W(k - 1)), 12.0, R12);
+    return flux4 + sgn(-vel) * corr;
+  }
+  if (k == nz && !c.top_lid) return 0.5 * (W(nz) + W(nz - 1));
+  return 0.0;
+}
+__device__ __forceinline__ double wflux(const Grid &g, const WColumn &c, int k, int j, int i) {
+  const int nz = g.nz;
+  if (k < 1 || k > nz || (k == nz && c.top_lid)) return 0.0;
+  const double vel = wvel(g, c, k, j, i);
+  auto W = [&](int kk) { return ld(c.w, ix3(kk, j, i, g.ny, g.nx)); };
+  if (k == 1) return vel * 0.5 * (W(1) + W(0));
+  if (k == nz) return vel * 0.5 * (W(nz) + W(nz - 1));
+  return flux3v(W(k - 2), W(k - 1), W(k), W(k + 1), vel);
+}
+
+// g.nz here is the mass level count; w has g.nz + 1 levels
+__global__ void k_vdiv_w(Grid g, WColumn c, double *tend) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j >= ny) return;
+  double t = 0.0;
+  if (k >= 1 && k <= nz - 1) t = -ld(g.rdn, k) * (wflux(g, c, k + 1, j, i) - wflux(g, c, k, j, i));
+  if (k == nz && !c.top_lid) t = t + 2.0 * ld(g.rdn, nz - 1) * wflux(g, c, nz, j, i);
+  tend[ix3(k, j, i, ny, nx)] = t;
+}
+
+// Its VJP: Fbar(k) = rdn(k) lam(k) [k <= nz-1] - rdn(k-1) lam(k-1) [k >= 2]
+// + 2 rdn(nz-1) lam(nz) [k = nz, open top]; w_bar(l) gathers
+// Fbar(k) vel(k) dh_k/dw(l) over the faces k = l-1 .. l+2 whose stencils hold
+// level l; velbar(k) = Fbar(k) h_k(w) and rom_bar(l) = (velbar(l) +
+// velbar(l+1)) / 2.  Outputs given as NULL are skipped.
+__global__ void k_vdiv_w_vjp(Grid g, WColumn c, const double *lam, double *w_bar, double *rom_bar) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int l = blockIdx.z;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i >= nx || j >= ny) return;
+  auto L = [&](int kk) { return ld(lam, ix3(kk, j, i, ny, nx)); };
+  auto fbar = [&](int k) {
+    double f = 0.0;
+    if (k <= nz - 1) f += ld(g.rdn, k) * L(k);
+    if (k >= 2) f -= ld(g.rdn, k - 1) * L(k - 1);
+    if (k == nz && !c.top_lid) f += 2.0 * ld(g.rdn, nz - 1) * L(nz);
+    return f;
+  };
+  auto live = [&](int k) { return k >= 1 && k <= nz && !(k == nz && c.top_lid); };
+  if (w_bar != nullptr) {
+    double acc = 0.0;
+    for (int k = l - 1; k <= l + 2; ++k) {
+      if (!live(k)) continue;
+      const double vel = wvel(g, c, k, j, i);
+      double wt = 0.0;
+      if (k == 1 || k == nz) {
+        wt = (l == k || l == k - 1) ? 0.5 : 0.0;
+      } else {
+        const double s = sgn(-vel);
+        switch (l - (k - 2)) {  // stencil w(k-2) .. w(k+1)
+          case 0: wt = w3<0>(s); break;
+          case 1: wt = w3<1>(s); break;
+          case 2: wt = w3<2>(s); break;
+          default: wt = w3<3>(s); break;
+        }
+      }
+      acc += fbar(k) * vel * wt;
+    }
+    w_bar[ix3(l, j, i, ny, nx)] = acc;
+  }
+  if (rom_bar != nullptr) {
+    auto velbar = [&](int k) { return live(k) ? fbar(k) * wface(g, c, k, j, i, wvel(g, c, k, j, i)) : 0.0; };
+    rom_bar[ix3(l, j, i, ny, nx)] = 0.5 * (velbar(l) + velbar(l + 1));
   }
 }
 

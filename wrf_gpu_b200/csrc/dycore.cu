@@ -1815,7 +1815,8 @@ extern "C" int wrfgpu_step_epilogue_device_lead(const wrfgpu_step_params *p, con
 extern "C" int wrfgpu_flux_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *q,
                                      const double *ru, const double *rv, const double *rom, const double *hfac,
                                      const double *vfac, double *tend, cudaStream_t stream) {
-  int rc = adv_op_check(p, m, q, ru, rv, rom, tend);
+  // rom NULL: the horizontal flux divergence alone
+  int rc = adv_op_check(p, m, q, ru, rv, rom != nullptr ? rom : ru, tend);
   if (rc) return rc;
   Grid g = make_grid(*p, *m, nullptr);
   AdvOpArgs a{ru, rv, rom, hfac != nullptr ? hfac : m->msftx, vfac};
@@ -1830,9 +1831,10 @@ extern "C" int wrfgpu_flux_advection_vjp(const wrfgpu_step_params *p, const wrfg
                                          const double *rom, const double *hfac, const double *vfac, double *q_bar,
                                          double *ru_bar, double *rv_bar, double *rom_bar, cudaStream_t stream) {
   const bool vel = ru_bar != nullptr || rv_bar != nullptr || rom_bar != nullptr;
-  // q is read only for the velocities' cotangents
-  int rc = adv_op_check(p, m, vel ? q : tend_bar, ru, rv, rom, tend_bar);
+  // q is read only for the velocities' cotangents; rom NULL: horizontal only
+  int rc = adv_op_check(p, m, vel ? q : tend_bar, ru, rv, rom != nullptr ? rom : ru, tend_bar);
   if (rc) return rc;
+  if (rom == nullptr && rom_bar != nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "rom_bar needs rom");
   if (q_bar == nullptr && !vel) return fail(WRFGPU_ERR_NULL_POINTER, "q_bar, ru_bar, rv_bar and rom_bar are all NULL");
   Grid g = make_grid(*p, *m, nullptr);
   AdvOpArgs a{ru, rv, rom, hfac != nullptr ? hfac : m->msftx, vfac};
@@ -1840,6 +1842,37 @@ extern "C" int wrfgpu_flux_advection_vjp(const wrfgpu_step_params *p, const wrfg
   k_scalar_adv_vjp<<<tgrd(p->nx, p->ny, nzl), tblk(), 0, stream>>>(g, a, vel ? q : tend_bar, tend_bar, q_bar, ru_bar,
                                                                      rv_bar, rom_bar);
   if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_scalar_adv_vjp launch failed");
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_w_vertical_advection(const wrfgpu_step_params *p, const wrfgpu_metrics *m, const double *w,
+                                           const double *rom, double *tend, cudaStream_t stream) {
+  if (p == nullptr || m == nullptr || w == nullptr || rom == nullptr || tend == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "an argument is NULL");
+  if (m->rdn == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "metrics rdn is needed");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  Grid g = make_grid(*p, *m, nullptr);
+  k_vdiv_w<<<grd(p->nx, p->ny, p->nz + 1), blk2(), 0, stream>>>(g, WColumn{w, rom, p->top_lid}, tend);
+  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_vdiv_w launch failed");
+  g_last_error.clear();
+  return WRFGPU_OK;
+}
+
+extern "C" int wrfgpu_w_vertical_advection_vjp(const wrfgpu_step_params *p, const wrfgpu_metrics *m,
+                                               const double *w, const double *rom, const double *tend_bar,
+                                               double *w_bar, double *rom_bar, cudaStream_t stream) {
+  if (p == nullptr || m == nullptr || w == nullptr || rom == nullptr || tend_bar == nullptr)
+    return fail(WRFGPU_ERR_NULL_POINTER, "an argument is NULL");
+  if (w_bar == nullptr && rom_bar == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "w_bar and rom_bar are NULL");
+  if (m->rdn == nullptr) return fail(WRFGPU_ERR_NULL_POINTER, "metrics rdn is needed");
+  int rc = wrfgpu_step_params_validate(p);
+  if (rc) return rc;
+  Grid g = make_grid(*p, *m, nullptr);
+  k_vdiv_w_vjp<<<grd(p->nx, p->ny, p->nz + 1), blk2(), 0, stream>>>(g, WColumn{w, rom, p->top_lid}, tend_bar, w_bar,
+                                                                   rom_bar);
+  if (cudaGetLastError() != cudaSuccess) return fail(WRFGPU_ERR_CUDA, "k_vdiv_w_vjp launch failed");
   g_last_error.clear();
   return WRFGPU_OK;
 }
