@@ -59,7 +59,17 @@ constexpr int D6_NS = (D6_R * D6_W + D6_TX * D6_TY - 1) / (D6_TX * D6_TY);
 // the u, v, w and theta cells at (k, j, i) for the block's D6_KC levels.  The
 // four fields' tiles (3-cell wrapped halo) of a level are staged together,
 // double-buffered across levels, then filtered from shared memory.
-__global__ void __launch_bounds__(D6_TX * D6_TY) k_diff6(Grid g, Diff6Args a) {
+// 5 resident blocks of 256 per SM (48 registers): 433 x 433 x 50, 0.886 vs
+// 0.930 ms/step at the compiler's 62 registers (6: 1.089).
+#ifndef WG_D6_MINB
+#define WG_D6_MINB 5
+#endif
+#if WG_D6_MINB > 0
+#define WG_D6_BOUNDS __launch_bounds__(D6_TX * D6_TY, WG_D6_MINB)
+#else
+#define WG_D6_BOUNDS __launch_bounds__(D6_TX * D6_TY)
+#endif
+__global__ void WG_D6_BOUNDS k_diff6(Grid g, Diff6Args a) {
   __shared__ double tile[2][4][D6_R][D6_W];
   const int i0 = blockIdx.x * D6_TX, j0 = blockIdx.y * D6_TY;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
