@@ -171,14 +171,25 @@ Grid make_grid(const wrfgpu_step_params &p, const wrfgpu_metrics &m, const doubl
 // Specified boundary work targets (coupling/boundary_apply.py:729-781) for
 // the normal momentum, from the time-interpolated strips.
 
+// The targets are read by advance_uv only where its relax weight is non-zero:
+// the relax_zone (<= nzone) columns (u) / rows (v) at each edge.  So only the
+// nzone columns / rows at each edge are formed: index t in [0, 2 nzone) maps
+// to t and x_len - 2 nzone + t (all columns when x_len <= 2 nzone, zero-padded
+// targets outside the nzone bands there as before).
+__device__ __forceinline__ int zone_index(int t, int len, int nzone) {
+  return (len <= 2 * nzone || t < nzone) ? t : len - 2 * nzone + t;
+}
+__host__ __device__ inline int zone_extent(int len, int nzone) { return len <= 2 * nzone ? len : 2 * nzone; }
+
 __global__ void k_bdy_target_u(Grid g, BdyLeaf b, const double *u_save, const double *muu, const double *muus,
                                int nzone, double *target) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int x_len = nx + 1;
+  const int t_ = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   int k = blockIdx.z;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  if (i > nx || j >= ny) return;
-  const int x_len = nx + 1;
+  if (t_ >= zone_extent(x_len, nzone) || j >= ny) return;
+  const int i = zone_index(t_, x_len, nzone);
   const size_t cu = ix3(k, j, i, ny, x_len);
   // last writer in the reference loop order: for b: W col b, then E col x_len-1-b
   int best = -1, side = 0;
@@ -198,12 +209,13 @@ __global__ void k_bdy_target_u(Grid g, BdyLeaf b, const double *u_save, const do
 
 __global__ void k_bdy_target_v(Grid g, BdyLeaf b, const double *v_save, const double *muv, const double *muvs,
                                int nzone, double *target) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int j = blockIdx.y * blockDim.y + threadIdx.y;
-  int k = blockIdx.z;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  if (i >= nx || j > ny) return;
   const int y_len = ny + 1;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t_ = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  if (i >= nx || t_ >= zone_extent(y_len, nzone)) return;
+  const int j = zone_index(t_, y_len, nzone);
   const size_t cv = ix3(k, j, i, y_len, nx);
   int best = -1, side = 2;
   for (int bb = 0; bb < nzone; ++bb) {
@@ -892,10 +904,12 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
     if (bdy_active) {
       const int nzone = p.spec_zone + p.relax_zone;
       PROF("k_bdy_target_u");
-      k_bdy_target_u<<<grd(nx + 1, ny, nz), blk2(), 0, stream>>>(g, bl_u, s.u, w.muu, w.muus, nzone, w.u_target);
+      k_bdy_target_u<<<grd(zone_extent(nx + 1, nzone), ny, nz), blk2(), 0, stream>>>(g, bl_u, s.u, w.muu, w.muus,
+                                                                                     nzone, w.u_target);
       LAUNCH_CHECK("k_bdy_target_u");
       PROF("k_bdy_target_v");
-      k_bdy_target_v<<<grd(nx, ny + 1, nz), blk2(), 0, stream>>>(g, bl_v, s.v, w.muv, w.muvs, nzone, w.v_target);
+      k_bdy_target_v<<<grd(nx, zone_extent(ny + 1, nzone), nz), blk2(), 0, stream>>>(g, bl_v, s.v, w.muv, w.muvs,
+                                                                                     nzone, w.v_target);
       LAUNCH_CHECK("k_bdy_target_v");
       const double strength = (p.normal_bdy_relax_strength < 0.0) ? 20.0 : p.normal_bdy_relax_strength;
       ba.u_target = w.u_target;
