@@ -120,6 +120,12 @@ def test_launch_count(lib):
     # map-factor reciprocals + 3 stages x (8 stage + 3 finish)
     # + 3 launches per substep x (1 + 3 + 6)
     assert n.value == 1 + 3 * 11 + 3 * 10
+    # limited moisture: one scale pass over the six species and six tendency
+    # passes in the final stage
+    for opt in (1, 2):
+        p = _params(lib, acoustic_substeps=6, moist_adv_opt=opt)
+        assert lib.wrfgpu_step_launch_count(ctypes.byref(p), ctypes.byref(n)) == 0
+        assert n.value == 1 + 3 * 11 + 3 * 10 + 7
     # specified boundaries (+2 target launches per stage) with the boundary
     # cadence: + the first stage's mu tendency, one relax launch per stage and
     # one zero-gradient w launch per substep

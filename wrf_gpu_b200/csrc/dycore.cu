@@ -81,6 +81,10 @@ struct Work {
   double *alt_raw, *alt, *pb, *c2a, *qtot, *al_ls, *php_ls, *php, *t_tend, *theta_w, *t2ave, *p, *pm1, *al;
   double *s1, *s2, *ru, *rv, *dvdxi, *hdiv;
   LimFaces limf;  // limiter face fluxes (scale pass -> tendency pass)
+  // per moisture species (set 0 = s1 / s2 / limf): the species are limited in
+  // one scale-pass launch, each into its own scratch
+  double *s1q[6], *s2q[6];
+  LimFaces limq[6];
   double *qtend[6];
   // u / v faces
   double *u_tend, *u_w, *cqu, *u_target, *v_tend, *v_w, *cqv, *v_target;
@@ -119,6 +123,17 @@ void carve(const wrfgpu_step_params &p, Carver &c, Work &w) {
   w.limf.lx = lim ? c.take(d.m) : nullptr; w.limf.ax = lim ? c.take(d.m) : nullptr;
   w.limf.ly = lim ? c.take(d.m) : nullptr; w.limf.ay = lim ? c.take(d.m) : nullptr;
   w.limf.lz = lim ? c.take(d.m) : nullptr; w.limf.az = lim ? c.take(d.m) : nullptr;
+  const bool limq = p.moist_adv_opt == 1 || p.moist_adv_opt == 2;
+  for (int q = 0; q < 6; ++q) {
+    if (q == 0 || !limq) {
+      w.s1q[q] = w.s1; w.s2q[q] = w.s2; w.limq[q] = w.limf;
+      continue;
+    }
+    w.s1q[q] = c.take(d.m);
+    w.s2q[q] = (p.moist_adv_opt == 2) ? c.take(d.m) : nullptr;  // the PD tendency reads s1 only
+    w.limq[q].lx = c.take(d.m); w.limq[q].ax = c.take(d.m); w.limq[q].ly = c.take(d.m);
+    w.limq[q].ay = c.take(d.m); w.limq[q].lz = c.take(d.m); w.limq[q].az = c.take(d.m);
+  }
   for (int s = 0; s < 6; ++s) w.qtend[s] = is_moist(p) ? c.take(d.m) : nullptr;
   w.u_tend = c.take(d.u); w.u_w = c.take(d.u); w.cqu = c.take(d.u);
   w.v_tend = c.take(d.v); w.v_w = c.take(d.v); w.cqv = c.take(d.v);
@@ -473,7 +488,7 @@ int wrfgpu_step_launch_count(const wrfgpu_step_params *p, int *launches) {
   for (int s = 0; s < 3; ++s) {
     n += 8;  // mass2d, transport, diag, uface, vface, mass, wface, coef
     if (s == 2 && (p->scalar_adv_opt == 1 || p->scalar_adv_opt == 2)) n += 2;
-    if (s == 2 && (p->moist_adv_opt == 1 || p->moist_adv_opt == 2)) n += 12;
+    if (s == 2 && (p->moist_adv_opt == 1 || p->moist_adv_opt == 2)) n += 7;  // one scale pass, six tendency passes
     if (bdy) n += 2;
     n += 3 * nsub[s];  // advance_uv, div_h, column
     n += 3;  // finish u, v, col
@@ -743,22 +758,43 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
       la.deg = deg;
       set_lim_constants(la, g.rdx, g.rdy);
       // float32 views of the same scratch for the mixed variant
-      LimFacesT<float> limf32{reinterpret_cast<float *>(w.limf.lx), reinterpret_cast<float *>(w.limf.ax),
-                              reinterpret_cast<float *>(w.limf.ly), reinterpret_cast<float *>(w.limf.ay),
-                              reinterpret_cast<float *>(w.limf.lz), reinterpret_cast<float *>(w.limf.az)};
+      auto f32 = [](const LimFaces &f) {
+        return LimFacesT<float>{reinterpret_cast<float *>(f.lx), reinterpret_cast<float *>(f.ax),
+                                reinterpret_cast<float *>(f.ly), reinterpret_cast<float *>(f.ay),
+                                reinterpret_cast<float *>(f.lz), reinterpret_cast<float *>(f.az)};
+      };
+      const LimFacesT<float> limf32 = f32(w.limf);
       float *s1f = reinterpret_cast<float *>(w.s1), *s2f = reinterpret_cast<float *>(w.s2);
-      const dim3 lim_grid = tgrd(nx, ny, march_nchunk(nz, kc));
-      auto scale_pass = [&](const double *fld, const double *fld_old) {
-        if (mixed)
-          kLimScaleF<<<lim_grid, tblk(), 0, stream>>>(g, la, fld, fld_old, s1f, s2f, limf32);
-        else
-          kLimScaleD<<<lim_grid, tblk(), 0, stream>>>(g, la, fld, fld_old, w.s1, w.s2, w.limf);
+      // one scale-pass launch over n fields (theta alone, or the six species),
+      // each into its own scratch set
+      auto scale_pass = [&](int n, const double *const *fld, const double *const *fld_old, int set0) {
+        const dim3 lim_grid(((nx + TSX - 1) / TSX) * n, (ny + TSY - 1) / TSY, march_nchunk(nz, kc));
+        if (mixed) {
+          LimBatch<float> lb{};
+          lb.n = n;
+          for (int t = 0; t < n; ++t) {
+            lb.field[t] = fld[t]; lb.field_old[t] = fld_old[t];
+            lb.s1[t] = reinterpret_cast<float *>(w.s1q[set0 + t]);
+            lb.s2[t] = reinterpret_cast<float *>(w.s2q[set0 + t]);
+            lb.fo[t] = f32(w.limq[set0 + t]);
+          }
+          kLimScaleF<<<lim_grid, tblk(), 0, stream>>>(g, la, lb);
+        } else {
+          LimBatch<double> lb{};
+          lb.n = n;
+          for (int t = 0; t < n; ++t) {
+            lb.field[t] = fld[t]; lb.field_old[t] = fld_old[t];
+            lb.s1[t] = w.s1q[set0 + t]; lb.s2[t] = w.s2q[set0 + t]; lb.fo[t] = w.limq[set0 + t];
+          }
+          kLimScaleD<<<lim_grid, tblk(), 0, stream>>>(g, la, lb);
+        }
       };
       if (lim_theta) {
         la.opt = p.scalar_adv_opt;
         la.offset = T0;
         PROF("k_lim_scale");
-        scale_pass(s.theta, origin.theta);
+        const double *th[1] = {s.theta}, *th0[1] = {origin.theta};
+        scale_pass(1, th, th0, 0);
         LAUNCH_CHECK("k_lim_scale");
         PROF("k_lim_tend");
         // theta's tendency stays float64 (the acoustic loop reads it)
@@ -774,17 +810,18 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
       if (lim_moist) {
         la.opt = p.moist_adv_opt;
         la.offset = 0.0;
+        PROF("k_lim_scale");
+        scale_pass(6, s.q, origin.q, 0);
+        LAUNCH_CHECK("k_lim_scale");
         for (int q = 0; q < 6; ++q) {
-          PROF("k_lim_scale");
-          scale_pass(s.q[q], origin.q[q]);
-          LAUNCH_CHECK("k_lim_scale");
           PROF("k_lim_tend");
           if (mixed)
             k_lim_tend_faces<float, float><<<grd(nx, ny, nz), blk2(), 0, stream>>>(
-                g, la, limf32, s1f, s2f, nullptr, s.mu_total, reinterpret_cast<float *>(w.qtend[q]));
+                g, la, f32(w.limq[q]), reinterpret_cast<float *>(w.s1q[q]), reinterpret_cast<float *>(w.s2q[q]),
+                nullptr, s.mu_total, reinterpret_cast<float *>(w.qtend[q]));
           else
-            k_lim_tend_faces<double, double><<<grd(nx, ny, nz), blk2(), 0, stream>>>(g, la, w.limf, w.s1, w.s2,
-                                                                                   nullptr, s.mu_total, w.qtend[q]);
+            k_lim_tend_faces<double, double><<<grd(nx, ny, nz), blk2(), 0, stream>>>(
+                g, la, w.limq[q], w.s1q[q], w.s2q[q], nullptr, s.mu_total, w.qtend[q]);
           LAUNCH_CHECK("k_lim_tend");
         }
       }

@@ -237,14 +237,32 @@ struct LimMarchSmem {
   ZConst zc[2];
 };
 
+// Up to six fields limited in one launch (the moisture species of the final
+// stage): field n's current and step-start values and its scratch (scales,
+// face fluxes).  The field index is the fastest of blockIdx.x, so the fields'
+// blocks of one tile run side by side and read the tile's transport
+// velocities through L2 once.
+template <typename F>
+struct LimBatch {
+  const double *field[6], *field_old[6];
+  F *s1[6], *s2[6];
+  LimFacesT<F> fo[6];
+  int n;
+};
+
 template <typename F, int KC, bool DEG>
-__global__ void WG_LIM_BOUNDS k_lim_march(Grid g, LimArgs a, const double *field,
-                                                         const double *field_old, F *s1w, F *s2w,
-                                                         LimFacesT<F> fo) {
+__global__ void WG_LIM_BOUNDS k_lim_march(Grid g, LimArgs a, LimBatch<F> lb) {
   __shared__ LimMarchSmem sm;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TSX, j0 = blockIdx.y * TSY;
+  const int bx = blockIdx.x / lb.n, fi = blockIdx.x - bx * lb.n;
+  const double *field = pick6(lb.field, fi), *field_old = pick6(lb.field_old, fi);
+  F *s1w = pick6(lb.s1, fi), *s2w = pick6(lb.s2, fi);
+  LimFacesT<F> fo = lb.fo[0];
+#pragma unroll
+  for (int t = 1; t < 6; ++t)
+    if (fi == t) fo = lb.fo[t];
+  const int i0 = bx * TSX, j0 = blockIdx.y * TSY;
   const int k0 = blockIdx.z * KC, k1 = min(nz, k0 + KC);
   const int i = i0 + tx, j = j0 + ty;
   const bool valid = i < nx && j < ny;
