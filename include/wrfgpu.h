@@ -84,9 +84,9 @@ typedef struct wrfgpu_step_params {
   double cfn, cfn1;
   /* Kernel tile shapes (no counterpart in the reference; results do not
    * depend on them): levels per block of the level-marching stencil kernels
-   * (5, 10 or 25), level lanes of the column kernel (8, 13 or 16) and its
-   * columns per block (16 or 32); 0 selects the built-in defaults (10, 16
-   * and 32).  wrfgpu_autotune picks them per grid. */
+   * (5, 10 or 25), level lanes of the column kernel (8, 13, 16 or 17) and
+   * its columns per block (16 or 32); 0 selects the built-in defaults (10,
+   * 17 and 32).  wrfgpu_autotune picks them per grid. */
   int march_levels;
   int column_lanes;
   int column_width;

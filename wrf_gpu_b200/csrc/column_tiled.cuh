@@ -23,7 +23,7 @@ namespace wg {
 #define WG_COL_TX 32
 #endif
 #ifndef WG_COL_TY
-#define WG_COL_TY 16
+#define WG_COL_TY 17
 #endif
 #ifndef WG_COL_MINB
 #define WG_COL_MINB 2
@@ -46,7 +46,7 @@ constexpr int COL_TX_CHOICES[] = {32, 16, 1};
 #define WG_COL_DEFAULT_WIDTH 32
 #endif
 constexpr int COL_DEFAULT_WIDTH = WG_COL_DEFAULT_WIDTH;
-constexpr int COL_TY_CHOICES[] = {8, 13, 16};
+constexpr int COL_TY_CHOICES[] = {8, 13, 16, 17};
 constexpr int col_minb(int tx) { return tx == 16 ? 2 * WG_COL_MINB : WG_COL_MINB; }
 // Levels per software-pipelined batch of the serial recurrences: the batch's
 // shared-memory operands are loaded before its first store, so the loads

@@ -445,8 +445,9 @@ int wrfgpu_step_params_validate(const wrfgpu_step_params *p) {
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "unknown precision mode");
   if (p->march_levels != 0 && p->march_levels != 5 && p->march_levels != 10 && p->march_levels != 25)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "march_levels must be 0, 5, 10 or 25");
-  if (p->column_lanes != 0 && p->column_lanes != 8 && p->column_lanes != 13 && p->column_lanes != 16)
-    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13 or 16");
+  if (p->column_lanes != 0 && p->column_lanes != 8 && p->column_lanes != 13 && p->column_lanes != 16 &&
+      p->column_lanes != 17)
+    return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_lanes must be 0, 8, 13, 16 or 17");
   if (p->column_width != 0 && p->column_width != 1 && p->column_width != 16 && p->column_width != 32)
     return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "column_width must be 0, 1, 16 or 32");
   if (p->physics != 0 && p->physics != 1) return fail(WRFGPU_ERR_UNSUPPORTED_CONFIG, "physics must be 0 or 1");
@@ -988,8 +989,14 @@ int rk3_step_impl(const wrfgpu_step_params *pp, const wrfgpu_metrics *mm, const 
     const bool pins = cad || nest_ph_pin;
 #define WG_COL(TX, TY) (pins ? k_column_tiled<TX, TY, true> : k_column_tiled<TX, TY, false>)
     auto kColumn = col_stream ? (pins ? k_column_stream<true> : k_column_stream<false>)
-                   : (cwidth == 16) ? ((lanes == 8) ? WG_COL(16, 8) : (lanes == 16) ? WG_COL(16, 16) : WG_COL(16, 13))
-                                    : ((lanes == 8) ? WG_COL(32, 8) : (lanes == 16) ? WG_COL(32, 16) : WG_COL(32, 13));
+                   : (cwidth == 16) ? ((lanes == 8)    ? WG_COL(16, 8)
+                                       : (lanes == 16) ? WG_COL(16, 16)
+                                       : (lanes == 17) ? WG_COL(16, 17)
+                                                       : WG_COL(16, 13))
+                                    : ((lanes == 8)    ? WG_COL(32, 8)
+                                       : (lanes == 16) ? WG_COL(32, 16)
+                                       : (lanes == 17) ? WG_COL(32, 17)
+                                                       : WG_COL(32, 13));
 #undef WG_COL
     const dim3 col_grid = col_stream ? dim3((nx + 31) / 32, (ny + CS_WARPS - 1) / CS_WARPS, 1)
                                      : dim3((nx + cwidth - 1) / cwidth, ny, 1);
