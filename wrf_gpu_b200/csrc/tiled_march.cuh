@@ -57,13 +57,14 @@ __device__ __forceinline__ P pick6(const P (&p)[6], int n) {
 }
 
 // Resident 256-thread blocks per SM requested from the register allocator
-// (timed at 433 x 433 x 50: 6 for the scalar advection, 5 for the limiter's
-// scale pass; unset: no request).
+// (timed at 433 x 433 x 50: 6 for the scalar advection, 4 for the limiter's
+// six-species scale pass -- 2.10 vs 2.22 ms/step at 5, 2.48 at 6; unset: no
+// request).
 #ifndef WG_SCALAR_MINB
 #define WG_SCALAR_MINB 6
 #endif
 #ifndef WG_LIM_MINB
-#define WG_LIM_MINB 5
+#define WG_LIM_MINB 4
 #endif
 #ifdef WG_SCALAR_MINB
 #define WG_SCALAR_BOUNDS __launch_bounds__(TSX * TSY, WG_SCALAR_MINB)
