@@ -57,11 +57,11 @@ __device__ __forceinline__ P pick6(const P (&p)[6], int n) {
 }
 
 // Resident 256-thread blocks per SM requested from the register allocator
-// (timed at 433 x 433 x 50: 6 for the scalar advection, 4 for the limiter's
-// six-species scale pass -- 2.10 vs 2.22 ms/step at 5, 2.48 at 6; unset: no
-// request).
+// (timed at 433 x 433 x 50: 5 for the scalar advection -- 2.19 vs 2.26
+// ms/step at 6, 2.43 at 7 --, 4 for the limiter's six-species scale pass --
+// 2.10 vs 2.22 ms/step at 5, 2.48 at 6, 2.44 at 3; unset: no request).
 #ifndef WG_SCALAR_MINB
-#define WG_SCALAR_MINB 6
+#define WG_SCALAR_MINB 5
 #endif
 #ifndef WG_LIM_MINB
 #define WG_LIM_MINB 4
